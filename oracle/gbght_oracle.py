@@ -1,0 +1,529 @@
+"""CPU oracle for the GBGHomogeneousTurbulence.jl IF-RK time step.
+
+TEST INFRASTRUCTURE ONLY. This module is the checker that the CUDA library is compared against.
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may import it.
+No product path calls it, and nothing in the library falls back to it.
+
+It restates, in FP64 NumPy with ``scipy.fft``, the algorithm of the reference's hot path: the
+coupled velocity + passive-scalar integrating-factor low-storage Runge–Kutta step with 2/3-rule
+dealiasing, Leray projection, ConstantPower band forcing, and Heun (ABM(1)) tracer advection with
+Catmull–Rom interpolation. Every array is kept in the reference's own layout. That layout is the
+column-major ``(kx, ky, kz, comp)`` array of the rfft, held here row-major as ``[comp][kz][ky][kx]``
+with ``kx`` in ``[0, N/2]``. It is full-size and unpruned, so the oracle shares no layout or pruning
+decision with the CUDA kernels.
+
+Field arithmetic lives in the reference's unvendored dependency ``GBGPeriodicFields`` (uuid
+``f1da9c2b-0ac1-4736-96f9-af1c25aedab1``, compat ``0.1.0``; ``Project.toml:7,17``). Its call sites in
+the reference fix what each operation must compute. Where PF's own convention is not visible, this
+file adopts one and says so at the function.
+
+Parity pinning: the reference ships no golden fields. This restatement is pinned against the
+reference's own known-answer tests, re-expressed in ``tests/test_oracle_known_answers.py``:
+- the closed-form observables;
+- exact diffusion;
+- the RK3 and RK4 self-convergence ratios, and the order under ConstantPower;
+- injected power equal to ε, and a solenoidal state;
+- the 2/3 closed ball against a 2N zero-padded product;
+- Parseval, and the planted reality violation;
+- tracer uniform flow, wrap, constant field and Heun order;
+- the classical Adams weights.
+
+The two config extensions are parity-unpinned: the k⁴ seed spectrum, defined in the package's
+seeder, and the uniform mean scalar gradient G, defined here in ``scalar_rhs``.
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+from fractions import Fraction
+
+import numpy as np
+import scipy.fft as sfft
+
+WORKERS = os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------------------------
+# Domain: grid, wavenumbers, the 2/3 closed-ball mask.  (src/SimulationDomain.jl:295-363)
+# ---------------------------------------------------------------------------------------------
+
+def _axis_integers(N: int) -> np.ndarray:
+    """FFT-order integer wavenumbers of a full axis: 0..N/2-1, then -N/2..-1."""
+    return np.fft.fftfreq(N, d=1.0 / N).round().astype(np.int64)
+
+
+class Domain:
+    """The fixed cubic box: `FixedDomain` (src/SimulationDomain.jl:275-328), TwoThirds dealiasing.
+
+    ``cutoff`` is ``T(2/3) * T(N/2) * T(2π/L)`` evaluated left to right in FP64, as
+    `_cutoff_wavenumber` does (src/SimulationDomain.jl:342-343). The mask keeps the closed ball
+    ``|κ|² ≤ cutoff²`` with ``|κ|² = κx² + κy² + κz²`` summed in that order
+    (src/SimulationDomain.jl:349-363; closed-ball test on the squares).
+    """
+
+    def __init__(self, N: int, L: float = 2 * math.pi):
+        self.N = int(N)
+        self.L = float(L)
+        N = self.N
+        s = 2 * math.pi / self.L
+        self.k0 = s
+        self.cutoff = (2 / 3) * (N / 2) * s
+        mx = np.arange(N // 2 + 1, dtype=np.int64)
+        my = _axis_integers(N)
+        mz = _axis_integers(N)
+        self.kx = (s * mx.astype(np.float64))[None, None, :]
+        self.ky = (s * my.astype(np.float64))[None, :, None]
+        self.kz = (s * mz.astype(np.float64))[:, None, None]
+        # squared wavenumber per mode, x + y + z in that order
+        self.k2 = (self.kx * self.kx + self.ky * self.ky) + self.kz * self.kz
+        # derivative multipliers: the Nyquist mode's derivative is zero (convention; masked anyway)
+        dx = self.kx.copy()
+        dy = self.ky.copy()
+        dz = self.kz.copy()
+        if N % 2 == 0:
+            dx[..., N // 2] = 0.0
+            dy[:, N // 2, :] = 0.0
+            dz[N // 2, :, :] = 0.0
+        self.dkx, self.dky, self.dkz = dx, dy, dz
+        self.mask = (self.k2 <= self.cutoff * self.cutoff).astype(np.float64)
+        # Hermitian weights of the half spectrum: modes with 0 < kx < N/2 stand for a conjugate pair
+        w = np.full(N // 2 + 1, 2.0)
+        w[0] = 1.0
+        if N % 2 == 0:
+            w[N // 2] = 1.0
+        self.hweight = w[None, None, :]
+        self.dx = self.L / N
+        self.shape_spectral = (N, N, N // 2 + 1)
+
+    # transforms: unnormalised forward, 1/N³ inverse (docs/src/validation.md:72-74)
+    def to_spectral(self, f: np.ndarray) -> np.ndarray:
+        return sfft.rfftn(f, axes=(-3, -2, -1), workers=WORKERS)
+
+    def to_physical(self, fh: np.ndarray) -> np.ndarray:
+        N = self.N
+        return sfft.irfftn(fh, s=(N, N, N), axes=(-3, -2, -1), workers=WORKERS)
+
+    # normalised inner product: box average, via Parseval (docs/src/notation.md:19)
+    def inner(self, a: np.ndarray, b: np.ndarray, weight=None) -> float:
+        prod = (np.conj(a) * b).real * self.hweight
+        if weight is not None:
+            prod = prod * weight
+        return float(prod.sum()) / float(self.N) ** 6
+
+
+# ---------------------------------------------------------------------------------------------
+# Spectral operators (the GBGPeriodicFields call sites listed in the module docstring).
+# ---------------------------------------------------------------------------------------------
+
+def curl(dom: Domain, uh: np.ndarray) -> np.ndarray:
+    """ω̂ = iκ × û (`curl!`, src/Observables.jl:330)."""
+    ux, uy, uz = uh
+    return np.stack([
+        1j * (dom.dky * uz - dom.dkz * uy),
+        1j * (dom.dkz * ux - dom.dkx * uz),
+        1j * (dom.dkx * uy - dom.dky * ux),
+    ])
+
+
+def leray(dom: Domain, vh: np.ndarray, mask=None) -> np.ndarray:
+    """ℙ(κ) = I − κκᵀ/|κ|², optionally with the dealias mask folded in
+    (`helmholtz_projection!`, src/Generator.jl:531-532; src/Propagator.jl:401). ℙ(0) = I."""
+    k2 = dom.k2
+    safe = np.where(k2 > 0, k2, 1.0)
+    kdotv = (dom.kx * vh[0] + dom.ky * vh[1]) + dom.kz * vh[2]
+    coef = np.where(k2 > 0, kdotv / safe, 0.0)
+    out = np.stack([vh[0] - dom.kx * coef, vh[1] - dom.ky * coef, vh[2] - dom.kz * coef])
+    if mask is not None:
+        out = out * mask
+    return out
+
+
+def reality_projection(dom: Domain, fh: np.ndarray) -> np.ndarray:
+    """`reality_projection!` (src/Propagator.jl:411-412): on the kx = 0 and kx = N/2 planes,
+    replace each conjugate pair (ky, kz) ↔ (−ky, −kz) by its Hermitian part, so that
+    f̂(−k) = conj f̂(k); self-conjugate modes keep their real part (adopted convention)."""
+    N = dom.N
+    out = fh.copy()
+    planes = [0] + ([N // 2] if N % 2 == 0 else [])
+    neg = (-np.arange(N)) % N
+    for p in planes:
+        plane = out[..., p]                      # [comp?][kz][ky]
+        # the partner of (kz, ky) is (−kz, −ky)
+        flipped = plane[..., neg, :][..., :, neg]
+        out[..., p] = 0.5 * (plane + np.conj(flipped))
+    return out
+
+
+# ---------------------------------------------------------------------------------------------
+# Flow conditions, forcing, generator.  (src/Generator.jl:81-140,484-581,648-730;
+# src/Forcing.jl:110-111,435-456,1069-1117)
+# ---------------------------------------------------------------------------------------------
+
+@dataclass
+class ConstantPower:
+    """`ConstantPower(domain; injection_rate, lowest_shell, highest_shell)` (src/Forcing.jl:1069)."""
+    injection_rate: float
+    lowest_shell: int = 1
+    highest_shell: float = 2
+
+
+@dataclass
+class Conditions:
+    viscosity: float
+    schmidt: float = 1.0
+    velocity_forcing: object = None          # None (NoForcing) or ConstantPower
+    scalar: bool = True
+    mean_gradient: tuple = (0.0, 0.0, 0.0)   # extension G1: uniform mean scalar gradient G
+
+    def __post_init__(self):
+        if not self.viscosity > 0:
+            raise ValueError(f"`viscosity` must be positive, got {self.viscosity}")
+        if not self.schmidt > 0:
+            raise ValueError(f"`schmidt` must be positive, got {self.schmidt}")
+
+    @property
+    def diffusivity(self) -> float:
+        return self.viscosity / self.schmidt
+
+
+def band_indicator(dom: Domain, forcing: ConstantPower) -> np.ndarray:
+    """Shells lowest..highest, shell h covering [h − ½, h + ½)·2π/L (`_shell_edges`,
+    src/Forcing.jl:435-439); the band test is on the squares, both edges included."""
+    k0 = 2 * math.pi / dom.L
+    lo = (forcing.lowest_shell - 0.5) * k0
+    top = forcing.highest_shell if math.isfinite(forcing.highest_shell) else math.ceil(math.sqrt(3) * dom.N / 2)
+    hi = (top + 0.5) * k0
+    return ((dom.k2 >= lo * lo) & (dom.k2 <= hi * hi)).astype(np.float64)
+
+
+def constant_power_amplitude(dom: Domain, forcing: ConstantPower, uh: np.ndarray, eps_T: float):
+    """A = ε / (2 k_band), clamped to 0 when the band is empty relative to the whole field
+    (`add_forcing_source!(::ConstantPower)` src/Forcing.jl:1104-1117, `_injection_amplitude`
+    :1091-1101, `_band_is_empty` :110-111, `_target_factor` :456 with ½ for the velocity)."""
+    band = band_indicator(dom, forcing)
+    band_raw = dom.inner(uh, uh, band)
+    whole_raw = dom.inner(uh, uh)
+    band_obs = 0.5 * band_raw
+    whole_obs = 0.5 * whole_raw
+    if not (math.isfinite(band_obs) and band_obs > 10 * eps_T * whole_obs):
+        return 0.0, band
+    return forcing.injection_rate / (2 * band_obs), band
+
+
+def velocity_rhs(dom: Domain, cond: Conditions, uh, u, w, eps_T):
+    """N̂_u = 𝔻ℙ FFT(u × ω) (negated Lamb vector, operands u, ω), mean mode zeroed, plus the
+    ConstantPower source on the stage û (`velocity_rhs!` src/Generator.jl:484-488,
+    `_velocity_advective_term!` :528-534, `mean_free_projection!` :486)."""
+    ux, uy, uz = u
+    wx, wy, wz = w
+    lamb_neg = np.stack([uy * wz - uz * wy, uz * wx - ux * wz, ux * wy - uy * wx])
+    nh = dom.to_spectral(lamb_neg)
+    nh = leray(dom, nh, dom.mask)
+    nh[:, 0, 0, 0] = 0.0
+    f = cond.velocity_forcing
+    if f is not None:
+        A, band = constant_power_amplitude(dom, f, uh, eps_T)
+        nh = nh + A * band * uh
+    return nh
+
+
+def scalar_rhs(dom: Domain, cond: Conditions, uh, u, phi):
+    """N̂_φ = −𝔻 iκ·FFT(uφ) (`_scalar_flux_divergence!`, src/Generator.jl:708-720, divergence
+    with α = −1), plus the mean-gradient source −G·û (extension G1: φ_total = G·x + φ, so
+    ∂tφ + u·∇φ = −u·G + ϰ∇²φ)."""
+    flux = u * phi[None]
+    fh = dom.to_spectral(flux)
+    div = 1j * ((dom.dkx * fh[0] + dom.dky * fh[1]) + dom.dkz * fh[2])
+    nh = -(dom.mask * div)
+    G = cond.mean_gradient
+    if any(g != 0.0 for g in G):
+        nh = nh - ((G[0] * uh[0] + G[1] * uh[1]) + G[2] * uh[2])
+    return nh
+
+
+# ---------------------------------------------------------------------------------------------
+# The low-storage IF-RK step.  (src/Propagator.jl:140-150,267-274,304-419)
+# ---------------------------------------------------------------------------------------------
+
+def _rk4_tableau():
+    a = (Fraction(0), Fraction(-567301805773, 1357537059087), Fraction(-2404267990393, 2016746695238),
+         Fraction(-3550918686646, 2091501179385), Fraction(-1275806237668, 842570457699))
+    b = (Fraction(1432997174477, 9575080441755), Fraction(5161836677717, 13612068292357),
+         Fraction(1720146321549, 2090206949498), Fraction(3134564353537, 4481467310338),
+         Fraction(2277821191437, 14882151754819))
+    c = (Fraction(1432997174477, 9575080441755), Fraction(2526269341429, 6820363962896),
+         Fraction(2006345519317, 3224310063776), Fraction(2802321613138, 2924317926251))
+    af = tuple(float(x) for x in a)
+    bf = tuple(float(x) for x in b)
+    cf = tuple(float(x) for x in c)
+    # d = (c₂, c₃ − c₂, c₄ − c₃, c₅ − c₄, 1 − c₅), subtracted in T after rounding (Propagator.jl:314-319)
+    d = (cf[0], cf[1] - cf[0], cf[2] - cf[1], cf[3] - cf[2], 1.0 - cf[3])
+    return af, bf, d
+
+
+def _rk3_tableau():
+    a = (0.0, float(Fraction(-5, 9)), float(Fraction(-153, 128)))
+    b = (float(Fraction(1, 3)), float(Fraction(15, 16)), float(Fraction(8, 15)))
+    d = (float(Fraction(1, 3)), float(Fraction(5, 12)), float(Fraction(1, 4)))
+    return a, b, d
+
+
+TABLEAUX = {"rk4": _rk4_tableau(), "rk3": _rk3_tableau()}
+
+
+@dataclass
+class State:
+    uh: np.ndarray                  # (3, N, N, N/2+1) complex128
+    phih: np.ndarray | None = None  # (N, N, N/2+1) complex128
+
+
+def step(dom: Domain, cond: Conditions, st: State, dt: float, scheme: str = "rk4") -> State:
+    """One step of `_low_storage_2n_step!` (src/Propagator.jl:326-419) with scheme "rk4"
+    (`IFLowStorageRK4`, :304-320) or "rk3" (`IFLowStorageRK3`, :267-274)."""
+    a, b, d = TABLEAUX[scheme]
+    eps_T = np.finfo(np.float64).eps
+    uh = st.uh.copy()
+    ph = None if st.phih is None else st.phih.copy()
+    has_scalar = ph is not None
+    hu = None
+    hp = None
+    dt = float(dt)
+    for i in range(len(a)):
+        u = dom.to_physical(uh)
+        w = dom.to_physical(curl(dom, uh))
+        nu_ = velocity_rhs(dom, cond, uh, u, w, eps_T)
+        if has_scalar:
+            phi = dom.to_physical(ph)
+            np_ = scalar_rhs(dom, cond, uh, u, phi)
+        hu = dt * nu_ if i == 0 else a[i] * hu + dt * nu_
+        E = np.exp((-(cond.viscosity * (d[i] * dt))) * dom.k2)
+        uh = E * (uh + b[i] * hu)
+        if i < len(a) - 1:
+            hu = E * hu
+        if has_scalar:
+            hp = dt * np_ if i == 0 else a[i] * hp + dt * np_
+            Ep = np.exp((-(cond.diffusivity * (d[i] * dt))) * dom.k2)
+            ph = Ep * (ph + b[i] * hp)
+            if i < len(a) - 1:
+                hp = Ep * hp
+    uh = leray(dom, uh)
+    uh = reality_projection(dom, uh)
+    if has_scalar:
+        ph = reality_projection(dom, ph)
+    return State(uh, ph)
+
+
+# ---------------------------------------------------------------------------------------------
+# Deposit, max speed, CFL.  (src/Propagator.jl:808-842; src/Observables.jl:304-305;
+# src/SimulationRun.jl:1051-1096)
+# ---------------------------------------------------------------------------------------------
+
+def deposit(dom: Domain, st: State):
+    """u, ω (and φ) in physical representation, and max|u| = √max(|u|²)."""
+    u = dom.to_physical(st.uh)
+    w = dom.to_physical(curl(dom, st.uh))
+    phi = None if st.phih is None else dom.to_physical(st.phih)
+    speed = math.sqrt(float(np.max((u[0] * u[0] + u[1] * u[1]) + u[2] * u[2])))
+    return u, w, phi, speed
+
+
+def cfl_timestep(dom: Domain, cond: Conditions, speed: float, cfl: float, max_dt: float = math.inf):
+    """Δt = min(C·Δx/max|u|, 1/(D·κ_min²), max_dt) (src/SimulationRun.jl:1051-1096)."""
+    if not math.isfinite(speed):
+        raise FloatingPointError("non-finite velocity: the run appears to have blown up")
+    dx = dom.L / dom.N
+    advective = cfl * dx / speed if speed > 0 else cfl * dx
+    D = max(cond.viscosity, cond.diffusivity) if cond.scalar else cond.viscosity
+    kmin = 2 * math.pi / dom.L
+    resolution = 1 / (D * kmin ** 2)
+    return min(advective, resolution, max_dt)
+
+
+# ---------------------------------------------------------------------------------------------
+# Tracers.  (src/Particles.jl:135-176,290-293; src/ParticlePropagator.jl:263-386)
+# ---------------------------------------------------------------------------------------------
+
+GAUSS_NODES = (-0.8611363115940526, -0.3399810435848563, 0.3399810435848563, 0.8611363115940526)
+GAUSS_WEIGHTS = (0.3478548451374538, 0.6521451548625461, 0.6521451548625461, 0.3478548451374538)
+
+
+def adams_weights(nodes, h):
+    """Integral over [0, h] of each Lagrange basis polynomial through `nodes`, by 4-point
+    Gauss–Legendre (`_adams_weights`, src/ParticlePropagator.jl:263-280)."""
+    n = len(nodes)
+    out = []
+    for j in range(n):
+        weight = 0.0
+        for xi, w in zip(GAUSS_NODES, GAUSS_WEIGHTS):
+            t = h * (xi + 1) / 2
+            basis = 1.0
+            for m in range(n):
+                if m == j:
+                    continue
+                basis *= (t - nodes[m]) / (nodes[j] - nodes[m])
+            weight += w * h / 2 * basis
+        out.append(weight)
+    return tuple(out)
+
+
+def wrap(x: np.ndarray, L: float) -> np.ndarray:
+    """Periodic reduction into [0, L): x − L·floor(x/L), a tiny negative result lifted by L, and
+    a result equal to L mapped to 0 (adopted convention for PF's `displace!` wrap)."""
+    y = x - L * np.floor(x / L)
+    y = np.where(y < 0.0, y + L, y)
+    return np.where(y >= L, 0.0, y)
+
+
+def catmull_rom_weights(t: np.ndarray):
+    """Catmull–Rom (Catmull & Rom 1974; Lalescu's 4-point C¹ kernel) weights for taps
+    i−1, i, i+1, i+2 at fraction t ∈ [0, 1)."""
+    wm1 = t * (t * (2.0 - t) - 1.0) * 0.5
+    w0 = (t * t * (3.0 * t - 5.0) + 2.0) * 0.5
+    w1 = t * (t * (4.0 - 3.0 * t) + 1.0) * 0.5
+    w2 = t * t * (t - 1.0) * 0.5
+    return (wm1, w0, w1, w2)
+
+
+def cell_and_fraction(x: np.ndarray, dx: float):
+    q = x / dx
+    i = np.floor(q)
+    return i.astype(np.int64), q - i
+
+
+def interpolate(dom: Domain, f: np.ndarray, X: np.ndarray) -> np.ndarray:
+    """CatmullRom (= LalescuSpline(4)) gather of the physical field f ([comp][z][y][x] or
+    [z][y][x]) at positions X (3, M) (`interpolate!`, src/Particles.jl:290-293). The sum runs
+    x innermost, then y, then z."""
+    N = dom.N
+    scalar = f.ndim == 3
+    comps = f[None] if scalar else f
+    ix, tx = cell_and_fraction(X[0], dom.dx)
+    iy, ty = cell_and_fraction(X[1], dom.dx)
+    iz, tz = cell_and_fraction(X[2], dom.dx)
+    wx, wy, wz = catmull_rom_weights(tx), catmull_rom_weights(ty), catmull_rom_weights(tz)
+    out = np.zeros((comps.shape[0], X.shape[1]))
+    for c in range(comps.shape[0]):
+        fc = comps[c]
+        acc_z = np.zeros(X.shape[1])
+        for cz in range(4):
+            zz = (iz + cz - 1) % N
+            acc_y = np.zeros(X.shape[1])
+            for cy in range(4):
+                yy = (iy + cy - 1) % N
+                acc_x = np.zeros(X.shape[1])
+                for cx in range(4):
+                    xx = (ix + cx - 1) % N
+                    acc_x = acc_x + wx[cx] * fc[zz, yy, xx]
+                acc_y = acc_y + wy[cy] * acc_x
+            acc_z = acc_z + wz[cz] * acc_y
+        out[c] = acc_z
+    return out[0] if scalar else out
+
+
+def advect_heun(dom: Domain, X: np.ndarray, f0: np.ndarray, u_new: np.ndarray, h: float):
+    """Heun = ABM(1) (src/ParticlePropagator.jl:165,288-315): X* = wrap(X + b₀f₀); f* = u(X*);
+    X ← wrap(X* + (β₀f* + (β₁ − b₀)f₀)). Each displacement is summed term by term, then added."""
+    (b0,) = adams_weights((0.0,), h)
+    Xs = wrap(X + b0 * f0, dom.L)
+    fstar = interpolate(dom, u_new, Xs)
+    beta = adams_weights((h, 0.0), h)
+    disp = beta[0] * fstar + (beta[1] - b0) * f0
+    return wrap(Xs + disp, dom.L), fstar
+
+
+# ---------------------------------------------------------------------------------------------
+# Observables and spectra.  (src/Observables.jl:84-173,345-370,502-514)
+# ---------------------------------------------------------------------------------------------
+
+def kinetic_energy(dom, uh):
+    return dom.inner(uh, uh) / 2
+
+
+def dissipation(dom, uh, nu):
+    return nu * dom.inner(uh, uh, dom.k2)
+
+
+def scalar_variance(dom, ph):
+    return dom.inner(ph, ph)
+
+
+def scalar_dissipation(dom, ph, kappa):
+    return 2 * kappa * dom.inner(ph, ph, dom.k2)
+
+
+def n_shells(N: int) -> int:
+    return int(math.floor(math.sqrt(3) * N / 2 + 0.5)) + 1
+
+
+def radial_spectrum(dom: Domain, fh: np.ndarray) -> np.ndarray:
+    """Shell sums of the Hermitian-weighted |f̂|²/N⁶, shell n = floor(|κ|/Δκ + ½) (shells
+    [n − ½, n + ½) as in `_shell_edges`, src/Forcing.jl:435-439)."""
+    dk = 2 * math.pi / dom.L
+    shell = np.floor(np.sqrt(dom.k2) / dk + 0.5).astype(np.int64)
+    p = (np.abs(fh) ** 2) * dom.hweight
+    if p.ndim == 4:
+        p = p.sum(axis=0)
+    out = np.zeros(n_shells(dom.N))
+    np.add.at(out, np.broadcast_to(shell, p.shape).ravel(), p.ravel())
+    return out / float(dom.N) ** 6
+
+
+def energy_spectrum(dom, uh):
+    """E(κ) = radial_spectrum/(2Δκ) (src/Observables.jl:502-514)."""
+    dk = 2 * math.pi / dom.L
+    return radial_spectrum(dom, uh) / (2 * dk)
+
+
+def scalar_spectrum(dom, ph):
+    """E_φ(κ) = radial_spectrum/Δκ (no reference function; the variance convention, no ½)."""
+    dk = 2 * math.pi / dom.L
+    return radial_spectrum(dom, ph) / dk
+
+
+# ---------------------------------------------------------------------------------------------
+# Run layer: one iteration of `advance!` (src/SimulationRun.jl:1155-1229).
+# ---------------------------------------------------------------------------------------------
+
+@dataclass
+class Run:
+    dom: Domain
+    cond: Conditions
+    state: State
+    X: np.ndarray | None = None       # (3, M) tracer positions
+    scheme: str = "rk4"
+    cfl: float = 0.5
+    max_dt: float = math.inf
+    time: float = 0.0
+    nstep: int = 0
+    u: np.ndarray = field(default=None, repr=False)
+    speed: float = 0.0
+    f0: np.ndarray | None = None
+    trail_time: float = 0.0
+
+    def __post_init__(self):
+        self.u, _, _, self.speed = deposit(self.dom, self.state)
+        if self.X is not None:
+            self.f0 = interpolate(self.dom, self.u, self.X)
+            self.trail_time = self.time
+
+    def advance(self, dt: float | None = None):
+        D = cfl_timestep(self.dom, self.cond, self.speed, self.cfl, self.max_dt) if dt is None else float(dt)
+        if not (math.isfinite(D) and D > 0):
+            raise ValueError(f"the timestep must be positive and finite, got {D}")
+        t_new = self.time + D
+        if not t_new > self.time:
+            raise ValueError(f"the timestep {D} is too small to advance the clock")
+        self.state = step(self.dom, self.cond, self.state, D, self.scheme)
+        self.u, _, _, self.speed = deposit(self.dom, self.state)
+        if self.X is not None:
+            self.X, _ = advect_heun(self.dom, self.X, self.f0, self.u, D)
+            self.f0 = interpolate(self.dom, self.u, self.X)
+            self.trail_time = t_new
+        if not math.isfinite(self.speed):
+            raise FloatingPointError(f"non-finite velocity at step {self.nstep + 1}")
+        if self.state.phih is not None and not math.isfinite(scalar_variance(self.dom, self.state.phih)):
+            raise FloatingPointError(f"non-finite scalar at step {self.nstep + 1}")
+        self.time = t_new
+        self.nstep += 1
+        return D

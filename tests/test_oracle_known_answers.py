@@ -1,0 +1,337 @@
+"""Pin the CPU oracle against the reference's own known-answer tests, re-expressed in NumPy.
+
+Each test cites the reference test it restates. These run on the CPU only; they make the oracle
+trustworthy before any GPU result is compared with it.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import gbght_oracle as O
+from gbght import seed as S
+
+TWO_PI = 2 * math.pi
+
+
+def _grid(N, L=TWO_PI):
+    x = np.arange(N) * (L / N)
+    z3, y3, x3 = np.meshgrid(x, x, x, indexing="ij")
+    return x3, y3, z3
+
+
+def diffnorm(a, b):
+    return math.sqrt(float(np.sum(np.abs(a - b) ** 2)))
+
+
+# --- test/observables_analytic.jl:43-88 -----------------------------------------------------------
+
+def test_observables_closed_forms():
+    N, A, B, C, D, nu, kap = 16, 0.7, -0.4, 1.1, 0.9, 0.03, 0.05
+    dom = O.Domain(N)
+    x, y, z = _grid(N)
+    u = np.stack([A * np.sin(y), B * np.sin(z), C * np.sin(x)])
+    phi = D * np.sin(x)
+    uh, ph = dom.to_spectral(u), dom.to_spectral(phi)
+    sq = A * A + B * B + C * C
+    assert O.kinetic_energy(dom, uh) == pytest.approx(sq / 4, rel=1e-13)
+    assert O.dissipation(dom, uh, nu) == pytest.approx(nu * sq / 2, rel=1e-13)
+    assert O.scalar_variance(dom, ph) == pytest.approx(D * D / 2, rel=1e-13)
+    assert O.scalar_dissipation(dom, ph, kap) == pytest.approx(kap * D * D, rel=1e-13)
+    E = O.energy_spectrum(dom, uh)
+    assert E[1] == pytest.approx(sq / 4, rel=1e-13)
+    assert E.sum() == pytest.approx(E[1], rel=1e-13)
+    _, _, _, speed = O.deposit(dom, O.State(uh, ph))
+    assert speed == pytest.approx(math.sqrt(sq), rel=1e-13)
+
+
+def test_mask_is_zero_one_and_cutoff():
+    # test/dealiasing.jl:14-20; test/observables_analytic.jl:96-103
+    for N in (12, 16, 48):
+        dom = O.Domain(N)
+        assert set(np.unique(dom.mask)) <= {0.0, 1.0}
+        assert dom.cutoff == pytest.approx((2 / 3) * (N / 2), rel=1e-14)
+    # N = 48: the cutoff rounds to exactly 16 and |κ|² = 256 lies on the closed ball's edge
+    dom = O.Domain(48)
+    assert dom.cutoff == 16.0
+    assert dom.mask[0, 0, 16] == 1.0 and dom.mask[0, 0, 17] == 0.0
+
+
+def test_parseval_spectrum_sums_to_energy():
+    # test/validation.jl:13-36
+    dom = O.Domain(32)
+    uh = S.seed_velocity(32, 0.7, seed=3)
+    E = O.energy_spectrum(dom, uh)
+    assert E.sum() * dom.k0 == pytest.approx(O.kinetic_energy(dom, uh), rel=1e-13)
+    ph = S.seed_scalar(32, 0.4, seed=4)
+    assert O.scalar_spectrum(dom, ph).sum() == pytest.approx(O.scalar_variance(dom, ph), rel=1e-13)
+
+
+# --- test/scalar.jl ----------------------------------------------------------------------------
+
+@pytest.mark.parametrize("scheme", ["rk3", "rk4"])
+def test_exact_diffusion_zero_velocity(scheme):
+    # test/scalar.jl:42-60: with u = 0 the scalar decays by the integrating factor alone
+    N, nu, Sc = 16, 0.1, 0.7
+    dom = O.Domain(N)
+    cond = O.Conditions(viscosity=nu, schmidt=Sc)
+    ph0 = S.seed_scalar(N, 1.0, seed=3)
+    st = O.State(np.zeros((3,) + dom.shape_spectral, complex), ph0.copy())
+    dt, n = 0.02, 25
+    for _ in range(n):
+        st = O.step(dom, cond, st, dt, scheme)
+    expected = ph0 * np.exp(-(nu / Sc) * dom.k2 * dt * n)
+    assert diffnorm(st.phih, expected) / math.sqrt(float(np.sum(np.abs(expected) ** 2))) < 1e-10
+
+
+def test_scalar_rhs_mean_exactly_zero():
+    # test/scalar.jl:95-118
+    N = 16
+    dom = O.Domain(N)
+    uh = S.seed_velocity(N, 0.5, seed=7)
+    ph = S.seed_scalar(N, 1.0, seed=8)
+    ph[0, 0, 0] = 3.0
+    u, phi = dom.to_physical(uh), dom.to_physical(ph)
+    nh = O.scalar_rhs(dom, O.Conditions(viscosity=0.05), uh, u, phi)
+    assert nh[0, 0, 0] == 0
+
+
+def test_scalar_mean_conserved():
+    # test/scalar.jl:80-93 (forcing aside: the scalar mean mode is untouched by the advection)
+    N = 16
+    dom = O.Domain(N)
+    cond = O.Conditions(viscosity=0.1)
+    ph = S.seed_scalar(N, 1.0, seed=6)
+    ph[0, 0, 0] = 3.0
+    st = O.State(S.seed_velocity(N, 0.5, seed=5), ph)
+    for _ in range(30):
+        st = O.step(dom, cond, st, 0.02, "rk4")
+    assert st.phih[0, 0, 0] == pytest.approx(3.0, rel=1e-13)
+
+
+# --- test/integrators.jl -----------------------------------------------------------------------
+
+def _integrate(dom, cond, uh0, ph0, dt, n, scheme):
+    st = O.State(uh0.copy(), None if ph0 is None else ph0.copy())
+    for _ in range(n):
+        st = O.step(dom, cond, st, dt, scheme)
+    return st
+
+
+def test_rk3_self_convergence_ratio():
+    # test/integrators.jl:49-78 and test/scalar.jl:63-78
+    N = 16
+    dom = O.Domain(N)
+    cond = O.Conditions(viscosity=0.1)
+    uh0, ph0 = S.seed_velocity(N, 0.5, seed=1), S.seed_scalar(N, 1.0, seed=2)
+    T, n = 0.4, 8
+    p1 = _integrate(dom, cond, uh0, ph0, T / n, n, "rk3")
+    p2 = _integrate(dom, cond, uh0, ph0, T / (2 * n), 2 * n, "rk3")
+    p4 = _integrate(dom, cond, uh0, ph0, T / (4 * n), 4 * n, "rk3")
+    assert 5.0 < diffnorm(p1.uh, p2.uh) / diffnorm(p2.uh, p4.uh) < 12.0
+    assert 5.0 < diffnorm(p1.phih, p2.phih) / diffnorm(p2.phih, p4.phih) < 12.0
+
+
+def test_rk4_self_convergence_ratio():
+    # test/integrators.jl:165-188
+    N = 32
+    dom = O.Domain(N)
+    cond = O.Conditions(viscosity=0.02)
+    uh0 = S.seed_velocity(N, 0.5, seed=7)
+    T, n = 0.5, 8
+    u1 = _integrate(dom, cond, uh0, None, T / n, n, "rk4")
+    u2 = _integrate(dom, cond, uh0, None, T / (2 * n), 2 * n, "rk4")
+    u4 = _integrate(dom, cond, uh0, None, T / (4 * n), 4 * n, "rk4")
+    assert 10.0 < diffnorm(u1.uh, u2.uh) / diffnorm(u2.uh, u4.uh) < 26.0
+
+
+@pytest.mark.parametrize("scheme,floor", [("rk3", 2.5), ("rk4", 3.5)])
+def test_order_kept_under_constant_power(scheme, floor):
+    # test/integrators.jl:132-162: a state-dependent forcing through the per-stage source keeps
+    # the scheme's order (measured ≥ 2.5 for RK3; RK4 held to ≥ 3.5 here)
+    N = 16
+    dom = O.Domain(N)
+    cond = O.Conditions(viscosity=0.05, velocity_forcing=O.ConstantPower(0.2))
+    uh0 = S.seed_velocity(N, 0.5, seed=7)
+    T = 0.2
+    ref = _integrate(dom, cond, uh0, None, T / 1024, 1024, scheme).uh
+    e32 = np.max(np.abs(_integrate(dom, cond, uh0, None, T / 32, 32, scheme).uh - ref))
+    e64 = np.max(np.abs(_integrate(dom, cond, uh0, None, T / 64, 64, scheme).uh - ref))
+    assert math.log2(e32 / e64) >= floor
+
+
+# --- test/forcing.jl ---------------------------------------------------------------------------
+
+def test_constant_power_injects_its_rate():
+    # test/forcing.jl:92-104: ⟨û, f⟩ = ε at rtol 1e-8
+    N = 24
+    dom = O.Domain(N)
+    uh = S.seed_velocity(N, 0.5, seed=11)
+    f = O.ConstantPower(0.3)
+    A, band = O.constant_power_amplitude(dom, f, uh, np.finfo(float).eps)
+    assert dom.inner(uh, A * band * uh) == pytest.approx(0.3, rel=1e-8)
+
+
+def test_constant_power_bounded_and_solenoidal():
+    # test/forcing.jl:115-122
+    N = 24
+    dom = O.Domain(N)
+    cond = O.Conditions(viscosity=0.05, velocity_forcing=O.ConstantPower(0.5))
+    st = _integrate(dom, cond, S.seed_velocity(N, 0.5, seed=11), None, 0.01, 100, "rk3")
+    k = O.kinetic_energy(dom, st.uh)
+    assert math.isfinite(k) and k > 0
+    div = (dom.kx * st.uh[0] + dom.ky * st.uh[1]) + dom.kz * st.uh[2]
+    assert math.sqrt(float(np.sum(np.abs(div) ** 2))) / math.sqrt(float(np.sum(np.abs(st.uh) ** 2))) < 1e-8
+
+
+def test_empty_band_clamps_amplitude():
+    # src/Forcing.jl:110-111,1091-1101: a band holding nothing gets A = 0, never an unbounded kick
+    N = 16
+    dom = O.Domain(N)
+    uh = S.seed_velocity(N, 0.5, seed=2)
+    band = O.band_indicator(dom, O.ConstantPower(0.1))
+    uh = uh * (1 - band)
+    A, _ = O.constant_power_amplitude(dom, O.ConstantPower(0.1), uh, np.finfo(float).eps)
+    assert A == 0.0
+
+
+# --- test/regressions/r6-inclusive-ball-exact.jl -------------------------------------------------
+
+def test_closed_ball_exact_against_zero_padded_product():
+    Np = 12
+    d1, d2 = O.Domain(Np), O.Domain(2 * Np)
+    uh = S.seed_velocity(Np, 0.5, seed=3)
+    rng = np.random.default_rng(11)
+    populated = 0
+    for i3 in range(Np):
+        for i2 in range(Np):
+            for i1 in range(Np // 2 + 1):
+                k = np.array([i1, O._axis_integers(Np)[i2], O._axis_integers(Np)[i3]], float)
+                if int(k @ k) != 16:
+                    continue
+                c = rng.standard_normal(3) + 1j * rng.standard_normal(3)
+                c = c - k * (k @ c) / 16
+                uh[:, i3, i2, i1] = 0.4 * c
+                populated += 1
+    assert populated == 5
+
+    def mapidx(i):
+        return i if i <= Np // 2 else i + Np
+
+    def term(dom, vh):
+        u = dom.to_physical(vh)
+        w = dom.to_physical(O.curl(dom, vh))
+        ln = np.stack([u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]])
+        return O.leray(dom, dom.to_spectral(ln))
+
+    big = np.zeros((3,) + d2.shape_spectral, complex)
+    for i3 in range(Np):
+        for i2 in range(Np):
+            big[:, mapidx(i3), mapidx(i2), : Np // 2 + 1] = 8 * uh[:, i3, i2, :]
+    raw = term(d1, uh)
+    full = term(d2, big)
+    oracle = np.zeros_like(raw)
+    for i3 in range(Np):
+        for i2 in range(Np):
+            oracle[:, i3, i2, :] = full[:, mapidx(i3), mapidx(i2), : Np // 2 + 1] / 8
+    kmag = np.sqrt(d1.k2)
+    ref = np.max(np.abs(oracle))
+    inside = kmag < 4 - 1e-9
+    on = np.abs(kmag - 4) < 1e-9
+    assert np.max(np.abs(raw - oracle) * inside) / ref < 1e-12
+    assert np.max(np.abs(raw - oracle) * on) / ref < 1e-12
+
+
+# --- test/regressions/r7-reality-projection-forced-run.jl -----------------------------------------
+
+def test_planted_anti_hermitian_pair_removed_by_one_step():
+    N = 16
+    dom = O.Domain(N)
+    uh = S.seed_velocity(N, 0.5, seed=1)
+    ph = S.seed_scalar(N, 0.5, seed=2)
+    d = 2e-6 * np.max(np.abs(uh[:, :, :, 0]))
+    uh[:, 0, 1, 0] += 1j * d
+    uh[:, 0, N - 1, 0] += 1j * d
+    ph[0, 1, 0] += 1j * d
+    ph[0, N - 1, 0] += 1j * d
+    st = O.step(dom, O.Conditions(viscosity=0.05, velocity_forcing=O.ConstantPower(0.1)), O.State(uh, ph), 0.01)
+    for f in (st.uh, st.phih):
+        plane = f[..., 0]
+        neg = (-np.arange(N)) % N
+        partner = np.conj(plane[..., neg, :][..., :, neg])
+        assert np.max(np.abs(plane - partner)) == 0.0
+
+
+# --- test/particles.jl -------------------------------------------------------------------------
+
+def test_adams_weights_classical():
+    # test/particles.jl:194-214
+    def nodes(k):
+        return tuple(-(i - 0.0) for i in range(k))
+    assert np.allclose(O.adams_weights(nodes(1), 1.0), [1.0])
+    assert np.allclose(O.adams_weights(nodes(2), 1.0), np.array([3, -1]) / 2)
+    assert np.allclose(O.adams_weights(nodes(4), 1.0), np.array([55, -59, 37, -9]) / 24)
+    assert np.allclose(O.adams_weights((1.0,) + nodes(1), 1.0), np.array([1, 1]) / 2)
+    assert np.allclose(O.adams_weights((1.0,) + nodes(2), 1.0), np.array([5, 8, -1]) / 12)
+
+
+def test_tracers_uniform_flow_exact_and_wrap():
+    # test/particles.jl:94-121
+    N = 16
+    dom = O.Domain(N)
+    X0 = np.array([[0.1, 1.0, 2.0], [0.2, 2.0, 3.0], [0.3, 3.0, 4.0]]).T.copy()  # (3, M)
+    u = np.zeros((3, N, N, N))
+    u[0] = 0.5
+    X, f0 = X0.copy(), O.interpolate(dom, u, X0)
+    for _ in range(20):
+        X, _ = O.advect_heun(dom, X, f0, u, 0.005)
+        f0 = O.interpolate(dom, u, X)
+    assert np.allclose(X[0], np.mod(X0[0] + 0.5 * 20 * 0.005, TWO_PI))
+    assert np.allclose(X[1:], X0[1:])
+    X = np.full((3, 1), 6.2)
+    u[0] = 1.0
+    f0 = O.interpolate(dom, u, X)
+    for _ in range(30):
+        X, _ = O.advect_heun(dom, X, f0, u, 0.02)
+        f0 = O.interpolate(dom, u, X)
+    assert np.all((X >= 0) & (X < TWO_PI))
+
+
+def test_constant_field_interpolates_exactly():
+    # test/particles.jl:134-140
+    N = 16
+    dom = O.Domain(N)
+    X = S.seed_tracers(200, seed=5)
+    f = np.full((N, N, N), 1.7)
+    assert np.allclose(O.interpolate(dom, f, X), 1.7, rtol=1e-14)
+
+
+def test_heun_second_order_on_straining_flow():
+    # test/particles.jl:24-60,216-231: u_x = cos(ωt)·s·(x − x_c), a field Catmull–Rom reproduces
+    N, s, w, xc, x0 = 16, 1.0, 3.0, math.pi, math.pi + 0.4
+    dom = O.Domain(N)
+
+    def exact(t):
+        return xc + (x0 - xc) * math.exp(s * math.sin(w * t) / w)
+
+    def field(t):
+        u = np.zeros((3, N, N, N))
+        xs = np.arange(N) * dom.dx
+        u[0] = (math.cos(w * t) * s * (xs - xc))[None, None, :]
+        return u
+
+    def err(n):
+        h = 2.0 / n
+        X = np.array([[x0], [1.0], [1.0]])
+        f0 = O.interpolate(dom, field(0.0), X)
+        t, largest = 0.0, 0.0
+        for _ in range(n):
+            un = field(t + h)
+            X, _ = O.advect_heun(dom, X, f0, un, h)
+            t += h
+            f0 = O.interpolate(dom, un, X)
+            largest = max(largest, abs(X[0, 0] - exact(t)))
+        return largest
+
+    e = [err(n) for n in (64, 128, 256)]
+    assert abs(math.log2(e[1] / e[2]) - 2.0) < 0.5
