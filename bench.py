@@ -1,0 +1,395 @@
+"""Benchmark: 512³ forced velocity + scalar IF-RK4 steps/s on one B200 (replicas on N GPUs).
+
+Workload (the headline configuration): a 512³ periodic box, ν = ϰ = 8.5e-4 (Sc = 1),
+ConstantPower forcing ε = 0.1 on shells 1–2 (|k| ≤ 2.5), uniform mean scalar gradient G = 1
+along x, 10⁶ uniform-random tracers advected by Heun with Catmull–Rom interpolation, IF-RK4 at
+CFL 0.5. Synthetic seeded start: k⁴exp(−2(k/4)²) spectrum, k = 0.5, ⟨φ²⟩ = 0.5. A step is one
+full iteration of the run layer (`advance!`): the 5-stage field step, the closing deposit, the
+tracer push and particle deposit, and the blow-up guards.
+
+`value` is steps/s of the plain FP64 form with the state resident in HBM, timed with CUDA events
+on the library's own stream. The FP32-mixed form is measured on the same workload and reported
+beside it. `e2e` is timed through the public API from pinned host buffers: the state upload, the
+K steps and the state download. Under torchrun every rank runs its own replica (the path does
+not shard), and the timed region is the max over ranks.
+
+--impl reference times the CPU restatement of the reference's step (NumPy + scipy.fft on all host
+cores) on a bounded sample of the same workload: one RK4 stage of the 512³ step per sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "gbghomogeneousturbulence.jl_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "512³ IF-RK4 steps/s, FP32-mixed vs FP64 on one B200 at ≤1e-5 spectrum err"
+WORKLOAD = dict(N=512, viscosity=8.5e-4, schmidt=1.0, injection_rate=0.1, shells=(1, 2), G=(1.0, 0.0, 0.0),
+                tracers=1_000_000, cfl=0.5, scheme="IFLowStorageRK4")
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+def _config(args, N):
+    return {"workload": f"{N}^3 forced velocity+scalar IF-RK4, nu=kappa={WORKLOAD['viscosity']}, "
+                        f"ConstantPower eps={WORKLOAD['injection_rate']} |k|<=2.5, G=1 along x, "
+                        f"{args.tracers} Heun/Catmull-Rom tracers, CFL {WORKLOAD['cfl']}",
+            "grid": N, "tracers": args.tracers, "scheme": "IFLowStorageRK4", "dealiasing": "2/3 closed ball",
+            "start": "seeded k^4 spectrum (synthetic), not a stationary state",
+            "l2": "inputs larger than L2 (state alone >= 1.3 GB)",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+# ------------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int, path: str | None):
+        self.device, self.path, self.proc = device, path, None
+
+    def __enter__(self):
+        try:
+            self.out = open(self.path, "w") if self.path else subprocess.PIPE
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.text = ""
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        if self.path:
+            self.out.close()
+            with open(self.path) as f:
+                self.text = f.read()
+        else:
+            self.text = out or ""
+
+    def summary(self):
+        rows = []
+        for line in self.text.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------------------------
+# our arm
+# ------------------------------------------------------------------------------------------------
+def algorithmic_bytes_per_step(N, K, w_complex, has_scalar=True):
+    """Bytes each kernel kind must move per step (the pruned transform design: inputs plus
+    outputs over the retained box, kx ∈ [0, K], ky', kz' ∈ [−K, K])."""
+    KX1, NY2 = K + 1, 2 * K + 1
+    S = 5
+    ninv, nfwd = (7, 6) if has_scalar else (6, 3)
+    b = {}
+    b["y_inverse"] = (S * ninv + 3) * N * KX1 * (NY2 + N) * w_complex
+    b["x_products"] = S * N * N * KX1 * (ninv + nfwd) * w_complex
+    b["y_forward"] = S * nfwd * N * KX1 * (N + NY2) * w_complex
+    nst = 4 if has_scalar else 3
+    state_rw = (S * nst + (S - 1) * nst + S * nst + (S - 1) * nst) * NY2 * NY2 * KX1 * w_complex
+    b["z_epilogue"] = S * (nfwd + ninv) * N * NY2 * KX1 * w_complex + state_rw
+    b["x_velocity"] = 3 * N * N * KX1 * w_complex + 3 * N ** 3 * (w_complex // 2)
+    return b
+
+
+def launches_per_step(has_scalar=True, forced=True):
+    return {"y_inverse": 6, "x_products": 5, "y_forward": 5, "z_epilogue": 5, "x_velocity": 1,
+            "force_amp": 5 if forced else 0, "reality": 1, "tracers": 1, "observables": 1 if has_scalar else 0}
+
+
+def make_inputs(N, M, seed_base=0):
+    from gbght import seed as S
+    uh = S.seed_velocity(N, 0.5, seed=seed_base + 0)
+    ph = S.seed_scalar(N, 0.5, seed=seed_base + 1)
+    X = S.seed_tracers(M, seed=seed_base + 2)
+    return uh, ph, X
+
+
+def pinned_like(a):
+    """A NumPy view of pinned (page-locked) host memory holding a copy of `a`."""
+    import torch
+    t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+    v = t.numpy().view(a.dtype).reshape(a.shape)
+    v[...] = a
+    return v, t
+
+
+def run_form(args, precision, device, inputs, timed=True):
+    import gbght
+    N, M = args.grid, args.tracers
+    uh, ph, X = inputs
+    setup = gbght.Setup(grid_points_per_axis=N, viscosity=WORKLOAD["viscosity"], schmidt=WORKLOAD["schmidt"],
+                        velocity_forcing=gbght.ConstantPower(WORKLOAD["injection_rate"], *WORKLOAD["shells"]),
+                        mean_gradient=WORKLOAD["G"], tracers=M, cfl=WORKLOAD["cfl"], precision=precision,
+                        device=device)
+    run = gbght.simulation(setup, uh, ph, X)
+    for _ in range(args.warmup):
+        run.advance(None)
+    return run
+
+
+def timed_steps(run, K, sampler=None):
+    run.synchronize()
+    run.profile(True)
+    run.timer_start()
+    for _ in range(K):
+        run.advance(None)
+    ms = run.timer_stop()
+    prof = run.profile_read()
+    run.profile(False)
+    return ms, prof
+
+
+def e2e_run(args, precision, device, inputs, K):
+    """Through the public API from pinned host buffers: upload the state and tracers, K steps with
+    their per-step host readbacks, download the final state."""
+    import gbght
+    N, M = args.grid, args.tracers
+    uh, ph, X = inputs
+    puh, t1 = pinned_like(uh)
+    pph, t2 = pinned_like(ph)
+    pX, t3 = pinned_like(X)
+    out_u = np.empty_like(uh)
+    out_p = np.empty_like(ph)
+    pu, t4 = pinned_like(out_u)
+    pp, t5 = pinned_like(out_p)
+    setup = gbght.Setup(grid_points_per_axis=N, viscosity=WORKLOAD["viscosity"], schmidt=WORKLOAD["schmidt"],
+                        velocity_forcing=gbght.ConstantPower(WORKLOAD["injection_rate"], *WORKLOAD["shells"]),
+                        mean_gradient=WORKLOAD["G"], tracers=M, cfl=WORKLOAD["cfl"], precision=precision,
+                        device=device)
+    run = gbght.Run(setup)
+    run.synchronize()
+    t0 = time.perf_counter()
+    run.import_state(puh, pph)
+    run.deposit()
+    run.import_tracers(pX)
+    run.deposit_tracers(0.0)
+    for _ in range(K):
+        run.advance(None)
+    u, p = run.export_state()
+    run.synchronize()
+    el = time.perf_counter() - t0
+    h2d = puh.nbytes + pph.nbytes + pX.nbytes + K * 8
+    # per step: max|u| (8 B) and the scalar-variance guard (4 doubles per ky' row, read back)
+    d2h = u.nbytes + p.nbytes + K * (8 + 4 * 8 * (2 * run.K + 1))
+    run.close()
+    return K / el, h2d / K, d2h / K
+
+
+def cpu_sample(args, inputs, n_samples=1, budget_s=150.0):
+    """One RK4 stage of the 512³ workload on the host oracle, plus a fifth of the tracer push."""
+    from oracle import gbght_oracle as O
+    N = args.grid
+    uh, ph, X = inputs
+    dom = O.Domain(N)
+    cond = O.Conditions(viscosity=WORKLOAD["viscosity"], schmidt=WORKLOAD["schmidt"],
+                        velocity_forcing=O.ConstantPower(WORKLOAD["injection_rate"], *WORKLOAD["shells"]),
+                        mean_gradient=WORKLOAD["G"])
+    Msub = max(1, args.tracers // 5)
+    Xs = X[:, :Msub].copy()
+    times = []
+    t_start = time.perf_counter()
+    for _ in range(n_samples):
+        t0 = time.perf_counter()
+        st = O.State(uh, ph)
+        # one stage: recoveries, both right-hand sides, the accumulator and IF update
+        u = dom.to_physical(st.uh)
+        w = dom.to_physical(O.curl(dom, st.uh))
+        phi = dom.to_physical(st.phih)
+        nu_ = O.velocity_rhs(dom, cond, st.uh, u, w, np.finfo(float).eps)
+        np_ = O.scalar_rhs(dom, cond, st.uh, u, phi)
+        E = np.exp((-(cond.viscosity * (0.2 * 1e-3))) * dom.k2)
+        _ = E * (st.uh + 0.1 * (1e-3 * nu_))
+        _ = E * (st.phih + 0.1 * (1e-3 * np_))
+        f0 = O.interpolate(dom, u, Xs)
+        O.advect_heun(dom, Xs, f0, u, 1e-3)
+        times.append(time.perf_counter() - t0)
+        del u, w, phi, nu_, np_, E
+        if time.perf_counter() - t_start > budget_s:
+            break
+    stage = statistics.mean(times)
+    return 1.0 / (5 * stage), len(times), stage
+
+
+def ours(args):
+    import torch
+    ws, rank, local = _dist()
+    device = local
+    torch.cuda.set_device(device)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    N = args.grid
+    inputs = make_inputs(N, args.tracers, seed_base=0)
+    hbm, peak_kind = _peaks()
+    results = {}
+    forms = ["fp64", "fp32_mixed"] if args.form == "both" else [args.form]
+    for form in forms:
+        run = run_form(args, form, device, inputs)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        clock_path = os.path.join(ROOT, "gpurun_out", f"clocks_{form}_rank{rank}.csv") \
+            if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else None
+        with ClockSampler(device, clock_path) as cs:
+            ms, prof = timed_steps(run, args.steps)
+        el = ms / 1e3
+        if ws > 1:
+            import torch.distributed as dist
+            t = torch.tensor([el], dtype=torch.float64, device=f"cuda:{device}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        spectra = (run.energy_spectrum(), run.scalar_spectrum())
+        results[form] = dict(el=el, prof=prof, clocks=cs.summary(), K=run.K, spectra=spectra)
+        run.close()
+        del run
+    # end-to-end through the public API (host buffers), the headline form
+    e2e_val, h2d, d2h = e2e_run(args, forms[0], device, inputs, args.steps)
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor([1.0 / e2e_val], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_val = 1.0 / float(t.item())
+    if rank == 0:
+        head = results[forms[0]]
+        value = ws * args.steps / head["el"]
+        w_complex = 16 if forms[0] == "fp64" else 8
+        ab = algorithmic_bytes_per_step(N, head["K"], w_complex)
+        prof = head["prof"]
+        kind = max(ab, key=lambda k: prof[k][1])
+        n_launch, tot_ms = prof[kind]
+        achieved = ab[kind] * args.steps / (tot_ms / 1e3) / 1e9 if tot_ms > 0 else 0.0
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(head["el"] * 1e3 / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64" if forms[0] == "fp64" else "f32",
+            "data": "synthetic (seeded k^4 spectrum, uniform tracers)", "config": _config(args, N),
+            "grid_point_stages_per_s": value * 5 * N ** 3,
+            "roofline": {"bound": "hbm", "kernel": kind, "achieved": round(achieved, 1), "peak": hbm,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                         "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                         "algorithmic_bytes_per_launch": ab[kind] / max(1, n_launch / args.steps),
+                         "avg_launch_ms": tot_ms / max(1, n_launch), "traffic": None},
+            "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in prof.items() if v[0]},
+            "gpu_launches": int(sum(v[0] for v in prof.values())),
+            "clocks": head["clocks"],
+            "e2e": {"value": round(e2e_val, 4), "unit": "steps/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+        }
+        if "fp32_mixed" in results and "fp64" in results:
+            m = results["fp32_mixed"]
+            mv = ws * args.steps / m["el"]
+            E64, P64 = results["fp64"]["spectra"]
+            E32, P32 = m["spectra"]
+            live = E64 > 1e-6 * E64.max()
+            livep = P64 > 1e-6 * P64.max()
+            line["forms"] = {"fp32_mixed": {"value": round(mv, 4), "unit": "steps/s",
+                                            "ratio_vs_fp64": round(mv / value, 3),
+                                            "clocks": m["clocks"],
+                                            "spectrum_rel_err_after_K_steps": float(np.max(np.abs(E32[live] - E64[live]) / E64[live])),
+                                            "scalar_spectrum_rel_err_after_K_steps": float(np.max(np.abs(P32[livep] - P64[livep]) / P64[livep]))}}
+        if ws == 1 and not args.no_cpu_baseline:
+            v, n, stage = cpu_sample(args, inputs, n_samples=1)
+            line["cpu_baseline"] = {"value": v, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+                                    "sample": f"one RK4 stage of the {N}^3 step (+ the push of {args.tracers // 5} tracers) "
+                                              f"on the NumPy/scipy.fft oracle, {stage:.1f} s; steps/s = 1/(5 x stage)"}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    N = args.grid
+    inputs = make_inputs(N, args.tracers, seed_base=0)
+    v, n, stage = cpu_sample(args, inputs, n_samples=max(1, args.steps), budget_s=150.0)
+    line = {"metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": ws, "steps": n, "warmup": 0,
+            "ms_per_step": 5 * stage * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded k^4 spectrum, uniform tracers)", "config": _config(args, N),
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"{n} sample(s) of one RK4 stage of the {N}^3 step (+ the push of "
+                                       f"{args.tracers // 5} tracers) on the NumPy/scipy.fft restatement; "
+                                       f"steps/s = 1/(5 x mean stage)"},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=WORKLOAD["N"])
+    ap.add_argument("--tracers", type=int, default=WORKLOAD["tracers"])
+    ap.add_argument("--form", default="both", choices=["both", "fp64", "fp32_mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        reference(args)
+    else:
+        ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,155 @@
+// The tile FFT: TL independent complex lines of length N, held in shared memory as N rows of TL
+// elements (element e of line l at buf[e*TL + l]). The lines are transformed together.
+//
+// Algorithm: Stockham autosort, decimation in time, mixed radix (Govindaraju et al., "High
+// Performance Discrete Fourier Transforms on Graphics Processors", SC 2008). Stage s has radix R,
+// and NS is the product of the radices before it. Butterfly j of a line reads
+// x[j + r·N/R] (r < R) and twiddles each input by w^(r·(j mod NS)·N/(NS·R)), with w = e^(∓2πi/N).
+// It then takes an R-point DFT and writes y[(j / NS)·NS·R + j mod NS + r·NS]. Each stage works in
+// place: every thread loads its butterflies, the block synchronises, then every thread stores.
+//
+// Consecutive threads take the same butterfly of consecutive lines (idx = j·TL + l). A quarter
+// warp of 8 threads therefore touches one row of TL elements, for every stage's reads and writes.
+// Rows are 128 bytes when TL·sizeof(element) = 128, so the shared-memory accesses are free of bank
+// conflicts whatever the stage's stride.
+//
+// SIGN = -1 is the forward (unnormalised) transform, SIGN = +1 the inverse (unnormalised).
+// `tw` holds e^(-2πi k/N) for k in [0, N), computed on the host in extended precision.
+#pragma once
+
+#include "gbght_common.cuh"
+
+namespace gbght {
+
+// Radix plans, innermost stage first. Every supported N is 2^a·3^b.
+template <int N> struct Radices;
+template <> struct Radices<8>   { static constexpr int n = 1; static constexpr int r[1] = {8}; };
+template <> struct Radices<12>  { static constexpr int n = 2; static constexpr int r[2] = {3, 4}; };
+template <> struct Radices<16>  { static constexpr int n = 2; static constexpr int r[2] = {4, 4}; };
+template <> struct Radices<24>  { static constexpr int n = 2; static constexpr int r[2] = {3, 8}; };
+template <> struct Radices<32>  { static constexpr int n = 2; static constexpr int r[2] = {4, 8}; };
+template <> struct Radices<48>  { static constexpr int n = 3; static constexpr int r[3] = {3, 4, 4}; };
+template <> struct Radices<64>  { static constexpr int n = 2; static constexpr int r[2] = {8, 8}; };
+template <> struct Radices<96>  { static constexpr int n = 3; static constexpr int r[3] = {3, 4, 8}; };
+template <> struct Radices<128> { static constexpr int n = 3; static constexpr int r[3] = {2, 8, 8}; };
+template <> struct Radices<192> { static constexpr int n = 3; static constexpr int r[3] = {3, 8, 8}; };
+template <> struct Radices<256> { static constexpr int n = 3; static constexpr int r[3] = {4, 8, 8}; };
+template <> struct Radices<384> { static constexpr int n = 4; static constexpr int r[4] = {3, 2, 8, 8}; };
+template <> struct Radices<512> { static constexpr int n = 3; static constexpr int r[3] = {8, 8, 8}; };
+
+template <int N> constexpr int stage_ns(int s) {
+  int p = 1;
+  for (int i = 0; i < s; ++i) p *= Radices<N>::r[i];
+  return p;
+}
+
+// ---- small DFTs in registers ------------------------------------------------------------------
+
+template <class T, int SIGN> GBGHT_HD void dft2(Cplx<T>* v) {
+  Cplx<T> a = v[0], b = v[1];
+  v[0] = a + b;
+  v[1] = a - b;
+}
+
+template <class T, int SIGN> GBGHT_HD void dft3(Cplx<T>* v) {
+  // X_k = Σ a_n e^(SIGN·2πi nk/3)
+  const T c1 = T(-0.5);
+  const T s1 = T(SIGN) * T(0.86602540378443864676372317075294);
+  Cplx<T> a0 = v[0], a1 = v[1], a2 = v[2];
+  Cplx<T> t = a1 + a2, d = a1 - a2;
+  Cplx<T> m = cmk<T>(a0.x + c1 * t.x, a0.y + c1 * t.y);
+  // s1 · i · d
+  Cplx<T> r = cmk<T>(-s1 * d.y, s1 * d.x);
+  v[0] = a0 + t;
+  v[1] = m + r;
+  v[2] = m - r;
+}
+
+template <class T, int SIGN> GBGHT_HD void dft4(Cplx<T>* v) {
+  Cplx<T> a0 = v[0], a1 = v[1], a2 = v[2], a3 = v[3];
+  Cplx<T> t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, d = a1 - a3;
+  Cplx<T> t3 = (SIGN < 0) ? mul_mi(d) : mul_i(d);
+  v[0] = t0 + t2;
+  v[2] = t0 - t2;
+  v[1] = t1 + t3;
+  v[3] = t1 - t3;
+}
+
+template <class T, int SIGN> GBGHT_HD void dft8(Cplx<T>* v) {
+  // even/odd split into two 4-point DFTs, then combine with w8^k = e^(SIGN·iπk/4)
+  Cplx<T> e[4] = {v[0], v[2], v[4], v[6]};
+  Cplx<T> o[4] = {v[1], v[3], v[5], v[7]};
+  dft4<T, SIGN>(e);
+  dft4<T, SIGN>(o);
+  const T h = T(0.70710678118654752440084436210485);
+  // w8^1 = (h, SIGN·h), w8^2 = SIGN·i, w8^3 = (-h, SIGN·h)
+  Cplx<T> o1 = cmk<T>(h * (o[1].x - T(SIGN) * o[1].y), h * (o[1].y + T(SIGN) * o[1].x));
+  Cplx<T> o2 = (SIGN < 0) ? mul_mi(o[2]) : mul_i(o[2]);
+  Cplx<T> o3 = cmk<T>(-h * (o[3].x + T(SIGN) * o[3].y), h * (T(SIGN) * o[3].x - o[3].y));
+  v[0] = e[0] + o[0];
+  v[4] = e[0] - o[0];
+  v[1] = e[1] + o1;
+  v[5] = e[1] - o1;
+  v[2] = e[2] + o2;
+  v[6] = e[2] - o2;
+  v[3] = e[3] + o3;
+  v[7] = e[3] - o3;
+}
+
+template <class T, int R, int SIGN> GBGHT_HD void dft(Cplx<T>* v) {
+  if constexpr (R == 2) dft2<T, SIGN>(v);
+  else if constexpr (R == 3) dft3<T, SIGN>(v);
+  else if constexpr (R == 4) dft4<T, SIGN>(v);
+  else if constexpr (R == 8) dft8<T, SIGN>(v);
+  else static_assert(R == 2, "unsupported radix");
+}
+
+// ---- the tile transform -------------------------------------------------------------------------
+
+template <class T, int N, int TL, int NT, int SIGN, int S = 0>
+GBGHT_HD void tile_fft(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTRICT tw) {
+  if constexpr (S < Radices<N>::n) {
+    constexpr int R = Radices<N>::r[S];
+    constexpr int NS = stage_ns<N>(S);
+    constexpr int NB = N / R;
+    constexpr int TOT = NB * TL;
+    constexpr int BPT = (TOT + NT - 1) / NT;
+    constexpr int TWS = N / (NS * R);
+    Cplx<T> v[BPT][R];
+#pragma unroll
+    for (int b = 0; b < BPT; ++b) {
+      const int idx = c.tid + b * NT;
+      if (BPT * NT == TOT || idx < TOT) {
+        const int l = idx % TL, j = idx / TL;
+        const int jm = j % NS;
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[b][r] = buf[(j + r * NB) * TL + l];
+        if constexpr (NS > 1) {
+#pragma unroll
+          for (int r = 1; r < R; ++r) {
+            Cplx<T> w = ldgc(tw + jm * r * TWS);
+            if constexpr (SIGN > 0) w = conj(w);
+            v[b][r] = v[b][r] * w;
+          }
+        }
+      }
+    }
+    GBGHT_SYNC();
+#pragma unroll
+    for (int b = 0; b < BPT; ++b) {
+      const int idx = c.tid + b * NT;
+      if (BPT * NT == TOT || idx < TOT) {
+        const int l = idx % TL, j = idx / TL;
+        const int jm = j % NS;
+        dft<T, R, SIGN>(v[b]);
+        const int base = (j / NS) * NS * R + jm;
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[(base + r * NS) * TL + l] = v[b][r];
+      }
+    }
+    GBGHT_SYNC();
+    tile_fft<T, N, TL, NT, SIGN, S + 1>(c, buf, tw);
+  }
+}
+
+}  // namespace gbght

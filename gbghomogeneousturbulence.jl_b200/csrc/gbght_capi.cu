@@ -1,0 +1,509 @@
+// The C ABI (include/gbght.h): argument checks, the run layer's schedule checks and clock, and
+// the calls into the engine. The checks and their messages follow the reference's own refusals;
+// each function's comment in gbght.h cites the interface it replaces.
+#include "../../include/gbght.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "gbght_engine.cuh"
+
+using gbght::Engine;
+
+struct gbght_run {
+  gbght_config cfg{};
+  std::unique_ptr<Engine> eng;
+  std::string err;
+  // the field side of the schedule (src/Cache.jl epochs)
+  int64_t fields_epoch = 0;
+  int64_t deposit_epoch = -1;
+  double max_speed = 0.0;
+  // the tracer side: the newest trail sample
+  bool sample_valid = false;
+  bool sample_at_positions = false;
+  int64_t sample_epoch = 0;
+  double sample_time = 0.0;
+  // the clock
+  double time = 0.0;
+  int64_t step = 0;
+};
+
+namespace {
+
+thread_local std::string g_global_error;
+
+int fail(gbght_run* r, int code, const std::string& msg) {
+  if (r) r->err = msg;
+  return code;
+}
+
+int engine_call(gbght_run* r, const char* e) {
+  if (!e) return GBGHT_OK;
+  return fail(r, GBGHT_ERR_CUDA, e);
+}
+
+// Carpenter & Kennedy (1994) five-stage 2N tableau and Williamson's three-stage one, as rounded
+// from their exact rationals (src/Propagator.jl:267-274,304-320); d = differences of the rounded
+// abscissae.
+struct Tableau {
+  int S;
+  double a[5], b[5], d[5];
+};
+
+Tableau tableau(int scheme) {
+  Tableau t{};
+  if (scheme == GBGHT_IFRK3) {
+    t.S = 3;
+    const double a[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
+    const double b[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+    const double d[3] = {1.0 / 3.0, 5.0 / 12.0, 1.0 / 4.0};
+    for (int i = 0; i < 3; ++i) { t.a[i] = a[i]; t.b[i] = b[i]; t.d[i] = d[i]; }
+    return t;
+  }
+  t.S = 5;
+  t.a[0] = 0.0;
+  t.a[1] = -567301805773.0 / 1357537059087.0;
+  t.a[2] = -2404267990393.0 / 2016746695238.0;
+  t.a[3] = -3550918686646.0 / 2091501179385.0;
+  t.a[4] = -1275806237668.0 / 842570457699.0;
+  t.b[0] = 1432997174477.0 / 9575080441755.0;
+  t.b[1] = 5161836677717.0 / 13612068292357.0;
+  t.b[2] = 1720146321549.0 / 2090206949498.0;
+  t.b[3] = 3134564353537.0 / 4481467310338.0;
+  t.b[4] = 2277821191437.0 / 14882151754819.0;
+  const double c2 = 1432997174477.0 / 9575080441755.0;
+  const double c3 = 2526269341429.0 / 6820363962896.0;
+  const double c4 = 2006345519317.0 / 3224310063776.0;
+  const double c5 = 2802321613138.0 / 2924317926251.0;
+  t.d[0] = c2;
+  t.d[1] = c3 - c2;
+  t.d[2] = c4 - c3;
+  t.d[3] = c5 - c4;
+  t.d[4] = 1.0 - c5;
+  return t;
+}
+
+bool finite_positive(double v) { return std::isfinite(v) && v > 0.0; }
+
+int check_run(gbght_run* r) { return r ? GBGHT_OK : GBGHT_ERR_ARGUMENT; }
+
+int require_deposit(gbght_run* r, const char* what) {
+  if (r->deposit_epoch != r->fields_epoch)
+    return fail(r, GBGHT_ERR_SCHEDULE,
+                std::string(what) + ": the deposited velocity is stale (the fields moved since the last "
+                "deposit); close each step with gbght_deposit");
+  return GBGHT_OK;
+}
+
+int do_deposit(gbght_run* r) {
+  double m2 = 0.0;
+  int rc = engine_call(r, r->eng->deposit(&m2));
+  if (rc) return rc;
+  r->max_speed = std::sqrt(m2);
+  r->deposit_epoch = r->fields_epoch;
+  return GBGHT_OK;
+}
+
+double cfl_dt(const gbght_run* r) {
+  const gbght_config& c = r->cfg;
+  const double dx = c.side_length / c.grid_points_per_axis;
+  const double advective = r->max_speed > 0 ? c.cfl * dx / r->max_speed : c.cfl * dx;
+  const double nu = c.viscosity, kap = c.viscosity / c.schmidt;
+  const double D = c.scalar ? std::max(nu, kap) : nu;
+  const double kmin = 2.0 * M_PI / c.side_length;
+  const double resolution = 1.0 / (D * kmin * kmin);
+  return std::min(std::min(advective, resolution), c.max_dt);
+}
+
+}  // namespace
+
+extern "C" {
+
+void gbght_config_default(gbght_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof *c);
+  c->grid_points_per_axis = 64;
+  c->side_length = 2.0 * M_PI;
+  c->precision = GBGHT_FP64;
+  c->scheme = GBGHT_IFRK4;
+  c->viscosity = 0.01;
+  c->schmidt = 1.0;
+  c->scalar = 1;
+  c->velocity_forcing = GBGHT_FORCING_NONE;
+  c->injection_rate = 0.0;
+  c->lowest_shell = 1;
+  c->highest_shell = 2.0;
+  c->tracers = 0;
+  c->cfl = 0.5;
+  c->max_dt = INFINITY;
+  c->device = 0;
+}
+
+const char* gbght_version(void) { return "gbght-b200 0.1.0"; }
+const char* gbght_global_error(void) { return g_global_error.c_str(); }
+const char* gbght_last_error(const gbght_run* r) { return r ? r->err.c_str() : "null run"; }
+
+int gbght_create(gbght_run** out, const gbght_config* cfg) {
+  if (!out || !cfg) {
+    g_global_error = "null argument";
+    return GBGHT_ERR_ARGUMENT;
+  }
+  *out = nullptr;
+  auto bad = [&](const std::string& m) {
+    g_global_error = m;
+    return GBGHT_ERR_ARGUMENT;
+  };
+  if (!gbght::supported_N(cfg->grid_points_per_axis))
+    return bad("grid_points_per_axis must be one of 8 12 16 24 32 48 64 96 128 192 256 384 512, got " +
+               std::to_string(cfg->grid_points_per_axis));
+  if (!finite_positive(cfg->side_length)) return bad("side_length must be positive and finite");
+  if (!(cfg->viscosity > 0))
+    return bad("`viscosity` must be positive, got " + std::to_string(cfg->viscosity) +
+               ": it sets the Reynolds number through Re = 1/ν, and a non-positive value has no dissipation scale");
+  if (!(cfg->schmidt > 0))
+    return bad("`schmidt` must be positive, got " + std::to_string(cfg->schmidt) +
+               ": the scalar diffusivity is ν/Sc, so a non-positive Schmidt number makes it infinite or negative");
+  if (cfg->precision != GBGHT_FP64 && cfg->precision != GBGHT_FP32_MIXED) return bad("unknown precision");
+  if (cfg->scheme != GBGHT_IFRK4 && cfg->scheme != GBGHT_IFRK3) return bad("unknown field integration scheme");
+  if (cfg->velocity_forcing != GBGHT_FORCING_NONE && cfg->velocity_forcing != GBGHT_FORCING_CONSTANT_POWER)
+    return bad("unknown velocity forcing");
+  if (cfg->velocity_forcing == GBGHT_FORCING_CONSTANT_POWER) {
+    if (!std::isfinite(cfg->injection_rate)) return bad("injection_rate must be finite");
+    if (cfg->lowest_shell < 1) return bad("lowest_shell must be at least 1");
+    if (!(cfg->highest_shell >= cfg->lowest_shell)) return bad("highest_shell must be at least lowest_shell");
+  }
+  for (int i = 0; i < 3; ++i)
+    if (!std::isfinite(cfg->mean_gradient[i])) return bad("mean_gradient must be finite");
+  if (!cfg->scalar && (cfg->mean_gradient[0] != 0 || cfg->mean_gradient[1] != 0 || cfg->mean_gradient[2] != 0))
+    return bad("a mean scalar gradient was given, but the run carries no scalar");
+  if (cfg->tracers < 0) return bad("tracers must be non-negative");
+  if (!finite_positive(cfg->cfl)) return bad("cfl must be positive and finite");
+  if (!(cfg->max_dt > 0)) return bad("max_dt must be positive");
+
+  auto r = std::make_unique<gbght_run>();
+  r->cfg = *cfg;
+  std::string err;
+  r->eng.reset(gbght::make_engine(cfg->grid_points_per_axis, cfg->precision, &err));
+  if (!r->eng) return bad(err);
+  gbght::RunParams p{};
+  p.N = cfg->grid_points_per_axis;
+  p.L = cfg->side_length;
+  p.precision = cfg->precision;
+  p.scheme = cfg->scheme;
+  p.viscosity = cfg->viscosity;
+  p.schmidt = cfg->schmidt;
+  p.scalar = cfg->scalar ? 1 : 0;
+  p.forcing = cfg->velocity_forcing;
+  p.injection_rate = cfg->injection_rate;
+  p.lowest_shell = cfg->lowest_shell;
+  p.highest_shell = cfg->highest_shell;
+  for (int i = 0; i < 3; ++i) p.G[i] = cfg->mean_gradient[i];
+  p.tracers = cfg->tracers;
+  p.device = cfg->device;
+  if (const char* e = r->eng->init(p)) {
+    g_global_error = e;
+    return GBGHT_ERR_CUDA;
+  }
+  *out = r.release();
+  return GBGHT_OK;
+}
+
+void gbght_destroy(gbght_run* r) { delete r; }
+
+int gbght_geometry(const gbght_run* r, int* K, double* cutoff) {
+  if (!r) return GBGHT_ERR_ARGUMENT;
+  if (K) *K = r->eng->K();
+  if (cutoff) *cutoff = r->eng->cutoff();
+  return GBGHT_OK;
+}
+
+int gbght_state_import(gbght_run* r, const double* u_hat, const double* phi_hat) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!u_hat) return fail(r, GBGHT_ERR_ARGUMENT, "u_hat is null");
+  if (r->cfg.scalar && !phi_hat)
+    return fail(r, GBGHT_ERR_ARGUMENT, "this run carries a passive scalar, so phi_hat must be given");
+  bool outside = false;
+  int rc = engine_call(r, r->eng->import_state(u_hat, phi_hat, &outside));
+  if (rc) return rc;
+  if (outside)
+    return fail(r, GBGHT_ERR_ARGUMENT,
+                "the state has content outside the retained 2/3 ball; this backend stores only the "
+                "retained modes (every state the seeders and steps produce is band-limited)");
+  r->fields_epoch += 1;   // a new state: the deposit is stale
+  return GBGHT_OK;
+}
+
+int gbght_state_export(gbght_run* r, double* u_hat, double* phi_hat) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!u_hat) return fail(r, GBGHT_ERR_ARGUMENT, "u_hat is null");
+  return engine_call(r, r->eng->export_state(u_hat, r->cfg.scalar ? phi_hat : nullptr));
+}
+
+int gbght_step(gbght_run* r, double dt) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!finite_positive(dt))
+    return fail(r, GBGHT_ERR_ARGUMENT, "the timestep must be positive and finite, got " + std::to_string(dt));
+  if (int rc = require_deposit(r, "step")) return rc;
+  const Tableau t = tableau(r->cfg.scheme);
+  int rc = engine_call(r, r->eng->step(dt, t.a, t.b, t.d, t.S));
+  if (rc) return rc;
+  r->fields_epoch += 1;
+  return GBGHT_OK;
+}
+
+int gbght_deposit(gbght_run* r) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  return do_deposit(r);
+}
+
+int gbght_max_speed(gbght_run* r, double* speed) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (r->deposit_epoch < 0) return fail(r, GBGHT_ERR_SCHEDULE, "max_speed: nothing has been deposited");
+  if (speed) *speed = r->max_speed;
+  return GBGHT_OK;
+}
+
+int gbght_cfl_timestep(gbght_run* r, double* dt) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (r->deposit_epoch < 0) return fail(r, GBGHT_ERR_SCHEDULE, "cfl_timestep: nothing has been deposited");
+  if (!std::isfinite(r->max_speed))
+    return fail(r, GBGHT_ERR_SCHEDULE,
+                "non-finite velocity at step " + std::to_string(r->step) + ": the run appears to have blown up");
+  if (dt) *dt = cfl_dt(r);
+  return GBGHT_OK;
+}
+
+int gbght_velocity_physical_export(gbght_run* r, double* u) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!u) return fail(r, GBGHT_ERR_ARGUMENT, "u is null");
+  if (r->deposit_epoch < 0) return fail(r, GBGHT_ERR_SCHEDULE, "velocity_physical: nothing has been deposited");
+  return engine_call(r, r->eng->velocity_export(u));
+}
+
+int gbght_velocity_physical_import(gbght_run* r, const double* u) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!u) return fail(r, GBGHT_ERR_ARGUMENT, "u is null");
+  int rc = engine_call(r, r->eng->velocity_import(u));
+  if (rc) return rc;
+  r->fields_epoch += 1;
+  r->deposit_epoch = r->fields_epoch;
+  return GBGHT_OK;
+}
+
+int gbght_observables(gbght_run* r, double out[4]) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!out) return fail(r, GBGHT_ERR_ARGUMENT, "out is null");
+  gbght::Observables o{};
+  int rc = engine_call(r, r->eng->observables(&o));
+  if (rc) return rc;
+  out[0] = o.k;
+  out[1] = o.eps;
+  out[2] = r->cfg.scalar ? o.var : NAN;
+  out[3] = r->cfg.scalar ? o.chi : NAN;
+  return GBGHT_OK;
+}
+
+int gbght_spectrum_length(const gbght_run* r, int* n) {
+  if (!r || !n) return GBGHT_ERR_ARGUMENT;
+  *n = int(std::floor(std::sqrt(3.0) * r->cfg.grid_points_per_axis / 2.0 + 0.5)) + 1;
+  return GBGHT_OK;
+}
+
+int gbght_spectrum(gbght_run* r, int which, double* out, int n) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!out || n <= 0) return fail(r, GBGHT_ERR_ARGUMENT, "out is null or empty");
+  if (which != 0 && which != 1) return fail(r, GBGHT_ERR_ARGUMENT, "which must be 0 (velocity) or 1 (scalar)");
+  if (which == 1 && !r->cfg.scalar) return fail(r, GBGHT_ERR_ARGUMENT, "the run carries no scalar");
+  return engine_call(r, r->eng->spectrum(which, out, n));
+}
+
+int gbght_tracers_import(gbght_run* r, const double* X) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (r->cfg.tracers <= 0) return fail(r, GBGHT_ERR_ARGUMENT, "the run was built without tracers");
+  if (!X) return fail(r, GBGHT_ERR_ARGUMENT, "X is null");
+  int rc = engine_call(r, r->eng->tracers_set(X));
+  if (rc) return rc;
+  r->sample_valid = false;
+  r->sample_at_positions = false;
+  return GBGHT_OK;
+}
+
+int gbght_tracers_export(gbght_run* r, double* X) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (r->cfg.tracers <= 0) return fail(r, GBGHT_ERR_ARGUMENT, "the run was built without tracers");
+  if (!X) return fail(r, GBGHT_ERR_ARGUMENT, "X is null");
+  return engine_call(r, r->eng->tracers_get(X));
+}
+
+int gbght_tracer_sample_export(gbght_run* r, double* values, double* t) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (r->cfg.tracers <= 0) return fail(r, GBGHT_ERR_ARGUMENT, "the run was built without tracers");
+  if (!r->sample_valid) return fail(r, GBGHT_ERR_SCHEDULE, "the trail holds no sample yet");
+  if (!r->sample_at_positions)
+    return fail(r, GBGHT_ERR_SCHEDULE, "the trail is stale: the positions moved since its newest sample");
+  if (t) *t = r->sample_time;
+  return values ? engine_call(r, r->eng->tracer_sample_get(values)) : GBGHT_OK;
+}
+
+static int advect_checks(gbght_run* r, double dt) {
+  if (r->cfg.tracers <= 0) return fail(r, GBGHT_ERR_ARGUMENT, "the run was built without tracers");
+  if (!finite_positive(dt))
+    return fail(r, GBGHT_ERR_ARGUMENT,
+                "`dt` must be positive and finite, got " + std::to_string(dt) +
+                    ": the samples a particle scheme integrates over must lie at increasing times");
+  if (!r->sample_valid || !r->sample_at_positions)
+    return fail(r, GBGHT_ERR_SCHEDULE, "the trail's newest sample was not taken at the current positions");
+  if (int rc = require_deposit(r, "advect")) return rc;
+  if (r->fields_epoch != r->sample_epoch + 1)
+    return fail(r, GBGHT_ERR_SCHEDULE,
+                "the fields must be exactly one step ahead of the tracer positions to advance them");
+  return GBGHT_OK;
+}
+
+int gbght_advect(gbght_run* r, double dt) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (int rc = advect_checks(r, dt)) return rc;
+  int rc = engine_call(r, r->eng->tracers_run(1, gbght::heun_weights(dt)));
+  if (rc) return rc;
+  rc = engine_call(r, r->eng->sync());
+  if (rc) return rc;
+  r->sample_at_positions = false;
+  return GBGHT_OK;
+}
+
+int gbght_deposit_tracers(gbght_run* r, double t) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (r->cfg.tracers <= 0) return fail(r, GBGHT_ERR_ARGUMENT, "the cache was built without tracers");
+  if (!std::isfinite(t)) return fail(r, GBGHT_ERR_ARGUMENT, "the sample time must be finite");
+  if (int rc = require_deposit(r, "deposit (particles)")) return rc;
+  if (r->sample_valid) {
+    if (!(t > r->sample_time))
+      return fail(r, GBGHT_ERR_ARGUMENT, "the sample time must be later than the previous sample's");
+    if (r->sample_at_positions)
+      return fail(r, GBGHT_ERR_SCHEDULE, "a second sample at the same positions: advance the tracers first");
+    if (r->fields_epoch != r->sample_epoch + 1)
+      return fail(r, GBGHT_ERR_SCHEDULE, "the fields and the tracer positions belong to different times");
+  }
+  int rc = engine_call(r, r->eng->tracers_run(0, gbght::HeunWeights{0, 0, 0}));
+  if (rc) return rc;
+  rc = engine_call(r, r->eng->sync());
+  if (rc) return rc;
+  r->sample_valid = true;
+  r->sample_at_positions = true;
+  r->sample_epoch = r->fields_epoch;
+  r->sample_time = t;
+  return GBGHT_OK;
+}
+
+int gbght_interpolate_velocity(gbght_run* r, const double* X, int64_t M, double* out) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (M < 0 || (M > 0 && (!X || !out))) return fail(r, GBGHT_ERR_ARGUMENT, "bad positions or output");
+  if (r->deposit_epoch < 0) return fail(r, GBGHT_ERR_SCHEDULE, "nothing has been deposited");
+  return engine_call(r, r->eng->gather(X, M, out));
+}
+
+int gbght_advance(gbght_run* r, double dt, double* dt_taken) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (int rc = require_deposit(r, "advance")) return rc;
+  double D = dt;
+  if (!(dt > 0)) {
+    if (!std::isfinite(r->max_speed))
+      return fail(r, GBGHT_ERR_SCHEDULE, "non-finite velocity at step " + std::to_string(r->step) +
+                                             ": the run appears to have blown up");
+    D = cfl_dt(r);
+  }
+  if (!finite_positive(D))
+    return fail(r, GBGHT_ERR_ARGUMENT, "the timestep must be positive and finite, got " + std::to_string(D));
+  const double t_new = r->time + D;
+  if (!(t_new > r->time))
+    return fail(r, GBGHT_ERR_ARGUMENT, "the timestep is too small to advance the clock");
+  const bool tracers = r->cfg.tracers > 0;
+  if (tracers && (!r->sample_valid || !r->sample_at_positions))
+    return fail(r, GBGHT_ERR_SCHEDULE, "the tracers' last push was never closed by a particle deposit");
+  if (tracers && r->sample_epoch != r->fields_epoch)
+    return fail(r, GBGHT_ERR_SCHEDULE, "the fields were stepped alone since the tracers' last sample");
+  const Tableau t = tableau(r->cfg.scheme);
+  int rc = engine_call(r, r->eng->step(D, t.a, t.b, t.d, t.S));
+  if (rc) return rc;
+  r->fields_epoch += 1;
+  if ((rc = do_deposit(r))) return rc;
+  if (tracers) {
+    // push and closing particle deposit in one launch; the same functions as advect + deposit
+    rc = engine_call(r, r->eng->tracers_run(2, gbght::heun_weights(D)));
+    if (rc) return rc;
+    r->sample_epoch = r->fields_epoch;
+    r->sample_time = t_new;
+    r->sample_at_positions = true;
+  }
+  if (!std::isfinite(r->max_speed))
+    return fail(r, GBGHT_ERR_SCHEDULE, "non-finite velocity at step " + std::to_string(r->step + 1) +
+                                           ": the run appears to have blown up");
+  if (r->cfg.scalar) {
+    gbght::Observables o{};
+    if ((rc = engine_call(r, r->eng->observables(&o)))) return rc;
+    if (!std::isfinite(o.var))
+      return fail(r, GBGHT_ERR_SCHEDULE, "non-finite scalar at step " + std::to_string(r->step + 1) +
+                                             ": the run appears to have blown up");
+  }
+  r->time = t_new;
+  r->step += 1;
+  if (dt_taken) *dt_taken = D;
+  return GBGHT_OK;
+}
+
+int gbght_clock(const gbght_run* r, double* time, int64_t* step) {
+  if (!r) return GBGHT_ERR_ARGUMENT;
+  if (time) *time = r->time;
+  if (step) *step = r->step;
+  return GBGHT_OK;
+}
+
+int gbght_set_clock(gbght_run* r, double time, int64_t step) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!std::isfinite(time) || step < 0) return fail(r, GBGHT_ERR_ARGUMENT, "bad clock");
+  r->time = time;
+  r->step = step;
+  return GBGHT_OK;
+}
+
+int gbght_status_word(gbght_run* r, uint32_t* word) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  uint32_t w = 0;
+  int rc = engine_call(r, r->eng->status(&w));
+  if (rc) return rc;
+  if (!std::isfinite(r->max_speed)) w |= GBGHT_STATUS_NONFINITE_SPEED;
+  if (word) *word = w;
+  return GBGHT_OK;
+}
+
+int gbght_profile(gbght_run* r, int enable) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  return engine_call(r, r->eng->profile(enable));
+}
+
+int gbght_profile_read(gbght_run* r, int kind, int64_t* launches, double* total_ms) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  int64_t n = 0;
+  double ms = 0.0;
+  const char* e = r->eng->profile_read(kind, &n, &ms);
+  if (e) return fail(r, GBGHT_ERR_ARGUMENT, e);
+  if (launches) *launches = n;
+  if (total_ms) *total_ms = ms;
+  return GBGHT_OK;
+}
+
+int gbght_timer(gbght_run* r, int op, double* ms) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (op != 0 && op != 1) return fail(r, GBGHT_ERR_ARGUMENT, "op must be 0 (start) or 1 (stop)");
+  return engine_call(r, r->eng->timer(op, ms));
+}
+
+int gbght_synchronize(gbght_run* r) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  return engine_call(r, r->eng->sync());
+}
+
+}  // extern "C"

@@ -1,0 +1,858 @@
+// Engine implementation: device buffers, kernel launches, and the sequence of one IF-RK step.
+//
+// Built by nvcc for sm_100a (the library), or by a host C++ compiler with -DGBGHT_EMU for the
+// CPU check of the kernel bodies (see gbght_engine.cuh).
+#include "gbght_engine.cuh"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <memory>
+
+namespace gbght {
+
+// ------------------------------------------------------------------------------------------------
+// Runtime: device memory and copies.
+// ------------------------------------------------------------------------------------------------
+#ifdef GBGHT_EMU
+using Stream = void*;
+static const char* rt_alloc(void** p, size_t n) {
+  *p = std::calloc(1, n ? n : 1);
+  return *p ? nullptr : "host allocation failed";
+}
+static void rt_free(void* p) { std::free(p); }
+static const char* rt_memset(void* p, int v, size_t n, Stream) { std::memset(p, v, n); return nullptr; }
+static const char* rt_h2d(void* d, const void* h, size_t n, Stream) { std::memcpy(d, h, n); return nullptr; }
+static const char* rt_d2h(void* h, const void* d, size_t n, Stream) { std::memcpy(h, d, n); return nullptr; }
+static const char* rt_sync(Stream) { return nullptr; }
+static const char* rt_check() { return nullptr; }
+#else
+using Stream = cudaStream_t;
+static thread_local char g_cuda_msg[256];
+static const char* cuda_err(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return nullptr;
+  std::snprintf(g_cuda_msg, sizeof g_cuda_msg, "%s: %s", what, cudaGetErrorString(e));
+  return g_cuda_msg;
+}
+static const char* rt_alloc(void** p, size_t n) {
+  const char* e = cuda_err(cudaMalloc(p, n ? n : 16), "cudaMalloc");
+  if (!e) e = cuda_err(cudaMemset(*p, 0, n ? n : 16), "cudaMemset");
+  return e;
+}
+static void rt_free(void* p) { if (p) cudaFree(p); }
+static const char* rt_memset(void* p, int v, size_t n, Stream s) { return cuda_err(cudaMemsetAsync(p, v, n, s), "cudaMemsetAsync"); }
+static const char* rt_h2d(void* d, const void* h, size_t n, Stream s) {
+  return cuda_err(cudaMemcpyAsync(d, h, n, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync H2D");
+}
+static const char* rt_d2h(void* h, const void* d, size_t n, Stream s) {
+  const char* e = cuda_err(cudaMemcpyAsync(h, d, n, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync D2H");
+  if (!e) e = cuda_err(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  return e;
+}
+static const char* rt_sync(Stream s) { return cuda_err(cudaStreamSynchronize(s), "cudaStreamSynchronize"); }
+static const char* rt_check() { return cuda_err(cudaGetLastError(), "kernel launch"); }
+#endif
+
+// ------------------------------------------------------------------------------------------------
+// Launch shapes.
+// ------------------------------------------------------------------------------------------------
+template <class T> struct Shape {
+  static constexpr int TLY = 128 / int(sizeof(Cplx<T>));   // y passes: 128-byte rows
+  static constexpr int TLZ = 64 / int(sizeof(Cplx<T>));    // z epilogue: 64-byte rows
+};
+constexpr int clamp_nt(int v) { return v < 64 ? 64 : (v > 256 ? 256 : v); }
+
+#ifdef GBGHT_EMU
+constexpr int kNT(int) { return 1; }
+#else
+constexpr int kNT(int v) { return clamp_nt(v); }
+#endif
+
+template <class F>
+static void emu_grid(int gx, int gy, int gz, size_t smem, F&& body) {
+  std::vector<double> sm((smem + sizeof(double) - 1) / sizeof(double) + 8);
+  for (int bz = 0; bz < gz; ++bz)
+    for (int by = 0; by < gy; ++by)
+      for (int bx = 0; bx < gx; ++bx) {
+        Cta c{0, bx, by, bz};
+        body(c, reinterpret_cast<void*>(sm.data()));
+      }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Kernels (CUDA build).
+// ------------------------------------------------------------------------------------------------
+#ifndef GBGHT_EMU
+#define CTA_CTX Cta c{int(threadIdx.x), int(blockIdx.x), int(blockIdx.y), int(blockIdx.z)}
+extern __shared__ __align__(16) unsigned char g_smem[];
+
+template <class T, int N, int TL, int NT>
+__global__ void __launch_bounds__(NT) k_y_inverse(Geometry g, const Cplx<T>* A, Cplx<T>* B, int c0, const Cplx<T>* tw) {
+  CTA_CTX;
+  body_y_inverse<T, N, TL, NT>(c, reinterpret_cast<Cplx<T>*>(g_smem), g, A, B, c0, tw);
+}
+template <class T, int N, int TL, int NT>
+__global__ void __launch_bounds__(NT) k_y_forward(Geometry g, const Cplx<T>* B, Cplx<T>* A, const Cplx<T>* tw) {
+  CTA_CTX;
+  body_y_forward<T, N, TL, NT>(c, reinterpret_cast<Cplx<T>*>(g_smem), g, B, A, tw);
+}
+template <class T, int N, int NT>
+__global__ void __launch_bounds__(NT) k_x_products(Geometry g, Cplx<T>* B, int has_scalar, const Cplx<T>* tw) {
+  CTA_CTX;
+  body_x_products<T, N, NT>(c, reinterpret_cast<Cplx<T>*>(g_smem), g, B, has_scalar, tw);
+}
+template <class T, int N, int NT>
+__global__ void __launch_bounds__(NT) k_x_velocity(Geometry g, const Cplx<T>* B, T* u, unsigned long long* maxbits,
+                                                   const Cplx<T>* tw) {
+  CTA_CTX;
+  Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
+  double* red = reinterpret_cast<double*>(sm + N * 8);
+  const double m = body_x_velocity<T, N, NT>(c, sm, red, g, B, u, tw);
+  if (threadIdx.x == 0) atomicMax(maxbits, static_cast<unsigned long long>(__double_as_longlong(m)));
+}
+template <class T, int N, int TL, int NT>
+__global__ void __launch_bounds__(NT) k_z_epilogue(Geometry g, Cplx<T>* A, Cplx<T>* S, Cplx<T>* H, StageArgs st,
+                                                   const double* amp, double* partial, const Cplx<T>* tw) {
+  CTA_CTX;
+  Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
+  Cplx<T>* Rt = W + N * TL;
+  double* red = reinterpret_cast<double*>(Rt + 3 * g.NY2 * TL);
+  const double e = body_z_epilogue<T, N, TL, NT>(c, W, Rt, red, g, A, S, H, st, amp, tw);
+  if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
+}
+template <class T, int N, int TL, int NT>
+__global__ void __launch_bounds__(NT) k_z_init(Geometry g, Cplx<T>* A, const Cplx<T>* S, int has_scalar, double* partial,
+                                               const Cplx<T>* tw) {
+  CTA_CTX;
+  Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
+  Cplx<T>* Rt = W + N * TL;
+  double* red = reinterpret_cast<double*>(Rt + 3 * g.NY2 * TL);
+  const double e = body_z_init<T, N, TL, NT>(c, W, Rt, red, g, A, S, has_scalar, tw);
+  if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
+}
+template <class T>
+__global__ void k_reality(Geometry g, Cplx<T>* S, int ncomp) {
+  reality_mode<T>(int(blockIdx.x * blockDim.x + threadIdx.x), g, S, ncomp);
+}
+// ConstantPower amplitude: band sum by thread 0; whole-field sum of the tile partials in a fixed
+// order (strided per thread, then a fixed tree).
+template <class T>
+__global__ void k_force_amp(Geometry g, const Cplx<T>* S, const double* partial, int npartial, double lo2,
+                            double hi2, double eps_rate, double eps_T, double* amp, unsigned int* status) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < npartial; i += 256) s += partial[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double whole = red[0];
+    const double band = band_energy_raw<T>(g, S, lo2, hi2);
+    const double n6 = double(g.N) * g.N * g.N * double(g.N) * g.N * g.N;
+    const double band_obs = 0.5 * (band / n6), whole_obs = 0.5 * (whole / n6);
+    double A = 0.0;
+    if (isfinite(band_obs) && band_obs > 10.0 * eps_T * whole_obs) A = eps_rate / (2.0 * band_obs);
+    else atomicOr(status, 0x2u);
+    amp[0] = A;
+    amp[1] = band_obs;
+    amp[2] = whole_obs;
+  }
+}
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) k_observables(Geometry g, const Cplx<T>* S, int has_scalar, double* out) {
+  CTA_CTX;
+  body_observables<T, NT>(c, reinterpret_cast<double*>(g_smem), g, S, has_scalar, out);
+}
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) k_spectrum(Geometry g, const Cplx<T>* S, int c0, int nc, int nshell, double* out) {
+  CTA_CTX;
+  double* hist = reinterpret_cast<double*>(g_smem);
+  body_spectrum<T, NT>(c, hist, hist + nshell, g, S, c0, nc, nshell, out);
+}
+template <class T>
+__global__ void k_tracers(int64_t M, int mode, const T* u, int N, double L, double* X, double* F, HeunWeights w) {
+  const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p < M) tracer_one<T>(p, M, mode, u, N, L, X, F, w);
+}
+template <class T>
+__global__ void k_to_T(const double* in, T* out, size_t n) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = T(in[i]);
+}
+#endif
+
+// ------------------------------------------------------------------------------------------------
+// Host helpers.
+// ------------------------------------------------------------------------------------------------
+static int compute_K(int N, double s, double cut2) {
+  int K = 0;
+  while (K + 1 < N / 2 + 1) {
+    const double k = s * double(K + 1);
+    if (k * k <= cut2) ++K;
+    else break;
+  }
+  return K;
+}
+
+
+template <class T, int N>
+class EngineImpl final : public Engine {
+  static constexpr int TLY = Shape<T>::TLY;
+  static constexpr int TLZ = Shape<T>::TLZ;
+  static constexpr int NTY = kNT(N * TLY / 8);
+  static constexpr int NTX = kNT(N);
+  static constexpr int NTZ = kNT(N * TLZ / 8);
+  static constexpr int NTR = kNT(256);
+
+ public:
+  ~EngineImpl() override {
+#ifndef GBGHT_EMU
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (auto& pr : pending_) {
+      cudaEventDestroy(pr.a);
+      cudaEventDestroy(pr.b);
+    }
+    for (cudaEvent_t e : pool_) cudaEventDestroy(e);
+    for (cudaEvent_t e : timer_ev_)
+      if (e) cudaEventDestroy(e);
+#endif
+    for (void* p : allocs_) rt_free(p);
+#ifndef GBGHT_EMU
+    if (stream_) cudaStreamDestroy(stream_);
+#endif
+  }
+
+  const char* init(const RunParams& p) override {
+    p_ = p;
+    const double s = 2.0 * M_PI / p.L;
+    const double cutoff = (2.0 / 3.0) * (double(N) / 2.0) * s;
+    cutoff_ = cutoff;
+    g_.N = N;
+    g_.s = s;
+    g_.cut2 = cutoff * cutoff;
+    g_.K = compute_K(N, s, g_.cut2);
+    g_.NY2 = 2 * g_.K + 1;
+    g_.KXP = ((g_.K + 1 + TLY - 1) / TLY) * TLY;
+    g_.inv_norm = 1.0 / (double(N) * double(N) * double(N));
+    if (g_.NY2 > N) return "grid too small for the retained band";
+    nS_ = size_t(g_.NY2) * g_.NY2 * g_.KXP;
+    nA_ = size_t(N) * g_.NY2 * g_.KXP;
+    nB_ = size_t(N) * N * g_.KXP;
+    nP_ = size_t(N) * N * N;
+    ntile_ = (g_.KXP / TLZ) * g_.NY2;
+    nshell_ = int(std::floor(std::sqrt(3.0) * N / 2.0 + 0.5)) + 1;
+#ifndef GBGHT_EMU
+    const char* e = cuda_err(cudaSetDevice(p.device), "cudaSetDevice");
+    if (e) return e;
+    e = cuda_err(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (e) return e;
+    if ((e = set_smem_attributes())) return e;
+#endif
+    const char* err = nullptr;
+    if ((err = alloc(&S_, 4 * nS_ * sizeof(Cplx<T>)))) return err;
+    if ((err = alloc(&H_, 4 * nS_ * sizeof(Cplx<T>)))) return err;
+    if ((err = alloc(&A_, 7 * nA_ * sizeof(Cplx<T>)))) return err;
+    if ((err = alloc(&B_, 7 * nB_ * sizeof(Cplx<T>)))) return err;
+    if ((err = alloc(&U_, 3 * nP_ * sizeof(T)))) return err;
+    if ((err = alloc(&tw_, N * sizeof(Cplx<T>)))) return err;
+    if ((err = alloc(&partial_, ntile_ * sizeof(double)))) return err;
+    if ((err = alloc(&amp_, 4 * sizeof(double)))) return err;
+    if ((err = alloc(&maxbits_, sizeof(unsigned long long)))) return err;
+    if ((err = alloc(&status_, sizeof(unsigned int)))) return err;
+    if ((err = alloc(&obs_, size_t(g_.NY2) * 4 * sizeof(double)))) return err;
+    if ((err = alloc(&spec_, size_t(g_.NY2) * nshell_ * sizeof(double)))) return err;
+    if (p.tracers > 0) {
+      if ((err = alloc(&X_, 3 * size_t(p.tracers) * sizeof(double)))) return err;
+      if ((err = alloc(&F_, 3 * size_t(p.tracers) * sizeof(double)))) return err;
+    }
+    // twiddles e^(-2πi k/N) in extended precision
+    std::vector<Cplx<T>> tw(N);
+    for (int k = 0; k < N; ++k) {
+      const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)N;
+      tw[k] = cmk<T>(T(cosl(a)), T(-sinl(a)));
+    }
+    if ((err = rt_h2d(tw_, tw.data(), N * sizeof(Cplx<T>), stream_))) return err;
+    return rt_sync(stream_);
+  }
+
+  int K() const override { return g_.K; }
+  double cutoff() const override { return cutoff_; }
+
+  // ---- state import / export (host arrays in the reference layout) ------------------------------
+  const char* import_state(const double* uh, const double* ph, bool* outside) override {
+    const int NH = N / 2 + 1;
+    const int nc = p_.scalar ? 4 : 3;
+    std::vector<Cplx<T>> host(4 * nS_, czero<T>());
+    *outside = false;
+    for (int cc = 0; cc < nc; ++cc) {
+      const double* src = cc < 3 ? uh + size_t(cc) * N * N * NH * 2 : ph;
+      for (int kz = 0; kz < N; ++kz)
+        for (int ky = 0; ky < N; ++ky)
+          for (int kx = 0; kx < NH; ++kx) {
+            const size_t si = ((size_t(kz) * N + ky) * NH + kx) * 2;
+            const double re = src[si], im = src[si + 1];
+            const int my = ky <= N / 2 ? ky : ky - N, mz = kz <= N / 2 ? kz : kz - N;
+            const bool in_box = kx <= g_.K && std::abs(my) <= g_.K && std::abs(mz) <= g_.K &&
+                                !(N % 2 == 0 && (ky == N / 2 || kz == N / 2));
+            bool retained = false;
+            if (in_box) {
+              const double kxd = g_.s * kx, kyd = g_.s * my, kzd = g_.s * mz;
+              retained = (kxd * kxd + kyd * kyd) + kzd * kzd <= g_.cut2;
+            }
+            if (!retained) {
+              if (re != 0.0 || im != 0.0) *outside = true;
+              continue;
+            }
+            const int qy = my >= 0 ? my : my + g_.NY2, qz = mz >= 0 ? mz : mz + g_.NY2;
+            host[idxS(g_, cc, qy, qz, kx)] = cmk<T>(T(re), T(im));
+          }
+    }
+    if (*outside) return nullptr;
+    const char* err = rt_h2d(S_, host.data(), 4 * nS_ * sizeof(Cplx<T>), stream_);
+    if (err) return err;
+    if ((err = rt_memset(H_, 0, 4 * nS_ * sizeof(Cplx<T>), stream_))) return err;
+    if ((err = z_init())) return err;
+    return rt_sync(stream_);
+  }
+
+  const char* export_state(double* uh, double* ph) override {
+    const int NH = N / 2 + 1;
+    std::vector<Cplx<T>> host(4 * nS_);
+    const char* err = rt_d2h(host.data(), S_, 4 * nS_ * sizeof(Cplx<T>), stream_);
+    if (err) return err;
+    const int nc = (p_.scalar && ph) ? 4 : 3;
+    for (int cc = 0; cc < nc; ++cc) {
+      double* dst = cc < 3 ? uh + size_t(cc) * N * N * NH * 2 : ph;
+      std::memset(dst, 0, size_t(N) * N * NH * 2 * sizeof(double));
+      for (int qy = 0; qy < g_.NY2; ++qy)
+        for (int qz = 0; qz < g_.NY2; ++qz)
+          for (int kx = 0; kx <= g_.K; ++kx) {
+            const int my = q_to_m(qy, g_.K, g_.NY2), mz = q_to_m(qz, g_.K, g_.NY2);
+            const int ky = my >= 0 ? my : my + N, kz = mz >= 0 ? mz : mz + N;
+            const Cplx<T> v = host[idxS(g_, cc, qy, qz, kx)];
+            const size_t di = ((size_t(kz) * N + ky) * NH + kx) * 2;
+            dst[di] = double(v.x);
+            dst[di + 1] = double(v.y);
+          }
+    }
+    return nullptr;
+  }
+
+  // ---- the step ---------------------------------------------------------------------------------
+  const char* step(double dt, const double* a, const double* b, const double* d, int S) override {
+    const double lo_hi[2] = {band_lo2(), band_hi2()};
+    for (int i = 0; i < S; ++i) {
+      StageArgs st;
+      st.a = a[i];
+      st.b = b[i];
+      st.dt = dt;
+      st.cu = -(p_.viscosity * (d[i] * dt));
+      st.cphi = -((p_.viscosity / p_.schmidt) * (d[i] * dt));
+      st.first = i == 0;
+      st.last = i == S - 1;
+      st.has_scalar = p_.scalar;
+      st.forced = p_.forcing != 0;
+      st.band_lo2 = lo_hi[0];
+      st.band_hi2 = lo_hi[1];
+      st.G[0] = p_.G[0];
+      st.G[1] = p_.G[1];
+      st.G[2] = p_.G[2];
+      const char* err = stage(st);
+      if (err) return err;
+    }
+    return rt_check();
+  }
+
+  const char* deposit(double* max_speed2) override {
+    const char* err = rt_memset(maxbits_, 0, sizeof(unsigned long long), stream_);
+    if (err) return err;
+    y_inverse(0, 3);
+    x_velocity();
+    if ((err = rt_check())) return err;
+    unsigned long long bits = 0;
+    if ((err = rt_d2h(&bits, maxbits_, sizeof bits, stream_))) return err;
+    double m;
+    std::memcpy(&m, &bits, sizeof m);
+    *max_speed2 = m;
+    return nullptr;
+  }
+
+  const char* velocity_export(double* u) override {
+    std::vector<T> host(3 * nP_);
+    const char* err = rt_d2h(host.data(), U_, 3 * nP_ * sizeof(T), stream_);
+    if (err) return err;
+    for (size_t i = 0; i < 3 * nP_; ++i) u[i] = double(host[i]);
+    return nullptr;
+  }
+
+  const char* velocity_import(const double* u) override {
+    std::vector<T> host(3 * nP_);
+    for (size_t i = 0; i < 3 * nP_; ++i) host[i] = T(u[i]);
+    const char* err = rt_h2d(U_, host.data(), 3 * nP_ * sizeof(T), stream_);
+    if (err) return err;
+    return rt_sync(stream_);
+  }
+
+  const char* observables(Observables* o) override {
+#ifdef GBGHT_EMU
+    emu_grid(g_.NY2, 1, 1, 4 * sizeof(double), [&](const Cta& c, void* sm) {
+      body_observables<T, 1>(c, static_cast<double*>(sm), g_, S_, p_.scalar, obs_);
+    });
+#else
+    pbegin(PROF_OBSERVABLES);
+    k_observables<T, NTR><<<g_.NY2, NTR, 4 * NTR * sizeof(double), stream_>>>(g_, S_, p_.scalar, obs_);
+    pend();
+#endif
+    const char* err = rt_check();
+    if (err) return err;
+    std::vector<double> host(size_t(g_.NY2) * 4);
+    if ((err = rt_d2h(host.data(), obs_, host.size() * sizeof(double), stream_))) return err;
+    double s[4] = {0, 0, 0, 0};
+    for (int qy = 0; qy < g_.NY2; ++qy)
+      for (int j = 0; j < 4; ++j) s[j] += host[qy * 4 + j];
+    const double n6 = double(N) * N * N * double(N) * N * N;
+    const double kappa = p_.viscosity / p_.schmidt;
+    o->k = 0.5 * (s[0] / n6);
+    o->eps = p_.viscosity * (s[1] / n6);
+    o->var = s[2] / n6;
+    o->chi = 2.0 * kappa * (s[3] / n6);
+    return nullptr;
+  }
+
+  const char* spectrum(int which, double* out, int nshell) override {
+    const int c0 = which == 0 ? 0 : 3, nc = which == 0 ? 3 : 1;
+    const size_t smem = (size_t(nshell_) + 2 * size_t(g_.KXP)) * sizeof(double);
+#ifdef GBGHT_EMU
+    emu_grid(g_.NY2, 1, 1, smem, [&](const Cta& c, void* sm) {
+      double* hist = static_cast<double*>(sm);
+      body_spectrum<T, 1>(c, hist, hist + nshell_, g_, S_, c0, nc, nshell_, spec_);
+    });
+#else
+    k_spectrum<T, 32><<<g_.NY2, 32, smem, stream_>>>(g_, S_, c0, nc, nshell_, spec_);
+#endif
+    const char* err = rt_check();
+    if (err) return err;
+    std::vector<double> host(size_t(g_.NY2) * nshell_);
+    if ((err = rt_d2h(host.data(), spec_, host.size() * sizeof(double), stream_))) return err;
+    const double n6 = double(N) * N * N * double(N) * N * N;
+    const double scale = which == 0 ? 1.0 / (2.0 * g_.s) : 1.0 / g_.s;
+    for (int n = 0; n < nshell && n < nshell_; ++n) {
+      double s = 0.0;
+      for (int qy = 0; qy < g_.NY2; ++qy) s += host[size_t(qy) * nshell_ + n];
+      out[n] = (s / n6) * scale;
+    }
+    for (int n = nshell_; n < nshell; ++n) out[n] = 0.0;
+    return nullptr;
+  }
+
+  // ---- tracers ----------------------------------------------------------------------------------
+  const char* tracers_set(const double* X) override {
+    if (!X_) return "the run carries no tracers";
+    const char* err = rt_h2d(X_, X, 3 * size_t(p_.tracers) * sizeof(double), stream_);
+    if (err) return err;
+    return rt_sync(stream_);
+  }
+  const char* tracers_get(double* X) override {
+    if (!X_) return "the run carries no tracers";
+    return rt_d2h(X, X_, 3 * size_t(p_.tracers) * sizeof(double), stream_);
+  }
+  const char* tracer_sample_get(double* F) override {
+    if (!F_) return "the run carries no tracers";
+    return rt_d2h(F, F_, 3 * size_t(p_.tracers) * sizeof(double), stream_);
+  }
+  const char* tracers_run(int mode, HeunWeights w) override {
+    if (!X_) return "the run carries no tracers";
+    run_tracers(p_.tracers, mode, X_, F_, w);
+    return rt_check();
+  }
+  const char* gather(const double* X, int64_t M, double* out) override {
+    if (M <= 0) return nullptr;
+    double *dX = nullptr, *dF = nullptr;
+    const char* err = rt_alloc(reinterpret_cast<void**>(&dX), 3 * size_t(M) * sizeof(double));
+    if (!err) err = rt_alloc(reinterpret_cast<void**>(&dF), 3 * size_t(M) * sizeof(double));
+    if (!err) err = rt_h2d(dX, X, 3 * size_t(M) * sizeof(double), stream_);
+    if (!err) {
+      run_tracers(M, 0, dX, dF, HeunWeights{0, 0, 0});
+      err = rt_check();
+    }
+    if (!err) err = rt_d2h(out, dF, 3 * size_t(M) * sizeof(double), stream_);
+    rt_free(dX);
+    rt_free(dF);
+    return err;
+  }
+
+  const char* sync() override { return rt_sync(stream_); }
+
+  const char* profile(int enable) override {
+#ifndef GBGHT_EMU
+    const char* e = collect();
+    if (e) return e;
+#endif
+    for (int k = 0; k < PROF_KINDS; ++k) {
+      prof_ms_[k] = 0.0;
+      prof_n_[k] = 0;
+    }
+    prof_on_ = enable != 0;
+    return nullptr;
+  }
+  const char* profile_read(int kind, int64_t* launches, double* total_ms) override {
+    if (kind < 0 || kind >= PROF_KINDS) return "unknown kernel kind";
+#ifndef GBGHT_EMU
+    const char* e = collect();
+    if (e) return e;
+#endif
+    *launches = prof_n_[kind];
+    *total_ms = prof_ms_[kind];
+    return nullptr;
+  }
+  const char* timer(int op, double* ms) override {
+#ifdef GBGHT_EMU
+    (void)op;
+    if (ms) *ms = 0.0;
+    return nullptr;
+#else
+    if (!timer_ev_[0]) {
+      for (auto& e : timer_ev_) {
+        const char* err = cuda_err(cudaEventCreate(&e), "cudaEventCreate");
+        if (err) return err;
+      }
+    }
+    if (op == 0) return cuda_err(cudaEventRecord(timer_ev_[0], stream_), "cudaEventRecord");
+    const char* err = cuda_err(cudaEventRecord(timer_ev_[1], stream_), "cudaEventRecord");
+    if (!err) err = cuda_err(cudaEventSynchronize(timer_ev_[1]), "cudaEventSynchronize");
+    float f = 0.f;
+    if (!err) err = cuda_err(cudaEventElapsedTime(&f, timer_ev_[0], timer_ev_[1]), "cudaEventElapsedTime");
+    if (ms) *ms = double(f);
+    return err;
+#endif
+  }
+
+  const char* status(uint32_t* word) override {
+    unsigned int v = 0;
+    const char* err = rt_d2h(&v, status_, sizeof v, stream_);
+    if (err) return err;
+    *word = v;
+    return rt_memset(status_, 0, sizeof v, stream_);
+  }
+
+ private:
+  // ---- per-kernel CUDA-event timing (profile on) ---------------------------------------------------
+#ifndef GBGHT_EMU
+  struct Pending {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  cudaEvent_t take_event() {
+    if (!pool_.empty()) {
+      cudaEvent_t e = pool_.back();
+      pool_.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+  void pbegin(int kind) {
+    if (!prof_on_) return;
+    cur_kind_ = kind;
+    cur_a_ = take_event();
+    cudaEventRecord(cur_a_, stream_);
+  }
+  void pend() {
+    if (!prof_on_ || !cur_a_) return;
+    cudaEvent_t b = take_event();
+    cudaEventRecord(b, stream_);
+    pending_.push_back(Pending{cur_kind_, cur_a_, b});
+    cur_a_ = nullptr;
+  }
+  const char* collect() {
+    if (pending_.empty()) return nullptr;
+    const char* e = rt_sync(stream_);
+    if (e) return e;
+    for (auto& pr : pending_) {
+      float f = 0.f;
+      cudaEventElapsedTime(&f, pr.a, pr.b);
+      prof_ms_[pr.kind] += double(f);
+      prof_n_[pr.kind] += 1;
+      pool_.push_back(pr.a);
+      pool_.push_back(pr.b);
+    }
+    pending_.clear();
+    return nullptr;
+  }
+  std::vector<Pending> pending_;
+  std::vector<cudaEvent_t> pool_;
+  cudaEvent_t cur_a_ = nullptr;
+  int cur_kind_ = 0;
+  cudaEvent_t timer_ev_[2] = {nullptr, nullptr};
+#else
+  void pbegin(int) {}
+  void pend() {}
+#endif
+  bool prof_on_ = false;
+  double prof_ms_[PROF_KINDS] = {};
+  int64_t prof_n_[PROF_KINDS] = {};
+
+  template <class P> const char* alloc(P** p, size_t n) {
+    void* v = nullptr;
+    const char* err = rt_alloc(&v, n);
+    if (err) return err;
+    allocs_.push_back(v);
+    *p = static_cast<P*>(v);
+    return nullptr;
+  }
+
+  double band_lo2() const {
+    const double lo = (p_.lowest_shell - 0.5) * g_.s;
+    return lo * lo;
+  }
+  double band_hi2() const {
+    const double top = std::isfinite(p_.highest_shell) ? p_.highest_shell : std::ceil(std::sqrt(3.0) * N / 2.0);
+    const double hi = (top + 0.5) * g_.s;
+    return hi * hi;
+  }
+
+  size_t smem_y() const { return size_t(N) * TLY * sizeof(Cplx<T>); }
+  size_t smem_x() const { return size_t(N) * 8 * sizeof(Cplx<T>) + size_t(NTX) * sizeof(double); }
+  size_t smem_z() const {
+    return (size_t(N) * TLZ + 3 * size_t(g_.NY2) * TLZ) * sizeof(Cplx<T>) + size_t(NTZ) * sizeof(double);
+  }
+
+#ifndef GBGHT_EMU
+  const char* set_smem_attributes() {
+    const char* e = nullptr;
+    auto set = [&](const void* f, size_t bytes) {
+      if (!e) e = cuda_err(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)),
+                           "cudaFuncSetAttribute");
+    };
+    set(reinterpret_cast<const void*>(k_y_inverse<T, N, TLY, NTY>), smem_y());
+    set(reinterpret_cast<const void*>(k_y_forward<T, N, TLY, NTY>), smem_y());
+    set(reinterpret_cast<const void*>(k_x_products<T, N, NTX>), smem_x());
+    set(reinterpret_cast<const void*>(k_x_velocity<T, N, NTX>), smem_x());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ>), smem_z());
+    set(reinterpret_cast<const void*>(k_z_init<T, N, TLZ, NTZ>), smem_z());
+    return e;
+  }
+#endif
+
+  void y_inverse(int c0, int nc) {
+#ifdef GBGHT_EMU
+    emu_grid(g_.KXP / TLY, N, nc, smem_y(), [&](const Cta& c, void* sm) {
+      body_y_inverse<T, N, TLY, 1>(c, static_cast<Cplx<T>*>(sm), g_, A_, B_, c0, tw_);
+    });
+#else
+    pbegin(PROF_Y_INVERSE);
+    k_y_inverse<T, N, TLY, NTY><<<dim3(g_.KXP / TLY, N, nc), NTY, smem_y(), stream_>>>(g_, A_, B_, c0, tw_);
+    pend();
+#endif
+  }
+  void y_forward(int nc) {
+#ifdef GBGHT_EMU
+    emu_grid(g_.KXP / TLY, N, nc, smem_y(), [&](const Cta& c, void* sm) {
+      body_y_forward<T, N, TLY, 1>(c, static_cast<Cplx<T>*>(sm), g_, B_, A_, tw_);
+    });
+#else
+    pbegin(PROF_Y_FORWARD);
+    k_y_forward<T, N, TLY, NTY><<<dim3(g_.KXP / TLY, N, nc), NTY, smem_y(), stream_>>>(g_, B_, A_, tw_);
+    pend();
+#endif
+  }
+  void x_products() {
+#ifdef GBGHT_EMU
+    emu_grid(N / 2, N, 1, smem_x(), [&](const Cta& c, void* sm) {
+      body_x_products<T, N, 1>(c, static_cast<Cplx<T>*>(sm), g_, B_, p_.scalar, tw_);
+    });
+#else
+    pbegin(PROF_X_PRODUCTS);
+    k_x_products<T, N, NTX><<<dim3(N / 2, N, 1), NTX, smem_x(), stream_>>>(g_, B_, p_.scalar, tw_);
+    pend();
+#endif
+  }
+  void x_velocity() {
+#ifdef GBGHT_EMU
+    unsigned long long* mb = maxbits_;
+    emu_grid(N / 4, N, 1, smem_x(), [&](const Cta& c, void* sm) {
+      Cplx<T>* s = static_cast<Cplx<T>*>(sm);
+      double* red = reinterpret_cast<double*>(s + N * 8);
+      const double m = body_x_velocity<T, N, 1>(c, s, red, g_, B_, U_, tw_);
+      unsigned long long bits;
+      std::memcpy(&bits, &m, sizeof bits);
+      if (bits > *mb) *mb = bits;
+    });
+#else
+    pbegin(PROF_X_VELOCITY);
+    k_x_velocity<T, N, NTX><<<dim3(N / 4, N, 1), NTX, smem_x(), stream_>>>(g_, B_, U_, maxbits_, tw_);
+    pend();
+#endif
+  }
+  void z_epilogue(const StageArgs& st) {
+#ifdef GBGHT_EMU
+    const int gx = g_.KXP / TLZ;
+    emu_grid(gx, g_.NY2, 1, smem_z(), [&](const Cta& c, void* sm) {
+      Cplx<T>* W = static_cast<Cplx<T>*>(sm);
+      Cplx<T>* Rt = W + N * TLZ;
+      double* red = reinterpret_cast<double*>(Rt + 3 * g_.NY2 * TLZ);
+      partial_[c.by * gx + c.bx] = body_z_epilogue<T, N, TLZ, 1>(c, W, Rt, red, g_, A_, S_, H_, st, amp_, tw_);
+    });
+#else
+    pbegin(PROF_Z_EPILOGUE);
+    k_z_epilogue<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, S_, H_, st, amp_,
+                                                                                           partial_, tw_);
+    pend();
+#endif
+  }
+  const char* z_init() {
+#ifdef GBGHT_EMU
+    const int gx = g_.KXP / TLZ;
+    emu_grid(gx, g_.NY2, 1, smem_z(), [&](const Cta& c, void* sm) {
+      Cplx<T>* W = static_cast<Cplx<T>*>(sm);
+      Cplx<T>* Rt = W + N * TLZ;
+      double* red = reinterpret_cast<double*>(Rt + 3 * g_.NY2 * TLZ);
+      partial_[c.by * gx + c.bx] = body_z_init<T, N, TLZ, 1>(c, W, Rt, red, g_, A_, S_, p_.scalar, tw_);
+    });
+#else
+    k_z_init<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, S_, p_.scalar, partial_,
+                                                                                       tw_);
+#endif
+    return rt_check();
+  }
+  void reality() {
+    const int n = g_.NY2 * g_.NY2;
+    const int nc = p_.scalar ? 4 : 3;
+#ifdef GBGHT_EMU
+    for (int i = 0; i < n; ++i) reality_mode<T>(i, g_, S_, nc);
+#else
+    pbegin(PROF_REALITY);
+    k_reality<T><<<(n + 255) / 256, 256, 0, stream_>>>(g_, S_, nc);
+    pend();
+#endif
+  }
+  void force_amp() {
+    const double eps_T = sizeof(T) == 8 ? DBL_EPSILON : double(FLT_EPSILON);
+#ifdef GBGHT_EMU
+    double whole = 0.0;
+    // the same association as the device tree: 256 strided partial sums, then pairwise halving
+    double red[256];
+    for (int t = 0; t < 256; ++t) {
+      double s = 0.0;
+      for (size_t i = t; i < ntile_; i += 256) s += partial_[i];
+      red[t] = s;
+    }
+    for (int w = 128; w > 0; w >>= 1)
+      for (int t = 0; t < w; ++t) red[t] += red[t + w];
+    whole = red[0];
+    const double band = band_energy_raw<T>(g_, S_, band_lo2(), band_hi2());
+    const double n6 = double(N) * N * N * double(N) * N * N;
+    const double band_obs = 0.5 * (band / n6), whole_obs = 0.5 * (whole / n6);
+    double A = 0.0;
+    if (std::isfinite(band_obs) && band_obs > 10.0 * eps_T * whole_obs) A = p_.injection_rate / (2.0 * band_obs);
+    else *status_ |= 0x2u;
+    amp_[0] = A;
+    amp_[1] = band_obs;
+    amp_[2] = whole_obs;
+#else
+    pbegin(PROF_FORCE_AMP);
+    k_force_amp<T><<<1, 256, 0, stream_>>>(g_, S_, partial_, int(ntile_), band_lo2(), band_hi2(), p_.injection_rate,
+                                           eps_T, amp_, status_);
+    pend();
+#endif
+  }
+  const char* stage(const StageArgs& st) {
+    const int ninv = p_.scalar ? 7 : 6;
+    const int nfwd = p_.scalar ? 6 : 3;
+    y_inverse(0, ninv);
+    x_products();
+    y_forward(nfwd);
+    if (st.forced) force_amp();
+    z_epilogue(st);
+    if (st.last) reality();
+    return rt_check();
+  }
+  void run_tracers(int64_t M, int mode, double* X, double* F, HeunWeights w) {
+#ifdef GBGHT_EMU
+    for (int64_t p = 0; p < M; ++p) tracer_one<T>(p, M, mode, U_, N, p_.L, X, F, w);
+#else
+    const int bs = 128;
+    pbegin(PROF_TRACERS);
+    k_tracers<T><<<unsigned((M + bs - 1) / bs), bs, 0, stream_>>>(M, mode, U_, N, p_.L, X, F, w);
+    pend();
+#endif
+  }
+
+  RunParams p_{};
+  Geometry g_{};
+  double cutoff_ = 0.0;
+  size_t nS_ = 0, nA_ = 0, nB_ = 0, nP_ = 0, ntile_ = 0;
+  int nshell_ = 0;
+  Stream stream_ = nullptr;
+  std::vector<void*> allocs_;
+  Cplx<T>*S_ = nullptr, *H_ = nullptr, *A_ = nullptr, *B_ = nullptr, *tw_ = nullptr;
+  T* U_ = nullptr;
+  double *partial_ = nullptr, *amp_ = nullptr, *obs_ = nullptr, *spec_ = nullptr;
+  double *X_ = nullptr, *F_ = nullptr;
+  unsigned long long* maxbits_ = nullptr;
+  unsigned int* status_ = nullptr;
+};
+
+#if defined(GBGHT_UNIT_FACTORY)
+template <class T, int N> Engine* new_engine();   // defined in the per-(T, N) units
+#else
+template <class T, int N>
+Engine* new_engine() {
+  return new EngineImpl<T, N>();
+}
+#endif
+
+#if defined(GBGHT_UNIT_T) && defined(GBGHT_UNIT_N)
+// one (precision, N) per translation unit, so the library's kernels compile in parallel
+template Engine* new_engine<GBGHT_UNIT_T, GBGHT_UNIT_N>();
+#endif
+
+#if !defined(GBGHT_UNIT_T)
+bool supported_N(int N) {
+  switch (N) {
+    case 8: case 12: case 16: case 24: case 32: case 48: case 64: case 96: case 128: case 192:
+    case 256: case 384: case 512:
+      return true;
+    default:
+      return false;
+  }
+}
+
+template <class T>
+static Engine* make_for(int N) {
+  switch (N) {
+    case 8: return new_engine<T, 8>();
+    case 12: return new_engine<T, 12>();
+    case 16: return new_engine<T, 16>();
+    case 24: return new_engine<T, 24>();
+    case 32: return new_engine<T, 32>();
+    case 48: return new_engine<T, 48>();
+    case 64: return new_engine<T, 64>();
+    case 96: return new_engine<T, 96>();
+    case 128: return new_engine<T, 128>();
+    case 192: return new_engine<T, 192>();
+    case 256: return new_engine<T, 256>();
+    case 384: return new_engine<T, 384>();
+    case 512: return new_engine<T, 512>();
+    default: return nullptr;
+  }
+}
+
+Engine* make_engine(int N, int precision, std::string* err) {
+  if (!supported_N(N)) {
+    *err = "grid_points_per_axis must be one of 8 12 16 24 32 48 64 96 128 192 256 384 512";
+    return nullptr;
+  }
+  Engine* e = precision == 1 ? make_for<float>(N) : make_for<double>(N);
+  if (!e) *err = "unsupported configuration";
+  return e;
+}
+#endif
+
+}  // namespace gbght

@@ -1,0 +1,94 @@
+// The engine: device buffers and the launch sequence of the IF-RK step for one (precision, N).
+//
+// The same source builds two ways. With nvcc it is the CUDA library: kernels launched on the
+// run's stream. With -DGBGHT_EMU and a host C++ compiler, every "device" buffer is host memory
+// and every launch runs the same CTA bodies block by block with one thread (NT = 1). That build
+// exists only to check the kernels' index arithmetic on a CPU against the oracle; the product
+// library is the CUDA build and has no host path.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "passes.cuh"
+#include "tracers.cuh"
+
+#ifndef GBGHT_EMU
+#include <cuda_runtime.h>
+#endif
+
+namespace gbght {
+
+// The parameters of a run that the engine needs (a copy of the public config, validated).
+struct RunParams {
+  int N;
+  double L;
+  int precision;
+  int scheme;
+  double viscosity, schmidt;
+  int scalar;
+  int forcing;
+  double injection_rate;
+  int lowest_shell;
+  double highest_shell;
+  double G[3];
+  int64_t tracers;
+  int device;
+};
+
+// Host-visible results of the reductions.
+struct Observables {
+  double k, eps, var, chi;
+};
+
+class Engine {
+ public:
+  virtual ~Engine() {}
+  // All methods return nullptr on success, else a static or engine-owned error message.
+  virtual const char* init(const RunParams& p) = 0;
+  virtual const char* import_state(const double* uh, const double* ph, bool* outside) = 0;
+  virtual const char* export_state(double* uh, double* ph) = 0;
+  virtual const char* step(double dt, const double* a, const double* b, const double* d, int S) = 0;
+  virtual const char* deposit(double* max_speed2) = 0;
+  virtual const char* velocity_export(double* u) = 0;
+  virtual const char* velocity_import(const double* u) = 0;
+  virtual const char* observables(Observables* o) = 0;
+  virtual const char* spectrum(int which, double* out, int nshell) = 0;
+  virtual const char* tracers_set(const double* X) = 0;
+  virtual const char* tracers_get(double* X) = 0;
+  virtual const char* tracer_sample_get(double* F) = 0;
+  // mode 0: sample at the positions; 1: Heun push; 2: Heun push + sample at the new positions
+  virtual const char* tracers_run(int mode, HeunWeights w) = 0;
+  virtual const char* gather(const double* X, int64_t M, double* out) = 0;
+  virtual const char* sync() = 0;
+  // CUDA-event timing on the run's stream: per-kernel launch counts and total milliseconds while
+  // profiling is on, and a start/stop pair around any region.
+  virtual const char* profile(int enable) = 0;
+  virtual const char* profile_read(int kind, int64_t* launches, double* total_ms) = 0;
+  virtual const char* timer(int op, double* ms) = 0;
+  virtual const char* status(uint32_t* word) = 0;
+  virtual int K() const = 0;
+  virtual double cutoff() const = 0;
+};
+
+// Kernel kinds reported by Engine::profile_read (and gbght_profile_read).
+enum ProfileKind {
+  PROF_Y_INVERSE = 0,
+  PROF_X_PRODUCTS = 1,
+  PROF_Y_FORWARD = 2,
+  PROF_Z_EPILOGUE = 3,
+  PROF_X_VELOCITY = 4,
+  PROF_FORCE_AMP = 5,
+  PROF_REALITY = 6,
+  PROF_TRACERS = 7,
+  PROF_OBSERVABLES = 8,
+  PROF_KINDS = 9
+};
+
+Engine* make_engine(int N, int precision, std::string* err);
+bool supported_N(int N);
+
+}  // namespace gbght

@@ -1,0 +1,616 @@
+// The passes of one IF-RK stage, written as CTA bodies (see gbght_common.cuh for the execution
+// model).
+//
+// Layouts in HBM (complex elements; K is the largest retained |m| per axis, NY2 = 2K+1, KXP is
+// K+1 rounded up to a whole number of 128-byte rows). Every retained mode of the 2/3 ball has
+// |m_x|, |m_y|, |m_z| ≤ K, so the spectral state is stored compactly. The transforms are pruned
+// to that box: an inverse pass never reads a mode outside the box, and a forward pass never writes
+// one.
+//   compact index q ∈ [0, NY2) ↔ m = q for q ≤ K, m = q − NY2 for q > K
+//   FFT row of q: e(q) = q (q ≤ K) or q + N − NY2 (q > K)
+//   S-layout  [c][ky'][kz'][kx]  state û, φ̂ and the accumulators h        (NY2·NY2·KXP)
+//   A-layout  [c][z][ky'][kx]    z-transformed spectra                     (N·NY2·KXP)
+//   B-layout  [c][z][y][kx]      y- and z-transformed spectra              (N·N·KXP)
+//   physical  [c][z][y][x]       real values, x contiguous                 (N·N·N)
+// Component slots: 0-2 velocity, 3-5 vorticity, 6 scalar (A and B). After the x-pass, B slots
+// 0-2 hold FFT(u×ω) and slots 3-5 hold FFT(uφ) (x transformed only). After the forward y-pass,
+// A slots 0-5 hold them y-transformed as well.
+//
+// A stage runs: y-inverse (A→B), x-pass (B→B: c2r, products, r2c), y-forward (B→A), then
+// z-forward + epilogue + z-inverse (A, S, H → S, H, A).
+#pragma once
+
+#include "fft_tile.cuh"
+
+namespace gbght {
+
+struct Geometry {
+  int N, K, NY2, KXP;
+  double s;          // 2π/L, the fundamental wavenumber
+  double cut2;       // square of the dealias cutoff T(2/3)·T(N/2)·T(2π/L)
+  double inv_norm;   // 1/N³, the inverse transform's normalisation
+};
+
+GBGHT_HD int q_to_m(int q, int K, int NY2) { return q <= K ? q : q - NY2; }
+GBGHT_HD int q_to_row(int q, int K, int N, int NY2) { return q <= K ? q : q + N - NY2; }
+
+GBGHT_HD size_t idxA(const Geometry& g, int c, int z, int q, int kx) {
+  return ((size_t(c) * g.N + z) * g.NY2 + q) * g.KXP + kx;
+}
+GBGHT_HD size_t idxB(const Geometry& g, int c, int z, int y, int kx) {
+  return ((size_t(c) * g.N + z) * g.N + y) * g.KXP + kx;
+}
+GBGHT_HD size_t idxS(const Geometry& g, int c, int qy, int qz, int kx) {
+  return ((size_t(c) * g.NY2 + qy) * g.NY2 + qz) * g.KXP + kx;
+}
+
+// ================================================================================================
+// y-inverse: A[c][z][ky'][tile] → B[c][z][y][tile], one tile of TL kx columns per CTA.
+// Grid: (KXP/TL, N, ncomp); c = c0 + bz.
+// ================================================================================================
+template <class T, int N, int TL, int NT>
+GBGHT_HD void body_y_inverse(const Cta& c, Cplx<T>* sm, const Geometry& g,
+                             const Cplx<T>* GBGHT_RESTRICT A, Cplx<T>* GBGHT_RESTRICT B,
+                             int c0, const Cplx<T>* GBGHT_RESTRICT tw) {
+  const int kx0 = c.bx * TL, z = c.by, comp = c0 + c.bz;
+  for (int i = c.tid; i < N * TL; i += NT) {
+    const int e = i / TL, l = i % TL;
+    Cplx<T> v = czero<T>();
+    int q = -1;
+    if (e <= g.K) q = e;
+    else if (e >= N - g.K) q = e - N + g.NY2;
+    if (q >= 0) v = A[idxA(g, comp, z, q, kx0 + l)];
+    sm[i] = v;
+  }
+  GBGHT_SYNC();
+  tile_fft<T, N, TL, NT, +1>(c, sm, tw);
+  for (int i = c.tid; i < N * TL; i += NT) {
+    const int y = i / TL, l = i % TL;
+    B[idxB(g, comp, z, y, kx0 + l)] = sm[i];
+  }
+}
+
+// ================================================================================================
+// y-forward: B[c][z][y][tile] → A[c][z][ky'][tile] (retained rows only).
+// Grid: (KXP/TL, N, ncomp).
+// ================================================================================================
+template <class T, int N, int TL, int NT>
+GBGHT_HD void body_y_forward(const Cta& c, Cplx<T>* sm, const Geometry& g,
+                             const Cplx<T>* GBGHT_RESTRICT B, Cplx<T>* GBGHT_RESTRICT A,
+                             const Cplx<T>* GBGHT_RESTRICT tw) {
+  const int kx0 = c.bx * TL, z = c.by, comp = c.bz;
+  for (int i = c.tid; i < N * TL; i += NT) {
+    const int y = i / TL, l = i % TL;
+    sm[i] = B[idxB(g, comp, z, y, kx0 + l)];
+  }
+  GBGHT_SYNC();
+  tile_fft<T, N, TL, NT, -1>(c, sm, tw);
+  for (int i = c.tid; i < g.NY2 * TL; i += NT) {
+    const int q = i / TL, l = i % TL;
+    A[idxA(g, comp, z, q, kx0 + l)] = sm[q_to_row(q, g.K, N, g.NY2) * TL + l];
+  }
+}
+
+// ================================================================================================
+// x-pass: for two points (z, y0) and (z, y0+1), c2r of u, ω, φ, the products u×ω and uφ, and
+// r2c of the six products. The spectra stay in B's slots (in place). Grid: (N/2, N).
+// Eight lines of the tile:
+//   inverse: line 3p+0 = u_x + i·u_y, 3p+1 = u_z + i·ω_x, 3p+2 = ω_y + i·ω_z (point p), line 6 =
+//            φ(p=0) + i·φ(p=1), line 7 unused
+//   forward: line 3p+0 = n_x + i·n_y, 3p+1 = n_z + i·f_x, 3p+2 = f_y + i·f_z, n = u×ω, f = uφ
+// Two real lines a, b share one complex transform ("two for one"). Inverse: Z[e] = A[e] + i·B[e]
+// for 0 ≤ e ≤ K, and Z[N−e] = conj(A[e]) + i·conj(B[e]); only the real parts of the kx = 0 bins
+// enter, as in a c2r. Forward: A[k] = (Z[k] + conj Z[N−k])/2, B[k] = (Z[k] − conj Z[N−k])/(2i).
+// ================================================================================================
+template <class T>
+GBGHT_HD void pack_pair(Cplx<T>* sm, int TL, int N, int line, int e, Cplx<T> a, Cplx<T> b, T sc) {
+  if (e == 0) {
+    sm[line] = cmk<T>(a.x * sc, b.x * sc);
+  } else {
+    sm[e * TL + line] = cmk<T>((a.x - b.y) * sc, (a.y + b.x) * sc);
+    sm[(N - e) * TL + line] = cmk<T>((a.x + b.y) * sc, (b.x - a.y) * sc);
+  }
+}
+
+template <class T>
+GBGHT_HD void unpack_pair(const Cplx<T>* sm, int TL, int N, int line, int k, Cplx<T>& a, Cplx<T>& b) {
+  const Cplx<T> z = sm[k * TL + line];
+  const Cplx<T> zc = conj(sm[((N - k) % N) * TL + line]);
+  const Cplx<T> sp = z + zc, sd = z - zc;
+  a = cmk<T>(sp.x * T(0.5), sp.y * T(0.5));
+  b = cmk<T>(sd.y * T(0.5), -sd.x * T(0.5));
+}
+
+template <class T, int N, int NT>
+GBGHT_HD void body_x_products(const Cta& c, Cplx<T>* sm, const Geometry& g,
+                              Cplx<T>* GBGHT_RESTRICT B, int has_scalar,
+                              const Cplx<T>* GBGHT_RESTRICT tw) {
+  constexpr int TL = 8;
+  const int y0 = 2 * c.bx, z = c.by;
+  const T sc = T(g.inv_norm);
+  const int KX1 = g.K + 1;
+  // zero rows that no mode reaches (K < e < N−K)
+  for (int i = c.tid; i < N * TL; i += NT) {
+    const int e = i / TL;
+    if (e > g.K && e < N - g.K) sm[i] = czero<T>();
+  }
+  if (!has_scalar)
+    for (int i = c.tid; i < N; i += NT) sm[i * TL + 6] = czero<T>();
+  for (int i = c.tid; i < N; i += NT) sm[i * TL + 7] = czero<T>();
+  // lines 0..5: three pairs per point
+  for (int i = c.tid; i < 2 * 3 * KX1; i += NT) {
+    const int e = i % KX1, pr = (i / KX1) % 3, p = i / (3 * KX1);
+    const int ca = 2 * pr, cb = 2 * pr + 1;   // (0,1), (2,3), (4,5)
+    const Cplx<T> a = B[idxB(g, ca, z, y0 + p, e)];
+    const Cplx<T> b = B[idxB(g, cb, z, y0 + p, e)];
+    pack_pair(sm, TL, N, 3 * p + pr, e, a, b, sc);
+  }
+  if (has_scalar)
+    for (int e = c.tid; e < KX1; e += NT) {
+      const Cplx<T> a = B[idxB(g, 6, z, y0, e)];
+      const Cplx<T> b = B[idxB(g, 6, z, y0 + 1, e)];
+      pack_pair(sm, TL, N, 6, e, a, b, sc);
+    }
+  GBGHT_SYNC();
+  tile_fft<T, N, TL, NT, +1>(c, sm, tw);
+  for (int x = c.tid; x < N; x += NT) {
+    Cplx<T>* row = sm + x * TL;
+    const Cplx<T> l6 = row[6];
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      const Cplx<T> L0 = row[3 * p], L1 = row[3 * p + 1], L2 = row[3 * p + 2];
+      const T ux = L0.x, uy = L0.y, uz = L1.x, wx = L1.y, wy = L2.x, wz = L2.y;
+      const T ph = p == 0 ? l6.x : l6.y;
+      const T nx = uy * wz - uz * wy, ny = uz * wx - ux * wz, nz = ux * wy - uy * wx;
+      row[3 * p] = cmk<T>(nx, ny);
+      row[3 * p + 1] = cmk<T>(nz, ux * ph);
+      row[3 * p + 2] = cmk<T>(uy * ph, uz * ph);
+    }
+  }
+  GBGHT_SYNC();
+  tile_fft<T, N, TL, NT, -1>(c, sm, tw);
+  // extract kx ∈ [0, KXP): products 0..2 = n, 3..5 = f; pad columns get zeros
+  const int ncomp = has_scalar ? 6 : 3;
+  for (int i = c.tid; i < 2 * 3 * g.KXP; i += NT) {
+    const int k = i % g.KXP, pr = (i / g.KXP) % 3, p = i / (3 * g.KXP);
+    Cplx<T> a = czero<T>(), b = czero<T>();
+    if (k < KX1) unpack_pair(sm, TL, N, 3 * p + pr, k, a, b);
+    const int ca = 2 * pr, cb = 2 * pr + 1;
+    if (ca < ncomp) B[idxB(g, ca, z, y0 + p, k)] = a;
+    if (cb < ncomp) B[idxB(g, cb, z, y0 + p, k)] = b;
+  }
+}
+
+// ================================================================================================
+// x-pass of the deposit: velocity to physical for four points (z, y0..y0+3), the physical
+// velocity written out, and the maximum of |u|² reduced. Grid: (N/4, N).
+//   line p (p < 4) = u_x + i·u_y of point p; line 4 = u_z(0) + i·u_z(1); line 5 = u_z(2) + i·u_z(3)
+// `red` is NT doubles of shared scratch; the CTA's maximum of |u|² is returned to thread 0.
+// ================================================================================================
+template <class T, int N, int NT>
+GBGHT_HD double body_x_velocity(const Cta& c, Cplx<T>* sm, double* red, const Geometry& g,
+                                const Cplx<T>* GBGHT_RESTRICT B, T* GBGHT_RESTRICT u_phys,
+                                const Cplx<T>* GBGHT_RESTRICT tw) {
+  constexpr int TL = 8;
+  const int y0 = 4 * c.bx, z = c.by;
+  const T sc = T(g.inv_norm);
+  const int KX1 = g.K + 1;
+  for (int i = c.tid; i < N * TL; i += NT) {
+    const int e = i / TL, l = i % TL;
+    if ((e > g.K && e < N - g.K) || l >= 6) sm[i] = czero<T>();
+  }
+  for (int i = c.tid; i < 6 * KX1; i += NT) {
+    const int e = i % KX1, line = i / KX1;
+    Cplx<T> a, b;
+    if (line < 4) {
+      a = B[idxB(g, 0, z, y0 + line, e)];
+      b = B[idxB(g, 1, z, y0 + line, e)];
+    } else {
+      const int p = 2 * (line - 4);
+      a = B[idxB(g, 2, z, y0 + p, e)];
+      b = B[idxB(g, 2, z, y0 + p + 1, e)];
+    }
+    pack_pair(sm, TL, N, line, e, a, b, sc);
+  }
+  GBGHT_SYNC();
+  tile_fft<T, N, TL, NT, +1>(c, sm, tw);
+  double m = 0.0;
+  for (int i = c.tid; i < 4 * N; i += NT) {
+    const int x = i % N, p = i / N;
+    const Cplx<T> uxy = sm[x * TL + p];
+    const Cplx<T> uzz = sm[x * TL + 4 + (p >> 1)];
+    const T uz = (p & 1) ? uzz.y : uzz.x;
+    const size_t base = (size_t(z) * N + (y0 + p)) * N + x;
+    const size_t comp = size_t(N) * N * N;
+    u_phys[base] = uxy.x;
+    u_phys[comp + base] = uxy.y;
+    u_phys[2 * comp + base] = uz;
+    const double sp = (double(uxy.x) * double(uxy.x) + double(uxy.y) * double(uxy.y)) + double(uz) * double(uz);
+    m = (sp > m || sp != sp) ? sp : m;
+  }
+  red[c.tid] = m;
+  GBGHT_SYNC();
+  if (c.tid == 0) {
+    double r = 0.0;
+    for (int i = 0; i < NT; ++i) r = (red[i] > r || red[i] != red[i]) ? red[i] : r;
+    return r;
+  }
+  return 0.0;
+}
+
+
+// Forward z-transform of A slots [c0, c0+3) of one tile into Rt[j][q][l] (retained rows only).
+template <class T, int N, int TL, int NT>
+GBGHT_HD void z_forward3(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, const Geometry& g,
+                         const Cplx<T>* GBGHT_RESTRICT A, int c0, int qy, int kx0,
+                         const Cplx<T>* GBGHT_RESTRICT tw) {
+  for (int j = 0; j < 3; ++j) {
+    for (int i = c.tid; i < N * TL; i += NT) {
+      const int z = i / TL, l = i % TL;
+      W[i] = A[idxA(g, c0 + j, z, qy, kx0 + l)];
+    }
+    GBGHT_SYNC();
+    tile_fft<T, N, TL, NT, -1>(c, W, tw);
+    for (int i = c.tid; i < g.NY2 * TL; i += NT) {
+      const int q = i / TL, l = i % TL;
+      Rt[(j * g.NY2 + q) * TL + l] = W[q_to_row(q, g.K, N, g.NY2) * TL + l];
+    }
+    GBGHT_SYNC();
+  }
+}
+
+// Inverse z-transform of one retained column set, value(q, l), into A slot `dst` of the tile.
+template <class T, int N, int TL, int NT, class F>
+GBGHT_HD void z_inverse1(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* GBGHT_RESTRICT A,
+                         int dst, int qy, int kx0, F&& value, const Cplx<T>* GBGHT_RESTRICT tw) {
+  for (int i = c.tid; i < N * TL; i += NT) {
+    const int e = i / TL;
+    if (e > g.K && e < N - g.K) W[i] = czero<T>();
+  }
+  for (int i = c.tid; i < g.NY2 * TL; i += NT) {
+    const int q = i / TL, l = i % TL;
+    W[q_to_row(q, g.K, N, g.NY2) * TL + l] = value(q, l);
+  }
+  GBGHT_SYNC();
+  tile_fft<T, N, TL, NT, +1>(c, W, tw);
+  for (int i = c.tid; i < N * TL; i += NT) {
+    const int z = i / TL, l = i % TL;
+    A[idxA(g, dst, z, qy, kx0 + l)] = W[i];
+  }
+  GBGHT_SYNC();
+}
+
+// ω̂ component o of iκ × û from the retained velocity columns Rt[0..2].
+template <class T, int TL>
+GBGHT_HD Cplx<T> curl_component(const Geometry& g, const Cplx<T>* Rt, int o, int q, int l, int kx0, double ky) {
+  const int kx = kx0 + l;
+  const int mz = q_to_m(q, g.K, g.NY2);
+  const T kX = T(g.s * double(kx)), kY = T(ky), kZ = T(g.s * double(mz));
+  const Cplx<T> u0 = Rt[(0 * g.NY2 + q) * TL + l], u1 = Rt[(1 * g.NY2 + q) * TL + l],
+                u2 = Rt[(2 * g.NY2 + q) * TL + l];
+  Cplx<T> cr;
+  if (o == 0) cr = scale(u2, kY) - scale(u1, kZ);
+  else if (o == 1) cr = scale(u0, kZ) - scale(u2, kX);
+  else cr = scale(u1, kX) - scale(u0, kY);
+  return mul_i(cr);
+}
+
+// ================================================================================================
+// z-forward + epilogue + z-inverse, one tile (ky', kx0..kx0+TL) per CTA. Grid: (KXP/TL, NY2).
+//
+// Epilogue per retained mode, stage i of the 2N loop (src/Propagator.jl:326-419):
+//   N̂_φ = −𝔻 iκ·FFT(uφ) − G·û_i                          (src/Generator.jl:708-720; G is an extension)
+//   N̂_u = 𝔻 ℙ FFT(u×ω), κ = 0 zeroed, + A 𝟙_band û_i     (src/Generator.jl:484-534, Forcing.jl:1104-1117)
+//   h ← dt·N̂ (i = 0) or a_i h + dt·N̂
+//   q ← E(q + b_i h), h ← E h (i < S−1), E = exp(c_i |κ|²), c_i = −D·(d_i·dt)
+//   last stage: û ← ℙ û                                  (src/Propagator.jl:401)
+// and the z-inverse of the new û, iκ×û and φ̂ into A slots 0..6 for the next stage's y-inverse.
+// `red` holds NT doubles; the CTA's sum of the Hermitian-weighted |û_new|² is returned to thread 0.
+// ================================================================================================
+struct StageArgs {
+  double a, b, dt;      // tableau a_i, b_i and the step
+  double cu, cphi;      // exponents c_i = −D·(d_i·dt) for velocity and scalar
+  int first, last;      // stage 0, stage S−1
+  int has_scalar;
+  int forced;           // velocity forcing active (ConstantPower)
+  double band_lo2, band_hi2;   // squared band edges
+  double G[3];          // mean scalar gradient (extension)
+};
+
+template <class T, int N, int TL, int NT>
+GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, const Geometry& g,
+                                Cplx<T>* GBGHT_RESTRICT A, Cplx<T>* GBGHT_RESTRICT S,
+                                Cplx<T>* GBGHT_RESTRICT H, const StageArgs& st,
+                                const double* GBGHT_RESTRICT force_amp,
+                                const Cplx<T>* GBGHT_RESTRICT tw) {
+  const int kx0 = c.bx * TL, qy = c.by;
+  const int NY2 = g.NY2;
+  const double s = g.s;
+  const int my = q_to_m(qy, g.K, NY2);
+  const double ky = s * double(my);
+
+  // ---------------- scalar -------------------------------------------------------------------------
+  if (st.has_scalar) {
+    z_forward3<T, N, TL, NT>(c, W, Rt, g, A, 3, qy, kx0, tw);
+    for (int i = c.tid; i < NY2 * TL; i += NT) {
+      const int q = i / TL, l = i % TL;
+      const int kx = kx0 + l;
+      const int mz = q_to_m(q, g.K, NY2);
+      const double kxd = s * double(kx), kzd = s * double(mz);
+      const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
+      const bool keep = kx <= g.K && k2 <= g.cut2;
+      const size_t si = idxS(g, 3, qy, q, kx);
+      Cplx<T> phi = S[si];
+      Cplx<T> nphi = czero<T>();
+      if (keep) {
+        const Cplx<T> fx = Rt[(0 * NY2 + q) * TL + l], fy = Rt[(1 * NY2 + q) * TL + l],
+                      fz = Rt[(2 * NY2 + q) * TL + l];
+        // −i(κx fx + κy fy + κz fz)
+        const Cplx<T> dsum = cmk<T>(T(kxd) * fx.x + T(ky) * fy.x + T(kzd) * fz.x,
+                                    T(kxd) * fx.y + T(ky) * fy.y + T(kzd) * fz.y);
+        nphi = mul_mi(dsum);
+      }
+      if (st.G[0] != 0.0 || st.G[1] != 0.0 || st.G[2] != 0.0) {
+        const Cplx<T> ux = S[idxS(g, 0, qy, q, kx)], uy = S[idxS(g, 1, qy, q, kx)],
+                      uz = S[idxS(g, 2, qy, q, kx)];
+        const T G0 = T(st.G[0]), G1 = T(st.G[1]), G2 = T(st.G[2]);
+        nphi = nphi - cmk<T>(G0 * ux.x + G1 * uy.x + G2 * uz.x, G0 * ux.y + G1 * uy.y + G2 * uz.y);
+      }
+      Cplx<T> h = st.first ? scale(nphi, T(st.dt))
+                           : scale(H[si], T(st.a)) + scale(nphi, T(st.dt));
+      const T E = T(exp(st.cphi * k2));
+      phi = scale(phi + scale(h, T(st.b)), E);
+      S[si] = phi;
+      if (!st.last) H[si] = scale(h, E);
+      Rt[(0 * NY2 + q) * TL + l] = phi;
+    }
+    GBGHT_SYNC();
+    z_inverse1<T, N, TL, NT>(c, W, g, A, 6, qy, kx0, [&](int q, int l) { return Rt[(0 * NY2 + q) * TL + l]; }, tw);
+  }
+
+  // ---------------- velocity -----------------------------------------------------------------------
+  z_forward3<T, N, TL, NT>(c, W, Rt, g, A, 0, qy, kx0, tw);
+  const double A_f = st.forced ? force_amp[0] : 0.0;
+  double esum = 0.0;
+  for (int i = c.tid; i < NY2 * TL; i += NT) {
+    const int q = i / TL, l = i % TL;
+    const int kx = kx0 + l;
+    const int mz = q_to_m(q, g.K, NY2);
+    const double kxd = s * double(kx), kzd = s * double(mz);
+    const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
+    const bool keep = kx <= g.K && k2 <= g.cut2;
+    const size_t s0 = idxS(g, 0, qy, q, kx), s1 = idxS(g, 1, qy, q, kx), s2 = idxS(g, 2, qy, q, kx);
+    Cplx<T> u0 = S[s0], u1 = S[s1], u2 = S[s2];
+    Cplx<T> n0 = czero<T>(), n1 = czero<T>(), n2 = czero<T>();
+    if (keep && k2 > 0.0) {
+      const Cplx<T> f0 = Rt[(0 * NY2 + q) * TL + l], f1 = Rt[(1 * NY2 + q) * TL + l],
+                    f2 = Rt[(2 * NY2 + q) * TL + l];
+      const T kX = T(kxd), kY = T(ky), kZ = T(kzd);
+      const T ik2 = T(1.0 / k2);
+      const Cplx<T> kd = cmk<T>((kX * f0.x + kY * f1.x + kZ * f2.x) * ik2, (kX * f0.y + kY * f1.y + kZ * f2.y) * ik2);
+      n0 = f0 - scale(kd, kX);
+      n1 = f1 - scale(kd, kY);
+      n2 = f2 - scale(kd, kZ);
+    }
+    if (A_f != 0.0 && k2 >= st.band_lo2 && k2 <= st.band_hi2) {
+      const T Af = T(A_f);
+      n0 = n0 + scale(u0, Af);
+      n1 = n1 + scale(u1, Af);
+      n2 = n2 + scale(u2, Af);
+    }
+    const T dt = T(st.dt), a = T(st.a), b = T(st.b);
+    Cplx<T> h0, h1, h2;
+    if (st.first) {
+      h0 = scale(n0, dt); h1 = scale(n1, dt); h2 = scale(n2, dt);
+    } else {
+      h0 = scale(H[s0], a) + scale(n0, dt);
+      h1 = scale(H[s1], a) + scale(n1, dt);
+      h2 = scale(H[s2], a) + scale(n2, dt);
+    }
+    const T E = T(exp(st.cu * k2));
+    u0 = scale(u0 + scale(h0, b), E);
+    u1 = scale(u1 + scale(h1, b), E);
+    u2 = scale(u2 + scale(h2, b), E);
+    if (st.last) {
+      if (k2 > 0.0) {
+        const T kX = T(kxd), kY = T(ky), kZ = T(kzd);
+        const T ik2 = T(1.0 / k2);
+        const Cplx<T> kd = cmk<T>((kX * u0.x + kY * u1.x + kZ * u2.x) * ik2, (kX * u0.y + kY * u1.y + kZ * u2.y) * ik2);
+        u0 = u0 - scale(kd, kX);
+        u1 = u1 - scale(kd, kY);
+        u2 = u2 - scale(kd, kZ);
+      }
+    } else {
+      H[s0] = scale(h0, E);
+      H[s1] = scale(h1, E);
+      H[s2] = scale(h2, E);
+    }
+    S[s0] = u0;
+    S[s1] = u1;
+    S[s2] = u2;
+    Rt[(0 * NY2 + q) * TL + l] = u0;
+    Rt[(1 * NY2 + q) * TL + l] = u1;
+    Rt[(2 * NY2 + q) * TL + l] = u2;
+    const double w = kx == 0 ? 1.0 : 2.0;
+    esum += w * ((double(u0.x) * u0.x + double(u0.y) * u0.y) + (double(u1.x) * u1.x + double(u1.y) * u1.y) +
+                 (double(u2.x) * u2.x + double(u2.y) * u2.y));
+  }
+  red[c.tid] = esum;
+  GBGHT_SYNC();
+  double total = 0.0;
+  if (c.tid == 0)
+    for (int i = 0; i < NT; ++i) total += red[i];
+  // z-inverse of û and of ω̂ = iκ × û
+  for (int o = 0; o < 3; ++o)
+    z_inverse1<T, N, TL, NT>(c, W, g, A, o, qy, kx0, [&](int q, int l) { return Rt[(o * NY2 + q) * TL + l]; }, tw);
+  for (int o = 0; o < 3; ++o)
+    z_inverse1<T, N, TL, NT>(c, W, g, A, 3 + o, qy, kx0,
+                             [&](int q, int l) { return curl_component<T, TL>(g, Rt, o, q, l, kx0, ky); }, tw);
+  return total;
+}
+
+// ================================================================================================
+// Reality projection of the kx = 0 plane of S slots [0, ncomp) (src/Propagator.jl:411-412): each
+// pair (m_y, m_z) ↔ (−m_y, −m_z) is replaced by its Hermitian part. One thread per compact mode;
+// the member with the smaller flat index writes both. Grid covers NY2·NY2 threads.
+// ================================================================================================
+template <class T>
+GBGHT_HD void reality_mode(int idx, const Geometry& g, Cplx<T>* S, int ncomp) {
+  const int NY2 = g.NY2;
+  if (idx >= NY2 * NY2) return;
+  const int qy = idx / NY2, qz = idx % NY2;
+  const int py = qy == 0 ? 0 : NY2 - qy;   // compact index of −m
+  const int pz = qz == 0 ? 0 : NY2 - qz;
+  const int pidx = py * NY2 + pz;
+  if (pidx < idx) return;
+  for (int cc = 0; cc < ncomp; ++cc) {
+    const size_t a = idxS(g, cc, qy, qz, 0), b = idxS(g, cc, py, pz, 0);
+    const Cplx<T> va = S[a], vb = S[b];
+    const Cplx<T> h = cmk<T>(T(0.5) * (va.x + vb.x), T(0.5) * (va.y - vb.y));
+    S[a] = h;
+    S[b] = conj(h);
+  }
+}
+
+// ================================================================================================
+// ConstantPower amplitude (src/Forcing.jl:1091-1117) for the stage state: the band sum is taken in
+// a fixed order by one thread; the whole-field sum adds the per-tile partials in a fixed order.
+// ================================================================================================
+template <class T>
+GBGHT_HD double band_energy_raw(const Geometry& g, const Cplx<T>* S, double lo2, double hi2) {
+  // Hermitian-weighted Σ|û|² over the band, unnormalised; m_a bounded by the band edge
+  int mb = int(std::sqrt(hi2) / g.s) + 1;
+  if (mb > g.K) mb = g.K;
+  double sum = 0.0;
+  for (int cc = 0; cc < 3; ++cc)
+    for (int my = -mb; my <= mb; ++my)
+      for (int mz = -mb; mz <= mb; ++mz)
+        for (int kx = 0; kx <= mb; ++kx) {
+          const double kxd = g.s * kx, kyd = g.s * my, kzd = g.s * mz;
+          const double k2 = (kxd * kxd + kyd * kyd) + kzd * kzd;
+          if (!(k2 >= lo2 && k2 <= hi2)) continue;
+          const int qy = my >= 0 ? my : my + g.NY2, qz = mz >= 0 ? mz : mz + g.NY2;
+          const Cplx<T> v = S[idxS(g, cc, qy, qz, kx)];
+          const double w = kx == 0 ? 1.0 : 2.0;
+          sum += w * (double(v.x) * v.x + double(v.y) * v.y);
+        }
+  return sum;
+}
+
+// ================================================================================================
+// z-inverse of the current state into A slots 0..6 (u, iκ×û, φ), and the tile's Hermitian-weighted
+// Σ|û|², with the same tiling as the epilogue. Used after an import to start a step.
+// ================================================================================================
+template <class T, int N, int TL, int NT>
+GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, const Geometry& g,
+                            Cplx<T>* GBGHT_RESTRICT A, const Cplx<T>* GBGHT_RESTRICT S, int has_scalar,
+                            const Cplx<T>* GBGHT_RESTRICT tw) {
+  const int kx0 = c.bx * TL, qy = c.by;
+  const int NY2 = g.NY2;
+  const double ky = g.s * double(q_to_m(qy, g.K, NY2));
+  double esum = 0.0;
+  for (int i = c.tid; i < NY2 * TL; i += NT) {
+    const int q = i / TL, l = i % TL;
+    const int kx = kx0 + l;
+    const Cplx<T> u0 = S[idxS(g, 0, qy, q, kx)], u1 = S[idxS(g, 1, qy, q, kx)], u2 = S[idxS(g, 2, qy, q, kx)];
+    Rt[(0 * NY2 + q) * TL + l] = u0;
+    Rt[(1 * NY2 + q) * TL + l] = u1;
+    Rt[(2 * NY2 + q) * TL + l] = u2;
+    const double w = kx == 0 ? 1.0 : 2.0;
+    esum += w * ((double(u0.x) * u0.x + double(u0.y) * u0.y) + (double(u1.x) * u1.x + double(u1.y) * u1.y) +
+                 (double(u2.x) * u2.x + double(u2.y) * u2.y));
+  }
+  red[c.tid] = esum;
+  GBGHT_SYNC();
+  double total = 0.0;
+  if (c.tid == 0)
+    for (int i = 0; i < NT; ++i) total += red[i];
+  for (int o = 0; o < 3; ++o)
+    z_inverse1<T, N, TL, NT>(c, W, g, A, o, qy, kx0, [&](int q, int l) { return Rt[(o * NY2 + q) * TL + l]; }, tw);
+  for (int o = 0; o < 3; ++o)
+    z_inverse1<T, N, TL, NT>(c, W, g, A, 3 + o, qy, kx0,
+                             [&](int q, int l) { return curl_component<T, TL>(g, Rt, o, q, l, kx0, ky); }, tw);
+  if (has_scalar)
+    z_inverse1<T, N, TL, NT>(c, W, g, A, 6, qy, kx0, [&](int q, int l) { return S[idxS(g, 3, qy, q, kx0 + l)]; }, tw);
+  return total;
+}
+
+// ================================================================================================
+// Observables: per ky' row, the Hermitian-weighted sums Σ|û|², Σκ²|û|², Σ|φ̂|², Σκ²|φ̂|²
+// (unnormalised), summed per thread and then in thread order. Grid: (NY2). `red` holds 4·NT.
+// ================================================================================================
+template <class T, int NT>
+GBGHT_HD void body_observables(const Cta& c, double* red, const Geometry& g, const Cplx<T>* GBGHT_RESTRICT S,
+                               int has_scalar, double* GBGHT_RESTRICT out) {
+  const int qy = c.bx;
+  const int NY2 = g.NY2, KX1 = g.K + 1;
+  const double ky = g.s * double(q_to_m(qy, g.K, NY2));
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int i = c.tid; i < NY2 * KX1; i += NT) {
+    const int qz = i / KX1, kx = i % KX1;
+    const double kxd = g.s * kx, kzd = g.s * q_to_m(qz, g.K, NY2);
+    const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
+    const double w = kx == 0 ? 1.0 : 2.0;
+    double e = 0.0;
+    for (int cc = 0; cc < 3; ++cc) {
+      const Cplx<T> v = S[idxS(g, cc, qy, qz, kx)];
+      e += double(v.x) * v.x + double(v.y) * v.y;
+    }
+    acc[0] += w * e;
+    acc[1] += w * k2 * e;
+    if (has_scalar) {
+      const Cplx<T> v = S[idxS(g, 3, qy, qz, kx)];
+      const double p = double(v.x) * v.x + double(v.y) * v.y;
+      acc[2] += w * p;
+      acc[3] += w * k2 * p;
+    }
+  }
+  for (int j = 0; j < 4; ++j) red[j * NT + c.tid] = acc[j];
+  GBGHT_SYNC();
+  if (c.tid == 0)
+    for (int j = 0; j < 4; ++j) {
+      double s = 0.0;
+      for (int i = 0; i < NT; ++i) s += red[j * NT + i];
+      out[qy * 4 + j] = s;
+    }
+}
+
+// ================================================================================================
+// Shell spectrum: per ky' row, the Hermitian-weighted Σ|f̂|² of each shell n = floor(|κ|/Δκ + ½),
+// for S slots [c0, c0+nc). Each kz' line is summed by thread 0 in kx order, so the result does
+// not depend on the launch. Grid: (NY2). `hist` holds nshell doubles, `vals` KXP·2 doubles.
+// ================================================================================================
+template <class T, int NT>
+GBGHT_HD void body_spectrum(const Cta& c, double* hist, double* vals, const Geometry& g,
+                            const Cplx<T>* GBGHT_RESTRICT S, int c0, int nc, int nshell,
+                            double* GBGHT_RESTRICT out) {
+  const int qy = c.bx;
+  const int NY2 = g.NY2, KX1 = g.K + 1;
+  const double ky = g.s * double(q_to_m(qy, g.K, NY2));
+  for (int i = c.tid; i < nshell; i += NT) hist[i] = 0.0;
+  GBGHT_SYNC();
+  for (int qz = 0; qz < NY2; ++qz) {
+    const double kzd = g.s * q_to_m(qz, g.K, NY2);
+    for (int kx = c.tid; kx < KX1; kx += NT) {
+      const double kxd = g.s * kx;
+      const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
+      double e = 0.0;
+      for (int cc = c0; cc < c0 + nc; ++cc) {
+        const Cplx<T> v = S[idxS(g, cc, qy, qz, kx)];
+        e += double(v.x) * v.x + double(v.y) * v.y;
+      }
+      vals[2 * kx] = (kx == 0 ? 1.0 : 2.0) * e;
+      vals[2 * kx + 1] = floor(sqrt(k2) / g.s + 0.5);
+    }
+    GBGHT_SYNC();
+    if (c.tid == 0)
+      for (int kx = 0; kx < KX1; ++kx) {
+        const int n = int(vals[2 * kx + 1]);
+        if (n < nshell) hist[n] += vals[2 * kx];
+      }
+    GBGHT_SYNC();
+  }
+  for (int i = c.tid; i < nshell; i += NT) out[size_t(qy) * nshell + i] = hist[i];
+}
+
+}  // namespace gbght

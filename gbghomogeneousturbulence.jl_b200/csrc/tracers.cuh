@@ -1,0 +1,178 @@
+// Lagrangian tracers: periodic wrap, Catmull–Rom gather, and the Heun (= ABM(1)) push.
+//
+// Positions are FP64 in both precision forms. The wrap and the displacement are evaluated with
+// round-to-nearest operations and no fused multiply-add, in the order the reference's update
+// reads (src/ParticlePropagator.jl:288-315), so a cell index floor(x/Δx) is reproducible.
+#pragma once
+
+#include "gbght_common.cuh"
+
+namespace gbght {
+
+GBGHT_HD double add_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dadd_rn(a, b);
+#else
+  return a + b;
+#endif
+}
+GBGHT_HD double sub_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dsub_rn(a, b);
+#else
+  return a - b;
+#endif
+}
+GBGHT_HD double mul_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+GBGHT_HD double div_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __ddiv_rn(a, b);
+#else
+  return a / b;
+#endif
+}
+
+// x − L·floor(x/L); a tiny negative result is lifted by L; a result equal to L maps to 0.
+GBGHT_HD double wrap_periodic(double x, double L) {
+  double y = sub_rn(x, mul_rn(L, floor(div_rn(x, L))));
+  if (y < 0.0) y = add_rn(y, L);
+  if (y >= L) y = 0.0;
+  return y;
+}
+
+// Catmull–Rom weights for taps i−1, i, i+1, i+2 at fraction t (Catmull & Rom 1974).
+GBGHT_HD void catmull_rom(double t, double w[4]) {
+  w[0] = mul_rn(mul_rn(t, sub_rn(mul_rn(t, sub_rn(2.0, t)), 1.0)), 0.5);
+  w[1] = mul_rn(add_rn(mul_rn(mul_rn(t, t), sub_rn(mul_rn(3.0, t), 5.0)), 2.0), 0.5);
+  w[2] = mul_rn(mul_rn(t, add_rn(mul_rn(t, sub_rn(4.0, mul_rn(3.0, t))), 1.0)), 0.5);
+  w[3] = mul_rn(mul_rn(mul_rn(t, t), sub_rn(t, 1.0)), 0.5);
+}
+
+// Cell i = floor(x/Δx) reduced into [0, N), and the fraction t = x/Δx − floor(x/Δx). A
+// non-finite position gives cell 0 and a non-finite fraction, so the gathered value is NaN and
+// no index leaves the field.
+GBGHT_HD void cell_fraction(double x, double dx, int N, int& i, double& t) {
+  const double q = div_rn(x, dx);
+  if (!(q - q == 0.0)) {
+    i = 0;
+    t = q - q;
+    return;
+  }
+  const double f = floor(q);
+  const double r = sub_rn(f, mul_rn(double(N), floor(div_rn(f, double(N)))));
+  i = int(r);
+  if (i < 0 || i >= N) i = 0;
+  t = sub_rn(q, f);
+}
+
+// Gather the three components of a physical field [3][N][N][N] at X; sums run x innermost,
+// then y, then z.
+template <class T>
+GBGHT_HD void gather3(const T* GBGHT_RESTRICT u, int N, double dx, double x, double y, double z,
+                      double out[3]) {
+  int ix, iy, iz;
+  double tx, ty, tz;
+  cell_fraction(x, dx, N, ix, tx);
+  cell_fraction(y, dx, N, iy, ty);
+  cell_fraction(z, dx, N, iz, tz);
+  double wx[4], wy[4], wz[4];
+  catmull_rom(tx, wx);
+  catmull_rom(ty, wy);
+  catmull_rom(tz, wz);
+  int xs[4], ys[4], zs[4];
+  for (int a = 0; a < 4; ++a) {
+    xs[a] = (ix + a - 1 + N) % N;
+    ys[a] = (iy + a - 1 + N) % N;
+    zs[a] = (iz + a - 1 + N) % N;
+  }
+  const size_t comp = size_t(N) * N * N;
+  for (int c = 0; c < 3; ++c) {
+    const T* f = u + c * comp;
+    double acc_z = 0.0;
+    for (int cz = 0; cz < 4; ++cz) {
+      double acc_y = 0.0;
+      for (int cy = 0; cy < 4; ++cy) {
+        const T* row = f + (size_t(zs[cz]) * N + ys[cy]) * N;
+        double acc_x = 0.0;
+        for (int cx = 0; cx < 4; ++cx) acc_x = add_rn(acc_x, mul_rn(wx[cx], double(ldg(row + xs[cx]))));
+        acc_y = add_rn(acc_y, mul_rn(wy[cy], acc_x));
+      }
+      acc_z = add_rn(acc_z, mul_rn(wz[cz], acc_y));
+    }
+    out[c] = acc_z;
+  }
+}
+
+struct HeunWeights {
+  double b0;      // predictor weight on f₀
+  double beta0;   // corrector weight on f*
+  double beta1m;  // corrector weight on f₀, β₁ − b₀
+};
+
+// One tracer: gather only (mode 0), Heun push (mode 1), or Heun push then the particle deposit
+// gather at the new position (mode 2). X and F are [3][M].
+template <class T>
+GBGHT_HD void tracer_one(int64_t p, int64_t M, int mode, const T* GBGHT_RESTRICT u, int N, double L,
+                         double* GBGHT_RESTRICT X, double* GBGHT_RESTRICT F, HeunWeights w) {
+  const double dx = div_rn(L, double(N));
+  double x[3] = {X[p], X[M + p], X[2 * M + p]};
+  double f[3];
+  if (mode != 0) {
+    const double f0[3] = {F[p], F[M + p], F[2 * M + p]};
+    double xs[3];
+    for (int c = 0; c < 3; ++c) xs[c] = wrap_periodic(add_rn(x[c], mul_rn(w.b0, f0[c])), L);
+    double fs[3];
+    gather3(u, N, dx, xs[0], xs[1], xs[2], fs);
+    for (int c = 0; c < 3; ++c) {
+      const double disp = add_rn(mul_rn(w.beta0, fs[c]), mul_rn(w.beta1m, f0[c]));
+      x[c] = wrap_periodic(add_rn(xs[c], disp), L);
+      X[c * M + p] = x[c];
+    }
+    if (mode == 1) return;
+  }
+  gather3(u, N, dx, x[0], x[1], x[2], f);
+  for (int c = 0; c < 3; ++c) F[c * M + p] = f[c];
+}
+
+// 4-point Gauss–Legendre Adams weights (src/ParticlePropagator.jl:263-280), host side.
+inline void adams_weights(const double* nodes, int n, double h, double* out) {
+  static const double gn[4] = {-0.8611363115940526, -0.3399810435848563, 0.3399810435848563,
+                               0.8611363115940526};
+  static const double gw[4] = {0.3478548451374538, 0.6521451548625461, 0.6521451548625461,
+                               0.3478548451374538};
+  for (int j = 0; j < n; ++j) {
+    double weight = 0.0;
+    for (int k = 0; k < 4; ++k) {
+      const double t = h * (gn[k] + 1) / 2;
+      double basis = 1.0;
+      for (int m = 0; m < n; ++m) {
+        if (m == j) continue;
+        basis *= (t - nodes[m]) / (nodes[j] - nodes[m]);
+      }
+      weight += gw[k] * h / 2 * basis;
+    }
+    out[j] = weight;
+  }
+}
+
+inline HeunWeights heun_weights(double h) {
+  HeunWeights w;
+  const double n1[1] = {0.0};
+  double b[1];
+  adams_weights(n1, 1, h, b);
+  const double n2[2] = {h, 0.0};
+  double beta[2];
+  adams_weights(n2, 2, h, beta);
+  w.b0 = b[0];
+  w.beta0 = beta[0];
+  w.beta1m = beta[1] - b[0];
+  return w;
+}
+
+}  // namespace gbght

@@ -1,1 +1,378 @@
-"""Host side of the B200 IF-RK time step (placeholder; the ctypes binding follows)."""
+"""Python host side of the B200 IF-RK time step: a ctypes binding of the C ABI (include/gbght.h).
+
+It mirrors the reference's run API (src/SimulationRun.jl, src/Propagator.jl,
+src/ParticlePropagator.jl) with the same names, argument meanings and refusals. An ArgumentError
+of the reference raises ``ValueError``; an ErrorException (a schedule refusal or a blow-up) raises
+``ScheduleError``.
+
+The compute runs in ``libgbght.so``, the CUDA library built in-tree by ``gbght_build.py``. There is no
+host fallback: if the library is missing, `load_library` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import seed  # noqa: F401  (host-side seeding, re-exported)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libgbght.so")
+
+FP64, FP32_MIXED = 0, 1
+IFRK4, IFRK3 = 0, 1
+FORCING_NONE, FORCING_CONSTANT_POWER = 0, 1
+OK, ERR_ARGUMENT, ERR_SCHEDULE, ERR_CUDA, ERR_DEVICE = 0, 1, 2, 3, 4
+
+
+class ScheduleError(RuntimeError):
+    """The reference's ErrorException: a refused schedule or a blow-up."""
+
+
+class DeviceError(RuntimeError):
+    """A CUDA runtime error or a raised device status bit."""
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("grid_points_per_axis", C.c_int),
+        ("side_length", C.c_double),
+        ("precision", C.c_int),
+        ("scheme", C.c_int),
+        ("viscosity", C.c_double),
+        ("schmidt", C.c_double),
+        ("scalar", C.c_int),
+        ("velocity_forcing", C.c_int),
+        ("injection_rate", C.c_double),
+        ("lowest_shell", C.c_int),
+        ("highest_shell", C.c_double),
+        ("mean_gradient", C.c_double * 3),
+        ("tracers", C.c_int64),
+        ("cfl", C.c_double),
+        ("max_dt", C.c_double),
+        ("device", C.c_int),
+    ]
+
+
+_DP = C.POINTER(C.c_double)
+_SIGNATURES = {
+    "gbght_config_default": (None, [C.POINTER(Config)]),
+    "gbght_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(Config)]),
+    "gbght_destroy": (None, [C.c_void_p]),
+    "gbght_last_error": (C.c_char_p, [C.c_void_p]),
+    "gbght_global_error": (C.c_char_p, []),
+    "gbght_version": (C.c_char_p, []),
+    "gbght_geometry": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), _DP]),
+    "gbght_state_import": (C.c_int, [C.c_void_p, _DP, _DP]),
+    "gbght_state_export": (C.c_int, [C.c_void_p, _DP, _DP]),
+    "gbght_step": (C.c_int, [C.c_void_p, C.c_double]),
+    "gbght_deposit": (C.c_int, [C.c_void_p]),
+    "gbght_max_speed": (C.c_int, [C.c_void_p, _DP]),
+    "gbght_cfl_timestep": (C.c_int, [C.c_void_p, _DP]),
+    "gbght_velocity_physical_export": (C.c_int, [C.c_void_p, _DP]),
+    "gbght_velocity_physical_import": (C.c_int, [C.c_void_p, _DP]),
+    "gbght_observables": (C.c_int, [C.c_void_p, _DP]),
+    "gbght_spectrum_length": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "gbght_spectrum": (C.c_int, [C.c_void_p, C.c_int, _DP, C.c_int]),
+    "gbght_tracers_import": (C.c_int, [C.c_void_p, _DP]),
+    "gbght_tracers_export": (C.c_int, [C.c_void_p, _DP]),
+    "gbght_tracer_sample_export": (C.c_int, [C.c_void_p, _DP, _DP]),
+    "gbght_advect": (C.c_int, [C.c_void_p, C.c_double]),
+    "gbght_deposit_tracers": (C.c_int, [C.c_void_p, C.c_double]),
+    "gbght_interpolate_velocity": (C.c_int, [C.c_void_p, _DP, C.c_int64, _DP]),
+    "gbght_advance": (C.c_int, [C.c_void_p, C.c_double, _DP]),
+    "gbght_clock": (C.c_int, [C.c_void_p, _DP, C.POINTER(C.c_int64)]),
+    "gbght_set_clock": (C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
+    "gbght_status_word": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32)]),
+    "gbght_synchronize": (C.c_int, [C.c_void_p]),
+    "gbght_profile": (C.c_int, [C.c_void_p, C.c_int]),
+    "gbght_profile_read": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64), _DP]),
+    "gbght_timer": (C.c_int, [C.c_void_p, C.c_int, _DP]),
+}
+
+KERNELS = ("y_inverse", "x_products", "y_forward", "z_epilogue", "x_velocity", "force_amp", "reality",
+           "tracers", "observables")
+
+_loaded: dict = {}
+
+
+def load_library(path: str | None = None):
+    """Load and type the C ABI from `path` (default: the in-tree CUDA library)."""
+    path = os.path.abspath(path or LIB_PATH)
+    if path in _loaded:
+        return _loaded[path]
+    if not os.path.exists(path):
+        raise OSError(f"the CUDA library {path} is missing: build it with "
+                      f"`python gbghomogeneousturbulence.jl_b200/gbght_build.py`")
+    lib = C.CDLL(path)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _loaded[path] = lib
+    return lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_DP)
+
+
+@dataclass
+class ConstantPower:
+    """`ConstantPower(domain; injection_rate, lowest_shell = 1, highest_shell = 2)`
+    (src/Forcing.jl:1069)."""
+    injection_rate: float
+    lowest_shell: int = 1
+    highest_shell: float = 2
+
+
+@dataclass
+class NoForcing:
+    """`NoForcing()` (src/Forcing.jl): a freely decaying field."""
+
+
+@dataclass
+class Setup:
+    """The run's defining parameters (`FixedDomain` + `FlowConditions` + run options)."""
+    grid_points_per_axis: int
+    side_length: float = 2 * math.pi
+    viscosity: float = 0.01
+    schmidt: float = 1.0
+    scalar: bool = True
+    velocity_forcing: object = field(default_factory=NoForcing)
+    mean_gradient: tuple = (0.0, 0.0, 0.0)
+    precision: str = "fp64"          # "fp64" or "fp32_mixed"
+    scheme: str = "IFLowStorageRK4"  # or "IFLowStorageRK3"
+    tracers: int = 0
+    cfl: float = 0.5
+    max_dt: float = math.inf
+    device: int = 0
+
+
+class Run:
+    """One run: `Simulation` (src/SimulationRun.jl:500-974) with its state, generator, registers,
+    cache and tracers, backed by a `gbght_run` handle."""
+
+    def __init__(self, setup: Setup, library: str | None = None):
+        self.setup = setup
+        self.lib = load_library(library)
+        cfg = Config()
+        self.lib.gbght_config_default(C.byref(cfg))
+        cfg.grid_points_per_axis = int(setup.grid_points_per_axis)
+        cfg.side_length = float(setup.side_length)
+        cfg.precision = {"fp64": FP64, "fp32_mixed": FP32_MIXED}[setup.precision]
+        cfg.scheme = {"IFLowStorageRK4": IFRK4, "IFLowStorageRK3": IFRK3}[setup.scheme]
+        cfg.viscosity = float(setup.viscosity)
+        cfg.schmidt = float(setup.schmidt)
+        cfg.scalar = 1 if setup.scalar else 0
+        f = setup.velocity_forcing
+        if isinstance(f, ConstantPower):
+            cfg.velocity_forcing = FORCING_CONSTANT_POWER
+            cfg.injection_rate = float(f.injection_rate)
+            cfg.lowest_shell = int(f.lowest_shell)
+            cfg.highest_shell = float(f.highest_shell)
+        elif f is None or isinstance(f, NoForcing):
+            cfg.velocity_forcing = FORCING_NONE
+        else:
+            raise ValueError(f"unsupported velocity forcing {f!r}")
+        for i in range(3):
+            cfg.mean_gradient[i] = float(setup.mean_gradient[i])
+        cfg.tracers = int(setup.tracers)
+        cfg.cfl = float(setup.cfl)
+        cfg.max_dt = float(setup.max_dt)
+        cfg.device = int(setup.device)
+        h = C.c_void_p()
+        rc = self.lib.gbght_create(C.byref(h), C.byref(cfg))
+        if rc != OK:
+            msg = self.lib.gbght_global_error().decode()
+            raise (ValueError if rc == ERR_ARGUMENT else DeviceError)(msg)
+        self.h = h
+        self.N = setup.grid_points_per_axis
+        K = C.c_int()
+        cut = C.c_double()
+        self.lib.gbght_geometry(self.h, C.byref(K), C.byref(cut))
+        self.K, self.cutoff = K.value, cut.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.gbght_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- errors -----------------------------------------------------------------------------------
+    def _check(self, rc: int):
+        if rc == OK:
+            return
+        msg = self.lib.gbght_last_error(self.h).decode()
+        if rc == ERR_ARGUMENT:
+            raise ValueError(msg)
+        if rc == ERR_SCHEDULE:
+            raise ScheduleError(msg)
+        raise DeviceError(msg)
+
+    # -- state ------------------------------------------------------------------------------------
+    @property
+    def spectral_shape(self):
+        return (self.N, self.N, self.N // 2 + 1)
+
+    def import_state(self, uh: np.ndarray, phih: np.ndarray | None = None):
+        u = np.ascontiguousarray(uh, dtype=np.complex128)
+        if u.shape != (3,) + self.spectral_shape:
+            raise ValueError(f"u_hat must have shape {(3,) + self.spectral_shape}")
+        p = None
+        if self.setup.scalar:
+            if phih is None:
+                raise ValueError("this run carries a passive scalar, so phi_hat must be given")
+            p = np.ascontiguousarray(phih, dtype=np.complex128)
+            if p.shape != self.spectral_shape:
+                raise ValueError(f"phi_hat must have shape {self.spectral_shape}")
+        self._check(self.lib.gbght_state_import(self.h, u.view(np.float64).ctypes.data_as(_DP),
+                                                None if p is None else p.view(np.float64).ctypes.data_as(_DP)))
+
+    def export_state(self):
+        u = np.zeros((3,) + self.spectral_shape, np.complex128)
+        p = np.zeros(self.spectral_shape, np.complex128) if self.setup.scalar else None
+        self._check(self.lib.gbght_state_export(self.h, u.view(np.float64).ctypes.data_as(_DP),
+                                                None if p is None else p.view(np.float64).ctypes.data_as(_DP)))
+        return u, p
+
+    # -- the field step (step!, deposit!) ----------------------------------------------------------
+    def step(self, dt: float):
+        self._check(self.lib.gbght_step(self.h, float(dt)))
+
+    def deposit(self):
+        self._check(self.lib.gbght_deposit(self.h))
+
+    def max_speed(self) -> float:
+        v = C.c_double()
+        self._check(self.lib.gbght_max_speed(self.h, C.byref(v)))
+        return v.value
+
+    def cfl_timestep(self) -> float:
+        v = C.c_double()
+        self._check(self.lib.gbght_cfl_timestep(self.h, C.byref(v)))
+        return v.value
+
+    def velocity_physical(self) -> np.ndarray:
+        u = np.zeros((3, self.N, self.N, self.N))
+        self._check(self.lib.gbght_velocity_physical_export(self.h, _ptr(u)))
+        return u
+
+    def deposit_prescribed_velocity(self, u: np.ndarray):
+        a = np.ascontiguousarray(u, dtype=np.float64)
+        self._check(self.lib.gbght_velocity_physical_import(self.h, _ptr(a)))
+
+    # -- observables --------------------------------------------------------------------------------
+    def observables(self) -> dict:
+        out = np.zeros(4)
+        self._check(self.lib.gbght_observables(self.h, _ptr(out)))
+        return {"kinetic_energy": out[0], "dissipation": out[1], "scalar_variance": out[2],
+                "scalar_dissipation": out[3]}
+
+    def _spectrum(self, which: int) -> np.ndarray:
+        n = C.c_int()
+        self.lib.gbght_spectrum_length(self.h, C.byref(n))
+        out = np.zeros(n.value)
+        self._check(self.lib.gbght_spectrum(self.h, which, _ptr(out), n.value))
+        return out
+
+    def energy_spectrum(self) -> np.ndarray:
+        return self._spectrum(0)
+
+    def scalar_spectrum(self) -> np.ndarray:
+        return self._spectrum(1)
+
+    # -- tracers (advect!, particle deposit!) -------------------------------------------------------
+    def import_tracers(self, X: np.ndarray):
+        a = np.ascontiguousarray(X, dtype=np.float64)
+        if a.shape != (3, self.setup.tracers):
+            raise ValueError(f"positions must have shape (3, {self.setup.tracers})")
+        self._check(self.lib.gbght_tracers_import(self.h, _ptr(a)))
+
+    def tracers(self) -> np.ndarray:
+        X = np.zeros((3, self.setup.tracers))
+        self._check(self.lib.gbght_tracers_export(self.h, _ptr(X)))
+        return X
+
+    def tracer_sample(self):
+        F = np.zeros((3, self.setup.tracers))
+        t = C.c_double()
+        self._check(self.lib.gbght_tracer_sample_export(self.h, _ptr(F), C.byref(t)))
+        return F, t.value
+
+    def advect(self, dt: float):
+        self._check(self.lib.gbght_advect(self.h, float(dt)))
+
+    def deposit_tracers(self, t: float):
+        self._check(self.lib.gbght_deposit_tracers(self.h, float(t)))
+
+    def interpolate_velocity(self, X: np.ndarray) -> np.ndarray:
+        a = np.ascontiguousarray(X, dtype=np.float64)
+        out = np.zeros_like(a)
+        self._check(self.lib.gbght_interpolate_velocity(self.h, _ptr(a), a.shape[1], _ptr(out)))
+        return out
+
+    # -- run layer (advance!) ------------------------------------------------------------------------
+    def advance(self, dt: float | None = None) -> float:
+        taken = C.c_double()
+        self._check(self.lib.gbght_advance(self.h, 0.0 if dt is None else float(dt), C.byref(taken)))
+        return taken.value
+
+    def clock(self):
+        t = C.c_double()
+        s = C.c_int64()
+        self.lib.gbght_clock(self.h, C.byref(t), C.byref(s))
+        return t.value, s.value
+
+    def status_word(self) -> int:
+        w = C.c_uint32()
+        self._check(self.lib.gbght_status_word(self.h, C.byref(w)))
+        return w.value
+
+    def synchronize(self):
+        self._check(self.lib.gbght_synchronize(self.h))
+
+    # -- CUDA-event timing on the run's stream ------------------------------------------------------
+    def profile(self, enable: bool):
+        self._check(self.lib.gbght_profile(self.h, 1 if enable else 0))
+
+    def profile_read(self) -> dict:
+        out = {}
+        for k, name in enumerate(KERNELS):
+            n = C.c_int64()
+            ms = C.c_double()
+            self._check(self.lib.gbght_profile_read(self.h, k, C.byref(n), C.byref(ms)))
+            out[name] = (n.value, ms.value)
+        return out
+
+    def timer_start(self):
+        self._check(self.lib.gbght_timer(self.h, 0, None))
+
+    def timer_stop(self) -> float:
+        ms = C.c_double()
+        self._check(self.lib.gbght_timer(self.h, 1, C.byref(ms)))
+        return ms.value
+
+
+def simulation(setup: Setup, uh: np.ndarray, phih: np.ndarray | None = None, X: np.ndarray | None = None,
+               library: str | None = None) -> Run:
+    """Build a run and make its first deposits, as `Simulation(...)` does
+    (src/SimulationRun.jl:750-931): import the state, deposit the fields, then place the tracers
+    and take their first sample at t = 0."""
+    run = Run(setup, library=library)
+    run.import_state(uh, phih)
+    run.deposit()
+    if setup.tracers:
+        if X is None:
+            raise ValueError("a run with tracers needs their positions")
+        run.import_tracers(X)
+        run.deposit_tracers(0.0)
+    return run

@@ -1,0 +1,203 @@
+/*
+ * gbght.h — C ABI of the B200-native IF-RK time step of GBGHomogeneousTurbulence.jl.
+ *
+ * One opaque handle holds a run: the domain, the flow conditions, the spectral state, the step's
+ * registers, the observables deposited at the end of an iteration, and (optionally) the tracers.
+ * The library owns all device memory. Every call returns a status code. gbght_last_error() returns
+ * the message of the last failing call on a handle, and gbght_global_error() that of a failed
+ * create. Calls on one handle are not thread-safe. They run on the handle's own CUDA stream, and
+ * every call that returns data to the host synchronises that stream.
+ *
+ * Arrays cross the boundary in the reference's own layouts:
+ *  - spectral fields: complex128 interleaved (re, im), row-major [comp][kz][ky][kx], kx in
+ *    [0, N/2]. This is the column-major (kx, ky, kz, comp) rfft array of the reference.
+ *    The forward transform is unnormalised, as in the reference (docs/src/validation.md:72-74).
+ *  - physical fields: float64 row-major [comp][z][y][x], node i at x = i·L/N.
+ *  - tracer positions and point values: float64 [3][M], the (M, 3) column-major array of the
+ *    reference's PointSet / VectorPointValues.
+ *
+ * Every entry point cites the reference interface it replaces (file:line within the reference
+ * project). Status codes map onto the reference's exception types: GBGHT_ERR_ARGUMENT is an
+ * ArgumentError, and GBGHT_ERR_SCHEDULE is an ErrorException (a schedule refusal or a blow-up).
+ */
+#ifndef GBGHT_H
+#define GBGHT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gbght_run gbght_run;
+
+enum gbght_status {
+  GBGHT_OK = 0,
+  GBGHT_ERR_ARGUMENT = 1,   /* ArgumentError: a bad argument or an unsupported configuration */
+  GBGHT_ERR_SCHEDULE = 2,   /* ErrorException: refused schedule (stale/missing deposit), blow-up */
+  GBGHT_ERR_CUDA = 3,       /* a CUDA runtime error; the message names the call */
+  GBGHT_ERR_DEVICE = 4      /* a device-side status bit was raised (see gbght_status_word) */
+};
+
+enum gbght_precision { GBGHT_FP64 = 0, GBGHT_FP32_MIXED = 1 };
+enum gbght_scheme { GBGHT_IFRK4 = 0, GBGHT_IFRK3 = 1 };
+enum gbght_forcing { GBGHT_FORCING_NONE = 0, GBGHT_FORCING_CONSTANT_POWER = 1 };
+enum gbght_tracer_scheme { GBGHT_HEUN = 0 };
+
+/* Device status bits (gbght_status_word). */
+#define GBGHT_STATUS_NONFINITE_SPEED 0x1u
+#define GBGHT_STATUS_EMPTY_BAND      0x2u
+
+typedef struct gbght_config {
+  int grid_points_per_axis;  /* N; supported: 8 12 16 24 32 48 64 96 128 192 256 384 512 */
+  double side_length;        /* L */
+  int precision;             /* gbght_precision */
+  int scheme;                /* gbght_scheme (field integration) */
+  double viscosity;          /* ν > 0 */
+  double schmidt;            /* Sc > 0; scalar diffusivity ν/Sc */
+  int scalar;                /* 1: carry the passive scalar */
+  int velocity_forcing;      /* gbght_forcing */
+  double injection_rate;     /* ConstantPower ε */
+  int lowest_shell;          /* ConstantPower band, shells [lowest − ½, highest + ½]·2π/L */
+  double highest_shell;
+  double mean_gradient[3];   /* uniform mean scalar gradient G (extension; 0 = none) */
+  int64_t tracers;           /* M ≥ 0 tracers */
+  double cfl;                /* C of the advective CFL rule */
+  double max_dt;             /* caller's ceiling on Δt (INFINITY = none) */
+  int device;                /* CUDA device ordinal */
+} gbght_config;
+
+/* Fill `cfg` with the defaults: N=64, L=2π, FP64, IF-RK4, ν=0.01, Sc=1, scalar on, no forcing,
+ * shells 1–2, G=0, no tracers, CFL 0.5, max_dt=∞, device 0. */
+void gbght_config_default(gbght_config* cfg);
+
+/* Build a run on a FixedDomain with TwoThirds dealiasing, with its generator and registers.
+ * Replaces FixedDomain(...) (src/SimulationDomain.jl:295-328), FlowConditions
+ * (src/Generator.jl:81-140), ConstantPower (src/Forcing.jl:1069-1075), allocate_buffers
+ * (src/Propagator.jl:717-723) and ObservablesCache (src/Cache.jl:150-173). The state starts at
+ * zero. */
+int gbght_create(gbght_run** out, const gbght_config* cfg);
+void gbght_destroy(gbght_run* run);
+const char* gbght_last_error(const gbght_run* run);
+const char* gbght_global_error(void);
+const char* gbght_version(void);
+
+/* Retained-band geometry: K (largest retained |m| per axis) and the dealias cutoff.
+ * Replaces max_retained_wavenumber (src/SimulationDomain.jl:413-419). */
+int gbght_geometry(const gbght_run* run, int* K, double* cutoff);
+
+/* Spectral state import/export, host arrays in the reference layout. phi_hat may be NULL when
+ * the run carries no scalar. Import refuses (ARGUMENT) a state with content outside the retained
+ * 2/3 ball: the library stores only the retained modes. Every state the reference's seeders
+ * and steps produce is band-limited. Import invalidates the deposit.
+ * Replaces ResolvedFields(û, φ̂) (src/State.jl:119-137) and the state read/write of
+ * ext/GBGHomogeneousTurbulenceHDF5Ext.jl. */
+int gbght_state_import(gbght_run* run, const double* u_hat, const double* phi_hat);
+int gbght_state_export(gbght_run* run, double* u_hat, double* phi_hat);
+
+/* One field step of the configured scheme with step dt > 0, in place. Requires a current field
+ * deposit, i.e. gbght_deposit after the last state change; otherwise SCHEDULE. The step is the
+ * coupled velocity + scalar 2N loop with the end-of-step Leray and reality projections.
+ * Replaces step!(::IFLowStorageRK4 / ::IFLowStorageRK3, state, generator, domain, buffers, cache,
+ * dt) (src/Propagator.jl:267-274,304-419). */
+int gbght_step(gbght_run* run, double dt);
+
+/* The closing field deposit: the velocity in physical representation and max|u|.
+ * Replaces deposit!(cache, state, domain, buffers) (src/Propagator.jl:808-842). */
+int gbght_deposit(gbght_run* run);
+
+/* The deposited max|u| (sqrt of the maximum of |u|²). Replaces max_speed(cache)
+ * (src/Cache.jl:416-421, src/Observables.jl:304-305). */
+int gbght_max_speed(gbght_run* run, double* speed);
+
+/* The advective CFL step for the deposited velocity. Replaces cfl_timestep(sim)
+ * (src/SimulationRun.jl:1051-1096). */
+int gbght_cfl_timestep(gbght_run* run, double* dt);
+
+/* Export the deposited physical velocity, [3][N][N][N] float64. Replaces velocity_physical(cache)
+ * (src/Cache.jl:291-299). */
+int gbght_velocity_physical_export(gbght_run* run, double* u);
+
+/* Write a prescribed physical velocity into the deposit slot, as the reference's test fake does
+ * (test/prescribed_flow.jl:16-21). The spectral state is untouched. The tracers are then advected
+ * in this field. */
+int gbght_velocity_physical_import(gbght_run* run, const double* u);
+
+/* Observables of the current state: k, ε, ⟨φ²⟩, ε_φ (FP64 reductions).
+ * Replaces kinetic_energy_and_dissipation (src/Observables.jl:170-173) and
+ * scalar_variance_and_dissipation (src/Observables.jl:345-380). */
+int gbght_observables(gbght_run* run, double out[4]);
+
+/* Shell spectrum of the velocity (which = 0, E(κ) = radial_spectrum/(2Δκ)) or of the scalar
+ * (which = 1, radial_spectrum/Δκ). Shell n covers [n − ½, n + ½)·Δκ. `n` is the capacity of
+ * `out`; gbght_spectrum_length gives the shell count. Replaces energy_spectrum
+ * (src/Observables.jl:502-514). */
+int gbght_spectrum_length(const gbght_run* run, int* n);
+int gbght_spectrum(gbght_run* run, int which, double* out, int n);
+
+/* Tracer positions [3][M], copied as given (the push wraps them into [0, L)). Import clears the
+ * trail. Replaces Tracers(domain; positions) (src/Particles.jl:145-176). */
+int gbght_tracers_import(gbght_run* run, const double* X);
+int gbght_tracers_export(gbght_run* run, double* X);
+
+/* The newest velocity sample at the tracers [3][M] and its time. Replaces
+ * velocity_at_particles_trail (src/Cache.jl). */
+int gbght_tracer_sample_export(gbght_run* run, double* values, double* t);
+
+/* Advance the tracers one Heun (= ABM(1)) step of size dt through the deposited velocity. The
+ * step requires the newest trail sample to be at the current positions, and the fields to be
+ * exactly one step ahead of it; otherwise SCHEDULE. Replaces advect!(Heun(), tracers, domain,
+ * cache, dt; traversal) (src/ParticlePropagator.jl:288-372). */
+int gbght_advect(gbght_run* run, double dt);
+
+/* The particle deposit: sample the deposited velocity at the tracers, labelled with time t.
+ * Replaces deposit!(cache, tracers, t; traversal) (src/ParticlePropagator.jl:378-386). */
+int gbght_deposit_tracers(gbght_run* run, double t);
+
+/* Catmull–Rom gather of the deposited velocity at arbitrary positions X [3][M] → out [3][M].
+ * Replaces interpolate_at_particles!(out, u, tracers) (src/Particles.jl:290-293). */
+int gbght_interpolate_velocity(gbght_run* run, const double* X, int64_t M, double* out);
+
+/* One iteration of the run layer: Δt (dt > 0 fixed, dt <= 0 the CFL rule), step, deposit, tracer
+ * push and particle deposit, blow-up guards, clock. The Δt taken is returned in *dt_taken (may be
+ * NULL). Replaces advance!(sim; dt) (src/SimulationRun.jl:1155-1229). */
+int gbght_advance(gbght_run* run, double dt, double* dt_taken);
+
+/* The run's clock. Replaces current_time / current_step (src/SimulationRun.jl). */
+int gbght_clock(const gbght_run* run, double* time, int64_t* step);
+int gbght_set_clock(gbght_run* run, double time, int64_t step);
+
+/* Device status bits raised since the last call (GBGHT_STATUS_*); reading clears them. */
+int gbght_status_word(gbght_run* run, uint32_t* word);
+
+/* CUDA-event timing on the run's own stream (no counterpart in the reference, which has no
+ * profiling; used by the benchmark to time kernels where they are launched).
+ * gbght_profile(run, 1) clears the counters and brackets every later kernel launch with events;
+ * gbght_profile(run, 0) stops. gbght_profile_read returns, for kernel kind `kind`
+ * (GBGHT_KERNEL_*), the number of launches and their summed duration in milliseconds.
+ * gbght_timer(run, 0, NULL) records a start event; gbght_timer(run, 1, &ms) records a stop
+ * event, waits for it and returns the elapsed milliseconds. */
+enum gbght_kernel {
+  GBGHT_KERNEL_Y_INVERSE = 0,   /* inverse y-transform pass */
+  GBGHT_KERNEL_X_PRODUCTS = 1,  /* x pass: c2r, u×ω and uφ, r2c */
+  GBGHT_KERNEL_Y_FORWARD = 2,   /* forward y-transform pass */
+  GBGHT_KERNEL_Z_EPILOGUE = 3,  /* z-forward, IF-RK stage update, z-inverse */
+  GBGHT_KERNEL_X_VELOCITY = 4,  /* deposit: physical velocity and max|u| */
+  GBGHT_KERNEL_FORCE_AMP = 5,   /* ConstantPower amplitude */
+  GBGHT_KERNEL_REALITY = 6,     /* end-of-step reality projection */
+  GBGHT_KERNEL_TRACERS = 7,     /* tracer gather / Heun push */
+  GBGHT_KERNEL_OBSERVABLES = 8  /* k, ε, ⟨φ²⟩, ε_φ reduction */
+};
+int gbght_profile(gbght_run* run, int enable);
+int gbght_profile_read(gbght_run* run, int kind, int64_t* launches, double* total_ms);
+int gbght_timer(gbght_run* run, int op, double* ms);
+
+/* Wait for all work queued on the run's stream. */
+int gbght_synchronize(gbght_run* run);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GBGHT_H */

@@ -1,0 +1,135 @@
+"""Parity of the CUDA library (sm_100a) with the CPU oracle, through the C ABI.
+
+The bar (FP64): relative L2 error of the spectral fields ≤ 1e-12 after 100 steps of the 64³
+decaying case, and equal tracer cell indices. The FP32-mixed form is held to a short-time field
+error and to per-shell spectrum errors of at most 1e-5, each against the FP64 oracle.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import gbght
+from gbght import seed as S
+from oracle import gbght_oracle as O
+from pairs import advance_both, compare, make_case, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def test_decaying_64_cubed_100_steps(cuda_library):
+    # the CPU-runnable case: 64³, ν = κ = 0.01, Sc = 1, unforced, IF-RK4, Δt = 0.005, 100 steps,
+    # k⁴ seed spectrum, k = 0.5, ⟨φ²⟩ = 0.5, 4096 tracers
+    run, orun = make_case(64, viscosity=0.01, tracers=4096, library=cuda_library)
+    advance_both(run, orun, 100, dt=0.005)
+    res = compare(run, orun, tol=1e-12)
+    assert res["X_err"] < 1e-10
+    F, t = run.tracer_sample()
+    assert t == pytest.approx(orun.time, rel=0, abs=0)
+    assert np.max(np.abs(F - orun.f0)) < 1e-10
+
+
+@pytest.mark.parametrize("N,steps", [(32, 20), (48, 5), (12, 10), (16, 10)])
+def test_forced_with_mean_gradient_cfl(cuda_library, N, steps):
+    run, orun = make_case(N, viscosity=0.01, forcing=0.1, G=(1.0, 0.0, 0.0), tracers=256, library=cuda_library)
+    taken = advance_both(run, orun, steps, dt=None)
+    for d_lib, d_ora in taken:
+        assert d_lib == pytest.approx(d_ora, rel=1e-12)
+    compare(run, orun, tol=1e-12)
+
+
+def test_rk3_velocity_only(cuda_library):
+    run, orun = make_case(32, scalar=False, forcing=0.2, scheme="IFLowStorageRK3", library=cuda_library)
+    advance_both(run, orun, 10, dt=0.01)
+    compare(run, orun, tol=1e-12)
+
+
+def test_larger_grids_short(cuda_library):
+    for N in (96, 128):
+        run, orun = make_case(N, viscosity=0.005, forcing=0.1, G=(1.0, 0.0, 0.0), tracers=1000, library=cuda_library)
+        advance_both(run, orun, 2, dt=0.002)
+        compare(run, orun, tol=1e-12)
+
+
+def test_observables_spectra_speed(cuda_library):
+    run, orun = make_case(64, forcing=0.1, library=cuda_library)
+    advance_both(run, orun, 3, dt=0.005)
+    ob = run.observables()
+    d, st = orun.dom, orun.state
+    assert ob["kinetic_energy"] == pytest.approx(O.kinetic_energy(d, st.uh), rel=1e-12)
+    assert ob["dissipation"] == pytest.approx(O.dissipation(d, st.uh, 0.01), rel=1e-12)
+    assert ob["scalar_variance"] == pytest.approx(O.scalar_variance(d, st.phih), rel=1e-12)
+    assert ob["scalar_dissipation"] == pytest.approx(O.scalar_dissipation(d, st.phih, 0.01), rel=1e-12)
+    assert np.allclose(run.energy_spectrum(), O.energy_spectrum(d, st.uh), rtol=1e-11, atol=1e-18)
+    assert np.allclose(run.scalar_spectrum(), O.scalar_spectrum(d, st.phih), rtol=1e-11, atol=1e-18)
+    assert run.max_speed() == pytest.approx(orun.speed, rel=1e-12)
+    assert np.max(np.abs(run.velocity_physical() - orun.u)) < 1e-12
+
+
+def test_exact_diffusion_with_zero_velocity(cuda_library):
+    # test/scalar.jl:42-60: φ̂(T) = exp(−ϰ|κ|²T) φ̂(0) to round-off
+    N, nu, Sc = 32, 0.1, 0.7
+    ph0 = S.seed_scalar(N, 1.0, seed=3)
+    run = gbght.simulation(gbght.Setup(grid_points_per_axis=N, viscosity=nu, schmidt=Sc),
+                           np.zeros((3, N, N, N // 2 + 1), complex), ph0, library=cuda_library)
+    for _ in range(25):
+        run.advance(0.02)
+    _, pe = run.export_state()
+    expected = ph0 * np.exp(-(nu / Sc) * S.wavenumbers(N)[3] * 0.5)
+    assert rel_l2(pe, expected) < 1e-10
+
+
+def test_planted_reality_violation_removed(cuda_library):
+    N = 32
+    uh = S.seed_velocity(N, 0.5, seed=1)
+    ph = S.seed_scalar(N, 0.5, seed=2)
+    d = 2e-6 * np.max(np.abs(uh[:, :, :, 0]))
+    uh[:, 0, 1, 0] += 1j * d
+    uh[:, 0, N - 1, 0] += 1j * d
+    ph[0, 1, 0] += 1j * d
+    ph[0, N - 1, 0] += 1j * d
+    run, _ = make_case(N, forcing=0.1, uh=uh, ph=ph, library=cuda_library)
+    run.advance(0.01)
+    ue, pe = run.export_state()
+    neg = (-np.arange(N)) % N
+    for f in (ue, pe):
+        plane = f[..., 0]
+        assert np.max(np.abs(plane - np.conj(plane[..., neg, :][..., :, neg]))) == 0.0
+
+
+def test_separate_calls_equal_advance(cuda_library):
+    a, _ = make_case(32, forcing=0.1, tracers=500, library=cuda_library)
+    b, _ = make_case(32, forcing=0.1, tracers=500, library=cuda_library)
+    a.advance(0.01)
+    b.step(0.01)
+    b.deposit()
+    b.advect(0.01)
+    b.deposit_tracers(0.01)
+    ua, pa = a.export_state()
+    ub, pb = b.export_state()
+    assert np.array_equal(ua, ub) and np.array_equal(pa, pb)
+    assert np.array_equal(a.tracers(), b.tracers())
+
+
+def test_nonfinite_state_trips_the_guard(cuda_library):
+    N = 32
+    uh = S.seed_velocity(N, 0.5, seed=0)
+    uh[0, 0, 1, 1] = complex(np.nan, 0.0)
+    run, _ = make_case(N, uh=uh, tracers=10, library=cuda_library)
+    with pytest.raises(gbght.ScheduleError, match="blown up"):
+        run.advance(0.01)
+
+
+def test_fp32_mixed_short_time_error(cuda_library):
+    # FP32 transforms, products and updates; FP64 integrating factor, forcing normalisation,
+    # spectra and tracer positions. Short-time field error and spectra against the FP64 oracle.
+    run, orun = make_case(64, forcing=0.1, G=(1.0, 0.0, 0.0), precision="fp32_mixed", tracers=1000,
+                          library=cuda_library)
+    advance_both(run, orun, 10, dt=0.005)
+    ue, pe = run.export_state()
+    assert rel_l2(ue, orun.state.uh) < 1e-5
+    assert rel_l2(pe, orun.state.phih) < 1e-5
+    for got, want in ((run.energy_spectrum(), O.energy_spectrum(orun.dom, orun.state.uh)),
+                      (run.scalar_spectrum(), O.scalar_spectrum(orun.dom, orun.state.phih))):
+        live = want > 1e-6 * want.max()
+        assert np.max(np.abs(got[live] - want[live]) / want[live]) < 1e-5

@@ -1,0 +1,99 @@
+"""The C ABI's argument and schedule refusals, which mirror the reference's ArgumentError and
+ErrorException cases. These run through the host-check build; the refusals are host code shared
+with the CUDA library."""
+import math
+
+import numpy as np
+import pytest
+
+import gbght
+from gbght import seed as S
+from pairs import make_case
+
+
+def test_bad_configurations_are_argument_errors(hostcheck_library):
+    with pytest.raises(ValueError, match="viscosity"):
+        gbght.Run(gbght.Setup(grid_points_per_axis=16, viscosity=0.0), library=hostcheck_library)
+    with pytest.raises(ValueError, match="schmidt"):
+        gbght.Run(gbght.Setup(grid_points_per_axis=16, schmidt=-1.0), library=hostcheck_library)
+    with pytest.raises(ValueError, match="grid_points_per_axis"):
+        gbght.Run(gbght.Setup(grid_points_per_axis=20), library=hostcheck_library)
+    with pytest.raises(ValueError, match="mean scalar gradient"):
+        gbght.Run(gbght.Setup(grid_points_per_axis=16, scalar=False, mean_gradient=(1.0, 0, 0)),
+                  library=hostcheck_library)
+
+
+def test_state_outside_the_retained_ball_is_refused(hostcheck_library):
+    N = 16
+    run = gbght.Run(gbght.Setup(grid_points_per_axis=N), library=hostcheck_library)
+    uh = S.seed_velocity(N, 0.5, seed=0)
+    ph = S.seed_scalar(N, 0.5, seed=1)
+    uh[0, 0, 0, N // 2] = 1.0            # the Nyquist plane: outside the 2/3 ball
+    with pytest.raises(ValueError, match="outside the retained"):
+        run.import_state(uh, ph)
+
+
+def test_step_needs_a_current_deposit(hostcheck_library):
+    run, _ = make_case(16, library=hostcheck_library)
+    run.step(0.01)
+    with pytest.raises(gbght.ScheduleError, match="stale"):
+        run.step(0.01)
+    run.deposit()
+    run.step(0.01)
+
+
+def test_nonpositive_or_nonfinite_steps_are_refused(hostcheck_library):
+    run, _ = make_case(16, tracers=4, library=hostcheck_library)
+    for bad in (0.0, -0.01, math.inf, math.nan):
+        with pytest.raises(ValueError):
+            run.step(bad)
+    with pytest.raises(ValueError):
+        run.advance(math.inf)
+
+
+def test_particle_schedule_refusals(hostcheck_library):
+    run, _ = make_case(16, tracers=4, library=hostcheck_library)
+    # the fields have not moved past the tracers' sample: the push is refused
+    with pytest.raises(gbght.ScheduleError, match="one step ahead"):
+        run.advect(0.01)
+    run.step(0.01)
+    run.deposit()
+    with pytest.raises(ValueError, match="positive"):
+        run.advect(-1.0)
+    # a second sample at the same positions is refused
+    with pytest.raises(gbght.ScheduleError):
+        run.deposit_tracers(0.01)
+    run.advect(0.01)
+    with pytest.raises(ValueError, match="later"):
+        run.deposit_tracers(0.0)
+    run.deposit_tracers(0.01)
+    # an iteration whose fields were stepped alone is refused whole
+    run.step(0.01)
+    run.deposit()
+    run.advect(0.01)
+    with pytest.raises(gbght.ScheduleError):
+        run.advance(0.01)
+
+
+def test_blowup_guard_names_the_step(hostcheck_library):
+    N = 16
+    uh = S.seed_velocity(N, 0.5, seed=0)
+    ph = S.seed_scalar(N, 0.5, seed=1)
+    uh[0, 0, 1, 1] = complex(np.nan, 0.0)   # a retained mode made non-finite on the host
+    run, _ = make_case(N, uh=uh, ph=ph, library=hostcheck_library)
+    assert not math.isfinite(run.max_speed())
+    with pytest.raises(gbght.ScheduleError, match="blown up"):
+        run.advance(None)
+    with pytest.raises(gbght.ScheduleError, match="blown up"):
+        run.advance(0.01)
+    assert run.status_word() & 0x1
+
+
+def test_empty_band_clamps_and_flags(hostcheck_library):
+    N = 16
+    uh = S.seed_velocity(N, 0.5, seed=0)
+    k2 = S.wavenumbers(N)[3]
+    uh = uh * ~((k2 >= 0.25) & (k2 <= 6.25))[None]
+    run, _ = make_case(N, uh=uh, forcing=0.1, library=hostcheck_library)
+    run.advance(0.01)
+    assert run.status_word() & 0x2
