@@ -106,13 +106,29 @@ template <class T, int R, int SIGN> GBGHT_HD void dft(Cplx<T>* v) {
 
 // ---- the tile transform -------------------------------------------------------------------------
 
-template <class T, int N, int TL, int NT, int SIGN, int S = 0>
+// Index of element e of line l in a tile of TL lines. With SWZ, the 16-byte chunks of each
+// 128-byte row are permuted by XOR with (e mod 8), so that both a row (fixed e, varying l) and a
+// column (fixed l, consecutive e) are read without bank conflicts.
+template <int TL, bool SWZ>
+GBGHT_HD int tix(int e, int l) {
+  if constexpr (!SWZ) {
+    return e * TL + l;
+  } else if constexpr (TL == 8) {
+    return e * 8 + (l ^ (e & 7));
+  } else {
+    static_assert(TL == 16, "swizzled tiles are 128-byte rows");
+    return e * 16 + ((((l >> 1) ^ (e & 7)) << 1) | (l & 1));
+  }
+}
+
+// ACT ≤ TL lines are transformed; lines ACT..TL−1 are left untouched.
+template <class T, int N, int TL, int NT, int SIGN, bool SWZ = false, int ACT = TL, int S = 0>
 GBGHT_HD void tile_fft(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTRICT tw) {
   if constexpr (S < Radices<N>::n) {
     constexpr int R = Radices<N>::r[S];
     constexpr int NS = stage_ns<N>(S);
     constexpr int NB = N / R;
-    constexpr int TOT = NB * TL;
+    constexpr int TOT = NB * ACT;
     constexpr int BPT = (TOT + NT - 1) / NT;
     constexpr int TWS = N / (NS * R);
     Cplx<T> v[BPT][R];
@@ -120,10 +136,10 @@ GBGHT_HD void tile_fft(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTRICT
     for (int b = 0; b < BPT; ++b) {
       const int idx = c.tid + b * NT;
       if (BPT * NT == TOT || idx < TOT) {
-        const int l = idx % TL, j = idx / TL;
+        const int l = idx % ACT, j = idx / ACT;
         const int jm = j % NS;
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[b][r] = buf[(j + r * NB) * TL + l];
+        for (int r = 0; r < R; ++r) v[b][r] = buf[tix<TL, SWZ>(j + r * NB, l)];
         if constexpr (NS > 1) {
 #pragma unroll
           for (int r = 1; r < R; ++r) {
@@ -139,16 +155,16 @@ GBGHT_HD void tile_fft(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTRICT
     for (int b = 0; b < BPT; ++b) {
       const int idx = c.tid + b * NT;
       if (BPT * NT == TOT || idx < TOT) {
-        const int l = idx % TL, j = idx / TL;
+        const int l = idx % ACT, j = idx / ACT;
         const int jm = j % NS;
         dft<T, R, SIGN>(v[b]);
         const int base = (j / NS) * NS * R + jm;
 #pragma unroll
-        for (int r = 0; r < R; ++r) buf[(base + r * NS) * TL + l] = v[b][r];
+        for (int r = 0; r < R; ++r) buf[tix<TL, SWZ>(base + r * NS, l)] = v[b][r];
       }
     }
     GBGHT_SYNC();
-    tile_fft<T, N, TL, NT, SIGN, S + 1>(c, buf, tw);
+    tile_fft<T, N, TL, NT, SIGN, SWZ, ACT, S + 1>(c, buf, tw);
   }
 }
 

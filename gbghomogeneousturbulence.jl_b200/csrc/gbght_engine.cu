@@ -86,51 +86,152 @@ static void emu_grid(int gx, int gy, int gz, size_t smem, F&& body) {
 // ------------------------------------------------------------------------------------------------
 #ifndef GBGHT_EMU
 #define CTA_CTX Cta c{int(threadIdx.x), int(blockIdx.x), int(blockIdx.y), int(blockIdx.z)}
-extern __shared__ __align__(16) unsigned char g_smem[];
+extern __shared__ __align__(1024) unsigned char g_smem[];
+
+__device__ __forceinline__ void init_bars(uint64_t* bar, int n) {
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < n; ++i) mbar_init(bar + i, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_proxy_async();
+  }
+  __syncthreads();
+}
+
+// rows of a 2-D tensor map per box along the row dimension: the largest divisor of N ≤ 256
+template <int N> constexpr int box_rows() { return N > 256 ? (N % 256 == 0 ? 256 : N / 2) : N; }
 
 template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT) k_y_inverse(Geometry g, const Cplx<T>* A, Cplx<T>* B, int c0, const Cplx<T>* tw) {
-  CTA_CTX;
-  body_y_inverse<T, N, TL, NT>(c, reinterpret_cast<Cplx<T>*>(g_smem), g, A, B, c0, tw);
-}
-template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT) k_y_forward(Geometry g, const Cplx<T>* B, Cplx<T>* A, const Cplx<T>* tw) {
-  CTA_CTX;
-  body_y_forward<T, N, TL, NT>(c, reinterpret_cast<Cplx<T>*>(g_smem), g, B, A, tw);
-}
-template <class T, int N, int NT>
-__global__ void __launch_bounds__(NT) k_x_products(Geometry g, Cplx<T>* B, int has_scalar, const Cplx<T>* tw) {
-  CTA_CTX;
-  body_x_products<T, N, NT>(c, reinterpret_cast<Cplx<T>*>(g_smem), g, B, has_scalar, tw);
-}
-template <class T, int N, int NT>
-__global__ void __launch_bounds__(NT) k_x_velocity(Geometry g, const Cplx<T>* B, T* u, unsigned long long* maxbits,
-                                                   const Cplx<T>* tw) {
+__global__ void __launch_bounds__(NT, 2) k_y_inverse(const __grid_constant__ TmaMaps m, Geometry g, int c0,
+                                                     const Cplx<T>* tw, unsigned int* status) {
   CTA_CTX;
   Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
-  double* red = reinterpret_cast<double*>(sm + N * 8);
-  const double m = body_x_velocity<T, N, NT>(c, sm, red, g, B, u, tw);
-  if (threadIdx.x == 0) atomicMax(maxbits, static_cast<unsigned long long>(__double_as_longlong(m)));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + N * TL);
+  init_bars(bar, 1);
+  const int kx0 = c.bx * TL, z = c.by, comp = c0 + c.bz;
+  if (c.tid == 0) {
+    const int row0 = (comp * N + z) * g.NY2;
+    mbar_expect_tx(bar, uint32_t(2 * (g.K + 1) * TL * sizeof(Cplx<T>)));
+    tma_load_2d(sm, &m.a_ld, 2 * kx0, row0, bar);                            // q 0..K   → rows 0..K
+    tma_load_2d(sm + (N - g.K - 1) * TL, &m.a_ld, 2 * kx0, row0 + g.K, bar);  // q K..2K → rows N−K−1..N−1
+  }
+  mbar_wait(bar, 0, status);
+  y_inverse_compute<T, N, TL, NT>(c, sm, g, tw);
+  fence_proxy_async();
+  __syncthreads();
+  if (c.tid == 0) {
+    constexpr int BY = box_rows<N>();
+    for (int y0 = 0; y0 < N; y0 += BY) tma_store_2d(&m.b, 2 * kx0, (comp * N + z) * N + y0, sm + y0 * TL);
+    bulk_commit();
+    bulk_wait_read();
+  }
 }
+
 template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT) k_z_epilogue(Geometry g, Cplx<T>* A, Cplx<T>* S, Cplx<T>* H, StageArgs st,
-                                                   const double* amp, double* partial, const Cplx<T>* tw) {
+__global__ void __launch_bounds__(NT, 2) k_y_forward(const __grid_constant__ TmaMaps m, Geometry g, const Cplx<T>* tw,
+                                                     unsigned int* status) {
+  CTA_CTX;
+  Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + N * TL);
+  init_bars(bar, 1);
+  const int kx0 = c.bx * TL, z = c.by, comp = c.bz;
+  constexpr int BY = box_rows<N>();
+  if (c.tid == 0) {
+    mbar_expect_tx(bar, uint32_t(N * TL * sizeof(Cplx<T>)));
+    for (int y0 = 0; y0 < N; y0 += BY) tma_load_2d(sm + y0 * TL, &m.b, 2 * kx0, (comp * N + z) * N + y0, bar);
+  }
+  mbar_wait(bar, 0, status);
+  tile_fft<T, N, TL, NT, -1>(c, sm, tw);
+  fence_proxy_async();
+  __syncthreads();
+  if (c.tid == 0) {
+    const int row0 = (comp * N + z) * g.NY2;
+    tma_store_2d(&m.a_st1, 2 * kx0, row0, sm);                                  // rows 0..K     → q 0..K
+    tma_store_2d(&m.a_st2, 2 * kx0, row0 + g.K + 1, sm + (N - g.K) * TL);         // rows N−K..N−1 → q K+1..2K
+    bulk_commit();
+    bulk_wait_read();
+  }
+}
+
+template <class T, int N, int NT>
+__global__ void __launch_bounds__(NT, 2) k_x_products(Geometry g, Cplx<T>* B, int has_scalar, int KXS,
+                                                      const Cplx<T>* tw, unsigned int* status) {
+  CTA_CTX;
+  using X = XShape<T>;
+  Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
+  Cplx<T>* stg = sm + N * X::TL;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(stg + 7 * X::P * KXS);
+  init_bars(bar, 1);
+  const int y0 = X::P * c.bx, z = c.by;
+  const int nin = has_scalar ? 7 : 6, nout = has_scalar ? 6 : 3;
+  const uint32_t row_bytes = uint32_t(KXS * sizeof(Cplx<T>));
+  if (c.tid == 0) {
+    mbar_expect_tx(bar, row_bytes * nin * X::P);
+    for (int cc = 0; cc < nin; ++cc)
+      for (int p = 0; p < X::P; ++p) bulk_load(stg + (cc * X::P + p) * KXS, B + idxB(g, cc, z, y0 + p, 0), row_bytes, bar);
+  }
+  mbar_wait(bar, 0, status);
+  x_products_compute<T, N, NT>(c, sm, stg, KXS, g, has_scalar, tw);
+  fence_proxy_async();
+  __syncthreads();
+  if (c.tid == 0) {
+    for (int cc = 0; cc < nout; ++cc)
+      for (int p = 0; p < X::P; ++p) bulk_store(B + idxB(g, cc, z, y0 + p, 0), stg + (cc * X::P + p) * KXS, row_bytes);
+    bulk_commit();
+    bulk_wait_read();
+  }
+}
+
+template <class T, int N, int NT>
+__global__ void __launch_bounds__(NT, 2) k_x_velocity(Geometry g, const Cplx<T>* B, T* u, int KXS,
+                                                      unsigned long long* maxbits, const Cplx<T>* tw,
+                                                      unsigned int* status) {
+  CTA_CTX;
+  using X = XShape<T>;
+  Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
+  Cplx<T>* stg = sm + N * X::TL;
+  double* red = reinterpret_cast<double*>(stg + 3 * X::PV * KXS);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(red + NT);
+  init_bars(bar, 1);
+  const int y0 = X::PV * c.bx, z = c.by;
+  const uint32_t row_bytes = uint32_t(KXS * sizeof(Cplx<T>));
+  if (c.tid == 0) {
+    mbar_expect_tx(bar, row_bytes * 3 * X::PV);
+    for (int cc = 0; cc < 3; ++cc)
+      for (int p = 0; p < X::PV; ++p) bulk_load(stg + (cc * X::PV + p) * KXS, B + idxB(g, cc, z, y0 + p, 0), row_bytes, bar);
+  }
+  mbar_wait(bar, 0, status);
+  const double mx = x_velocity_compute<T, N, NT>(c, sm, stg, KXS, red, g, u, tw);
+  if (c.tid == 0) atomicMax(maxbits, static_cast<unsigned long long>(__double_as_longlong(mx)));
+}
+
+template <class T, int N, int TL, int NT>
+__global__ void __launch_bounds__(NT, 2) k_z_epilogue(const __grid_constant__ TmaMaps m, Geometry g, Cplx<T>* A,
+                                                      Cplx<T>* S, Cplx<T>* H, StageArgs st, const double* amp,
+                                                      double* partial, const Cplx<T>* tw, unsigned int* status) {
   CTA_CTX;
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
   Cplx<T>* Rt = W + N * TL;
   double* red = reinterpret_cast<double*>(Rt + 3 * g.NY2 * TL);
-  const double e = body_z_epilogue<T, N, TL, NT>(c, W, Rt, red, g, A, S, H, st, amp, tw);
-  if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(red + NT);
+  init_bars(bar, 2);
+  ZTileIO<T, N, TL> io{g, A, c.by, c.bx * TL, &m.az, bar, {0u, 0u}, status};
+  const double e = body_z_epilogue<T, N, TL, NT>(c, W, Rt, red, g, io, S, H, st, amp, tw);
+  if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
 }
+
 template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT) k_z_init(Geometry g, Cplx<T>* A, const Cplx<T>* S, int has_scalar, double* partial,
-                                               const Cplx<T>* tw) {
+__global__ void __launch_bounds__(NT, 2) k_z_init(const __grid_constant__ TmaMaps m, Geometry g, Cplx<T>* A,
+                                                  const Cplx<T>* S, int has_scalar, double* partial, const Cplx<T>* tw,
+                                                  unsigned int* status) {
   CTA_CTX;
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
   Cplx<T>* Rt = W + N * TL;
   double* red = reinterpret_cast<double*>(Rt + 3 * g.NY2 * TL);
-  const double e = body_z_init<T, N, TL, NT>(c, W, Rt, red, g, A, S, has_scalar, tw);
-  if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(red + NT);
+  init_bars(bar, 2);
+  ZTileIO<T, N, TL> io{g, A, c.by, c.bx * TL, &m.az, bar, {0u, 0u}, status};
+  const double e = body_z_init<T, N, TL, NT>(c, W, Rt, red, g, io, S, has_scalar, tw);
+  if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
 }
 template <class T>
 __global__ void k_reality(Geometry g, Cplx<T>* S, int ncomp) {
@@ -270,6 +371,9 @@ class EngineImpl final : public Engine {
       if ((err = alloc(&X_, 3 * size_t(p.tracers) * sizeof(double)))) return err;
       if ((err = alloc(&F_, 3 * size_t(p.tracers) * sizeof(double)))) return err;
     }
+#ifndef GBGHT_EMU
+    if ((err = make_maps())) return err;
+#endif
     // twiddles e^(-2πi k/N) in extended precision
     std::vector<Cplx<T>> tw(N);
     for (int k = 0; k < N; ++k) {
@@ -379,6 +483,9 @@ class EngineImpl final : public Engine {
     double m;
     std::memcpy(&m, &bits, sizeof m);
     *max_speed2 = m;
+    unsigned int st = 0;
+    if ((err = rt_d2h(&st, status_, sizeof st, stream_))) return err;
+    if (st & GBGHT_DEV_TIMEOUT) return "a bulk copy did not complete within its bounded wait (device status 0x4)";
     return nullptr;
   }
 
@@ -617,10 +724,18 @@ class EngineImpl final : public Engine {
     return hi * hi;
   }
 
-  size_t smem_y() const { return size_t(N) * TLY * sizeof(Cplx<T>); }
-  size_t smem_x() const { return size_t(N) * 8 * sizeof(Cplx<T>) + size_t(NTX) * sizeof(double); }
+  static constexpr size_t kBarBytes = 32;
+  int kxs() const { return x_kxs(g_.K, int(sizeof(Cplx<T>))); }
+  size_t smem_y() const { return size_t(N) * TLY * sizeof(Cplx<T>) + kBarBytes; }
+  size_t smem_x() const {
+    return size_t(N) * XShape<T>::TL * sizeof(Cplx<T>) + size_t(7) * XShape<T>::P * kxs() * sizeof(Cplx<T>) + kBarBytes;
+  }
+  size_t smem_xv() const {
+    return size_t(N) * XShape<T>::TL * sizeof(Cplx<T>) + size_t(3) * XShape<T>::PV * kxs() * sizeof(Cplx<T>) +
+           size_t(NTX) * sizeof(double) + kBarBytes;
+  }
   size_t smem_z() const {
-    return (size_t(N) * TLZ + 3 * size_t(g_.NY2) * TLZ) * sizeof(Cplx<T>) + size_t(NTZ) * sizeof(double);
+    return (size_t(N) * TLZ + 3 * size_t(g_.NY2) * TLZ) * sizeof(Cplx<T>) + size_t(NTZ) * sizeof(double) + kBarBytes;
   }
 
 #ifndef GBGHT_EMU
@@ -633,60 +748,120 @@ class EngineImpl final : public Engine {
     set(reinterpret_cast<const void*>(k_y_inverse<T, N, TLY, NTY>), smem_y());
     set(reinterpret_cast<const void*>(k_y_forward<T, N, TLY, NTY>), smem_y());
     set(reinterpret_cast<const void*>(k_x_products<T, N, NTX>), smem_x());
-    set(reinterpret_cast<const void*>(k_x_velocity<T, N, NTX>), smem_x());
+    set(reinterpret_cast<const void*>(k_x_velocity<T, N, NTX>), smem_xv());
     set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ>), smem_z());
     set(reinterpret_cast<const void*>(k_z_init<T, N, TLZ, NTZ>), smem_z());
     return e;
+  }
+
+  // Tensor maps over A and B (see TmaMaps in passes.cuh), encoded through the driver entry point.
+  const char* make_maps() {
+    using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    const char* e = cuda_err(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q),
+                             "cudaGetDriverEntryPoint(cuTensorMapEncodeTiled)");
+    if (e) return e;
+    if (!fn || q != cudaDriverEntryPointSuccess) return "cuTensorMapEncodeTiled is unavailable";
+    Encode encode = reinterpret_cast<Encode>(fn);
+    const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const cuuint64_t inner = cuuint64_t(2) * g_.KXP;                // reals per row
+    const cuuint64_t pitch = cuuint64_t(g_.KXP) * sizeof(Cplx<T>);  // bytes per row
+    const cuuint32_t ones[3] = {1, 1, 1};
+    auto map2 = [&](CUtensorMap* m, void* base, cuuint64_t rows, cuuint32_t bx, cuuint32_t by) -> bool {
+      const cuuint64_t dims[2] = {inner, rows};
+      const cuuint64_t strides[1] = {pitch};
+      const cuuint32_t box[2] = {bx, by};
+      return encode(m, dt, 2, base, dims, strides, box, ones, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    const cuuint32_t bxy = 2 * TLY, bxz = 2 * TLZ;
+    const cuuint32_t K1 = cuuint32_t(g_.K + 1), K0 = cuuint32_t(g_.K);
+    const cuuint32_t BY = cuuint32_t(N > 256 ? (N % 256 == 0 ? 256 : N / 2) : N);
+    if (!map2(&maps_.a_ld, A_, cuuint64_t(7) * N * g_.NY2, bxy, K1)) return "tensor map a_ld";
+    if (!map2(&maps_.a_st1, A_, cuuint64_t(7) * N * g_.NY2, bxy, K1)) return "tensor map a_st1";
+    if (!map2(&maps_.a_st2, A_, cuuint64_t(7) * N * g_.NY2, bxy, K0)) return "tensor map a_st2";
+    if (!map2(&maps_.b, B_, cuuint64_t(7) * N * N, bxy, BY)) return "tensor map b";
+    {
+      const cuuint64_t dims[3] = {inner, cuuint64_t(g_.NY2), cuuint64_t(7) * N};
+      const cuuint64_t strides[2] = {pitch, pitch * g_.NY2};
+      const cuuint32_t box[3] = {bxz, 1, BY};
+      if (encode(&maps_.az, dt, 3, A_, dims, strides, box, ones, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return "tensor map az";
+    }
+    return nullptr;
   }
 #endif
 
   void y_inverse(int c0, int nc) {
 #ifdef GBGHT_EMU
     emu_grid(g_.KXP / TLY, N, nc, smem_y(), [&](const Cta& c, void* sm) {
-      body_y_inverse<T, N, TLY, 1>(c, static_cast<Cplx<T>*>(sm), g_, A_, B_, c0, tw_);
+      Cplx<T>* t = static_cast<Cplx<T>*>(sm);
+      y_inverse_load_host<T, N, TLY>(c, t, g_, A_, c0);
+      y_inverse_compute<T, N, TLY, 1>(c, t, g_, tw_);
+      y_store_host<T, N, TLY>(c, t, g_, B_, c0 + c.bz);
     });
 #else
     pbegin(PROF_Y_INVERSE);
-    k_y_inverse<T, N, TLY, NTY><<<dim3(g_.KXP / TLY, N, nc), NTY, smem_y(), stream_>>>(g_, A_, B_, c0, tw_);
+    k_y_inverse<T, N, TLY, NTY><<<dim3(g_.KXP / TLY, N, nc), NTY, smem_y(), stream_>>>(maps_, g_, c0, tw_, status_);
     pend();
 #endif
   }
   void y_forward(int nc) {
 #ifdef GBGHT_EMU
     emu_grid(g_.KXP / TLY, N, nc, smem_y(), [&](const Cta& c, void* sm) {
-      body_y_forward<T, N, TLY, 1>(c, static_cast<Cplx<T>*>(sm), g_, B_, A_, tw_);
+      Cplx<T>* t = static_cast<Cplx<T>*>(sm);
+      y_forward_load_host<T, N, TLY>(c, t, g_, B_);
+      tile_fft<T, N, TLY, 1, -1>(c, t, tw_);
+      y_forward_store_host<T, N, TLY>(c, t, g_, A_);
     });
 #else
     pbegin(PROF_Y_FORWARD);
-    k_y_forward<T, N, TLY, NTY><<<dim3(g_.KXP / TLY, N, nc), NTY, smem_y(), stream_>>>(g_, B_, A_, tw_);
+    k_y_forward<T, N, TLY, NTY><<<dim3(g_.KXP / TLY, N, nc), NTY, smem_y(), stream_>>>(maps_, g_, tw_, status_);
     pend();
 #endif
   }
   void x_products() {
+    using X = XShape<T>;
+    const int KXS = kxs();
 #ifdef GBGHT_EMU
-    emu_grid(N / 2, N, 1, smem_x(), [&](const Cta& c, void* sm) {
-      body_x_products<T, N, 1>(c, static_cast<Cplx<T>*>(sm), g_, B_, p_.scalar, tw_);
+    emu_grid(N / X::P, N, 1, smem_x(), [&](const Cta& c, void* sm) {
+      Cplx<T>* t = static_cast<Cplx<T>*>(sm);
+      Cplx<T>* stg = t + N * X::TL;
+      x_stage_in_host<T, X::P>(c, stg, KXS, g_, B_, p_.scalar ? 7 : 6);
+      x_products_compute<T, N, 1>(c, t, stg, KXS, g_, p_.scalar, tw_);
+      x_stage_out_host<T, X::P>(c, stg, KXS, g_, B_, p_.scalar ? 6 : 3);
     });
 #else
     pbegin(PROF_X_PRODUCTS);
-    k_x_products<T, N, NTX><<<dim3(N / 2, N, 1), NTX, smem_x(), stream_>>>(g_, B_, p_.scalar, tw_);
+    k_x_products<T, N, NTX><<<dim3(N / X::P, N, 1), NTX, smem_x(), stream_>>>(g_, B_, p_.scalar, KXS, tw_, status_);
     pend();
 #endif
   }
   void x_velocity() {
+    using X = XShape<T>;
+    const int KXS = kxs();
 #ifdef GBGHT_EMU
     unsigned long long* mb = maxbits_;
-    emu_grid(N / 4, N, 1, smem_x(), [&](const Cta& c, void* sm) {
-      Cplx<T>* s = static_cast<Cplx<T>*>(sm);
-      double* red = reinterpret_cast<double*>(s + N * 8);
-      const double m = body_x_velocity<T, N, 1>(c, s, red, g_, B_, U_, tw_);
+    emu_grid(N / X::PV, N, 1, smem_xv(), [&](const Cta& c, void* sm) {
+      Cplx<T>* t = static_cast<Cplx<T>*>(sm);
+      Cplx<T>* stg = t + N * X::TL;
+      double* red = reinterpret_cast<double*>(stg + 3 * X::PV * KXS);
+      x_stage_in_host<T, X::PV>(c, stg, KXS, g_, B_, 3);
+      const double m = x_velocity_compute<T, N, 1>(c, t, stg, KXS, red, g_, U_, tw_);
       unsigned long long bits;
       std::memcpy(&bits, &m, sizeof bits);
       if (bits > *mb) *mb = bits;
     });
 #else
     pbegin(PROF_X_VELOCITY);
-    k_x_velocity<T, N, NTX><<<dim3(N / 4, N, 1), NTX, smem_x(), stream_>>>(g_, B_, U_, maxbits_, tw_);
+    k_x_velocity<T, N, NTX><<<dim3(N / X::PV, N, 1), NTX, smem_xv(), stream_>>>(g_, B_, U_, KXS, maxbits_, tw_,
+                                                                                 status_);
     pend();
 #endif
   }
@@ -697,12 +872,13 @@ class EngineImpl final : public Engine {
       Cplx<T>* W = static_cast<Cplx<T>*>(sm);
       Cplx<T>* Rt = W + N * TLZ;
       double* red = reinterpret_cast<double*>(Rt + 3 * g_.NY2 * TLZ);
-      partial_[c.by * gx + c.bx] = body_z_epilogue<T, N, TLZ, 1>(c, W, Rt, red, g_, A_, S_, H_, st, amp_, tw_);
+      ZTileIO<T, N, TLZ> io{g_, A_, c.by, c.bx * TLZ, nullptr, nullptr, {0u, 0u}, nullptr};
+      partial_[c.by * gx + c.bx] = body_z_epilogue<T, N, TLZ, 1>(c, W, Rt, red, g_, io, S_, H_, st, amp_, tw_);
     });
 #else
     pbegin(PROF_Z_EPILOGUE);
-    k_z_epilogue<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, S_, H_, st, amp_,
-                                                                                           partial_, tw_);
+    k_z_epilogue<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(
+        maps_, g_, A_, S_, H_, st, amp_, partial_, tw_, status_);
     pend();
 #endif
   }
@@ -713,11 +889,12 @@ class EngineImpl final : public Engine {
       Cplx<T>* W = static_cast<Cplx<T>*>(sm);
       Cplx<T>* Rt = W + N * TLZ;
       double* red = reinterpret_cast<double*>(Rt + 3 * g_.NY2 * TLZ);
-      partial_[c.by * gx + c.bx] = body_z_init<T, N, TLZ, 1>(c, W, Rt, red, g_, A_, S_, p_.scalar, tw_);
+      ZTileIO<T, N, TLZ> io{g_, A_, c.by, c.bx * TLZ, nullptr, nullptr, {0u, 0u}, nullptr};
+      partial_[c.by * gx + c.bx] = body_z_init<T, N, TLZ, 1>(c, W, Rt, red, g_, io, S_, p_.scalar, tw_);
     });
 #else
-    k_z_init<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, S_, p_.scalar, partial_,
-                                                                                       tw_);
+    k_z_init<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(maps_, g_, A_, S_, p_.scalar,
+                                                                                       partial_, tw_, status_);
 #endif
     return rt_check();
   }
@@ -786,6 +963,7 @@ class EngineImpl final : public Engine {
 
   RunParams p_{};
   Geometry g_{};
+  TmaMaps maps_{};
   double cutoff_ = 0.0;
   size_t nS_ = 0, nA_ = 0, nB_ = 0, nP_ = 0, ntile_ = 0;
   int nshell_ = 0;

@@ -21,6 +21,7 @@
 #pragma once
 
 #include "fft_tile.cuh"
+#include "tma.cuh"
 
 namespace gbght {
 
@@ -45,183 +46,230 @@ GBGHT_HD size_t idxS(const Geometry& g, int c, int qy, int qz, int kx) {
 }
 
 // ================================================================================================
-// y-inverse: A[c][z][ky'][tile] → B[c][z][y][tile], one tile of TL kx columns per CTA.
-// Grid: (KXP/TL, N, ncomp); c = c0 + bz.
+// Tensor maps for the TMA tile copies (device build only).
+//   a_ld   A as rows of KXP elements (dims {2·KXP reals, 7·N·NY2 rows}), box {2·TLY, K+1}
+//   a_st1  the same rows, box {2·TLY, K+1};  a_st2: box {2·TLY, K}
+//   b      B as rows (dims {2·KXP, 7·N·N}), box {2·TLY, BY}, BY the largest divisor of N ≤ 256
+//   az     A as (x, q, c·N + z) (dims {2·KXP, NY2, 7·N}), box {2·TLZ, 1, BZ}, BZ = BY
+// Innermost coordinates are 2·kx0 reals with kx0 a multiple of the tile width, so every copy
+// starts on a 64- or 128-byte boundary.
 // ================================================================================================
-template <class T, int N, int TL, int NT>
-GBGHT_HD void body_y_inverse(const Cta& c, Cplx<T>* sm, const Geometry& g,
-                             const Cplx<T>* GBGHT_RESTRICT A, Cplx<T>* GBGHT_RESTRICT B,
-                             int c0, const Cplx<T>* GBGHT_RESTRICT tw) {
+struct TmaMaps {
+#if defined(__CUDACC__) && !defined(GBGHT_EMU)
+  CUtensorMap a_ld, a_st1, a_st2, b, az;
+#else
+  int unused;
+#endif
+};
+
+// ================================================================================================
+// y-inverse: A[c][z][ky'][tile] → B[c][z][y][tile], one tile of TL kx columns per CTA.
+// Grid: (KXP/TL, N, ncomp); c = c0 + bz. The tile is N rows of TL elements (rows of 128 bytes).
+// Compact rows q ≤ K land in rows 0..K, rows q > K in rows N−NY2+q; the rows between are zero.
+// ================================================================================================
+template <class T, int N, int TL>
+GBGHT_HD void y_inverse_load_host(const Cta& c, Cplx<T>* sm, const Geometry& g, const Cplx<T>* A, int c0) {
   const int kx0 = c.bx * TL, z = c.by, comp = c0 + c.bz;
-  for (int i = c.tid; i < N * TL; i += NT) {
-    const int e = i / TL, l = i % TL;
-    Cplx<T> v = czero<T>();
-    int q = -1;
-    if (e <= g.K) q = e;
-    else if (e >= N - g.K) q = e - N + g.NY2;
-    if (q >= 0) v = A[idxA(g, comp, z, q, kx0 + l)];
-    sm[i] = v;
-  }
+  for (int e = 0; e < N; ++e)
+    for (int l = 0; l < TL; ++l) {
+      int q = -1;
+      if (e <= g.K) q = e;
+      else if (e >= N - g.K) q = e - N + g.NY2;
+      sm[e * TL + l] = q >= 0 ? A[idxA(g, comp, z, q, kx0 + l)] : czero<T>();
+    }
+}
+
+template <class T, int N, int TL>
+GBGHT_HD void y_store_host(const Cta& c, const Cplx<T>* sm, const Geometry& g, Cplx<T>* B, int comp) {
+  const int kx0 = c.bx * TL, z = c.by;
+  for (int y = 0; y < N; ++y)
+    for (int l = 0; l < TL; ++l) B[idxB(g, comp, z, y, kx0 + l)] = sm[y * TL + l];
+}
+
+template <class T, int N, int TL>
+GBGHT_HD void y_forward_load_host(const Cta& c, Cplx<T>* sm, const Geometry& g, const Cplx<T>* B) {
+  const int kx0 = c.bx * TL, z = c.by, comp = c.bz;
+  for (int y = 0; y < N; ++y)
+    for (int l = 0; l < TL; ++l) sm[y * TL + l] = B[idxB(g, comp, z, y, kx0 + l)];
+}
+
+template <class T, int N, int TL>
+GBGHT_HD void y_forward_store_host(const Cta& c, const Cplx<T>* sm, const Geometry& g, Cplx<T>* A) {
+  const int kx0 = c.bx * TL, z = c.by, comp = c.bz;
+  for (int q = 0; q < g.NY2; ++q)
+    for (int l = 0; l < TL; ++l) A[idxA(g, comp, z, q, kx0 + l)] = sm[q_to_row(q, g.K, N, g.NY2) * TL + l];
+}
+
+// zero rows K < e < N−K, then the inverse transform
+template <class T, int N, int TL, int NT>
+GBGHT_HD void y_inverse_compute(const Cta& c, Cplx<T>* sm, const Geometry& g, const Cplx<T>* GBGHT_RESTRICT tw) {
+  for (int i = c.tid; i < (N - 2 * g.K - 1) * TL; i += NT) sm[(g.K + 1) * TL + i] = czero<T>();
   GBGHT_SYNC();
   tile_fft<T, N, TL, NT, +1>(c, sm, tw);
-  for (int i = c.tid; i < N * TL; i += NT) {
-    const int y = i / TL, l = i % TL;
-    B[idxB(g, comp, z, y, kx0 + l)] = sm[i];
-  }
 }
 
 // ================================================================================================
-// y-forward: B[c][z][y][tile] → A[c][z][ky'][tile] (retained rows only).
-// Grid: (KXP/TL, N, ncomp).
-// ================================================================================================
-template <class T, int N, int TL, int NT>
-GBGHT_HD void body_y_forward(const Cta& c, Cplx<T>* sm, const Geometry& g,
-                             const Cplx<T>* GBGHT_RESTRICT B, Cplx<T>* GBGHT_RESTRICT A,
-                             const Cplx<T>* GBGHT_RESTRICT tw) {
-  const int kx0 = c.bx * TL, z = c.by, comp = c.bz;
-  for (int i = c.tid; i < N * TL; i += NT) {
-    const int y = i / TL, l = i % TL;
-    sm[i] = B[idxB(g, comp, z, y, kx0 + l)];
-  }
-  GBGHT_SYNC();
-  tile_fft<T, N, TL, NT, -1>(c, sm, tw);
-  for (int i = c.tid; i < g.NY2 * TL; i += NT) {
-    const int q = i / TL, l = i % TL;
-    A[idxA(g, comp, z, q, kx0 + l)] = sm[q_to_row(q, g.K, N, g.NY2) * TL + l];
-  }
-}
-
-// ================================================================================================
-// x-pass: for two points (z, y0) and (z, y0+1), c2r of u, ω, φ, the products u×ω and uφ, and
-// r2c of the six products. The spectra stay in B's slots (in place). Grid: (N/2, N).
-// Eight lines of the tile:
-//   inverse: line 3p+0 = u_x + i·u_y, 3p+1 = u_z + i·ω_x, 3p+2 = ω_y + i·ω_z (point p), line 6 =
-//            φ(p=0) + i·φ(p=1), line 7 unused
+// x-pass: for P points (z, y0..y0+P−1), c2r of u, ω, φ, the products u×ω and uφ, and r2c of the
+// six products. The spectra stay in B's slots (in place). Grid: (N/P, N).
+// P = TL/4 points share one tile of TL lines (TL = 8 for FP64, 16 for FP32; rows of 128 bytes,
+// swizzled so that rows and columns are both conflict-free):
+//   inverse: line 3p+0 = u_x + i·u_y, 3p+1 = u_z + i·ω_x, 3p+2 = ω_y + i·ω_z (point p), and line
+//            3P + p/2 = φ(p) + i·φ(p+1) for even p: 3P + P/2 lines in use
 //   forward: line 3p+0 = n_x + i·n_y, 3p+1 = n_z + i·f_x, 3p+2 = f_y + i·f_z, n = u×ω, f = uφ
 // Two real lines a, b share one complex transform ("two for one"). Inverse: Z[e] = A[e] + i·B[e]
 // for 0 ≤ e ≤ K, and Z[N−e] = conj(A[e]) + i·conj(B[e]); only the real parts of the kx = 0 bins
 // enter, as in a c2r. Forward: A[k] = (Z[k] + conj Z[N−k])/2, B[k] = (Z[k] − conj Z[N−k])/(2i).
+// The spectra move through a staging area of rows [c][p][KXS] (KXS ≥ K+1 elements, a multiple
+// of 16 bytes), copied whole to and from B.
 // ================================================================================================
-template <class T>
-GBGHT_HD void pack_pair(Cplx<T>* sm, int TL, int N, int line, int e, Cplx<T> a, Cplx<T> b, T sc) {
+template <class T, int SWZ_TL>
+GBGHT_HD void pack_pair(Cplx<T>* sm, int N, int line, int e, Cplx<T> a, Cplx<T> b, T sc) {
   if (e == 0) {
-    sm[line] = cmk<T>(a.x * sc, b.x * sc);
+    sm[tix<SWZ_TL, true>(0, line)] = cmk<T>(a.x * sc, b.x * sc);
   } else {
-    sm[e * TL + line] = cmk<T>((a.x - b.y) * sc, (a.y + b.x) * sc);
-    sm[(N - e) * TL + line] = cmk<T>((a.x + b.y) * sc, (b.x - a.y) * sc);
+    sm[tix<SWZ_TL, true>(e, line)] = cmk<T>((a.x - b.y) * sc, (a.y + b.x) * sc);
+    sm[tix<SWZ_TL, true>(N - e, line)] = cmk<T>((a.x + b.y) * sc, (b.x - a.y) * sc);
   }
 }
 
-template <class T>
-GBGHT_HD void unpack_pair(const Cplx<T>* sm, int TL, int N, int line, int k, Cplx<T>& a, Cplx<T>& b) {
-  const Cplx<T> z = sm[k * TL + line];
-  const Cplx<T> zc = conj(sm[((N - k) % N) * TL + line]);
+template <class T, int SWZ_TL>
+GBGHT_HD void unpack_pair(const Cplx<T>* sm, int N, int line, int k, Cplx<T>& a, Cplx<T>& b) {
+  const Cplx<T> z = sm[tix<SWZ_TL, true>(k, line)];
+  const Cplx<T> zc = conj(sm[tix<SWZ_TL, true>((N - k) % N, line)]);
   const Cplx<T> sp = z + zc, sd = z - zc;
   a = cmk<T>(sp.x * T(0.5), sp.y * T(0.5));
   b = cmk<T>(sd.y * T(0.5), -sd.x * T(0.5));
 }
 
+template <class T> struct XShape {
+  static constexpr int TL = 128 / int(sizeof(Cplx<T>));
+  static constexpr int P = TL / 4;                 // points per tile (products pass)
+  static constexpr int ACT_INV = 3 * P + P / 2;
+  static constexpr int ACT_FWD = 3 * P;
+  static constexpr int PV = TL / 2;                // points per tile (deposit pass)
+  static constexpr int ACT_V = PV + PV / 2;
+};
+
+GBGHT_HD int x_kxs(int K, int elem_bytes) {
+  const int per = 16 / elem_bytes;   // elements per 16 bytes (1 for FP64 complex, 2 for FP32)
+  return ((K + 1 + per - 1) / per) * per;
+}
+
+// staging ← B rows (comps [0, nc) of points y0..y0+P−1)
+template <class T, int P>
+GBGHT_HD void x_stage_in_host(const Cta& c, Cplx<T>* stg, int KXS, const Geometry& g, const Cplx<T>* B, int nc) {
+  const int y0 = P * c.bx, z = c.by;
+  for (int cc = 0; cc < nc; ++cc)
+    for (int p = 0; p < P; ++p)
+      for (int e = 0; e < KXS; ++e) stg[(cc * P + p) * KXS + e] = B[idxB(g, cc, z, y0 + p, e)];
+}
+template <class T, int P>
+GBGHT_HD void x_stage_out_host(const Cta& c, const Cplx<T>* stg, int KXS, const Geometry& g, Cplx<T>* B, int nc) {
+  const int y0 = P * c.bx, z = c.by;
+  for (int cc = 0; cc < nc; ++cc)
+    for (int p = 0; p < P; ++p)
+      for (int e = 0; e < KXS; ++e) B[idxB(g, cc, z, y0 + p, e)] = stg[(cc * P + p) * KXS + e];
+}
+
+// pack, inverse, products, forward, unpack: staging (7 comps in) → staging (6 comps out)
 template <class T, int N, int NT>
-GBGHT_HD void body_x_products(const Cta& c, Cplx<T>* sm, const Geometry& g,
-                              Cplx<T>* GBGHT_RESTRICT B, int has_scalar,
-                              const Cplx<T>* GBGHT_RESTRICT tw) {
-  constexpr int TL = 8;
-  const int y0 = 2 * c.bx, z = c.by;
+GBGHT_HD void x_products_compute(const Cta& c, Cplx<T>* sm, Cplx<T>* stg, int KXS, const Geometry& g,
+                                 int has_scalar, const Cplx<T>* GBGHT_RESTRICT tw) {
+  using X = XShape<T>;
+  constexpr int TL = X::TL, P = X::P;
   const T sc = T(g.inv_norm);
   const int KX1 = g.K + 1;
-  // zero rows that no mode reaches (K < e < N−K)
-  for (int i = c.tid; i < N * TL; i += NT) {
-    const int e = i / TL;
-    if (e > g.K && e < N - g.K) sm[i] = czero<T>();
+  // rows that no mode reaches (K < e < N−K), in every line the inverse uses
+  for (int i = c.tid; i < (N - 2 * g.K - 1) * TL; i += NT) sm[(g.K + 1) * TL + i] = czero<T>();
+  // velocity and vorticity pairs: line 3p+pr holds comps (2pr, 2pr+1) of point p
+  for (int i = c.tid; i < 3 * P * KX1; i += NT) {
+    const int e = i % KX1, line = i / KX1;
+    const int p = line / 3, pr = line % 3;
+    const Cplx<T> a = stg[((2 * pr) * P + p) * KXS + e];
+    const Cplx<T> b = stg[((2 * pr + 1) * P + p) * KXS + e];
+    pack_pair<T, TL>(sm, N, line, e, a, b, sc);
   }
-  if (!has_scalar)
-    for (int i = c.tid; i < N; i += NT) sm[i * TL + 6] = czero<T>();
-  for (int i = c.tid; i < N; i += NT) sm[i * TL + 7] = czero<T>();
-  // lines 0..5: three pairs per point
-  for (int i = c.tid; i < 2 * 3 * KX1; i += NT) {
-    const int e = i % KX1, pr = (i / KX1) % 3, p = i / (3 * KX1);
-    const int ca = 2 * pr, cb = 2 * pr + 1;   // (0,1), (2,3), (4,5)
-    const Cplx<T> a = B[idxB(g, ca, z, y0 + p, e)];
-    const Cplx<T> b = B[idxB(g, cb, z, y0 + p, e)];
-    pack_pair(sm, TL, N, 3 * p + pr, e, a, b, sc);
-  }
-  if (has_scalar)
-    for (int e = c.tid; e < KX1; e += NT) {
-      const Cplx<T> a = B[idxB(g, 6, z, y0, e)];
-      const Cplx<T> b = B[idxB(g, 6, z, y0 + 1, e)];
-      pack_pair(sm, TL, N, 6, e, a, b, sc);
-    }
-  GBGHT_SYNC();
-  tile_fft<T, N, TL, NT, +1>(c, sm, tw);
-  for (int x = c.tid; x < N; x += NT) {
-    Cplx<T>* row = sm + x * TL;
-    const Cplx<T> l6 = row[6];
-#pragma unroll
-    for (int p = 0; p < 2; ++p) {
-      const Cplx<T> L0 = row[3 * p], L1 = row[3 * p + 1], L2 = row[3 * p + 2];
-      const T ux = L0.x, uy = L0.y, uz = L1.x, wx = L1.y, wy = L2.x, wz = L2.y;
-      const T ph = p == 0 ? l6.x : l6.y;
-      const T nx = uy * wz - uz * wy, ny = uz * wx - ux * wz, nz = ux * wy - uy * wx;
-      row[3 * p] = cmk<T>(nx, ny);
-      row[3 * p + 1] = cmk<T>(nz, ux * ph);
-      row[3 * p + 2] = cmk<T>(uy * ph, uz * ph);
-    }
-  }
-  GBGHT_SYNC();
-  tile_fft<T, N, TL, NT, -1>(c, sm, tw);
-  // extract kx ∈ [0, KXP): products 0..2 = n, 3..5 = f; pad columns get zeros
-  const int ncomp = has_scalar ? 6 : 3;
-  for (int i = c.tid; i < 2 * 3 * g.KXP; i += NT) {
-    const int k = i % g.KXP, pr = (i / g.KXP) % 3, p = i / (3 * g.KXP);
+  // scalar pairs: line 3P + h holds φ of points 2h and 2h+1
+  for (int i = c.tid; i < (P / 2) * KX1; i += NT) {
+    const int e = i % KX1, h = i / KX1;
     Cplx<T> a = czero<T>(), b = czero<T>();
-    if (k < KX1) unpack_pair(sm, TL, N, 3 * p + pr, k, a, b);
-    const int ca = 2 * pr, cb = 2 * pr + 1;
-    if (ca < ncomp) B[idxB(g, ca, z, y0 + p, k)] = a;
-    if (cb < ncomp) B[idxB(g, cb, z, y0 + p, k)] = b;
+    if (has_scalar) {
+      a = stg[(6 * P + 2 * h) * KXS + e];
+      b = stg[(6 * P + 2 * h + 1) * KXS + e];
+    }
+    pack_pair<T, TL>(sm, N, 3 * P + h, e, a, b, sc);
+  }
+  GBGHT_SYNC();
+  tile_fft<T, N, TL, NT, +1, true, X::ACT_INV>(c, sm, tw);
+  for (int x = c.tid; x < N; x += NT) {
+#pragma unroll
+    for (int h = 0; h < P / 2; ++h) {
+      const Cplx<T> lp = sm[tix<TL, true>(x, 3 * P + h)];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int p = 2 * h + q;
+        const Cplx<T> L0 = sm[tix<TL, true>(x, 3 * p)], L1 = sm[tix<TL, true>(x, 3 * p + 1)],
+                      L2 = sm[tix<TL, true>(x, 3 * p + 2)];
+        const T ux = L0.x, uy = L0.y, uz = L1.x, wx = L1.y, wy = L2.x, wz = L2.y;
+        const T ph = q == 0 ? lp.x : lp.y;
+        const T nx = uy * wz - uz * wy, ny = uz * wx - ux * wz, nz = ux * wy - uy * wx;
+        sm[tix<TL, true>(x, 3 * p)] = cmk<T>(nx, ny);
+        sm[tix<TL, true>(x, 3 * p + 1)] = cmk<T>(nz, ux * ph);
+        sm[tix<TL, true>(x, 3 * p + 2)] = cmk<T>(uy * ph, uz * ph);
+      }
+    }
+  }
+  GBGHT_SYNC();
+  tile_fft<T, N, TL, NT, -1, true, X::ACT_FWD>(c, sm, tw);
+  // unpack into the staging rows of the six products; the columns past K get zeros
+  for (int i = c.tid; i < 3 * P * KXS; i += NT) {
+    const int k = i % KXS, line = i / KXS;
+    const int p = line / 3, pr = line % 3;
+    Cplx<T> a = czero<T>(), b = czero<T>();
+    if (k < KX1) unpack_pair<T, TL>(sm, N, line, k, a, b);
+    stg[((2 * pr) * P + p) * KXS + k] = a;
+    stg[((2 * pr + 1) * P + p) * KXS + k] = b;
   }
 }
 
 // ================================================================================================
-// x-pass of the deposit: velocity to physical for four points (z, y0..y0+3), the physical
-// velocity written out, and the maximum of |u|² reduced. Grid: (N/4, N).
-//   line p (p < 4) = u_x + i·u_y of point p; line 4 = u_z(0) + i·u_z(1); line 5 = u_z(2) + i·u_z(3)
+// x-pass of the deposit: the velocity to physical for PV = TL/2 points (z, y0..y0+PV−1), written
+// out, and the maximum of |u|² reduced. Grid: (N/PV, N).
+//   line p (p < PV) = u_x + i·u_y of point p; line PV + h = u_z(2h) + i·u_z(2h+1)
 // `red` is NT doubles of shared scratch; the CTA's maximum of |u|² is returned to thread 0.
 // ================================================================================================
 template <class T, int N, int NT>
-GBGHT_HD double body_x_velocity(const Cta& c, Cplx<T>* sm, double* red, const Geometry& g,
-                                const Cplx<T>* GBGHT_RESTRICT B, T* GBGHT_RESTRICT u_phys,
-                                const Cplx<T>* GBGHT_RESTRICT tw) {
-  constexpr int TL = 8;
-  const int y0 = 4 * c.bx, z = c.by;
+GBGHT_HD double x_velocity_compute(const Cta& c, Cplx<T>* sm, Cplx<T>* stg, int KXS, double* red, const Geometry& g,
+                                   T* GBGHT_RESTRICT u_phys, const Cplx<T>* GBGHT_RESTRICT tw) {
+  using X = XShape<T>;
+  constexpr int TL = X::TL, PV = X::PV;
+  const int y0 = PV * c.bx, z = c.by;
   const T sc = T(g.inv_norm);
   const int KX1 = g.K + 1;
-  for (int i = c.tid; i < N * TL; i += NT) {
-    const int e = i / TL, l = i % TL;
-    if ((e > g.K && e < N - g.K) || l >= 6) sm[i] = czero<T>();
-  }
-  for (int i = c.tid; i < 6 * KX1; i += NT) {
+  for (int i = c.tid; i < (N - 2 * g.K - 1) * TL; i += NT) sm[(g.K + 1) * TL + i] = czero<T>();
+  for (int i = c.tid; i < X::ACT_V * KX1; i += NT) {
     const int e = i % KX1, line = i / KX1;
     Cplx<T> a, b;
-    if (line < 4) {
-      a = B[idxB(g, 0, z, y0 + line, e)];
-      b = B[idxB(g, 1, z, y0 + line, e)];
+    if (line < PV) {
+      a = stg[(0 * PV + line) * KXS + e];
+      b = stg[(1 * PV + line) * KXS + e];
     } else {
-      const int p = 2 * (line - 4);
-      a = B[idxB(g, 2, z, y0 + p, e)];
-      b = B[idxB(g, 2, z, y0 + p + 1, e)];
+      const int p = 2 * (line - PV);
+      a = stg[(2 * PV + p) * KXS + e];
+      b = stg[(2 * PV + p + 1) * KXS + e];
     }
-    pack_pair(sm, TL, N, line, e, a, b, sc);
+    pack_pair<T, TL>(sm, N, line, e, a, b, sc);
   }
   GBGHT_SYNC();
-  tile_fft<T, N, TL, NT, +1>(c, sm, tw);
+  tile_fft<T, N, TL, NT, +1, true, X::ACT_V>(c, sm, tw);
   double m = 0.0;
-  for (int i = c.tid; i < 4 * N; i += NT) {
+  const size_t comp = size_t(N) * N * N;
+  for (int i = c.tid; i < PV * N; i += NT) {
     const int x = i % N, p = i / N;
-    const Cplx<T> uxy = sm[x * TL + p];
-    const Cplx<T> uzz = sm[x * TL + 4 + (p >> 1)];
+    const Cplx<T> uxy = sm[tix<TL, true>(x, p)];
+    const Cplx<T> uzz = sm[tix<TL, true>(x, PV + (p >> 1))];
     const T uz = (p & 1) ? uzz.y : uzz.x;
     const size_t base = (size_t(z) * N + (y0 + p)) * N + x;
-    const size_t comp = size_t(N) * N * N;
     u_phys[base] = uxy.x;
     u_phys[comp + base] = uxy.y;
     u_phys[2 * comp + base] = uz;
@@ -238,17 +286,72 @@ GBGHT_HD double body_x_velocity(const Cta& c, Cplx<T>* sm, double* red, const Ge
   return 0.0;
 }
 
+// ================================================================================================
+// z-forward + epilogue + z-inverse helpers
+// ================================================================================================
 
-// Forward z-transform of A slots [c0, c0+3) of one tile into Rt[j][q][l] (retained rows only).
-template <class T, int N, int TL, int NT>
-GBGHT_HD void z_forward3(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, const Geometry& g,
-                         const Cplx<T>* GBGHT_RESTRICT A, int c0, int qy, int kx0,
+// I/O of one z tile (the TL kx columns kx0.. of row ky' = qy, all z): tile loads of A slots into
+// W buffers and tile stores of W buffers into A slots. Device build: TMA with the `az` map (one
+// barrier per buffer, bounded waits); host-check build: plain copies.
+template <class T, int N, int TL>
+struct ZTileIO {
+  const Geometry& g;
+  Cplx<T>* A;
+  int qy, kx0;
+  const void* map;        // the `az` CUtensorMap (device build)
+  uint64_t* bar;          // two shared-memory barriers (device build)
+  uint32_t phase[2];
+  unsigned int* status;
+  static constexpr int BZ = N > 256 ? (N % 256 == 0 ? 256 : N / 2) : N;
+
+  GBGHT_HD void load(const Cta& c, int slot, Cplx<T>* W, int b) {
+#ifdef __CUDA_ARCH__
+    if (c.tid == 0) {
+      mbar_expect_tx(bar + b, uint32_t(N * TL * sizeof(Cplx<T>)));
+      for (int z0 = 0; z0 < N; z0 += BZ)
+        tma_load_3d(W + z0 * TL, static_cast<const CUtensorMap*>(map), 2 * kx0, qy, slot * N + z0, bar + b);
+    }
+#else
+    for (int z = 0; z < N; ++z)
+      for (int l = 0; l < TL; ++l) W[z * TL + l] = A[idxA(g, slot, z, qy, kx0 + l)];
+#endif
+  }
+  GBGHT_HD void wait(const Cta& c, int b) {
+#ifdef __CUDA_ARCH__
+    mbar_wait(bar + b, phase[b], status);
+    phase[b] ^= 1u;
+#endif
+  }
+  GBGHT_HD void store(const Cta& c, int slot, const Cplx<T>* W) {
+#ifdef __CUDA_ARCH__
+    fence_proxy_async();
+    __syncthreads();
+    if (c.tid == 0) {
+      for (int z0 = 0; z0 < N; z0 += BZ)
+        tma_store_3d(static_cast<const CUtensorMap*>(map), 2 * kx0, qy, slot * N + z0, W + z0 * TL);
+      bulk_commit();
+    }
+#else
+    for (int z = 0; z < N; ++z)
+      for (int l = 0; l < TL; ++l) A[idxA(g, slot, z, qy, kx0 + l)] = W[z * TL + l];
+#endif
+  }
+  // wait until every committed store has finished reading shared memory
+  GBGHT_HD void drain(const Cta& c) {
+#ifdef __CUDA_ARCH__
+    if (c.tid == 0) bulk_wait_read();
+    __syncthreads();
+#endif
+  }
+};
+
+// Forward z-transform of A slots [c0, c0+3) of the tile into Rt[j][q][l] (retained rows only).
+template <class T, int N, int TL, int NT, class IO>
+GBGHT_HD void z_forward3(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, const Geometry& g, IO& io, int c0,
                          const Cplx<T>* GBGHT_RESTRICT tw) {
   for (int j = 0; j < 3; ++j) {
-    for (int i = c.tid; i < N * TL; i += NT) {
-      const int z = i / TL, l = i % TL;
-      W[i] = A[idxA(g, c0 + j, z, qy, kx0 + l)];
-    }
+    io.load(c, c0 + j, W, 0);
+    io.wait(c, 0);
     GBGHT_SYNC();
     tile_fft<T, N, TL, NT, -1>(c, W, tw);
     for (int i = c.tid; i < g.NY2 * TL; i += NT) {
@@ -260,24 +363,18 @@ GBGHT_HD void z_forward3(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, const Geometry& 
 }
 
 // Inverse z-transform of one retained column set, value(q, l), into A slot `dst` of the tile.
-template <class T, int N, int TL, int NT, class F>
-GBGHT_HD void z_inverse1(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* GBGHT_RESTRICT A,
-                         int dst, int qy, int kx0, F&& value, const Cplx<T>* GBGHT_RESTRICT tw) {
-  for (int i = c.tid; i < N * TL; i += NT) {
-    const int e = i / TL;
-    if (e > g.K && e < N - g.K) W[i] = czero<T>();
-  }
+template <class T, int N, int TL, int NT, class IO, class F>
+GBGHT_HD void z_inverse1(const Cta& c, Cplx<T>* W, const Geometry& g, IO& io, int dst, F&& value,
+                         const Cplx<T>* GBGHT_RESTRICT tw) {
+  io.drain(c);   // the previous store from W has been read out
+  for (int i = c.tid; i < (N - 2 * g.K - 1) * TL; i += NT) W[(g.K + 1) * TL + i] = czero<T>();
   for (int i = c.tid; i < g.NY2 * TL; i += NT) {
     const int q = i / TL, l = i % TL;
     W[q_to_row(q, g.K, N, g.NY2) * TL + l] = value(q, l);
   }
   GBGHT_SYNC();
   tile_fft<T, N, TL, NT, +1>(c, W, tw);
-  for (int i = c.tid; i < N * TL; i += NT) {
-    const int z = i / TL, l = i % TL;
-    A[idxA(g, dst, z, qy, kx0 + l)] = W[i];
-  }
-  GBGHT_SYNC();
+  io.store(c, dst, W);
 }
 
 // ω̂ component o of iκ × û from the retained velocity columns Rt[0..2].
@@ -317,12 +414,10 @@ struct StageArgs {
   double G[3];          // mean scalar gradient (extension)
 };
 
-template <class T, int N, int TL, int NT>
-GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, const Geometry& g,
-                                Cplx<T>* GBGHT_RESTRICT A, Cplx<T>* GBGHT_RESTRICT S,
-                                Cplx<T>* GBGHT_RESTRICT H, const StageArgs& st,
-                                const double* GBGHT_RESTRICT force_amp,
-                                const Cplx<T>* GBGHT_RESTRICT tw) {
+template <class T, int N, int TL, int NT, class IO>
+GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, const Geometry& g, IO& io,
+                                Cplx<T>* GBGHT_RESTRICT S, Cplx<T>* GBGHT_RESTRICT H, const StageArgs& st,
+                                const double* GBGHT_RESTRICT force_amp, const Cplx<T>* GBGHT_RESTRICT tw) {
   const int kx0 = c.bx * TL, qy = c.by;
   const int NY2 = g.NY2;
   const double s = g.s;
@@ -331,7 +426,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* r
 
   // ---------------- scalar -------------------------------------------------------------------------
   if (st.has_scalar) {
-    z_forward3<T, N, TL, NT>(c, W, Rt, g, A, 3, qy, kx0, tw);
+    z_forward3<T, N, TL, NT>(c, W, Rt, g, io, 3, tw);
     for (int i = c.tid; i < NY2 * TL; i += NT) {
       const int q = i / TL, l = i % TL;
       const int kx = kx0 + l;
@@ -365,11 +460,12 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* r
       Rt[(0 * NY2 + q) * TL + l] = phi;
     }
     GBGHT_SYNC();
-    z_inverse1<T, N, TL, NT>(c, W, g, A, 6, qy, kx0, [&](int q, int l) { return Rt[(0 * NY2 + q) * TL + l]; }, tw);
+    z_inverse1<T, N, TL, NT>(c, W, g, io, 6, [&](int q, int l) { return Rt[(0 * NY2 + q) * TL + l]; }, tw);
+    io.drain(c);
   }
 
   // ---------------- velocity -----------------------------------------------------------------------
-  z_forward3<T, N, TL, NT>(c, W, Rt, g, A, 0, qy, kx0, tw);
+  z_forward3<T, N, TL, NT>(c, W, Rt, g, io, 0, tw);
   const double A_f = st.forced ? force_amp[0] : 0.0;
   double esum = 0.0;
   for (int i = c.tid; i < NY2 * TL; i += NT) {
@@ -442,10 +538,11 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* r
     for (int i = 0; i < NT; ++i) total += red[i];
   // z-inverse of û and of ω̂ = iκ × û
   for (int o = 0; o < 3; ++o)
-    z_inverse1<T, N, TL, NT>(c, W, g, A, o, qy, kx0, [&](int q, int l) { return Rt[(o * NY2 + q) * TL + l]; }, tw);
+    z_inverse1<T, N, TL, NT>(c, W, g, io, o, [&](int q, int l) { return Rt[(o * NY2 + q) * TL + l]; }, tw);
   for (int o = 0; o < 3; ++o)
-    z_inverse1<T, N, TL, NT>(c, W, g, A, 3 + o, qy, kx0,
+    z_inverse1<T, N, TL, NT>(c, W, g, io, 3 + o,
                              [&](int q, int l) { return curl_component<T, TL>(g, Rt, o, q, l, kx0, ky); }, tw);
+  io.drain(c);
   return total;
 }
 
@@ -501,10 +598,9 @@ GBGHT_HD double band_energy_raw(const Geometry& g, const Cplx<T>* S, double lo2,
 // z-inverse of the current state into A slots 0..6 (u, iκ×û, φ), and the tile's Hermitian-weighted
 // Σ|û|², with the same tiling as the epilogue. Used after an import to start a step.
 // ================================================================================================
-template <class T, int N, int TL, int NT>
-GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, const Geometry& g,
-                            Cplx<T>* GBGHT_RESTRICT A, const Cplx<T>* GBGHT_RESTRICT S, int has_scalar,
-                            const Cplx<T>* GBGHT_RESTRICT tw) {
+template <class T, int N, int TL, int NT, class IO>
+GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, const Geometry& g, IO& io,
+                            const Cplx<T>* GBGHT_RESTRICT S, int has_scalar, const Cplx<T>* GBGHT_RESTRICT tw) {
   const int kx0 = c.bx * TL, qy = c.by;
   const int NY2 = g.NY2;
   const double ky = g.s * double(q_to_m(qy, g.K, NY2));
@@ -526,12 +622,13 @@ GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, 
   if (c.tid == 0)
     for (int i = 0; i < NT; ++i) total += red[i];
   for (int o = 0; o < 3; ++o)
-    z_inverse1<T, N, TL, NT>(c, W, g, A, o, qy, kx0, [&](int q, int l) { return Rt[(o * NY2 + q) * TL + l]; }, tw);
+    z_inverse1<T, N, TL, NT>(c, W, g, io, o, [&](int q, int l) { return Rt[(o * NY2 + q) * TL + l]; }, tw);
   for (int o = 0; o < 3; ++o)
-    z_inverse1<T, N, TL, NT>(c, W, g, A, 3 + o, qy, kx0,
+    z_inverse1<T, N, TL, NT>(c, W, g, io, 3 + o,
                              [&](int q, int l) { return curl_component<T, TL>(g, Rt, o, q, l, kx0, ky); }, tw);
   if (has_scalar)
-    z_inverse1<T, N, TL, NT>(c, W, g, A, 6, qy, kx0, [&](int q, int l) { return S[idxS(g, 3, qy, q, kx0 + l)]; }, tw);
+    z_inverse1<T, N, TL, NT>(c, W, g, io, 6, [&](int q, int l) { return S[idxS(g, 3, qy, q, kx0 + l)]; }, tw);
+  io.drain(c);
   return total;
 }
 

@@ -48,6 +48,7 @@ enum gbght_tracer_scheme { GBGHT_HEUN = 0 };
 /* Device status bits (gbght_status_word). */
 #define GBGHT_STATUS_NONFINITE_SPEED 0x1u
 #define GBGHT_STATUS_EMPTY_BAND      0x2u
+#define GBGHT_STATUS_COPY_TIMEOUT    0x4u  /* a bulk copy missed its bounded wait */
 
 typedef struct gbght_config {
   int grid_points_per_axis;  /* N; supported: 8 12 16 24 32 48 64 96 128 192 256 384 512 */
