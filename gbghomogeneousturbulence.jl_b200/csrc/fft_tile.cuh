@@ -8,10 +8,10 @@
 // It then takes an R-point DFT and writes y[(j / NS)·NS·R + j mod NS + r·NS]. Each stage works in
 // place: every thread loads its butterflies, the block synchronises, then every thread stores.
 //
-// Consecutive threads take the same butterfly of consecutive lines (idx = j·TL + l). A quarter
-// warp of 8 threads therefore touches one row of TL elements, for every stage's reads and writes.
+// Consecutive threads take the same butterfly of consecutive lines (idx = j·ACT + l). A quarter
+// warp of 8 threads therefore touches one row of the tile, for every stage's reads and writes.
 // Rows are 128 bytes when TL·sizeof(element) = 128, so the shared-memory accesses are free of bank
-// conflicts whatever the stage's stride.
+// conflicts whatever the stage's stride. The swizzled layout (tix) keeps columns conflict-free too.
 //
 // SIGN = -1 is the forward (unnormalised) transform, SIGN = +1 the inverse (unnormalised).
 // `tw` holds e^(-2πi k/N) for k in [0, N), computed on the host in extended precision.
@@ -121,9 +121,39 @@ GBGHT_HD int tix(int e, int l) {
   }
 }
 
-// ACT ≤ TL lines are transformed; lines ACT..TL−1 are left untouched.
-template <class T, int N, int TL, int NT, int SIGN, bool SWZ = false, int ACT = TL, int S = 0>
-GBGHT_HD void tile_fft(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTRICT tw) {
+// Twiddles w^(jm·r·TWS), r = 1..R−1, from one table read: w₂ = w₁², w₃ = w₂w₁, w₄ = w₂², w₅ = w₄w₁,
+// w₆ = w₄w₂, w₇ = w₄w₃ (at most three products deep, so a few ulp of error).
+template <class T, int R, int SIGN>
+GBGHT_HD void twiddles(const Cplx<T>* GBGHT_RESTRICT tw, int k, Cplx<T>* w) {
+  w[1] = ldgc(tw + k);
+  if constexpr (SIGN > 0) w[1] = conj(w[1]);
+  if constexpr (R > 2) w[2] = w[1] * w[1];
+  if constexpr (R > 3) w[3] = w[2] * w[1];
+  if constexpr (R > 4) {
+    w[4] = w[2] * w[2];
+    w[5] = w[4] * w[1];
+    w[6] = w[4] * w[2];
+    w[7] = w[4] * w[3];
+  }
+}
+
+// The tile buffer as the default source of the first stage and sink of the last one.
+template <class T, int TL, bool SWZ>
+struct TileBuf {
+  static constexpr bool kExternal = false;   // the first stage reads the tile it writes
+  Cplx<T>* buf;
+  GBGHT_HD Cplx<T> load(int e, int l) const { return buf[tix<TL, SWZ>(e, l)]; }
+  GBGHT_HD void store(int e, int l, Cplx<T> v) const { buf[tix<TL, SWZ>(e, l)] = v; }
+};
+
+// ACT ≤ TL lines are transformed; lines ACT..TL−1 are left untouched. The first stage reads its
+// inputs through `src.load(e, l)` (a source with kExternal = true never aliases the tile) and the last stage writes its outputs through
+// `dst.store(e, l, v)`; every other access goes through the tile in shared memory. With the
+// defaults both are the tile itself, and the transform is in place. With an external source the
+// first stage loads straight into registers (from global memory, say), and with an external sink
+// the last stage stores straight out, so neither costs a pass through shared memory.
+template <class T, int N, int TL, int NT, int SIGN, bool SWZ = false, int ACT = TL, int S = 0, class Src, class Dst>
+GBGHT_HD void tile_fft_io(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTRICT tw, const Src& src, const Dst& dst) {
   if constexpr (S < Radices<N>::n) {
     constexpr int R = Radices<N>::r[S];
     constexpr int NS = stage_ns<N>(S);
@@ -131,41 +161,51 @@ GBGHT_HD void tile_fft(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTRICT
     constexpr int TOT = NB * ACT;
     constexpr int BPT = (TOT + NT - 1) / NT;
     constexpr int TWS = N / (NS * R);
+    constexpr bool FIRST = S == 0, LAST = S + 1 == Radices<N>::n;
     Cplx<T> v[BPT][R];
 #pragma unroll
     for (int b = 0; b < BPT; ++b) {
       const int idx = c.tid + b * NT;
       if (BPT * NT == TOT || idx < TOT) {
         const int l = idx % ACT, j = idx / ACT;
-        const int jm = j % NS;
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[b][r] = buf[tix<TL, SWZ>(j + r * NB, l)];
-        if constexpr (NS > 1) {
-#pragma unroll
-          for (int r = 1; r < R; ++r) {
-            Cplx<T> w = ldgc(tw + jm * r * TWS);
-            if constexpr (SIGN > 0) w = conj(w);
-            v[b][r] = v[b][r] * w;
-          }
+        for (int r = 0; r < R; ++r) {
+          if constexpr (FIRST) v[b][r] = src.load(j + r * NB, l);
+          else v[b][r] = buf[tix<TL, SWZ>(j + r * NB, l)];
         }
       }
     }
-    GBGHT_SYNC();
+    if constexpr (!FIRST || !Src::kExternal) GBGHT_SYNC();
 #pragma unroll
     for (int b = 0; b < BPT; ++b) {
       const int idx = c.tid + b * NT;
       if (BPT * NT == TOT || idx < TOT) {
         const int l = idx % ACT, j = idx / ACT;
         const int jm = j % NS;
+        if constexpr (NS > 1) {
+          Cplx<T> w[R];
+          twiddles<T, R, SIGN>(tw, jm * TWS, w);
+#pragma unroll
+          for (int r = 1; r < R; ++r) v[b][r] = v[b][r] * w[r];
+        }
         dft<T, R, SIGN>(v[b]);
         const int base = (j / NS) * NS * R + jm;
 #pragma unroll
-        for (int r = 0; r < R; ++r) buf[tix<TL, SWZ>(base + r * NS, l)] = v[b][r];
+        for (int r = 0; r < R; ++r) {
+          if constexpr (LAST) dst.store(base + r * NS, l, v[b][r]);
+          else buf[tix<TL, SWZ>(base + r * NS, l)] = v[b][r];
+        }
       }
     }
     GBGHT_SYNC();
-    tile_fft<T, N, TL, NT, SIGN, SWZ, ACT, S + 1>(c, buf, tw);
+    tile_fft_io<T, N, TL, NT, SIGN, SWZ, ACT, S + 1>(c, buf, tw, src, dst);
   }
+}
+
+template <class T, int N, int TL, int NT, int SIGN, bool SWZ = false, int ACT = TL>
+GBGHT_HD void tile_fft(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTRICT tw) {
+  const TileBuf<T, TL, SWZ> tb{buf};
+  tile_fft_io<T, N, TL, NT, SIGN, SWZ, ACT>(c, buf, tw, tb, tb);
 }
 
 }  // namespace gbght

@@ -153,84 +153,40 @@ __global__ void __launch_bounds__(NT, 2) k_y_forward(const __grid_constant__ Tma
 }
 
 template <class T, int N, int NT>
-__global__ void __launch_bounds__(NT, 2) k_x_products(Geometry g, Cplx<T>* B, int has_scalar, int KXS,
-                                                      const Cplx<T>* tw, unsigned int* status) {
+__global__ void __launch_bounds__(NT, 2) k_x_products(Geometry g, Cplx<T>* B, int has_scalar, const Cplx<T>* tw) {
   CTA_CTX;
-  using X = XShape<T>;
-  Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
-  Cplx<T>* stg = sm + N * X::TL;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(stg + 7 * X::P * KXS);
-  init_bars(bar, 1);
-  const int y0 = X::P * c.bx, z = c.by;
-  const int nin = has_scalar ? 7 : 6, nout = has_scalar ? 6 : 3;
-  const uint32_t row_bytes = uint32_t(KXS * sizeof(Cplx<T>));
-  if (c.tid == 0) {
-    mbar_expect_tx(bar, row_bytes * nin * X::P);
-    for (int cc = 0; cc < nin; ++cc)
-      for (int p = 0; p < X::P; ++p) bulk_load(stg + (cc * X::P + p) * KXS, B + idxB(g, cc, z, y0 + p, 0), row_bytes, bar);
-  }
-  mbar_wait(bar, 0, status);
-  x_products_compute<T, N, NT>(c, sm, stg, KXS, g, has_scalar, tw);
-  fence_proxy_async();
-  __syncthreads();
-  if (c.tid == 0) {
-    for (int cc = 0; cc < nout; ++cc)
-      for (int p = 0; p < X::P; ++p) bulk_store(B + idxB(g, cc, z, y0 + p, 0), stg + (cc * X::P + p) * KXS, row_bytes);
-    bulk_commit();
-    bulk_wait_read();
-  }
+  body_x_products<T, N, NT>(c, reinterpret_cast<Cplx<T>*>(g_smem), g, B, has_scalar, tw);
 }
 
 template <class T, int N, int NT>
-__global__ void __launch_bounds__(NT, 2) k_x_velocity(Geometry g, const Cplx<T>* B, T* u, int KXS,
-                                                      unsigned long long* maxbits, const Cplx<T>* tw,
-                                                      unsigned int* status) {
+__global__ void __launch_bounds__(NT, 2) k_x_velocity(Geometry g, const Cplx<T>* B, T* u, unsigned long long* maxbits,
+                                                      const Cplx<T>* tw) {
   CTA_CTX;
-  using X = XShape<T>;
   Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
-  Cplx<T>* stg = sm + N * X::TL;
-  double* red = reinterpret_cast<double*>(stg + 3 * X::PV * KXS);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(red + NT);
-  init_bars(bar, 1);
-  const int y0 = X::PV * c.bx, z = c.by;
-  const uint32_t row_bytes = uint32_t(KXS * sizeof(Cplx<T>));
-  if (c.tid == 0) {
-    mbar_expect_tx(bar, row_bytes * 3 * X::PV);
-    for (int cc = 0; cc < 3; ++cc)
-      for (int p = 0; p < X::PV; ++p) bulk_load(stg + (cc * X::PV + p) * KXS, B + idxB(g, cc, z, y0 + p, 0), row_bytes, bar);
-  }
-  mbar_wait(bar, 0, status);
-  const double mx = x_velocity_compute<T, N, NT>(c, sm, stg, KXS, red, g, u, tw);
+  double* red = reinterpret_cast<double*>(sm + N * XShape<T>::TL);
+  const double mx = body_x_velocity<T, N, NT>(c, sm, red, g, B, u, tw);
   if (c.tid == 0) atomicMax(maxbits, static_cast<unsigned long long>(__double_as_longlong(mx)));
 }
 
 template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT, 2) k_z_epilogue(const __grid_constant__ TmaMaps m, Geometry g, Cplx<T>* A,
-                                                      Cplx<T>* S, Cplx<T>* H, StageArgs st, const double* amp,
-                                                      double* partial, const Cplx<T>* tw, unsigned int* status) {
+__global__ void __launch_bounds__(NT, 2) k_z_epilogue(Geometry g, Cplx<T>* A, Cplx<T>* S, Cplx<T>* H, StageArgs st,
+                                                      const double* amp, double* partial, const Cplx<T>* tw) {
   CTA_CTX;
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
   Cplx<T>* Rt = W + N * TL;
   double* red = reinterpret_cast<double*>(Rt + 3 * g.NY2 * TL);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(red + NT);
-  init_bars(bar, 2);
-  ZTileIO<T, N, TL> io{g, A, c.by, c.bx * TL, &m.az, bar, {0u, 0u}, status};
-  const double e = body_z_epilogue<T, N, TL, NT>(c, W, Rt, red, g, io, S, H, st, amp, tw);
+  const double e = body_z_epilogue<T, N, TL, NT>(c, W, Rt, red, g, A, S, H, st, amp, tw);
   if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
 }
 
 template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT, 2) k_z_init(const __grid_constant__ TmaMaps m, Geometry g, Cplx<T>* A,
-                                                  const Cplx<T>* S, int has_scalar, double* partial, const Cplx<T>* tw,
-                                                  unsigned int* status) {
+__global__ void __launch_bounds__(NT, 2) k_z_init(Geometry g, Cplx<T>* A, const Cplx<T>* S, int has_scalar, double* partial,
+                                                  const Cplx<T>* tw) {
   CTA_CTX;
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
   Cplx<T>* Rt = W + N * TL;
   double* red = reinterpret_cast<double*>(Rt + 3 * g.NY2 * TL);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(red + NT);
-  init_bars(bar, 2);
-  ZTileIO<T, N, TL> io{g, A, c.by, c.bx * TL, &m.az, bar, {0u, 0u}, status};
-  const double e = body_z_init<T, N, TL, NT>(c, W, Rt, red, g, io, S, has_scalar, tw);
+  const double e = body_z_init<T, N, TL, NT>(c, W, Rt, red, g, A, S, has_scalar, tw);
   if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
 }
 template <class T>
@@ -725,17 +681,11 @@ class EngineImpl final : public Engine {
   }
 
   static constexpr size_t kBarBytes = 32;
-  int kxs() const { return x_kxs(g_.K, int(sizeof(Cplx<T>))); }
   size_t smem_y() const { return size_t(N) * TLY * sizeof(Cplx<T>) + kBarBytes; }
-  size_t smem_x() const {
-    return size_t(N) * XShape<T>::TL * sizeof(Cplx<T>) + size_t(7) * XShape<T>::P * kxs() * sizeof(Cplx<T>) + kBarBytes;
-  }
-  size_t smem_xv() const {
-    return size_t(N) * XShape<T>::TL * sizeof(Cplx<T>) + size_t(3) * XShape<T>::PV * kxs() * sizeof(Cplx<T>) +
-           size_t(NTX) * sizeof(double) + kBarBytes;
-  }
+  size_t smem_x() const { return size_t(N) * XShape<T>::TL * sizeof(Cplx<T>); }
+  size_t smem_xv() const { return size_t(N) * XShape<T>::TL * sizeof(Cplx<T>) + size_t(NTX) * sizeof(double); }
   size_t smem_z() const {
-    return (size_t(N) * TLZ + 3 * size_t(g_.NY2) * TLZ) * sizeof(Cplx<T>) + size_t(NTZ) * sizeof(double) + kBarBytes;
+    return (size_t(N) * TLZ + 3 * size_t(g_.NY2) * TLZ) * sizeof(Cplx<T>) + size_t(NTZ) * sizeof(double);
   }
 
 #ifndef GBGHT_EMU
@@ -828,40 +778,31 @@ class EngineImpl final : public Engine {
   }
   void x_products() {
     using X = XShape<T>;
-    const int KXS = kxs();
 #ifdef GBGHT_EMU
     emu_grid(N / X::P, N, 1, smem_x(), [&](const Cta& c, void* sm) {
-      Cplx<T>* t = static_cast<Cplx<T>*>(sm);
-      Cplx<T>* stg = t + N * X::TL;
-      x_stage_in_host<T, X::P>(c, stg, KXS, g_, B_, p_.scalar ? 7 : 6);
-      x_products_compute<T, N, 1>(c, t, stg, KXS, g_, p_.scalar, tw_);
-      x_stage_out_host<T, X::P>(c, stg, KXS, g_, B_, p_.scalar ? 6 : 3);
+      body_x_products<T, N, 1>(c, static_cast<Cplx<T>*>(sm), g_, B_, p_.scalar, tw_);
     });
 #else
     pbegin(PROF_X_PRODUCTS);
-    k_x_products<T, N, NTX><<<dim3(N / X::P, N, 1), NTX, smem_x(), stream_>>>(g_, B_, p_.scalar, KXS, tw_, status_);
+    k_x_products<T, N, NTX><<<dim3(N / X::P, N, 1), NTX, smem_x(), stream_>>>(g_, B_, p_.scalar, tw_);
     pend();
 #endif
   }
   void x_velocity() {
     using X = XShape<T>;
-    const int KXS = kxs();
 #ifdef GBGHT_EMU
     unsigned long long* mb = maxbits_;
     emu_grid(N / X::PV, N, 1, smem_xv(), [&](const Cta& c, void* sm) {
       Cplx<T>* t = static_cast<Cplx<T>*>(sm);
-      Cplx<T>* stg = t + N * X::TL;
-      double* red = reinterpret_cast<double*>(stg + 3 * X::PV * KXS);
-      x_stage_in_host<T, X::PV>(c, stg, KXS, g_, B_, 3);
-      const double m = x_velocity_compute<T, N, 1>(c, t, stg, KXS, red, g_, U_, tw_);
+      double* red = reinterpret_cast<double*>(t + N * X::TL);
+      const double m = body_x_velocity<T, N, 1>(c, t, red, g_, B_, U_, tw_);
       unsigned long long bits;
       std::memcpy(&bits, &m, sizeof bits);
       if (bits > *mb) *mb = bits;
     });
 #else
     pbegin(PROF_X_VELOCITY);
-    k_x_velocity<T, N, NTX><<<dim3(N / X::PV, N, 1), NTX, smem_xv(), stream_>>>(g_, B_, U_, KXS, maxbits_, tw_,
-                                                                                 status_);
+    k_x_velocity<T, N, NTX><<<dim3(N / X::PV, N, 1), NTX, smem_xv(), stream_>>>(g_, B_, U_, maxbits_, tw_);
     pend();
 #endif
   }
@@ -872,13 +813,12 @@ class EngineImpl final : public Engine {
       Cplx<T>* W = static_cast<Cplx<T>*>(sm);
       Cplx<T>* Rt = W + N * TLZ;
       double* red = reinterpret_cast<double*>(Rt + 3 * g_.NY2 * TLZ);
-      ZTileIO<T, N, TLZ> io{g_, A_, c.by, c.bx * TLZ, nullptr, nullptr, {0u, 0u}, nullptr};
-      partial_[c.by * gx + c.bx] = body_z_epilogue<T, N, TLZ, 1>(c, W, Rt, red, g_, io, S_, H_, st, amp_, tw_);
+      partial_[c.by * gx + c.bx] = body_z_epilogue<T, N, TLZ, 1>(c, W, Rt, red, g_, A_, S_, H_, st, amp_, tw_);
     });
 #else
     pbegin(PROF_Z_EPILOGUE);
-    k_z_epilogue<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(
-        maps_, g_, A_, S_, H_, st, amp_, partial_, tw_, status_);
+    k_z_epilogue<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, S_, H_, st, amp_,
+                                                                                           partial_, tw_);
     pend();
 #endif
   }
@@ -889,12 +829,11 @@ class EngineImpl final : public Engine {
       Cplx<T>* W = static_cast<Cplx<T>*>(sm);
       Cplx<T>* Rt = W + N * TLZ;
       double* red = reinterpret_cast<double*>(Rt + 3 * g_.NY2 * TLZ);
-      ZTileIO<T, N, TLZ> io{g_, A_, c.by, c.bx * TLZ, nullptr, nullptr, {0u, 0u}, nullptr};
-      partial_[c.by * gx + c.bx] = body_z_init<T, N, TLZ, 1>(c, W, Rt, red, g_, io, S_, p_.scalar, tw_);
+      partial_[c.by * gx + c.bx] = body_z_init<T, N, TLZ, 1>(c, W, Rt, red, g_, A_, S_, p_.scalar, tw_);
     });
 #else
-    k_z_init<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(maps_, g_, A_, S_, p_.scalar,
-                                                                                       partial_, tw_, status_);
+    k_z_init<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, S_, p_.scalar, partial_,
+                                                                                       tw_);
 #endif
     return rt_check();
   }

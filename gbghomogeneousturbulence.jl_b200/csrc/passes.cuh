@@ -155,52 +155,55 @@ GBGHT_HD int x_kxs(int K, int elem_bytes) {
   return ((K + 1 + per - 1) / per) * per;
 }
 
-// staging ← B rows (comps [0, nc) of points y0..y0+P−1)
-template <class T, int P>
-GBGHT_HD void x_stage_in_host(const Cta& c, Cplx<T>* stg, int KXS, const Geometry& g, const Cplx<T>* B, int nc) {
-  const int y0 = P * c.bx, z = c.by;
-  for (int cc = 0; cc < nc; ++cc)
-    for (int p = 0; p < P; ++p)
-      for (int e = 0; e < KXS; ++e) stg[(cc * P + p) * KXS + e] = B[idxB(g, cc, z, y0 + p, e)];
-}
-template <class T, int P>
-GBGHT_HD void x_stage_out_host(const Cta& c, const Cplx<T>* stg, int KXS, const Geometry& g, Cplx<T>* B, int nc) {
-  const int y0 = P * c.bx, z = c.by;
-  for (int cc = 0; cc < nc; ++cc)
-    for (int p = 0; p < P; ++p)
-      for (int e = 0; e < KXS; ++e) B[idxB(g, cc, z, y0 + p, e)] = stg[(cc * P + p) * KXS + e];
-}
+// Source of the x-pass inverse's first stage: row e of line l, packed two-for-one straight from B
+// (a c2r input: only the real part of the kx = 0 bin, rows K < e < N−K zero), scaled by 1/N³.
+// Lines 3p..3p+2 pair comps (0,1), (2,3), (4,5) of point p; line 3P + h pairs φ of points 2h, 2h+1.
+template <class T, int N, int P>
+struct XPackedSource {
+  static constexpr bool kExternal = true;
+  const Geometry& g;
+  const Cplx<T>* B;
+  int z, y0, has_scalar;
+  T sc;
+  GBGHT_HD Cplx<T> load(int e, int l) const {
+    const int K = g.K;
+    if (e > K && e < N - K) return czero<T>();
+    int ca, cb, ya, yb;
+    if (l < 3 * P) {
+      const int p = l / 3, pr = l % 3;
+      ca = 2 * pr;
+      cb = 2 * pr + 1;
+      ya = yb = y0 + p;
+    } else {
+      if (!has_scalar) return czero<T>();
+      const int h = l - 3 * P;
+      ca = cb = 6;
+      ya = y0 + 2 * h;
+      yb = ya + 1;
+    }
+    if (e == 0) {
+      const Cplx<T> a = B[idxB(g, ca, z, ya, 0)], b = B[idxB(g, cb, z, yb, 0)];
+      return cmk<T>(a.x * sc, b.x * sc);
+    }
+    if (e <= K) {
+      const Cplx<T> a = B[idxB(g, ca, z, ya, e)], b = B[idxB(g, cb, z, yb, e)];
+      return cmk<T>((a.x - b.y) * sc, (a.y + b.x) * sc);
+    }
+    const Cplx<T> a = B[idxB(g, ca, z, ya, N - e)], b = B[idxB(g, cb, z, yb, N - e)];
+    return cmk<T>((a.x + b.y) * sc, (b.x - a.y) * sc);
+  }
+};
 
-// pack, inverse, products, forward, unpack: staging (7 comps in) → staging (6 comps out)
+// inverse (from B), products, forward, unpack (to B): one tile of P points per CTA
 template <class T, int N, int NT>
-GBGHT_HD void x_products_compute(const Cta& c, Cplx<T>* sm, Cplx<T>* stg, int KXS, const Geometry& g,
-                                 int has_scalar, const Cplx<T>* GBGHT_RESTRICT tw) {
+GBGHT_HD void body_x_products(const Cta& c, Cplx<T>* sm, const Geometry& g, Cplx<T>* GBGHT_RESTRICT B,
+                              int has_scalar, const Cplx<T>* GBGHT_RESTRICT tw) {
   using X = XShape<T>;
   constexpr int TL = X::TL, P = X::P;
-  const T sc = T(g.inv_norm);
+  const int y0 = P * c.bx, z = c.by;
   const int KX1 = g.K + 1;
-  // rows that no mode reaches (K < e < N−K), in every line the inverse uses
-  for (int i = c.tid; i < (N - 2 * g.K - 1) * TL; i += NT) sm[(g.K + 1) * TL + i] = czero<T>();
-  // velocity and vorticity pairs: line 3p+pr holds comps (2pr, 2pr+1) of point p
-  for (int i = c.tid; i < 3 * P * KX1; i += NT) {
-    const int e = i % KX1, line = i / KX1;
-    const int p = line / 3, pr = line % 3;
-    const Cplx<T> a = stg[((2 * pr) * P + p) * KXS + e];
-    const Cplx<T> b = stg[((2 * pr + 1) * P + p) * KXS + e];
-    pack_pair<T, TL>(sm, N, line, e, a, b, sc);
-  }
-  // scalar pairs: line 3P + h holds φ of points 2h and 2h+1
-  for (int i = c.tid; i < (P / 2) * KX1; i += NT) {
-    const int e = i % KX1, h = i / KX1;
-    Cplx<T> a = czero<T>(), b = czero<T>();
-    if (has_scalar) {
-      a = stg[(6 * P + 2 * h) * KXS + e];
-      b = stg[(6 * P + 2 * h + 1) * KXS + e];
-    }
-    pack_pair<T, TL>(sm, N, 3 * P + h, e, a, b, sc);
-  }
-  GBGHT_SYNC();
-  tile_fft<T, N, TL, NT, +1, true, X::ACT_INV>(c, sm, tw);
+  const XPackedSource<T, N, P> src{g, B, z, y0, has_scalar, T(g.inv_norm)};
+  tile_fft_io<T, N, TL, NT, +1, true, X::ACT_INV>(c, sm, tw, src, TileBuf<T, TL, true>{sm});
   for (int x = c.tid; x < N; x += NT) {
 #pragma unroll
     for (int h = 0; h < P / 2; ++h) {
@@ -221,47 +224,68 @@ GBGHT_HD void x_products_compute(const Cta& c, Cplx<T>* sm, Cplx<T>* stg, int KX
   }
   GBGHT_SYNC();
   tile_fft<T, N, TL, NT, -1, true, X::ACT_FWD>(c, sm, tw);
-  // unpack into the staging rows of the six products; the columns past K get zeros
-  for (int i = c.tid; i < 3 * P * KXS; i += NT) {
-    const int k = i % KXS, line = i / KXS;
+  // unpack the six products of each point into B slots 0..5 (0..2 without a scalar); columns
+  // past K get zeros
+  const int nline = has_scalar ? 3 * P : P * 3;
+  for (int i = c.tid; i < nline * g.KXP; i += NT) {
+    const int k = i % g.KXP, line = i / g.KXP;
     const int p = line / 3, pr = line % 3;
+    if (!has_scalar && pr > 0 && 2 * pr >= 3) {
+    }
     Cplx<T> a = czero<T>(), b = czero<T>();
     if (k < KX1) unpack_pair<T, TL>(sm, N, line, k, a, b);
-    stg[((2 * pr) * P + p) * KXS + k] = a;
-    stg[((2 * pr + 1) * P + p) * KXS + k] = b;
+    const int ca = 2 * pr, cb = 2 * pr + 1;
+    const int nout = has_scalar ? 6 : 3;
+    if (ca < nout) B[idxB(g, ca, z, y0 + p, k)] = a;
+    if (cb < nout) B[idxB(g, cb, z, y0 + p, k)] = b;
   }
 }
 
-// ================================================================================================
-// x-pass of the deposit: the velocity to physical for PV = TL/2 points (z, y0..y0+PV−1), written
-// out, and the maximum of |u|² reduced. Grid: (N/PV, N).
-//   line p (p < PV) = u_x + i·u_y of point p; line PV + h = u_z(2h) + i·u_z(2h+1)
-// `red` is NT doubles of shared scratch; the CTA's maximum of |u|² is returned to thread 0.
-// ================================================================================================
+// Source of the deposit's inverse: line p (p < PV) = u_x + i·u_y of point p; line PV + h =
+// u_z(2h) + i·u_z(2h+1).
+template <class T, int N, int PV>
+struct XVelocitySource {
+  static constexpr bool kExternal = true;
+  const Geometry& g;
+  const Cplx<T>* B;
+  int z, y0;
+  T sc;
+  GBGHT_HD Cplx<T> load(int e, int l) const {
+    const int K = g.K;
+    if (e > K && e < N - K) return czero<T>();
+    int ca, cb, ya, yb;
+    if (l < PV) {
+      ca = 0;
+      cb = 1;
+      ya = yb = y0 + l;
+    } else {
+      ca = cb = 2;
+      ya = y0 + 2 * (l - PV);
+      yb = ya + 1;
+    }
+    if (e == 0) {
+      const Cplx<T> a = B[idxB(g, ca, z, ya, 0)], b = B[idxB(g, cb, z, yb, 0)];
+      return cmk<T>(a.x * sc, b.x * sc);
+    }
+    if (e <= K) {
+      const Cplx<T> a = B[idxB(g, ca, z, ya, e)], b = B[idxB(g, cb, z, yb, e)];
+      return cmk<T>((a.x - b.y) * sc, (a.y + b.x) * sc);
+    }
+    const Cplx<T> a = B[idxB(g, ca, z, ya, N - e)], b = B[idxB(g, cb, z, yb, N - e)];
+    return cmk<T>((a.x + b.y) * sc, (b.x - a.y) * sc);
+  }
+};
+
+// The deposit's x-pass: physical velocity of PV points written out, max |u|² returned to thread 0.
 template <class T, int N, int NT>
-GBGHT_HD double x_velocity_compute(const Cta& c, Cplx<T>* sm, Cplx<T>* stg, int KXS, double* red, const Geometry& g,
-                                   T* GBGHT_RESTRICT u_phys, const Cplx<T>* GBGHT_RESTRICT tw) {
+GBGHT_HD double body_x_velocity(const Cta& c, Cplx<T>* sm, double* red, const Geometry& g,
+                                const Cplx<T>* GBGHT_RESTRICT B, T* GBGHT_RESTRICT u_phys,
+                                const Cplx<T>* GBGHT_RESTRICT tw) {
   using X = XShape<T>;
   constexpr int TL = X::TL, PV = X::PV;
   const int y0 = PV * c.bx, z = c.by;
-  const T sc = T(g.inv_norm);
-  const int KX1 = g.K + 1;
-  for (int i = c.tid; i < (N - 2 * g.K - 1) * TL; i += NT) sm[(g.K + 1) * TL + i] = czero<T>();
-  for (int i = c.tid; i < X::ACT_V * KX1; i += NT) {
-    const int e = i % KX1, line = i / KX1;
-    Cplx<T> a, b;
-    if (line < PV) {
-      a = stg[(0 * PV + line) * KXS + e];
-      b = stg[(1 * PV + line) * KXS + e];
-    } else {
-      const int p = 2 * (line - PV);
-      a = stg[(2 * PV + p) * KXS + e];
-      b = stg[(2 * PV + p + 1) * KXS + e];
-    }
-    pack_pair<T, TL>(sm, N, line, e, a, b, sc);
-  }
-  GBGHT_SYNC();
-  tile_fft<T, N, TL, NT, +1, true, X::ACT_V>(c, sm, tw);
+  const XVelocitySource<T, N, PV> src{g, B, z, y0, T(g.inv_norm)};
+  tile_fft_io<T, N, TL, NT, +1, true, X::ACT_V>(c, sm, tw, src, TileBuf<T, TL, true>{sm});
   double m = 0.0;
   const size_t comp = size_t(N) * N * N;
   for (int i = c.tid; i < PV * N; i += NT) {
@@ -290,91 +314,65 @@ GBGHT_HD double x_velocity_compute(const Cta& c, Cplx<T>* sm, Cplx<T>* stg, int 
 // z-forward + epilogue + z-inverse helpers
 // ================================================================================================
 
-// I/O of one z tile (the TL kx columns kx0.. of row ky' = qy, all z): tile loads of A slots into
-// W buffers and tile stores of W buffers into A slots. Device build: TMA with the `az` map (one
-// barrier per buffer, bounded waits); host-check build: plain copies.
+// Register-direct I/O of one z tile (the TL kx columns kx0.. of row ky' = qy, all z).
+// Forward: the first stage reads A slot `slot` rows z straight from global memory, and the last
+// stage keeps only the retained rows, written compactly into Rt[j] (rows q).
 template <class T, int N, int TL>
-struct ZTileIO {
+struct ZGlobalSource {
+  static constexpr bool kExternal = true;
+  const Geometry& g;
+  const Cplx<T>* A;
+  int slot, qy, kx0;
+  GBGHT_HD Cplx<T> load(int e, int l) const { return A[idxA(g, slot, e, qy, kx0 + l)]; }
+};
+template <class T, int N, int TL>
+struct ZRetainedSink {
+  const Geometry& g;
+  Cplx<T>* Rj;   // Rt + j·NY2·TL
+  GBGHT_HD void store(int e, int l, Cplx<T> v) const {
+    if (e <= g.K) Rj[e * TL + l] = v;
+    else if (e >= N - g.K) Rj[(e - N + g.NY2) * TL + l] = v;
+  }
+};
+// Inverse: the first stage reads value(q, l) for retained rows and zero elsewhere; the last stage
+// writes A slot `slot` rows z straight to global memory.
+template <class T, int N, int TL, class F>
+struct ZValueSource {
+  static constexpr bool kExternal = true;
+  const Geometry& g;
+  const F& value;
+  GBGHT_HD Cplx<T> load(int e, int l) const {
+    if (e <= g.K) return value(e, l);
+    if (e >= N - g.K) return value(e - N + g.NY2, l);
+    return czero<T>();
+  }
+};
+template <class T, int N, int TL>
+struct ZGlobalSink {
   const Geometry& g;
   Cplx<T>* A;
-  int qy, kx0;
-  const void* map;        // the `az` CUtensorMap (device build)
-  uint64_t* bar;          // two shared-memory barriers (device build)
-  uint32_t phase[2];
-  unsigned int* status;
-  static constexpr int BZ = N > 256 ? (N % 256 == 0 ? 256 : N / 2) : N;
-
-  GBGHT_HD void load(const Cta& c, int slot, Cplx<T>* W, int b) {
-#ifdef __CUDA_ARCH__
-    if (c.tid == 0) {
-      mbar_expect_tx(bar + b, uint32_t(N * TL * sizeof(Cplx<T>)));
-      for (int z0 = 0; z0 < N; z0 += BZ)
-        tma_load_3d(W + z0 * TL, static_cast<const CUtensorMap*>(map), 2 * kx0, qy, slot * N + z0, bar + b);
-    }
-#else
-    for (int z = 0; z < N; ++z)
-      for (int l = 0; l < TL; ++l) W[z * TL + l] = A[idxA(g, slot, z, qy, kx0 + l)];
-#endif
-  }
-  GBGHT_HD void wait(const Cta& c, int b) {
-#ifdef __CUDA_ARCH__
-    mbar_wait(bar + b, phase[b], status);
-    phase[b] ^= 1u;
-#endif
-  }
-  GBGHT_HD void store(const Cta& c, int slot, const Cplx<T>* W) {
-#ifdef __CUDA_ARCH__
-    fence_proxy_async();
-    __syncthreads();
-    if (c.tid == 0) {
-      for (int z0 = 0; z0 < N; z0 += BZ)
-        tma_store_3d(static_cast<const CUtensorMap*>(map), 2 * kx0, qy, slot * N + z0, W + z0 * TL);
-      bulk_commit();
-    }
-#else
-    for (int z = 0; z < N; ++z)
-      for (int l = 0; l < TL; ++l) A[idxA(g, slot, z, qy, kx0 + l)] = W[z * TL + l];
-#endif
-  }
-  // wait until every committed store has finished reading shared memory
-  GBGHT_HD void drain(const Cta& c) {
-#ifdef __CUDA_ARCH__
-    if (c.tid == 0) bulk_wait_read();
-    __syncthreads();
-#endif
-  }
+  int slot, qy, kx0;
+  GBGHT_HD void store(int e, int l, Cplx<T> v) const { A[idxA(g, slot, e, qy, kx0 + l)] = v; }
 };
 
 // Forward z-transform of A slots [c0, c0+3) of the tile into Rt[j][q][l] (retained rows only).
-template <class T, int N, int TL, int NT, class IO>
-GBGHT_HD void z_forward3(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, const Geometry& g, IO& io, int c0,
-                         const Cplx<T>* GBGHT_RESTRICT tw) {
+template <class T, int N, int TL, int NT>
+GBGHT_HD void z_forward3(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, const Geometry& g, const Cplx<T>* A, int c0,
+                         int qy, int kx0, const Cplx<T>* GBGHT_RESTRICT tw) {
   for (int j = 0; j < 3; ++j) {
-    io.load(c, c0 + j, W, 0);
-    io.wait(c, 0);
-    GBGHT_SYNC();
-    tile_fft<T, N, TL, NT, -1>(c, W, tw);
-    for (int i = c.tid; i < g.NY2 * TL; i += NT) {
-      const int q = i / TL, l = i % TL;
-      Rt[(j * g.NY2 + q) * TL + l] = W[q_to_row(q, g.K, N, g.NY2) * TL + l];
-    }
-    GBGHT_SYNC();
+    const ZGlobalSource<T, N, TL> src{g, A, c0 + j, qy, kx0};
+    const ZRetainedSink<T, N, TL> dst{g, Rt + j * g.NY2 * TL};
+    tile_fft_io<T, N, TL, NT, -1>(c, W, tw, src, dst);
   }
 }
 
-// Inverse z-transform of one retained column set, value(q, l), into A slot `dst` of the tile.
-template <class T, int N, int TL, int NT, class IO, class F>
-GBGHT_HD void z_inverse1(const Cta& c, Cplx<T>* W, const Geometry& g, IO& io, int dst, F&& value,
-                         const Cplx<T>* GBGHT_RESTRICT tw) {
-  io.drain(c);   // the previous store from W has been read out
-  for (int i = c.tid; i < (N - 2 * g.K - 1) * TL; i += NT) W[(g.K + 1) * TL + i] = czero<T>();
-  for (int i = c.tid; i < g.NY2 * TL; i += NT) {
-    const int q = i / TL, l = i % TL;
-    W[q_to_row(q, g.K, N, g.NY2) * TL + l] = value(q, l);
-  }
-  GBGHT_SYNC();
-  tile_fft<T, N, TL, NT, +1>(c, W, tw);
-  io.store(c, dst, W);
+// Inverse z-transform of one retained column set, value(q, l), into A slot `slot` of the tile.
+template <class T, int N, int TL, int NT, class F>
+GBGHT_HD void z_inverse1(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* A, int slot, int qy, int kx0,
+                         const F& value, const Cplx<T>* GBGHT_RESTRICT tw) {
+  const ZValueSource<T, N, TL, F> src{g, value};
+  const ZGlobalSink<T, N, TL> dst{g, A, slot, qy, kx0};
+  tile_fft_io<T, N, TL, NT, +1>(c, W, tw, src, dst);
 }
 
 // ω̂ component o of iκ × û from the retained velocity columns Rt[0..2].
@@ -414,9 +412,9 @@ struct StageArgs {
   double G[3];          // mean scalar gradient (extension)
 };
 
-template <class T, int N, int TL, int NT, class IO>
-GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, const Geometry& g, IO& io,
-                                Cplx<T>* GBGHT_RESTRICT S, Cplx<T>* GBGHT_RESTRICT H, const StageArgs& st,
+template <class T, int N, int TL, int NT>
+GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, const Geometry& g,
+                                Cplx<T>* GBGHT_RESTRICT A, Cplx<T>* GBGHT_RESTRICT S, Cplx<T>* GBGHT_RESTRICT H, const StageArgs& st,
                                 const double* GBGHT_RESTRICT force_amp, const Cplx<T>* GBGHT_RESTRICT tw) {
   const int kx0 = c.bx * TL, qy = c.by;
   const int NY2 = g.NY2;
@@ -426,7 +424,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* r
 
   // ---------------- scalar -------------------------------------------------------------------------
   if (st.has_scalar) {
-    z_forward3<T, N, TL, NT>(c, W, Rt, g, io, 3, tw);
+    z_forward3<T, N, TL, NT>(c, W, Rt, g, A, 3, qy, kx0, tw);
     for (int i = c.tid; i < NY2 * TL; i += NT) {
       const int q = i / TL, l = i % TL;
       const int kx = kx0 + l;
@@ -460,12 +458,12 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* r
       Rt[(0 * NY2 + q) * TL + l] = phi;
     }
     GBGHT_SYNC();
-    z_inverse1<T, N, TL, NT>(c, W, g, io, 6, [&](int q, int l) { return Rt[(0 * NY2 + q) * TL + l]; }, tw);
-    io.drain(c);
+    const auto phi_new = [&](int q, int l) { return Rt[(0 * NY2 + q) * TL + l]; };
+    z_inverse1<T, N, TL, NT>(c, W, g, A, 6, qy, kx0, phi_new, tw);
   }
 
   // ---------------- velocity -----------------------------------------------------------------------
-  z_forward3<T, N, TL, NT>(c, W, Rt, g, io, 0, tw);
+  z_forward3<T, N, TL, NT>(c, W, Rt, g, A, 0, qy, kx0, tw);
   const double A_f = st.forced ? force_amp[0] : 0.0;
   double esum = 0.0;
   for (int i = c.tid; i < NY2 * TL; i += NT) {
@@ -537,12 +535,14 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* r
   if (c.tid == 0)
     for (int i = 0; i < NT; ++i) total += red[i];
   // z-inverse of û and of ω̂ = iκ × û
-  for (int o = 0; o < 3; ++o)
-    z_inverse1<T, N, TL, NT>(c, W, g, io, o, [&](int q, int l) { return Rt[(o * NY2 + q) * TL + l]; }, tw);
-  for (int o = 0; o < 3; ++o)
-    z_inverse1<T, N, TL, NT>(c, W, g, io, 3 + o,
-                             [&](int q, int l) { return curl_component<T, TL>(g, Rt, o, q, l, kx0, ky); }, tw);
-  io.drain(c);
+  for (int o = 0; o < 3; ++o) {
+    const auto u_new = [&](int q, int l) { return Rt[(o * NY2 + q) * TL + l]; };
+    z_inverse1<T, N, TL, NT>(c, W, g, A, o, qy, kx0, u_new, tw);
+  }
+  for (int o = 0; o < 3; ++o) {
+    const auto w_new = [&](int q, int l) { return curl_component<T, TL>(g, Rt, o, q, l, kx0, ky); };
+    z_inverse1<T, N, TL, NT>(c, W, g, A, 3 + o, qy, kx0, w_new, tw);
+  }
   return total;
 }
 
@@ -598,9 +598,9 @@ GBGHT_HD double band_energy_raw(const Geometry& g, const Cplx<T>* S, double lo2,
 // z-inverse of the current state into A slots 0..6 (u, iκ×û, φ), and the tile's Hermitian-weighted
 // Σ|û|², with the same tiling as the epilogue. Used after an import to start a step.
 // ================================================================================================
-template <class T, int N, int TL, int NT, class IO>
-GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, const Geometry& g, IO& io,
-                            const Cplx<T>* GBGHT_RESTRICT S, int has_scalar, const Cplx<T>* GBGHT_RESTRICT tw) {
+template <class T, int N, int TL, int NT>
+GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, const Geometry& g,
+                            Cplx<T>* GBGHT_RESTRICT A, const Cplx<T>* GBGHT_RESTRICT S, int has_scalar, const Cplx<T>* GBGHT_RESTRICT tw) {
   const int kx0 = c.bx * TL, qy = c.by;
   const int NY2 = g.NY2;
   const double ky = g.s * double(q_to_m(qy, g.K, NY2));
@@ -621,14 +621,18 @@ GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, 
   double total = 0.0;
   if (c.tid == 0)
     for (int i = 0; i < NT; ++i) total += red[i];
-  for (int o = 0; o < 3; ++o)
-    z_inverse1<T, N, TL, NT>(c, W, g, io, o, [&](int q, int l) { return Rt[(o * NY2 + q) * TL + l]; }, tw);
-  for (int o = 0; o < 3; ++o)
-    z_inverse1<T, N, TL, NT>(c, W, g, io, 3 + o,
-                             [&](int q, int l) { return curl_component<T, TL>(g, Rt, o, q, l, kx0, ky); }, tw);
-  if (has_scalar)
-    z_inverse1<T, N, TL, NT>(c, W, g, io, 6, [&](int q, int l) { return S[idxS(g, 3, qy, q, kx0 + l)]; }, tw);
-  io.drain(c);
+  for (int o = 0; o < 3; ++o) {
+    const auto u_new = [&](int q, int l) { return Rt[(o * NY2 + q) * TL + l]; };
+    z_inverse1<T, N, TL, NT>(c, W, g, A, o, qy, kx0, u_new, tw);
+  }
+  for (int o = 0; o < 3; ++o) {
+    const auto w_new = [&](int q, int l) { return curl_component<T, TL>(g, Rt, o, q, l, kx0, ky); };
+    z_inverse1<T, N, TL, NT>(c, W, g, A, 3 + o, qy, kx0, w_new, tw);
+  }
+  if (has_scalar) {
+    const auto phi = [&](int q, int l) { return S[idxS(g, 3, qy, q, kx0 + l)]; };
+    z_inverse1<T, N, TL, NT>(c, W, g, A, 6, qy, kx0, phi, tw);
+  }
   return total;
 }
 
