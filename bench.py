@@ -297,7 +297,7 @@ def ours(args):
         run.close()
         del run
     # end-to-end through the public API (host buffers), the headline form
-    e2e_val, h2d, d2h = e2e_run(args, forms[0], device, inputs, args.steps)
+    e2e_val, h2d, d2h = (float("nan"), 0, 0) if args.no_e2e else e2e_run(args, forms[0], device, inputs, args.steps)
     if ws > 1:
         import torch.distributed as dist
         t = torch.tensor([1.0 / e2e_val], dtype=torch.float64, device=f"cuda:{device}")
@@ -382,6 +382,7 @@ def main():
     ap.add_argument("--tracers", type=int, default=WORKLOAD["tracers"])
     ap.add_argument("--form", default="both", choices=["both", "fp64", "fp32_mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (quick kernel timing)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -8,8 +8,9 @@
 // It then takes an R-point DFT and writes y[(j / NS)·NS·R + j mod NS + r·NS]. Each stage works in
 // place: every thread loads its butterflies, the block synchronises, then every thread stores.
 //
-// Consecutive threads take the same butterfly of consecutive lines (idx = j·ACT + l). A quarter
-// warp of 8 threads therefore touches one row of the tile, for every stage's reads and writes.
+// Consecutive threads take the same butterfly of consecutive lines (idx = j·TL + l; the threads of
+// lines at or past ACT stay idle). A quarter warp of 8 threads therefore touches one row of the
+// tile, for every stage's reads and writes.
 // Rows are 128 bytes when TL·sizeof(element) = 128, so the shared-memory accesses are free of bank
 // conflicts whatever the stage's stride. The swizzled layout (tix) keeps columns conflict-free too.
 //
@@ -158,7 +159,7 @@ GBGHT_HD void tile_fft_io(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTR
     constexpr int R = Radices<N>::r[S];
     constexpr int NS = stage_ns<N>(S);
     constexpr int NB = N / R;
-    constexpr int TOT = NB * ACT;
+    constexpr int TOT = NB * TL;
     constexpr int BPT = (TOT + NT - 1) / NT;
     constexpr int TWS = N / (NS * R);
     constexpr bool FIRST = S == 0, LAST = S + 1 == Radices<N>::n;
@@ -166,8 +167,8 @@ GBGHT_HD void tile_fft_io(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTR
 #pragma unroll
     for (int b = 0; b < BPT; ++b) {
       const int idx = c.tid + b * NT;
-      if (BPT * NT == TOT || idx < TOT) {
-        const int l = idx % ACT, j = idx / ACT;
+      const int l = idx % TL, j = idx / TL;
+      if ((BPT * NT == TOT || idx < TOT) && (ACT == TL || l < ACT)) {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           if constexpr (FIRST) v[b][r] = src.load(j + r * NB, l);
@@ -179,8 +180,8 @@ GBGHT_HD void tile_fft_io(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTR
 #pragma unroll
     for (int b = 0; b < BPT; ++b) {
       const int idx = c.tid + b * NT;
-      if (BPT * NT == TOT || idx < TOT) {
-        const int l = idx % ACT, j = idx / ACT;
+      const int l = idx % TL, j = idx / TL;
+      if ((BPT * NT == TOT || idx < TOT) && (ACT == TL || l < ACT)) {
         const int jm = j % NS;
         if constexpr (NS > 1) {
           Cplx<T> w[R];
