@@ -120,6 +120,11 @@ double cfl_dt(const gbght_run* r) {
 
 }  // namespace
 
+namespace gbght {
+// The message gbght_global_error() returns, set by entry points that have no run handle.
+void set_global_error(const std::string& msg) { g_global_error = msg; }
+}  // namespace gbght
+
 extern "C" {
 
 void gbght_config_default(gbght_config* c) {

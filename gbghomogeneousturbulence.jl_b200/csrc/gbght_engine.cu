@@ -3,6 +3,7 @@
 // Built by nvcc for sm_100a (the library), or by a host C++ compiler with -DGBGHT_EMU for the
 // CPU check of the kernel bodies (see gbght_engine.cuh).
 #include "gbght_engine.cuh"
+#include "kernels.cuh"
 
 #include <algorithm>
 #include <cfloat>
@@ -81,167 +82,6 @@ static void emu_grid(int gx, int gy, int gz, size_t smem, F&& body) {
       }
 }
 
-// ------------------------------------------------------------------------------------------------
-// Kernels (CUDA build).
-// ------------------------------------------------------------------------------------------------
-#ifndef GBGHT_EMU
-#define CTA_CTX Cta c{int(threadIdx.x), int(blockIdx.x), int(blockIdx.y), int(blockIdx.z)}
-extern __shared__ __align__(1024) unsigned char g_smem[];
-
-__device__ __forceinline__ void init_bars(uint64_t* bar, int n) {
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < n; ++i) mbar_init(bar + i, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    fence_proxy_async();
-  }
-  __syncthreads();
-}
-
-// rows of a 2-D tensor map per box along the row dimension: the largest divisor of N ≤ 256
-template <int N> constexpr int box_rows() { return N > 256 ? (N % 256 == 0 ? 256 : N / 2) : N; }
-
-template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT, 2) k_y_inverse(const __grid_constant__ TmaMaps m, Geometry g, int c0,
-                                                     const Cplx<T>* tw, unsigned int* status) {
-  CTA_CTX;
-  Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + N * TL);
-  init_bars(bar, 1);
-  const int kx0 = c.bx * TL, z = c.by, comp = c0 + c.bz;
-  if (c.tid == 0) {
-    const int row0 = (comp * N + z) * g.NY2;
-    mbar_expect_tx(bar, uint32_t(2 * (g.K + 1) * TL * sizeof(Cplx<T>)));
-    tma_load_2d(sm, &m.a_ld, 2 * kx0, row0, bar);                            // q 0..K   → rows 0..K
-    tma_load_2d(sm + (N - g.K - 1) * TL, &m.a_ld, 2 * kx0, row0 + g.K, bar);  // q K..2K → rows N−K−1..N−1
-  }
-  mbar_wait(bar, 0, status);
-  y_inverse_compute<T, N, TL, NT>(c, sm, g, tw);
-  fence_proxy_async();
-  __syncthreads();
-  if (c.tid == 0) {
-    constexpr int BY = box_rows<N>();
-    for (int y0 = 0; y0 < N; y0 += BY) tma_store_2d(&m.b, 2 * kx0, (comp * N + z) * N + y0, sm + y0 * TL);
-    bulk_commit();
-    bulk_wait_read();
-  }
-}
-
-template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT, 2) k_y_forward(const __grid_constant__ TmaMaps m, Geometry g, const Cplx<T>* tw,
-                                                     unsigned int* status) {
-  CTA_CTX;
-  Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + N * TL);
-  init_bars(bar, 1);
-  const int kx0 = c.bx * TL, z = c.by, comp = c.bz;
-  constexpr int BY = box_rows<N>();
-  if (c.tid == 0) {
-    mbar_expect_tx(bar, uint32_t(N * TL * sizeof(Cplx<T>)));
-    for (int y0 = 0; y0 < N; y0 += BY) tma_load_2d(sm + y0 * TL, &m.b, 2 * kx0, (comp * N + z) * N + y0, bar);
-  }
-  mbar_wait(bar, 0, status);
-  tile_fft<T, N, TL, NT, -1>(c, sm, tw);
-  fence_proxy_async();
-  __syncthreads();
-  if (c.tid == 0) {
-    const int row0 = (comp * N + z) * g.NY2;
-    tma_store_2d(&m.a_st1, 2 * kx0, row0, sm);                                  // rows 0..K     → q 0..K
-    tma_store_2d(&m.a_st2, 2 * kx0, row0 + g.K + 1, sm + (N - g.K) * TL);         // rows N−K..N−1 → q K+1..2K
-    bulk_commit();
-    bulk_wait_read();
-  }
-}
-
-template <class T, int N, int NT>
-__global__ void __launch_bounds__(NT, 2) k_x_products(Geometry g, Cplx<T>* B, int has_scalar, const Cplx<T>* tw) {
-  CTA_CTX;
-  body_x_products<T, N, NT>(c, reinterpret_cast<Cplx<T>*>(g_smem), g, B, has_scalar, tw);
-}
-
-template <class T, int N, int NT>
-__global__ void __launch_bounds__(NT, 2) k_x_velocity(Geometry g, const Cplx<T>* B, T* u, unsigned long long* maxbits,
-                                                      const Cplx<T>* tw) {
-  CTA_CTX;
-  Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
-  double* red = reinterpret_cast<double*>(sm + N * XShape<T>::TL);
-  const double mx = body_x_velocity<T, N, NT>(c, sm, red, g, B, u, tw);
-  if (c.tid == 0) atomicMax(maxbits, static_cast<unsigned long long>(__double_as_longlong(mx)));
-}
-
-template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT, 2) k_z_epilogue(Geometry g, Cplx<T>* A, Cplx<T>* S, Cplx<T>* H, StageArgs st,
-                                                      const double* amp, double* partial, const Cplx<T>* tw) {
-  CTA_CTX;
-  Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
-  Cplx<T>* Rt = W + N * TL;
-  double* red = reinterpret_cast<double*>(Rt + 3 * g.NY2 * TL);
-  const double e = body_z_epilogue<T, N, TL, NT>(c, W, Rt, red, g, A, S, H, st, amp, tw);
-  if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
-}
-
-template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT, 2) k_z_init(Geometry g, Cplx<T>* A, const Cplx<T>* S, int has_scalar, double* partial,
-                                                  const Cplx<T>* tw) {
-  CTA_CTX;
-  Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
-  Cplx<T>* Rt = W + N * TL;
-  double* red = reinterpret_cast<double*>(Rt + 3 * g.NY2 * TL);
-  const double e = body_z_init<T, N, TL, NT>(c, W, Rt, red, g, A, S, has_scalar, tw);
-  if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
-}
-template <class T>
-__global__ void k_reality(Geometry g, Cplx<T>* S, int ncomp) {
-  reality_mode<T>(int(blockIdx.x * blockDim.x + threadIdx.x), g, S, ncomp);
-}
-// ConstantPower amplitude: band sum by thread 0; whole-field sum of the tile partials in a fixed
-// order (strided per thread, then a fixed tree).
-template <class T>
-__global__ void k_force_amp(Geometry g, const Cplx<T>* S, const double* partial, int npartial, double lo2,
-                            double hi2, double eps_rate, double eps_T, double* amp, unsigned int* status) {
-  __shared__ double red[256];
-  double s = 0.0;
-  for (int i = threadIdx.x; i < npartial; i += 256) s += partial[i];
-  red[threadIdx.x] = s;
-  __syncthreads();
-  for (int w = 128; w > 0; w >>= 1) {
-    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    const double whole = red[0];
-    const double band = band_energy_raw<T>(g, S, lo2, hi2);
-    const double n6 = double(g.N) * g.N * g.N * double(g.N) * g.N * g.N;
-    const double band_obs = 0.5 * (band / n6), whole_obs = 0.5 * (whole / n6);
-    double A = 0.0;
-    if (isfinite(band_obs) && band_obs > 10.0 * eps_T * whole_obs) A = eps_rate / (2.0 * band_obs);
-    else atomicOr(status, 0x2u);
-    amp[0] = A;
-    amp[1] = band_obs;
-    amp[2] = whole_obs;
-  }
-}
-template <class T, int NT>
-__global__ void __launch_bounds__(NT) k_observables(Geometry g, const Cplx<T>* S, int has_scalar, double* out) {
-  CTA_CTX;
-  body_observables<T, NT>(c, reinterpret_cast<double*>(g_smem), g, S, has_scalar, out);
-}
-template <class T, int NT>
-__global__ void __launch_bounds__(NT) k_spectrum(Geometry g, const Cplx<T>* S, int c0, int nc, int nshell, double* out) {
-  CTA_CTX;
-  double* hist = reinterpret_cast<double*>(g_smem);
-  body_spectrum<T, NT>(c, hist, hist + nshell, g, S, c0, nc, nshell, out);
-}
-template <class T>
-__global__ void k_tracers(int64_t M, int mode, const T* u, int N, double L, double* X, double* F, HeunWeights w) {
-  const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (p < M) tracer_one<T>(p, M, mode, u, N, L, X, F, w);
-}
-template <class T>
-__global__ void k_to_T(const double* in, T* out, size_t n) {
-  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = T(in[i]);
-}
-#endif
 
 // ------------------------------------------------------------------------------------------------
 // Host helpers.

@@ -600,7 +600,8 @@ GBGHT_HD double band_energy_raw(const Geometry& g, const Cplx<T>* S, double lo2,
 // ================================================================================================
 template <class T, int N, int TL, int NT>
 GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, const Geometry& g,
-                            Cplx<T>* GBGHT_RESTRICT A, const Cplx<T>* GBGHT_RESTRICT S, int has_scalar, const Cplx<T>* GBGHT_RESTRICT tw) {
+                            Cplx<T>* GBGHT_RESTRICT A, const Cplx<T>* GBGHT_RESTRICT S, int has_scalar,
+                            const Cplx<T>* GBGHT_RESTRICT tw, int vorticity = 1) {
   const int kx0 = c.bx * TL, qy = c.by;
   const int NY2 = g.NY2;
   const double ky = g.s * double(q_to_m(qy, g.K, NY2));
@@ -625,7 +626,7 @@ GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, 
     const auto u_new = [&](int q, int l) { return Rt[(o * NY2 + q) * TL + l]; };
     z_inverse1<T, N, TL, NT>(c, W, g, A, o, qy, kx0, u_new, tw);
   }
-  for (int o = 0; o < 3; ++o) {
+  for (int o = 0; o < 3 && vorticity; ++o) {
     const auto w_new = [&](int q, int l) { return curl_component<T, TL>(g, Rt, o, q, l, kx0, ky); };
     z_inverse1<T, N, TL, NT>(c, W, g, A, 3 + o, qy, kx0, w_new, tw);
   }
