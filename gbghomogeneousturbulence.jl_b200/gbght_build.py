@@ -40,6 +40,7 @@ def _units():
     """(name, defines) of every translation unit: one per (precision, N) for the engine, and the
     C ABI with the engine factory."""
     units = [("capi", ["-DGBGHT_UNIT_CAPI"], "gbght_capi.cu"),
+             ("noalloc", [], "gbght_noalloc.cu"),
              ("factory", ["-DGBGHT_UNIT_FACTORY"], "gbght_engine.cu")]
     for t in PRECISIONS:
         for n in SIZES:

@@ -194,6 +194,25 @@ int gbght_profile(gbght_run* run, int enable);
 int gbght_profile_read(gbght_run* run, int kind, int64_t* launches, double* total_ms);
 int gbght_timer(gbght_run* run, int op, double* ms);
 
+/* No counterpart in the reference: an allocation-free form of the deposit's velocity recovery,
+ * for callers that cannot allocate device memory. A caller whose device memory is owned by another
+ * allocator (for example a framework's caching pool that has reserved the GPU) cannot call
+ * cudaMalloc, and neither can a loop that keeps the reference's rule of no field-scale allocation
+ * inside a step. This call takes no run handle and allocates nothing. It reads the spectral
+ * velocity u_hat (device memory, complex128 [3][N][N][N/2+1], the reference layout), writes the
+ * physical velocity u (device memory, float64 [3][N][N][N]) and, if max_speed is not NULL,
+ * returns max|u| on the host. The values are those gbght_deposit + gbght_velocity_physical_export
+ * give for the same spectrum (FP64).
+ * Every intermediate lives in one file-scope device array of 12 MiB, held by each GPU that loads
+ * the library until the process exits. N is limited to 8, 12, 16, 24, 32, 48 or 64; a larger N is
+ * refused with GBGHT_ERR_ARGUMENT, as is a spectrum with content outside the retained 2/3 ball.
+ * The first call on a device looks up the array's address and should come before any stream
+ * capture. Calls share the array, so two calls whose work overlaps on the GPU race: serialise
+ * them. `stream` is a cudaStream_t (NULL: the default stream). The call synchronises that stream
+ * once, to read back max|u|. Errors are reported through gbght_global_error(). */
+int gbght_velocity_physical_noalloc(int grid_points_per_axis, double side_length, const double* u_hat,
+                                    double* u, double* max_speed, void* stream);
+
 /* Wait for all work queued on the run's stream. */
 int gbght_synchronize(gbght_run* run);
 

@@ -1,0 +1,69 @@
+"""The allocation-free velocity recovery against the regular deposit, through the C ABI.
+
+gbght_velocity_physical_noalloc serves callers that cannot allocate device memory: one whose
+memory is owned by another allocator (a framework's caching pool that holds the GPU), or a loop
+that keeps the rule of no field-scale allocation inside a step. It keeps every intermediate in
+one static device array. Here the caller's buffers are torch tensors (the caller's allocator, not
+the library's). Two calls in a row, on different spectra, must each match what gbght_deposit +
+gbght_velocity_physical_export give for the same spectrum: a stale scratch array would show up
+on the second call.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import gbght
+from gbght import seed as S
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def _regular(lib_path, N, uh):
+    run = gbght.Run(gbght.Setup(grid_points_per_axis=N, scalar=False), library=lib_path)
+    run.import_state(uh)
+    run.deposit()
+    u, m = run.velocity_physical(), run.max_speed()
+    run.close()
+    return u, m
+
+
+def test_noalloc_velocity_matches_the_regular_deposit(cuda_library):
+    import torch
+
+    lib = ctypes.CDLL(cuda_library)
+    fn = lib.gbght_velocity_physical_noalloc
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                   ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+    lib.gbght_global_error.restype = ctypes.c_char_p
+    N = 32
+    stream = torch.cuda.current_stream()
+    for call, seed in enumerate((11, 12)):
+        uh = S.seed_velocity(N, 0.5 + 0.25 * call, seed=seed)
+        u_ref, m_ref = _regular(cuda_library, N, uh)
+        d_uh = torch.from_numpy(uh.view(np.float64).copy()).cuda()
+        d_u = torch.full((3, N, N, N), float("nan"), dtype=torch.float64, device="cuda")
+        m = ctypes.c_double(-1.0)
+        torch.cuda.synchronize()
+        rc = fn(N, 2 * np.pi, d_uh.data_ptr(), d_u.data_ptr(), ctypes.byref(m), stream.cuda_stream)
+        assert rc == 0, lib.gbght_global_error().decode()
+        torch.cuda.synchronize()
+        u = d_u.cpu().numpy()
+        err = np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref)
+        assert err <= TOL, (call, err)
+        assert m.value == pytest.approx(m_ref, rel=TOL)
+
+
+def test_noalloc_refuses_grids_beyond_its_array(cuda_library):
+    lib = ctypes.CDLL(cuda_library)
+    fn = lib.gbght_velocity_physical_noalloc
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                   ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+    lib.gbght_global_error.restype = ctypes.c_char_p
+    rc = fn(128, 2 * np.pi, ctypes.c_void_p(16), ctypes.c_void_p(16), None, None)
+    assert rc == gbght.ERR_ARGUMENT
+    assert b"at most 64" in lib.gbght_global_error()
