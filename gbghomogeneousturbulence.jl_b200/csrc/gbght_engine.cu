@@ -102,7 +102,12 @@ class EngineImpl final : public Engine {
   static constexpr int TLY = Shape<T>::TLY;
   static constexpr int TLZ = Shape<T>::TLZ;
   static constexpr int NTY = kNT(N * TLY / 8);
-  static constexpr int NTX = kNT(N);
+  static constexpr int NTX = kNT(N);            // (unused by the warp-per-line x passes)
+#ifdef GBGHT_EMU
+  static constexpr int NTXP = 1, NTXV = 1;
+#else
+  static constexpr int NTXP = 32 * 7, NTXV = 32 * 6;   // one warp per line
+#endif
   static constexpr int NTZ = kNT(N * TLZ / 8);
   static constexpr int NTR = kNT(256);
 
@@ -522,8 +527,8 @@ class EngineImpl final : public Engine {
 
   static constexpr size_t kBarBytes = 32;
   size_t smem_y() const { return size_t(N) * TLY * sizeof(Cplx<T>) + kBarBytes; }
-  size_t smem_x() const { return size_t(N) * XShape<T>::TL * sizeof(Cplx<T>); }
-  size_t smem_xv() const { return size_t(N) * XShape<T>::TL * sizeof(Cplx<T>) + size_t(NTX) * sizeof(double); }
+  size_t smem_x() const { return size_t(N) * XShape<T>::ACT_INV * sizeof(Cplx<T>); }
+  size_t smem_xv() const { return size_t(N) * XShape<T>::ACT_V * sizeof(Cplx<T>) + size_t(NTXV) * sizeof(double); }
   size_t smem_z() const {
     return (size_t(N) * TLZ + 3 * size_t(g_.NY2) * TLZ) * sizeof(Cplx<T>) + size_t(NTZ) * sizeof(double);
   }
@@ -537,8 +542,8 @@ class EngineImpl final : public Engine {
     };
     set(reinterpret_cast<const void*>(k_y_inverse<T, N, TLY, NTY>), smem_y());
     set(reinterpret_cast<const void*>(k_y_forward<T, N, TLY, NTY>), smem_y());
-    set(reinterpret_cast<const void*>(k_x_products<T, N, NTX>), smem_x());
-    set(reinterpret_cast<const void*>(k_x_velocity<T, N, NTX>), smem_xv());
+    set(reinterpret_cast<const void*>(k_x_products<T, N, NTXP>), smem_x());
+    set(reinterpret_cast<const void*>(k_x_velocity<T, N, NTXV>), smem_xv());
     set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ>), smem_z());
     set(reinterpret_cast<const void*>(k_z_init<T, N, TLZ, NTZ>), smem_z());
     return e;
@@ -624,7 +629,7 @@ class EngineImpl final : public Engine {
     });
 #else
     pbegin(PROF_X_PRODUCTS);
-    k_x_products<T, N, NTX><<<dim3(N / X::P, N, 1), NTX, smem_x(), stream_>>>(g_, B_, p_.scalar, tw_);
+    k_x_products<T, N, NTXP><<<dim3(N / X::P, N, 1), NTXP, smem_x(), stream_>>>(g_, B_, p_.scalar, tw_);
     pend();
 #endif
   }
@@ -634,7 +639,7 @@ class EngineImpl final : public Engine {
     unsigned long long* mb = maxbits_;
     emu_grid(N / X::PV, N, 1, smem_xv(), [&](const Cta& c, void* sm) {
       Cplx<T>* t = static_cast<Cplx<T>*>(sm);
-      double* red = reinterpret_cast<double*>(t + N * X::TL);
+      double* red = reinterpret_cast<double*>(t + N * X::ACT_V);
       const double m = body_x_velocity<T, N, 1>(c, t, red, g_, B_, U_, tw_);
       unsigned long long bits;
       std::memcpy(&bits, &m, sizeof bits);
@@ -642,7 +647,7 @@ class EngineImpl final : public Engine {
     });
 #else
     pbegin(PROF_X_VELOCITY);
-    k_x_velocity<T, N, NTX><<<dim3(N / X::PV, N, 1), NTX, smem_xv(), stream_>>>(g_, B_, U_, maxbits_, tw_);
+    k_x_velocity<T, N, NTXV><<<dim3(N / X::PV, N, 1), NTXV, smem_xv(), stream_>>>(g_, B_, U_, maxbits_, tw_);
     pend();
 #endif
   }

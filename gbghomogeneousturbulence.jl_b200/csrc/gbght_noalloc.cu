@@ -169,7 +169,7 @@ int run_n(const Layout& o, unsigned char* base, const double* u_hat, double* u, 
   constexpr int TLY = 128 / int(sizeof(Cplx<double>));
   constexpr int TLZ = 64 / int(sizeof(Cplx<double>));
   constexpr int NTY = N * TLY / 8 < 64 ? 64 : (N * TLY / 8 > 256 ? 256 : N * TLY / 8);
-  constexpr int NTX = N < 64 ? 64 : (N > 256 ? 256 : N);
+  constexpr int NTX = 32 * 6;   // the deposit's x pass: one warp per line
   constexpr int NTZ = N * TLZ / 8 < 64 ? 64 : (N * TLZ / 8 > 256 ? 256 : N * TLZ / 8);
   const Geometry& g = o.g;
   auto* tw = reinterpret_cast<Cplx<double>*>(base + o.tw);
@@ -201,7 +201,7 @@ int run_n(const Layout& o, unsigned char* base, const double* u_hat, double* u, 
   gbght::k_z_init<double, N, TLZ, NTZ><<<dim3(g.KXP / TLZ, g.NY2, 1), NTZ, smem_z, st>>>(g, A, S, 0, partial, tw, 0);
   const size_t smem_y = size_t(N) * TLY * sizeof(Cplx<double>) + 32;
   gbght::k_y_inverse<double, N, TLY, NTY><<<dim3(g.KXP / TLY, N, 3), NTY, smem_y, st>>>(maps, g, 0, tw, flag);
-  const size_t smem_xv = size_t(N) * gbght::XShape<double>::TL * sizeof(Cplx<double>) + size_t(NTX) * sizeof(double);
+  const size_t smem_xv = size_t(N) * gbght::XShape<double>::ACT_V * sizeof(Cplx<double>) + size_t(NTX) * sizeof(double);
   gbght::k_x_velocity<double, N, NTX><<<dim3(N / gbght::XShape<double>::PV, N, 1), NTX, smem_xv, st>>>(g, B, u, maxbits,
                                                                                                       tw);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "kernel launch");

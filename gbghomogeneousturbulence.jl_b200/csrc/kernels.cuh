@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(NT, 2) k_x_velocity(Geometry g, const Cplx<T>*
                                                       const Cplx<T>* tw) {
   CTA_CTX;
   Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
-  double* red = reinterpret_cast<double*>(sm + N * XShape<T>::TL);
+  double* red = reinterpret_cast<double*>(sm + N * XShape<T>::ACT_V);
   const double mx = body_x_velocity<T, N, NT>(c, sm, red, g, B, u, tw);
   if (c.tid == 0) atomicMax(maxbits, static_cast<unsigned long long>(__double_as_longlong(mx)));
 }

@@ -22,6 +22,7 @@
 
 #include "fft_tile.cuh"
 #include "tma.cuh"
+#include "warp_fft.cuh"
 
 namespace gbght {
 
@@ -194,50 +195,72 @@ struct XPackedSource {
   }
 };
 
-// inverse (from B), products, forward, unpack (to B): one tile of P points per CTA
+// One line of an (e, l)-indexed source, for the warp-per-line transform.
+template <class Src>
+struct LineOfSource {
+  static constexpr bool kExternal = true;
+  const Src& s;
+  int l;
+  GBGHT_HD auto load(int e) const { return s.load(e, l); }
+};
+
+// inverse (from B), products, forward, unpack (to B): one tile of P points per CTA, one warp per
+// line. Lines live at sm + l·N. Block-wide barriers: two (before and after the products).
 template <class T, int N, int NT>
 GBGHT_HD void body_x_products(const Cta& c, Cplx<T>* sm, const Geometry& g, Cplx<T>* GBGHT_RESTRICT B,
                               int has_scalar, const Cplx<T>* GBGHT_RESTRICT tw) {
   using X = XShape<T>;
-  constexpr int TL = X::TL, P = X::P;
+  constexpr int P = X::P, NW = 7;
   const int y0 = P * c.bx, z = c.by;
   const int KX1 = g.K + 1;
   const XPackedSource<T, N, P> src{g, B, z, y0, has_scalar, T(g.inv_norm)};
-  tile_fft_io<T, N, TL, NT, +1, true, X::ACT_INV>(c, sm, tw, src, TileBuf<T, TL, true>{sm});
+  const auto lines = [&](int l) { return sm + l * N; };
+  const auto from_b = [&](int l) { return LineOfSource<XPackedSource<T, N, P>>{src, l}; };
+  const auto in_smem = [&](int l) { return LineBuf<T>{sm + l * N}; };
+  warp_fft_lines<T, N, NW, NT, +1>(c, X::ACT_INV, lines, from_b, in_smem, tw);
+  GBGHT_SYNC();
   for (int x = c.tid; x < N; x += NT) {
+    const int ix = lidx<T>(x);
 #pragma unroll
     for (int h = 0; h < P / 2; ++h) {
-      const Cplx<T> lp = sm[tix<TL, true>(x, 3 * P + h)];
+      const Cplx<T> lp = sm[(3 * P + h) * N + ix];
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         const int p = 2 * h + q;
-        const Cplx<T> L0 = sm[tix<TL, true>(x, 3 * p)], L1 = sm[tix<TL, true>(x, 3 * p + 1)],
-                      L2 = sm[tix<TL, true>(x, 3 * p + 2)];
+        const Cplx<T> L0 = sm[(3 * p) * N + ix], L1 = sm[(3 * p + 1) * N + ix], L2 = sm[(3 * p + 2) * N + ix];
         const T ux = L0.x, uy = L0.y, uz = L1.x, wx = L1.y, wy = L2.x, wz = L2.y;
         const T ph = q == 0 ? lp.x : lp.y;
         const T nx = uy * wz - uz * wy, ny = uz * wx - ux * wz, nz = ux * wy - uy * wx;
-        sm[tix<TL, true>(x, 3 * p)] = cmk<T>(nx, ny);
-        sm[tix<TL, true>(x, 3 * p + 1)] = cmk<T>(nz, ux * ph);
-        sm[tix<TL, true>(x, 3 * p + 2)] = cmk<T>(uy * ph, uz * ph);
+        sm[(3 * p) * N + ix] = cmk<T>(nx, ny);
+        sm[(3 * p + 1) * N + ix] = cmk<T>(nz, ux * ph);
+        sm[(3 * p + 2) * N + ix] = cmk<T>(uy * ph, uz * ph);
       }
     }
   }
   GBGHT_SYNC();
-  tile_fft<T, N, TL, NT, -1, true, X::ACT_FWD>(c, sm, tw);
-  // unpack the six products of each point into B slots 0..5 (0..2 without a scalar); columns
-  // past K get zeros
-  const int nline = has_scalar ? 3 * P : P * 3;
-  for (int i = c.tid; i < nline * g.KXP; i += NT) {
-    const int k = i % g.KXP, line = i / g.KXP;
-    const int p = line / 3, pr = line % 3;
-    if (!has_scalar && pr > 0 && 2 * pr >= 3) {
+  warp_fft_lines<T, N, NW, NT, -1>(c, X::ACT_FWD, lines, in_smem, in_smem, tw);
+  // unpack each line (by its owning warp) into B: line 3p+pr → comps (2pr, 2pr+1) of point p;
+  // columns past K get zeros
+  const int nout = has_scalar ? 6 : 3;
+  for (int t = c.tid; t < 32 * NW; t += NT) {
+    const int w = t >> 5, lane = t & 31;
+    for (int line = w; line < X::ACT_FWD; line += NW) {
+      const int p = line / 3, pr = line % 3;
+      const int ca = 2 * pr, cb = 2 * pr + 1;
+      const Cplx<T>* L = sm + line * N;
+      for (int k = lane; k < g.KXP; k += 32) {
+        Cplx<T> a = czero<T>(), b = czero<T>();
+        if (k < KX1) {
+          const Cplx<T> zk = L[lidx<T>(k)];
+          const Cplx<T> zc = conj(L[lidx<T>((N - k) % N)]);
+          const Cplx<T> sp = zk + zc, sd = zk - zc;
+          a = cmk<T>(sp.x * T(0.5), sp.y * T(0.5));
+          b = cmk<T>(sd.y * T(0.5), -sd.x * T(0.5));
+        }
+        if (ca < nout) B[idxB(g, ca, z, y0 + p, k)] = a;
+        if (cb < nout) B[idxB(g, cb, z, y0 + p, k)] = b;
+      }
     }
-    Cplx<T> a = czero<T>(), b = czero<T>();
-    if (k < KX1) unpack_pair<T, TL>(sm, N, line, k, a, b);
-    const int ca = 2 * pr, cb = 2 * pr + 1;
-    const int nout = has_scalar ? 6 : 3;
-    if (ca < nout) B[idxB(g, ca, z, y0 + p, k)] = a;
-    if (cb < nout) B[idxB(g, cb, z, y0 + p, k)] = b;
   }
 }
 
@@ -277,21 +300,27 @@ struct XVelocitySource {
 };
 
 // The deposit's x-pass: physical velocity of PV points written out, max |u|² returned to thread 0.
+// One warp per line (ACT_V lines at sm + l·N).
 template <class T, int N, int NT>
 GBGHT_HD double body_x_velocity(const Cta& c, Cplx<T>* sm, double* red, const Geometry& g,
                                 const Cplx<T>* GBGHT_RESTRICT B, T* GBGHT_RESTRICT u_phys,
                                 const Cplx<T>* GBGHT_RESTRICT tw) {
   using X = XShape<T>;
-  constexpr int TL = X::TL, PV = X::PV;
+  constexpr int PV = X::PV, NW = 6;
   const int y0 = PV * c.bx, z = c.by;
   const XVelocitySource<T, N, PV> src{g, B, z, y0, T(g.inv_norm)};
-  tile_fft_io<T, N, TL, NT, +1, true, X::ACT_V>(c, sm, tw, src, TileBuf<T, TL, true>{sm});
+  const auto lines = [&](int l) { return sm + l * N; };
+  const auto from_b = [&](int l) { return LineOfSource<XVelocitySource<T, N, PV>>{src, l}; };
+  const auto in_smem = [&](int l) { return LineBuf<T>{sm + l * N}; };
+  warp_fft_lines<T, N, NW, NT, +1>(c, X::ACT_V, lines, from_b, in_smem, tw);
+  GBGHT_SYNC();
   double m = 0.0;
   const size_t comp = size_t(N) * N * N;
   for (int i = c.tid; i < PV * N; i += NT) {
     const int x = i % N, p = i / N;
-    const Cplx<T> uxy = sm[tix<TL, true>(x, p)];
-    const Cplx<T> uzz = sm[tix<TL, true>(x, PV + (p >> 1))];
+    const int ix = lidx<T>(x);
+    const Cplx<T> uxy = sm[p * N + ix];
+    const Cplx<T> uzz = sm[(PV + (p >> 1)) * N + ix];
     const T uz = (p & 1) ? uzz.y : uzz.x;
     const size_t base = (size_t(z) * N + (y0 + p)) * N + x;
     u_phys[base] = uxy.x;
