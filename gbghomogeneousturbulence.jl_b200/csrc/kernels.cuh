@@ -80,13 +80,13 @@ __global__ void __launch_bounds__(NT, 2) k_y_forward(const __grid_constant__ Tma
 }
 
 template <class T, int N, int NT>
-__global__ void __launch_bounds__(NT, 2) k_x_products(Geometry g, Cplx<T>* B, int has_scalar, const Cplx<T>* tw) {
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_x_products(Geometry g, Cplx<T>* B, int has_scalar, const Cplx<T>* tw) {
   CTA_CTX;
   body_x_products<T, N, NT>(c, reinterpret_cast<Cplx<T>*>(g_smem), g, B, has_scalar, tw);
 }
 
 template <class T, int N, int NT>
-__global__ void __launch_bounds__(NT, 2) k_x_velocity(Geometry g, const Cplx<T>* B, T* u, unsigned long long* maxbits,
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_x_velocity(Geometry g, const Cplx<T>* B, T* u, unsigned long long* maxbits,
                                                       const Cplx<T>* tw) {
   CTA_CTX;
   Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
