@@ -39,6 +39,10 @@ METRIC = "512³ IF-RK4 steps/s, FP32-mixed vs FP64 on one B200 at ≤1e-5 spectr
 WORKLOAD = dict(N=512, viscosity=8.5e-4, schmidt=1.0, injection_rate=0.1, shells=(1, 2), G=(1.0, 0.0, 0.0),
                 tracers=1_000_000, cfl=0.5, scheme="IFLowStorageRK4")
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# DRAM traffic per launch over algorithmic bytes, from the ncu capture of the kernel at 256³
+# (profiles/x_products_256cubed_fp64.md), applied to the 512³ launch: the traffic scales with the
+# tiles processed.
+TRAFFIC_RATIO = {("x_products", "fp64"): 1.141 / 1.171}
 FALLBACK_HBM = 6650.0
 
 
@@ -322,7 +326,10 @@ def ours(args):
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                          "unit": "GB/s", "frac": round(achieved / hbm, 4),
                          "algorithmic_bytes_per_launch": ab[kind] / max(1, n_launch / args.steps),
-                         "avg_launch_ms": tot_ms / max(1, n_launch), "traffic": None},
+                         "avg_launch_ms": tot_ms / max(1, n_launch),
+                         "traffic": (round(ab[kind] / max(1, n_launch / args.steps) * TRAFFIC_RATIO[(kind, forms[0])])
+                                     if (kind, forms[0]) in TRAFFIC_RATIO else None),
+                         "traffic_source": "ncu dram__bytes_read+write at 256^3 scaled by units (profiles/)"},
             "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in prof.items() if v[0]},
             "gpu_launches": int(sum(v[0] for v in prof.values())),
             "clocks": head["clocks"],
