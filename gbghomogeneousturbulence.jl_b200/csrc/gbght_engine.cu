@@ -154,6 +154,9 @@ class EngineImpl final : public Engine {
     e = cuda_err(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     if (e) return e;
     if ((e = set_smem_attributes())) return e;
+    if ((e = cuda_err(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, p.device),
+                      "cudaDeviceGetAttribute")))
+      return e;
 #endif
     const char* err = nullptr;
     if ((err = alloc(&S_, 4 * nS_ * sizeof(Cplx<T>)))) return err;
@@ -527,7 +530,10 @@ class EngineImpl final : public Engine {
 
   static constexpr size_t kBarBytes = 32;
   size_t smem_y() const { return size_t(N) * TLY * sizeof(Cplx<T>) + kBarBytes; }
-  size_t smem_x() const { return size_t(N) * XShape<T>::ACT_INV * sizeof(Cplx<T>); }
+  size_t smem_x() const {
+    return size_t(N) * XShape<T>::ACT_INV * sizeof(Cplx<T>) +
+           size_t(7) * XShape<T>::P * x_kxs(g_.K, int(sizeof(Cplx<T>))) * sizeof(Cplx<T>) + kBarBytes;
+  }
   size_t smem_xv() const { return size_t(N) * XShape<T>::ACT_V * sizeof(Cplx<T>) + size_t(NTXV) * sizeof(double); }
   size_t smem_z() const {
     return (size_t(N) * TLZ + 3 * size_t(g_.NY2) * TLZ) * sizeof(Cplx<T>) + size_t(NTZ) * sizeof(double);
@@ -623,13 +629,18 @@ class EngineImpl final : public Engine {
   }
   void x_products() {
     using X = XShape<T>;
+    const int KXS = x_kxs(g_.K, int(sizeof(Cplx<T>)));
+    const int ntiles = (N / X::P) * N;
+    const int grid = std::min(ntiles, 2 * sm_count_);
 #ifdef GBGHT_EMU
-    emu_grid(N / X::P, N, 1, smem_x(), [&](const Cta& c, void* sm) {
-      body_x_products<T, N, 1>(c, static_cast<Cplx<T>*>(sm), g_, B_, p_.scalar, tw_);
+    emu_grid(grid, 1, 1, smem_x(), [&](const Cta& c, void* sm) {
+      Cplx<T>* t = static_cast<Cplx<T>*>(sm);
+      Cplx<T>* stg = t + N * X::ACT_INV;
+      body_x_products<T, N, 1>(c, t, stg, KXS, nullptr, grid, g_, B_, p_.scalar, tw_, status_);
     });
 #else
     pbegin(PROF_X_PRODUCTS);
-    k_x_products<T, N, NTXP><<<dim3(N / X::P, N, 1), NTXP, smem_x(), stream_>>>(g_, B_, p_.scalar, tw_);
+    k_x_products<T, N, NTXP><<<grid, NTXP, smem_x(), stream_>>>(g_, B_, p_.scalar, KXS, tw_, status_);
     pend();
 #endif
   }
@@ -751,6 +762,7 @@ class EngineImpl final : public Engine {
   double cutoff_ = 0.0;
   size_t nS_ = 0, nA_ = 0, nB_ = 0, nP_ = 0, ntile_ = 0;
   int nshell_ = 0;
+  int sm_count_ = 4;
   Stream stream_ = nullptr;
   std::vector<void*> allocs_;
   Cplx<T>*S_ = nullptr, *H_ = nullptr, *A_ = nullptr, *B_ = nullptr, *tw_ = nullptr;

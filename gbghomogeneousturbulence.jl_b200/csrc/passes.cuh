@@ -204,63 +204,144 @@ struct LineOfSource {
   GBGHT_HD auto load(int e) const { return s.load(e, l); }
 };
 
-// inverse (from B), products, forward, unpack (to B): one tile of P points per CTA, one warp per
-// line. Lines live at sm + l·N. Block-wide barriers: two (before and after the products).
+// Source of the x-pass inverse's first stage from the staging rows [c][p][KXS] in shared memory
+// (the same packing as XPackedSource).
+template <class T, int N, int P>
+struct XStagedSource {
+  static constexpr bool kExternal = true;
+  const Geometry& g;
+  const Cplx<T>* stg;
+  int KXS, has_scalar;
+  T sc;
+  GBGHT_HD Cplx<T> load(int e, int l) const {
+    const int K = g.K;
+    if (e > K && e < N - K) return czero<T>();
+    int ra, rb;   // staging rows of the pair
+    if (l < 3 * P) {
+      const int p = l / 3, pr = l % 3;
+      ra = (2 * pr) * P + p;
+      rb = (2 * pr + 1) * P + p;
+    } else {
+      if (!has_scalar) return czero<T>();
+      const int h = l - 3 * P;
+      ra = 6 * P + 2 * h;
+      rb = ra + 1;
+    }
+    const int m = e <= K ? e : N - e;
+    const Cplx<T> a = stg[ra * KXS + m], b = stg[rb * KXS + m];
+    if (e == 0) return cmk<T>(a.x * sc, b.x * sc);
+    if (e <= K) return cmk<T>((a.x - b.y) * sc, (a.y + b.x) * sc);
+    return cmk<T>((a.x + b.y) * sc, (b.x - a.y) * sc);
+  }
+};
+
+// Staging of one x tile: the rows B[c][z][y0+p][0..KXS) of comps c < nin, as untiled bulk copies
+// completing on `bar` (device), or plain copies (host-check build).
+template <class T, int P>
+struct XStaging {
+  const Geometry& g;
+  const Cplx<T>* B;
+  Cplx<T>* stg;
+  int KXS, nin;
+  uint64_t* bar;
+  unsigned int* status;
+  GBGHT_HD void issue(const Cta& c, int z, int y0) const {
+#ifdef __CUDA_ARCH__
+    if (c.tid == 0) {
+      const uint32_t row = uint32_t(KXS * sizeof(Cplx<T>));
+      mbar_expect_tx(bar, row * uint32_t(nin * P));
+      for (int cc = 0; cc < nin; ++cc)
+        for (int p = 0; p < P; ++p) bulk_load(stg + (cc * P + p) * KXS, B + idxB(g, cc, z, y0 + p, 0), row, bar);
+    }
+#else
+    (void)c;
+    for (int cc = 0; cc < nin; ++cc)
+      for (int p = 0; p < P; ++p)
+        for (int e = 0; e < KXS; ++e) stg[(cc * P + p) * KXS + e] = B[idxB(g, cc, z, y0 + p, e)];
+#endif
+  }
+  GBGHT_HD void wait(uint32_t phase) const {
+#ifdef __CUDA_ARCH__
+    mbar_wait(bar, phase, status);
+#else
+    (void)phase;
+#endif
+  }
+};
+
+// inverse, products, forward, unpack for the x tiles bx, bx + grid, …: one warp per line, lines at
+// sm + l·N, the next tile's spectra prefetched into the staging rows while the current tile is
+// transformed. Block-wide barriers per tile: after the first inverse stage (the staging is free
+// again), and before and after the products.
 template <class T, int N, int NT>
-GBGHT_HD void body_x_products(const Cta& c, Cplx<T>* sm, const Geometry& g, Cplx<T>* GBGHT_RESTRICT B,
-                              int has_scalar, const Cplx<T>* GBGHT_RESTRICT tw) {
+GBGHT_HD void body_x_products(const Cta& c, Cplx<T>* sm, Cplx<T>* stg, int KXS, uint64_t* bar, int grid,
+                              const Geometry& g, Cplx<T>* GBGHT_RESTRICT B, int has_scalar,
+                              const Cplx<T>* GBGHT_RESTRICT tw, unsigned int* status) {
   using X = XShape<T>;
   constexpr int P = X::P, NW = 7;
-  const int y0 = P * c.bx, z = c.by;
   const int KX1 = g.K + 1;
-  const XPackedSource<T, N, P> src{g, B, z, y0, has_scalar, T(g.inv_norm)};
+  const int nin = has_scalar ? 7 : 6, nout = has_scalar ? 6 : 3;
+  const int tiles_y = N / P, ntiles = tiles_y * N;
+  const XStaging<T, P> stage{g, B, stg, KXS, nin, bar, status};
+  const XStagedSource<T, N, P> src{g, stg, KXS, has_scalar, T(g.inv_norm)};
   const auto lines = [&](int l) { return sm + l * N; };
-  const auto from_b = [&](int l) { return LineOfSource<XPackedSource<T, N, P>>{src, l}; };
+  const auto from_stg = [&](int l) { return LineOfSource<XStagedSource<T, N, P>>{src, l}; };
   const auto in_smem = [&](int l) { return LineBuf<T>{sm + l * N}; };
-  warp_fft_lines<T, N, NW, NT, +1>(c, X::ACT_INV, lines, from_b, in_smem, tw);
-  GBGHT_SYNC();
-  for (int x = c.tid; x < N; x += NT) {
-    const int ix = lidx<T>(x);
+  uint32_t phase = 0;
+  if (c.bx < ntiles) stage.issue(c, c.bx / tiles_y, P * (c.bx % tiles_y));
+  for (int tile = c.bx; tile < ntiles; tile += grid) {
+    const int z = tile / tiles_y, y0 = P * (tile % tiles_y);
+    stage.wait(phase);
+    phase ^= 1u;
+    warp_fft_lines<T, N, NW, NT, +1, 0, 1>(c, X::ACT_INV, lines, from_stg, in_smem, tw);
+    GBGHT_SYNC();
+    const int next = tile + grid;
+    if (next < ntiles) stage.issue(c, next / tiles_y, P * (next % tiles_y));
+    warp_fft_lines<T, N, NW, NT, +1, 1>(c, X::ACT_INV, lines, from_stg, in_smem, tw);
+    GBGHT_SYNC();
+    for (int x = c.tid; x < N; x += NT) {
+      const int ix = lidx<T>(x);
 #pragma unroll
-    for (int h = 0; h < P / 2; ++h) {
-      const Cplx<T> lp = sm[(3 * P + h) * N + ix];
+      for (int h = 0; h < P / 2; ++h) {
+        const Cplx<T> lp = sm[(3 * P + h) * N + ix];
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int p = 2 * h + q;
-        const Cplx<T> L0 = sm[(3 * p) * N + ix], L1 = sm[(3 * p + 1) * N + ix], L2 = sm[(3 * p + 2) * N + ix];
-        const T ux = L0.x, uy = L0.y, uz = L1.x, wx = L1.y, wy = L2.x, wz = L2.y;
-        const T ph = q == 0 ? lp.x : lp.y;
-        const T nx = uy * wz - uz * wy, ny = uz * wx - ux * wz, nz = ux * wy - uy * wx;
-        sm[(3 * p) * N + ix] = cmk<T>(nx, ny);
-        sm[(3 * p + 1) * N + ix] = cmk<T>(nz, ux * ph);
-        sm[(3 * p + 2) * N + ix] = cmk<T>(uy * ph, uz * ph);
-      }
-    }
-  }
-  GBGHT_SYNC();
-  warp_fft_lines<T, N, NW, NT, -1>(c, X::ACT_FWD, lines, in_smem, in_smem, tw);
-  // unpack each line (by its owning warp) into B: line 3p+pr → comps (2pr, 2pr+1) of point p;
-  // columns past K get zeros
-  const int nout = has_scalar ? 6 : 3;
-  for (int t = c.tid; t < 32 * NW; t += NT) {
-    const int w = t >> 5, lane = t & 31;
-    for (int line = w; line < X::ACT_FWD; line += NW) {
-      const int p = line / 3, pr = line % 3;
-      const int ca = 2 * pr, cb = 2 * pr + 1;
-      const Cplx<T>* L = sm + line * N;
-      for (int k = lane; k < g.KXP; k += 32) {
-        Cplx<T> a = czero<T>(), b = czero<T>();
-        if (k < KX1) {
-          const Cplx<T> zk = L[lidx<T>(k)];
-          const Cplx<T> zc = conj(L[lidx<T>((N - k) % N)]);
-          const Cplx<T> sp = zk + zc, sd = zk - zc;
-          a = cmk<T>(sp.x * T(0.5), sp.y * T(0.5));
-          b = cmk<T>(sd.y * T(0.5), -sd.x * T(0.5));
+        for (int q = 0; q < 2; ++q) {
+          const int p = 2 * h + q;
+          const Cplx<T> L0 = sm[(3 * p) * N + ix], L1 = sm[(3 * p + 1) * N + ix], L2 = sm[(3 * p + 2) * N + ix];
+          const T ux = L0.x, uy = L0.y, uz = L1.x, wx = L1.y, wy = L2.x, wz = L2.y;
+          const T ph = q == 0 ? lp.x : lp.y;
+          const T nx = uy * wz - uz * wy, ny = uz * wx - ux * wz, nz = ux * wy - uy * wx;
+          sm[(3 * p) * N + ix] = cmk<T>(nx, ny);
+          sm[(3 * p + 1) * N + ix] = cmk<T>(nz, ux * ph);
+          sm[(3 * p + 2) * N + ix] = cmk<T>(uy * ph, uz * ph);
         }
-        if (ca < nout) B[idxB(g, ca, z, y0 + p, k)] = a;
-        if (cb < nout) B[idxB(g, cb, z, y0 + p, k)] = b;
       }
     }
+    GBGHT_SYNC();
+    warp_fft_lines<T, N, NW, NT, -1>(c, X::ACT_FWD, lines, in_smem, in_smem, tw);
+    // unpack each line (by its owning warp) into B: line 3p+pr → comps (2pr, 2pr+1) of point p;
+    // columns past K get zeros
+    for (int t = c.tid; t < 32 * NW; t += NT) {
+      const int w = t >> 5, lane = t & 31;
+      for (int line = w; line < X::ACT_FWD; line += NW) {
+        const int p = line / 3, pr = line % 3;
+        const int ca = 2 * pr, cb = 2 * pr + 1;
+        const Cplx<T>* L = sm + line * N;
+        for (int k = lane; k < g.KXP; k += 32) {
+          Cplx<T> a = czero<T>(), b = czero<T>();
+          if (k < KX1) {
+            const Cplx<T> zk = L[lidx<T>(k)];
+            const Cplx<T> zc = conj(L[lidx<T>((N - k) % N)]);
+            const Cplx<T> sp = zk + zc, sd = zk - zc;
+            a = cmk<T>(sp.x * T(0.5), sp.y * T(0.5));
+            b = cmk<T>(sd.y * T(0.5), -sd.x * T(0.5));
+          }
+          if (ca < nout) B[idxB(g, ca, z, y0 + p, k)] = a;
+          if (cb < nout) B[idxB(g, cb, z, y0 + p, k)] = b;
+        }
+      }
+    }
+    GBGHT_SYNC();   // the lines are rewritten by the next tile's inverse
   }
 }
 

@@ -41,13 +41,14 @@ struct LineBuf {
   GBGHT_HD void store(int e, Cplx<T> v) const { line[lidx<T>(e)] = v; }
 };
 
-// Transform line `w` of each of NW warps (or, with NLPW > 1 lines per warp, lines w + k·NW).
+// Transform line `w` of each of NW warps (lines w + k·NW when nlines > NW), stages [S, S_END).
 // `lines(w)` returns the shared-memory base of line w; `src(w)`/`dst(w)` the first-stage source
 // and last-stage sink of line w. Only lines w < nlines are transformed.
-template <class T, int N, int NW, int NT, int SIGN, int S = 0, class LineOf, class SrcOf, class DstOf>
+template <class T, int N, int NW, int NT, int SIGN, int S = 0, int S_END = Radices<N>::n, class LineOf, class SrcOf,
+          class DstOf>
 GBGHT_HD void warp_fft_lines(const Cta& c, int nlines, const LineOf& lines, const SrcOf& src, const DstOf& dst,
                              const Cplx<T>* GBGHT_RESTRICT tw) {
-  if constexpr (S < Radices<N>::n) {
+  if constexpr (S < S_END) {
     constexpr int R = Radices<N>::r[S];
     constexpr int NS = stage_ns<N>(S);
     constexpr int NB = N / R;
@@ -110,7 +111,7 @@ GBGHT_HD void warp_fft_lines(const Cta& c, int nlines, const LineOf& lines, cons
       }
       warp_sync();
     }
-    warp_fft_lines<T, N, NW, NT, SIGN, S + 1>(c, nlines, lines, src, dst, tw);
+    warp_fft_lines<T, N, NW, NT, SIGN, S + 1, S_END>(c, nlines, lines, src, dst, tw);
   }
 }
 
