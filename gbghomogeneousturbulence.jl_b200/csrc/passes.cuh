@@ -269,80 +269,101 @@ struct XStaging {
   }
 };
 
-// inverse, products, forward, unpack for the x tiles bx, bx + grid, …: one warp per line, lines at
-// sm + l·N, the next tile's spectra prefetched into the staging rows while the current tile is
-// transformed. Block-wide barriers per tile: after the first inverse stage (the staging is free
-// again), and before and after the products.
+#ifdef __CUDA_ARCH__
+#define GBGHT_NOINLINE __noinline__
+#else
+#define GBGHT_NOINLINE
+#endif
+
+// One x tile: the inverse of the staged spectra (the first stage reads the staging; after it the
+// staging is free and the next tile's copies are issued), the products, the forward transform and
+// the unpack into B. Kept out of line: inlined into the persistent loop below, its lane-dependent
+// index arithmetic is hoisted out of the loop and the kernel spills.
+template <class T, int N, int NT>
+GBGHT_HD void x_tile(const Cta& c, Cplx<T>* sm, const XStaging<T, XShape<T>::P>& stage,
+                                    const XStagedSource<T, N, XShape<T>::P>& src, const Geometry& g,
+                                    Cplx<T>* GBGHT_RESTRICT B, int nout, int z, int y0, int next_z, int next_y0,
+                                    const Cplx<T>* GBGHT_RESTRICT tw) {
+  using X = XShape<T>;
+  constexpr int P = X::P, NW = 7;
+  const int KX1 = g.K + 1;
+  const auto lines = [&](int l) { return sm + l * N; };
+  const auto from_stg = [&](int l) { return LineOfSource<XStagedSource<T, N, P>>{src, l}; };
+  const auto in_smem = [&](int l) { return LineBuf<T>{sm + l * N}; };
+  warp_fft_lines<T, N, NW, NT, +1, 0, 1>(c, X::ACT_INV, lines, from_stg, in_smem, tw);
+  GBGHT_SYNC();
+  if (next_z >= 0) stage.issue(c, next_z, next_y0);
+  warp_fft_lines<T, N, NW, NT, +1, 1>(c, X::ACT_INV, lines, from_stg, in_smem, tw);
+  GBGHT_SYNC();
+  for (int x = c.tid; x < N; x += NT) {
+    const int ix = lidx<T>(x);
+#pragma unroll
+    for (int h = 0; h < P / 2; ++h) {
+      const Cplx<T> lp = sm[(3 * P + h) * N + ix];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int p = 2 * h + q;
+        const Cplx<T> L0 = sm[(3 * p) * N + ix], L1 = sm[(3 * p + 1) * N + ix], L2 = sm[(3 * p + 2) * N + ix];
+        const T ux = L0.x, uy = L0.y, uz = L1.x, wx = L1.y, wy = L2.x, wz = L2.y;
+        const T ph = q == 0 ? lp.x : lp.y;
+        const T nx = uy * wz - uz * wy, ny = uz * wx - ux * wz, nz = ux * wy - uy * wx;
+        sm[(3 * p) * N + ix] = cmk<T>(nx, ny);
+        sm[(3 * p + 1) * N + ix] = cmk<T>(nz, ux * ph);
+        sm[(3 * p + 2) * N + ix] = cmk<T>(uy * ph, uz * ph);
+      }
+    }
+  }
+  GBGHT_SYNC();
+  warp_fft_lines<T, N, NW, NT, -1>(c, X::ACT_FWD, lines, in_smem, in_smem, tw);
+  // unpack each line (by its owning warp) into B: line 3p+pr → comps (2pr, 2pr+1) of point p;
+  // columns past K get zeros
+  for (int t = c.tid; t < 32 * NW; t += NT) {
+    const int w = t >> 5, lane = t & 31;
+    for (int line = w; line < X::ACT_FWD; line += NW) {
+      const int p = line / 3, pr = line % 3;
+      const int ca = 2 * pr, cb = 2 * pr + 1;
+      const Cplx<T>* L = sm + line * N;
+      for (int k = lane; k < g.KXP; k += 32) {
+        Cplx<T> a = czero<T>(), b = czero<T>();
+        if (k < KX1) {
+          const Cplx<T> zk = L[lidx<T>(k)];
+          const Cplx<T> zc = conj(L[lidx<T>((N - k) % N)]);
+          const Cplx<T> sp = zk + zc, sd = zk - zc;
+          a = cmk<T>(sp.x * T(0.5), sp.y * T(0.5));
+          b = cmk<T>(sd.y * T(0.5), -sd.x * T(0.5));
+        }
+        if (ca < nout) B[idxB(g, ca, z, y0 + p, k)] = a;
+        if (cb < nout) B[idxB(g, cb, z, y0 + p, k)] = b;
+      }
+    }
+  }
+  GBGHT_SYNC();   // the lines are rewritten by the next tile's inverse
+}
+
+// The x pass over the tiles bx, bx + grid, …: one warp per line, lines at sm + l·N, the next
+// tile's spectra prefetched into the staging rows while the current tile is transformed.
 template <class T, int N, int NT>
 GBGHT_HD void body_x_products(const Cta& c, Cplx<T>* sm, Cplx<T>* stg, int KXS, uint64_t* bar, int grid,
                               const Geometry& g, Cplx<T>* GBGHT_RESTRICT B, int has_scalar,
                               const Cplx<T>* GBGHT_RESTRICT tw, unsigned int* status) {
   using X = XShape<T>;
-  constexpr int P = X::P, NW = 7;
-  const int KX1 = g.K + 1;
+  constexpr int P = X::P;
   const int nin = has_scalar ? 7 : 6, nout = has_scalar ? 6 : 3;
   const int tiles_y = N / P, ntiles = tiles_y * N;
   const XStaging<T, P> stage{g, B, stg, KXS, nin, bar, status};
   const XStagedSource<T, N, P> src{g, stg, KXS, has_scalar, T(g.inv_norm)};
-  const auto lines = [&](int l) { return sm + l * N; };
-  const auto from_stg = [&](int l) { return LineOfSource<XStagedSource<T, N, P>>{src, l}; };
-  const auto in_smem = [&](int l) { return LineBuf<T>{sm + l * N}; };
-  uint32_t phase = 0;
-  if (c.bx < ntiles) stage.issue(c, c.bx / tiles_y, P * (c.bx % tiles_y));
-  for (int tile = c.bx; tile < ntiles; tile += grid) {
-    const int z = tile / tiles_y, y0 = P * (tile % tiles_y);
-    stage.wait(phase);
-    phase ^= 1u;
-    warp_fft_lines<T, N, NW, NT, +1, 0, 1>(c, X::ACT_INV, lines, from_stg, in_smem, tw);
-    GBGHT_SYNC();
-    const int next = tile + grid;
-    if (next < ntiles) stage.issue(c, next / tiles_y, P * (next % tiles_y));
-    warp_fft_lines<T, N, NW, NT, +1, 1>(c, X::ACT_INV, lines, from_stg, in_smem, tw);
-    GBGHT_SYNC();
-    for (int x = c.tid; x < N; x += NT) {
-      const int ix = lidx<T>(x);
-#pragma unroll
-      for (int h = 0; h < P / 2; ++h) {
-        const Cplx<T> lp = sm[(3 * P + h) * N + ix];
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int p = 2 * h + q;
-          const Cplx<T> L0 = sm[(3 * p) * N + ix], L1 = sm[(3 * p + 1) * N + ix], L2 = sm[(3 * p + 2) * N + ix];
-          const T ux = L0.x, uy = L0.y, uz = L1.x, wx = L1.y, wy = L2.x, wz = L2.y;
-          const T ph = q == 0 ? lp.x : lp.y;
-          const T nx = uy * wz - uz * wy, ny = uz * wx - ux * wz, nz = ux * wy - uy * wx;
-          sm[(3 * p) * N + ix] = cmk<T>(nx, ny);
-          sm[(3 * p + 1) * N + ix] = cmk<T>(nz, ux * ph);
-          sm[(3 * p + 2) * N + ix] = cmk<T>(uy * ph, uz * ph);
-        }
-      }
-    }
-    GBGHT_SYNC();
-    warp_fft_lines<T, N, NW, NT, -1>(c, X::ACT_FWD, lines, in_smem, in_smem, tw);
-    // unpack each line (by its owning warp) into B: line 3p+pr → comps (2pr, 2pr+1) of point p;
-    // columns past K get zeros
-    for (int t = c.tid; t < 32 * NW; t += NT) {
-      const int w = t >> 5, lane = t & 31;
-      for (int line = w; line < X::ACT_FWD; line += NW) {
-        const int p = line / 3, pr = line % 3;
-        const int ca = 2 * pr, cb = 2 * pr + 1;
-        const Cplx<T>* L = sm + line * N;
-        for (int k = lane; k < g.KXP; k += 32) {
-          Cplx<T> a = czero<T>(), b = czero<T>();
-          if (k < KX1) {
-            const Cplx<T> zk = L[lidx<T>(k)];
-            const Cplx<T> zc = conj(L[lidx<T>((N - k) % N)]);
-            const Cplx<T> sp = zk + zc, sd = zk - zc;
-            a = cmk<T>(sp.x * T(0.5), sp.y * T(0.5));
-            b = cmk<T>(sd.y * T(0.5), -sd.x * T(0.5));
-          }
-          if (ca < nout) B[idxB(g, ca, z, y0 + p, k)] = a;
-          if (cb < nout) B[idxB(g, cb, z, y0 + p, k)] = b;
-        }
-      }
-    }
-    GBGHT_SYNC();   // the lines are rewritten by the next tile's inverse
-  }
+  // Two tiles per CTA, written out rather than looped (a loop around the tile makes the compiler
+  // keep the tile's index arithmetic live across iterations, and the kernel spills): tile bx, then
+  // tile bx + grid, whose spectra are copied in while the first is transformed.
+  const int t0 = c.bx, t1 = c.bx + grid;
+  if (t0 >= ntiles) return;
+  stage.issue(c, t0 / tiles_y, P * (t0 % tiles_y));
+  stage.wait(0u);
+  x_tile<T, N, NT>(c, sm, stage, src, g, B, nout, t0 / tiles_y, P * (t0 % tiles_y), t1 < ntiles ? t1 / tiles_y : -1,
+                   t1 < ntiles ? P * (t1 % tiles_y) : 0, tw);
+  if (t1 >= ntiles) return;
+  stage.wait(1u);
+  x_tile<T, N, NT>(c, sm, stage, src, g, B, nout, t1 / tiles_y, P * (t1 % tiles_y), -1, 0, tw);
 }
 
 // Source of the deposit's inverse: line p (p < PV) = u_x + i·u_y of point p; line PV + h =
