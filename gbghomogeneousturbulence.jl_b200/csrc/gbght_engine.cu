@@ -631,7 +631,7 @@ class EngineImpl final : public Engine {
     using X = XShape<T>;
     const int KXS = x_kxs(g_.K, int(sizeof(Cplx<T>)));
     const int ntiles = (N / X::P) * N;
-    const int grid = (ntiles + 1) / 2;   // two tiles per CTA
+    const int grid = (ntiles + XT - 1) / XT;   // XT tiles per CTA
 #ifdef GBGHT_EMU
     emu_grid(grid, 1, 1, smem_x(), [&](const Cta& c, void* sm) {
       Cplx<T>* t = static_cast<Cplx<T>*>(sm);

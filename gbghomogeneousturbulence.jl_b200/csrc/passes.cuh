@@ -340,6 +340,25 @@ GBGHT_HD void x_tile(const Cta& c, Cplx<T>* sm, const XStaging<T, XShape<T>::P>&
   GBGHT_SYNC();   // the lines are rewritten by the next tile's inverse
 }
 
+// Tiles I, I+1, … < XT of this CTA (tile index bx + i·grid); tile I's spectra are already being
+// copied into the staging rows.
+constexpr int XT = 4;
+template <class T, int N, int NT, int I>
+GBGHT_HD void x_tile_chain(const Cta& c, Cplx<T>* sm, const XStaging<T, XShape<T>::P>& stage,
+                           const XStagedSource<T, N, XShape<T>::P>& src, const Geometry& g, Cplx<T>* B, int nout,
+                           int grid, int ntiles, const Cplx<T>* tw) {
+  if constexpr (I < XT) {
+    constexpr int P = XShape<T>::P;
+    const int tiles_y = N / P;
+    const int t = c.bx + I * grid, tn = t + grid;
+    const bool more = I + 1 < XT && tn < ntiles;
+    stage.wait(uint32_t(I & 1));
+    x_tile<T, N, NT>(c, sm, stage, src, g, B, nout, t / tiles_y, P * (t % tiles_y), more ? tn / tiles_y : -1,
+                     more ? P * (tn % tiles_y) : 0, tw);
+    if (more) x_tile_chain<T, N, NT, I + 1>(c, sm, stage, src, g, B, nout, grid, ntiles, tw);
+  }
+}
+
 // The x pass over the tiles bx, bx + grid, …: one warp per line, lines at sm + l·N, the next
 // tile's spectra prefetched into the staging rows while the current tile is transformed.
 template <class T, int N, int NT>
@@ -352,18 +371,13 @@ GBGHT_HD void body_x_products(const Cta& c, Cplx<T>* sm, Cplx<T>* stg, int KXS, 
   const int tiles_y = N / P, ntiles = tiles_y * N;
   const XStaging<T, P> stage{g, B, stg, KXS, nin, bar, status};
   const XStagedSource<T, N, P> src{g, stg, KXS, has_scalar, T(g.inv_norm)};
-  // Two tiles per CTA, written out rather than looped (a loop around the tile makes the compiler
-  // keep the tile's index arithmetic live across iterations, and the kernel spills): tile bx, then
-  // tile bx + grid, whose spectra are copied in while the first is transformed.
-  const int t0 = c.bx, t1 = c.bx + grid;
-  if (t0 >= ntiles) return;
-  stage.issue(c, t0 / tiles_y, P * (t0 % tiles_y));
-  stage.wait(0u);
-  x_tile<T, N, NT>(c, sm, stage, src, g, B, nout, t0 / tiles_y, P * (t0 % tiles_y), t1 < ntiles ? t1 / tiles_y : -1,
-                   t1 < ntiles ? P * (t1 % tiles_y) : 0, tw);
-  if (t1 >= ntiles) return;
-  stage.wait(1u);
-  x_tile<T, N, NT>(c, sm, stage, src, g, B, nout, t1 / tiles_y, P * (t1 % tiles_y), -1, 0, tw);
+  // XT tiles per CTA, written out by template recursion rather than looped (a loop around the
+  // tile makes the compiler keep the tile's index arithmetic live across iterations, and the
+  // kernel spills): tile bx + i·grid, with the spectra of tile i + 1 copied in while tile i is
+  // transformed.
+  if (c.bx >= ntiles) return;
+  stage.issue(c, c.bx / tiles_y, P * (c.bx % tiles_y));
+  x_tile_chain<T, N, NT, 0>(c, sm, stage, src, g, B, nout, grid, ntiles, tw);
 }
 
 // Source of the deposit's inverse: line p (p < PV) = u_x + i·u_y of point p; line PV + h =
