@@ -342,7 +342,7 @@ GBGHT_HD void x_tile(const Cta& c, Cplx<T>* sm, const XStaging<T, XShape<T>::P>&
 
 // Tiles I, I+1, … < XT of this CTA (tile index bx + i·grid); tile I's spectra are already being
 // copied into the staging rows.
-constexpr int XT = 4;
+constexpr int XT = 2;
 template <class T, int N, int NT, int I>
 GBGHT_HD void x_tile_chain(const Cta& c, Cplx<T>* sm, const XStaging<T, XShape<T>::P>& stage,
                            const XStagedSource<T, N, XShape<T>::P>& src, const Geometry& g, Cplx<T>* B, int nout,
