@@ -345,6 +345,8 @@ def ours(args):
             livep = P64 > 1e-6 * P64.max()
             line["forms"] = {"fp32_mixed": {"value": round(mv, 4), "unit": "steps/s",
                                             "ratio_vs_fp64": round(mv / value, 3),
+                                            "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)}
+                                                        for k, v in m["prof"].items() if v[0]},
                                             "clocks": m["clocks"],
                                             "spectrum_rel_err_after_K_steps": float(np.max(np.abs(E32[live] - E64[live]) / E64[live])),
                                             "scalar_spectrum_rel_err_after_K_steps": float(np.max(np.abs(P32[livep] - P64[livep]) / P64[livep]))}}
