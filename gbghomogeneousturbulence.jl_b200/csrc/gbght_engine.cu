@@ -62,7 +62,6 @@ static const char* rt_check() { return cuda_err(cudaGetLastError(), "kernel laun
 template <class T> struct Shape {
   static constexpr int TLY = 128 / int(sizeof(Cplx<T>));   // y passes: 128-byte rows
   static constexpr int TLZ = 64 / int(sizeof(Cplx<T>));    // z epilogue: 64-byte rows
-  static constexpr int TLZW = sizeof(T) == 8 ? 4 : 8;      // warp-per-line z epilogue: lines per CTA
 };
 constexpr int clamp_nt(int v) { return v < 64 ? 64 : (v > 256 ? 256 : v); }
 
@@ -102,12 +101,6 @@ template <class T, int N>
 class EngineImpl final : public Engine {
   static constexpr int TLY = Shape<T>::TLY;
   static constexpr int TLZ = Shape<T>::TLZ;
-  static constexpr int TLZW = Shape<T>::TLZW;
-#ifdef GBGHT_EMU
-  static constexpr int NTZW = 1;
-#else
-  static constexpr int NTZW = 32 * TLZW;
-#endif
   static constexpr int NTY = kNT(N * TLY / 8);
   static constexpr int NTX = kNT(N);            // (unused by the warp-per-line x passes)
 #ifdef GBGHT_EMU
@@ -153,7 +146,7 @@ class EngineImpl final : public Engine {
     nA_ = size_t(N) * g_.NY2 * g_.KXP;
     nB_ = size_t(N) * N * g_.KXP;
     nP_ = size_t(N) * N * N;
-    ntile_ = std::max((g_.KXP / TLZ) * g_.NY2, (g_.KXP / TLZW) * g_.NY2);
+    ntile_ = (g_.KXP / TLZ) * g_.NY2;
     nshell_ = int(std::floor(std::sqrt(3.0) * N / 2.0 + 0.5)) + 1;
 #ifndef GBGHT_EMU
     const char* e = cuda_err(cudaSetDevice(p.device), "cudaSetDevice");
@@ -542,9 +535,6 @@ class EngineImpl final : public Engine {
            size_t(7) * XShape<T>::P * x_kxs(g_.K, int(sizeof(Cplx<T>))) * sizeof(Cplx<T>) + kBarBytes;
   }
   size_t smem_xv() const { return size_t(N) * XShape<T>::ACT_V * sizeof(Cplx<T>) + size_t(NTXV) * sizeof(double); }
-  size_t smem_zw() const {
-    return (size_t(N) * TLZW + 3 * size_t(g_.NY2) * TLZW) * sizeof(Cplx<T>) + size_t(32) * TLZW * sizeof(double);
-  }
   size_t smem_z() const {
     return (size_t(N) * TLZ + 3 * size_t(g_.NY2) * TLZ) * sizeof(Cplx<T>) + size_t(NTZ) * sizeof(double);
   }
@@ -561,7 +551,6 @@ class EngineImpl final : public Engine {
     set(reinterpret_cast<const void*>(k_x_products<T, N, NTXP>), smem_x());
     set(reinterpret_cast<const void*>(k_x_velocity<T, N, NTXV>), smem_xv());
     set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ>), smem_z());
-    set(reinterpret_cast<const void*>(k_z_epilogue_w<T, N, TLZW, NTZW>), smem_zw());
     set(reinterpret_cast<const void*>(k_z_init<T, N, TLZ, NTZ>), smem_z());
     return e;
   }
@@ -674,18 +663,18 @@ class EngineImpl final : public Engine {
 #endif
   }
   void z_epilogue(const StageArgs& st) {
-    const int gx = g_.KXP / TLZW;
 #ifdef GBGHT_EMU
-    emu_grid(gx, g_.NY2, 1, smem_zw(), [&](const Cta& c, void* sm) {
-      Cplx<T>* LB = static_cast<Cplx<T>*>(sm);
-      Cplx<T>* Rt = LB + N * TLZW;
-      double* red = reinterpret_cast<double*>(Rt + 3 * g_.NY2 * TLZW);
-      partial_[c.by * gx + c.bx] = body_z_epilogue_w<T, N, TLZW, 1>(c, LB, Rt, red, g_, A_, S_, H_, st, amp_, tw_);
+    const int gx = g_.KXP / TLZ;
+    emu_grid(gx, g_.NY2, 1, smem_z(), [&](const Cta& c, void* sm) {
+      Cplx<T>* W = static_cast<Cplx<T>*>(sm);
+      Cplx<T>* Rt = W + N * TLZ;
+      double* red = reinterpret_cast<double*>(Rt + 3 * g_.NY2 * TLZ);
+      partial_[c.by * gx + c.bx] = body_z_epilogue<T, N, TLZ, 1>(c, W, Rt, red, g_, A_, S_, H_, st, amp_, tw_);
     });
 #else
     pbegin(PROF_Z_EPILOGUE);
-    k_z_epilogue_w<T, N, TLZW, NTZW><<<dim3(gx, g_.NY2, 1), NTZW, smem_zw(), stream_>>>(g_, A_, S_, H_, st, amp_,
-                                                                                         partial_, tw_);
+    k_z_epilogue<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, S_, H_, st, amp_,
+                                                                                           partial_, tw_);
     pend();
 #endif
   }

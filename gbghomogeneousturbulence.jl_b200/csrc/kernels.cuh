@@ -112,17 +112,6 @@ __global__ void __launch_bounds__(NT, 2) k_z_epilogue(Geometry g, Cplx<T>* A, Cp
 }
 
 template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT, 2) k_z_epilogue_w(Geometry g, Cplx<T>* A, Cplx<T>* S, Cplx<T>* H, StageArgs st,
-                                                        const double* amp, double* partial, const Cplx<T>* tw) {
-  CTA_CTX;
-  Cplx<T>* LB = reinterpret_cast<Cplx<T>*>(g_smem);
-  Cplx<T>* Rt = LB + N * TL;
-  double* red = reinterpret_cast<double*>(Rt + 3 * g.NY2 * TL);
-  const double e = body_z_epilogue_w<T, N, TL, NT>(c, LB, Rt, red, g, A, S, H, st, amp, tw);
-  if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
-}
-
-template <class T, int N, int TL, int NT>
 __global__ void __launch_bounds__(NT, 2) k_z_init(Geometry g, Cplx<T>* A, const Cplx<T>* S, int has_scalar, double* partial,
                                                   const Cplx<T>* tw, int vorticity = 1) {
   CTA_CTX;

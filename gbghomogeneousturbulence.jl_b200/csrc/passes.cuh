@@ -692,218 +692,6 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* r
 }
 
 // ================================================================================================
-// The same z-forward + epilogue + z-inverse with one warp per z-line: a CTA holds TL lines (the
-// columns kx0..kx0+TL−1 of row ky' = qy), warp w owns column kx0 + w from its six forward
-// transforms through its seven inverse ones, and the only block-wide barrier is the final
-// reduction of the energy partial. Line buffers at LB + w·N (swizzled, warp_fft.cuh); retained
-// spectra at Rt[(j·TL + w)·NY2 + q]. Grid: (KXP/TL, NY2), NT = 32·TL threads.
-// ================================================================================================
-template <class T, int N>
-struct ZColumnSource {
-  static constexpr bool kExternal = true;
-  const Geometry& g;
-  const Cplx<T>* A;
-  int slot, qy, kx;
-  GBGHT_HD Cplx<T> load(int e) const { return A[idxA(g, slot, e, qy, kx)]; }
-};
-template <class T, int N>
-struct ZColumnSink {
-  const Geometry& g;
-  Cplx<T>* A;
-  int slot, qy, kx;
-  GBGHT_HD void store(int e, Cplx<T> v) const { A[idxA(g, slot, e, qy, kx)] = v; }
-};
-template <class T, int N>
-struct ZRetainedColumn {
-  const Geometry& g;
-  Cplx<T>* R;   // NY2 values of this column
-  GBGHT_HD void store(int e, Cplx<T> v) const {
-    if (e <= g.K) R[e] = v;
-    else if (e >= N - g.K) R[e - N + g.NY2] = v;
-  }
-};
-template <class T, int N, class F>
-struct ZRetainedValues {
-  static constexpr bool kExternal = true;
-  const Geometry& g;
-  F value;
-  GBGHT_HD Cplx<T> load(int e) const {
-    if (e <= g.K) return value(e);
-    if (e >= N - g.K) return value(e - N + g.NY2);
-    return czero<T>();
-  }
-};
-
-template <class T, int N, int TL, int NT>
-GBGHT_HD double body_z_epilogue_w(const Cta& c, Cplx<T>* LB, Cplx<T>* Rt, double* red, const Geometry& g,
-                                  Cplx<T>* GBGHT_RESTRICT A, Cplx<T>* GBGHT_RESTRICT S, Cplx<T>* GBGHT_RESTRICT H,
-                                  const StageArgs& st, const double* GBGHT_RESTRICT force_amp,
-                                  const Cplx<T>* GBGHT_RESTRICT tw) {
-  const int kx0 = c.bx * TL, qy = c.by;
-  const int NY2 = g.NY2;
-  const double s = g.s;
-  const double ky = s * double(q_to_m(qy, g.K, NY2));
-  const auto lines = [&](int l) { return LB + l * N; };
-  const auto ret = [&](int j, int l) { return Rt + (j * TL + l) * NY2; };
-  auto forward3 = [&](int c0) {
-    for (int j = 0; j < 3; ++j) {
-      const auto src = [&](int l) { return ZColumnSource<T, N>{g, A, c0 + j, qy, kx0 + l}; };
-      const auto dst = [&](int l) { return ZRetainedColumn<T, N>{g, ret(j, l)}; };
-      warp_fft_lines<T, N, TL, NT, -1>(c, TL, lines, src, dst, tw);
-    }
-  };
-  double esum[(32 * TL + NT - 1) / NT] = {};
-  // ---------------- scalar -------------------------------------------------------------------------
-  if (st.has_scalar) {
-    forward3(3);
-    for (int t = c.tid; t < 32 * TL; t += NT) {
-      const int l = t >> 5, lane = t & 31, kx = kx0 + l;
-      const double kxd = s * double(kx);
-      for (int q = lane; q < NY2; q += 32) {
-        const double kzd = s * double(q_to_m(q, g.K, NY2));
-        const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
-        const bool keep = kx <= g.K && k2 <= g.cut2;
-        const size_t si = idxS(g, 3, qy, q, kx);
-        Cplx<T> phi = S[si];
-        Cplx<T> nphi = czero<T>();
-        if (keep) {
-          const Cplx<T> fx = ret(0, l)[q], fy = ret(1, l)[q], fz = ret(2, l)[q];
-          const Cplx<T> dsum = cmk<T>(T(kxd) * fx.x + T(ky) * fy.x + T(kzd) * fz.x,
-                                      T(kxd) * fx.y + T(ky) * fy.y + T(kzd) * fz.y);
-          nphi = mul_mi(dsum);
-        }
-        if (st.G[0] != 0.0 || st.G[1] != 0.0 || st.G[2] != 0.0) {
-          const Cplx<T> ux = S[idxS(g, 0, qy, q, kx)], uy = S[idxS(g, 1, qy, q, kx)], uz = S[idxS(g, 2, qy, q, kx)];
-          const T G0 = T(st.G[0]), G1 = T(st.G[1]), G2 = T(st.G[2]);
-          nphi = nphi - cmk<T>(G0 * ux.x + G1 * uy.x + G2 * uz.x, G0 * ux.y + G1 * uy.y + G2 * uz.y);
-        }
-        Cplx<T> h = st.first ? scale(nphi, T(st.dt)) : scale(H[si], T(st.a)) + scale(nphi, T(st.dt));
-        const T E = T(exp(st.cphi * k2));
-        phi = scale(phi + scale(h, T(st.b)), E);
-        S[si] = phi;
-        if (!st.last) H[si] = scale(h, E);
-        ret(0, l)[q] = phi;
-      }
-    }
-    warp_sync();
-    const auto src = [&](int l) {
-      const Cplx<T>* R0 = ret(0, l);
-      const auto val = [R0](int q) { return R0[q]; };
-      return ZRetainedValues<T, N, decltype(val)>{g, val};
-    };
-    const auto dst = [&](int l) { return ZColumnSink<T, N>{g, A, 6, qy, kx0 + l}; };
-    warp_fft_lines<T, N, TL, NT, +1>(c, TL, lines, src, dst, tw);
-  }
-  // ---------------- velocity -----------------------------------------------------------------------
-  forward3(0);
-  const double A_f = st.forced ? force_amp[0] : 0.0;
-  for (int t = c.tid; t < 32 * TL; t += NT) {
-    const int l = t >> 5, lane = t & 31, kx = kx0 + l;
-    const double kxd = s * double(kx);
-    double acc = 0.0;
-    for (int q = lane; q < NY2; q += 32) {
-      const double kzd = s * double(q_to_m(q, g.K, NY2));
-      const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
-      const bool keep = kx <= g.K && k2 <= g.cut2;
-      const size_t s0 = idxS(g, 0, qy, q, kx), s1 = idxS(g, 1, qy, q, kx), s2 = idxS(g, 2, qy, q, kx);
-      Cplx<T> u0 = S[s0], u1 = S[s1], u2 = S[s2];
-      Cplx<T> n0 = czero<T>(), n1 = czero<T>(), n2 = czero<T>();
-      const T kX = T(kxd), kY = T(ky), kZ = T(kzd);
-      if (keep && k2 > 0.0) {
-        const Cplx<T> f0 = ret(0, l)[q], f1 = ret(1, l)[q], f2 = ret(2, l)[q];
-        const T ik2 = T(1.0 / k2);
-        const Cplx<T> kd = cmk<T>((kX * f0.x + kY * f1.x + kZ * f2.x) * ik2, (kX * f0.y + kY * f1.y + kZ * f2.y) * ik2);
-        n0 = f0 - scale(kd, kX);
-        n1 = f1 - scale(kd, kY);
-        n2 = f2 - scale(kd, kZ);
-      }
-      if (A_f != 0.0 && k2 >= st.band_lo2 && k2 <= st.band_hi2) {
-        const T Af = T(A_f);
-        n0 = n0 + scale(u0, Af);
-        n1 = n1 + scale(u1, Af);
-        n2 = n2 + scale(u2, Af);
-      }
-      const T dt = T(st.dt), a = T(st.a), b = T(st.b);
-      Cplx<T> h0, h1, h2;
-      if (st.first) {
-        h0 = scale(n0, dt); h1 = scale(n1, dt); h2 = scale(n2, dt);
-      } else {
-        h0 = scale(H[s0], a) + scale(n0, dt);
-        h1 = scale(H[s1], a) + scale(n1, dt);
-        h2 = scale(H[s2], a) + scale(n2, dt);
-      }
-      const T E = T(exp(st.cu * k2));
-      u0 = scale(u0 + scale(h0, b), E);
-      u1 = scale(u1 + scale(h1, b), E);
-      u2 = scale(u2 + scale(h2, b), E);
-      if (st.last) {
-        if (k2 > 0.0) {
-          const T ik2 = T(1.0 / k2);
-          const Cplx<T> kd = cmk<T>((kX * u0.x + kY * u1.x + kZ * u2.x) * ik2, (kX * u0.y + kY * u1.y + kZ * u2.y) * ik2);
-          u0 = u0 - scale(kd, kX);
-          u1 = u1 - scale(kd, kY);
-          u2 = u2 - scale(kd, kZ);
-        }
-      } else {
-        H[s0] = scale(h0, E);
-        H[s1] = scale(h1, E);
-        H[s2] = scale(h2, E);
-      }
-      S[s0] = u0;
-      S[s1] = u1;
-      S[s2] = u2;
-      ret(0, l)[q] = u0;
-      ret(1, l)[q] = u1;
-      ret(2, l)[q] = u2;
-      const double w = kx == 0 ? 1.0 : 2.0;
-      acc += w * ((double(u0.x) * u0.x + double(u0.y) * u0.y) + (double(u1.x) * u1.x + double(u1.y) * u1.y) +
-                  (double(u2.x) * u2.x + double(u2.y) * u2.y));
-    }
-    esum[(t - c.tid) / NT] = acc;
-  }
-  warp_sync();
-  for (int o = 0; o < 3; ++o) {
-    const auto src = [&](int l) {
-      const Cplx<T>* Ro = ret(o, l);
-      const auto val = [Ro](int q) { return Ro[q]; };
-      return ZRetainedValues<T, N, decltype(val)>{g, val};
-    };
-    const auto dst = [&](int l) { return ZColumnSink<T, N>{g, A, o, qy, kx0 + l}; };
-    warp_fft_lines<T, N, TL, NT, +1>(c, TL, lines, src, dst, tw);
-  }
-  for (int o = 0; o < 3; ++o) {
-    const auto src = [&](int l) {
-      const Cplx<T>* R0 = ret(0, l);
-      const Cplx<T>* R1 = ret(1, l);
-      const Cplx<T>* R2 = ret(2, l);
-      const int kx = kx0 + l;
-      const int K = g.K, NY2v = NY2;
-      const double sv = s;
-      const T kX = T(sv * double(kx)), kY = T(ky);
-      const auto val = [=](int q) {
-        const T kZ = T(sv * double(q <= K ? q : q - NY2v));
-        const Cplx<T> u0 = R0[q], u1 = R1[q], u2 = R2[q];
-        Cplx<T> cr;
-        if (o == 0) cr = scale(u2, kY) - scale(u1, kZ);
-        else if (o == 1) cr = scale(u0, kZ) - scale(u2, kX);
-        else cr = scale(u1, kX) - scale(u0, kY);
-        return mul_i(cr);
-      };
-      return ZRetainedValues<T, N, decltype(val)>{g, val};
-    };
-    const auto dst = [&](int l) { return ZColumnSink<T, N>{g, A, 3 + o, qy, kx0 + l}; };
-    warp_fft_lines<T, N, TL, NT, +1>(c, TL, lines, src, dst, tw);
-  }
-  // the tile's energy partial: per-thread sums, then added in thread order
-  for (int t = c.tid; t < 32 * TL; t += NT) red[t] = esum[(t - c.tid) / NT];
-  GBGHT_SYNC();
-  double total = 0.0;
-  if (c.tid == 0)
-    for (int i = 0; i < 32 * TL; ++i) total += red[i];
-  return total;
-}
-
-// ================================================================================================
 // Reality projection of the kx = 0 plane of S slots [0, ncomp) (src/Propagator.jl:411-412): each
 // pair (m_y, m_z) ↔ (−m_y, −m_z) is replaced by its Hermitian part. One thread per compact mode;
 // the member with the smaller flat index writes both. Grid covers NY2·NY2 threads.
