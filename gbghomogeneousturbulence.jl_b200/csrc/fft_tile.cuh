@@ -18,24 +18,28 @@
 // `tw` holds e^(-2πi k/N) for k in [0, N), computed on the host in extended precision.
 #pragma once
 
+#include <type_traits>
+
 #include "gbght_common.cuh"
 
 namespace gbght {
 
-// Radix plans, innermost stage first. Every supported N is 2^a·3^b.
+// Radix plans, innermost stage first. Every supported N is 2^a·3^b. Every plan starts and ends
+// with the same radix, so the rows a thread writes in a forward transform's last stage are the rows
+// it reads in an inverse transform's first stage (the z epilogue keeps them in registers).
 template <int N> struct Radices;
 template <> struct Radices<8>   { static constexpr int n = 1; static constexpr int r[1] = {8}; };
-template <> struct Radices<12>  { static constexpr int n = 2; static constexpr int r[2] = {3, 4}; };
+template <> struct Radices<12>  { static constexpr int n = 3; static constexpr int r[3] = {2, 3, 2}; };
 template <> struct Radices<16>  { static constexpr int n = 2; static constexpr int r[2] = {4, 4}; };
-template <> struct Radices<24>  { static constexpr int n = 2; static constexpr int r[2] = {3, 8}; };
-template <> struct Radices<32>  { static constexpr int n = 2; static constexpr int r[2] = {4, 8}; };
-template <> struct Radices<48>  { static constexpr int n = 3; static constexpr int r[3] = {3, 4, 4}; };
+template <> struct Radices<24>  { static constexpr int n = 4; static constexpr int r[4] = {2, 3, 2, 2}; };
+template <> struct Radices<32>  { static constexpr int n = 3; static constexpr int r[3] = {4, 2, 4}; };
+template <> struct Radices<48>  { static constexpr int n = 3; static constexpr int r[3] = {4, 3, 4}; };
 template <> struct Radices<64>  { static constexpr int n = 2; static constexpr int r[2] = {8, 8}; };
-template <> struct Radices<96>  { static constexpr int n = 3; static constexpr int r[3] = {3, 4, 8}; };
-template <> struct Radices<128> { static constexpr int n = 3; static constexpr int r[3] = {2, 8, 8}; };
-template <> struct Radices<192> { static constexpr int n = 3; static constexpr int r[3] = {3, 8, 8}; };
-template <> struct Radices<256> { static constexpr int n = 3; static constexpr int r[3] = {4, 8, 8}; };
-template <> struct Radices<384> { static constexpr int n = 4; static constexpr int r[4] = {3, 2, 8, 8}; };
+template <> struct Radices<96>  { static constexpr int n = 4; static constexpr int r[4] = {4, 3, 2, 4}; };
+template <> struct Radices<128> { static constexpr int n = 3; static constexpr int r[3] = {8, 2, 8}; };
+template <> struct Radices<192> { static constexpr int n = 3; static constexpr int r[3] = {8, 3, 8}; };
+template <> struct Radices<256> { static constexpr int n = 3; static constexpr int r[3] = {8, 4, 8}; };
+template <> struct Radices<384> { static constexpr int n = 4; static constexpr int r[4] = {8, 2, 3, 8}; };
 template <> struct Radices<512> { static constexpr int n = 3; static constexpr int r[3] = {8, 8, 8}; };
 
 template <int N> constexpr int stage_ns(int s) {
@@ -138,6 +142,14 @@ GBGHT_HD void twiddles(const Cplx<T>* GBGHT_RESTRICT tw, int k, Cplx<T>* w) {
   }
 }
 
+// A source or sink with kIndexed = true is called as load_rb(e, l, r, b) / store_rb(e, l, v, r, b),
+// with the radix index r and the thread's butterfly slot b as compile-time constants after
+// unrolling, so it can keep values in a per-thread register array.
+template <class F, class = void>
+struct is_indexed : std::false_type {};
+template <class F>
+struct is_indexed<F, std::void_t<decltype(F::kIndexed)>> : std::bool_constant<F::kIndexed> {};
+
 // The tile buffer as the default source of the first stage and sink of the last one.
 template <class T, int TL, bool SWZ>
 struct TileBuf {
@@ -171,8 +183,12 @@ GBGHT_HD void tile_fft_io(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTR
       if ((BPT * NT == TOT || idx < TOT) && (ACT == TL || l < ACT)) {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          if constexpr (FIRST) v[b][r] = src.load(j + r * NB, l);
-          else v[b][r] = buf[tix<TL, SWZ>(j + r * NB, l)];
+          if constexpr (FIRST) {
+            if constexpr (is_indexed<Src>::value) v[b][r] = src.load_rb(j + r * NB, l, r, b);
+            else v[b][r] = src.load(j + r * NB, l);
+          } else {
+            v[b][r] = buf[tix<TL, SWZ>(j + r * NB, l)];
+          }
         }
       }
     }
@@ -193,8 +209,12 @@ GBGHT_HD void tile_fft_io(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTR
         const int base = (j / NS) * NS * R + jm;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          if constexpr (LAST) dst.store(base + r * NS, l, v[b][r]);
-          else buf[tix<TL, SWZ>(base + r * NS, l)] = v[b][r];
+          if constexpr (LAST) {
+            if constexpr (is_indexed<Dst>::value) dst.store_rb(base + r * NS, l, v[b][r], r, b);
+            else dst.store(base + r * NS, l, v[b][r]);
+          } else {
+            buf[tix<TL, SWZ>(base + r * NS, l)] = v[b][r];
+          }
         }
       }
     }

@@ -142,6 +142,7 @@ class EngineImpl final : public Engine {
     g_.KXP = ((g_.K + 1 + TLY - 1) / TLY) * TLY;
     g_.inv_norm = 1.0 / (double(N) * double(N) * double(N));
     if (g_.NY2 > N) return "grid too small for the retained band";
+    if (g_.K > ZOwn<T, N, TLZ, NTZ>::KMAX) return "retained band wider than the z tile's row slots";
     nS_ = size_t(g_.NY2) * g_.NY2 * g_.KXP;
     nA_ = size_t(N) * g_.NY2 * g_.KXP;
     nB_ = size_t(N) * N * g_.KXP;
@@ -536,7 +537,7 @@ class EngineImpl final : public Engine {
   }
   size_t smem_xv() const { return size_t(N) * XShape<T>::ACT_V * sizeof(Cplx<T>) + size_t(NTXV) * sizeof(double); }
   size_t smem_z() const {
-    return (size_t(N) * TLZ + 3 * size_t(g_.NY2) * TLZ) * sizeof(Cplx<T>) + size_t(NTZ) * sizeof(double);
+    return size_t(N) * TLZ * sizeof(Cplx<T>) + size_t(NTZ) * sizeof(double) + 16;
   }
 
 #ifndef GBGHT_EMU
@@ -667,9 +668,9 @@ class EngineImpl final : public Engine {
     const int gx = g_.KXP / TLZ;
     emu_grid(gx, g_.NY2, 1, smem_z(), [&](const Cta& c, void* sm) {
       Cplx<T>* W = static_cast<Cplx<T>*>(sm);
-      Cplx<T>* Rt = W + N * TLZ;
-      double* red = reinterpret_cast<double*>(Rt + 3 * g_.NY2 * TLZ);
-      partial_[c.by * gx + c.bx] = body_z_epilogue<T, N, TLZ, 1>(c, W, Rt, red, g_, A_, S_, H_, st, amp_, tw_);
+      double* red = reinterpret_cast<double*>(W + N * TLZ);
+      ZRowsReg<T, ZOwn<T, N, TLZ, 1>> rows;
+      partial_[c.by * gx + c.bx] = body_z_epilogue<T, N, TLZ, 1>(c, W, red, g_, rows, A_, S_, H_, st, amp_, tw_);
     });
 #else
     pbegin(PROF_Z_EPILOGUE);
@@ -683,9 +684,9 @@ class EngineImpl final : public Engine {
     const int gx = g_.KXP / TLZ;
     emu_grid(gx, g_.NY2, 1, smem_z(), [&](const Cta& c, void* sm) {
       Cplx<T>* W = static_cast<Cplx<T>*>(sm);
-      Cplx<T>* Rt = W + N * TLZ;
-      double* red = reinterpret_cast<double*>(Rt + 3 * g_.NY2 * TLZ);
-      partial_[c.by * gx + c.bx] = body_z_init<T, N, TLZ, 1>(c, W, Rt, red, g_, A_, S_, p_.scalar, tw_);
+      double* red = reinterpret_cast<double*>(W + N * TLZ);
+      ZRowsReg<T, ZOwn<T, N, TLZ, 1>> rows;
+      partial_[c.by * gx + c.bx] = body_z_init<T, N, TLZ, 1>(c, W, red, g_, rows, A_, S_, p_.scalar, tw_);
     });
 #else
     k_z_init<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, S_, p_.scalar, partial_,

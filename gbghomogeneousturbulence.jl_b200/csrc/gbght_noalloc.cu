@@ -197,7 +197,7 @@ int run_n(const Layout& o, unsigned char* base, const double* u_hat, double* u, 
   const size_t nref = size_t(3) * N * N * (N / 2 + 1);
   k_compact_reference<<<unsigned((nref + 255) / 256), 256, 0, st>>>(g, reinterpret_cast<const Cplx<double>*>(u_hat),
                                                                   S, flag);
-  const size_t smem_z = (size_t(N) * TLZ + 3 * size_t(g.NY2) * TLZ) * sizeof(Cplx<double>) + size_t(NTZ) * sizeof(double);
+  const size_t smem_z = size_t(N) * TLZ * sizeof(Cplx<double>) + size_t(NTZ) * sizeof(double) + 16;
   gbght::k_z_init<double, N, TLZ, NTZ><<<dim3(g.KXP / TLZ, g.NY2, 1), NTZ, smem_z, st>>>(g, A, S, 0, partial, tw, 0);
   const size_t smem_y = size_t(N) * TLY * sizeof(Cplx<double>) + 32;
   gbght::k_y_inverse<double, N, TLY, NTY><<<dim3(g.KXP / TLY, N, 3), NTY, smem_y, st>>>(maps, g, 0, tw, flag);

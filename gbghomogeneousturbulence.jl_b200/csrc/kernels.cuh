@@ -100,14 +100,43 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_x_velocity(Geome
   if (c.tid == 0) atomicMax(maxbits, static_cast<unsigned long long>(__double_as_longlong(mx)));
 }
 
+// The owned rows of a z tile (ZOwn) live in TMEM where every warp is fully active in every
+// stage, else in registers. `run(rows)` runs the body between the allocation and the release.
+// `slot` is 4 bytes of shared memory for the allocation's address.
+template <class T, int N, int TL, int NT, class F>
+__device__ __forceinline__ double with_z_rows(uint32_t* slot, const F& run) {
+  using O = ZOwn<T, N, TL, NT>;
+  using Sh = ZTmemShape<T, N, O, NT>;
+  if constexpr (Sh::kUse) {
+    const int warp = int(threadIdx.x) >> 5;
+    if (warp == 0) tmem_alloc(slot, Sh::NCOLS);
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const uint32_t base = *slot + (uint32_t((warp & 3) * 32) << 16) + uint32_t((warp >> 2) * Sh::COLS);
+    ZRowsTmem<T, O> rows{base};
+    const double e = run(rows);
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    if (warp == 0) tmem_dealloc(*slot, Sh::NCOLS);
+    return e;
+  } else {
+    ZRowsReg<T, O> rows;
+    return run(rows);
+  }
+}
+
 template <class T, int N, int TL, int NT>
 __global__ void __launch_bounds__(NT, 2) k_z_epilogue(Geometry g, Cplx<T>* A, Cplx<T>* S, Cplx<T>* H, StageArgs st,
                                                       const double* amp, double* partial, const Cplx<T>* tw) {
   CTA_CTX;
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
-  Cplx<T>* Rt = W + N * TL;
-  double* red = reinterpret_cast<double*>(Rt + 3 * g.NY2 * TL);
-  const double e = body_z_epilogue<T, N, TL, NT>(c, W, Rt, red, g, A, S, H, st, amp, tw);
+  double* red = reinterpret_cast<double*>(W + N * TL);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(red + NT);
+  const double e = with_z_rows<T, N, TL, NT>(slot, [&](auto& rows) {
+    return body_z_epilogue<T, N, TL, NT>(c, W, red, g, rows, A, S, H, st, amp, tw);
+  });
   if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
 }
 
@@ -116,9 +145,11 @@ __global__ void __launch_bounds__(NT, 2) k_z_init(Geometry g, Cplx<T>* A, const 
                                                   const Cplx<T>* tw, int vorticity = 1) {
   CTA_CTX;
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
-  Cplx<T>* Rt = W + N * TL;
-  double* red = reinterpret_cast<double*>(Rt + 3 * g.NY2 * TL);
-  const double e = body_z_init<T, N, TL, NT>(c, W, Rt, red, g, A, S, has_scalar, tw, vorticity);
+  double* red = reinterpret_cast<double*>(W + N * TL);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(red + NT);
+  const double e = with_z_rows<T, N, TL, NT>(slot, [&](auto& rows) {
+    return body_z_init<T, N, TL, NT>(c, W, red, g, rows, A, S, has_scalar, tw, vorticity);
+  });
   if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
 }
 template <class T>

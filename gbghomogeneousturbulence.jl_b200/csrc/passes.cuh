@@ -22,6 +22,7 @@
 
 #include "fft_tile.cuh"
 #include "tma.cuh"
+#include "tmem.cuh"
 #include "warp_fft.cuh"
 
 namespace gbght {
@@ -460,8 +461,8 @@ GBGHT_HD double body_x_velocity(const Cta& c, Cplx<T>* sm, double* red, const Ge
 // ================================================================================================
 
 // Register-direct I/O of one z tile (the TL kx columns kx0.. of row ky' = qy, all z).
-// Forward: the first stage reads A slot `slot` rows z straight from global memory, and the last
-// stage keeps only the retained rows, written compactly into Rt[j] (rows q).
+// Forward: the first stage reads A slot `slot` rows z straight from global memory; the last stage
+// keeps only the retained rows, in the registers of the thread that computes them (ZOwn below).
 template <class T, int N, int TL>
 struct ZGlobalSource {
   static constexpr bool kExternal = true;
@@ -470,15 +471,146 @@ struct ZGlobalSource {
   int slot, qy, kx0;
   GBGHT_HD Cplx<T> load(int e, int l) const { return A[idxA(g, slot, e, qy, kx0 + l)]; }
 };
-template <class T, int N, int TL>
-struct ZRetainedSink {
-  const Geometry& g;
-  Cplx<T>* Rj;   // Rt + j·NY2·TL
-  GBGHT_HD void store(int e, int l, Cplx<T> v) const {
-    if (e <= g.K) Rj[e * TL + l] = v;
-    else if (e >= N - g.K) Rj[(e - N + g.NY2) * TL + l] = v;
+// Per-thread ownership of a z tile's retained rows. In tile_fft_io, slot b of thread t takes
+// butterfly j = (t + b·NT) / TL of line l = (t + b·NT) mod TL in every stage. The plans start and
+// end with the same radix R, so the last stage of a forward transform writes rows j + r·N/R, which
+// are the rows the first stage of an inverse transform reads: the thread that produces a retained
+// value is the thread that consumes it, and the retained rows stay in its registers between the
+// transforms (no shared-memory copy, no barrier). Row bands r whose rows j + r·N/R have |m| > K for
+// every j get no register.
+template <class T, int N, int TL, int NT>
+struct ZOwn {
+  static constexpr int R = Radices<N>::r[0];
+  static_assert(R == Radices<N>::r[Radices<N>::n - 1], "the z epilogue needs equal first and last radix");
+  static constexpr int NB = N / R;
+  static constexpr int TOT = NB * TL;
+  static constexpr int BPT = (TOT + NT - 1) / NT;
+  static constexpr int KMAX = N / 3 + 1;   // bounds K = max |m| of the 2/3 ball for every side length
+  static constexpr int lead() { int a = 0; while (a < R && a * NB <= KMAX) ++a; return a; }
+  static constexpr int tail() { int b = R; while (b > 0 && b * NB - 1 >= N - KMAX) --b; return b; }
+  static constexpr int A0 = lead(), B0 = tail() > lead() ? tail() : lead();
+  static constexpr int NSLOT = A0 + (R - B0);
+  GBGHT_HD static constexpr bool may(int r) { return r < A0 || r >= B0; }
+  GBGHT_HD static constexpr int slot(int r) { return r < A0 ? r : r - B0 + A0; }
+};
+
+// Storage of the owned rows: three components × BPT × NSLOT complex values per thread.
+// ZRowsReg keeps them in registers (the host-check build, and small N); ZRowsTmem keeps them in the
+// thread's private TMEM lane. Both expose put / put_done / get / get3; put_done makes the puts
+// visible to later gets.
+template <class T, class O>
+struct ZRowsReg {
+  Cplx<T> v[3][O::BPT][O::NSLOT];
+  GBGHT_HD void put(int c, int b, int sl, Cplx<T> x) { v[c][b][sl] = x; }
+  GBGHT_HD void put_done() const {}
+  GBGHT_HD Cplx<T> get(int c, int b, int sl) const { return v[c][b][sl]; }
+  GBGHT_HD void get3(int b, int sl, Cplx<T>& a0, Cplx<T>& a1, Cplx<T>& a2) const {
+    a0 = v[0][b][sl];
+    a1 = v[1][b][sl];
+    a2 = v[2][b][sl];
   }
 };
+
+// TMEM columns per thread and per CTA for the owned rows of a z tile.
+template <class T, int N, class O, int NT>
+struct ZTmemShape {
+  static constexpr int WPC = int(sizeof(Cplx<T>)) / 4;            // 32-bit words per value
+  static constexpr int COLS = 3 * O::BPT * O::NSLOT * WPC;         // per thread
+  static constexpr int WPQ = (NT / 32 + 3) / 4;                    // warps per lane quarter
+  static constexpr int NEED = COLS * WPQ;
+  static constexpr int NCOLS = NEED <= 32 ? 32 : NEED <= 64 ? 64 : NEED <= 128 ? 128 : NEED <= 256 ? 256 : 512;
+  // Warp-collective access needs every thread of every warp active in every stage.
+  static constexpr bool kUse = N >= 64 && NT % 32 == 0 && O::BPT * NT == O::TOT && NEED <= 256;
+};
+
+#if defined(__CUDACC__) && !defined(GBGHT_EMU)
+template <class T, class O>
+struct ZRowsTmem {
+  static constexpr int WPC = int(sizeof(Cplx<T>)) / 4;
+  uint32_t base;   // this thread's warp: lane quarter and column block
+  __device__ static uint32_t col(int c, int b, int sl) { return uint32_t(((c * O::BPT + b) * O::NSLOT + sl) * WPC); }
+  __device__ static Cplx<T> unpack(const uint32_t* w) {
+    if constexpr (WPC == 4)
+      return cmk<T>(__hiloint2double(int(w[1]), int(w[0])), __hiloint2double(int(w[3]), int(w[2])));
+    else
+      return cmk<T>(__uint_as_float(w[0]), __uint_as_float(w[1]));
+  }
+  // put and get3 follow per-row branches: reconverge the warp before the collective access.
+  __device__ void put(int c, int b, int sl, Cplx<T> x) const {
+    __syncwarp();
+    if constexpr (WPC == 4)
+      tmem_st4(base + col(c, b, sl), uint32_t(__double2loint(x.x)), uint32_t(__double2hiint(x.x)),
+               uint32_t(__double2loint(x.y)), uint32_t(__double2hiint(x.y)));
+    else
+      tmem_st2(base + col(c, b, sl), __float_as_uint(x.x), __float_as_uint(x.y));
+  }
+  __device__ void put_done() const { tmem_wait_st(); }
+  __device__ Cplx<T> get(int c, int b, int sl) const {
+    uint32_t w[WPC];
+    if constexpr (WPC == 4) tmem_ld4(base + col(c, b, sl), w);
+    else tmem_ld2(base + col(c, b, sl), w);
+    return unpack(w);
+  }
+  __device__ void get3(int b, int sl, Cplx<T>& a0, Cplx<T>& a1, Cplx<T>& a2) const {
+    __syncwarp();
+    uint32_t w[3 * WPC];
+    if constexpr (WPC == 4) tmem_ld4x3(base + col(0, b, sl), base + col(1, b, sl), base + col(2, b, sl), w);
+    else tmem_ld2x3(base + col(0, b, sl), base + col(1, b, sl), base + col(2, b, sl), w);
+    a0 = unpack(w);
+    a1 = unpack(w + WPC);
+    a2 = unpack(w + 2 * WPC);
+  }
+};
+#endif
+
+// The last stage of a forward transform into component `comp` of the owned rows.
+template <class T, class O, class Rows>
+struct ZOwnSink {
+  static constexpr bool kIndexed = true;
+  Rows& rows;
+  int comp;
+  GBGHT_HD void store_rb(int, int, Cplx<T> v, int r, int b) const {
+    if (O::may(r)) rows.put(comp, b, O::slot(r), v);
+  }
+};
+
+// The first stage of an inverse transform from x[b][slot] on retained rows, zero elsewhere.
+template <class T, int N, class O>
+struct ZOwnSource {
+  static constexpr bool kExternal = true;
+  static constexpr bool kIndexed = true;
+  const Geometry& g;
+  const Cplx<T> (&x)[O::BPT][O::NSLOT];
+  GBGHT_HD Cplx<T> load_rb(int e, int, int r, int b) const {
+    if (!O::may(r)) return czero<T>();
+    const Cplx<T> v = x[b][O::slot(r)];
+    return (e <= g.K || e >= N - g.K) ? v : czero<T>();
+  }
+};
+
+// Every slot of the thread with a register: slot b, band r (slot index sl), whether the row
+// e = j + r·N/R is retained, its compact index q and m_z, and the column l. The loops unroll, so
+// (b, sl) are compile-time indices.
+template <class T, int N, int TL, int NT, class F>
+GBGHT_HD void for_own_slots(const Cta& c, const Geometry& g, const F& f) {
+  using O = ZOwn<T, N, TL, NT>;
+#pragma unroll
+  for (int b = 0; b < O::BPT; ++b) {
+    const int idx = c.tid + b * NT;
+    const bool active = O::BPT * NT == O::TOT || idx < O::TOT;
+    const int l = idx % TL, j = idx / TL;
+#pragma unroll
+    for (int r = 0; r < O::R; ++r) {
+      if (!O::may(r)) continue;
+      const int e = j + r * O::NB;
+      const bool ret = active && (e <= g.K || e >= N - g.K);
+      const int q = e <= g.K ? e : e - N + g.NY2;
+      const int mz = e <= g.K ? e : e - N;
+      f(b, O::slot(r), ret, q, mz, l);
+    }
+  }
+}
+
 // Inverse: the first stage reads value(q, l) for retained rows and zero elsewhere; the last stage
 // writes A slot `slot` rows z straight to global memory.
 template <class T, int N, int TL, class F>
@@ -500,18 +632,26 @@ struct ZGlobalSink {
   GBGHT_HD void store(int e, int l, Cplx<T> v) const { A[idxA(g, slot, e, qy, kx0 + l)] = v; }
 };
 
-// Forward z-transform of A slots [c0, c0+3) of the tile into Rt[j][q][l] (retained rows only).
-template <class T, int N, int TL, int NT>
-GBGHT_HD void z_forward3(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, const Geometry& g, const Cplx<T>* A, int c0,
-                         int qy, int kx0, const Cplx<T>* GBGHT_RESTRICT tw) {
-  for (int j = 0; j < 3; ++j) {
-    const ZGlobalSource<T, N, TL> src{g, A, c0 + j, qy, kx0};
-    const ZRetainedSink<T, N, TL> dst{g, Rt + j * g.NY2 * TL};
-    tile_fft_io<T, N, TL, NT, -1>(c, W, tw, src, dst);
-  }
+// Forward z-transform of A slot `slot` of the tile into component `comp` of the owned rows.
+template <class T, int N, int TL, int NT, class O, class Rows>
+GBGHT_HD void z_forward_own(const Cta& c, Cplx<T>* W, const Geometry& g, const Cplx<T>* A, int slot, int qy, int kx0,
+                            Rows& rows, int comp, const Cplx<T>* GBGHT_RESTRICT tw) {
+  const ZGlobalSource<T, N, TL> src{g, A, slot, qy, kx0};
+  const ZOwnSink<T, O, Rows> dst{rows, comp};
+  tile_fft_io<T, N, TL, NT, -1>(c, W, tw, src, dst);
+  rows.put_done();
 }
 
-// Inverse z-transform of one retained column set, value(q, l), into A slot `slot` of the tile.
+// Inverse z-transform of the owned values x (retained rows) into A slot `slot` of the tile.
+template <class T, int N, int TL, int NT, class O>
+GBGHT_HD void z_inverse_own(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* A, int slot, int qy, int kx0,
+                            const Cplx<T> (&x)[O::BPT][O::NSLOT], const Cplx<T>* GBGHT_RESTRICT tw) {
+  const ZOwnSource<T, N, O> src{g, x};
+  const ZGlobalSink<T, N, TL> dst{g, A, slot, qy, kx0};
+  tile_fft_io<T, N, TL, NT, +1>(c, W, tw, src, dst);
+}
+
+// Inverse z-transform of value(q, l) (retained rows q) into A slot `slot` of the tile.
 template <class T, int N, int TL, int NT, class F>
 GBGHT_HD void z_inverse1(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* A, int slot, int qy, int kx0,
                          const F& value, const Cplx<T>* GBGHT_RESTRICT tw) {
@@ -520,19 +660,40 @@ GBGHT_HD void z_inverse1(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* A
   tile_fft_io<T, N, TL, NT, +1>(c, W, tw, src, dst);
 }
 
-// ω̂ component o of iκ × û from the retained velocity columns Rt[0..2].
-template <class T, int TL>
-GBGHT_HD Cplx<T> curl_component(const Geometry& g, const Cplx<T>* Rt, int o, int q, int l, int kx0, double ky) {
-  const int kx = kx0 + l;
-  const int mz = q_to_m(q, g.K, g.NY2);
-  const T kX = T(g.s * double(kx)), kY = T(ky), kZ = T(g.s * double(mz));
-  const Cplx<T> u0 = Rt[(0 * g.NY2 + q) * TL + l], u1 = Rt[(1 * g.NY2 + q) * TL + l],
-                u2 = Rt[(2 * g.NY2 + q) * TL + l];
+// Component o of iκ × û at wavenumber (kX, kY, kZ).
+template <class T>
+GBGHT_HD Cplx<T> curl_of(int o, Cplx<T> u0, Cplx<T> u1, Cplx<T> u2, T kX, T kY, T kZ) {
   Cplx<T> cr;
   if (o == 0) cr = scale(u2, kY) - scale(u1, kZ);
   else if (o == 1) cr = scale(u0, kZ) - scale(u2, kX);
   else cr = scale(u1, kX) - scale(u0, kY);
   return mul_i(cr);
+}
+
+// The z-inverse of the owned velocity rows into A slots 0..2, and of iκ × û into slots 3..5
+// (3..5 only when `vorticity`).
+template <class T, int N, int TL, int NT, class O, class Rows>
+GBGHT_HD void z_inverse_velocity(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* A, int qy, int kx0, double ky,
+                                 const Rows& rows, int vorticity, const Cplx<T>* GBGHT_RESTRICT tw) {
+  for (int o = 0; o < 3; ++o) {
+    Cplx<T> x[O::BPT][O::NSLOT];
+#pragma unroll
+    for (int b = 0; b < O::BPT; ++b)
+#pragma unroll
+      for (int sl = 0; sl < O::NSLOT; ++sl) x[b][sl] = rows.get(o, b, sl);
+    z_inverse_own<T, N, TL, NT, O>(c, W, g, A, o, qy, kx0, x, tw);
+  }
+  if (!vorticity) return;
+  const T kY = T(ky);
+  for (int o = 0; o < 3; ++o) {
+    Cplx<T> x[O::BPT][O::NSLOT];
+    for_own_slots<T, N, TL, NT>(c, g, [&](int b, int sl, bool, int, int mz, int l) {
+      Cplx<T> u0, u1, u2;
+      rows.get3(b, sl, u0, u1, u2);
+      x[b][sl] = curl_of<T>(o, u0, u1, u2, T(g.s * double(kx0 + l)), kY, T(g.s * double(mz)));
+    });
+    z_inverse_own<T, N, TL, NT, O>(c, W, g, A, 3 + o, qy, kx0, x, tw);
+  }
 }
 
 // ================================================================================================
@@ -557,137 +718,133 @@ struct StageArgs {
   double G[3];          // mean scalar gradient (extension)
 };
 
-template <class T, int N, int TL, int NT>
-GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, const Geometry& g,
+template <class T, int N, int TL, int NT, class Rows>
+GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, double* red, const Geometry& g, Rows& rows,
                                 Cplx<T>* GBGHT_RESTRICT A, Cplx<T>* GBGHT_RESTRICT S, Cplx<T>* GBGHT_RESTRICT H, const StageArgs& st,
                                 const double* GBGHT_RESTRICT force_amp, const Cplx<T>* GBGHT_RESTRICT tw) {
+  using O = ZOwn<T, N, TL, NT>;
   const int kx0 = c.bx * TL, qy = c.by;
-  const int NY2 = g.NY2;
   const double s = g.s;
-  const int my = q_to_m(qy, g.K, NY2);
-  const double ky = s * double(my);
+  const double ky = s * double(q_to_m(qy, g.K, g.NY2));
 
   // ---------------- scalar -------------------------------------------------------------------------
   if (st.has_scalar) {
-    z_forward3<T, N, TL, NT>(c, W, Rt, g, A, 3, qy, kx0, tw);
-    for (int i = c.tid; i < NY2 * TL; i += NT) {
-      const int q = i / TL, l = i % TL;
-      const int kx = kx0 + l;
-      const int mz = q_to_m(q, g.K, NY2);
-      const double kxd = s * double(kx), kzd = s * double(mz);
-      const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
-      const bool keep = kx <= g.K && k2 <= g.cut2;
-      const size_t si = idxS(g, 3, qy, q, kx);
-      Cplx<T> phi = S[si];
-      Cplx<T> nphi = czero<T>();
-      if (keep) {
-        const Cplx<T> fx = Rt[(0 * NY2 + q) * TL + l], fy = Rt[(1 * NY2 + q) * TL + l],
-                      fz = Rt[(2 * NY2 + q) * TL + l];
-        // −i(κx fx + κy fy + κz fz)
-        const Cplx<T> dsum = cmk<T>(T(kxd) * fx.x + T(ky) * fy.x + T(kzd) * fz.x,
-                                    T(kxd) * fx.y + T(ky) * fy.y + T(kzd) * fz.y);
-        nphi = mul_mi(dsum);
+    for (int o = 0; o < 3; ++o) z_forward_own<T, N, TL, NT, O>(c, W, g, A, 3 + o, qy, kx0, rows, o, tw);
+    Cplx<T> x[O::BPT][O::NSLOT];
+    for_own_slots<T, N, TL, NT>(c, g, [&](int b, int sl, bool ret, int q, int mz, int l) {
+      Cplx<T> fx, fy, fz;
+      rows.get3(b, sl, fx, fy, fz);
+      Cplx<T> phi = czero<T>();
+      if (ret) {
+        const int kx = kx0 + l;
+        const double kxd = s * double(kx), kzd = s * double(mz);
+        const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
+        const bool keep = kx <= g.K && k2 <= g.cut2;
+        const size_t si = idxS(g, 3, qy, q, kx);
+        phi = S[si];
+        Cplx<T> nphi = czero<T>();
+        if (keep) {
+          // −i(κx fx + κy fy + κz fz)
+          const Cplx<T> dsum = cmk<T>(T(kxd) * fx.x + T(ky) * fy.x + T(kzd) * fz.x,
+                                      T(kxd) * fx.y + T(ky) * fy.y + T(kzd) * fz.y);
+          nphi = mul_mi(dsum);
+        }
+        if (st.G[0] != 0.0 || st.G[1] != 0.0 || st.G[2] != 0.0) {
+          const Cplx<T> ux = S[idxS(g, 0, qy, q, kx)], uy = S[idxS(g, 1, qy, q, kx)],
+                        uz = S[idxS(g, 2, qy, q, kx)];
+          const T G0 = T(st.G[0]), G1 = T(st.G[1]), G2 = T(st.G[2]);
+          nphi = nphi - cmk<T>(G0 * ux.x + G1 * uy.x + G2 * uz.x, G0 * ux.y + G1 * uy.y + G2 * uz.y);
+        }
+        Cplx<T> h = st.first ? scale(nphi, T(st.dt))
+                             : scale(H[si], T(st.a)) + scale(nphi, T(st.dt));
+        const T E = T(exp(st.cphi * k2));
+        phi = scale(phi + scale(h, T(st.b)), E);
+        S[si] = phi;
+        if (!st.last) H[si] = scale(h, E);
       }
-      if (st.G[0] != 0.0 || st.G[1] != 0.0 || st.G[2] != 0.0) {
-        const Cplx<T> ux = S[idxS(g, 0, qy, q, kx)], uy = S[idxS(g, 1, qy, q, kx)],
-                      uz = S[idxS(g, 2, qy, q, kx)];
-        const T G0 = T(st.G[0]), G1 = T(st.G[1]), G2 = T(st.G[2]);
-        nphi = nphi - cmk<T>(G0 * ux.x + G1 * uy.x + G2 * uz.x, G0 * ux.y + G1 * uy.y + G2 * uz.y);
-      }
-      Cplx<T> h = st.first ? scale(nphi, T(st.dt))
-                           : scale(H[si], T(st.a)) + scale(nphi, T(st.dt));
-      const T E = T(exp(st.cphi * k2));
-      phi = scale(phi + scale(h, T(st.b)), E);
-      S[si] = phi;
-      if (!st.last) H[si] = scale(h, E);
-      Rt[(0 * NY2 + q) * TL + l] = phi;
-    }
-    GBGHT_SYNC();
-    const auto phi_new = [&](int q, int l) { return Rt[(0 * NY2 + q) * TL + l]; };
-    z_inverse1<T, N, TL, NT>(c, W, g, A, 6, qy, kx0, phi_new, tw);
+      x[b][sl] = phi;
+    });
+    z_inverse_own<T, N, TL, NT, O>(c, W, g, A, 6, qy, kx0, x, tw);
   }
 
   // ---------------- velocity -----------------------------------------------------------------------
-  z_forward3<T, N, TL, NT>(c, W, Rt, g, A, 0, qy, kx0, tw);
+  for (int o = 0; o < 3; ++o) z_forward_own<T, N, TL, NT, O>(c, W, g, A, o, qy, kx0, rows, o, tw);
   const double A_f = st.forced ? force_amp[0] : 0.0;
   double esum = 0.0;
-  for (int i = c.tid; i < NY2 * TL; i += NT) {
-    const int q = i / TL, l = i % TL;
-    const int kx = kx0 + l;
-    const int mz = q_to_m(q, g.K, NY2);
-    const double kxd = s * double(kx), kzd = s * double(mz);
-    const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
-    const bool keep = kx <= g.K && k2 <= g.cut2;
-    const size_t s0 = idxS(g, 0, qy, q, kx), s1 = idxS(g, 1, qy, q, kx), s2 = idxS(g, 2, qy, q, kx);
-    Cplx<T> u0 = S[s0], u1 = S[s1], u2 = S[s2];
-    Cplx<T> n0 = czero<T>(), n1 = czero<T>(), n2 = czero<T>();
-    if (keep && k2 > 0.0) {
-      const Cplx<T> f0 = Rt[(0 * NY2 + q) * TL + l], f1 = Rt[(1 * NY2 + q) * TL + l],
-                    f2 = Rt[(2 * NY2 + q) * TL + l];
-      const T kX = T(kxd), kY = T(ky), kZ = T(kzd);
-      const T ik2 = T(1.0 / k2);
-      const Cplx<T> kd = cmk<T>((kX * f0.x + kY * f1.x + kZ * f2.x) * ik2, (kX * f0.y + kY * f1.y + kZ * f2.y) * ik2);
-      n0 = f0 - scale(kd, kX);
-      n1 = f1 - scale(kd, kY);
-      n2 = f2 - scale(kd, kZ);
-    }
-    if (A_f != 0.0 && k2 >= st.band_lo2 && k2 <= st.band_hi2) {
-      const T Af = T(A_f);
-      n0 = n0 + scale(u0, Af);
-      n1 = n1 + scale(u1, Af);
-      n2 = n2 + scale(u2, Af);
-    }
-    const T dt = T(st.dt), a = T(st.a), b = T(st.b);
-    Cplx<T> h0, h1, h2;
-    if (st.first) {
-      h0 = scale(n0, dt); h1 = scale(n1, dt); h2 = scale(n2, dt);
-    } else {
-      h0 = scale(H[s0], a) + scale(n0, dt);
-      h1 = scale(H[s1], a) + scale(n1, dt);
-      h2 = scale(H[s2], a) + scale(n2, dt);
-    }
-    const T E = T(exp(st.cu * k2));
-    u0 = scale(u0 + scale(h0, b), E);
-    u1 = scale(u1 + scale(h1, b), E);
-    u2 = scale(u2 + scale(h2, b), E);
-    if (st.last) {
-      if (k2 > 0.0) {
+  for_own_slots<T, N, TL, NT>(c, g, [&](int b, int sl, bool ret, int q, int mz, int l) {
+    Cplx<T> f0, f1, f2;
+    rows.get3(b, sl, f0, f1, f2);
+    Cplx<T> u0 = czero<T>(), u1 = czero<T>(), u2 = czero<T>();
+    if (ret) {
+      const int kx = kx0 + l;
+      const double kxd = s * double(kx), kzd = s * double(mz);
+      const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
+      const bool keep = kx <= g.K && k2 <= g.cut2;
+      const size_t s0 = idxS(g, 0, qy, q, kx), s1 = idxS(g, 1, qy, q, kx), s2 = idxS(g, 2, qy, q, kx);
+      u0 = S[s0];
+      u1 = S[s1];
+      u2 = S[s2];
+      Cplx<T> n0 = czero<T>(), n1 = czero<T>(), n2 = czero<T>();
+      if (keep && k2 > 0.0) {
         const T kX = T(kxd), kY = T(ky), kZ = T(kzd);
         const T ik2 = T(1.0 / k2);
-        const Cplx<T> kd = cmk<T>((kX * u0.x + kY * u1.x + kZ * u2.x) * ik2, (kX * u0.y + kY * u1.y + kZ * u2.y) * ik2);
-        u0 = u0 - scale(kd, kX);
-        u1 = u1 - scale(kd, kY);
-        u2 = u2 - scale(kd, kZ);
+        const Cplx<T> kd = cmk<T>((kX * f0.x + kY * f1.x + kZ * f2.x) * ik2, (kX * f0.y + kY * f1.y + kZ * f2.y) * ik2);
+        n0 = f0 - scale(kd, kX);
+        n1 = f1 - scale(kd, kY);
+        n2 = f2 - scale(kd, kZ);
       }
-    } else {
-      H[s0] = scale(h0, E);
-      H[s1] = scale(h1, E);
-      H[s2] = scale(h2, E);
+      if (A_f != 0.0 && k2 >= st.band_lo2 && k2 <= st.band_hi2) {
+        const T Af = T(A_f);
+        n0 = n0 + scale(u0, Af);
+        n1 = n1 + scale(u1, Af);
+        n2 = n2 + scale(u2, Af);
+      }
+      const T dt = T(st.dt), a = T(st.a), bb = T(st.b);
+      Cplx<T> h0, h1, h2;
+      if (st.first) {
+        h0 = scale(n0, dt); h1 = scale(n1, dt); h2 = scale(n2, dt);
+      } else {
+        h0 = scale(H[s0], a) + scale(n0, dt);
+        h1 = scale(H[s1], a) + scale(n1, dt);
+        h2 = scale(H[s2], a) + scale(n2, dt);
+      }
+      const T E = T(exp(st.cu * k2));
+      u0 = scale(u0 + scale(h0, bb), E);
+      u1 = scale(u1 + scale(h1, bb), E);
+      u2 = scale(u2 + scale(h2, bb), E);
+      if (st.last) {
+        if (k2 > 0.0) {
+          const T kX = T(kxd), kY = T(ky), kZ = T(kzd);
+          const T ik2 = T(1.0 / k2);
+          const Cplx<T> kd = cmk<T>((kX * u0.x + kY * u1.x + kZ * u2.x) * ik2, (kX * u0.y + kY * u1.y + kZ * u2.y) * ik2);
+          u0 = u0 - scale(kd, kX);
+          u1 = u1 - scale(kd, kY);
+          u2 = u2 - scale(kd, kZ);
+        }
+      } else {
+        H[s0] = scale(h0, E);
+        H[s1] = scale(h1, E);
+        H[s2] = scale(h2, E);
+      }
+      S[s0] = u0;
+      S[s1] = u1;
+      S[s2] = u2;
+      const double w = kx == 0 ? 1.0 : 2.0;
+      esum += w * ((double(u0.x) * u0.x + double(u0.y) * u0.y) + (double(u1.x) * u1.x + double(u1.y) * u1.y) +
+                   (double(u2.x) * u2.x + double(u2.y) * u2.y));
     }
-    S[s0] = u0;
-    S[s1] = u1;
-    S[s2] = u2;
-    Rt[(0 * NY2 + q) * TL + l] = u0;
-    Rt[(1 * NY2 + q) * TL + l] = u1;
-    Rt[(2 * NY2 + q) * TL + l] = u2;
-    const double w = kx == 0 ? 1.0 : 2.0;
-    esum += w * ((double(u0.x) * u0.x + double(u0.y) * u0.y) + (double(u1.x) * u1.x + double(u1.y) * u1.y) +
-                 (double(u2.x) * u2.x + double(u2.y) * u2.y));
-  }
+    rows.put(0, b, sl, u0);
+    rows.put(1, b, sl, u1);
+    rows.put(2, b, sl, u2);
+  });
+  rows.put_done();
   red[c.tid] = esum;
   GBGHT_SYNC();
   double total = 0.0;
   if (c.tid == 0)
     for (int i = 0; i < NT; ++i) total += red[i];
   // z-inverse of û and of ω̂ = iκ × û
-  for (int o = 0; o < 3; ++o) {
-    const auto u_new = [&](int q, int l) { return Rt[(o * NY2 + q) * TL + l]; };
-    z_inverse1<T, N, TL, NT>(c, W, g, A, o, qy, kx0, u_new, tw);
-  }
-  for (int o = 0; o < 3; ++o) {
-    const auto w_new = [&](int q, int l) { return curl_component<T, TL>(g, Rt, o, q, l, kx0, ky); };
-    z_inverse1<T, N, TL, NT>(c, W, g, A, 3 + o, qy, kx0, w_new, tw);
-  }
+  z_inverse_velocity<T, N, TL, NT, O>(c, W, g, A, qy, kx0, ky, rows, 1, tw);
   return total;
 }
 
@@ -743,38 +900,36 @@ GBGHT_HD double band_energy_raw(const Geometry& g, const Cplx<T>* S, double lo2,
 // z-inverse of the current state into A slots 0..6 (u, iκ×û, φ), and the tile's Hermitian-weighted
 // Σ|û|², with the same tiling as the epilogue. Used after an import to start a step.
 // ================================================================================================
-template <class T, int N, int TL, int NT>
-GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, Cplx<T>* Rt, double* red, const Geometry& g,
+template <class T, int N, int TL, int NT, class Rows>
+GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, double* red, const Geometry& g, Rows& rows,
                             Cplx<T>* GBGHT_RESTRICT A, const Cplx<T>* GBGHT_RESTRICT S, int has_scalar,
                             const Cplx<T>* GBGHT_RESTRICT tw, int vorticity = 1) {
+  using O = ZOwn<T, N, TL, NT>;
   const int kx0 = c.bx * TL, qy = c.by;
-  const int NY2 = g.NY2;
-  const double ky = g.s * double(q_to_m(qy, g.K, NY2));
+  const double ky = g.s * double(q_to_m(qy, g.K, g.NY2));
   double esum = 0.0;
-  for (int i = c.tid; i < NY2 * TL; i += NT) {
-    const int q = i / TL, l = i % TL;
-    const int kx = kx0 + l;
-    const Cplx<T> u0 = S[idxS(g, 0, qy, q, kx)], u1 = S[idxS(g, 1, qy, q, kx)], u2 = S[idxS(g, 2, qy, q, kx)];
-    Rt[(0 * NY2 + q) * TL + l] = u0;
-    Rt[(1 * NY2 + q) * TL + l] = u1;
-    Rt[(2 * NY2 + q) * TL + l] = u2;
-    const double w = kx == 0 ? 1.0 : 2.0;
-    esum += w * ((double(u0.x) * u0.x + double(u0.y) * u0.y) + (double(u1.x) * u1.x + double(u1.y) * u1.y) +
-                 (double(u2.x) * u2.x + double(u2.y) * u2.y));
-  }
+  for_own_slots<T, N, TL, NT>(c, g, [&](int b, int sl, bool ret, int q, int, int l) {
+    Cplx<T> u0 = czero<T>(), u1 = czero<T>(), u2 = czero<T>();
+    if (ret) {
+      const int kx = kx0 + l;
+      u0 = S[idxS(g, 0, qy, q, kx)];
+      u1 = S[idxS(g, 1, qy, q, kx)];
+      u2 = S[idxS(g, 2, qy, q, kx)];
+      const double w = kx == 0 ? 1.0 : 2.0;
+      esum += w * ((double(u0.x) * u0.x + double(u0.y) * u0.y) + (double(u1.x) * u1.x + double(u1.y) * u1.y) +
+                   (double(u2.x) * u2.x + double(u2.y) * u2.y));
+    }
+    rows.put(0, b, sl, u0);
+    rows.put(1, b, sl, u1);
+    rows.put(2, b, sl, u2);
+  });
+  rows.put_done();
   red[c.tid] = esum;
   GBGHT_SYNC();
   double total = 0.0;
   if (c.tid == 0)
     for (int i = 0; i < NT; ++i) total += red[i];
-  for (int o = 0; o < 3; ++o) {
-    const auto u_new = [&](int q, int l) { return Rt[(o * NY2 + q) * TL + l]; };
-    z_inverse1<T, N, TL, NT>(c, W, g, A, o, qy, kx0, u_new, tw);
-  }
-  for (int o = 0; o < 3 && vorticity; ++o) {
-    const auto w_new = [&](int q, int l) { return curl_component<T, TL>(g, Rt, o, q, l, kx0, ky); };
-    z_inverse1<T, N, TL, NT>(c, W, g, A, 3 + o, qy, kx0, w_new, tw);
-  }
+  z_inverse_velocity<T, N, TL, NT, O>(c, W, g, A, qy, kx0, ky, rows, vorticity, tw);
   if (has_scalar) {
     const auto phi = [&](int q, int l) { return S[idxS(g, 3, qy, q, kx0 + l)]; };
     z_inverse1<T, N, TL, NT>(c, W, g, A, 6, qy, kx0, phi, tw);
