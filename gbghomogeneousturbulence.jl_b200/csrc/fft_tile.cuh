@@ -126,11 +126,21 @@ GBGHT_HD int tix(int e, int l) {
   }
 }
 
+// The twiddle table e^(-2πi k/N): a pointer is a table in global memory (read through the
+// read-only path); SharedTwiddles is a copy in shared memory, for kernels whose L1 cannot keep the
+// table next to their streaming traffic.
+template <class T>
+struct SharedTwiddles {
+  const Cplx<T>* p;
+};
+template <class T> GBGHT_HD Cplx<T> tw_at(const Cplx<T>* GBGHT_RESTRICT tw, int k) { return ldgc(tw + k); }
+template <class T> GBGHT_HD Cplx<T> tw_at(const SharedTwiddles<T>& tw, int k) { return tw.p[k]; }
+
 // Twiddles w^(jm·r·TWS), r = 1..R−1, from one table read: w₂ = w₁², w₃ = w₂w₁, w₄ = w₂², w₅ = w₄w₁,
 // w₆ = w₄w₂, w₇ = w₄w₃ (at most three products deep, so a few ulp of error).
-template <class T, int R, int SIGN>
-GBGHT_HD void twiddles(const Cplx<T>* GBGHT_RESTRICT tw, int k, Cplx<T>* w) {
-  w[1] = ldgc(tw + k);
+template <class T, int R, int SIGN, class TW>
+GBGHT_HD void twiddles(const TW& tw, int k, Cplx<T>* w) {
+  w[1] = tw_at<T>(tw, k);
   if constexpr (SIGN > 0) w[1] = conj(w[1]);
   if constexpr (R > 2) w[2] = w[1] * w[1];
   if constexpr (R > 3) w[3] = w[2] * w[1];
@@ -165,9 +175,14 @@ struct TileBuf {
 // defaults both are the tile itself, and the transform is in place. With an external source the
 // first stage loads straight into registers (from global memory, say), and with an external sink
 // the last stage stores straight out, so neither costs a pass through shared memory.
-template <class T, int N, int TL, int NT, int SIGN, bool SWZ = false, int ACT = TL, int S = 0, class Src, class Dst>
-GBGHT_HD void tile_fft_io(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTRICT tw, const Src& src, const Dst& dst) {
-  if constexpr (S < Radices<N>::n) {
+//
+// Stages [S, S_END) run; a call that stops early leaves the partial transform in the tile, and a
+// later call with S = the stop resumes it (the caller can act between the two, after the barrier
+// that ends every stage).
+template <class T, int N, int TL, int NT, int SIGN, bool SWZ = false, int ACT = TL, int S = 0,
+          int S_END = Radices<N>::n, class Src, class Dst, class TW>
+GBGHT_HD void tile_fft_io(const Cta& c, Cplx<T>* buf, const TW& tw, const Src& src, const Dst& dst) {
+  if constexpr (S < S_END) {
     constexpr int R = Radices<N>::r[S];
     constexpr int NS = stage_ns<N>(S);
     constexpr int NB = N / R;
@@ -219,7 +234,7 @@ GBGHT_HD void tile_fft_io(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTR
       }
     }
     GBGHT_SYNC();
-    tile_fft_io<T, N, TL, NT, SIGN, SWZ, ACT, S + 1>(c, buf, tw, src, dst);
+    tile_fft_io<T, N, TL, NT, SIGN, SWZ, ACT, S + 1, S_END>(c, buf, tw, src, dst);
   }
 }
 

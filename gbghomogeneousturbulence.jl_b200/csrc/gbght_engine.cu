@@ -67,8 +67,10 @@ constexpr int clamp_nt(int v) { return v < 64 ? 64 : (v > 256 ? 256 : v); }
 
 #ifdef GBGHT_EMU
 constexpr int kNT(int) { return 1; }
+constexpr int kNTZ(int) { return 1; }
 #else
 constexpr int kNT(int v) { return clamp_nt(v); }
+constexpr int kNTZ(int v) { return v < 64 ? 64 : (v > 512 ? 512 : v); }
 #endif
 
 template <class F>
@@ -108,7 +110,9 @@ class EngineImpl final : public Engine {
 #else
   static constexpr int NTXP = 32 * 7, NTXV = 32 * 6;   // one warp per line
 #endif
-  static constexpr int NTZ = kNT(N * TLZ / 8);
+  // z epilogue: one thread per butterfly of the first and last radix-R stage (N/R·TLZ of them),
+  // up to 512
+  static constexpr int NTZ = kNTZ(N * TLZ / Radices<N>::r[0]);
   static constexpr int NTR = kNT(256);
 
  public:
@@ -536,9 +540,12 @@ class EngineImpl final : public Engine {
            size_t(7) * XShape<T>::P * x_kxs(g_.K, int(sizeof(Cplx<T>))) * sizeof(Cplx<T>) + kBarBytes;
   }
   size_t smem_xv() const { return size_t(N) * XShape<T>::ACT_V * sizeof(Cplx<T>) + size_t(NTXV) * sizeof(double); }
+  // z init: the FFT tile, NT doubles, the TMEM address
   size_t smem_z() const {
     return size_t(N) * TLZ * sizeof(Cplx<T>) + size_t(NTZ) * sizeof(double) + 16;
   }
+  // z epilogue: the FFT tile, NT doubles, barriers, the TMEM address, the staging region
+  size_t smem_ze() const { return ZLayout<T, N, TLZ, NTZ>::bytes(g_.K); }
 
 #ifndef GBGHT_EMU
   const char* set_smem_attributes() {
@@ -551,7 +558,7 @@ class EngineImpl final : public Engine {
     set(reinterpret_cast<const void*>(k_y_forward<T, N, TLY, NTY>), smem_y());
     set(reinterpret_cast<const void*>(k_x_products<T, N, NTXP>), smem_x());
     set(reinterpret_cast<const void*>(k_x_velocity<T, N, NTXV>), smem_xv());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ>), smem_z());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ>), smem_ze());
     set(reinterpret_cast<const void*>(k_z_init<T, N, TLZ, NTZ>), smem_z());
     return e;
   }
@@ -582,7 +589,7 @@ class EngineImpl final : public Engine {
     };
     const cuuint32_t bxy = 2 * TLY, bxz = 2 * TLZ;
     const cuuint32_t K1 = cuuint32_t(g_.K + 1), K0 = cuuint32_t(g_.K);
-    const cuuint32_t BY = cuuint32_t(N > 256 ? (N % 256 == 0 ? 256 : N / 2) : N);
+    const cuuint32_t BY = cuuint32_t(box_rows<N>());
     if (!map2(&maps_.a_ld, A_, cuuint64_t(7) * N * g_.NY2, bxy, K1)) return "tensor map a_ld";
     if (!map2(&maps_.a_st1, A_, cuuint64_t(7) * N * g_.NY2, bxy, K1)) return "tensor map a_st1";
     if (!map2(&maps_.a_st2, A_, cuuint64_t(7) * N * g_.NY2, bxy, K0)) return "tensor map a_st2";
@@ -595,6 +602,15 @@ class EngineImpl final : public Engine {
                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return "tensor map az";
+    }
+    for (int which = 0; which < 2; ++which) {   // s3 over S, h3 over H
+      const cuuint64_t dims[3] = {inner, cuuint64_t(g_.NY2), cuuint64_t(4) * g_.NY2};
+      const cuuint64_t strides[2] = {pitch, pitch * g_.NY2};
+      const cuuint32_t box[3] = {bxz, K1, 1};
+      if (encode(which == 0 ? &maps_.s3 : &maps_.h3, dt, 3, which == 0 ? S_ : H_, dims, strides, box, ones,
+                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return which == 0 ? "tensor map s3" : "tensor map h3";
     }
     return nullptr;
   }
@@ -666,16 +682,20 @@ class EngineImpl final : public Engine {
   void z_epilogue(const StageArgs& st) {
 #ifdef GBGHT_EMU
     const int gx = g_.KXP / TLZ;
-    emu_grid(gx, g_.NY2, 1, smem_z(), [&](const Cta& c, void* sm) {
-      Cplx<T>* W = static_cast<Cplx<T>*>(sm);
-      double* red = reinterpret_cast<double*>(W + N * TLZ);
+    emu_grid(gx, g_.NY2, 1, ZLayout<T, N, TLZ, 1>::bytes(g_.K), [&](const Cta& c, void* sm) {
+      using L = ZLayout<T, N, TLZ, 1>;
+      unsigned char* base = static_cast<unsigned char*>(sm);
+      Cplx<T>* W = reinterpret_cast<Cplx<T>*>(base);
+      double* red = reinterpret_cast<double*>(base + L::kRed);
+      Cplx<T>* R = reinterpret_cast<Cplx<T>*>(base + L::kStage);
       ZRowsReg<T, ZOwn<T, N, TLZ, 1>> rows;
-      partial_[c.by * gx + c.bx] = body_z_epilogue<T, N, TLZ, 1>(c, W, red, g_, rows, A_, S_, H_, st, amp_, tw_);
+      partial_[c.by * gx + c.bx] = body_z_epilogue<T, N, TLZ, 1>(c, W, R, nullptr, red, g_, maps_, rows, A_, S_, H_,
+                                                                  st, amp_, tw_, status_);
     });
 #else
     pbegin(PROF_Z_EPILOGUE);
-    k_z_epilogue<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, S_, H_, st, amp_,
-                                                                                           partial_, tw_);
+    k_z_epilogue<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_ze(), stream_>>>(
+        maps_, g_, A_, S_, H_, st, amp_, partial_, tw_, status_);
     pend();
 #endif
   }

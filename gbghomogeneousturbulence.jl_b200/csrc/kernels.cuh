@@ -24,9 +24,6 @@ __device__ __forceinline__ void init_bars(uint64_t* bar, int n) {
   __syncthreads();
 }
 
-// rows of a 2-D tensor map per box along the row dimension: the largest divisor of N ≤ 256
-template <int N> constexpr int box_rows() { return N > 256 ? (N % 256 == 0 ? 256 : N / 2) : N; }
-
 template <class T, int N, int TL, int NT>
 __global__ void __launch_bounds__(NT, 2) k_y_inverse(const __grid_constant__ TmaMaps m, Geometry g, int c0,
                                                      const Cplx<T>* tw, unsigned int* status) {
@@ -127,21 +124,30 @@ __device__ __forceinline__ double with_z_rows(uint32_t* slot, const F& run) {
   }
 }
 
+// Shared memory: ZLayout (the FFT tile, NT doubles, barriers, the TMEM address, the twiddle table,
+// the staging region).
 template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT, 2) k_z_epilogue(Geometry g, Cplx<T>* A, Cplx<T>* S, Cplx<T>* H, StageArgs st,
-                                                      const double* amp, double* partial, const Cplx<T>* tw) {
+__global__ void __launch_bounds__(NT, NT > 256 ? 1 : 2) k_z_epilogue(const __grid_constant__ TmaMaps m, Geometry g, Cplx<T>* A,
+                                                      Cplx<T>* S, Cplx<T>* H, StageArgs st, const double* amp,
+                                                      double* partial, const Cplx<T>* tw, unsigned int* status) {
   CTA_CTX;
+  using L = ZLayout<T, N, TL, NT>;
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
-  double* red = reinterpret_cast<double*>(W + N * TL);
-  uint32_t* slot = reinterpret_cast<uint32_t*>(red + NT);
+  double* red = reinterpret_cast<double*>(g_smem + L::kRed);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(g_smem + L::kBar);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(g_smem + L::kSlot);
+  Cplx<T>* R = reinterpret_cast<Cplx<T>*>(g_smem + L::kStage);
+  Cplx<T>* twS = reinterpret_cast<Cplx<T>*>(g_smem + L::kTw);
+  for (int i = c.tid; i < N; i += NT) twS[i] = tw[i];
+  init_bars(bar, 3);   // its barrier also publishes the twiddle table
   const double e = with_z_rows<T, N, TL, NT>(slot, [&](auto& rows) {
-    return body_z_epilogue<T, N, TL, NT>(c, W, red, g, rows, A, S, H, st, amp, tw);
+    return body_z_epilogue<T, N, TL, NT>(c, W, R, bar, red, g, m, rows, A, S, H, st, amp, twS, status);
   });
   if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
 }
 
 template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT, 2) k_z_init(Geometry g, Cplx<T>* A, const Cplx<T>* S, int has_scalar, double* partial,
+__global__ void __launch_bounds__(NT, NT > 256 ? 1 : 2) k_z_init(Geometry g, Cplx<T>* A, const Cplx<T>* S, int has_scalar, double* partial,
                                                   const Cplx<T>* tw, int vorticity = 1) {
   CTA_CTX;
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);

@@ -53,12 +53,16 @@ GBGHT_HD size_t idxS(const Geometry& g, int c, int qy, int qz, int kx) {
 //   a_st1  the same rows, box {2·TLY, K+1};  a_st2: box {2·TLY, K}
 //   b      B as rows (dims {2·KXP, 7·N·N}), box {2·TLY, BY}, BY the largest divisor of N ≤ 256
 //   az     A as (x, q, c·N + z) (dims {2·KXP, NY2, 7·N}), box {2·TLZ, 1, BZ}, BZ = BY
+//   s3/h3  S and H as (x, q_z, c·NY2 + q_y) (dims {2·KXP, NY2, 4·NY2}), box {2·TLZ, K+1, 1}
 // Innermost coordinates are 2·kx0 reals with kx0 a multiple of the tile width, so every copy
 // starts on a 64- or 128-byte boundary.
 // ================================================================================================
+// Rows per box of the tensor maps along a length-N dimension: the largest divisor of N ≤ 256.
+template <int N> constexpr int box_rows() { return N > 256 ? (N % 256 == 0 ? 256 : N / 2) : N; }
+
 struct TmaMaps {
 #if defined(__CUDACC__) && !defined(GBGHT_EMU)
-  CUtensorMap a_ld, a_st1, a_st2, b, az;
+  CUtensorMap a_ld, a_st1, a_st2, b, az, s3, h3;
 #else
   int unused;
 #endif
@@ -471,6 +475,116 @@ struct ZGlobalSource {
   int slot, qy, kx0;
   GBGHT_HD Cplx<T> load(int e, int l) const { return A[idxA(g, slot, e, qy, kx0 + l)]; }
 };
+// Staged z tiles: A slot `slot` of the tile (N rows of TL elements, the layout of the tile FFT's
+// buffer) copied by the TMA engine (map az) into buffer `bf` (0 or 1) of the staging region, so
+// the copy of the next transform's input runs while the current one computes. The copy completes
+// a phase of barrier bf; the caller tracks the parities. The host-check build copies at issue.
+template <class T, int N, int TL>
+struct ZStagedSource {
+  static constexpr bool kExternal = true;
+  const Cplx<T>* P;
+  GBGHT_HD Cplx<T> load(int e, int l) const { return P[e * TL + l]; }
+};
+
+template <class T, int N, int TL>
+struct ZStaging {
+  const Geometry& g;
+  const Cplx<T>* A;
+  const TmaMaps& maps;
+  Cplx<T>* R;           // the staging region: two buffers of N·TL elements
+  uint64_t* bar;        // barriers 0 and 1
+  unsigned int* status;
+  int qy, kx0;
+  GBGHT_HD Cplx<T>* buf(int bf) const { return R + bf * (N * TL); }
+  GBGHT_HD void issue(const Cta& c, int bf, int slot) const {
+#if defined(__CUDA_ARCH__)
+    if (c.tid == 0) {
+      constexpr int BZ = box_rows<N>();
+      mbar_expect_tx(bar + bf, uint32_t(N * TL * sizeof(Cplx<T>)));
+      for (int z0 = 0; z0 < N; z0 += BZ) tma_load_3d(buf(bf) + z0 * TL, &maps.az, 2 * kx0, qy, slot * N + z0, bar + bf);
+    }
+#else
+    (void)c;
+    Cplx<T>* P = buf(bf);
+    for (int e = 0; e < N; ++e)
+      for (int l = 0; l < TL; ++l) P[e * TL + l] = A[idxA(g, slot, e, qy, kx0 + l)];
+#endif
+  }
+  GBGHT_HD void wait(int bf, int parity) const {
+#if defined(__CUDA_ARCH__)
+    mbar_wait(bar + bf, uint32_t(parity), status);
+#else
+    (void)bf;
+    (void)parity;
+#endif
+  }
+};
+
+// Staged state for one half of the epilogue: half h holds the compact rows q in [h·(K+1),
+// (h+1)·(K+1)) of up to six components of S and H (the tile's TL columns), copied by the TMA engine
+// (maps s3 and h3) into the staging region as component i at rows i·rows(K) (K + 1 rounded up so
+// that every copy starts on a 128-byte boundary). Component codes: c for S slot c, 4 + c for H
+// slot c. Rows past 2K read as zero.
+template <class T, int N, int TL>
+struct ZStateStaging {
+  static constexpr int kRowBytes = TL * int(sizeof(Cplx<T>));
+  GBGHT_HD static int rows(int K) { return ((K + 1) * kRowBytes + 127) / 128 * 128 / kRowBytes; }
+  const Geometry& g;
+  const Cplx<T>* S;
+  const Cplx<T>* H;
+  const TmaMaps& maps;
+  Cplx<T>* R;
+  uint64_t* bar;        // barrier 2
+  unsigned int* status;
+  int qy, kx0;
+  GBGHT_HD void issue(const Cta& c, int h, const int* codes, int n) const {
+    const int KR = g.K + 1, KS = rows(g.K);
+#if defined(__CUDA_ARCH__)
+    if (c.tid == 0) {
+      mbar_expect_tx(bar, uint32_t(n * KR * TL * sizeof(Cplx<T>)));
+      for (int i = 0; i < n; ++i)
+        tma_load_3d(R + i * KS * TL, codes[i] < 4 ? &maps.s3 : &maps.h3, 2 * kx0, h * KR, (codes[i] & 3) * g.NY2 + qy,
+                    bar);
+    }
+#else
+    (void)c;
+    for (int i = 0; i < n; ++i) {
+      const Cplx<T>* src = codes[i] < 4 ? S : H;
+      for (int t = 0; t < KR; ++t)
+        for (int l = 0; l < TL; ++l) {
+          const int q = h * KR + t;
+          R[(i * KS + t) * TL + l] = q < g.NY2 ? src[idxS(g, codes[i] & 3, qy, q, kx0 + l)] : czero<T>();
+        }
+    }
+#endif
+  }
+  GBGHT_HD void wait(int parity) const {
+#if defined(__CUDA_ARCH__)
+    mbar_wait(bar, uint32_t(parity), status);
+#else
+    (void)parity;
+#endif
+  }
+  // component i of the staged list at compact row q of half h, column l
+  GBGHT_HD Cplx<T> at(int i, int q, int h, int l) const { return R[(i * rows(g.K) + (q - h * (g.K + 1))) * TL + l]; }
+};
+
+// Shared memory of the z epilogue: the FFT tile W, NT doubles, four barriers, the TMEM address,
+// the twiddle table, then the staging region (two A tiles, or six state components of K + 1 rows).
+template <class T, int N, int TL, int NT>
+struct ZLayout {
+  static constexpr size_t kRed = size_t(N) * TL * sizeof(Cplx<T>);
+  static constexpr size_t kBar = kRed + size_t(NT) * sizeof(double);
+  static constexpr size_t kSlot = kBar + 4 * sizeof(uint64_t);
+  static constexpr size_t kTw = kSlot + 16;
+  static constexpr size_t kStage = (kTw + size_t(N) * sizeof(Cplx<T>) + 127) / 128 * 128;
+  GBGHT_HD static size_t stage_elems(int K) {
+    const size_t a = 2 * size_t(N) * TL, b = 6 * size_t(ZStateStaging<T, N, TL>::rows(K)) * TL;
+    return a > b ? a : b;
+  }
+  GBGHT_HD static size_t bytes(int K) { return kStage + stage_elems(K) * sizeof(Cplx<T>); }
+};
+
 // Per-thread ownership of a z tile's retained rows. In tile_fft_io, slot b of thread t takes
 // butterfly j = (t + b·NT) / TL of line l = (t + b·NT) mod TL in every stage. The plans start and
 // end with the same radix R, so the last stage of a forward transform writes rows j + r·N/R, which
@@ -492,6 +606,10 @@ struct ZOwn {
   static constexpr int NSLOT = A0 + (R - B0);
   GBGHT_HD static constexpr bool may(int r) { return r < A0 || r >= B0; }
   GBGHT_HD static constexpr int slot(int r) { return r < A0 ? r : r - B0 + A0; }
+  // Retained rows of the leading bands have q = m ≤ K (half 0), those of the trailing bands
+  // q = m + NY2 > K (half 1).
+  GBGHT_HD static constexpr int half(int r) { return r < A0 ? 0 : 1; }
+  static_assert(A0 * NB - 1 < N - KMAX && B0 * NB > KMAX, "a row band mixes both halves of the retained rows");
 };
 
 // Storage of the owned rows: three components × BPT × NSLOT complex values per thread.
@@ -591,7 +709,7 @@ struct ZOwnSource {
 // Every slot of the thread with a register: slot b, band r (slot index sl), whether the row
 // e = j + r·N/R is retained, its compact index q and m_z, and the column l. The loops unroll, so
 // (b, sl) are compile-time indices.
-template <class T, int N, int TL, int NT, class F>
+template <class T, int N, int TL, int NT, int HALF = -1, class F>
 GBGHT_HD void for_own_slots(const Cta& c, const Geometry& g, const F& f) {
   using O = ZOwn<T, N, TL, NT>;
 #pragma unroll
@@ -601,7 +719,7 @@ GBGHT_HD void for_own_slots(const Cta& c, const Geometry& g, const F& f) {
     const int l = idx % TL, j = idx / TL;
 #pragma unroll
     for (int r = 0; r < O::R; ++r) {
-      if (!O::may(r)) continue;
+      if (!O::may(r) || (HALF >= 0 && O::half(r) != HALF)) continue;
       const int e = j + r * O::NB;
       const bool ret = active && (e <= g.K || e >= N - g.K);
       const int q = e <= g.K ? e : e - N + g.NY2;
@@ -633,28 +751,49 @@ struct ZGlobalSink {
 };
 
 // Forward z-transform of A slot `slot` of the tile into component `comp` of the owned rows.
-template <class T, int N, int TL, int NT, class O, class Rows>
+template <class T, int N, int TL, int NT, class O, class Rows, class TW>
 GBGHT_HD void z_forward_own(const Cta& c, Cplx<T>* W, const Geometry& g, const Cplx<T>* A, int slot, int qy, int kx0,
-                            Rows& rows, int comp, const Cplx<T>* GBGHT_RESTRICT tw) {
+                            Rows& rows, int comp, const TW& tw) {
   const ZGlobalSource<T, N, TL> src{g, A, slot, qy, kx0};
   const ZOwnSink<T, O, Rows> dst{rows, comp};
   tile_fft_io<T, N, TL, NT, -1>(c, W, tw, src, dst);
   rows.put_done();
 }
 
+// Forward z-transform of the tile staged in buffer bf (barrier parity `parity`) into component
+// `comp` of the owned rows. `after()` runs once the first stage has read the buffer (after the
+// barrier that ends the stage), for the caller to start the next copy into it.
+template <class T, int N, int TL, int NT, class O, class Rows, class After, class TW>
+GBGHT_HD void z_forward_staged(const Cta& c, Cplx<T>* W, const ZStaging<T, N, TL>& stg, int bf, int parity, Rows& rows,
+                               int comp, const After& after, const TW& tw) {
+  stg.wait(bf, parity);
+  const ZStagedSource<T, N, TL> src{stg.buf(bf)};
+  const ZOwnSink<T, O, Rows> dst{rows, comp};
+  if constexpr (Radices<N>::n == 1) {
+    tile_fft_io<T, N, TL, NT, -1>(c, W, tw, src, dst);
+    after();
+  } else {
+    const TileBuf<T, TL, false> tb{W};
+    tile_fft_io<T, N, TL, NT, -1, false, TL, 0, 1>(c, W, tw, src, tb);
+    after();
+    tile_fft_io<T, N, TL, NT, -1, false, TL, 1>(c, W, tw, tb, dst);
+  }
+  rows.put_done();
+}
+
 // Inverse z-transform of the owned values x (retained rows) into A slot `slot` of the tile.
-template <class T, int N, int TL, int NT, class O>
+template <class T, int N, int TL, int NT, class O, class TW>
 GBGHT_HD void z_inverse_own(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* A, int slot, int qy, int kx0,
-                            const Cplx<T> (&x)[O::BPT][O::NSLOT], const Cplx<T>* GBGHT_RESTRICT tw) {
+                            const Cplx<T> (&x)[O::BPT][O::NSLOT], const TW& tw) {
   const ZOwnSource<T, N, O> src{g, x};
   const ZGlobalSink<T, N, TL> dst{g, A, slot, qy, kx0};
   tile_fft_io<T, N, TL, NT, +1>(c, W, tw, src, dst);
 }
 
 // Inverse z-transform of value(q, l) (retained rows q) into A slot `slot` of the tile.
-template <class T, int N, int TL, int NT, class F>
+template <class T, int N, int TL, int NT, class F, class TW>
 GBGHT_HD void z_inverse1(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* A, int slot, int qy, int kx0,
-                         const F& value, const Cplx<T>* GBGHT_RESTRICT tw) {
+                         const F& value, const TW& tw) {
   const ZValueSource<T, N, TL, F> src{g, value};
   const ZGlobalSink<T, N, TL> dst{g, A, slot, qy, kx0};
   tile_fft_io<T, N, TL, NT, +1>(c, W, tw, src, dst);
@@ -672,9 +811,9 @@ GBGHT_HD Cplx<T> curl_of(int o, Cplx<T> u0, Cplx<T> u1, Cplx<T> u2, T kX, T kY, 
 
 // The z-inverse of the owned velocity rows into A slots 0..2, and of iκ × û into slots 3..5
 // (3..5 only when `vorticity`).
-template <class T, int N, int TL, int NT, class O, class Rows>
+template <class T, int N, int TL, int NT, class O, class Rows, class TW>
 GBGHT_HD void z_inverse_velocity(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* A, int qy, int kx0, double ky,
-                                 const Rows& rows, int vorticity, const Cplx<T>* GBGHT_RESTRICT tw) {
+                                 const Rows& rows, int vorticity, const TW& tw) {
   for (int o = 0; o < 3; ++o) {
     Cplx<T> x[O::BPT][O::NSLOT];
 #pragma unroll
@@ -719,124 +858,185 @@ struct StageArgs {
 };
 
 template <class T, int N, int TL, int NT, class Rows>
-GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, double* red, const Geometry& g, Rows& rows,
-                                Cplx<T>* GBGHT_RESTRICT A, Cplx<T>* GBGHT_RESTRICT S, Cplx<T>* GBGHT_RESTRICT H, const StageArgs& st,
-                                const double* GBGHT_RESTRICT force_amp, const Cplx<T>* GBGHT_RESTRICT tw) {
+GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* bar, double* red, const Geometry& g,
+                                const TmaMaps& maps, Rows& rows, Cplx<T>* GBGHT_RESTRICT A, Cplx<T>* GBGHT_RESTRICT S,
+                                Cplx<T>* GBGHT_RESTRICT H, const StageArgs& st, const double* GBGHT_RESTRICT force_amp,
+                                const Cplx<T>* twS, unsigned int* status) {
   using O = ZOwn<T, N, TL, NT>;
+  using H0 = std::integral_constant<int, 0>;
+  const SharedTwiddles<T> tw{twS};
+  using H1 = std::integral_constant<int, 1>;
   const int kx0 = c.bx * TL, qy = c.by;
   const double s = g.s;
   const double ky = s * double(q_to_m(qy, g.K, g.NY2));
+  const bool withG = st.G[0] != 0.0 || st.G[1] != 0.0 || st.G[2] != 0.0;
+
+  // Staging: the three forward transforms of a part read A tiles copied into buffers 0, 1, 0 of
+  // the staging region; once the last has read its tile, the region takes the state of half 0,
+  // then (after a barrier) that of half 1. Buffer 0 and the state barrier complete two phases per
+  // part, buffer 1 one.
+  const ZStaging<T, N, TL> stg{g, A, maps, R, bar, status, qy, kx0};
+  const ZStateStaging<T, N, TL> sst{g, S, H, maps, R, bar + 2, status, qy, kx0};
+  int par1 = 0;
+  const auto forward3 = [&](int c0, const int* codes, int n) {
+    z_forward_staged<T, N, TL, NT, O>(c, W, stg, 0, 0, rows, 0, [&] { stg.issue(c, 0, c0 + 2); }, tw);
+    z_forward_staged<T, N, TL, NT, O>(c, W, stg, 1, par1, rows, 1, [] {}, tw);
+    par1 ^= 1;
+    z_forward_staged<T, N, TL, NT, O>(c, W, stg, 0, 1, rows, 2, [&] { sst.issue(c, 0, codes, n); }, tw);
+  };
 
   // ---------------- scalar -------------------------------------------------------------------------
   if (st.has_scalar) {
-    for (int o = 0; o < 3; ++o) z_forward_own<T, N, TL, NT, O>(c, W, g, A, 3 + o, qy, kx0, rows, o, tw);
+    stg.issue(c, 0, 3);
+    stg.issue(c, 1, 4);
+    int codes[6], n = 0;
+    codes[n++] = 3;                      // φ̂
+    if (!st.first) codes[n++] = 4 + 3;   // h_φ
+    const int iG = n;
+    if (withG) {                         // û for −G·û
+      codes[n++] = 0;
+      codes[n++] = 1;
+      codes[n++] = 2;
+    }
+    forward3(3, codes, n);
     Cplx<T> x[O::BPT][O::NSLOT];
-    for_own_slots<T, N, TL, NT>(c, g, [&](int b, int sl, bool ret, int q, int mz, int l) {
-      Cplx<T> fx, fy, fz;
-      rows.get3(b, sl, fx, fy, fz);
-      Cplx<T> phi = czero<T>();
+    const auto half = [&](auto hc) {
+      constexpr int h = decltype(hc)::value;
+      sst.wait(h);
+      for_own_slots<T, N, TL, NT, h>(c, g, [&](int b, int sl, bool ret, int q, int mz, int l) {
+        Cplx<T> fx, fy, fz;
+        rows.get3(b, sl, fx, fy, fz);
+        Cplx<T> phi = czero<T>();
+        if (ret) {
+          const int kx = kx0 + l;
+          const double kxd = s * double(kx), kzd = s * double(mz);
+          const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
+          const bool keep = kx <= g.K && k2 <= g.cut2;
+          const size_t si = idxS(g, 3, qy, q, kx);
+          phi = sst.at(0, q, h, l);
+          Cplx<T> nphi = czero<T>();
+          if (keep) {
+            // −i(κx fx + κy fy + κz fz)
+            const Cplx<T> dsum = cmk<T>(T(kxd) * fx.x + T(ky) * fy.x + T(kzd) * fz.x,
+                                        T(kxd) * fx.y + T(ky) * fy.y + T(kzd) * fz.y);
+            nphi = mul_mi(dsum);
+          }
+          if (withG) {
+            const Cplx<T> ux = sst.at(iG, q, h, l), uy = sst.at(iG + 1, q, h, l), uz = sst.at(iG + 2, q, h, l);
+            const T G0 = T(st.G[0]), G1 = T(st.G[1]), G2 = T(st.G[2]);
+            nphi = nphi - cmk<T>(G0 * ux.x + G1 * uy.x + G2 * uz.x, G0 * ux.y + G1 * uy.y + G2 * uz.y);
+          }
+          Cplx<T> hh = st.first ? scale(nphi, T(st.dt))
+                                : scale(sst.at(1, q, h, l), T(st.a)) + scale(nphi, T(st.dt));
+          const T E = T(exp(st.cphi * k2));
+          phi = scale(phi + scale(hh, T(st.b)), E);
+          S[si] = phi;
+          if (!st.last) H[si] = scale(hh, E);
+        }
+        x[b][sl] = phi;
+      });
+    };
+    half(H0{});
+    GBGHT_SYNC();
+    sst.issue(c, 1, codes, n);
+    half(H1{});
+    GBGHT_SYNC();
+    // the velocity part's first two tiles load during the scalar's inverse transform
+    stg.issue(c, 0, 0);
+    stg.issue(c, 1, 1);
+    z_inverse_own<T, N, TL, NT, O>(c, W, g, A, 6, qy, kx0, x, tw);
+  } else {
+    stg.issue(c, 0, 0);
+    stg.issue(c, 1, 1);
+  }
+
+  // ---------------- velocity -----------------------------------------------------------------------
+  int codes[6], n = 0;
+  codes[n++] = 0;
+  codes[n++] = 1;
+  codes[n++] = 2;
+  if (!st.first) {
+    codes[n++] = 4;
+    codes[n++] = 5;
+    codes[n++] = 6;
+  }
+  forward3(0, codes, n);
+  const double A_f = st.forced ? force_amp[0] : 0.0;
+  double esum = 0.0;
+  const auto half = [&](auto hc) {
+    constexpr int h = decltype(hc)::value;
+    sst.wait(h);
+    for_own_slots<T, N, TL, NT, h>(c, g, [&](int b, int sl, bool ret, int q, int mz, int l) {
+      Cplx<T> f0, f1, f2;
+      rows.get3(b, sl, f0, f1, f2);
+      Cplx<T> u0 = czero<T>(), u1 = czero<T>(), u2 = czero<T>();
       if (ret) {
         const int kx = kx0 + l;
         const double kxd = s * double(kx), kzd = s * double(mz);
         const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
         const bool keep = kx <= g.K && k2 <= g.cut2;
-        const size_t si = idxS(g, 3, qy, q, kx);
-        phi = S[si];
-        Cplx<T> nphi = czero<T>();
-        if (keep) {
-          // −i(κx fx + κy fy + κz fz)
-          const Cplx<T> dsum = cmk<T>(T(kxd) * fx.x + T(ky) * fy.x + T(kzd) * fz.x,
-                                      T(kxd) * fx.y + T(ky) * fy.y + T(kzd) * fz.y);
-          nphi = mul_mi(dsum);
-        }
-        if (st.G[0] != 0.0 || st.G[1] != 0.0 || st.G[2] != 0.0) {
-          const Cplx<T> ux = S[idxS(g, 0, qy, q, kx)], uy = S[idxS(g, 1, qy, q, kx)],
-                        uz = S[idxS(g, 2, qy, q, kx)];
-          const T G0 = T(st.G[0]), G1 = T(st.G[1]), G2 = T(st.G[2]);
-          nphi = nphi - cmk<T>(G0 * ux.x + G1 * uy.x + G2 * uz.x, G0 * ux.y + G1 * uy.y + G2 * uz.y);
-        }
-        Cplx<T> h = st.first ? scale(nphi, T(st.dt))
-                             : scale(H[si], T(st.a)) + scale(nphi, T(st.dt));
-        const T E = T(exp(st.cphi * k2));
-        phi = scale(phi + scale(h, T(st.b)), E);
-        S[si] = phi;
-        if (!st.last) H[si] = scale(h, E);
-      }
-      x[b][sl] = phi;
-    });
-    z_inverse_own<T, N, TL, NT, O>(c, W, g, A, 6, qy, kx0, x, tw);
-  }
-
-  // ---------------- velocity -----------------------------------------------------------------------
-  for (int o = 0; o < 3; ++o) z_forward_own<T, N, TL, NT, O>(c, W, g, A, o, qy, kx0, rows, o, tw);
-  const double A_f = st.forced ? force_amp[0] : 0.0;
-  double esum = 0.0;
-  for_own_slots<T, N, TL, NT>(c, g, [&](int b, int sl, bool ret, int q, int mz, int l) {
-    Cplx<T> f0, f1, f2;
-    rows.get3(b, sl, f0, f1, f2);
-    Cplx<T> u0 = czero<T>(), u1 = czero<T>(), u2 = czero<T>();
-    if (ret) {
-      const int kx = kx0 + l;
-      const double kxd = s * double(kx), kzd = s * double(mz);
-      const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
-      const bool keep = kx <= g.K && k2 <= g.cut2;
-      const size_t s0 = idxS(g, 0, qy, q, kx), s1 = idxS(g, 1, qy, q, kx), s2 = idxS(g, 2, qy, q, kx);
-      u0 = S[s0];
-      u1 = S[s1];
-      u2 = S[s2];
-      Cplx<T> n0 = czero<T>(), n1 = czero<T>(), n2 = czero<T>();
-      if (keep && k2 > 0.0) {
-        const T kX = T(kxd), kY = T(ky), kZ = T(kzd);
-        const T ik2 = T(1.0 / k2);
-        const Cplx<T> kd = cmk<T>((kX * f0.x + kY * f1.x + kZ * f2.x) * ik2, (kX * f0.y + kY * f1.y + kZ * f2.y) * ik2);
-        n0 = f0 - scale(kd, kX);
-        n1 = f1 - scale(kd, kY);
-        n2 = f2 - scale(kd, kZ);
-      }
-      if (A_f != 0.0 && k2 >= st.band_lo2 && k2 <= st.band_hi2) {
-        const T Af = T(A_f);
-        n0 = n0 + scale(u0, Af);
-        n1 = n1 + scale(u1, Af);
-        n2 = n2 + scale(u2, Af);
-      }
-      const T dt = T(st.dt), a = T(st.a), bb = T(st.b);
-      Cplx<T> h0, h1, h2;
-      if (st.first) {
-        h0 = scale(n0, dt); h1 = scale(n1, dt); h2 = scale(n2, dt);
-      } else {
-        h0 = scale(H[s0], a) + scale(n0, dt);
-        h1 = scale(H[s1], a) + scale(n1, dt);
-        h2 = scale(H[s2], a) + scale(n2, dt);
-      }
-      const T E = T(exp(st.cu * k2));
-      u0 = scale(u0 + scale(h0, bb), E);
-      u1 = scale(u1 + scale(h1, bb), E);
-      u2 = scale(u2 + scale(h2, bb), E);
-      if (st.last) {
-        if (k2 > 0.0) {
+        const size_t s0 = idxS(g, 0, qy, q, kx), s1 = idxS(g, 1, qy, q, kx), s2 = idxS(g, 2, qy, q, kx);
+        u0 = sst.at(0, q, h, l);
+        u1 = sst.at(1, q, h, l);
+        u2 = sst.at(2, q, h, l);
+        Cplx<T> n0 = czero<T>(), n1 = czero<T>(), n2 = czero<T>();
+        if (keep && k2 > 0.0) {
           const T kX = T(kxd), kY = T(ky), kZ = T(kzd);
           const T ik2 = T(1.0 / k2);
-          const Cplx<T> kd = cmk<T>((kX * u0.x + kY * u1.x + kZ * u2.x) * ik2, (kX * u0.y + kY * u1.y + kZ * u2.y) * ik2);
-          u0 = u0 - scale(kd, kX);
-          u1 = u1 - scale(kd, kY);
-          u2 = u2 - scale(kd, kZ);
+          const Cplx<T> kd = cmk<T>((kX * f0.x + kY * f1.x + kZ * f2.x) * ik2, (kX * f0.y + kY * f1.y + kZ * f2.y) * ik2);
+          n0 = f0 - scale(kd, kX);
+          n1 = f1 - scale(kd, kY);
+          n2 = f2 - scale(kd, kZ);
         }
-      } else {
-        H[s0] = scale(h0, E);
-        H[s1] = scale(h1, E);
-        H[s2] = scale(h2, E);
+        if (A_f != 0.0 && k2 >= st.band_lo2 && k2 <= st.band_hi2) {
+          const T Af = T(A_f);
+          n0 = n0 + scale(u0, Af);
+          n1 = n1 + scale(u1, Af);
+          n2 = n2 + scale(u2, Af);
+        }
+        const T dt = T(st.dt), a = T(st.a), bb = T(st.b);
+        Cplx<T> h0, h1, h2;
+        if (st.first) {
+          h0 = scale(n0, dt); h1 = scale(n1, dt); h2 = scale(n2, dt);
+        } else {
+          h0 = scale(sst.at(3, q, h, l), a) + scale(n0, dt);
+          h1 = scale(sst.at(4, q, h, l), a) + scale(n1, dt);
+          h2 = scale(sst.at(5, q, h, l), a) + scale(n2, dt);
+        }
+        const T E = T(exp(st.cu * k2));
+        u0 = scale(u0 + scale(h0, bb), E);
+        u1 = scale(u1 + scale(h1, bb), E);
+        u2 = scale(u2 + scale(h2, bb), E);
+        if (st.last) {
+          if (k2 > 0.0) {
+            const T kX = T(kxd), kY = T(ky), kZ = T(kzd);
+            const T ik2 = T(1.0 / k2);
+            const Cplx<T> kd = cmk<T>((kX * u0.x + kY * u1.x + kZ * u2.x) * ik2, (kX * u0.y + kY * u1.y + kZ * u2.y) * ik2);
+            u0 = u0 - scale(kd, kX);
+            u1 = u1 - scale(kd, kY);
+            u2 = u2 - scale(kd, kZ);
+          }
+        } else {
+          H[s0] = scale(h0, E);
+          H[s1] = scale(h1, E);
+          H[s2] = scale(h2, E);
+        }
+        S[s0] = u0;
+        S[s1] = u1;
+        S[s2] = u2;
+        const double w = kx == 0 ? 1.0 : 2.0;
+        esum += w * ((double(u0.x) * u0.x + double(u0.y) * u0.y) + (double(u1.x) * u1.x + double(u1.y) * u1.y) +
+                     (double(u2.x) * u2.x + double(u2.y) * u2.y));
       }
-      S[s0] = u0;
-      S[s1] = u1;
-      S[s2] = u2;
-      const double w = kx == 0 ? 1.0 : 2.0;
-      esum += w * ((double(u0.x) * u0.x + double(u0.y) * u0.y) + (double(u1.x) * u1.x + double(u1.y) * u1.y) +
-                   (double(u2.x) * u2.x + double(u2.y) * u2.y));
-    }
-    rows.put(0, b, sl, u0);
-    rows.put(1, b, sl, u1);
-    rows.put(2, b, sl, u2);
-  });
+      rows.put(0, b, sl, u0);
+      rows.put(1, b, sl, u1);
+      rows.put(2, b, sl, u2);
+    });
+  };
+  half(H0{});
+  GBGHT_SYNC();
+  sst.issue(c, 1, codes, n);
+  half(H1{});
   rows.put_done();
   red[c.tid] = esum;
   GBGHT_SYNC();
