@@ -285,6 +285,7 @@ class EngineImpl final : public Engine {
     const char* err = rt_memset(maxbits_, 0, sizeof(unsigned long long), stream_);
     if (err) return err;
     y_inverse(0, 3);
+    bu_fresh_ = true;
     x_velocity();
     if ((err = rt_check())) return err;
     unsigned long long bits = 0;
@@ -700,6 +701,7 @@ class EngineImpl final : public Engine {
 #endif
   }
   const char* z_init() {
+    bu_fresh_ = false;   // A is rewritten
 #ifdef GBGHT_EMU
     const int gx = g_.KXP / TLZ;
     emu_grid(gx, g_.NY2, 1, smem_z(), [&](const Cta& c, void* sm) {
@@ -758,7 +760,10 @@ class EngineImpl final : public Engine {
   const char* stage(const StageArgs& st) {
     const int ninv = p_.scalar ? 7 : 6;
     const int nfwd = p_.scalar ? 6 : 3;
-    y_inverse(0, ninv);
+    // B slots 0..2 still hold the deposit's y-inverse of the same A slots at a step's first stage
+    if (st.first && bu_fresh_) y_inverse(3, ninv - 3);
+    else y_inverse(0, ninv);
+    bu_fresh_ = false;
     x_products();
     y_forward(nfwd);
     if (st.forced) force_amp();
@@ -784,6 +789,7 @@ class EngineImpl final : public Engine {
   size_t nS_ = 0, nA_ = 0, nB_ = 0, nP_ = 0, ntile_ = 0;
   int nshell_ = 0;
   int sm_count_ = 4;
+  bool bu_fresh_ = false;   // B slots 0..2 = y-inverse of the current A slots 0..2 (set by the deposit)
   Stream stream_ = nullptr;
   std::vector<void*> allocs_;
   Cplx<T>*S_ = nullptr, *H_ = nullptr, *A_ = nullptr, *B_ = nullptr, *tw_ = nullptr;

@@ -1,11 +1,12 @@
 // Warp-per-line FFT: each warp owns whole lines of length N in shared memory and transforms them
 // with no block-wide barrier (its radix stages are separated by __syncwarp only).
 //
-// A line is N contiguous complex elements, XOR-swizzled within each 128-byte row: element e sits
-// at lidx(e) = e with its 16-byte chunk index (e mod 8 for FP64, (e/2) mod 8 for FP32) XORed with
-// the row index mod 8. Every access pattern of the Stockham stages below is then free of bank
-// conflicts for FP64. Those patterns are: reads x[j + r·N/R], writes y[(j/NS)·NS·R + j mod NS + r·NS],
-// and the column walks of the x pass.
+// A line is N contiguous complex elements, XOR-swizzled within each 128-byte row. For FP64, element
+// e sits at lidx(e) = e with its 16-byte chunk index (e mod 8) XORed with the row index mod 8. For FP32,
+// the element's index within its row (e mod 16) is XORed with (5 × row) mod 16. The access patterns
+// of the Stockham stages below are reads x[j + r·N/R], writes y[(j/NS)·NS·R + j mod NS + r·NS], and
+// the column walks of the x pass. FP64 serves them free of bank conflicts. FP32 is conflict-free on
+// the 512-point plan and within 6% of the ideal wavefront count on the others.
 //
 // The algorithm is the Stockham autosort of fft_tile.cuh (same radices, same twiddles, same
 // results), with butterfly j of a stage taken by lane j mod 32 of the owning warp. As there, the
@@ -24,7 +25,7 @@ namespace gbght {
 template <class T>
 GBGHT_HD int lidx(int e) {
   if constexpr (sizeof(Cplx<T>) == 16) return e ^ ((e >> 3) & 7);
-  else return e ^ (((e >> 4) & 7) << 1);
+  else return e ^ (((e >> 4) * 5) & 15);
 }
 
 GBGHT_HD void warp_sync() {
