@@ -222,7 +222,7 @@ def e2e_run(args, precision, device, inputs, K):
     run.deposit_tracers(0.0)
     for _ in range(K):
         run.advance(None)
-    u, p = run.export_state()
+    u, p = run.export_state(out=(pu, pp))
     run.synchronize()
     el = time.perf_counter() - t0
     h2d = puh.nbytes + pph.nbytes + pX.nbytes + K * 8

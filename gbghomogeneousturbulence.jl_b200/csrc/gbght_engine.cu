@@ -27,6 +27,7 @@ static void rt_free(void* p) { std::free(p); }
 static const char* rt_memset(void* p, int v, size_t n, Stream) { std::memset(p, v, n); return nullptr; }
 static const char* rt_h2d(void* d, const void* h, size_t n, Stream) { std::memcpy(d, h, n); return nullptr; }
 static const char* rt_d2h(void* h, const void* d, size_t n, Stream) { std::memcpy(h, d, n); return nullptr; }
+static const char* rt_d2d(void* d, const void* s, size_t n, Stream) { std::memcpy(d, s, n); return nullptr; }
 static const char* rt_sync(Stream) { return nullptr; }
 static const char* rt_check() { return nullptr; }
 #else
@@ -46,6 +47,9 @@ static void rt_free(void* p) { if (p) cudaFree(p); }
 static const char* rt_memset(void* p, int v, size_t n, Stream s) { return cuda_err(cudaMemsetAsync(p, v, n, s), "cudaMemsetAsync"); }
 static const char* rt_h2d(void* d, const void* h, size_t n, Stream s) {
   return cuda_err(cudaMemcpyAsync(d, h, n, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync H2D");
+}
+static const char* rt_d2d(void* d, const void* src, size_t n, Stream s) {
+  return cuda_err(cudaMemcpyAsync(d, src, n, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync D2D");
 }
 static const char* rt_d2h(void* h, const void* d, size_t n, Stream s) {
   const char* e = cuda_err(cudaMemcpyAsync(h, d, n, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync D2H");
@@ -174,6 +178,9 @@ class EngineImpl final : public Engine {
     if ((err = alloc(&amp_, 4 * sizeof(double)))) return err;
     if ((err = alloc(&maxbits_, sizeof(unsigned long long)))) return err;
     if ((err = alloc(&status_, sizeof(unsigned int)))) return err;
+    if ((err = alloc(&flag_, sizeof(unsigned int)))) return err;
+    // B doubles as the staging of one reference-layout component at import and export
+    if (7 * nB_ * sizeof(Cplx<T>) < ref_comp_elems() * sizeof(Cplx<double>)) return "B too small to stage a component";
     if ((err = alloc(&obs_, size_t(g_.NY2) * 4 * sizeof(double)))) return err;
     if ((err = alloc(&spec_, size_t(g_.NY2) * nshell_ * sizeof(double)))) return err;
     if (p.tracers > 0) {
@@ -197,61 +204,56 @@ class EngineImpl final : public Engine {
   double cutoff() const override { return cutoff_; }
 
   // ---- state import / export (host arrays in the reference layout) ------------------------------
+  // Each component crosses in the reference layout through B (scratch between steps), and a
+  // kernel converts it on the device. Import compacts into H, which is dead between steps, so a
+  // refused import (content outside the retained ball) leaves S as it was.
+  size_t ref_comp_elems() const { return size_t(N) * N * (N / 2 + 1); }
   const char* import_state(const double* uh, const double* ph, bool* outside) override {
-    const int NH = N / 2 + 1;
     const int nc = p_.scalar ? 4 : 3;
-    std::vector<Cplx<T>> host(4 * nS_, czero<T>());
+    const size_t nref = ref_comp_elems();
     *outside = false;
-    for (int cc = 0; cc < nc; ++cc) {
-      const double* src = cc < 3 ? uh + size_t(cc) * N * N * NH * 2 : ph;
-      for (int kz = 0; kz < N; ++kz)
-        for (int ky = 0; ky < N; ++ky)
-          for (int kx = 0; kx < NH; ++kx) {
-            const size_t si = ((size_t(kz) * N + ky) * NH + kx) * 2;
-            const double re = src[si], im = src[si + 1];
-            const int my = ky <= N / 2 ? ky : ky - N, mz = kz <= N / 2 ? kz : kz - N;
-            const bool in_box = kx <= g_.K && std::abs(my) <= g_.K && std::abs(mz) <= g_.K &&
-                                !(N % 2 == 0 && (ky == N / 2 || kz == N / 2));
-            bool retained = false;
-            if (in_box) {
-              const double kxd = g_.s * kx, kyd = g_.s * my, kzd = g_.s * mz;
-              retained = (kxd * kxd + kyd * kyd) + kzd * kzd <= g_.cut2;
-            }
-            if (!retained) {
-              if (re != 0.0 || im != 0.0) *outside = true;
-              continue;
-            }
-            const int qy = my >= 0 ? my : my + g_.NY2, qz = mz >= 0 ? mz : mz + g_.NY2;
-            host[idxS(g_, cc, qy, qz, kx)] = cmk<T>(T(re), T(im));
-          }
+    bu_fresh_ = false;   // B is overwritten
+    Cplx<double>* ref = reinterpret_cast<Cplx<double>*>(B_);
+    const char* err = rt_memset(H_, 0, 4 * nS_ * sizeof(Cplx<T>), stream_);
+    if (!err) err = rt_memset(flag_, 0, sizeof(unsigned int), stream_);
+    for (int cc = 0; cc < nc && !err; ++cc) {
+      const double* src = cc < 3 ? uh + size_t(cc) * nref * 2 : ph;
+      err = rt_h2d(ref, src, nref * sizeof(Cplx<double>), stream_);
+      if (err) break;
+#ifdef GBGHT_EMU
+      for (size_t i = 0; i < nref; ++i) import_mode<T>(i, g_, ref, H_ + cc * nS_, flag_);
+#else
+      k_import<T><<<unsigned((nref + 255) / 256), 256, 0, stream_>>>(g_, ref, H_ + cc * nS_, flag_);
+      err = rt_check();
+#endif
     }
-    if (*outside) return nullptr;
-    const char* err = rt_h2d(S_, host.data(), 4 * nS_ * sizeof(Cplx<T>), stream_);
+    unsigned int fl = 0;
+    if (!err) err = rt_d2h(&fl, flag_, sizeof fl, stream_);
     if (err) return err;
+    if (fl & 1u) {
+      *outside = true;
+      return nullptr;
+    }
+    if ((err = rt_d2d(S_, H_, 4 * nS_ * sizeof(Cplx<T>), stream_))) return err;
     if ((err = rt_memset(H_, 0, 4 * nS_ * sizeof(Cplx<T>), stream_))) return err;
     if ((err = z_init())) return err;
     return rt_sync(stream_);
   }
 
   const char* export_state(double* uh, double* ph) override {
-    const int NH = N / 2 + 1;
-    std::vector<Cplx<T>> host(4 * nS_);
-    const char* err = rt_d2h(host.data(), S_, 4 * nS_ * sizeof(Cplx<T>), stream_);
-    if (err) return err;
+    const size_t nref = ref_comp_elems();
     const int nc = (p_.scalar && ph) ? 4 : 3;
+    bu_fresh_ = false;   // B is overwritten
+    Cplx<double>* ref = reinterpret_cast<Cplx<double>*>(B_);
     for (int cc = 0; cc < nc; ++cc) {
-      double* dst = cc < 3 ? uh + size_t(cc) * N * N * NH * 2 : ph;
-      std::memset(dst, 0, size_t(N) * N * NH * 2 * sizeof(double));
-      for (int qy = 0; qy < g_.NY2; ++qy)
-        for (int qz = 0; qz < g_.NY2; ++qz)
-          for (int kx = 0; kx <= g_.K; ++kx) {
-            const int my = q_to_m(qy, g_.K, g_.NY2), mz = q_to_m(qz, g_.K, g_.NY2);
-            const int ky = my >= 0 ? my : my + N, kz = mz >= 0 ? mz : mz + N;
-            const Cplx<T> v = host[idxS(g_, cc, qy, qz, kx)];
-            const size_t di = ((size_t(kz) * N + ky) * NH + kx) * 2;
-            dst[di] = double(v.x);
-            dst[di + 1] = double(v.y);
-          }
+      double* dst = cc < 3 ? uh + size_t(cc) * nref * 2 : ph;
+#ifdef GBGHT_EMU
+      for (size_t i = 0; i < nref; ++i) export_mode<T>(i, g_, S_ + cc * nS_, ref);
+#else
+      k_export<T><<<unsigned((nref + 255) / 256), 256, 0, stream_>>>(g_, S_ + cc * nS_, ref);
+      if (const char* e = rt_check()) return e;
+#endif
+      if (const char* e = rt_d2h(dst, ref, nref * sizeof(Cplx<double>), stream_)) return e;
     }
     return nullptr;
   }
@@ -798,6 +800,7 @@ class EngineImpl final : public Engine {
   double *X_ = nullptr, *F_ = nullptr;
   unsigned long long* maxbits_ = nullptr;
   unsigned int* status_ = nullptr;
+  unsigned int* flag_ = nullptr;     // import: content outside the retained ball
 };
 
 #if defined(GBGHT_UNIT_FACTORY)

@@ -206,6 +206,14 @@ __global__ void k_tracers(int64_t M, int mode, const T* u, int N, double L, doub
   if (p < M) tracer_one<T>(p, M, mode, u, N, L, X, F, w);
 }
 template <class T>
+__global__ void k_import(Geometry g, const Cplx<double>* ref, Cplx<T>* Sc, unsigned int* flag) {
+  import_mode<T>(size_t(blockIdx.x) * blockDim.x + threadIdx.x, g, ref, Sc, flag);
+}
+template <class T>
+__global__ void k_export(Geometry g, const Cplx<T>* Sc, Cplx<double>* ref) {
+  export_mode<T>(size_t(blockIdx.x) * blockDim.x + threadIdx.x, g, Sc, ref);
+}
+template <class T>
 __global__ void k_to_T(const double* in, T* out, size_t n) {
   const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < n) out[i] = T(in[i]);

@@ -1138,6 +1138,53 @@ GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, double* red, const Geometr
 }
 
 // ================================================================================================
+// State import and export: one component in the reference layout [kz][ky][kx] (kx ≤ N/2,
+// complex128) against one compact S component. One thread per reference mode i.
+// Import keeps the retained 2/3 ball and reports content anywhere else (Nyquist planes included)
+// in bit 0 of `flag`; export writes the compact box and zero elsewhere.
+// ================================================================================================
+template <class T>
+GBGHT_HD void import_mode(size_t i, const Geometry& g, const Cplx<double>* ref, Cplx<T>* Sc, unsigned int* flag) {
+  const int N = g.N, NH = N / 2 + 1;
+  if (i >= size_t(N) * N * NH) return;
+  const int kx = int(i % NH), ky = int((i / NH) % N), kz = int(i / (size_t(NH) * N));
+  const Cplx<double> v = ref[i];
+  const int my = ky <= N / 2 ? ky : ky - N, mz = kz <= N / 2 ? kz : kz - N;
+  const bool in_box = kx <= g.K && (my < 0 ? -my : my) <= g.K && (mz < 0 ? -mz : mz) <= g.K &&
+                      !(N % 2 == 0 && (ky == N / 2 || kz == N / 2));
+  bool retained = false;
+  if (in_box) {
+    const double kxd = g.s * kx, kyd = g.s * my, kzd = g.s * mz;
+    retained = (kxd * kxd + kyd * kyd) + kzd * kzd <= g.cut2;
+  }
+  if (retained) {
+    const int qy = my >= 0 ? my : my + g.NY2, qz = mz >= 0 ? mz : mz + g.NY2;
+    Sc[idxS(g, 0, qy, qz, kx)] = cmk<T>(T(v.x), T(v.y));
+  } else if (v.x != 0.0 || v.y != 0.0) {
+#ifdef __CUDA_ARCH__
+    atomicOr(flag, 1u);
+#else
+    *flag |= 1u;
+#endif
+  }
+}
+
+template <class T>
+GBGHT_HD void export_mode(size_t i, const Geometry& g, const Cplx<T>* Sc, Cplx<double>* ref) {
+  const int N = g.N, NH = N / 2 + 1;
+  if (i >= size_t(N) * N * NH) return;
+  const int kx = int(i % NH), ky = int((i / NH) % N), kz = int(i / (size_t(NH) * N));
+  const int my = ky <= N / 2 ? ky : ky - N, mz = kz <= N / 2 ? kz : kz - N;
+  Cplx<double> v = cmk<double>(0.0, 0.0);
+  if (kx <= g.K && (my < 0 ? -my : my) <= g.K && (mz < 0 ? -mz : mz) <= g.K) {
+    const int qy = my >= 0 ? my : my + g.NY2, qz = mz >= 0 ? mz : mz + g.NY2;
+    const Cplx<T> w = Sc[idxS(g, 0, qy, qz, kx)];
+    v = cmk<double>(double(w.x), double(w.y));
+  }
+  ref[i] = v;
+}
+
+// ================================================================================================
 // Observables: per ky' row, the Hermitian-weighted sums Σ|û|², Σκ²|û|², Σ|φ̂|², Σκ²|φ̂|²
 // (unnormalised), summed per thread and then in thread order. Grid: (NY2). `red` holds 4·NT.
 // ================================================================================================

@@ -237,9 +237,21 @@ class Run:
         self._check(self.lib.gbght_state_import(self.h, u.view(np.float64).ctypes.data_as(_DP),
                                                 None if p is None else p.view(np.float64).ctypes.data_as(_DP)))
 
-    def export_state(self):
-        u = np.zeros((3,) + self.spectral_shape, np.complex128)
-        p = np.zeros(self.spectral_shape, np.complex128) if self.setup.scalar else None
+    def export_state(self, out=None):
+        """û (and φ̂) in the reference layout. `out = (u, p)` receives them in place (contiguous
+        complex128 arrays of the right shapes, e.g. in pinned memory); by default new arrays."""
+        if out is None:
+            u = np.zeros((3,) + self.spectral_shape, np.complex128)
+            p = np.zeros(self.spectral_shape, np.complex128) if self.setup.scalar else None
+        else:
+            u, p = out
+            if u.dtype != np.complex128 or u.shape != (3,) + self.spectral_shape or not u.flags.c_contiguous:
+                raise ValueError(f"out u must be a contiguous complex128 array of shape {(3,) + self.spectral_shape}")
+            if self.setup.scalar and (p is None or p.dtype != np.complex128 or p.shape != self.spectral_shape
+                                      or not p.flags.c_contiguous):
+                raise ValueError(f"out p must be a contiguous complex128 array of shape {self.spectral_shape}")
+            if not self.setup.scalar:
+                p = None
         self._check(self.lib.gbght_state_export(self.h, u.view(np.float64).ctypes.data_as(_DP),
                                                 None if p is None else p.view(np.float64).ctypes.data_as(_DP)))
         return u, p
