@@ -150,7 +150,8 @@ def algorithmic_bytes_per_step(N, K, w_complex, has_scalar=True):
 
 def launches_per_step(has_scalar=True, forced=True):
     return {"y_inverse": 6, "x_products": 5, "y_forward": 5, "z_epilogue": 5, "x_velocity": 1,
-            "force_amp": 5 if forced else 0, "reality": 1, "tracers": 1, "observables": 1 if has_scalar else 0}
+            "force_amp": 5 if forced else 0, "reality": 1, "tracers": 1, "observables": 1 if has_scalar else 0,
+            "traversal": 3}
 
 
 def make_inputs(N, M, seed_base=0):

@@ -184,8 +184,14 @@ class EngineImpl final : public Engine {
     if ((err = alloc(&obs_, size_t(g_.NY2) * 4 * sizeof(double)))) return err;
     if ((err = alloc(&spec_, size_t(g_.NY2) * nshell_ * sizeof(double)))) return err;
     if (p.tracers > 0) {
+      if (p.tracers > int64_t(UINT32_MAX)) return "too many tracers for a 32-bit traversal order";
       if ((err = alloc(&X_, 3 * size_t(p.tracers) * sizeof(double)))) return err;
       if ((err = alloc(&F_, 3 * size_t(p.tracers) * sizeof(double)))) return err;
+      const size_t nt = size_t(traversal_tiles(N));
+      nbins_ = int(nt * nt * nt);
+      if ((err = alloc(&tkey_, size_t(p.tracers) * sizeof(uint32_t)))) return err;
+      if ((err = alloc(&torder_, size_t(p.tracers) * sizeof(uint32_t)))) return err;
+      if ((err = alloc(&tcount_, size_t(nbins_) * sizeof(uint32_t)))) return err;
     }
 #ifndef GBGHT_EMU
     if ((err = make_maps())) return err;
@@ -386,7 +392,8 @@ class EngineImpl final : public Engine {
   }
   const char* tracers_run(int mode, HeunWeights w) override {
     if (!X_) return "the run carries no tracers";
-    run_tracers(p_.tracers, mode, X_, F_, w);
+    if (const char* e = rebuild_traversal()) return e;
+    run_tracers(p_.tracers, mode, X_, F_, w, torder_);
     return rt_check();
   }
   const char* gather(const double* X, int64_t M, double* out) override {
@@ -773,15 +780,48 @@ class EngineImpl final : public Engine {
     if (st.last) reality();
     return rt_check();
   }
-  void run_tracers(int64_t M, int mode, double* X, double* F, HeunWeights w) {
+  void run_tracers(int64_t M, int mode, double* X, double* F, HeunWeights w, const uint32_t* order = nullptr) {
 #ifdef GBGHT_EMU
-    for (int64_t p = 0; p < M; ++p) tracer_one<T>(p, M, mode, U_, N, p_.L, X, F, w);
+    for (int64_t i = 0; i < M; ++i) tracer_one<T>(order ? int64_t(order[i]) : i, M, mode, U_, N, p_.L, X, F, w);
 #else
     const int bs = 128;
     pbegin(PROF_TRACERS);
-    k_tracers<T><<<unsigned((M + bs - 1) / bs), bs, 0, stream_>>>(M, mode, U_, N, p_.L, X, F, w);
+    k_tracers<T><<<unsigned((M + bs - 1) / bs), bs, 0, stream_>>>(M, mode, U_, N, p_.L, X, F, w, order);
     pend();
 #endif
+  }
+  // The traversal order of the run's tracers from their current positions (rebuilt before every
+  // tracer pass, as the reference's automatic mode does each iteration).
+  const char* rebuild_traversal() {
+    const int64_t M = p_.tracers;
+    const double dx = div_rn(p_.L, double(N));
+    const char* err = rt_memset(tcount_, 0, size_t(nbins_) * sizeof(uint32_t), stream_);
+    if (err) return err;
+#ifdef GBGHT_EMU
+    for (int64_t p = 0; p < M; ++p) {
+      tkey_[p] = traversal_key(X_, p, M, N, dx);
+      ++tcount_[tkey_[p]];
+    }
+    uint32_t run = 0;
+    for (int b = 0; b < nbins_; ++b) {
+      const uint32_t c = tcount_[b];
+      tcount_[b] = run;
+      run += c;
+    }
+    for (int64_t p = 0; p < M; ++p) torder_[tcount_[tkey_[p]]++] = uint32_t(p);
+#else
+    const unsigned grid = unsigned((M + 255) / 256);
+    pbegin(PROF_TRAVERSAL);
+    k_trav_count<<<grid, 256, 0, stream_>>>(M, X_, N, dx, tkey_, tcount_);
+    pend();
+    pbegin(PROF_TRAVERSAL);
+    k_trav_scan<<<1, kScanThreads, 0, stream_>>>(tcount_, nbins_);
+    pend();
+    pbegin(PROF_TRAVERSAL);
+    k_trav_scatter<<<grid, 256, 0, stream_>>>(M, tkey_, tcount_, torder_);
+    pend();
+#endif
+    return rt_check();
   }
 
   RunParams p_{};
@@ -801,6 +841,8 @@ class EngineImpl final : public Engine {
   unsigned long long* maxbits_ = nullptr;
   unsigned int* status_ = nullptr;
   unsigned int* flag_ = nullptr;     // import: content outside the retained ball
+  uint32_t *tkey_ = nullptr, *torder_ = nullptr, *tcount_ = nullptr;   // the traversal sort
+  int nbins_ = 0;
 };
 
 #if defined(GBGHT_UNIT_FACTORY)

@@ -85,7 +85,8 @@ enum ProfileKind {
   PROF_REALITY = 6,
   PROF_TRACERS = 7,
   PROF_OBSERVABLES = 8,
-  PROF_KINDS = 9
+  PROF_TRAVERSAL = 9,
+  PROF_KINDS = 10
 };
 
 Engine* make_engine(int N, int precision, std::string* err);

@@ -201,9 +201,48 @@ __global__ void __launch_bounds__(NT) k_spectrum(Geometry g, const Cplx<T>* S, i
   body_spectrum<T, NT>(c, hist, hist + nshell, g, S, c0, nc, nshell, out);
 }
 template <class T>
-__global__ void k_tracers(int64_t M, int mode, const T* u, int N, double L, double* X, double* F, HeunWeights w) {
+__global__ void k_tracers(int64_t M, int mode, const T* u, int N, double L, double* X, double* F, HeunWeights w,
+                          const uint32_t* order) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < M) tracer_one<T>(order ? int64_t(order[i]) : i, M, mode, u, N, L, X, F, w);
+}
+
+// The traversal rebuild, a counting sort by tile: keys and tile counts, an exclusive scan of the
+// counts (one block), then each tracer takes the next slot of its tile. The order within a tile
+// follows the atomics and may differ between rebuilds; the gathers' results do not depend on it.
+static __global__ void k_trav_count(int64_t M, const double* X, int N, double dx, uint32_t* key, uint32_t* count) {
   const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (p < M) tracer_one<T>(p, M, mode, u, N, L, X, F, w);
+  if (p >= M) return;
+  const uint32_t k = traversal_key(X, p, M, N, dx);
+  key[p] = k;
+  atomicAdd(count + k, 1u);
+}
+constexpr int kScanThreads = 1024;
+static __global__ void __launch_bounds__(kScanThreads) k_trav_scan(uint32_t* count, int nbins) {
+  __shared__ uint32_t part[kScanThreads];
+  const int per = (nbins + kScanThreads - 1) / kScanThreads;
+  const int b0 = int(threadIdx.x) * per, b1 = min(nbins, b0 + per);
+  uint32_t s = 0;
+  for (int b = b0; b < b1; ++b) s += count[b];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int off = 1; off < kScanThreads; off <<= 1) {   // inclusive scan of the partial sums
+    const uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  uint32_t run = threadIdx.x == 0 ? 0u : part[threadIdx.x - 1];
+  for (int b = b0; b < b1; ++b) {
+    const uint32_t c = count[b];
+    count[b] = run;
+    run += c;
+  }
+}
+static __global__ void k_trav_scatter(int64_t M, const uint32_t* key, uint32_t* offset, uint32_t* order) {
+  const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= M) return;
+  order[atomicAdd(offset + key[p], 1u)] = uint32_t(p);
 }
 template <class T>
 __global__ void k_import(Geometry g, const Cplx<double>* ref, Cplx<T>* Sc, unsigned int* flag) {

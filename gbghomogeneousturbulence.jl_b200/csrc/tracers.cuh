@@ -109,6 +109,21 @@ GBGHT_HD void gather3(const T* GBGHT_RESTRICT u, int N, double dx, double x, dou
   }
 }
 
+// Traversal order (src/Particles.jl:220-271): tracers are visited tile by tile, in tiles of 8³
+// cells, so the 64-point gathers of neighbouring threads share cache lines. Only the visiting
+// order changes; every tracer's arithmetic is the same. The key is the tile of the cell that
+// cell_fraction gives the position.
+GBGHT_HD int traversal_tiles(int N) { return (N + 7) / 8; }
+GBGHT_HD uint32_t traversal_key(const double* GBGHT_RESTRICT X, int64_t p, int64_t M, int N, double dx) {
+  int i[3];
+  for (int c = 0; c < 3; ++c) {
+    double t;
+    cell_fraction(X[c * M + p], dx, N, i[c], t);
+  }
+  const uint32_t T = uint32_t(traversal_tiles(N));
+  return (uint32_t(i[2] >> 3) * T + uint32_t(i[1] >> 3)) * T + uint32_t(i[0] >> 3);
+}
+
 struct HeunWeights {
   double b0;      // predictor weight on f₀
   double beta0;   // corrector weight on f*

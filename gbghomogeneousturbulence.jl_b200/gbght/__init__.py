@@ -94,7 +94,7 @@ _SIGNATURES = {
 }
 
 KERNELS = ("y_inverse", "x_products", "y_forward", "z_epilogue", "x_velocity", "force_amp", "reality",
-           "tracers", "observables")
+           "tracers", "observables", "traversal")
 
 _loaded: dict = {}
 

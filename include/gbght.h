@@ -188,7 +188,8 @@ enum gbght_kernel {
   GBGHT_KERNEL_FORCE_AMP = 5,   /* ConstantPower amplitude */
   GBGHT_KERNEL_REALITY = 6,     /* end-of-step reality projection */
   GBGHT_KERNEL_TRACERS = 7,     /* tracer gather / Heun push */
-  GBGHT_KERNEL_OBSERVABLES = 8  /* k, ε, ⟨φ²⟩, ε_φ reduction */
+  GBGHT_KERNEL_OBSERVABLES = 8, /* k, ε, ⟨φ²⟩, ε_φ reduction */
+  GBGHT_KERNEL_TRAVERSAL = 9    /* tracer traversal order: tile keys, scan, scatter */
 };
 int gbght_profile(gbght_run* run, int enable);
 int gbght_profile_read(gbght_run* run, int kind, int64_t* launches, double* total_ms);
