@@ -549,7 +549,10 @@ class EngineImpl final : public Engine {
     return size_t(N) * XShape<T>::ACT_INV * sizeof(Cplx<T>) +
            size_t(7) * XShape<T>::P * x_kxs(g_.K, int(sizeof(Cplx<T>))) * sizeof(Cplx<T>) + kBarBytes;
   }
-  size_t smem_xv() const { return size_t(N) * XShape<T>::ACT_V * sizeof(Cplx<T>) + size_t(NTXV) * sizeof(double); }
+  size_t smem_xv() const {
+    return size_t(N) * XShape<T>::ACT_V * sizeof(Cplx<T>) + size_t((NTXV + 1) & ~1) * sizeof(double) +
+           size_t(3) * XShape<T>::PV * x_kxs(g_.K, int(sizeof(Cplx<T>))) * sizeof(Cplx<T>) + kBarBytes;
+  }
   // z init: the FFT tile, NT doubles, the TMEM address
   size_t smem_z() const {
     return size_t(N) * TLZ * sizeof(Cplx<T>) + size_t(NTZ) * sizeof(double) + 16;
@@ -673,19 +676,23 @@ class EngineImpl final : public Engine {
   }
   void x_velocity() {
     using X = XShape<T>;
+    const int KXS = x_kxs(g_.K, int(sizeof(Cplx<T>)));
+    const int ntiles = (N / X::PV) * N;
+    const int grid = (ntiles + XT - 1) / XT;   // XT tiles per CTA
 #ifdef GBGHT_EMU
     unsigned long long* mb = maxbits_;
-    emu_grid(N / X::PV, N, 1, smem_xv(), [&](const Cta& c, void* sm) {
+    emu_grid(grid, 1, 1, smem_xv(), [&](const Cta& c, void* sm) {
       Cplx<T>* t = static_cast<Cplx<T>*>(sm);
       double* red = reinterpret_cast<double*>(t + N * X::ACT_V);
-      const double m = body_x_velocity<T, N, 1>(c, t, red, g_, B_, U_, tw_);
+      Cplx<T>* stg = reinterpret_cast<Cplx<T>*>(red + 2);   // NT = 1 double, padded to 16 bytes
+      const double m = body_x_velocity<T, N, 1>(c, t, red, stg, KXS, nullptr, grid, g_, B_, U_, tw_, status_);
       unsigned long long bits;
       std::memcpy(&bits, &m, sizeof bits);
       if (bits > *mb) *mb = bits;
     });
 #else
     pbegin(PROF_X_VELOCITY);
-    k_x_velocity<T, N, NTXV><<<dim3(N / X::PV, N, 1), NTXV, smem_xv(), stream_>>>(g_, B_, U_, maxbits_, tw_);
+    k_x_velocity<T, N, NTXV><<<grid, NTXV, smem_xv(), stream_>>>(g_, B_, U_, maxbits_, KXS, tw_, status_);
     pend();
 #endif
   }

@@ -201,9 +201,12 @@ int run_n(const Layout& o, unsigned char* base, const double* u_hat, double* u, 
   gbght::k_z_init<double, N, TLZ, NTZ><<<dim3(g.KXP / TLZ, g.NY2, 1), NTZ, smem_z, st>>>(g, A, S, 0, partial, tw, 0);
   const size_t smem_y = size_t(N) * TLY * sizeof(Cplx<double>) + 32;
   gbght::k_y_inverse<double, N, TLY, NTY><<<dim3(g.KXP / TLY, N, 3), NTY, smem_y, st>>>(maps, g, 0, tw, flag);
-  const size_t smem_xv = size_t(N) * gbght::XShape<double>::ACT_V * sizeof(Cplx<double>) + size_t(NTX) * sizeof(double);
-  gbght::k_x_velocity<double, N, NTX><<<dim3(N / gbght::XShape<double>::PV, N, 1), NTX, smem_xv, st>>>(g, B, u, maxbits,
-                                                                                                      tw);
+  const int KXS = gbght::x_kxs(g.K, int(sizeof(Cplx<double>)));
+  const size_t smem_xv = size_t(N) * gbght::XShape<double>::ACT_V * sizeof(Cplx<double>) + size_t(NTX) * sizeof(double) +
+                         size_t(3) * gbght::XShape<double>::PV * KXS * sizeof(Cplx<double>) + 32;
+  const int ntiles_x = (N / gbght::XShape<double>::PV) * N;
+  gbght::k_x_velocity<double, N, NTX><<<unsigned((ntiles_x + gbght::XT - 1) / gbght::XT), NTX, smem_xv, st>>>(
+      g, B, u, maxbits, KXS, tw, flag);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "kernel launch");
   return GBGHT_OK;
 }

@@ -87,13 +87,17 @@ __global__ void __launch_bounds__(NT, 2) k_x_products(Geometry g, Cplx<T>* B, in
   body_x_products<T, N, NT>(c, sm, stg, KXS, bar, int(gridDim.x), g, B, has_scalar, tw, status);
 }
 
+// Shared memory: the ACT_V lines, NT doubles, the staging rows (3·PV·KXS), one barrier (32 bytes).
 template <class T, int N, int NT>
-__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_x_velocity(Geometry g, const Cplx<T>* B, T* u, unsigned long long* maxbits,
-                                                      const Cplx<T>* tw) {
+__global__ void __launch_bounds__(NT, 2) k_x_velocity(Geometry g, const Cplx<T>* B, T* u, unsigned long long* maxbits,
+                                                      int KXS, const Cplx<T>* tw, unsigned int* status) {
   CTA_CTX;
   Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
   double* red = reinterpret_cast<double*>(sm + N * XShape<T>::ACT_V);
-  const double mx = body_x_velocity<T, N, NT>(c, sm, red, g, B, u, tw);
+  Cplx<T>* stg = reinterpret_cast<Cplx<T>*>(red + NT);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(stg + 3 * XShape<T>::PV * KXS);
+  init_bars(bar, 1);
+  const double mx = body_x_velocity<T, N, NT>(c, sm, red, stg, KXS, bar, int(gridDim.x), g, B, u, tw, status);
   if (c.tid == 0) atomicMax(maxbits, static_cast<unsigned long long>(__double_as_longlong(mx)));
 }
 

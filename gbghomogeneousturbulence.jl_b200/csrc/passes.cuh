@@ -385,55 +385,54 @@ GBGHT_HD void body_x_products(const Cta& c, Cplx<T>* sm, Cplx<T>* stg, int KXS, 
   x_tile_chain<T, N, NT, 0>(c, sm, stage, src, g, B, nout, grid, ntiles, tw);
 }
 
-// Source of the deposit's inverse: line p (p < PV) = u_x + i·u_y of point p; line PV + h =
-// u_z(2h) + i·u_z(2h+1).
+// Source of the deposit's inverse from the staging rows [c][p][KXS] (c = 0..2) in shared memory:
+// line p (p < PV) = u_x + i·u_y of point p; line PV + h = u_z(2h) + i·u_z(2h+1). Packed two-for-one
+// as in XStagedSource (a c2r input: only the real part of the kx = 0 bin, rows K < e < N−K zero),
+// scaled by 1/N³.
 template <class T, int N, int PV>
-struct XVelocitySource {
+struct XVelocityStagedSource {
   static constexpr bool kExternal = true;
   const Geometry& g;
-  const Cplx<T>* B;
-  int z, y0;
+  const Cplx<T>* stg;
+  int KXS;
   T sc;
   GBGHT_HD Cplx<T> load(int e, int l) const {
     const int K = g.K;
     if (e > K && e < N - K) return czero<T>();
-    int ca, cb, ya, yb;
+    int ra, rb;   // staging rows of the pair
     if (l < PV) {
-      ca = 0;
-      cb = 1;
-      ya = yb = y0 + l;
+      ra = l;
+      rb = PV + l;
     } else {
-      ca = cb = 2;
-      ya = y0 + 2 * (l - PV);
-      yb = ya + 1;
+      ra = 2 * PV + 2 * (l - PV);
+      rb = ra + 1;
     }
-    if (e == 0) {
-      const Cplx<T> a = B[idxB(g, ca, z, ya, 0)], b = B[idxB(g, cb, z, yb, 0)];
-      return cmk<T>(a.x * sc, b.x * sc);
-    }
-    if (e <= K) {
-      const Cplx<T> a = B[idxB(g, ca, z, ya, e)], b = B[idxB(g, cb, z, yb, e)];
-      return cmk<T>((a.x - b.y) * sc, (a.y + b.x) * sc);
-    }
-    const Cplx<T> a = B[idxB(g, ca, z, ya, N - e)], b = B[idxB(g, cb, z, yb, N - e)];
+    const int m = e <= K ? e : N - e;
+    const Cplx<T> a = stg[ra * KXS + m], b = stg[rb * KXS + m];
+    if (e == 0) return cmk<T>(a.x * sc, b.x * sc);
+    if (e <= K) return cmk<T>((a.x - b.y) * sc, (a.y + b.x) * sc);
     return cmk<T>((a.x + b.y) * sc, (b.x - a.y) * sc);
   }
 };
 
-// The deposit's x-pass: physical velocity of PV points written out, max |u|² returned to thread 0.
-// One warp per line (ACT_V lines at sm + l·N).
-template <class T, int N, int NT>
-GBGHT_HD double body_x_velocity(const Cta& c, Cplx<T>* sm, double* red, const Geometry& g,
-                                const Cplx<T>* GBGHT_RESTRICT B, T* GBGHT_RESTRICT u_phys,
-                                const Cplx<T>* GBGHT_RESTRICT tw) {
+GBGHT_HD double max_nan(double a, double b) { return (b > a || b != b) ? b : a; }
+
+// One deposit tile (PV points z, y0..y0+PV−1): the inverse of the staged spectra (after its first
+// stage the staging is free and the next tile's copies are issued), then the physical velocity
+// written out; returns this thread's max |u|² (NaN wins).
+template <class T, int N, int NT, class TW>
+GBGHT_HD double x_velocity_tile(const Cta& c, Cplx<T>* sm, const XStaging<T, XShape<T>::PV>& stage,
+                                const XVelocityStagedSource<T, N, XShape<T>::PV>& src, T* GBGHT_RESTRICT u_phys,
+                                int z, int y0, int next_z, int next_y0, const TW& tw) {
   using X = XShape<T>;
   constexpr int PV = X::PV, NW = 6;
-  const int y0 = PV * c.bx, z = c.by;
-  const XVelocitySource<T, N, PV> src{g, B, z, y0, T(g.inv_norm)};
   const auto lines = [&](int l) { return sm + l * N; };
-  const auto from_b = [&](int l) { return LineOfSource<XVelocitySource<T, N, PV>>{src, l}; };
+  const auto from_stg = [&](int l) { return LineOfSource<XVelocityStagedSource<T, N, PV>>{src, l}; };
   const auto in_smem = [&](int l) { return LineBuf<T>{sm + l * N}; };
-  warp_fft_lines<T, N, NW, NT, +1>(c, X::ACT_V, lines, from_b, in_smem, tw);
+  warp_fft_lines<T, N, NW, NT, +1, 0, 1>(c, X::ACT_V, lines, from_stg, in_smem, tw);
+  GBGHT_SYNC();
+  if (next_z >= 0) stage.issue(c, next_z, next_y0);
+  warp_fft_lines<T, N, NW, NT, +1, 1>(c, X::ACT_V, lines, from_stg, in_smem, tw);
   GBGHT_SYNC();
   double m = 0.0;
   const size_t comp = size_t(N) * N * N;
@@ -448,13 +447,56 @@ GBGHT_HD double body_x_velocity(const Cta& c, Cplx<T>* sm, double* red, const Ge
     u_phys[comp + base] = uxy.y;
     u_phys[2 * comp + base] = uz;
     const double sp = (double(uxy.x) * double(uxy.x) + double(uxy.y) * double(uxy.y)) + double(uz) * double(uz);
-    m = (sp > m || sp != sp) ? sp : m;
+    m = max_nan(m, sp);
+  }
+  GBGHT_SYNC();   // the lines are rewritten by the next tile's inverse
+  return m;
+}
+
+// Tiles I, I+1, … < XT of this CTA (tile bx + i·grid), written out by template recursion as in
+// the x pass; tile I's spectra are already being copied into the staging rows.
+template <class T, int N, int NT, int I, class TW>
+GBGHT_HD double x_velocity_chain(const Cta& c, Cplx<T>* sm, const XStaging<T, XShape<T>::PV>& stage,
+                                 const XVelocityStagedSource<T, N, XShape<T>::PV>& src, T* u_phys, int grid,
+                                 int ntiles, const TW& tw) {
+  if constexpr (I < XT) {
+    constexpr int PV = XShape<T>::PV;
+    const int tiles_y = N / PV;
+    const int t = c.bx + I * grid, tn = t + grid;
+    const bool more = I + 1 < XT && tn < ntiles;
+    stage.wait(uint32_t(I & 1));
+    double m = x_velocity_tile<T, N, NT>(c, sm, stage, src, u_phys, t / tiles_y, PV * (t % tiles_y),
+                                         more ? tn / tiles_y : -1, more ? PV * (tn % tiles_y) : 0, tw);
+    if (more) m = max_nan(m, x_velocity_chain<T, N, NT, I + 1>(c, sm, stage, src, u_phys, grid, ntiles, tw));
+    return m;
+  } else {
+    return 0.0;
+  }
+}
+
+// The deposit's x pass over the tiles bx, bx + grid, …: physical velocity of PV points per tile
+// written out, max |u|² returned to thread 0. One warp per line (ACT_V lines at sm + l·N); the next
+// tile's spectra are prefetched into the staging rows (3·PV rows of KXS) while the current tile is
+// transformed. `red` holds NT doubles.
+template <class T, int N, int NT, class TW>
+GBGHT_HD double body_x_velocity(const Cta& c, Cplx<T>* sm, double* red, Cplx<T>* stg, int KXS, uint64_t* bar,
+                                int grid, const Geometry& g, const Cplx<T>* GBGHT_RESTRICT B,
+                                T* GBGHT_RESTRICT u_phys, const TW& tw, unsigned int* status) {
+  using X = XShape<T>;
+  constexpr int PV = X::PV;
+  const int tiles_y = N / PV, ntiles = tiles_y * N;
+  double m = 0.0;
+  if (c.bx < ntiles) {
+    const XStaging<T, PV> stage{g, B, stg, KXS, 3, bar, status};
+    const XVelocityStagedSource<T, N, PV> src{g, stg, KXS, T(g.inv_norm)};
+    stage.issue(c, c.bx / tiles_y, PV * (c.bx % tiles_y));
+    m = x_velocity_chain<T, N, NT, 0>(c, sm, stage, src, u_phys, grid, ntiles, tw);
   }
   red[c.tid] = m;
   GBGHT_SYNC();
   if (c.tid == 0) {
     double r = 0.0;
-    for (int i = 0; i < NT; ++i) r = (red[i] > r || red[i] != red[i]) ? red[i] : r;
+    for (int i = 0; i < NT; ++i) r = max_nan(r, red[i]);
     return r;
   }
   return 0.0;
