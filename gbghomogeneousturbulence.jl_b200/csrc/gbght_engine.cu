@@ -65,7 +65,7 @@ static const char* rt_check() { return cuda_err(cudaGetLastError(), "kernel laun
 // ------------------------------------------------------------------------------------------------
 template <class T> struct Shape {
   static constexpr int TLY = 128 / int(sizeof(Cplx<T>));   // y passes: 128-byte rows
-  static constexpr int TLZ = 64 / int(sizeof(Cplx<T>));    // z epilogue: 64-byte rows
+  static constexpr int TLZ = 4;                             // z epilogue: 4 columns (64-byte rows in FP64)
 };
 constexpr int clamp_nt(int v) { return v < 64 ? 64 : (v > 256 ? 256 : v); }
 
