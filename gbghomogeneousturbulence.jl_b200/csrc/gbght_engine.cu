@@ -112,7 +112,7 @@ class EngineImpl final : public Engine {
 #ifdef GBGHT_EMU
   static constexpr int NTXP = 1, NTXV = 1;
 #else
-  static constexpr int NTXP = 32 * 7, NTXV = 32 * 6;   // one warp per line
+  static constexpr int NTXP = 32 * XShape<T>::NW, NTXV = 32 * 6;   // one warp per line
 #endif
   // z epilogue: one thread per butterfly of the first and last radix-R stage (N/R·TLZ of them),
   // up to 512

@@ -152,6 +152,7 @@ template <class T> struct XShape {
   static constexpr int P = TL / 4;                 // points per tile (products pass)
   static constexpr int ACT_INV = 3 * P + P / 2;
   static constexpr int ACT_FWD = 3 * P;
+  static constexpr int NW = sizeof(Cplx<T>) == 16 ? 7 : 8;   // warps of the x pass (≥ 1 turnaround item per thread)
   static constexpr int PV = TL / 2;                // points per tile (deposit pass)
   static constexpr int ACT_V = PV + PV / 2;
 };
@@ -280,6 +281,74 @@ struct XStaging {
 #define GBGHT_NOINLINE
 #endif
 
+// The turnaround of an x tile. Every plan starts and ends with the same radix R, so butterfly j of
+// the inverse's last stage produces exactly the points x = j + r·N/R (r < R) that butterfly j of
+// the forward's first stage consumes. One thread per (j, point p) therefore runs, in registers:
+// - the last inverse stage of lines 3p, 3p+1, 3p+2 (u, ω) and of p's φ line;
+// - the products n = u×ω and f = uφ at those R points;
+// - the first forward stage of the three product lines.
+// Only the product lines' first-stage outputs (rows j·R + r) go back to shared memory. All reads
+// come before the barrier and all writes after it, since the outputs overwrite rows that other
+// threads read.
+template <class T, int N, int NT>
+GBGHT_HD void x_turnaround(const Cta& c, Cplx<T>* sm, const Cplx<T>* GBGHT_RESTRICT tw) {
+  constexpr int P = XShape<T>::P;
+  constexpr int S = Radices<N>::n - 1;
+  constexpr int R = Radices<N>::r[S];
+  static_assert(S > 0 && R == Radices<N>::r[0], "the turnaround needs two stages or more and equal end radices");
+  constexpr int NB = N / R;
+  constexpr int ITEMS = NB * P;
+  constexpr int SLOTS = (ITEMS + NT - 1) / NT;
+  Cplx<T> out[SLOTS][3][R];
+  const auto inv_last = [&](int line, int j, Cplx<T>* v) {
+    const Cplx<T>* L = sm + line * N;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = L[lidx<T>(j + r * NB)];
+    Cplx<T> w[R];
+    twiddles<T, R, +1>(tw, j, w);
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = v[r] * w[r];
+    dft<T, R, +1>(v);
+  };
+#pragma unroll
+  for (int s = 0; s < SLOTS; ++s) {
+    const int it = c.tid + s * NT;
+    if (SLOTS * NT == ITEMS || it < ITEMS) {
+      const int j = it % NB, p = it / NB;
+      Cplx<T> ph[R], a[R], b[R], d[R];
+      inv_last(3 * P + p / 2, j, ph);   // φ(2h) + i·φ(2h+1)
+      inv_last(3 * p, j, a);            // u_x + i·u_y
+      inv_last(3 * p + 1, j, b);        // u_z + i·ω_x
+      inv_last(3 * p + 2, j, d);        // ω_y + i·ω_z
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const T ux = a[r].x, uy = a[r].y, uz = b[r].x, wx = b[r].y, wy = d[r].x, wz = d[r].y;
+        const T phi = (p & 1) ? ph[r].y : ph[r].x;
+        out[s][0][r] = cmk<T>(uy * wz - uz * wy, uz * wx - ux * wz);
+        out[s][1][r] = cmk<T>(ux * wy - uy * wx, ux * phi);
+        out[s][2][r] = cmk<T>(uy * phi, uz * phi);
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) dft<T, R, -1>(out[s][k]);
+    }
+  }
+  GBGHT_SYNC();
+#pragma unroll
+  for (int s = 0; s < SLOTS; ++s) {
+    const int it = c.tid + s * NT;
+    if (SLOTS * NT == ITEMS || it < ITEMS) {
+      const int j = it % NB, p = it / NB;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        Cplx<T>* L = sm + (3 * p + k) * N;
+#pragma unroll
+        for (int r = 0; r < R; ++r) L[lidx<T>(j * R + r)] = out[s][k][r];
+      }
+    }
+  }
+  GBGHT_SYNC();
+}
+
 // One x tile: the inverse of the staged spectra (the first stage reads the staging; after it the
 // staging is free and the next tile's copies are issued), the products, the forward transform and
 // the unpack into B. Kept out of line: inlined into the persistent loop below, its lane-dependent
@@ -290,7 +359,7 @@ GBGHT_HD void x_tile(const Cta& c, Cplx<T>* sm, const XStaging<T, XShape<T>::P>&
                                     Cplx<T>* GBGHT_RESTRICT B, int nout, int z, int y0, int next_z, int next_y0,
                                     const Cplx<T>* GBGHT_RESTRICT tw) {
   using X = XShape<T>;
-  constexpr int P = X::P, NW = 7;
+  constexpr int P = X::P, NW = X::NW;
   const int KX1 = g.K + 1;
   const auto lines = [&](int l) { return sm + l * N; };
   const auto from_stg = [&](int l) { return LineOfSource<XStagedSource<T, N, P>>{src, l}; };
@@ -298,6 +367,14 @@ GBGHT_HD void x_tile(const Cta& c, Cplx<T>* sm, const XStaging<T, XShape<T>::P>&
   warp_fft_lines<T, N, NW, NT, +1, 0, 1>(c, X::ACT_INV, lines, from_stg, in_smem, tw);
   GBGHT_SYNC();
   if (next_z >= 0) stage.issue(c, next_z, next_y0);
+  if constexpr (Radices<N>::n >= 2) {
+    // inverse stages up to the last, then the turnaround (last inverse stage, products, first
+    // forward stage), then the forward's remaining stages
+    warp_fft_lines<T, N, NW, NT, +1, 1, Radices<N>::n - 1>(c, X::ACT_INV, lines, from_stg, in_smem, tw);
+    GBGHT_SYNC();
+    x_turnaround<T, N, NT>(c, sm, tw);
+    warp_fft_lines<T, N, NW, NT, -1, 1>(c, X::ACT_FWD, lines, in_smem, in_smem, tw);
+  } else {
   warp_fft_lines<T, N, NW, NT, +1, 1>(c, X::ACT_INV, lines, from_stg, in_smem, tw);
   GBGHT_SYNC();
   for (int x = c.tid; x < N; x += NT) {
@@ -320,6 +397,7 @@ GBGHT_HD void x_tile(const Cta& c, Cplx<T>* sm, const XStaging<T, XShape<T>::P>&
   }
   GBGHT_SYNC();
   warp_fft_lines<T, N, NW, NT, -1>(c, X::ACT_FWD, lines, in_smem, in_smem, tw);
+  }
   // unpack each line (by its owning warp) into B: line 3p+pr → comps (2pr, 2pr+1) of point p;
   // columns past K get zeros
   for (int t = c.tid; t < 32 * NW; t += NT) {
