@@ -280,6 +280,13 @@ struct XStaging {
 #else
 #define GBGHT_NOINLINE
 #endif
+// A host-device function kept out of line on the device: one copy of a body that a kernel calls
+// several times, to keep the kernel's code within the instruction cache.
+#ifdef __CUDACC__
+#define GBGHT_HD_OUTLINE __host__ __device__ __noinline__
+#else
+#define GBGHT_HD_OUTLINE inline
+#endif
 
 // The turnaround of an x tile. Every plan starts and ends with the same radix R, so butterfly j of
 // the inverse's last stage produces exactly the points x = j + r·N/R (r < R) that butterfly j of
@@ -584,17 +591,10 @@ GBGHT_HD double body_x_velocity(const Cta& c, Cplx<T>* sm, double* red, Cplx<T>*
 // z-forward + epilogue + z-inverse helpers
 // ================================================================================================
 
-// Register-direct I/O of one z tile (the TL kx columns kx0.. of row ky' = qy, all z).
-// Forward: the first stage reads A slot `slot` rows z straight from global memory; the last stage
-// keeps only the retained rows, in the registers of the thread that computes them (ZOwn below).
-template <class T, int N, int TL>
-struct ZGlobalSource {
-  static constexpr bool kExternal = true;
-  const Geometry& g;
-  const Cplx<T>* A;
-  int slot, qy, kx0;
-  GBGHT_HD Cplx<T> load(int e, int l) const { return A[idxA(g, slot, e, qy, kx0 + l)]; }
-};
+// I/O of one z tile (the TL kx columns kx0.. of row ky' = qy, all z). The forward transforms'
+// first stage reads a staged copy (below), and their last stage keeps only the retained rows, in
+// the thread that computes them (ZOwn below).
+//
 // Staged z tiles: A slot `slot` of the tile (N rows of TL elements, the layout of the tile FFT's
 // buffer) copied by the TMA engine (map az) into buffer `bf` (0 or 1) of the staging region, so
 // the copy of the next transform's input runs while the current one computes. The copy completes
@@ -870,19 +870,10 @@ struct ZGlobalSink {
   GBGHT_HD void store(int e, int l, Cplx<T> v) const { A[idxA(g, slot, e, qy, kx0 + l)] = v; }
 };
 
-// Forward z-transform of A slot `slot` of the tile into component `comp` of the owned rows.
-template <class T, int N, int TL, int NT, class O, class Rows, class TW>
-GBGHT_HD void z_forward_own(const Cta& c, Cplx<T>* W, const Geometry& g, const Cplx<T>* A, int slot, int qy, int kx0,
-                            Rows& rows, int comp, const TW& tw) {
-  const ZGlobalSource<T, N, TL> src{g, A, slot, qy, kx0};
-  const ZOwnSink<T, O, Rows> dst{rows, comp};
-  tile_fft_io<T, N, TL, NT, -1>(c, W, tw, src, dst);
-  rows.put_done();
-}
-
 // Forward z-transform of the tile staged in buffer bf (barrier parity `parity`) into component
 // `comp` of the owned rows. `after()` runs once the first stage has read the buffer (after the
-// barrier that ends the stage), for the caller to start the next copy into it.
+// barrier that ends the stage), for the caller to start the next copy into it. Kept inline: out
+// of line, the staging objects and the row store go through local memory and the kernel slows.
 template <class T, int N, int TL, int NT, class O, class Rows, class After, class TW>
 GBGHT_HD void z_forward_staged(const Cta& c, Cplx<T>* W, const ZStaging<T, N, TL>& stg, int bf, int parity, Rows& rows,
                                int comp, const After& after, const TW& tw) {
@@ -901,11 +892,18 @@ GBGHT_HD void z_forward_staged(const Cta& c, Cplx<T>* W, const ZStaging<T, N, TL
   rows.put_done();
 }
 
-// Inverse z-transform of the owned values x (retained rows) into A slot `slot` of the tile.
+// The owned values of one component, passed by value (in registers) to the out-of-line inverse.
+template <class T, class O>
+struct OwnVals {
+  Cplx<T> v[O::BPT][O::NSLOT];
+};
+
+// Inverse z-transform of the owned values x (retained rows) into A slot `slot` of the tile. One
+// out-of-line copy serves the epilogue's seven inverse transforms.
 template <class T, int N, int TL, int NT, class O, class TW>
-GBGHT_HD void z_inverse_own(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* A, int slot, int qy, int kx0,
-                            const Cplx<T> (&x)[O::BPT][O::NSLOT], const TW& tw) {
-  const ZOwnSource<T, N, O> src{g, x};
+GBGHT_HD_OUTLINE void z_inverse_own(const Cta c, Cplx<T>* W, const Geometry g, Cplx<T>* A, int slot, int qy, int kx0,
+                                    const OwnVals<T, O> x, const TW tw) {
+  const ZOwnSource<T, N, O> src{g, x.v};
   const ZGlobalSink<T, N, TL> dst{g, A, slot, qy, kx0};
   tile_fft_io<T, N, TL, NT, +1>(c, W, tw, src, dst);
 }
@@ -935,21 +933,21 @@ template <class T, int N, int TL, int NT, class O, class Rows, class TW>
 GBGHT_HD void z_inverse_velocity(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* A, int qy, int kx0, double ky,
                                  const Rows& rows, int vorticity, const TW& tw) {
   for (int o = 0; o < 3; ++o) {
-    Cplx<T> x[O::BPT][O::NSLOT];
+    OwnVals<T, O> x;
 #pragma unroll
     for (int b = 0; b < O::BPT; ++b)
 #pragma unroll
-      for (int sl = 0; sl < O::NSLOT; ++sl) x[b][sl] = rows.get(o, b, sl);
+      for (int sl = 0; sl < O::NSLOT; ++sl) x.v[b][sl] = rows.get(o, b, sl);
     z_inverse_own<T, N, TL, NT, O>(c, W, g, A, o, qy, kx0, x, tw);
   }
   if (!vorticity) return;
   const T kY = T(ky);
   for (int o = 0; o < 3; ++o) {
-    Cplx<T> x[O::BPT][O::NSLOT];
+    OwnVals<T, O> x;
     for_own_slots<T, N, TL, NT>(c, g, [&](int b, int sl, bool, int, int mz, int l) {
       Cplx<T> u0, u1, u2;
       rows.get3(b, sl, u0, u1, u2);
-      x[b][sl] = curl_of<T>(o, u0, u1, u2, T(g.s * double(kx0 + l)), kY, T(g.s * double(mz)));
+      x.v[b][sl] = curl_of<T>(o, u0, u1, u2, T(g.s * double(kx0 + l)), kY, T(g.s * double(mz)));
     });
     z_inverse_own<T, N, TL, NT, O>(c, W, g, A, 3 + o, qy, kx0, x, tw);
   }
@@ -1019,7 +1017,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
       codes[n++] = 2;
     }
     forward3(3, codes, n);
-    Cplx<T> x[O::BPT][O::NSLOT];
+    OwnVals<T, O> x;
     const auto half = [&](auto hc) {
       constexpr int h = decltype(hc)::value;
       sst.wait(h);
@@ -1053,7 +1051,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
           S[si] = phi;
           if (!st.last) H[si] = scale(hh, E);
         }
-        x[b][sl] = phi;
+        x.v[b][sl] = phi;
       });
     };
     half(H0{});
