@@ -53,6 +53,24 @@ def _dist():
     return ws, rank, local
 
 
+def max_over_ranks(x, device="cpu"):
+    """The largest of x over the ranks of the process group (x itself without one). Every rank
+    calls it, in the same order, so the collective steps match across ranks."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world_size, steps, slowest_s):
+    """Whole-job steps/s of independent replicas: every rank runs `steps` steps of its own field,
+    and the job takes as long as its slowest rank."""
+    return world_size * steps / slowest_s
+
+
 def _peaks():
     try:
         with open(PEAKS_FILE) as f:
@@ -291,12 +309,7 @@ def ours(args):
             if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else None
         with ClockSampler(device, clock_path) as cs:
             ms, prof = timed_steps(run, args.steps)
-        el = ms / 1e3
-        if ws > 1:
-            import torch.distributed as dist
-            t = torch.tensor([el], dtype=torch.float64, device=f"cuda:{device}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el = max_over_ranks(ms / 1e3, f"cuda:{device}")
         spectra = (run.energy_spectrum(), run.scalar_spectrum())
         results[form] = dict(el=el, prof=prof, clocks=cs.summary(), K=run.K, spectra=spectra)
         run.close()
@@ -304,13 +317,10 @@ def ours(args):
     # end-to-end through the public API (host buffers), the headline form
     e2e_val, h2d, d2h = (float("nan"), 0, 0) if args.no_e2e else e2e_run(args, forms[0], device, inputs, args.steps)
     if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor([1.0 / e2e_val], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_val = 1.0 / float(t.item())
+        e2e_val = 1.0 / max_over_ranks(1.0 / e2e_val, f"cuda:{device}")
     if rank == 0:
         head = results[forms[0]]
-        value = ws * args.steps / head["el"]
+        value = replica_rate(ws, args.steps, head["el"])
         w_complex = 16 if forms[0] == "fp64" else 8
         ab = algorithmic_bytes_per_step(N, head["K"], w_complex)
         prof = head["prof"]
@@ -339,7 +349,7 @@ def ours(args):
         }
         if "fp32_mixed" in results and "fp64" in results:
             m = results["fp32_mixed"]
-            mv = ws * args.steps / m["el"]
+            mv = replica_rate(ws, args.steps, m["el"])
             E64, P64 = results["fp64"]["spectra"]
             E32, P32 = m["spectra"]
             live = E64 > 1e-6 * E64.max()
