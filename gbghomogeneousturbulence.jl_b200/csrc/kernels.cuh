@@ -222,25 +222,41 @@ static __global__ void k_trav_count(int64_t M, const double* X, int N, double dx
   atomicAdd(count + k, 1u);
 }
 constexpr int kScanThreads = 1024;
+// Exclusive scan of the tile counts in one block: warp w scans the contiguous segment
+// [w·seg, (w+1)·seg) in coalesced chunks of 32 with shuffles, after a first pass that sums the
+// segments and scans those sums.
 static __global__ void __launch_bounds__(kScanThreads) k_trav_scan(uint32_t* count, int nbins) {
-  __shared__ uint32_t part[kScanThreads];
-  const int per = (nbins + kScanThreads - 1) / kScanThreads;
-  const int b0 = int(threadIdx.x) * per, b1 = min(nbins, b0 + per);
+  __shared__ uint32_t wsum[kScanThreads / 32];
+  const int lane = int(threadIdx.x) & 31, w = int(threadIdx.x) >> 5;
+  constexpr int NWARP = kScanThreads / 32;
+  const int seg = ((nbins + NWARP - 1) / NWARP + 31) / 32 * 32;
+  const int b0 = w * seg, b1 = min(nbins, b0 + seg);
   uint32_t s = 0;
-  for (int b = b0; b < b1; ++b) s += count[b];
-  part[threadIdx.x] = s;
+  for (int b = b0 + lane; b < b1; b += 32) s += count[b];
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if (lane == 0) wsum[w] = s;
   __syncthreads();
-  for (int off = 1; off < kScanThreads; off <<= 1) {   // inclusive scan of the partial sums
-    const uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
+  if (w == 0) {   // exclusive scan of the segment sums
+    const uint32_t v = wsum[lane];
+    uint32_t inc = v;
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, inc, off);
+      if (lane >= off) inc += t;
+    }
+    wsum[lane] = inc - v;
   }
-  uint32_t run = threadIdx.x == 0 ? 0u : part[threadIdx.x - 1];
-  for (int b = b0; b < b1; ++b) {
-    const uint32_t c = count[b];
-    count[b] = run;
-    run += c;
+  __syncthreads();
+  uint32_t carry = wsum[w];
+  for (int base = b0; base < b1; base += 32) {
+    const int b = base + lane;
+    const uint32_t v = b < b1 ? count[b] : 0u;
+    uint32_t inc = v;
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, inc, off);
+      if (lane >= off) inc += t;
+    }
+    if (b < b1) count[b] = carry + inc - v;
+    carry += __shfl_sync(0xffffffffu, inc, 31);
   }
 }
 static __global__ void k_trav_scatter(int64_t M, const uint32_t* key, uint32_t* offset, uint32_t* order) {
