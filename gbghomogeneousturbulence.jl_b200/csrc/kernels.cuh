@@ -166,23 +166,42 @@ template <class T>
 __global__ void k_reality(Geometry g, Cplx<T>* S, int ncomp) {
   reality_mode<T>(int(blockIdx.x * blockDim.x + threadIdx.x), g, S, ncomp);
 }
-// ConstantPower amplitude: band sum by thread 0; whole-field sum of the tile partials in a fixed
-// order (strided per thread, then a fixed tree).
+// ConstantPower amplitude: the band sum and the whole-field sum of the tile partials, each in a
+// fixed order (strided per thread, then a fixed tree), so the amplitude is the same on every run.
 template <class T>
 __global__ void k_force_amp(Geometry g, const Cplx<T>* S, const double* partial, int npartial, double lo2,
                             double hi2, double eps_rate, double eps_T, double* amp, unsigned int* status) {
-  __shared__ double red[256];
+  __shared__ double red[256], bred[256];
   double s = 0.0;
   for (int i = threadIdx.x; i < npartial; i += 256) s += partial[i];
   red[threadIdx.x] = s;
+  // the band sum over the box |m_a| ≤ mb, split over the threads in a fixed assignment
+  int mb = int(sqrt(hi2) / g.s) + 1;
+  if (mb > g.K) mb = g.K;
+  const int side = 2 * mb + 1, nbox = 3 * side * side * (mb + 1);
+  double b = 0.0;
+  for (int i = threadIdx.x; i < nbox; i += 256) {
+    const int kx = i % (mb + 1), mz = (i / (mb + 1)) % side - mb, my = (i / ((mb + 1) * side)) % side - mb;
+    const int cc = i / ((mb + 1) * side * side);
+    const double kxd = g.s * kx, kyd = g.s * my, kzd = g.s * mz;
+    const double k2 = (kxd * kxd + kyd * kyd) + kzd * kzd;
+    if (!(k2 >= lo2 && k2 <= hi2)) continue;
+    const int qy = my >= 0 ? my : my + g.NY2, qz = mz >= 0 ? mz : mz + g.NY2;
+    const Cplx<T> v = S[idxS(g, cc, qy, qz, kx)];
+    b += (kx == 0 ? 1.0 : 2.0) * (double(v.x) * v.x + double(v.y) * v.y);
+  }
+  bred[threadIdx.x] = b;
   __syncthreads();
-  for (int w = 128; w > 0; w >>= 1) {
-    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+  for (int w = 128; w > 0; w >>= 1) {   // fixed-order trees
+    if (threadIdx.x < w) {
+      red[threadIdx.x] += red[threadIdx.x + w];
+      bred[threadIdx.x] += bred[threadIdx.x + w];
+    }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
     const double whole = red[0];
-    const double band = band_energy_raw<T>(g, S, lo2, hi2);
+    const double band = bred[0];
     const double n6 = double(g.N) * g.N * g.N * double(g.N) * g.N * g.N;
     const double band_obs = 0.5 * (band / n6), whole_obs = 0.5 * (whole / n6);
     double A = 0.0;
