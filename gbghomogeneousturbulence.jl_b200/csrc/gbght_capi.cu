@@ -447,9 +447,9 @@ int gbght_advance(gbght_run* r, double dt, double* dt_taken) {
     return fail(r, GBGHT_ERR_SCHEDULE, "non-finite velocity at step " + std::to_string(r->step + 1) +
                                            ": the run appears to have blown up");
   if (r->cfg.scalar) {
-    gbght::Observables o{};
-    if ((rc = engine_call(r, r->eng->observables(&o)))) return rc;
-    if (!std::isfinite(o.var))
+    double var = 0.0;
+    if ((rc = engine_call(r, r->eng->scalar_variance(&var)))) return rc;
+    if (!std::isfinite(var))
       return fail(r, GBGHT_ERR_SCHEDULE, "non-finite scalar at step " + std::to_string(r->step + 1) +
                                              ": the run appears to have blown up");
   }

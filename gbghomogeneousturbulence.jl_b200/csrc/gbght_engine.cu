@@ -323,23 +323,35 @@ class EngineImpl final : public Engine {
     return rt_sync(stream_);
   }
 
-  const char* observables(Observables* o) override {
+  // the four raw sums of body_observables over all ky' rows (mode 2: the scalar sums only)
+  const char* observable_sums(int mode, double s[4]) {
 #ifdef GBGHT_EMU
     emu_grid(g_.NY2, 1, 1, 4 * sizeof(double), [&](const Cta& c, void* sm) {
-      body_observables<T, 1>(c, static_cast<double*>(sm), g_, S_, p_.scalar, obs_);
+      body_observables<T, 1>(c, static_cast<double*>(sm), g_, S_, mode, obs_);
     });
 #else
     pbegin(PROF_OBSERVABLES);
-    k_observables<T, NTR><<<g_.NY2, NTR, 4 * NTR * sizeof(double), stream_>>>(g_, S_, p_.scalar, obs_);
+    k_observables<T, NTR><<<g_.NY2, NTR, 4 * NTR * sizeof(double), stream_>>>(g_, S_, mode, obs_);
     pend();
 #endif
     const char* err = rt_check();
     if (err) return err;
     std::vector<double> host(size_t(g_.NY2) * 4);
     if ((err = rt_d2h(host.data(), obs_, host.size() * sizeof(double), stream_))) return err;
-    double s[4] = {0, 0, 0, 0};
+    for (int j = 0; j < 4; ++j) s[j] = 0.0;
     for (int qy = 0; qy < g_.NY2; ++qy)
       for (int j = 0; j < 4; ++j) s[j] += host[qy * 4 + j];
+    return nullptr;
+  }
+  const char* scalar_variance(double* var) override {
+    double s[4];
+    if (const char* err = observable_sums(p_.scalar ? 2 : 0, s)) return err;
+    *var = s[2] / (double(N) * N * N * double(N) * N * N);
+    return nullptr;
+  }
+  const char* observables(Observables* o) override {
+    double s[4];
+    if (const char* err = observable_sums(p_.scalar, s)) return err;
     const double n6 = double(N) * N * N * double(N) * N * N;
     const double kappa = p_.viscosity / p_.schmidt;
     o->k = 0.5 * (s[0] / n6);

@@ -56,6 +56,8 @@ class Engine {
   virtual const char* velocity_export(double* u) = 0;
   virtual const char* velocity_import(const double* u) = 0;
   virtual const char* observables(Observables* o) = 0;
+  // the scalar variance alone (the blow-up guard of advance!), reading φ̂ only
+  virtual const char* scalar_variance(double* var) = 0;
   virtual const char* spectrum(int which, double* out, int nshell) = 0;
   virtual const char* tracers_set(const double* X) = 0;
   virtual const char* tracers_get(double* X) = 0;

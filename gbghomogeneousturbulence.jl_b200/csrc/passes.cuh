@@ -1305,6 +1305,7 @@ GBGHT_HD void export_mode(size_t i, const Geometry& g, const Cplx<T>* Sc, Cplx<d
 // ================================================================================================
 // Observables: per ky' row, the Hermitian-weighted sums Σ|û|², Σκ²|û|², Σ|φ̂|², Σκ²|φ̂|²
 // (unnormalised), summed per thread and then in thread order. Grid: (NY2). `red` holds 4·NT.
+// has_scalar = 2 takes the scalar sums only (the velocity sums are left at zero).
 // ================================================================================================
 template <class T, int NT>
 GBGHT_HD void body_observables(const Cta& c, double* red, const Geometry& g, const Cplx<T>* GBGHT_RESTRICT S,
@@ -1318,13 +1319,15 @@ GBGHT_HD void body_observables(const Cta& c, double* red, const Geometry& g, con
     const double kxd = g.s * kx, kzd = g.s * q_to_m(qz, g.K, NY2);
     const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
     const double w = kx == 0 ? 1.0 : 2.0;
-    double e = 0.0;
-    for (int cc = 0; cc < 3; ++cc) {
-      const Cplx<T> v = S[idxS(g, cc, qy, qz, kx)];
-      e += double(v.x) * v.x + double(v.y) * v.y;
+    if (has_scalar != 2) {
+      double e = 0.0;
+      for (int cc = 0; cc < 3; ++cc) {
+        const Cplx<T> v = S[idxS(g, cc, qy, qz, kx)];
+        e += double(v.x) * v.x + double(v.y) * v.y;
+      }
+      acc[0] += w * e;
+      acc[1] += w * k2 * e;
     }
-    acc[0] += w * e;
-    acc[1] += w * k2 * e;
     if (has_scalar) {
       const Cplx<T> v = S[idxS(g, 3, qy, qz, kx)];
       const double p = double(v.x) * v.x + double(v.y) * v.y;

@@ -139,6 +139,17 @@ def test_nonfinite_state_trips_the_guard(cuda_library):
         run.advance(0.01)
 
 
+def test_nonfinite_scalar_is_a_blow_up(cuda_library):
+    # A non-finite scalar is a blow-up. The x pass packs n_z and uφ into one complex line, so
+    # within the step it also reaches the velocity, and the velocity guard (checked first) names it.
+    N = 32
+    ph = S.seed_scalar(N, 0.5, seed=1)
+    ph[1, 1, 1] = complex(np.inf, 0.0)
+    run, _ = make_case(N, ph=ph, library=cuda_library)
+    with pytest.raises(gbght.ScheduleError, match="blown up"):
+        run.advance(0.01)
+
+
 def test_fp32_mixed_short_time_error(cuda_library):
     # FP32 transforms, products and updates; FP64 integrating factor, forcing normalisation,
     # spectra and tracer positions. Short-time field error and spectra against the FP64 oracle.
