@@ -317,26 +317,61 @@ GBGHT_HD void x_turnaround(const Cta& c, Cplx<T>* sm, const Cplx<T>* GBGHT_RESTR
     for (int r = 1; r < R; ++r) v[r] = v[r] * w[r];
     dft<T, R, +1>(v);
   };
+  const auto products = [&](int p, const Cplx<T>* a, const Cplx<T>* b, const Cplx<T>* d, const Cplx<T>* ph,
+                            Cplx<T> (&o)[3][R]) {
 #pragma unroll
-  for (int s = 0; s < SLOTS; ++s) {
-    const int it = c.tid + s * NT;
-    if (SLOTS * NT == ITEMS || it < ITEMS) {
-      const int j = it % NB, p = it / NB;
-      Cplx<T> ph[R], a[R], b[R], d[R];
-      inv_last(3 * P + p / 2, j, ph);   // φ(2h) + i·φ(2h+1)
-      inv_last(3 * p, j, a);            // u_x + i·u_y
-      inv_last(3 * p + 1, j, b);        // u_z + i·ω_x
-      inv_last(3 * p + 2, j, d);        // ω_y + i·ω_z
+    for (int r = 0; r < R; ++r) {
+      const T ux = a[r].x, uy = a[r].y, uz = b[r].x, wx = b[r].y, wy = d[r].x, wz = d[r].y;
+      const T phi = (p & 1) ? ph[r].y : ph[r].x;
+      o[0][r] = cmk<T>(uy * wz - uz * wy, uz * wx - ux * wz);
+      o[1][r] = cmk<T>(ux * wy - uy * wx, ux * phi);
+      o[2][r] = cmk<T>(uy * phi, uz * phi);
+    }
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const T ux = a[r].x, uy = a[r].y, uz = b[r].x, wx = b[r].y, wy = d[r].x, wz = d[r].y;
-        const T phi = (p & 1) ? ph[r].y : ph[r].x;
-        out[s][0][r] = cmk<T>(uy * wz - uz * wy, uz * wx - ux * wz);
-        out[s][1][r] = cmk<T>(ux * wy - uy * wx, ux * phi);
-        out[s][2][r] = cmk<T>(uy * phi, uz * phi);
+    for (int k = 0; k < 3; ++k) dft<T, R, -1>(o[k]);
+  };
+  // When the items leave enough threads idle (FP64), those threads run the φ lines' last stage
+  // in place meanwhile, and each item reads φ after a barrier instead of transforming its φ line
+  // itself (that transform is shared by two points).
+  constexpr int PHI = NB * (P / 2);
+  constexpr bool kPhiAside = SLOTS == 1 && ITEMS + PHI <= NT;
+  if constexpr (kPhiAside) {
+    const int it = c.tid;
+    const int j = it % NB, p = it / NB;
+    Cplx<T> a[R], b[R], d[R];
+    if (it < ITEMS) {
+      inv_last(3 * p, j, a);        // u_x + i·u_y
+      inv_last(3 * p + 1, j, b);    // u_z + i·ω_x
+      inv_last(3 * p + 2, j, d);    // ω_y + i·ω_z
+    } else if (it < ITEMS + PHI) {
+      const int k = it - ITEMS, jj = k % NB, h = k / NB;
+      Cplx<T> v[R];
+      inv_last(3 * P + h, jj, v);   // φ(2h) + i·φ(2h+1), back into its line (rows jj + r·NB)
+      Cplx<T>* L = sm + (3 * P + h) * N;
+#pragma unroll
+      for (int r = 0; r < R; ++r) L[lidx<T>(jj + r * NB)] = v[r];
+    }
+    GBGHT_SYNC();
+    if (it < ITEMS) {
+      const Cplx<T>* L = sm + (3 * P + p / 2) * N;
+      Cplx<T> ph[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) ph[r] = L[lidx<T>(j + r * NB)];
+      products(p, a, b, d, ph, out[0]);
+    }
+  } else {
+#pragma unroll
+    for (int s = 0; s < SLOTS; ++s) {
+      const int it = c.tid + s * NT;
+      if (SLOTS * NT == ITEMS || it < ITEMS) {
+        const int j = it % NB, p = it / NB;
+        Cplx<T> ph[R], a[R], b[R], d[R];
+        inv_last(3 * P + p / 2, j, ph);   // φ(2h) + i·φ(2h+1)
+        inv_last(3 * p, j, a);            // u_x + i·u_y
+        inv_last(3 * p + 1, j, b);        // u_z + i·ω_x
+        inv_last(3 * p + 2, j, d);        // ω_y + i·ω_z
+        products(p, a, b, d, ph, out[s]);
       }
-#pragma unroll
-      for (int k = 0; k < 3; ++k) dft<T, R, -1>(out[s][k]);
     }
   }
   GBGHT_SYNC();
