@@ -25,7 +25,7 @@ __device__ __forceinline__ void init_bars(uint64_t* bar, int n) {
 }
 
 template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT, 2) k_y_inverse(const __grid_constant__ TmaMaps m, Geometry g, int c0,
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_y_inverse(const __grid_constant__ TmaMaps m, Geometry g, int c0,
                                                      const Cplx<T>* tw, unsigned int* status) {
   CTA_CTX;
   Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(NT, 2) k_y_inverse(const __grid_constant__ Tma
 }
 
 template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT, 2) k_y_forward(const __grid_constant__ TmaMaps m, Geometry g, const Cplx<T>* tw,
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_y_forward(const __grid_constant__ TmaMaps m, Geometry g, const Cplx<T>* tw,
                                                      unsigned int* status) {
   CTA_CTX;
   Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
