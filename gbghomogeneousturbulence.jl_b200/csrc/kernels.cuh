@@ -131,7 +131,7 @@ __device__ __forceinline__ double with_z_rows(uint32_t* slot, const F& run) {
 // Shared memory: ZLayout (the FFT tile, NT doubles, barriers, the TMEM address, the twiddle table,
 // the staging region).
 template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT, NT > 256 ? 1 : 2) k_z_epilogue(const __grid_constant__ TmaMaps m, Geometry g, Cplx<T>* A,
+__global__ void __launch_bounds__(NT, NT > 256 ? 1 : (sizeof(T) == 8 ? 2 : 4)) k_z_epilogue(const __grid_constant__ TmaMaps m, Geometry g, Cplx<T>* A,
                                                       Cplx<T>* S, Cplx<T>* H, StageArgs st, const double* amp,
                                                       double* partial, const Cplx<T>* tw, unsigned int* status) {
   CTA_CTX;
