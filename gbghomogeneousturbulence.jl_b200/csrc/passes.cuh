@@ -116,40 +116,21 @@ GBGHT_HD void y_inverse_compute(const Cta& c, Cplx<T>* sm, const Geometry& g, co
 
 // ================================================================================================
 // x-pass: for P points (z, y0..y0+P−1), c2r of u, ω, φ, the products u×ω and uφ, and r2c of the
-// six products. The spectra stay in B's slots (in place). Grid: (N/P, N).
-// P = TL/4 points share one tile of TL lines (TL = 8 for FP64, 16 for FP32; rows of 128 bytes,
-// swizzled so that rows and columns are both conflict-free):
+// six products. The spectra stay in B's slots (in place). Two tiles per CTA.
+// P = TL/4 points (2 in FP64, 4 in FP32) share a tile of lines, each line N elements in shared
+// memory, transformed by one warp (warp_fft.cuh):
 //   inverse: line 3p+0 = u_x + i·u_y, 3p+1 = u_z + i·ω_x, 3p+2 = ω_y + i·ω_z (point p), and line
 //            3P + p/2 = φ(p) + i·φ(p+1) for even p: 3P + P/2 lines in use
 //   forward: line 3p+0 = n_x + i·n_y, 3p+1 = n_z + i·f_x, 3p+2 = f_y + i·f_z, n = u×ω, f = uφ
 // Two real lines a, b share one complex transform ("two for one"). Inverse: Z[e] = A[e] + i·B[e]
 // for 0 ≤ e ≤ K, and Z[N−e] = conj(A[e]) + i·conj(B[e]); only the real parts of the kx = 0 bins
 // enter, as in a c2r. Forward: A[k] = (Z[k] + conj Z[N−k])/2, B[k] = (Z[k] − conj Z[N−k])/(2i).
-// The spectra move through a staging area of rows [c][p][KXS] (KXS ≥ K+1 elements, a multiple
-// of 16 bytes), copied whole to and from B.
+// The spectra come in through a staging area of rows [c][p][KXS] (KXS ≥ K+1 elements, a
+// multiple of 16 bytes), filled by bulk copies from B.
 // ================================================================================================
-template <class T, int SWZ_TL>
-GBGHT_HD void pack_pair(Cplx<T>* sm, int N, int line, int e, Cplx<T> a, Cplx<T> b, T sc) {
-  if (e == 0) {
-    sm[tix<SWZ_TL, true>(0, line)] = cmk<T>(a.x * sc, b.x * sc);
-  } else {
-    sm[tix<SWZ_TL, true>(e, line)] = cmk<T>((a.x - b.y) * sc, (a.y + b.x) * sc);
-    sm[tix<SWZ_TL, true>(N - e, line)] = cmk<T>((a.x + b.y) * sc, (b.x - a.y) * sc);
-  }
-}
-
-template <class T, int SWZ_TL>
-GBGHT_HD void unpack_pair(const Cplx<T>* sm, int N, int line, int k, Cplx<T>& a, Cplx<T>& b) {
-  const Cplx<T> z = sm[tix<SWZ_TL, true>(k, line)];
-  const Cplx<T> zc = conj(sm[tix<SWZ_TL, true>((N - k) % N, line)]);
-  const Cplx<T> sp = z + zc, sd = z - zc;
-  a = cmk<T>(sp.x * T(0.5), sp.y * T(0.5));
-  b = cmk<T>(sd.y * T(0.5), -sd.x * T(0.5));
-}
-
 template <class T> struct XShape {
   static constexpr int TL = 128 / int(sizeof(Cplx<T>));
-  static constexpr int P = TL / 4;                 // points per tile (products pass)
+  static constexpr int P = TL / 4;                 // points per tile (x pass)
   static constexpr int ACT_INV = 3 * P + P / 2;
   static constexpr int ACT_FWD = 3 * P;
   static constexpr int NW = sizeof(Cplx<T>) == 16 ? 7 : 8;   // warps of the x pass (≥ 1 turnaround item per thread)
@@ -392,9 +373,8 @@ GBGHT_HD void x_turnaround(const Cta& c, Cplx<T>* sm, const Cplx<T>* GBGHT_RESTR
 }
 
 // One x tile: the inverse of the staged spectra (the first stage reads the staging; after it the
-// staging is free and the next tile's copies are issued), the products, the forward transform and
-// the unpack into B. Kept out of line: inlined into the persistent loop below, its lane-dependent
-// index arithmetic is hoisted out of the loop and the kernel spills.
+// staging is free and the next tile's copies are issued), the turnaround (last inverse stage,
+// products, first forward stage), the rest of the forward transform, and the unpack into B.
 template <class T, int N, int NT>
 GBGHT_HD void x_tile(const Cta& c, Cplx<T>* sm, const XStaging<T, XShape<T>::P>& stage,
                                     const XStagedSource<T, N, XShape<T>::P>& src, const Geometry& g,
