@@ -143,45 +143,6 @@ GBGHT_HD int x_kxs(int K, int elem_bytes) {
   return ((K + 1 + per - 1) / per) * per;
 }
 
-// Source of the x-pass inverse's first stage: row e of line l, packed two-for-one straight from B
-// (a c2r input: only the real part of the kx = 0 bin, rows K < e < N−K zero), scaled by 1/N³.
-// Lines 3p..3p+2 pair comps (0,1), (2,3), (4,5) of point p; line 3P + h pairs φ of points 2h, 2h+1.
-template <class T, int N, int P>
-struct XPackedSource {
-  static constexpr bool kExternal = true;
-  const Geometry& g;
-  const Cplx<T>* B;
-  int z, y0, has_scalar;
-  T sc;
-  GBGHT_HD Cplx<T> load(int e, int l) const {
-    const int K = g.K;
-    if (e > K && e < N - K) return czero<T>();
-    int ca, cb, ya, yb;
-    if (l < 3 * P) {
-      const int p = l / 3, pr = l % 3;
-      ca = 2 * pr;
-      cb = 2 * pr + 1;
-      ya = yb = y0 + p;
-    } else {
-      if (!has_scalar) return czero<T>();
-      const int h = l - 3 * P;
-      ca = cb = 6;
-      ya = y0 + 2 * h;
-      yb = ya + 1;
-    }
-    if (e == 0) {
-      const Cplx<T> a = B[idxB(g, ca, z, ya, 0)], b = B[idxB(g, cb, z, yb, 0)];
-      return cmk<T>(a.x * sc, b.x * sc);
-    }
-    if (e <= K) {
-      const Cplx<T> a = B[idxB(g, ca, z, ya, e)], b = B[idxB(g, cb, z, yb, e)];
-      return cmk<T>((a.x - b.y) * sc, (a.y + b.x) * sc);
-    }
-    const Cplx<T> a = B[idxB(g, ca, z, ya, N - e)], b = B[idxB(g, cb, z, yb, N - e)];
-    return cmk<T>((a.x + b.y) * sc, (b.x - a.y) * sc);
-  }
-};
-
 // One line of an (e, l)-indexed source, for the warp-per-line transform.
 template <class Src>
 struct LineOfSource {
@@ -191,8 +152,10 @@ struct LineOfSource {
   GBGHT_HD auto load(int e) const { return s.load(e, l); }
 };
 
-// Source of the x-pass inverse's first stage from the staging rows [c][p][KXS] in shared memory
-// (the same packing as XPackedSource).
+// Source of the x-pass inverse's first stage: row e of line l from the staging rows [c][p][KXS]
+// in shared memory, packed two-for-one (a c2r input: only the real part of the kx = 0 bin, rows
+// K < e < N−K zero), scaled by 1/N³. Lines 3p..3p+2 pair comps (0,1), (2,3), (4,5) of point p;
+// line 3P + h pairs φ of points 2h, 2h+1.
 template <class T, int N, int P>
 struct XStagedSource {
   static constexpr bool kExternal = true;
@@ -256,11 +219,6 @@ struct XStaging {
   }
 };
 
-#ifdef __CUDA_ARCH__
-#define GBGHT_NOINLINE __noinline__
-#else
-#define GBGHT_NOINLINE
-#endif
 // A host-device function kept out of line on the device: one copy of a body that a kernel calls
 // several times, to keep the kernel's code within the instruction cache.
 #ifdef __CUDACC__
