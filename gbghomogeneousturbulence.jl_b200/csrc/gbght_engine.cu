@@ -106,6 +106,9 @@ static int compute_K(int N, double s, double cut2) {
 template <class T, int N>
 class EngineImpl final : public Engine {
   static constexpr int TLY = Shape<T>::TLY;
+  // The y tiles' TMA copies start at row offsets K+1, N−K−1 and N−K, which must be 128-byte
+  // aligned in shared memory: rows of exactly 128 bytes make every row offset aligned.
+  static_assert(TLY * sizeof(Cplx<T>) == 128, "y tiles need 128-byte rows");
   static constexpr int TLZ = Shape<T>::TLZ;
   static constexpr int NTY = kNT(N * TLY / 8);
   static constexpr int NTX = kNT(N);            // (unused by the warp-per-line x passes)
