@@ -156,7 +156,9 @@ def algorithmic_bytes_per_step(N, K, w_complex, has_scalar=True):
     S = 5
     ninv, nfwd = (7, 6) if has_scalar else (6, 3)
     b = {}
-    b["y_inverse"] = (S * ninv + 3) * N * KX1 * (NY2 + N) * w_complex
+    # S stages of ninv slots, except the first stage's velocity slots, which reuse the closing
+    # deposit's y-inverse of the previous step; plus that deposit (3 slots)
+    b["y_inverse"] = ((S - 1) * ninv + (ninv - 3) + 3) * N * KX1 * (NY2 + N) * w_complex
     b["x_products"] = S * N * N * KX1 * (ninv + nfwd) * w_complex
     b["y_forward"] = S * nfwd * N * KX1 * (N + NY2) * w_complex
     nst = 4 if has_scalar else 3
