@@ -51,6 +51,23 @@ def test_larger_grids_short(cuda_library):
         compare(run, orun, tol=1e-12)
 
 
+@pytest.mark.parametrize("N,precision", [(192, "fp64"), (256, "fp64"), (256, "fp32_mixed")])
+def test_production_paths_one_step(cuda_library, N, precision):
+    # The paths the 512³ benchmark runs, on a radix-3 plan (192 = 8·3·8) and on 256 = 8·4·8:
+    # - TMEM-resident z rows;
+    # - the FP64 turnaround with the φ lines transformed aside;
+    # - the FP32 occupancy of the y and z passes;
+    # - the traversal sort.
+    run, orun = make_case(N, viscosity=0.005, forcing=0.1, G=(1.0, 0.0, 0.0), tracers=2000, precision=precision,
+                          library=cuda_library)
+    advance_both(run, orun, 1, dt=0.002)
+    if precision == "fp64":
+        res = compare(run, orun, tol=1e-12)
+        assert res["X_err"] < 1e-10
+    else:
+        compare(run, orun, tol=1e-5, check_tracers=False)
+
+
 def test_observables_spectra_speed(cuda_library):
     run, orun = make_case(64, forcing=0.1, library=cuda_library)
     advance_both(run, orun, 3, dt=0.005)
