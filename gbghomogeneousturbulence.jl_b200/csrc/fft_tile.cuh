@@ -11,8 +11,8 @@
 // Consecutive threads take the same butterfly of consecutive lines (idx = j·TL + l; the threads of
 // lines at or past ACT stay idle). A quarter warp of 8 threads therefore touches one row of the
 // tile, for every stage's reads and writes.
-// Rows are 128 bytes when TL·sizeof(element) = 128, so the shared-memory accesses are free of bank
-// conflicts whatever the stage's stride. The swizzled layout (tix) keeps columns conflict-free too.
+// Rows are 64 or 128 bytes, so the shared-memory accesses are free of bank conflicts whatever the
+// stage's stride.
 //
 // SIGN = -1 is the forward (unnormalised) transform, SIGN = +1 the inverse (unnormalised).
 // `tw` holds e^(-2πi k/N) for k in [0, N), computed on the host in extended precision.
@@ -111,20 +111,9 @@ template <class T, int R, int SIGN> GBGHT_HD void dft(Cplx<T>* v) {
 
 // ---- the tile transform -------------------------------------------------------------------------
 
-// Index of element e of line l in a tile of TL lines. With SWZ, the 16-byte chunks of each
-// 128-byte row are permuted by XOR with (e mod 8), so that both a row (fixed e, varying l) and a
-// column (fixed l, consecutive e) are read without bank conflicts.
-template <int TL, bool SWZ>
-GBGHT_HD int tix(int e, int l) {
-  if constexpr (!SWZ) {
-    return e * TL + l;
-  } else if constexpr (TL == 8) {
-    return e * 8 + (l ^ (e & 7));
-  } else {
-    static_assert(TL == 16, "swizzled tiles are 128-byte rows");
-    return e * 16 + ((((l >> 1) ^ (e & 7)) << 1) | (l & 1));
-  }
-}
+// Index of element e of line l in a tile of TL lines.
+template <int TL>
+GBGHT_HD int tix(int e, int l) { return e * TL + l; }
 
 // The twiddle table e^(-2πi k/N): a pointer is a table in global memory (read through the
 // read-only path); SharedTwiddles is a copy in shared memory, for kernels whose L1 cannot keep the
@@ -161,12 +150,12 @@ template <class F>
 struct is_indexed<F, std::void_t<decltype(F::kIndexed)>> : std::bool_constant<F::kIndexed> {};
 
 // The tile buffer as the default source of the first stage and sink of the last one.
-template <class T, int TL, bool SWZ>
+template <class T, int TL>
 struct TileBuf {
   static constexpr bool kExternal = false;   // the first stage reads the tile it writes
   Cplx<T>* buf;
-  GBGHT_HD Cplx<T> load(int e, int l) const { return buf[tix<TL, SWZ>(e, l)]; }
-  GBGHT_HD void store(int e, int l, Cplx<T> v) const { buf[tix<TL, SWZ>(e, l)] = v; }
+  GBGHT_HD Cplx<T> load(int e, int l) const { return buf[tix<TL>(e, l)]; }
+  GBGHT_HD void store(int e, int l, Cplx<T> v) const { buf[tix<TL>(e, l)] = v; }
 };
 
 // ACT ≤ TL lines are transformed; lines ACT..TL−1 are left untouched. The first stage reads its
@@ -179,7 +168,7 @@ struct TileBuf {
 // Stages [S, S_END) run; a call that stops early leaves the partial transform in the tile, and a
 // later call with S = the stop resumes it (the caller can act between the two, after the barrier
 // that ends every stage).
-template <class T, int N, int TL, int NT, int SIGN, bool SWZ = false, int ACT = TL, int S = 0,
+template <class T, int N, int TL, int NT, int SIGN, int ACT = TL, int S = 0,
           int S_END = Radices<N>::n, class Src, class Dst, class TW>
 GBGHT_HD void tile_fft_io(const Cta& c, Cplx<T>* buf, const TW& tw, const Src& src, const Dst& dst) {
   if constexpr (S < S_END) {
@@ -202,7 +191,7 @@ GBGHT_HD void tile_fft_io(const Cta& c, Cplx<T>* buf, const TW& tw, const Src& s
             if constexpr (is_indexed<Src>::value) v[b][r] = src.load_rb(j + r * NB, l, r, b);
             else v[b][r] = src.load(j + r * NB, l);
           } else {
-            v[b][r] = buf[tix<TL, SWZ>(j + r * NB, l)];
+            v[b][r] = buf[tix<TL>(j + r * NB, l)];
           }
         }
       }
@@ -228,20 +217,20 @@ GBGHT_HD void tile_fft_io(const Cta& c, Cplx<T>* buf, const TW& tw, const Src& s
             if constexpr (is_indexed<Dst>::value) dst.store_rb(base + r * NS, l, v[b][r], r, b);
             else dst.store(base + r * NS, l, v[b][r]);
           } else {
-            buf[tix<TL, SWZ>(base + r * NS, l)] = v[b][r];
+            buf[tix<TL>(base + r * NS, l)] = v[b][r];
           }
         }
       }
     }
     GBGHT_SYNC();
-    tile_fft_io<T, N, TL, NT, SIGN, SWZ, ACT, S + 1, S_END>(c, buf, tw, src, dst);
+    tile_fft_io<T, N, TL, NT, SIGN, ACT, S + 1, S_END>(c, buf, tw, src, dst);
   }
 }
 
-template <class T, int N, int TL, int NT, int SIGN, bool SWZ = false, int ACT = TL>
+template <class T, int N, int TL, int NT, int SIGN, int ACT = TL>
 GBGHT_HD void tile_fft(const Cta& c, Cplx<T>* buf, const Cplx<T>* GBGHT_RESTRICT tw) {
-  const TileBuf<T, TL, SWZ> tb{buf};
-  tile_fft_io<T, N, TL, NT, SIGN, SWZ, ACT>(c, buf, tw, tb, tb);
+  const TileBuf<T, TL> tb{buf};
+  tile_fft_io<T, N, TL, NT, SIGN, ACT>(c, buf, tw, tb, tb);
 }
 
 }  // namespace gbght

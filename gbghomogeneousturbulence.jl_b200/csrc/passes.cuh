@@ -857,10 +857,10 @@ GBGHT_HD void z_forward_staged(const Cta& c, Cplx<T>* W, const ZStaging<T, N, TL
     tile_fft_io<T, N, TL, NT, -1>(c, W, tw, src, dst);
     after();
   } else {
-    const TileBuf<T, TL, false> tb{W};
-    tile_fft_io<T, N, TL, NT, -1, false, TL, 0, 1>(c, W, tw, src, tb);
+    const TileBuf<T, TL> tb{W};
+    tile_fft_io<T, N, TL, NT, -1, TL, 0, 1>(c, W, tw, src, tb);
     after();
-    tile_fft_io<T, N, TL, NT, -1, false, TL, 1>(c, W, tw, tb, dst);
+    tile_fft_io<T, N, TL, NT, -1, TL, 1>(c, W, tw, tb, dst);
   }
   rows.put_done();
 }
