@@ -88,6 +88,21 @@ Tableau tableau(int scheme) {
 
 bool finite_positive(double v) { return std::isfinite(v) && v > 0.0; }
 
+// The band's shell bounds, as `_check_shells` (src/Forcing.jl:387-403) refuses them: the lowest
+// at least 1, the highest an integer shell or infinity, and not below the lowest.
+std::string shell_error(int lowest, double highest) {
+  if (lowest < 1)
+    return "`lowest_shell` must be at least 1, got " + std::to_string(lowest) +
+           ": shell 0 is the mean (κ = 0) mode, which a band forcing cannot legitimately drive";
+  if (!(highest == INFINITY || (std::isfinite(highest) && highest == std::floor(highest))))
+    return "`highest_shell` must be an integer shell or `Inf` (every retained mode but the mean), got " +
+           std::to_string(highest);
+  if (!(highest >= lowest))
+    return "`highest_shell` must be at least `lowest_shell`, got " + std::to_string(highest) + " < " +
+           std::to_string(lowest) + ": the band would be empty and the forcing would silently do nothing";
+  return std::string();
+}
+
 int check_run(gbght_run* r) { return r ? GBGHT_OK : GBGHT_ERR_ARGUMENT; }
 
 int require_deposit(gbght_run* r, const char* what) {
@@ -141,6 +156,11 @@ void gbght_config_default(gbght_config* c) {
   c->injection_rate = 0.0;
   c->lowest_shell = 1;
   c->highest_shell = 2.0;
+  c->linear_rate = 0.0;
+  c->scalar_forcing = GBGHT_FORCING_NONE;
+  c->scalar_linear_rate = 0.0;
+  c->scalar_lowest_shell = 1;
+  c->scalar_highest_shell = 2.0;
   c->tracers = 0;
   c->cfl = 0.5;
   c->max_dt = INFINITY;
@@ -173,12 +193,26 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
                ": the scalar diffusivity is ν/Sc, so a non-positive Schmidt number makes it infinite or negative");
   if (cfg->precision != GBGHT_FP64 && cfg->precision != GBGHT_FP32_MIXED) return bad("unknown precision");
   if (cfg->scheme != GBGHT_IFRK4 && cfg->scheme != GBGHT_IFRK3) return bad("unknown field integration scheme");
-  if (cfg->velocity_forcing != GBGHT_FORCING_NONE && cfg->velocity_forcing != GBGHT_FORCING_CONSTANT_POWER)
+  if (cfg->velocity_forcing != GBGHT_FORCING_NONE && cfg->velocity_forcing != GBGHT_FORCING_CONSTANT_POWER &&
+      cfg->velocity_forcing != GBGHT_FORCING_LINEAR)
     return bad("unknown velocity forcing");
-  if (cfg->velocity_forcing == GBGHT_FORCING_CONSTANT_POWER) {
-    if (!std::isfinite(cfg->injection_rate)) return bad("injection_rate must be finite");
-    if (cfg->lowest_shell < 1) return bad("lowest_shell must be at least 1");
-    if (!(cfg->highest_shell >= cfg->lowest_shell)) return bad("highest_shell must be at least lowest_shell");
+  if (cfg->velocity_forcing == GBGHT_FORCING_CONSTANT_POWER && !std::isfinite(cfg->injection_rate))
+    return bad("injection_rate must be finite");
+  if (cfg->velocity_forcing == GBGHT_FORCING_LINEAR && !std::isfinite(cfg->linear_rate))
+    return bad("the Linear rate must be finite");
+  if (cfg->velocity_forcing != GBGHT_FORCING_NONE) {
+    std::string m = shell_error(cfg->lowest_shell, cfg->highest_shell);
+    if (!m.empty()) return bad(m);
+  }
+  if (cfg->scalar_forcing != GBGHT_FORCING_NONE && cfg->scalar_forcing != GBGHT_FORCING_LINEAR)
+    return bad("unsupported scalar forcing: the scalar takes NoForcing or Linear");
+  if (cfg->scalar_forcing != GBGHT_FORCING_NONE) {
+    if (!cfg->scalar)
+      return bad("a Linear scalar forcing was given, but the run carries no scalar: set `scalar = 1`, or "
+                 "leave `scalar_forcing` at NoForcing");
+    if (!std::isfinite(cfg->scalar_linear_rate)) return bad("the scalar Linear rate must be finite");
+    std::string m = shell_error(cfg->scalar_lowest_shell, cfg->scalar_highest_shell);
+    if (!m.empty()) return bad(m);
   }
   for (int i = 0; i < 3; ++i)
     if (!std::isfinite(cfg->mean_gradient[i])) return bad("mean_gradient must be finite");
@@ -205,6 +239,11 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
   p.injection_rate = cfg->injection_rate;
   p.lowest_shell = cfg->lowest_shell;
   p.highest_shell = cfg->highest_shell;
+  p.linear_rate = cfg->velocity_forcing == GBGHT_FORCING_LINEAR ? cfg->linear_rate : 0.0;
+  p.scalar_forcing = cfg->scalar_forcing;
+  p.scalar_linear_rate = cfg->scalar_forcing == GBGHT_FORCING_LINEAR ? cfg->scalar_linear_rate : 0.0;
+  p.scalar_lowest_shell = cfg->scalar_lowest_shell;
+  p.scalar_highest_shell = cfg->scalar_highest_shell;
   for (int i = 0; i < 3; ++i) p.G[i] = cfg->mean_gradient[i];
   p.tracers = cfg->tracers;
   p.device = cfg->device;

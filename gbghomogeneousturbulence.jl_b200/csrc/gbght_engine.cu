@@ -280,9 +280,14 @@ class EngineImpl final : public Engine {
       st.first = i == 0;
       st.last = i == S - 1;
       st.has_scalar = p_.scalar;
-      st.forced = p_.forcing != 0;
+      st.forced = p_.forcing == 1;
       st.band_lo2 = lo_hi[0];
       st.band_hi2 = lo_hi[1];
+      // Linear: the steady rate A on the band enters the exponent as (d_i·dt)·A
+      st.lin_u = (d[i] * dt) * p_.linear_rate;
+      st.lin_phi = (d[i] * dt) * p_.scalar_linear_rate;
+      st.sband_lo2 = shell_lo2(p_.scalar_lowest_shell);
+      st.sband_hi2 = shell_hi2(p_.scalar_highest_shell);
       st.G[0] = p_.G[0];
       st.G[1] = p_.G[1];
       st.G[2] = p_.G[2];
@@ -548,15 +553,19 @@ class EngineImpl final : public Engine {
     return nullptr;
   }
 
-  double band_lo2() const {
-    const double lo = (p_.lowest_shell - 0.5) * g_.s;
+  // Squared edges of shells lowest..highest, shell h covering [h − ½, h + ½)·2π/L; an infinite
+  // highest shell stands for the grid's corner shell ⌈√3 N/2⌉ (src/Forcing.jl:435-441).
+  double shell_lo2(int lowest) const {
+    const double lo = (lowest - 0.5) * g_.s;
     return lo * lo;
   }
-  double band_hi2() const {
-    const double top = std::isfinite(p_.highest_shell) ? p_.highest_shell : std::ceil(std::sqrt(3.0) * N / 2.0);
+  double shell_hi2(double highest) const {
+    const double top = std::isfinite(highest) ? highest : std::ceil(std::sqrt(3.0) * N / 2.0);
     const double hi = (top + 0.5) * g_.s;
     return hi * hi;
   }
+  double band_lo2() const { return shell_lo2(p_.lowest_shell); }
+  double band_hi2() const { return shell_hi2(p_.highest_shell); }
 
   static constexpr size_t kBarBytes = 32;
   size_t smem_y() const { return size_t(N) * TLY * sizeof(Cplx<T>) + kBarBytes; }

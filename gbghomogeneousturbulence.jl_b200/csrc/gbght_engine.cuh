@@ -30,10 +30,15 @@ struct RunParams {
   int scheme;
   double viscosity, schmidt;
   int scalar;
-  int forcing;
-  double injection_rate;
-  int lowest_shell;
+  int forcing;               // velocity: gbght_forcing
+  double injection_rate;     // ConstantPower ε
+  int lowest_shell;          // velocity band
   double highest_shell;
+  double linear_rate;        // velocity Linear A (0 unless Linear)
+  int scalar_forcing;        // scalar: NONE or LINEAR
+  double scalar_linear_rate; // scalar Linear A (0 unless Linear)
+  int scalar_lowest_shell;   // scalar band
+  double scalar_highest_shell;
   double G[3];
   int64_t tracers;
   int device;

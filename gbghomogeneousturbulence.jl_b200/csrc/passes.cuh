@@ -933,7 +933,8 @@ GBGHT_HD void z_inverse_velocity(const Cta& c, Cplx<T>* W, const Geometry& g, Cp
 //   N̂_φ = −𝔻 iκ·FFT(uφ) − G·û_i                          (src/Generator.jl:708-720; G is an extension)
 //   N̂_u = 𝔻 ℙ FFT(u×ω), κ = 0 zeroed, + A 𝟙_band û_i     (src/Generator.jl:484-534, Forcing.jl:1104-1117)
 //   h ← dt·N̂ (i = 0) or a_i h + dt·N̂
-//   q ← E(q + b_i h), h ← E h (i < S−1), E = exp(c_i |κ|²), c_i = −D·(d_i·dt)
+//   q ← E(q + b_i h), h ← E h (i < S−1), E = exp(c_i |κ|² + r_i), c_i = −D·(d_i·dt),
+//   r_i = (d_i·dt)·A on a Linear forcing's band and 0 elsewhere (src/Generator.jl:565-581)
 //   last stage: û ← ℙ û                                  (src/Propagator.jl:401)
 // and the z-inverse of the new û, iκ×û and φ̂ into A slots 0..6 for the next stage's y-inverse.
 // `red` holds NT doubles; the CTA's sum of the Hermitian-weighted |û_new|² is returned to thread 0.
@@ -944,7 +945,9 @@ struct StageArgs {
   int first, last;      // stage 0, stage S−1
   int has_scalar;
   int forced;           // velocity forcing active (ConstantPower)
-  double band_lo2, band_hi2;   // squared band edges
+  double band_lo2, band_hi2;   // squared edges of the velocity forcing's band
+  double lin_u, lin_phi;       // (d_i·dt)·A of a Linear forcing, velocity and scalar (0: none)
+  double sband_lo2, sband_hi2; // squared edges of the scalar forcing's band
   double G[3];          // mean scalar gradient (extension)
 };
 
@@ -1019,7 +1022,8 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
           }
           Cplx<T> hh = st.first ? scale(nphi, T(st.dt))
                                 : scale(sst.at(1, q, h, l), T(st.a)) + scale(nphi, T(st.dt));
-          const T E = T(exp(st.cphi * k2));
+          const double rphi = (k2 >= st.sband_lo2 && k2 <= st.sband_hi2) ? st.lin_phi : 0.0;
+          const T E = T(exp(st.cphi * k2 + rphi));
           phi = scale(phi + scale(hh, T(st.b)), E);
           S[si] = phi;
           if (!st.last) H[si] = scale(hh, E);
@@ -1094,7 +1098,8 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
           h1 = scale(sst.at(4, q, h, l), a) + scale(n1, dt);
           h2 = scale(sst.at(5, q, h, l), a) + scale(n2, dt);
         }
-        const T E = T(exp(st.cu * k2));
+        const double ru = (k2 >= st.band_lo2 && k2 <= st.band_hi2) ? st.lin_u : 0.0;
+        const T E = T(exp(st.cu * k2 + ru));
         u0 = scale(u0 + scale(h0, bb), E);
         u1 = scale(u1 + scale(h1, bb), E);
         u2 = scale(u2 + scale(h2, bb), E);

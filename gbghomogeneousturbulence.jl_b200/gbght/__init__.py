@@ -24,7 +24,7 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "libgbght.so")
 
 FP64, FP32_MIXED = 0, 1
 IFRK4, IFRK3 = 0, 1
-FORCING_NONE, FORCING_CONSTANT_POWER = 0, 1
+FORCING_NONE, FORCING_CONSTANT_POWER, FORCING_LINEAR = 0, 1, 2
 OK, ERR_ARGUMENT, ERR_SCHEDULE, ERR_CUDA, ERR_DEVICE = 0, 1, 2, 3, 4
 
 
@@ -54,6 +54,11 @@ class Config(C.Structure):
         ("cfl", C.c_double),
         ("max_dt", C.c_double),
         ("device", C.c_int),
+        ("linear_rate", C.c_double),
+        ("scalar_forcing", C.c_int),
+        ("scalar_linear_rate", C.c_double),
+        ("scalar_lowest_shell", C.c_int),
+        ("scalar_highest_shell", C.c_double),
     ]
 
 
@@ -130,6 +135,15 @@ class ConstantPower:
 
 
 @dataclass
+class Linear:
+    """`Linear(domain; rate, lowest_shell = 1, highest_shell = 2)` (src/Forcing.jl:636-643): the
+    steady rate A on the band, folded into the integrating factor. Either field may take it."""
+    rate: float
+    lowest_shell: int = 1
+    highest_shell: float = 2
+
+
+@dataclass
 class NoForcing:
     """`NoForcing()` (src/Forcing.jl): a freely decaying field."""
 
@@ -143,6 +157,7 @@ class Setup:
     schmidt: float = 1.0
     scalar: bool = True
     velocity_forcing: object = field(default_factory=NoForcing)
+    scalar_forcing: object = field(default_factory=NoForcing)
     mean_gradient: tuple = (0.0, 0.0, 0.0)
     precision: str = "fp64"          # "fp64" or "fp32_mixed"
     scheme: str = "IFLowStorageRK4"  # or "IFLowStorageRK3"
@@ -174,10 +189,25 @@ class Run:
             cfg.injection_rate = float(f.injection_rate)
             cfg.lowest_shell = int(f.lowest_shell)
             cfg.highest_shell = float(f.highest_shell)
+        elif isinstance(f, Linear):
+            cfg.velocity_forcing = FORCING_LINEAR
+            cfg.linear_rate = float(f.rate)
+            cfg.lowest_shell = int(f.lowest_shell)
+            cfg.highest_shell = float(f.highest_shell)
         elif f is None or isinstance(f, NoForcing):
             cfg.velocity_forcing = FORCING_NONE
         else:
             raise ValueError(f"unsupported velocity forcing {f!r}")
+        f = setup.scalar_forcing
+        if isinstance(f, Linear):
+            cfg.scalar_forcing = FORCING_LINEAR
+            cfg.scalar_linear_rate = float(f.rate)
+            cfg.scalar_lowest_shell = int(f.lowest_shell)
+            cfg.scalar_highest_shell = float(f.highest_shell)
+        elif f is None or isinstance(f, NoForcing):
+            cfg.scalar_forcing = FORCING_NONE
+        else:
+            raise ValueError(f"unsupported scalar forcing {f!r}: the scalar takes NoForcing or Linear")
         for i in range(3):
             cfg.mean_gradient[i] = float(setup.mean_gradient[i])
         cfg.tracers = int(setup.tracers)

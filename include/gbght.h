@@ -42,7 +42,10 @@ enum gbght_status {
 
 enum gbght_precision { GBGHT_FP64 = 0, GBGHT_FP32_MIXED = 1 };
 enum gbght_scheme { GBGHT_IFRK4 = 0, GBGHT_IFRK3 = 1 };
-enum gbght_forcing { GBGHT_FORCING_NONE = 0, GBGHT_FORCING_CONSTANT_POWER = 1 };
+/* NONE: NoForcing. CONSTANT_POWER: ConstantPower, velocity only (src/Forcing.jl:1069-1117).
+ * LINEAR: Linear, a steady rate A on the band folded into the integrating factor,
+ * exp((A(κ) − D|κ|²)·δt) (src/Forcing.jl:636-653, src/Generator.jl:565-581). */
+enum gbght_forcing { GBGHT_FORCING_NONE = 0, GBGHT_FORCING_CONSTANT_POWER = 1, GBGHT_FORCING_LINEAR = 2 };
 enum gbght_tracer_scheme { GBGHT_HEUN = 0 };
 
 /* Device status bits (gbght_status_word). */
@@ -60,22 +63,31 @@ typedef struct gbght_config {
   int scalar;                /* 1: carry the passive scalar */
   int velocity_forcing;      /* gbght_forcing */
   double injection_rate;     /* ConstantPower ε */
-  int lowest_shell;          /* ConstantPower band, shells [lowest − ½, highest + ½]·2π/L */
-  double highest_shell;
+  int lowest_shell;          /* velocity forcing band, shells [lowest − ½, highest + ½]·2π/L; */
+  double highest_shell;      /* an integer shell, or INFINITY: every mode but the mean */
   double mean_gradient[3];   /* uniform mean scalar gradient G (extension; 0 = none) */
   int64_t tracers;           /* M ≥ 0 tracers */
   double cfl;                /* C of the advective CFL rule */
   double max_dt;             /* caller's ceiling on Δt (INFINITY = none) */
   int device;                /* CUDA device ordinal */
+  /* Appended after `device`, so a caller that fills the struct through gbght_config_default keeps
+   * its layout for the fields above. */
+  double linear_rate;        /* velocity Linear A (velocity_forcing == GBGHT_FORCING_LINEAR) */
+  int scalar_forcing;        /* gbght_forcing for the scalar: NONE or LINEAR; needs scalar = 1 */
+  double scalar_linear_rate; /* scalar Linear A */
+  int scalar_lowest_shell;   /* scalar Linear band, as lowest_shell / highest_shell */
+  double scalar_highest_shell;
 } gbght_config;
 
-/* Fill `cfg` with the defaults: N=64, L=2π, FP64, IF-RK4, ν=0.01, Sc=1, scalar on, no forcing,
- * shells 1–2, G=0, no tracers, CFL 0.5, max_dt=∞, device 0. */
+/* Fill `cfg` with the defaults: N=64, L=2π, FP64, IF-RK4, ν=0.01, Sc=1, scalar on, no forcing
+ * of either field, shells 1–2 for both bands, rates 0, G=0, no tracers, CFL 0.5, max_dt=∞,
+ * device 0. */
 void gbght_config_default(gbght_config* cfg);
 
 /* Build a run on a FixedDomain with TwoThirds dealiasing, with its generator and registers.
  * Replaces FixedDomain(...) (src/SimulationDomain.jl:295-328), FlowConditions
- * (src/Generator.jl:81-140), ConstantPower (src/Forcing.jl:1069-1075), allocate_buffers
+ * (src/Generator.jl:81-140), ConstantPower (src/Forcing.jl:1069-1075), Linear
+ * (src/Forcing.jl:636-643) for either field, allocate_buffers
  * (src/Propagator.jl:717-723) and ObservablesCache (src/Cache.jl:150-173). The state starts at
  * zero. */
 int gbght_create(gbght_run** out, const gbght_config* cfg);

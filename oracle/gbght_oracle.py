@@ -6,7 +6,7 @@ No product path calls it, and nothing in the library falls back to it.
 
 It restates, in FP64 NumPy with ``scipy.fft``, the algorithm of the reference's hot path: the
 coupled velocity + passive-scalar integrating-factor low-storage Runge–Kutta step with 2/3-rule
-dealiasing, Leray projection, ConstantPower band forcing, and Heun (ABM(1)) tracer advection with
+dealiasing, Leray projection, ConstantPower and Linear band forcing, and Heun (ABM(1)) tracer advection with
 Catmull–Rom interpolation. Every array is kept in the reference's own layout. That layout is the
 column-major ``(kx, ky, kz, comp)`` array of the rfft, held here row-major as ``[comp][kz][ky][kx]``
 with ``kx`` in ``[0, N/2]``. It is full-size and unpruned, so the oracle shares no layout or pruning
@@ -22,6 +22,7 @@ reference's own known-answer tests, re-expressed in ``tests/test_oracle_known_an
 - the closed-form observables;
 - exact diffusion;
 - the RK3 and RK4 self-convergence ratios, and the order under ConstantPower;
+- the Linear rate's exact growth of a single mode, and the Linear scalar's variance growth;
 - injected power equal to ε, and a solenoidal state;
 - the 2/3 closed ball against a 2N zero-padded product;
 - Parseval, and the planted reality violation;
@@ -169,25 +170,38 @@ class ConstantPower:
 
 
 @dataclass
+class Linear:
+    """`Linear(domain; rate, lowest_shell = 1, highest_shell = 2)` (src/Forcing.jl:636-643): a steady
+    rate A on the band, folded into the integrating factor (`steady_linear_rate`, :648-653)."""
+    rate: float
+    lowest_shell: int = 1
+    highest_shell: float = 2
+
+
+@dataclass
 class Conditions:
     viscosity: float
     schmidt: float = 1.0
-    velocity_forcing: object = None          # None (NoForcing) or ConstantPower
+    velocity_forcing: object = None          # None (NoForcing), ConstantPower or Linear
     scalar: bool = True
     mean_gradient: tuple = (0.0, 0.0, 0.0)   # extension G1: uniform mean scalar gradient G
+    scalar_forcing: object = None            # None (NoForcing) or Linear
 
     def __post_init__(self):
         if not self.viscosity > 0:
             raise ValueError(f"`viscosity` must be positive, got {self.viscosity}")
         if not self.schmidt > 0:
             raise ValueError(f"`schmidt` must be positive, got {self.schmidt}")
+        if self.scalar_forcing is not None and not self.scalar:
+            # src/Generator.jl:312-316
+            raise ValueError("a scalar forcing was given, but the run carries no scalar")
 
     @property
     def diffusivity(self) -> float:
         return self.viscosity / self.schmidt
 
 
-def band_indicator(dom: Domain, forcing: ConstantPower) -> np.ndarray:
+def band_indicator(dom: Domain, forcing) -> np.ndarray:
     """Shells lowest..highest, shell h covering [h − ½, h + ½)·2π/L (`_shell_edges`,
     src/Forcing.jl:435-439); the band test is on the squares, both edges included."""
     k0 = 2 * math.pi / dom.L
@@ -222,7 +236,7 @@ def velocity_rhs(dom: Domain, cond: Conditions, uh, u, w, eps_T):
     nh = leray(dom, nh, dom.mask)
     nh[:, 0, 0, 0] = 0.0
     f = cond.velocity_forcing
-    if f is not None:
+    if isinstance(f, ConstantPower):
         A, band = constant_power_amplitude(dom, f, uh, eps_T)
         nh = nh + A * band * uh
     return nh
@@ -278,6 +292,20 @@ class State:
     phih: np.ndarray | None = None  # (N, N, N/2+1) complex128
 
 
+def steady_rate(dom: Domain, forcing) -> np.ndarray:
+    """The per-mode steady linear rate: A on the band for Linear, zero otherwise
+    (`steady_linear_rate` src/Forcing.jl:281,648-653)."""
+    if isinstance(forcing, Linear):
+        return forcing.rate * band_indicator(dom, forcing)
+    return np.zeros_like(dom.k2)
+
+
+def integrating_factor(dom: Domain, diffusivity: float, rate: np.ndarray, delta: float) -> np.ndarray:
+    """exp((A(κ) − D|κ|²)·δ) with δ = d_i·Δt: coefficient −D·δ on |κ|², offset A scaled by δ
+    (`velocity_integrating_factor` / `scalar_integrating_factor` src/Generator.jl:565-581)."""
+    return np.exp((-(diffusivity * delta)) * dom.k2 + delta * rate)
+
+
 def step(dom: Domain, cond: Conditions, st: State, dt: float, scheme: str = "rk4") -> State:
     """One step of `_low_storage_2n_step!` (src/Propagator.jl:326-419) with scheme "rk4"
     (`IFLowStorageRK4`, :304-320) or "rk3" (`IFLowStorageRK3`, :267-274)."""
@@ -289,6 +317,8 @@ def step(dom: Domain, cond: Conditions, st: State, dt: float, scheme: str = "rk4
     hu = None
     hp = None
     dt = float(dt)
+    rate_u = steady_rate(dom, cond.velocity_forcing)
+    rate_p = steady_rate(dom, cond.scalar_forcing) if has_scalar else None
     for i in range(len(a)):
         u = dom.to_physical(uh)
         w = dom.to_physical(curl(dom, uh))
@@ -297,13 +327,13 @@ def step(dom: Domain, cond: Conditions, st: State, dt: float, scheme: str = "rk4
             phi = dom.to_physical(ph)
             np_ = scalar_rhs(dom, cond, uh, u, phi)
         hu = dt * nu_ if i == 0 else a[i] * hu + dt * nu_
-        E = np.exp((-(cond.viscosity * (d[i] * dt))) * dom.k2)
+        E = integrating_factor(dom, cond.viscosity, rate_u, d[i] * dt)
         uh = E * (uh + b[i] * hu)
         if i < len(a) - 1:
             hu = E * hu
         if has_scalar:
             hp = dt * np_ if i == 0 else a[i] * hp + dt * np_
-            Ep = np.exp((-(cond.diffusivity * (d[i] * dt))) * dom.k2)
+            Ep = integrating_factor(dom, cond.diffusivity, rate_p, d[i] * dt)
             ph = Ep * (ph + b[i] * hp)
             if i < len(a) - 1:
                 hp = Ep * hp

@@ -17,24 +17,43 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
+def oracle_forcing(f):
+    """The oracle's counterpart of a library forcing object (None for NoForcing)."""
+    if f is None or isinstance(f, gbght.NoForcing):
+        return None
+    if isinstance(f, gbght.ConstantPower):
+        return O.ConstantPower(f.injection_rate, f.lowest_shell, f.highest_shell)
+    if isinstance(f, gbght.Linear):
+        return O.Linear(f.rate, f.lowest_shell, f.highest_shell)
+    raise ValueError(f"no oracle forcing for {f!r}")
+
+
 def make_case(N, *, viscosity=0.01, schmidt=1.0, scalar=True, forcing=None, G=(0.0, 0.0, 0.0), tracers=0,
               scheme="IFLowStorageRK4", precision="fp64", cfl=0.5, seeds=(0, 1, 2), energy=0.5, variance=0.5,
-              library=None, uh=None, ph=None, X=None):
-    """Build a library run and an oracle run on identical seeded inputs, both freshly deposited."""
+              library=None, uh=None, ph=None, X=None, scalar_forcing=None):
+    """Build a library run and an oracle run on identical seeded inputs, both freshly deposited.
+
+    `forcing` is a ConstantPower ε (a number) or a library forcing object; `scalar_forcing` is a
+    library forcing object for the scalar."""
     if uh is None:
         uh = S.seed_velocity(N, energy, seed=seeds[0])
     if ph is None and scalar:
         ph = S.seed_scalar(N, variance, seed=seeds[1])
     if X is None and tracers:
         X = S.seed_tracers(tracers, seed=seeds[2])
-    lib_forcing = gbght.ConstantPower(forcing) if forcing else gbght.NoForcing()
+    if isinstance(forcing, (int, float)):
+        lib_forcing = gbght.ConstantPower(forcing) if forcing else gbght.NoForcing()
+    else:
+        lib_forcing = forcing or gbght.NoForcing()
+    lib_sforcing = scalar_forcing or gbght.NoForcing()
     setup = gbght.Setup(grid_points_per_axis=N, viscosity=viscosity, schmidt=schmidt, scalar=scalar,
-                        velocity_forcing=lib_forcing, mean_gradient=G, tracers=tracers, scheme=scheme,
-                        precision=precision, cfl=cfl)
+                        velocity_forcing=lib_forcing, scalar_forcing=lib_sforcing, mean_gradient=G,
+                        tracers=tracers, scheme=scheme, precision=precision, cfl=cfl)
     run = gbght.simulation(setup, uh, ph if scalar else None, X, library=library)
     dom = O.Domain(N)
     cond = O.Conditions(viscosity=viscosity, schmidt=schmidt, scalar=scalar,
-                        velocity_forcing=O.ConstantPower(forcing) if forcing else None, mean_gradient=G)
+                        velocity_forcing=oracle_forcing(lib_forcing), mean_gradient=G,
+                        scalar_forcing=oracle_forcing(lib_sforcing))
     orun = O.Run(dom, cond, O.State(uh.copy(), ph.copy() if scalar else None),
                  X=None if not tracers else X.copy(), scheme={"IFLowStorageRK4": "rk4", "IFLowStorageRK3": "rk3"}[scheme],
                  cfl=cfl)

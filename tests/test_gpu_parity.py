@@ -68,6 +68,35 @@ def test_production_paths_one_step(cuda_library, N, precision):
         compare(run, orun, tol=1e-5, check_tracers=False)
 
 
+@pytest.mark.parametrize("N,precision,steps", [(64, "fp64", 20), (256, "fp64", 1), (64, "fp32_mixed", 10)])
+def test_linear_forcing_both_fields(cuda_library, N, precision, steps):
+    # Linear on the velocity (shells 1–2) and on the scalar (shells 2–Inf): the steady rate in the
+    # integrating factor of both fields' epilogues, beside the mean gradient and the tracers
+    run, orun = make_case(N, viscosity=0.005, forcing=gbght.Linear(0.7), scalar_forcing=gbght.Linear(0.4, 2, math.inf),
+                          G=(0.0, 1.0, 0.0), tracers=1000, precision=precision, library=cuda_library)
+    advance_both(run, orun, steps, dt=0.004)
+    if precision == "fp64":
+        res = compare(run, orun, tol=1e-12)
+        assert res["X_err"] < 1e-10
+    else:
+        compare(run, orun, tol=1e-5, check_tracers=False)
+
+
+def test_scalar_linear_exact_growth_with_zero_velocity(cuda_library):
+    # test/forcing.jl:124-139 held to the closed form φ̂(T) = exp((A·band − ϰ|κ|²)T) φ̂(0)
+    N, nu, Sc, A = 32, 0.05, 1.0, 1.0
+    band = O.band_indicator(O.Domain(N), O.Linear(A))
+    ph0 = S.seed_scalar(N, 0.1, seed=9) * (band + 0.1 * (1 - band))
+    run = gbght.simulation(gbght.Setup(grid_points_per_axis=N, viscosity=nu, schmidt=Sc, scalar_forcing=gbght.Linear(A)),
+                           np.zeros((3, N, N, N // 2 + 1), complex), ph0, library=cuda_library)
+    for _ in range(40):
+        run.advance(0.01)
+    _, pe = run.export_state()
+    expected = ph0 * np.exp((A * band - (nu / Sc) * S.wavenumbers(N)[3]) * 0.4)
+    assert rel_l2(pe, expected) < 1e-12
+    assert run.observables()["scalar_variance"] > O.scalar_variance(O.Domain(N), ph0)
+
+
 def test_observables_spectra_speed(cuda_library):
     run, orun = make_case(64, forcing=0.1, library=cuda_library)
     advance_both(run, orun, 3, dt=0.005)

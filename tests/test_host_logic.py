@@ -23,6 +23,28 @@ def test_bad_configurations_are_argument_errors(hostcheck_library):
                   library=hostcheck_library)
 
 
+def test_bad_forcing_bands_are_argument_errors(hostcheck_library):
+    # src/Forcing.jl:387-403 (`_check_shells`) for both fields' bands; src/Generator.jl:312-316
+    def run(**kw):
+        return gbght.Run(gbght.Setup(grid_points_per_axis=16, **kw), library=hostcheck_library)
+    for make in (lambda f: run(velocity_forcing=f), lambda f: run(scalar_forcing=f)):
+        with pytest.raises(ValueError, match="lowest_shell"):
+            make(gbght.Linear(0.5, lowest_shell=0))
+        with pytest.raises(ValueError, match="integer shell"):
+            make(gbght.Linear(0.5, highest_shell=2.5))
+        with pytest.raises(ValueError, match="at least `lowest_shell`"):
+            make(gbght.Linear(0.5, lowest_shell=3, highest_shell=2))
+        with pytest.raises(ValueError, match="finite"):
+            make(gbght.Linear(math.nan))
+        make(gbght.Linear(0.5, highest_shell=math.inf)).close()
+    with pytest.raises(ValueError, match="lowest_shell"):
+        run(velocity_forcing=gbght.ConstantPower(0.1, lowest_shell=0))
+    with pytest.raises(ValueError, match="carries no scalar"):
+        run(scalar=False, scalar_forcing=gbght.Linear(1.0))
+    with pytest.raises(ValueError, match="scalar takes NoForcing or Linear"):
+        run(scalar_forcing=gbght.ConstantPower(0.1))
+
+
 def test_state_outside_the_retained_ball_is_refused(hostcheck_library):
     N = 16
     run = gbght.Run(gbght.Setup(grid_points_per_axis=N), library=hostcheck_library)

@@ -5,6 +5,8 @@ one thread per block and every launch run block by block on the CPU. Agreement h
 level shows that the kernels' layouts, pruning, index arithmetic and launch sequence restate the
 reference's step. The GPU suite (test_gpu_parity.py) repeats these comparisons on the device.
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -24,6 +26,16 @@ from pairs import advance_both, compare, make_case, rel_l2
 def test_step_matches_oracle(hostcheck_library, N, steps, forcing, G):
     run, orun = make_case(N, forcing=forcing, G=G, tracers=32, library=hostcheck_library)
     advance_both(run, orun, steps, dt=0.005)
+    res = compare(run, orun, tol=2e-14)
+    assert res["X_err"] < 1e-13
+
+
+@pytest.mark.parametrize("scheme", ["IFLowStorageRK4", "IFLowStorageRK3"])
+def test_linear_forcing_both_fields_matches_oracle(hostcheck_library, scheme):
+    # Linear on the velocity (shells 1–2) and on the scalar (shells 2–Inf), with the mean gradient
+    run, orun = make_case(16, forcing=gbght.Linear(0.7), scalar_forcing=gbght.Linear(0.4, 2, math.inf),
+                          G=(0.0, 0.0, 1.0), tracers=16, scheme=scheme, library=hostcheck_library)
+    advance_both(run, orun, 4, dt=0.01)
     res = compare(run, orun, tol=2e-14)
     assert res["X_err"] < 1e-13
 

@@ -145,13 +145,15 @@ def test_rk4_self_convergence_ratio():
     assert 10.0 < diffnorm(u1.uh, u2.uh) / diffnorm(u2.uh, u4.uh) < 26.0
 
 
+@pytest.mark.parametrize("forcing", [O.ConstantPower(0.2), O.Linear(0.5)], ids=["constant_power", "linear"])
 @pytest.mark.parametrize("scheme,floor", [("rk3", 2.5), ("rk4", 3.5)])
-def test_order_kept_under_constant_power(scheme, floor):
-    # test/integrators.jl:132-162: a state-dependent forcing through the per-stage source keeps
-    # the scheme's order (measured ≥ 2.5 for RK3; RK4 held to ≥ 3.5 here)
+def test_order_kept_under_forcing(scheme, floor, forcing):
+    # test/integrators.jl:132-162: a state-dependent forcing through the per-stage source and a
+    # steady rate through the integrating factor keep the scheme's order (measured ≥ 2.5 for RK3;
+    # RK4 held to ≥ 3.5 here)
     N = 16
     dom = O.Domain(N)
-    cond = O.Conditions(viscosity=0.05, velocity_forcing=O.ConstantPower(0.2))
+    cond = O.Conditions(viscosity=0.05, velocity_forcing=forcing)
     uh0 = S.seed_velocity(N, 0.5, seed=7)
     T = 0.2
     ref = _integrate(dom, cond, uh0, None, T / 1024, 1024, scheme).uh
@@ -193,6 +195,78 @@ def test_empty_band_clamps_amplitude():
     uh = uh * (1 - band)
     A, _ = O.constant_power_amplitude(dom, O.ConstantPower(0.1), uh, np.finfo(float).eps)
     assert A == 0.0
+
+
+def test_linear_rate_amplitude():
+    # test/forcing.jl:80-90: A on the band, zero outside, on exactly the band's modes
+    dom = O.Domain(24)
+    f = O.Linear(0.7)
+    rate = O.steady_rate(dom, f)
+    assert rate.max() == 0.7 and rate.min() == 0.0
+    assert np.array_equal(rate != 0, O.band_indicator(dom, f) != 0)
+    assert not np.any(O.steady_rate(dom, O.ConstantPower(0.1)))   # only Linear is steady
+
+
+@pytest.mark.parametrize("N", [16, 24])
+def test_linear_unbounded_band_is_every_mode_but_the_mean(N):
+    # test/forcing.jl:457-461: highest_shell = Inf forces every stored mode except κ = 0
+    rate = O.steady_rate(O.Domain(N), O.Linear(0.1, highest_shell=math.inf))
+    assert np.count_nonzero(rate == 0) == 1 and rate[0, 0, 0] == 0
+    assert np.all((rate == 0) | (rate == 0.1))
+
+
+def test_linear_injects_energy_stays_solenoidal():
+    # test/forcing.jl:106-113
+    N = 24
+    dom = O.Domain(N)
+    uh0 = S.seed_velocity(N, 0.5, seed=11)
+    unforced = _integrate(dom, O.Conditions(viscosity=0.05), uh0, None, 0.01, 60, "rk3")
+    forced = _integrate(dom, O.Conditions(viscosity=0.05, velocity_forcing=O.Linear(1.0)), uh0, None, 0.01, 60, "rk3")
+    assert O.kinetic_energy(dom, forced.uh) > O.kinetic_energy(dom, unforced.uh)
+    div = (dom.kx * forced.uh[0] + dom.ky * forced.uh[1]) + dom.kz * forced.uh[2]
+    assert math.sqrt(float(np.sum(np.abs(div) ** 2))) / math.sqrt(float(np.sum(np.abs(forced.uh) ** 2))) < 1e-8
+
+
+@pytest.mark.parametrize("scheme", ["rk3", "rk4"])
+def test_linear_shear_mode_grows_exactly(scheme):
+    # A single shear mode u = (sin y, 0, 0) has u×ω = (0, ½ sin 2y, 0), a gradient that the Leray
+    # projection removes: the mode evolves by the integrating factor alone, at net rate A − ν|κ|².
+    N, nu, A = 16, 0.05, 0.7
+    dom = O.Domain(N)
+    x3, y3, z3 = _grid(N)
+    u = np.stack([np.sin(y3), np.zeros_like(y3), np.zeros_like(y3)])
+    uh0 = dom.to_spectral(u)
+    cond = O.Conditions(viscosity=nu, scalar=False, velocity_forcing=O.Linear(A))
+    dt, n = 0.02, 25
+    st = _integrate(dom, cond, uh0, None, dt, n, scheme)
+    expected = uh0 * math.exp((A - nu) * dt * n)
+    assert diffnorm(st.uh, expected) / math.sqrt(float(np.sum(np.abs(expected) ** 2))) < 1e-12
+
+
+@pytest.mark.parametrize("scheme", ["rk3", "rk4"])
+def test_scalar_linear_grows_exactly_with_zero_velocity(scheme):
+    # test/forcing.jl:124-139 (variance builds), held here to the closed form: with u = 0 the
+    # scalar moves by the integrating factor alone, φ̂(T) = exp((A·band − ϰ|κ|²)T) φ̂(0). The seed
+    # keeps shells 1–2 and a weaker copy of the rest, standing in for the test's peak at shell 2.
+    N, nu, Sc, A = 24, 0.05, 1.0, 1.0
+    dom = O.Domain(N)
+    f = O.Linear(A)
+    band = O.band_indicator(dom, f)
+    ph0 = S.seed_scalar(N, 0.1, seed=9) * (band + 0.1 * (1 - band))
+    cond = O.Conditions(viscosity=nu, schmidt=Sc, scalar_forcing=f)
+    st = O.State(np.zeros((3,) + dom.shape_spectral, complex), ph0.copy())
+    dt, n = 0.01, 40
+    for _ in range(n):
+        st = O.step(dom, cond, st, dt, scheme)
+    assert O.scalar_variance(dom, st.phih) > O.scalar_variance(dom, ph0)
+    expected = ph0 * np.exp((A * band - (nu / Sc) * dom.k2) * dt * n)
+    assert diffnorm(st.phih, expected) / math.sqrt(float(np.sum(np.abs(expected) ** 2))) < 1e-12
+
+
+def test_scalar_forcing_needs_the_scalar():
+    # src/Generator.jl:312-316
+    with pytest.raises(ValueError, match="no scalar"):
+        O.Conditions(viscosity=0.1, scalar=False, scalar_forcing=O.Linear(1.0))
 
 
 # --- test/regressions/r6-inclusive-ball-exact.jl -------------------------------------------------
