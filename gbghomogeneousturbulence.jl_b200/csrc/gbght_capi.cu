@@ -103,6 +103,69 @@ std::string shell_error(int lowest, double highest) {
   return std::string();
 }
 
+// A field's forcing block, refused as the reference's constructors refuse it
+// (src/Forcing.jl:558-572, 636-643, 828-875, 1069-1075). `who` names the field.
+std::string forcing_error(const gbght_forcing_params& f, const char* who) {
+  const std::string w = std::string(who) + " ";
+  switch (f.kind) {
+    case GBGHT_FORCING_NONE:
+      return std::string();
+    case GBGHT_FORCING_CONSTANT_POWER:
+      if (!std::isfinite(f.rate)) return w + "ConstantPower `injection_rate` must be finite";
+      break;
+    case GBGHT_FORCING_LINEAR:
+      if (!std::isfinite(f.rate)) return w + "Linear `rate` must be finite";
+      break;
+    case GBGHT_FORCING_VARIANCE_CONTROLLER:
+      if (!(std::isfinite(f.target) && f.target > 0))
+        return w + "VarianceController `target` must be finite and positive, got " + std::to_string(f.target) +
+               ": it is the variance the controller holds, and the rate divides by the band's own variance";
+      if (!(std::isfinite(f.gain) && f.gain >= 0))
+        return w + "VarianceController `gain` must be finite and non-negative, got " + std::to_string(f.gain) +
+               ": a negative gain makes the restoring term push the variance AWAY from the target";
+      if (!finite_positive(f.turnover_time))
+        return w + "VarianceController `turnover_time` must be finite and positive, got " +
+               std::to_string(f.turnover_time);
+      break;
+    case GBGHT_FORCING_VARIANCE_RESCALING:
+      if (f.over != GBGHT_OVER_BAND && f.over != GBGHT_OVER_TOTAL)
+        return w + "VarianceRescaling `over` must be :band or :total";
+      if (!(std::isfinite(f.target) && f.target >= 0))
+        return w + "VarianceRescaling `target` must be finite and non-negative, got " + std::to_string(f.target) +
+               ": it is the kinetic energy or scalar variance the forcing holds, and the rescale takes its "
+               "square root";
+      break;
+    default:
+      return w + "forcing: unknown kind " + std::to_string(f.kind);
+  }
+  const std::string m = shell_error(f.lowest_shell, f.highest_shell);
+  return m.empty() ? m : w + "forcing: " + m;
+}
+
+gbght::ForcingParams to_forcing(const gbght_forcing_params& f) {
+  gbght::ForcingParams p{};
+  p.kind = f.kind;
+  p.rate = f.rate;
+  p.target = f.target;
+  p.gain = f.gain;
+  p.turnover_time = f.turnover_time;
+  p.over = f.over;
+  p.lowest_shell = f.lowest_shell;
+  p.highest_shell = f.highest_shell;
+  return p;
+}
+
+void forcing_default(gbght_forcing_params* f) {
+  f->kind = GBGHT_FORCING_NONE;
+  f->rate = 0.0;
+  f->target = 0.0;
+  f->gain = 1.0;
+  f->turnover_time = 0.0;
+  f->over = GBGHT_OVER_BAND;
+  f->lowest_shell = 1;
+  f->highest_shell = 2.0;
+}
+
 int check_run(gbght_run* r) { return r ? GBGHT_OK : GBGHT_ERR_ARGUMENT; }
 
 int require_deposit(gbght_run* r, const char* what) {
@@ -152,15 +215,8 @@ void gbght_config_default(gbght_config* c) {
   c->viscosity = 0.01;
   c->schmidt = 1.0;
   c->scalar = 1;
-  c->velocity_forcing = GBGHT_FORCING_NONE;
-  c->injection_rate = 0.0;
-  c->lowest_shell = 1;
-  c->highest_shell = 2.0;
-  c->linear_rate = 0.0;
-  c->scalar_forcing = GBGHT_FORCING_NONE;
-  c->scalar_linear_rate = 0.0;
-  c->scalar_lowest_shell = 1;
-  c->scalar_highest_shell = 2.0;
+  forcing_default(&c->velocity_forcing);
+  forcing_default(&c->scalar_forcing);
   c->tracers = 0;
   c->cfl = 0.5;
   c->max_dt = INFINITY;
@@ -193,27 +249,15 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
                ": the scalar diffusivity is ν/Sc, so a non-positive Schmidt number makes it infinite or negative");
   if (cfg->precision != GBGHT_FP64 && cfg->precision != GBGHT_FP32_MIXED) return bad("unknown precision");
   if (cfg->scheme != GBGHT_IFRK4 && cfg->scheme != GBGHT_IFRK3) return bad("unknown field integration scheme");
-  if (cfg->velocity_forcing != GBGHT_FORCING_NONE && cfg->velocity_forcing != GBGHT_FORCING_CONSTANT_POWER &&
-      cfg->velocity_forcing != GBGHT_FORCING_LINEAR)
-    return bad("unknown velocity forcing");
-  if (cfg->velocity_forcing == GBGHT_FORCING_CONSTANT_POWER && !std::isfinite(cfg->injection_rate))
-    return bad("injection_rate must be finite");
-  if (cfg->velocity_forcing == GBGHT_FORCING_LINEAR && !std::isfinite(cfg->linear_rate))
-    return bad("the Linear rate must be finite");
-  if (cfg->velocity_forcing != GBGHT_FORCING_NONE) {
-    std::string m = shell_error(cfg->lowest_shell, cfg->highest_shell);
+  {
+    std::string m = forcing_error(cfg->velocity_forcing, "velocity");
+    if (!m.empty()) return bad(m);
+    m = forcing_error(cfg->scalar_forcing, "scalar");
     if (!m.empty()) return bad(m);
   }
-  if (cfg->scalar_forcing != GBGHT_FORCING_NONE && cfg->scalar_forcing != GBGHT_FORCING_LINEAR)
-    return bad("unsupported scalar forcing: the scalar takes NoForcing or Linear");
-  if (cfg->scalar_forcing != GBGHT_FORCING_NONE) {
-    if (!cfg->scalar)
-      return bad("a Linear scalar forcing was given, but the run carries no scalar: set `scalar = 1`, or "
-                 "leave `scalar_forcing` at NoForcing");
-    if (!std::isfinite(cfg->scalar_linear_rate)) return bad("the scalar Linear rate must be finite");
-    std::string m = shell_error(cfg->scalar_lowest_shell, cfg->scalar_highest_shell);
-    if (!m.empty()) return bad(m);
-  }
+  if (cfg->scalar_forcing.kind != GBGHT_FORCING_NONE && !cfg->scalar)
+    return bad("a scalar forcing was given, but the run carries no scalar: set `scalar = 1`, or leave "
+               "`scalar_forcing` at NoForcing");
   for (int i = 0; i < 3; ++i)
     if (!std::isfinite(cfg->mean_gradient[i])) return bad("mean_gradient must be finite");
   if (!cfg->scalar && (cfg->mean_gradient[0] != 0 || cfg->mean_gradient[1] != 0 || cfg->mean_gradient[2] != 0))
@@ -235,15 +279,8 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
   p.viscosity = cfg->viscosity;
   p.schmidt = cfg->schmidt;
   p.scalar = cfg->scalar ? 1 : 0;
-  p.forcing = cfg->velocity_forcing;
-  p.injection_rate = cfg->injection_rate;
-  p.lowest_shell = cfg->lowest_shell;
-  p.highest_shell = cfg->highest_shell;
-  p.linear_rate = cfg->velocity_forcing == GBGHT_FORCING_LINEAR ? cfg->linear_rate : 0.0;
-  p.scalar_forcing = cfg->scalar_forcing;
-  p.scalar_linear_rate = cfg->scalar_forcing == GBGHT_FORCING_LINEAR ? cfg->scalar_linear_rate : 0.0;
-  p.scalar_lowest_shell = cfg->scalar_lowest_shell;
-  p.scalar_highest_shell = cfg->scalar_highest_shell;
+  p.vf = to_forcing(cfg->velocity_forcing);
+  p.sf = cfg->scalar ? to_forcing(cfg->scalar_forcing) : gbght::ForcingParams{};
   for (int i = 0; i < 3; ++i) p.G[i] = cfg->mean_gradient[i];
   p.tracers = cfg->tracers;
   p.device = cfg->device;

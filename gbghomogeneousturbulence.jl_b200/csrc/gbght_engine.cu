@@ -178,13 +178,14 @@ class EngineImpl final : public Engine {
     if ((err = alloc(&U_, 3 * nP_ * sizeof(T)))) return err;
     if ((err = alloc(&tw_, N * sizeof(Cplx<T>)))) return err;
     if ((err = alloc(&partial_, ntile_ * sizeof(double)))) return err;
-    if ((err = alloc(&amp_, 4 * sizeof(double)))) return err;
+    if ((err = alloc(&amp_, 16 * sizeof(double)))) return err;   // 4 per field and role
     if ((err = alloc(&maxbits_, sizeof(unsigned long long)))) return err;
     if ((err = alloc(&status_, sizeof(unsigned int)))) return err;
     if ((err = alloc(&flag_, sizeof(unsigned int)))) return err;
     // B doubles as the staging of one reference-layout component at import and export
     if (7 * nB_ * sizeof(Cplx<T>) < ref_comp_elems() * sizeof(Cplx<double>)) return "B too small to stage a component";
     if ((err = alloc(&obs_, size_t(g_.NY2) * 4 * sizeof(double)))) return err;
+    if ((err = alloc(&fobs_, size_t(g_.NY2) * 4 * sizeof(double)))) return err;
     if ((err = alloc(&spec_, size_t(g_.NY2) * nshell_ * sizeof(double)))) return err;
     if (p.tracers > 0) {
       if (p.tracers > int64_t(UINT32_MAX)) return "too many tracers for a 32-bit traversal order";
@@ -270,6 +271,7 @@ class EngineImpl final : public Engine {
   // ---- the step ---------------------------------------------------------------------------------
   const char* step(double dt, const double* a, const double* b, const double* d, int S) override {
     const double lo_hi[2] = {band_lo2(), band_hi2()};
+    const double slo_hi[2] = {sband_lo2(), sband_hi2()};
     for (int i = 0; i < S; ++i) {
       StageArgs st;
       st.a = a[i];
@@ -280,14 +282,15 @@ class EngineImpl final : public Engine {
       st.first = i == 0;
       st.last = i == S - 1;
       st.has_scalar = p_.scalar;
-      st.forced = p_.forcing == 1;
+      st.forced = stage_source(p_.vf.kind);
+      st.sforced = p_.scalar && stage_source(p_.sf.kind);
       st.band_lo2 = lo_hi[0];
       st.band_hi2 = lo_hi[1];
       // Linear: the steady rate A on the band enters the exponent as (d_i·dt)·A
-      st.lin_u = (d[i] * dt) * p_.linear_rate;
-      st.lin_phi = (d[i] * dt) * p_.scalar_linear_rate;
-      st.sband_lo2 = shell_lo2(p_.scalar_lowest_shell);
-      st.sband_hi2 = shell_hi2(p_.scalar_highest_shell);
+      st.lin_u = p_.vf.kind == kForceLinear ? (d[i] * dt) * p_.vf.rate : 0.0;
+      st.lin_phi = p_.sf.kind == kForceLinear ? (d[i] * dt) * p_.sf.rate : 0.0;
+      st.sband_lo2 = slo_hi[0];
+      st.sband_hi2 = slo_hi[1];
       st.G[0] = p_.G[0];
       st.G[1] = p_.G[1];
       st.G[2] = p_.G[2];
@@ -564,8 +567,25 @@ class EngineImpl final : public Engine {
     const double hi = (top + 0.5) * g_.s;
     return hi * hi;
   }
-  double band_lo2() const { return shell_lo2(p_.lowest_shell); }
-  double band_hi2() const { return shell_hi2(p_.highest_shell); }
+  double band_lo2() const { return shell_lo2(p_.vf.lowest_shell); }
+  double band_hi2() const { return shell_hi2(p_.vf.highest_shell); }
+  double sband_lo2() const { return shell_lo2(p_.sf.lowest_shell); }
+  double sband_hi2() const { return shell_hi2(p_.sf.highest_shell); }
+  // ConstantPower and VarianceController act through a per-stage source A·𝟙_band·f
+  static bool stage_source(int kind) { return kind == kForceConstantPower || kind == kForceController; }
+  AmpArgs amp_args(const ForcingParams& f, bool scalar) const {
+    AmpArgs a{};
+    a.kind = f.kind;
+    a.rate = f.rate;
+    a.target = f.target;
+    a.gain = f.gain;
+    a.turnover_time = f.turnover_time;
+    a.over = f.over;
+    a.factor = scalar ? 1.0 : 0.5;
+    a.diffusivity = scalar ? p_.viscosity / p_.schmidt : p_.viscosity;
+    a.eps_T = sizeof(T) == 8 ? DBL_EPSILON : double(FLT_EPSILON);
+    return a;
+  }
 
   static constexpr size_t kBarBytes = 32;
   size_t smem_y() const { return size_t(N) * TLY * sizeof(Cplx<T>) + kBarBytes; }
@@ -767,35 +787,95 @@ class EngineImpl final : public Engine {
     pend();
 #endif
   }
-  void force_amp() {
-    const double eps_T = sizeof(T) == 8 ? DBL_EPSILON : double(FLT_EPSILON);
+  // The observables' row sums of the state into fobs_ (mode 0 velocity, 1 both, 2 scalar), for the
+  // band forcings that read the whole field's variance and dissipation.
+  void row_sums(int mode) {
 #ifdef GBGHT_EMU
-    double whole = 0.0;
-    // the same association as the device tree: 256 strided partial sums, then pairwise halving
-    double red[256];
-    for (int t = 0; t < 256; ++t) {
-      double s = 0.0;
-      for (size_t i = t; i < ntile_; i += 256) s += partial_[i];
-      red[t] = s;
-    }
-    for (int w = 128; w > 0; w >>= 1)
-      for (int t = 0; t < w; ++t) red[t] += red[t + w];
-    whole = red[0];
-    const double band = band_energy_raw<T>(g_, S_, band_lo2(), band_hi2());
-    const double n6 = double(N) * N * N * double(N) * N * N;
-    const double band_obs = 0.5 * (band / n6), whole_obs = 0.5 * (whole / n6);
-    double A = 0.0;
-    if (std::isfinite(band_obs) && band_obs > 10.0 * eps_T * whole_obs) A = p_.injection_rate / (2.0 * band_obs);
-    else *status_ |= 0x2u;
-    amp_[0] = A;
-    amp_[1] = band_obs;
-    amp_[2] = whole_obs;
+    emu_grid(g_.NY2, 1, 1, 4 * sizeof(double), [&](const Cta& c, void* sm) {
+      body_observables<T, 1>(c, static_cast<double*>(sm), g_, S_, mode, fobs_);
+    });
 #else
-    pbegin(PROF_FORCE_AMP);
-    k_force_amp<T><<<1, 256, 0, stream_>>>(g_, S_, partial_, int(ntile_), band_lo2(), band_hi2(), p_.injection_rate,
-                                           eps_T, amp_, status_);
+    pbegin(PROF_OBSERVABLES);
+    k_observables<T, NTR><<<g_.NY2, NTR, 4 * NTR * sizeof(double), stream_>>>(g_, S_, mode, fobs_);
     pend();
 #endif
+  }
+  // One field's amplitude (or rescale factor) into out[0..2]; see k_force_amp.
+  void amp_launch(const AmpArgs& a, int c0, int nc, const double* whole, const double* dir, int nwhole, int stride,
+                  double lo2, double hi2, double* out) {
+#ifdef GBGHT_EMU
+    // the same association as the device tree: 256 strided partial sums, then pairwise halving
+    double red[256], dred[256];
+    for (int t = 0; t < 256; ++t) {
+      double s = 0.0, d = 0.0;
+      for (int i = t; i < nwhole; i += 256) {
+        s += whole[size_t(i) * stride];
+        if (dir) d += dir[size_t(i) * stride];
+      }
+      red[t] = s;
+      dred[t] = d;
+    }
+    for (int w = 128; w > 0; w >>= 1)
+      for (int t = 0; t < w; ++t) {
+        red[t] += red[t + w];
+        dred[t] += dred[t + w];
+      }
+    const double band = band_energy_raw<T>(g_, S_, lo2, hi2, c0, nc);
+    const double n6 = double(N) * N * N * double(N) * N * N;
+    bool empty;
+    out[0] = forcing_amplitude(a, red[0], band, dred[0], n6, &out[1], &out[2], &empty);
+    if (empty) *status_ |= 0x2u;
+#else
+    pbegin(PROF_FORCE_AMP);
+    k_force_amp<T><<<1, 256, 0, stream_>>>(g_, S_, c0, nc, whole, dir, nwhole, stride, lo2, hi2, a, out, status_);
+    pend();
+#endif
+  }
+  // The per-stage amplitudes at the stage state: the velocity's in amp_[0], the scalar's in amp_[4].
+  // The velocity's ConstantPower takes its whole-field sum from the previous epilogue's tile
+  // partials; every other source reads the observables' row sums.
+  void force_amp(const StageArgs& st) {
+    const bool vrows = st.forced && p_.vf.kind != kForceConstantPower;
+    if (vrows || st.sforced) row_sums(vrows ? (st.sforced ? 1 : 0) : 2);
+    if (st.forced) {
+      if (vrows)
+        amp_launch(amp_args(p_.vf, false), 0, 3, fobs_, fobs_ + 1, g_.NY2, 4, band_lo2(), band_hi2(), amp_);
+      else
+        amp_launch(amp_args(p_.vf, false), 0, 3, partial_, nullptr, int(ntile_), 1, band_lo2(), band_hi2(), amp_);
+    }
+    if (st.sforced)
+      amp_launch(amp_args(p_.sf, true), 3, 1, fobs_ + 2, fobs_ + 3, g_.NY2, 4, sband_lo2(), sband_hi2(), amp_ + 4);
+  }
+  // VarianceRescaling after the last stage (`finalize!`, src/Generator.jl:396-400): the factor from
+  // the end-of-step state, then the band's rescale; velocity first, then the scalar.
+  void rescale(int c0, int nc, double lo2, double hi2, const double* factor) {
+    int mb = int(std::sqrt(hi2) / g_.s) + 1;
+    if (mb > g_.K) mb = g_.K;
+    const long side = 2 * mb + 1, nbox = long(nc) * side * side * (mb + 1);
+#ifdef GBGHT_EMU
+    if (factor[0] != 1.0)
+      for (long i = 0; i < nbox; ++i) rescale_mode<T>(i, g_, S_, c0, mb, lo2, hi2, factor[0]);
+#else
+    const long blocks = std::min<long>((nbox + 255) / 256, long(sm_count_) * 8);
+    pbegin(PROF_FORCE_AMP);
+    k_rescale<T><<<unsigned(blocks), 256, 0, stream_>>>(g_, S_, c0, nc, lo2, hi2, factor);
+    pend();
+#endif
+  }
+  // Returns whether a field was rescaled (the A slots then no longer hold its z-inverse).
+  bool project() {
+    const bool v = p_.vf.kind == kForceRescaling, s = p_.sf.kind == kForceRescaling;
+    if (!v && !s) return false;
+    row_sums(v ? (s ? 1 : 0) : 2);
+    if (v) {
+      amp_launch(amp_args(p_.vf, false), 0, 3, fobs_, nullptr, g_.NY2, 4, band_lo2(), band_hi2(), amp_ + 8);
+      rescale(0, 3, band_lo2(), band_hi2(), amp_ + 8);
+    }
+    if (s) {
+      amp_launch(amp_args(p_.sf, true), 3, 1, fobs_ + 2, nullptr, g_.NY2, 4, sband_lo2(), sband_hi2(), amp_ + 12);
+      rescale(3, 1, sband_lo2(), sband_hi2(), amp_ + 12);
+    }
+    return true;
   }
   const char* stage(const StageArgs& st) {
     const int ninv = p_.scalar ? 7 : 6;
@@ -806,9 +886,16 @@ class EngineImpl final : public Engine {
     bu_fresh_ = false;
     x_products();
     y_forward(nfwd);
-    if (st.forced) force_amp();
+    if (st.forced || st.sforced) force_amp(st);
     z_epilogue(st);
-    if (st.last) reality();
+    if (st.last) {
+      const bool rescaled = project();
+      reality();
+      // The last epilogue left the z-inverse of the unrescaled state in A; the deposit and the next
+      // stage read A, so it is rebuilt from the rescaled state. (The reality projection needs no
+      // rebuild: it changes only the anti-Hermitian part, which the real inverse does not see.)
+      if (rescaled) return z_init();
+    }
     return rt_check();
   }
   void run_tracers(int64_t M, int mode, double* X, double* F, HeunWeights w, const uint32_t* order = nullptr) {
@@ -867,7 +954,7 @@ class EngineImpl final : public Engine {
   std::vector<void*> allocs_;
   Cplx<T>*S_ = nullptr, *H_ = nullptr, *A_ = nullptr, *B_ = nullptr, *tw_ = nullptr;
   T* U_ = nullptr;
-  double *partial_ = nullptr, *amp_ = nullptr, *obs_ = nullptr, *spec_ = nullptr;
+  double *partial_ = nullptr, *amp_ = nullptr, *obs_ = nullptr, *fobs_ = nullptr, *spec_ = nullptr;
   double *X_ = nullptr, *F_ = nullptr;
   unsigned long long* maxbits_ = nullptr;
   unsigned int* status_ = nullptr;

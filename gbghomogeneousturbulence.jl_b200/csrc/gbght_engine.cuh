@@ -22,6 +22,20 @@
 
 namespace gbght {
 
+// One field's forcing (a copy of gbght_forcing_params, validated). kind: 0 none,
+// 1 ConstantPower, 2 Linear, 3 VarianceController, 4 VarianceRescaling.
+struct ForcingParams {
+  int kind;
+  double rate;            // ConstantPower ε, or Linear A
+  double target;          // VarianceController k∞, or VarianceRescaling target
+  double gain;            // VarianceController G
+  double turnover_time;   // VarianceController tℓ
+  int over;               // VarianceRescaling: 0 band, 1 total
+  int lowest_shell;
+  double highest_shell;
+};
+enum ForcingKind { kForceNone = 0, kForceConstantPower = 1, kForceLinear = 2, kForceController = 3, kForceRescaling = 4 };
+
 // The parameters of a run that the engine needs (a copy of the public config, validated).
 struct RunParams {
   int N;
@@ -30,15 +44,8 @@ struct RunParams {
   int scheme;
   double viscosity, schmidt;
   int scalar;
-  int forcing;               // velocity: gbght_forcing
-  double injection_rate;     // ConstantPower ε
-  int lowest_shell;          // velocity band
-  double highest_shell;
-  double linear_rate;        // velocity Linear A (0 unless Linear)
-  int scalar_forcing;        // scalar: NONE or LINEAR
-  double scalar_linear_rate; // scalar Linear A (0 unless Linear)
-  int scalar_lowest_shell;   // scalar band
-  double scalar_highest_shell;
+  ForcingParams vf;          // velocity forcing
+  ForcingParams sf;          // scalar forcing (kind 0 when the run carries no scalar)
   double G[3];
   int64_t tracers;
   int device;

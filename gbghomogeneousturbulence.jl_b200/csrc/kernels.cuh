@@ -166,23 +166,30 @@ template <class T>
 __global__ void k_reality(Geometry g, Cplx<T>* S, int ncomp) {
   reality_mode<T>(int(blockIdx.x * blockDim.x + threadIdx.x), g, S, ncomp);
 }
-// ConstantPower amplitude: the band sum and the whole-field sum of the tile partials, each in a
-// fixed order (strided per thread, then a fixed tree), so the amplitude is the same on every run.
+// A band forcing's amplitude (or rescale factor, see forcing_amplitude) for field slots
+// [c0, c0 + nc) of S. The whole-field sum adds whole[i·stride] (i < nwhole: the epilogue's tile
+// partials, or the observables rows), the Dirichlet sum dir[i·stride] likewise when dir is given;
+// the band sum runs over the box |m_a| ≤ mb. Each is summed per thread in a strided order and then
+// by a fixed tree, so the result is the same on every run. out[0..2] = (A, band, whole).
 template <class T>
-__global__ void k_force_amp(Geometry g, const Cplx<T>* S, const double* partial, int npartial, double lo2,
-                            double hi2, double eps_rate, double eps_T, double* amp, unsigned int* status) {
-  __shared__ double red[256], bred[256];
-  double s = 0.0;
-  for (int i = threadIdx.x; i < npartial; i += 256) s += partial[i];
+__global__ void k_force_amp(Geometry g, const Cplx<T>* S, int c0, int nc, const double* whole, const double* dir,
+                            int nwhole, int stride, double lo2, double hi2, AmpArgs a, double* out,
+                            unsigned int* status) {
+  __shared__ double red[256], bred[256], dred[256];
+  double s = 0.0, d = 0.0;
+  for (int i = threadIdx.x; i < nwhole; i += 256) {
+    s += whole[size_t(i) * stride];
+    if (dir) d += dir[size_t(i) * stride];
+  }
   red[threadIdx.x] = s;
-  // the band sum over the box |m_a| ≤ mb, split over the threads in a fixed assignment
+  dred[threadIdx.x] = d;
   int mb = int(sqrt(hi2) / g.s) + 1;
   if (mb > g.K) mb = g.K;
-  const int side = 2 * mb + 1, nbox = 3 * side * side * (mb + 1);
+  const int side = 2 * mb + 1, nbox = nc * side * side * (mb + 1);
   double b = 0.0;
   for (int i = threadIdx.x; i < nbox; i += 256) {
     const int kx = i % (mb + 1), mz = (i / (mb + 1)) % side - mb, my = (i / ((mb + 1) * side)) % side - mb;
-    const int cc = i / ((mb + 1) * side * side);
+    const int cc = c0 + i / ((mb + 1) * side * side);
     const double kxd = g.s * kx, kyd = g.s * my, kzd = g.s * mz;
     const double k2 = (kxd * kxd + kyd * kyd) + kzd * kzd;
     if (!(k2 >= lo2 && k2 <= hi2)) continue;
@@ -196,21 +203,34 @@ __global__ void k_force_amp(Geometry g, const Cplx<T>* S, const double* partial,
     if (threadIdx.x < w) {
       red[threadIdx.x] += red[threadIdx.x + w];
       bred[threadIdx.x] += bred[threadIdx.x + w];
+      dred[threadIdx.x] += dred[threadIdx.x + w];
     }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    const double whole = red[0];
-    const double band = bred[0];
     const double n6 = double(g.N) * g.N * g.N * double(g.N) * g.N * g.N;
-    const double band_obs = 0.5 * (band / n6), whole_obs = 0.5 * (whole / n6);
-    double A = 0.0;
-    if (isfinite(band_obs) && band_obs > 10.0 * eps_T * whole_obs) A = eps_rate / (2.0 * band_obs);
-    else atomicOr(status, 0x2u);
-    amp[0] = A;
-    amp[1] = band_obs;
-    amp[2] = whole_obs;
+    double band_obs, whole_obs;
+    bool empty;
+    const double A = forcing_amplitude(a, red[0], bred[0], dred[0], n6, &band_obs, &whole_obs, &empty);
+    if (empty) atomicOr(status, 0x2u);
+    out[0] = A;
+    out[1] = band_obs;
+    out[2] = whole_obs;
   }
+}
+
+// VarianceRescaling's post-step rescale of slots [c0, c0 + nc) over the box |m_a| ≤ mb
+// (grid-stride), by the factor in factor[0]. A factor of exactly 1 (an empty band) leaves the
+// field untouched.
+template <class T>
+__global__ void k_rescale(Geometry g, Cplx<T>* S, int c0, int nc, double lo2, double hi2, const double* factor) {
+  const double s = factor[0];
+  if (s == 1.0) return;
+  int mb = int(sqrt(hi2) / g.s) + 1;
+  if (mb > g.K) mb = g.K;
+  const long side = 2 * mb + 1, nbox = long(nc) * side * side * (mb + 1);
+  for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nbox; i += long(gridDim.x) * blockDim.x)
+    rescale_mode<T>(i, g, S, c0, mb, lo2, hi2, s);
 }
 template <class T, int NT>
 __global__ void __launch_bounds__(NT) k_observables(Geometry g, const Cplx<T>* S, int has_scalar, double* out) {

@@ -944,7 +944,8 @@ struct StageArgs {
   double cu, cphi;      // exponents c_i = −D·(d_i·dt) for velocity and scalar
   int first, last;      // stage 0, stage S−1
   int has_scalar;
-  int forced;           // velocity forcing active (ConstantPower)
+  int forced, sforced;  // a per-stage source A·𝟙_band·f on the velocity, on the scalar
+                        // (ConstantPower, VarianceController); A in force_amp[0], force_amp[4]
   double band_lo2, band_hi2;   // squared edges of the velocity forcing's band
   double lin_u, lin_phi;       // (d_i·dt)·A of a Linear forcing, velocity and scalar (0: none)
   double sband_lo2, sband_hi2; // squared edges of the scalar forcing's band
@@ -993,6 +994,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
       codes[n++] = 2;
     }
     forward3(3, codes, n);
+    const double A_s = st.sforced ? force_amp[4] : 0.0;
     OwnVals<T, O> x;
     const auto half = [&](auto hc) {
       constexpr int h = decltype(hc)::value;
@@ -1020,6 +1022,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
             const T G0 = T(st.G[0]), G1 = T(st.G[1]), G2 = T(st.G[2]);
             nphi = nphi - cmk<T>(G0 * ux.x + G1 * uy.x + G2 * uz.x, G0 * ux.y + G1 * uy.y + G2 * uz.y);
           }
+          if (A_s != 0.0 && k2 >= st.sband_lo2 && k2 <= st.sband_hi2) nphi = nphi + scale(phi, T(A_s));
           Cplx<T> hh = st.first ? scale(nphi, T(st.dt))
                                 : scale(sst.at(1, q, h, l), T(st.a)) + scale(nphi, T(st.dt));
           const double rphi = (k2 >= st.sband_lo2 && k2 <= st.sband_hi2) ? st.lin_phi : 0.0;
@@ -1172,12 +1175,13 @@ GBGHT_HD void reality_mode(int idx, const Geometry& g, Cplx<T>* S, int ncomp) {
 // a fixed order by one thread; the whole-field sum adds the per-tile partials in a fixed order.
 // ================================================================================================
 template <class T>
-GBGHT_HD double band_energy_raw(const Geometry& g, const Cplx<T>* S, double lo2, double hi2) {
-  // Hermitian-weighted Σ|û|² over the band, unnormalised; m_a bounded by the band edge
+GBGHT_HD double band_energy_raw(const Geometry& g, const Cplx<T>* S, double lo2, double hi2, int c0 = 0, int nc = 3) {
+  // Hermitian-weighted Σ|f̂|² of slots [c0, c0 + nc) over the band, unnormalised; m_a bounded by
+  // the band edge
   int mb = int(std::sqrt(hi2) / g.s) + 1;
   if (mb > g.K) mb = g.K;
   double sum = 0.0;
-  for (int cc = 0; cc < 3; ++cc)
+  for (int cc = c0; cc < c0 + nc; ++cc)
     for (int my = -mb; my <= mb; ++my)
       for (int mz = -mb; mz <= mb; ++mz)
         for (int kx = 0; kx <= mb; ++kx) {
@@ -1192,6 +1196,65 @@ GBGHT_HD double band_energy_raw(const Geometry& g, const Cplx<T>* S, double lo2,
   return sum;
 }
 
+// ================================================================================================
+// The number a band forcing solves for from a field's raw, unnormalised sums (whole Σw|f̂|², band
+// Σ_band w|f̂|², Dirichlet Σw|κ|²|f̂|², each divided by N⁶ to give the mean over the box):
+//  - ConstantPower: A = ε/(2 k_band) (src/Forcing.jl:1091-1117);
+//  - VarianceController: A = (ε_f − G(k − k∞)/tℓ)/(2 k_band), ε_f = 2·c·D·⟨f, |κ|²f⟩
+//    (src/Forcing.jl:1041-1067);
+//  - VarianceRescaling: the factor √(target_band/k_band) of the post-step rescale, target_band the
+//    target (:band) or max(0, target − k + k_band) (:total) (src/Forcing.jl:575-596).
+// c is ½ for the velocity and 1 for the scalar (`_target_factor`, :456). An empty band — not above
+// 10·eps·whole (`_band_is_empty`, :110-111) — gives A = 0, or the factor 1 (the band left alone),
+// and raises *empty.
+// ================================================================================================
+struct AmpArgs {
+  int kind;              // ForcingKind
+  double rate;           // ConstantPower ε
+  double target, gain, turnover_time;
+  int over;              // VarianceRescaling: 0 band, 1 total
+  double factor;         // ½ velocity, 1 scalar
+  double diffusivity;    // ν or ν/Sc
+  double eps_T;          // the field precision's machine epsilon
+};
+
+GBGHT_HD double forcing_amplitude(const AmpArgs& a, double whole_raw, double band_raw, double dir_raw,
+                                  double n6, double* band_obs, double* whole_obs, bool* empty) {
+  const double band = a.factor * (band_raw / n6), whole = a.factor * (whole_raw / n6);
+  *band_obs = band;
+  *whole_obs = whole;
+  if (a.kind == 4) {   // VarianceRescaling: the emptiness test on the raw sums, as the reference
+    *empty = !(std::isfinite(band_raw) && band_raw > 10.0 * a.eps_T * whole_raw);
+    if (*empty) return 1.0;
+    const double target_band = a.over == 1 ? std::fmax(0.0, a.target - whole + band) : a.target;
+    return std::sqrt(target_band / band);
+  }
+  *empty = !(std::isfinite(band) && band > 10.0 * a.eps_T * whole);
+  if (*empty) return 0.0;
+  if (a.kind == 3) {   // VarianceController
+    const double dissipation = 2.0 * a.factor * a.diffusivity * (dir_raw / n6);
+    const double restoring = a.gain * (whole - a.target) / a.turnover_time;
+    return (dissipation - restoring) / (2.0 * band);
+  }
+  return a.rate / (2.0 * band);   // ConstantPower
+}
+
+// VarianceRescaling's rescale of one mode of the box |m_a| ≤ mb over slots c0..: i enumerates
+// (slot, my, mz, kx) with kx fastest; a mode in the band becomes f + (s − 1)·f, the reference's
+// convolve!(f, f, band, s − 1, 1) (src/Forcing.jl:595).
+template <class T>
+GBGHT_HD void rescale_mode(long i, const Geometry& g, Cplx<T>* S, int c0, int mb, double lo2, double hi2,
+                           double factor) {
+  const int side = 2 * mb + 1;
+  const int kx = int(i % (mb + 1)), mz = int((i / (mb + 1)) % side) - mb, my = int((i / ((mb + 1) * side)) % side) - mb;
+  const int cc = c0 + int(i / (long(mb + 1) * side * side));
+  const double kxd = g.s * kx, kyd = g.s * my, kzd = g.s * mz;
+  const double k2 = (kxd * kxd + kyd * kyd) + kzd * kzd;
+  if (!(k2 >= lo2 && k2 <= hi2)) return;
+  const int qy = my >= 0 ? my : my + g.NY2, qz = mz >= 0 ? mz : mz + g.NY2;
+  Cplx<T>& v = S[idxS(g, cc, qy, qz, kx)];
+  v = v + scale(v, T(factor - 1.0));
+}
 // ================================================================================================
 // z-inverse of the current state into A slots 0..6 (u, iκ×û, φ), and the tile's Hermitian-weighted
 // Σ|û|², with the same tiling as the epilogue. Used after an import to start a step.

@@ -24,7 +24,8 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "libgbght.so")
 
 FP64, FP32_MIXED = 0, 1
 IFRK4, IFRK3 = 0, 1
-FORCING_NONE, FORCING_CONSTANT_POWER, FORCING_LINEAR = 0, 1, 2
+FORCING_NONE, FORCING_CONSTANT_POWER, FORCING_LINEAR, FORCING_VARIANCE_CONTROLLER, FORCING_VARIANCE_RESCALING = 0, 1, 2, 3, 4
+OVER = {"band": 0, "total": 1}
 OK, ERR_ARGUMENT, ERR_SCHEDULE, ERR_CUDA, ERR_DEVICE = 0, 1, 2, 3, 4
 
 
@@ -36,6 +37,19 @@ class DeviceError(RuntimeError):
     """A CUDA runtime error or a raised device status bit."""
 
 
+class ForcingParams(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int),
+        ("rate", C.c_double),
+        ("target", C.c_double),
+        ("gain", C.c_double),
+        ("turnover_time", C.c_double),
+        ("over", C.c_int),
+        ("lowest_shell", C.c_int),
+        ("highest_shell", C.c_double),
+    ]
+
+
 class Config(C.Structure):
     _fields_ = [
         ("grid_points_per_axis", C.c_int),
@@ -45,20 +59,13 @@ class Config(C.Structure):
         ("viscosity", C.c_double),
         ("schmidt", C.c_double),
         ("scalar", C.c_int),
-        ("velocity_forcing", C.c_int),
-        ("injection_rate", C.c_double),
-        ("lowest_shell", C.c_int),
-        ("highest_shell", C.c_double),
+        ("velocity_forcing", ForcingParams),
+        ("scalar_forcing", ForcingParams),
         ("mean_gradient", C.c_double * 3),
         ("tracers", C.c_int64),
         ("cfl", C.c_double),
         ("max_dt", C.c_double),
         ("device", C.c_int),
-        ("linear_rate", C.c_double),
-        ("scalar_forcing", C.c_int),
-        ("scalar_linear_rate", C.c_double),
-        ("scalar_lowest_shell", C.c_int),
-        ("scalar_highest_shell", C.c_double),
     ]
 
 
@@ -144,8 +151,52 @@ class Linear:
 
 
 @dataclass
+class VarianceController:
+    """`VarianceController(domain; target, gain = 1, turnover_time, lowest_shell = 1,
+    highest_shell = 2)` (src/Forcing.jl:828-875). The turnover time tℓ is given explicitly: the
+    reference derives a default from its stationary-state model, which this backend does not carry."""
+    target: float
+    turnover_time: float
+    gain: float = 1.0
+    lowest_shell: int = 1
+    highest_shell: float = 2
+
+
+@dataclass
+class VarianceRescaling:
+    """`VarianceRescaling(domain; target, over, lowest_shell = 1, highest_shell = 2)`
+    (src/Forcing.jl:558-572), `over` "band" or "total"."""
+    target: float
+    over: str
+    lowest_shell: int = 1
+    highest_shell: float = 2
+
+
+@dataclass
 class NoForcing:
     """`NoForcing()` (src/Forcing.jl): a freely decaying field."""
+
+
+def _fill_forcing(p: ForcingParams, f, who: str) -> None:
+    """Write one field's forcing object into its gbght_forcing_params block (defaults already set)."""
+    if f is None or isinstance(f, NoForcing):
+        p.kind = FORCING_NONE
+        return
+    if isinstance(f, ConstantPower):
+        p.kind, p.rate = FORCING_CONSTANT_POWER, float(f.injection_rate)
+    elif isinstance(f, Linear):
+        p.kind, p.rate = FORCING_LINEAR, float(f.rate)
+    elif isinstance(f, VarianceController):
+        p.kind, p.target, p.gain, p.turnover_time = (FORCING_VARIANCE_CONTROLLER, float(f.target), float(f.gain),
+                                                      float(f.turnover_time))
+    elif isinstance(f, VarianceRescaling):
+        if f.over not in OVER:
+            raise ValueError(f"VarianceRescaling `over` must be :band or :total; got :{f.over}")
+        p.kind, p.target, p.over = FORCING_VARIANCE_RESCALING, float(f.target), OVER[f.over]
+    else:
+        raise ValueError(f"unsupported {who} forcing {f!r}")
+    p.lowest_shell = int(f.lowest_shell)
+    p.highest_shell = float(f.highest_shell)
 
 
 @dataclass
@@ -183,31 +234,8 @@ class Run:
         cfg.viscosity = float(setup.viscosity)
         cfg.schmidt = float(setup.schmidt)
         cfg.scalar = 1 if setup.scalar else 0
-        f = setup.velocity_forcing
-        if isinstance(f, ConstantPower):
-            cfg.velocity_forcing = FORCING_CONSTANT_POWER
-            cfg.injection_rate = float(f.injection_rate)
-            cfg.lowest_shell = int(f.lowest_shell)
-            cfg.highest_shell = float(f.highest_shell)
-        elif isinstance(f, Linear):
-            cfg.velocity_forcing = FORCING_LINEAR
-            cfg.linear_rate = float(f.rate)
-            cfg.lowest_shell = int(f.lowest_shell)
-            cfg.highest_shell = float(f.highest_shell)
-        elif f is None or isinstance(f, NoForcing):
-            cfg.velocity_forcing = FORCING_NONE
-        else:
-            raise ValueError(f"unsupported velocity forcing {f!r}")
-        f = setup.scalar_forcing
-        if isinstance(f, Linear):
-            cfg.scalar_forcing = FORCING_LINEAR
-            cfg.scalar_linear_rate = float(f.rate)
-            cfg.scalar_lowest_shell = int(f.lowest_shell)
-            cfg.scalar_highest_shell = float(f.highest_shell)
-        elif f is None or isinstance(f, NoForcing):
-            cfg.scalar_forcing = FORCING_NONE
-        else:
-            raise ValueError(f"unsupported scalar forcing {f!r}: the scalar takes NoForcing or Linear")
+        _fill_forcing(cfg.velocity_forcing, setup.velocity_forcing, "velocity")
+        _fill_forcing(cfg.scalar_forcing, setup.scalar_forcing, "scalar")
         for i in range(3):
             cfg.mean_gradient[i] = float(setup.mean_gradient[i])
         cfg.tracers = int(setup.tracers)

@@ -42,10 +42,41 @@ enum gbght_status {
 
 enum gbght_precision { GBGHT_FP64 = 0, GBGHT_FP32_MIXED = 1 };
 enum gbght_scheme { GBGHT_IFRK4 = 0, GBGHT_IFRK3 = 1 };
-/* NONE: NoForcing. CONSTANT_POWER: ConstantPower, velocity only (src/Forcing.jl:1069-1117).
- * LINEAR: Linear, a steady rate A on the band folded into the integrating factor,
- * exp((A(κ) − D|κ|²)·δt) (src/Forcing.jl:636-653, src/Generator.jl:565-581). */
-enum gbght_forcing { GBGHT_FORCING_NONE = 0, GBGHT_FORCING_CONSTANT_POWER = 1, GBGHT_FORCING_LINEAR = 2 };
+/* The forcing strategies (src/Forcing.jl), for either field:
+ *  NONE                 NoForcing.
+ *  CONSTANT_POWER       ConstantPower (:1069-1117): A = ε/(2 k_band) re-solved at every stage, a
+ *                       per-stage source A·𝟙_band·f.
+ *  LINEAR               Linear (:636-653): a steady rate A on the band, folded into the
+ *                       integrating factor exp((A(κ) − D|κ|²)·δt) (src/Generator.jl:565-581).
+ *  VARIANCE_CONTROLLER  VarianceController (:1041-1067): A = (ε − G(k − k∞)/tℓ)/(2 k_band) at
+ *                       every stage, with k and ε the field's whole variance and dissipation.
+ *  VARIANCE_RESCALING   VarianceRescaling (:575-596): after the step, the band is rescaled by one
+ *                       factor so the band's (`over` = 0) or the whole field's (`over` = 1)
+ *                       variance equals `target`. First order in time, as in the reference.
+ * The variance is ½⟨|u|²⟩ for the velocity and ⟨φ²⟩ for the scalar (src/Forcing.jl:456). */
+enum gbght_forcing {
+  GBGHT_FORCING_NONE = 0,
+  GBGHT_FORCING_CONSTANT_POWER = 1,
+  GBGHT_FORCING_LINEAR = 2,
+  GBGHT_FORCING_VARIANCE_CONTROLLER = 3,
+  GBGHT_FORCING_VARIANCE_RESCALING = 4
+};
+enum gbght_rescaling_over { GBGHT_OVER_BAND = 0, GBGHT_OVER_TOTAL = 1 };
+
+/* One field's forcing: the kind and the parameters that kind reads. The band is the shells
+ * lowest..highest, shell h covering [h − ½, h + ½)·2π/L; highest is an integer shell or INFINITY
+ * (every mode but the mean). */
+typedef struct gbght_forcing_params {
+  int kind;               /* gbght_forcing */
+  double rate;            /* ConstantPower injection_rate ε, or Linear rate A */
+  double target;          /* VarianceController k∞ (> 0), or VarianceRescaling target (≥ 0) */
+  double gain;            /* VarianceController gain G ≥ 0 */
+  double turnover_time;   /* VarianceController tℓ > 0, given explicitly */
+  int over;               /* VarianceRescaling: gbght_rescaling_over */
+  int lowest_shell;       /* ≥ 1 */
+  double highest_shell;   /* ≥ lowest_shell */
+} gbght_forcing_params;
+
 enum gbght_tracer_scheme { GBGHT_HEUN = 0 };
 
 /* Device status bits (gbght_status_word). */
@@ -61,33 +92,24 @@ typedef struct gbght_config {
   double viscosity;          /* ν > 0 */
   double schmidt;            /* Sc > 0; scalar diffusivity ν/Sc */
   int scalar;                /* 1: carry the passive scalar */
-  int velocity_forcing;      /* gbght_forcing */
-  double injection_rate;     /* ConstantPower ε */
-  int lowest_shell;          /* velocity forcing band, shells [lowest − ½, highest + ½]·2π/L; */
-  double highest_shell;      /* an integer shell, or INFINITY: every mode but the mean */
+  gbght_forcing_params velocity_forcing;   /* any kind */
+  gbght_forcing_params scalar_forcing;     /* any kind; needs scalar = 1 unless NONE */
   double mean_gradient[3];   /* uniform mean scalar gradient G (extension; 0 = none) */
   int64_t tracers;           /* M ≥ 0 tracers */
   double cfl;                /* C of the advective CFL rule */
   double max_dt;             /* caller's ceiling on Δt (INFINITY = none) */
   int device;                /* CUDA device ordinal */
-  /* Appended after `device`, so a caller that fills the struct through gbght_config_default keeps
-   * its layout for the fields above. */
-  double linear_rate;        /* velocity Linear A (velocity_forcing == GBGHT_FORCING_LINEAR) */
-  int scalar_forcing;        /* gbght_forcing for the scalar: NONE or LINEAR; needs scalar = 1 */
-  double scalar_linear_rate; /* scalar Linear A */
-  int scalar_lowest_shell;   /* scalar Linear band, as lowest_shell / highest_shell */
-  double scalar_highest_shell;
 } gbght_config;
 
 /* Fill `cfg` with the defaults: N=64, L=2π, FP64, IF-RK4, ν=0.01, Sc=1, scalar on, no forcing
- * of either field, shells 1–2 for both bands, rates 0, G=0, no tracers, CFL 0.5, max_dt=∞,
- * device 0. */
+ * of either field (each forcing block: rate 0, target 0, gain 1, turnover time 0, over = band,
+ * shells 1–2), G=0, no tracers, CFL 0.5, max_dt=∞, device 0. */
 void gbght_config_default(gbght_config* cfg);
 
 /* Build a run on a FixedDomain with TwoThirds dealiasing, with its generator and registers.
  * Replaces FixedDomain(...) (src/SimulationDomain.jl:295-328), FlowConditions
- * (src/Generator.jl:81-140), ConstantPower (src/Forcing.jl:1069-1075), Linear
- * (src/Forcing.jl:636-643) for either field, allocate_buffers
+ * (src/Generator.jl:81-140), the forcings of either field (ConstantPower src/Forcing.jl:1069-1075,
+ * Linear :636-643, VarianceController :828-875, VarianceRescaling :558-572), allocate_buffers
  * (src/Propagator.jl:717-723) and ObservablesCache (src/Cache.jl:150-173). The state starts at
  * zero. */
 int gbght_create(gbght_run** out, const gbght_config* cfg);

@@ -6,7 +6,8 @@ No product path calls it, and nothing in the library falls back to it.
 
 It restates, in FP64 NumPy with ``scipy.fft``, the algorithm of the reference's hot path: the
 coupled velocity + passive-scalar integrating-factor low-storage Runge–Kutta step with 2/3-rule
-dealiasing, Leray projection, ConstantPower and Linear band forcing, and Heun (ABM(1)) tracer advection with
+dealiasing, Leray projection, the band forcings (ConstantPower, Linear, VarianceController,
+VarianceRescaling) on either field, and Heun (ABM(1)) tracer advection with
 Catmull–Rom interpolation. Every array is kept in the reference's own layout. That layout is the
 column-major ``(kx, ky, kz, comp)`` array of the rfft, held here row-major as ``[comp][kz][ky][kx]``
 with ``kx`` in ``[0, N/2]``. It is full-size and unpruned, so the oracle shares no layout or pruning
@@ -23,6 +24,8 @@ reference's own known-answer tests, re-expressed in ``tests/test_oracle_known_an
 - exact diffusion;
 - the RK3 and RK4 self-convergence ratios, and the order under ConstantPower;
 - the Linear rate's exact growth of a single mode, and the Linear scalar's variance growth;
+- VarianceController's amplitude, its scalar dissipation, the marginal law at gain 0 and the
+  order kept; VarianceRescaling's uniform rescale on an unbounded band and its first order;
 - injected power equal to ε, and a solenoidal state;
 - the 2/3 closed ball against a 2N zero-padded product;
 - Parseval, and the planted reality violation;
@@ -179,13 +182,35 @@ class Linear:
 
 
 @dataclass
+class VarianceController:
+    """`VarianceController(domain; target, gain = 1, turnover_time, lowest_shell, highest_shell)`
+    (src/Forcing.jl:828-875), with tℓ given explicitly; the amplitude is re-solved at every stage
+    (`add_forcing_source!(::VarianceController)` :1041-1067)."""
+    target: float
+    turnover_time: float
+    gain: float = 1.0
+    lowest_shell: int = 1
+    highest_shell: float = 2
+
+
+@dataclass
+class VarianceRescaling:
+    """`VarianceRescaling(domain; target, over, lowest_shell, highest_shell)` (src/Forcing.jl:558-572):
+    a post-step rescale of the band (`project_forcing!` :575-596)."""
+    target: float
+    over: str                                # "band" or "total"
+    lowest_shell: int = 1
+    highest_shell: float = 2
+
+
+@dataclass
 class Conditions:
     viscosity: float
     schmidt: float = 1.0
-    velocity_forcing: object = None          # None (NoForcing), ConstantPower or Linear
+    velocity_forcing: object = None          # None (NoForcing), or one of the forcing classes above
     scalar: bool = True
     mean_gradient: tuple = (0.0, 0.0, 0.0)   # extension G1: uniform mean scalar gradient G
-    scalar_forcing: object = None            # None (NoForcing) or Linear
+    scalar_forcing: object = None            # likewise, for the scalar
 
     def __post_init__(self):
         if not self.viscosity > 0:
@@ -211,18 +236,63 @@ def band_indicator(dom: Domain, forcing) -> np.ndarray:
     return ((dom.k2 >= lo * lo) & (dom.k2 <= hi * hi)).astype(np.float64)
 
 
-def constant_power_amplitude(dom: Domain, forcing: ConstantPower, uh: np.ndarray, eps_T: float):
-    """A = ε / (2 k_band), clamped to 0 when the band is empty relative to the whole field
-    (`add_forcing_source!(::ConstantPower)` src/Forcing.jl:1104-1117, `_injection_amplitude`
-    :1091-1101, `_band_is_empty` :110-111, `_target_factor` :456 with ½ for the velocity)."""
+def target_factor(field: np.ndarray) -> float:
+    """½ for the velocity (kinetic energy), 1 for the scalar (variance) (`_target_factor`,
+    src/Forcing.jl:456)."""
+    return 0.5 if field.ndim == 4 else 1.0
+
+
+def band_is_empty(band_value: float, whole_value: float, eps_T: float) -> bool:
+    """`_band_is_empty` (src/Forcing.jl:110-111)."""
+    return not (math.isfinite(band_value) and band_value > 10 * eps_T * whole_value)
+
+
+def constant_power_amplitude(dom: Domain, forcing, fh: np.ndarray, eps_T: float, diffusivity: float = 0.0):
+    """The per-stage amplitude A of a band source A·𝟙_band·f at the stage field f, with the band.
+    ConstantPower: A = ε/(2 k_band) (`add_forcing_source!(::ConstantPower)` src/Forcing.jl:1104-1117,
+    `_injection_amplitude` :1091-1101). VarianceController: A = (ε_f − G(k − k∞)/tℓ)/(2 k_band), with
+    k the whole field's variance and ε_f = 2·c·D·⟨f, |κ|²f⟩ its dissipation (:1041-1067). c is the
+    target factor; an empty band gives A = 0."""
+    c = target_factor(fh)
     band = band_indicator(dom, forcing)
-    band_raw = dom.inner(uh, uh, band)
-    whole_raw = dom.inner(uh, uh)
-    band_obs = 0.5 * band_raw
-    whole_obs = 0.5 * whole_raw
-    if not (math.isfinite(band_obs) and band_obs > 10 * eps_T * whole_obs):
+    band_obs = c * dom.inner(fh, fh, band)
+    whole_obs = c * dom.inner(fh, fh)
+    if band_is_empty(band_obs, whole_obs, eps_T):
         return 0.0, band
+    if isinstance(forcing, VarianceController):
+        dissipation = 2 * c * diffusivity * dom.inner(fh, fh, dom.k2)
+        restoring = forcing.gain * (whole_obs - forcing.target) / forcing.turnover_time
+        return (dissipation - restoring) / (2 * band_obs), band
     return forcing.injection_rate / (2 * band_obs), band
+
+
+def stage_source(dom: Domain, forcing, fh: np.ndarray, eps_T: float, diffusivity: float):
+    """The additive source of a per-stage forcing (ConstantPower, VarianceController), else None."""
+    if isinstance(forcing, (ConstantPower, VarianceController)):
+        A, band = constant_power_amplitude(dom, forcing, fh, eps_T, diffusivity)
+        return A * band * fh
+    return None
+
+
+def project_forcing(dom: Domain, forcing, fh: np.ndarray, eps_T: float) -> np.ndarray:
+    """VarianceRescaling's post-step rescale (`project_forcing!` src/Forcing.jl:575-596): the band
+    takes one factor √(target_band/k_band) so the band (:band) or the whole field (:total) holds
+    the target; an empty band is left alone. Other forcings project nothing."""
+    if not isinstance(forcing, VarianceRescaling):
+        return fh
+    c = target_factor(fh)
+    band = band_indicator(dom, forcing)
+    band_raw = dom.inner(fh, fh, band)
+    whole_raw = dom.inner(fh, fh)
+    band_value = c * band_raw
+    if band_is_empty(band_raw, whole_raw, eps_T):
+        return fh
+    if forcing.over == "total":
+        target_band = max(0.0, forcing.target - c * whole_raw + band_value)
+    else:
+        target_band = forcing.target
+    scale = math.sqrt(target_band / band_value)
+    return fh + (scale - 1) * band * fh
 
 
 def velocity_rhs(dom: Domain, cond: Conditions, uh, u, w, eps_T):
@@ -235,14 +305,13 @@ def velocity_rhs(dom: Domain, cond: Conditions, uh, u, w, eps_T):
     nh = dom.to_spectral(lamb_neg)
     nh = leray(dom, nh, dom.mask)
     nh[:, 0, 0, 0] = 0.0
-    f = cond.velocity_forcing
-    if isinstance(f, ConstantPower):
-        A, band = constant_power_amplitude(dom, f, uh, eps_T)
-        nh = nh + A * band * uh
+    src = stage_source(dom, cond.velocity_forcing, uh, eps_T, cond.viscosity)
+    if src is not None:
+        nh = nh + src
     return nh
 
 
-def scalar_rhs(dom: Domain, cond: Conditions, uh, u, phi):
+def scalar_rhs(dom: Domain, cond: Conditions, uh, u, phi, ph=None, eps_T: float = np.finfo(np.float64).eps):
     """N̂_φ = −𝔻 iκ·FFT(uφ) (`_scalar_flux_divergence!`, src/Generator.jl:708-720, divergence
     with α = −1), plus the mean-gradient source −G·û (extension G1: φ_total = G·x + φ, so
     ∂tφ + u·∇φ = −u·G + ϰ∇²φ)."""
@@ -253,6 +322,11 @@ def scalar_rhs(dom: Domain, cond: Conditions, uh, u, phi):
     G = cond.mean_gradient
     if any(g != 0.0 for g in G):
         nh = nh - ((G[0] * uh[0] + G[1] * uh[1]) + G[2] * uh[2])
+    if ph is not None:
+        # the scalar forcing's source at the stage φ̂ (`scalar_rhs!` src/Generator.jl:650-653)
+        src = stage_source(dom, cond.scalar_forcing, ph, eps_T, cond.diffusivity)
+        if src is not None:
+            nh = nh + src
     return nh
 
 
@@ -325,7 +399,7 @@ def step(dom: Domain, cond: Conditions, st: State, dt: float, scheme: str = "rk4
         nu_ = velocity_rhs(dom, cond, uh, u, w, eps_T)
         if has_scalar:
             phi = dom.to_physical(ph)
-            np_ = scalar_rhs(dom, cond, uh, u, phi)
+            np_ = scalar_rhs(dom, cond, uh, u, phi, ph, eps_T)
         hu = dt * nu_ if i == 0 else a[i] * hu + dt * nu_
         E = integrating_factor(dom, cond.viscosity, rate_u, d[i] * dt)
         uh = E * (uh + b[i] * hu)
@@ -337,6 +411,10 @@ def step(dom: Domain, cond: Conditions, st: State, dt: float, scheme: str = "rk4
             ph = Ep * (ph + b[i] * hp)
             if i < len(a) - 1:
                 hp = Ep * hp
+    # post-step forcing projections, velocity first (`finalize!` src/Generator.jl:396-400)
+    uh = project_forcing(dom, cond.velocity_forcing, uh, eps_T)
+    if has_scalar:
+        ph = project_forcing(dom, cond.scalar_forcing, ph, eps_T)
     uh = leray(dom, uh)
     uh = reality_projection(dom, uh)
     if has_scalar:

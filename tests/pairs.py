@@ -25,6 +25,10 @@ def oracle_forcing(f):
         return O.ConstantPower(f.injection_rate, f.lowest_shell, f.highest_shell)
     if isinstance(f, gbght.Linear):
         return O.Linear(f.rate, f.lowest_shell, f.highest_shell)
+    if isinstance(f, gbght.VarianceController):
+        return O.VarianceController(f.target, f.turnover_time, f.gain, f.lowest_shell, f.highest_shell)
+    if isinstance(f, gbght.VarianceRescaling):
+        return O.VarianceRescaling(f.target, f.over, f.lowest_shell, f.highest_shell)
     raise ValueError(f"no oracle forcing for {f!r}")
 
 

@@ -33,7 +33,7 @@ def test_library_reports_its_version(cuda_library):
 
 def test_config_layout_matches_the_header(cuda_library):
     # gbght_config_default fills the ctypes mirror of gbght_config: every default lands in its
-    # own field, so the mirror's offsets agree with the C struct, the appended fields included.
+    # own field, so the mirror's offsets agree with the C struct, the forcing blocks included.
     import math
     import gbght
     lib = gbght.load_library(cuda_library)
@@ -41,7 +41,8 @@ def test_config_layout_matches_the_header(cuda_library):
     lib.gbght_config_default(ctypes.byref(cfg))
     assert (cfg.grid_points_per_axis, cfg.precision, cfg.scheme, cfg.scalar) == (64, 0, 0, 1)
     assert cfg.side_length == 2 * math.pi and cfg.viscosity == 0.01 and cfg.schmidt == 1.0
-    assert (cfg.velocity_forcing, cfg.lowest_shell, cfg.highest_shell) == (0, 1, 2.0)
+    for f in (cfg.velocity_forcing, cfg.scalar_forcing):
+        assert (f.kind, f.rate, f.target, f.gain, f.turnover_time, f.over) == (0, 0.0, 0.0, 1.0, 0.0, 0)
+        assert (f.lowest_shell, f.highest_shell) == (1, 2.0)
+    assert tuple(cfg.mean_gradient) == (0.0, 0.0, 0.0) and cfg.tracers == 0
     assert cfg.cfl == 0.5 and cfg.max_dt == math.inf and cfg.device == 0
-    assert (cfg.linear_rate, cfg.scalar_forcing, cfg.scalar_linear_rate) == (0.0, 0, 0.0)
-    assert (cfg.scalar_lowest_shell, cfg.scalar_highest_shell) == (1, 2.0)

@@ -82,6 +82,40 @@ def test_linear_forcing_both_fields(cuda_library, N, precision, steps):
         compare(run, orun, tol=1e-5, check_tracers=False)
 
 
+BAND_FORCINGS = {
+    "controller_u+cp_phi": (gbght.VarianceController(0.4, turnover_time=0.5, gain=2.0), gbght.ConstantPower(0.2)),
+    "cp_u+controller_phi": (gbght.ConstantPower(0.1),
+                            gbght.VarianceController(0.3, turnover_time=0.5, gain=1.0, highest_shell=3)),
+    "rescale_total_u+band_phi": (gbght.VarianceRescaling(0.45, "total"), gbght.VarianceRescaling(0.2, "band", 1, math.inf)),
+}
+
+
+@pytest.mark.parametrize("name", list(BAND_FORCINGS))
+@pytest.mark.parametrize("N,precision,steps", [(64, "fp64", 10), (256, "fp64", 1), (64, "fp32_mixed", 5)])
+def test_band_forcings_both_fields(cuda_library, name, N, precision, steps):
+    # per-stage amplitudes (ConstantPower, VarianceController) and the post-step rescale
+    # (VarianceRescaling) on each field, with the mean gradient and the tracers
+    vf, sf = BAND_FORCINGS[name]
+    run, orun = make_case(N, viscosity=0.005, forcing=vf, scalar_forcing=sf, G=(1.0, 0.0, 0.0), tracers=1000,
+                          precision=precision, library=cuda_library)
+    advance_both(run, orun, steps, dt=0.004)
+    if precision == "fp64":
+        res = compare(run, orun, tol=1e-12)
+        assert res["X_err"] < 1e-10
+    else:
+        compare(run, orun, tol=1e-5, check_tracers=False)
+
+
+def test_rescaling_holds_the_target_exactly(cuda_library):
+    run, _ = make_case(64, forcing=gbght.VarianceRescaling(0.45, "total"),
+                       scalar_forcing=gbght.VarianceRescaling(0.6, "total", 1, math.inf), library=cuda_library)
+    for _ in range(3):
+        run.advance(0.005)
+        ob = run.observables()
+        assert ob["kinetic_energy"] == pytest.approx(0.45, rel=1e-13)
+        assert ob["scalar_variance"] == pytest.approx(0.6, rel=1e-13)
+
+
 def test_scalar_linear_exact_growth_with_zero_velocity(cuda_library):
     # test/forcing.jl:124-139 held to the closed form φ̂(T) = exp((A·band − ϰ|κ|²)T) φ̂(0)
     N, nu, Sc, A = 32, 0.05, 1.0, 1.0

@@ -41,8 +41,29 @@ def test_bad_forcing_bands_are_argument_errors(hostcheck_library):
         run(velocity_forcing=gbght.ConstantPower(0.1, lowest_shell=0))
     with pytest.raises(ValueError, match="carries no scalar"):
         run(scalar=False, scalar_forcing=gbght.Linear(1.0))
-    with pytest.raises(ValueError, match="scalar takes NoForcing or Linear"):
-        run(scalar_forcing=gbght.ConstantPower(0.1))
+
+
+def test_bad_controller_and_rescaling_are_argument_errors(hostcheck_library):
+    # src/Forcing.jl:558-572 (VarianceRescaling) and :828-875 (VarianceController)
+    def run(**kw):
+        return gbght.Run(gbght.Setup(grid_points_per_axis=16, **kw), library=hostcheck_library)
+    for field in ("velocity_forcing", "scalar_forcing"):
+        with pytest.raises(ValueError, match="`target` must be finite and positive"):
+            run(**{field: gbght.VarianceController(0.0, turnover_time=1.0)})
+        with pytest.raises(ValueError, match="`gain` must be finite and non-negative"):
+            run(**{field: gbght.VarianceController(1.5, turnover_time=1.0, gain=-1.0)})
+        with pytest.raises(ValueError, match="`gain` must be finite and non-negative"):
+            run(**{field: gbght.VarianceController(1.5, turnover_time=1.0, gain=math.inf)})
+        with pytest.raises(ValueError, match="`turnover_time` must be finite and positive"):
+            run(**{field: gbght.VarianceController(1.5, turnover_time=0.0)})
+        run(**{field: gbght.VarianceController(1.5, turnover_time=1.0, gain=0.0)}).close()   # the marginal law
+        with pytest.raises(ValueError, match="`target` must be finite and non-negative"):
+            run(**{field: gbght.VarianceRescaling(-1.0, "band")})
+        with pytest.raises(ValueError, match="`over` must be :band or :total"):
+            run(**{field: gbght.VarianceRescaling(1.0, "shell")})
+        with pytest.raises(ValueError, match="lowest_shell"):
+            run(**{field: gbght.VarianceRescaling(1.0, "total", lowest_shell=0)})
+        run(**{field: gbght.VarianceRescaling(0.0, "total", highest_shell=math.inf)}).close()
 
 
 def test_state_outside_the_retained_ball_is_refused(hostcheck_library):

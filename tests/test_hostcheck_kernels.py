@@ -40,6 +40,31 @@ def test_linear_forcing_both_fields_matches_oracle(hostcheck_library, scheme):
     assert res["X_err"] < 1e-13
 
 
+@pytest.mark.parametrize("vf,sf", [
+    (gbght.VarianceController(0.4, turnover_time=0.5, gain=2.0), gbght.ConstantPower(0.2)),
+    (gbght.ConstantPower(0.1), gbght.VarianceController(0.3, turnover_time=0.5, gain=1.0, highest_shell=3)),
+    (gbght.VarianceRescaling(0.45, "total"), gbght.VarianceRescaling(0.2, "band", 1, math.inf)),
+    (gbght.VarianceRescaling(0.3, "band", 2, 3), gbght.VarianceRescaling(0.6, "total")),
+], ids=["controller_u+cp_phi", "cp_u+controller_phi", "rescale_total_u+band_phi", "rescale_band_u+total_phi"])
+def test_band_forcings_both_fields_match_oracle(hostcheck_library, vf, sf):
+    # the per-stage amplitudes (ConstantPower, VarianceController) and the post-step rescale
+    # (VarianceRescaling) on each field, with the mean gradient and the tracers
+    run, orun = make_case(16, forcing=vf, scalar_forcing=sf, G=(1.0, 0.0, 0.0), tracers=16, library=hostcheck_library)
+    advance_both(run, orun, 4, dt=0.01)
+    res = compare(run, orun, tol=2e-14)
+    assert res["X_err"] < 1e-13
+
+
+def test_rescaling_holds_the_target_exactly(hostcheck_library):
+    run, _ = make_case(16, forcing=gbght.VarianceRescaling(0.45, "total"),
+                       scalar_forcing=gbght.VarianceRescaling(0.6, "total", 1, math.inf), library=hostcheck_library)
+    for _ in range(3):
+        run.advance(0.01)
+        ob = run.observables()
+        assert ob["kinetic_energy"] == pytest.approx(0.45, rel=1e-13)
+        assert ob["scalar_variance"] == pytest.approx(0.6, rel=1e-13)
+
+
 def test_rk3_and_cfl_steps_match(hostcheck_library):
     run, orun = make_case(16, forcing=0.2, scheme="IFLowStorageRK3", tracers=16, library=hostcheck_library)
     taken = advance_both(run, orun, 5, dt=None)

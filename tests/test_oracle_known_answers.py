@@ -145,7 +145,8 @@ def test_rk4_self_convergence_ratio():
     assert 10.0 < diffnorm(u1.uh, u2.uh) / diffnorm(u2.uh, u4.uh) < 26.0
 
 
-@pytest.mark.parametrize("forcing", [O.ConstantPower(0.2), O.Linear(0.5)], ids=["constant_power", "linear"])
+@pytest.mark.parametrize("forcing", [O.ConstantPower(0.2), O.Linear(0.5), O.VarianceController(1.5, turnover_time=1.0)],
+                         ids=["constant_power", "linear", "variance_controller"])
 @pytest.mark.parametrize("scheme,floor", [("rk3", 2.5), ("rk4", 3.5)])
 def test_order_kept_under_forcing(scheme, floor, forcing):
     # test/integrators.jl:132-162: a state-dependent forcing through the per-stage source and a
@@ -261,6 +262,129 @@ def test_scalar_linear_grows_exactly_with_zero_velocity(scheme):
     assert O.scalar_variance(dom, st.phih) > O.scalar_variance(dom, ph0)
     expected = ph0 * np.exp((A * band - (nu / Sc) * dom.k2) * dt * n)
     assert diffnorm(st.phih, expected) / math.sqrt(float(np.sum(np.abs(expected) ** 2))) < 1e-12
+
+
+def test_scalar_constant_power_injects_its_rate():
+    # the scalar's ConstantPower (target factor 1): d⟨φ²⟩/dt = 2⟨φ, f⟩ = ε_φ
+    N = 24
+    dom = O.Domain(N)
+    ph = S.seed_scalar(N, 0.4, seed=12)
+    src = O.stage_source(dom, O.ConstantPower(0.3), ph, np.finfo(float).eps, 0.05)
+    assert 2 * dom.inner(ph, src) == pytest.approx(0.3, rel=1e-12)
+
+
+def test_variance_controller_holds_the_whole_field_normalising_by_the_band():
+    # test/forcing.jl:322-349: A = (ε − G(k − k∞)/tℓ)/(2 k_band), read back off the applied source
+    N, nu = 24, 0.05
+    dom = O.Domain(N)
+    uh = S.seed_velocity(N, 0.5, seed=11)
+    f = O.VarianceController(0.5, turnover_time=0.8, gain=1.0)
+    src = O.stage_source(dom, f, uh, np.finfo(float).eps, nu)
+    band = O.band_indicator(dom, f)
+    k_whole = 0.5 * dom.inner(uh, uh)
+    k_band = 0.5 * dom.inner(uh, uh, band)
+    eps = nu * dom.inner(uh, uh, dom.k2)
+    expected = (eps - f.gain * (k_whole - f.target) / f.turnover_time) / (2 * k_band)
+    probe = band * uh
+    applied = dom.inner(src, probe) / dom.inner(probe, probe)
+    assert applied == pytest.approx(expected, rel=1e-10)
+    wrong = (eps - f.gain * (k_band - f.target) / f.turnover_time) / (2 * k_band)
+    assert not applied == pytest.approx(wrong, rel=1e-3)
+
+
+def test_variance_controller_scalar_dissipation_matches():
+    # test/forcing.jl:486-518: at gain 0 the scalar controller's A is ConstantPower's at ε = ε_φ,
+    # and halving ϰ halves it
+    N = 16
+    dom = O.Domain(N)
+    ph = S.seed_scalar(N, 0.4, seed=31)
+    kappa = 0.05 / 0.7
+    eps_phi = O.scalar_dissipation(dom, ph, kappa)
+    eT = np.finfo(float).eps
+    A_ctrl, _ = O.constant_power_amplitude(dom, O.VarianceController(1.0, turnover_time=1.0, gain=0.0), ph, eT, kappa)
+    A_cp, _ = O.constant_power_amplitude(dom, O.ConstantPower(eps_phi), ph, eT, kappa)
+    assert A_ctrl == pytest.approx(A_cp, rel=1e-12)
+    A_half, _ = O.constant_power_amplitude(dom, O.VarianceController(1.0, turnover_time=1.0, gain=0.0), ph, eT,
+                                           kappa / 2)
+    assert A_half == pytest.approx(A_cp / 2, rel=1e-12)
+
+
+def test_variance_controller_gain_zero_is_the_marginal_law():
+    # test/forcing.jl:388-405: k conserved at its initial value, never restored to the target
+    N = 24
+    dom = O.Domain(N)
+    cond = O.Conditions(viscosity=0.05, scalar=False, velocity_forcing=O.VarianceController(1.5, 1.0, gain=0.0))
+    run = O.Run(dom, cond, O.State(S.seed_velocity(N, 0.5, seed=3), None), scheme="rk4", cfl=0.5)
+    k0 = O.kinetic_energy(dom, run.state.uh)
+    for _ in range(150):
+        run.advance(None)
+    k = O.kinetic_energy(dom, run.state.uh)
+    assert k == pytest.approx(k0, rel=0.05)
+    assert abs(k - 1.5) > 0.8
+
+
+def test_variance_controller_relaxes_to_its_target():
+    # dk/dt = −G(k − k∞)/tℓ, exactly for the continuous law: after t = tℓ/G the gap has shrunk by e
+    N = 16
+    dom = O.Domain(N)
+    f = O.VarianceController(0.8, turnover_time=0.5, gain=1.0)
+    cond = O.Conditions(viscosity=0.05, scalar=False, velocity_forcing=f)
+    uh0 = S.seed_velocity(N, 0.5, seed=4)
+    dt, n = 0.005, 100
+    st = _integrate(dom, cond, uh0, None, dt, n, "rk4")
+    k = O.kinetic_energy(dom, st.uh)
+    expected = 0.8 + (0.5 - 0.8) * math.exp(-f.gain * dt * n / f.turnover_time)
+    assert k == pytest.approx(expected, rel=1e-6)
+
+
+@pytest.mark.parametrize("N", [16, 24])
+@pytest.mark.parametrize("over", ["band", "total"])
+def test_variance_rescaling_unbounded_band_rescales_the_whole_field(N, over):
+    # test/forcing.jl:440-452: with highest_shell = Inf both modes hold k = target exactly, by one
+    # uniform factor
+    dom = O.Domain(N)
+    uh = S.seed_velocity(N, 0.7, seed=N)
+    expected = uh * math.sqrt(1.3 / O.kinetic_energy(dom, uh))
+    v = O.project_forcing(dom, O.VarianceRescaling(1.3, over, highest_shell=math.inf), uh, np.finfo(float).eps)
+    assert O.kinetic_energy(dom, v) == pytest.approx(1.3, rel=1e-12)
+    assert np.max(np.abs(v - expected)) <= 1e-12 * np.max(np.abs(expected))
+
+
+def test_variance_rescaling_band_and_total():
+    # src/Forcing.jl:575-596: :band holds the band's value, :total the whole field's; a :total
+    # target below what lies outside the band zeroes the band; an empty band is left alone
+    N = 16
+    dom = O.Domain(N)
+    eT = np.finfo(float).eps
+    uh = S.seed_velocity(N, 0.5, seed=5)
+    f = O.VarianceRescaling(0.2, "band")
+    band = O.band_indicator(dom, f)
+    v = O.project_forcing(dom, f, uh, eT)
+    assert O.kinetic_energy(dom, band * v) == pytest.approx(0.2, rel=1e-12)
+    assert np.array_equal((1 - band) * v, (1 - band) * uh)
+    v = O.project_forcing(dom, O.VarianceRescaling(0.7, "total"), uh, eT)
+    assert O.kinetic_energy(dom, v) == pytest.approx(0.7, rel=1e-12)
+    outside = O.kinetic_energy(dom, (1 - band) * uh)
+    v = O.project_forcing(dom, O.VarianceRescaling(0.5 * outside, "total"), uh, eT)
+    assert np.max(np.abs(band * v)) == 0.0
+    empty = (1 - band) * uh
+    assert np.array_equal(O.project_forcing(dom, O.VarianceRescaling(0.7, "total"), empty, eT), empty)
+    ph = S.seed_scalar(N, 0.4, seed=6)   # the scalar's variance, target factor 1
+    w = O.project_forcing(dom, O.VarianceRescaling(0.9, "total"), ph, eT)
+    assert O.scalar_variance(dom, w) == pytest.approx(0.9, rel=1e-12)
+
+
+def test_variance_rescaling_costs_the_order():
+    # test/integrators.jl:159-161: the post-step projection is first order, by construction
+    N = 16
+    dom = O.Domain(N)
+    cond = O.Conditions(viscosity=0.05, velocity_forcing=O.VarianceRescaling(1.5, "total"))
+    uh0 = S.seed_velocity(N, 0.5, seed=7)
+    T = 0.2
+    ref = _integrate(dom, cond, uh0, None, T / 1024, 1024, "rk3").uh
+    e32 = np.max(np.abs(_integrate(dom, cond, uh0, None, T / 32, 32, "rk3").uh - ref))
+    e64 = np.max(np.abs(_integrate(dom, cond, uh0, None, T / 64, 64, "rk3").uh - ref))
+    assert math.log2(e32 / e64) < 1.5
 
 
 def test_scalar_forcing_needs_the_scalar():
