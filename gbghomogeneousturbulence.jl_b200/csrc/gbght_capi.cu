@@ -53,8 +53,10 @@ struct Tableau {
   double a[5], b[5], d[5];
 };
 
+// IFHeun and IFSSPRK3 are not low-storage schemes: the engine builds their stages itself (S = 0).
 Tableau tableau(int scheme) {
   Tableau t{};
+  if (scheme == GBGHT_IFHEUN || scheme == GBGHT_IFSSPRK3) return t;
   if (scheme == GBGHT_IFRK3) {
     t.S = 3;
     const double a[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
@@ -223,6 +225,18 @@ void gbght_config_default(gbght_config* c) {
   c->device = 0;
 }
 
+int gbght_recommended_cfl(int scheme, double* cfl) {
+  // `_base_cfl` (src/Propagator.jl:906-913); the 2/3 rule's factor (2/3)/(2/3) leaves it unchanged
+  if (!cfl) return GBGHT_ERR_ARGUMENT;
+  switch (scheme) {
+    case GBGHT_IFRK4: *cfl = 0.96; return GBGHT_OK;
+    case GBGHT_IFRK3: *cfl = 0.5; return GBGHT_OK;
+    case GBGHT_IFSSPRK3: *cfl = 0.5; return GBGHT_OK;
+    case GBGHT_IFHEUN: *cfl = 0.25; return GBGHT_OK;
+    default: return GBGHT_ERR_ARGUMENT;
+  }
+}
+
 const char* gbght_version(void) { return "gbght-b200 0.1.0"; }
 const char* gbght_global_error(void) { return g_global_error.c_str(); }
 const char* gbght_last_error(const gbght_run* r) { return r ? r->err.c_str() : "null run"; }
@@ -248,7 +262,9 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
     return bad("`schmidt` must be positive, got " + std::to_string(cfg->schmidt) +
                ": the scalar diffusivity is ν/Sc, so a non-positive Schmidt number makes it infinite or negative");
   if (cfg->precision != GBGHT_FP64 && cfg->precision != GBGHT_FP32_MIXED) return bad("unknown precision");
-  if (cfg->scheme != GBGHT_IFRK4 && cfg->scheme != GBGHT_IFRK3) return bad("unknown field integration scheme");
+  if (cfg->scheme != GBGHT_IFRK4 && cfg->scheme != GBGHT_IFRK3 && cfg->scheme != GBGHT_IFHEUN &&
+      cfg->scheme != GBGHT_IFSSPRK3)
+    return bad("unknown field integration scheme");
   {
     std::string m = forcing_error(cfg->velocity_forcing, "velocity");
     if (!m.empty()) return bad(m);

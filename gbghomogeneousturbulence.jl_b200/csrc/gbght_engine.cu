@@ -269,33 +269,81 @@ class EngineImpl final : public Engine {
   }
 
   // ---- the step ---------------------------------------------------------------------------------
+  // The common part of a stage's arguments: the forcings, the bands, the mean gradient.
+  StageArgs stage_base(double dt) const {
+    StageArgs st{};
+    st.dt = dt;
+    st.has_scalar = p_.scalar;
+    st.forced = stage_source(p_.vf.kind);
+    st.sforced = p_.scalar && stage_source(p_.sf.kind);
+    st.band_lo2 = band_lo2();
+    st.band_hi2 = band_hi2();
+    st.sband_lo2 = sband_lo2();
+    st.sband_hi2 = sband_hi2();
+    st.G[0] = p_.G[0];
+    st.G[1] = p_.G[1];
+    st.G[2] = p_.G[2];
+    return st;
+  }
+  // The integrating factors of a span δ: E = exp(−D·δ·|κ|² + δ·A), A a Linear forcing's rate on
+  // its band (src/Generator.jl:565-581). `second` selects the stage's second factor.
+  void set_factor(StageArgs& st, double delta, bool second) const {
+    const double cu = -(p_.viscosity * delta), cphi = -((p_.viscosity / p_.schmidt) * delta);
+    const double lu = p_.vf.kind == kForceLinear ? delta * p_.vf.rate : 0.0;
+    const double lphi = p_.sf.kind == kForceLinear ? delta * p_.sf.rate : 0.0;
+    if (second) {
+      st.cu2 = cu;
+      st.cphi2 = cphi;
+      st.lin_u2 = lu;
+      st.lin_phi2 = lphi;
+    } else {
+      st.cu = cu;
+      st.cphi = cphi;
+      st.lin_u = lu;
+      st.lin_phi = lphi;
+    }
+  }
   const char* step(double dt, const double* a, const double* b, const double* d, int S) override {
-    const double lo_hi[2] = {band_lo2(), band_hi2()};
-    const double slo_hi[2] = {sband_lo2(), sband_hi2()};
-    for (int i = 0; i < S; ++i) {
-      StageArgs st;
+    if (p_.scheme == 2) {   // IFHeun: predictor, corrector
+      StageArgs st = stage_base(dt);
+      st.kind = kHeunPredictor;
+      st.first = 1;
+      st.write_h = 1;
+      set_factor(st, dt, false);
+      if (const char* err = stage(st)) return err;
+      st = stage_base(dt);
+      st.kind = kHeunCorrector;
+      st.last = 1;
+      st.read_h = 1;
+      if (const char* err = stage(st)) return err;
+      return rt_check();
+    }
+    if (p_.scheme == 3) {   // IFSSPRK3: forward to t_n+1, back to the midpoint, forward again
+      const double span1[3] = {dt, -dt / 2, dt / 2}, span2[3] = {0.0, dt / 2, dt};
+      for (int i = 0; i < 3; ++i) {
+        StageArgs st = stage_base(dt);
+        st.kind = kSsp1 + i;
+        st.first = i == 0;
+        st.last = i == 2;
+        st.read_h = i > 0;
+        st.write_h = i == 0;
+        set_factor(st, span1[i], false);
+        if (i > 0) set_factor(st, span2[i], true);
+        if (const char* err = stage(st)) return err;
+      }
+      return rt_check();
+    }
+    for (int i = 0; i < S; ++i) {   // the low-storage 2N schemes
+      StageArgs st = stage_base(dt);
+      st.kind = kLowStorage;
       st.a = a[i];
       st.b = b[i];
-      st.dt = dt;
-      st.cu = -(p_.viscosity * (d[i] * dt));
-      st.cphi = -((p_.viscosity / p_.schmidt) * (d[i] * dt));
       st.first = i == 0;
       st.last = i == S - 1;
-      st.has_scalar = p_.scalar;
-      st.forced = stage_source(p_.vf.kind);
-      st.sforced = p_.scalar && stage_source(p_.sf.kind);
-      st.band_lo2 = lo_hi[0];
-      st.band_hi2 = lo_hi[1];
-      // Linear: the steady rate A on the band enters the exponent as (d_i·dt)·A
-      st.lin_u = p_.vf.kind == kForceLinear ? (d[i] * dt) * p_.vf.rate : 0.0;
-      st.lin_phi = p_.sf.kind == kForceLinear ? (d[i] * dt) * p_.sf.rate : 0.0;
-      st.sband_lo2 = slo_hi[0];
-      st.sband_hi2 = slo_hi[1];
-      st.G[0] = p_.G[0];
-      st.G[1] = p_.G[1];
-      st.G[2] = p_.G[2];
-      const char* err = stage(st);
-      if (err) return err;
+      st.read_h = !st.first;
+      st.write_h = !st.last;
+      set_factor(st, d[i] * dt, false);
+      if (const char* err = stage(st)) return err;
     }
     return rt_check();
   }
@@ -615,7 +663,8 @@ class EngineImpl final : public Engine {
     set(reinterpret_cast<const void*>(k_y_forward<T, N, TLY, NTY>), smem_y());
     set(reinterpret_cast<const void*>(k_x_products<T, N, NTXP>), smem_x());
     set(reinterpret_cast<const void*>(k_x_velocity<T, N, NTXV>), smem_xv());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, true>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, false>), smem_ze());
     set(reinterpret_cast<const void*>(k_z_init<T, N, TLZ, NTZ>), smem_z());
     return e;
   }
@@ -750,13 +799,22 @@ class EngineImpl final : public Engine {
       double* red = reinterpret_cast<double*>(base + L::kRed);
       Cplx<T>* R = reinterpret_cast<Cplx<T>*>(base + L::kStage);
       ZRowsReg<T, ZOwn<T, N, TLZ, 1>> rows;
-      partial_[c.by * gx + c.bx] = body_z_epilogue<T, N, TLZ, 1>(c, W, R, nullptr, red, g_, maps_, rows, A_, S_, H_,
-                                                                  st, amp_, tw_, status_);
+      partial_[c.by * gx + c.bx] =
+          st.kind == kLowStorage
+              ? body_z_epilogue<T, N, TLZ, 1, true>(c, W, R, nullptr, red, g_, maps_, rows, A_, S_, H_, st, amp_, tw_,
+                                                    status_)
+              : body_z_epilogue<T, N, TLZ, 1, false>(c, W, R, nullptr, red, g_, maps_, rows, A_, S_, H_, st, amp_, tw_,
+                                                     status_);
     });
 #else
     pbegin(PROF_Z_EPILOGUE);
-    k_z_epilogue<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_ze(), stream_>>>(
-        maps_, g_, A_, S_, H_, st, amp_, partial_, tw_, status_);
+    // the low-storage schemes run an instantiation without the other schemes' stage kinds
+    if (st.kind == kLowStorage)
+      k_z_epilogue<T, N, TLZ, NTZ, true><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_ze(), stream_>>>(
+          maps_, g_, A_, S_, H_, st, amp_, partial_, tw_, status_);
+    else
+      k_z_epilogue<T, N, TLZ, NTZ, false><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_ze(), stream_>>>(
+          maps_, g_, A_, S_, H_, st, amp_, partial_, tw_, status_);
     pend();
 #endif
   }

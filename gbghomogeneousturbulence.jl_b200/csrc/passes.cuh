@@ -940,19 +940,60 @@ GBGHT_HD void z_inverse_velocity(const Cta& c, Cplx<T>* W, const Geometry& g, Cp
 // `red` holds NT doubles; the CTA's sum of the Hermitian-weighted |û_new|² is returned to thread 0.
 // ================================================================================================
 struct StageArgs {
-  double a, b, dt;      // tableau a_i, b_i and the step
-  double cu, cphi;      // exponents c_i = −D·(d_i·dt) for velocity and scalar
-  int first, last;      // stage 0, stage S−1
+  int kind;             // StageKind: the scheme's update at this stage
+  double a, b, dt;      // tableau a_i, b_i (low storage) and the step
+  double cu, cphi;      // exponents c = −D·δ of the stage's first factor E₁, velocity and scalar
+  double cu2, cphi2;    // the second factor E₂ of a two-factor SSPRK3 stage
+  int first, last;      // the step's first stage (state = the step's start), its last
+  int read_h, write_h;  // the stage reads / writes the second register H
   int has_scalar;
   int forced, sforced;  // a per-stage source A·𝟙_band·f on the velocity, on the scalar
                         // (ConstantPower, VarianceController); A in force_amp[0], force_amp[4]
   double band_lo2, band_hi2;   // squared edges of the velocity forcing's band
-  double lin_u, lin_phi;       // (d_i·dt)·A of a Linear forcing, velocity and scalar (0: none)
+  double lin_u, lin_phi;       // δ·A of a Linear forcing in E₁, velocity and scalar (0: none)
+  double lin_u2, lin_phi2;     // the same in E₂
   double sband_lo2, sband_hi2; // squared edges of the scalar forcing's band
   double G[3];          // mean scalar gradient (extension)
 };
 
-template <class T, int N, int TL, int NT, class Rows>
+// The stage kinds. Low storage (src/Propagator.jl:326-419): h ← Δt·N (first) or a h + Δt·N,
+// q ← E₁(q + b h), h ← E₁ h. IFHeun (:456-544), predictor: q ← E₁(q + Δt N₁), h ← E₁q + (Δt/2)(E₁N₁);
+// corrector: q ← h + (Δt/2) N₂. IFSSPRK3 (:599-691), with q⁽⁰⁾ kept in h: stage 1 h ← q,
+// q ← E₁(q + Δt N) (E₁ = E(Δt)); stage 2 q ← ¼·E₁(q + Δt N) + E₂(¾ h) (E₁ = E(−Δt/2), E₂ = E(Δt/2));
+// stage 3 q ← E₂(⅓ h) + ⅔·E₁(q + Δt N) (E₁ = E(Δt/2), E₂ = E(Δt)). Each grouping is the reference's.
+enum StageKind { kLowStorage = 0, kHeunPredictor = 1, kHeunCorrector = 2, kSsp1 = 3, kSsp2 = 4, kSsp3 = 5 };
+
+// LS selects the low-storage update at compile time: the benchmark's path carries no other kind.
+template <class T, bool LS>
+GBGHT_HD Cplx<T> scheme_update(const StageArgs& st, Cplx<T> q, Cplx<T> h, Cplx<T> n, T E1, T E2, Cplx<T>* hw) {
+  const T dt = T(st.dt);
+  if (LS) {
+    const Cplx<T> hh = st.first ? scale(n, dt) : scale(h, T(st.a)) + scale(n, dt);
+    *hw = scale(hh, E1);
+    return scale(q + scale(hh, T(st.b)), E1);
+  }
+  switch (st.kind) {
+    case kHeunPredictor:
+      *hw = scale(q, E1) + scale(scale(n, E1), dt / T(2));
+      return scale(q + scale(n, dt), E1);
+    case kHeunCorrector:
+      return h + scale(n, dt / T(2));
+    case kSsp1:
+      *hw = q;
+      return scale(q + scale(n, dt), E1);
+    case kSsp2:
+      return scale(scale(q + scale(n, dt), E1), T(0.25)) + scale(scale(h, T(0.75)), E2);
+    case kSsp3:
+      return scale(scale(h, T(1.0 / 3.0)), E2) + scale(scale(q + scale(n, dt), E1), T(2.0 / 3.0));
+    default: {
+      const Cplx<T> hh = st.first ? scale(n, dt) : scale(h, T(st.a)) + scale(n, dt);
+      *hw = scale(hh, E1);
+      return scale(q + scale(hh, T(st.b)), E1);
+    }
+  }
+}
+
+template <class T, int N, int TL, int NT, bool LS, class Rows>
 GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* bar, double* red, const Geometry& g,
                                 const TmaMaps& maps, Rows& rows, Cplx<T>* GBGHT_RESTRICT A, Cplx<T>* GBGHT_RESTRICT S,
                                 Cplx<T>* GBGHT_RESTRICT H, const StageArgs& st, const double* GBGHT_RESTRICT force_amp,
@@ -986,7 +1027,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
     stg.issue(c, 1, 4);
     int codes[6], n = 0;
     codes[n++] = 3;                      // φ̂
-    if (!st.first) codes[n++] = 4 + 3;   // h_φ
+    if (st.read_h) codes[n++] = 4 + 3;   // h_φ
     const int iG = n;
     if (withG) {                         // û for −G·û
       codes[n++] = 0;
@@ -1023,13 +1064,13 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
             nphi = nphi - cmk<T>(G0 * ux.x + G1 * uy.x + G2 * uz.x, G0 * ux.y + G1 * uy.y + G2 * uz.y);
           }
           if (A_s != 0.0 && k2 >= st.sband_lo2 && k2 <= st.sband_hi2) nphi = nphi + scale(phi, T(A_s));
-          Cplx<T> hh = st.first ? scale(nphi, T(st.dt))
-                                : scale(sst.at(1, q, h, l), T(st.a)) + scale(nphi, T(st.dt));
-          const double rphi = (k2 >= st.sband_lo2 && k2 <= st.sband_hi2) ? st.lin_phi : 0.0;
-          const T E = T(exp(st.cphi * k2 + rphi));
-          phi = scale(phi + scale(hh, T(st.b)), E);
+          const bool sband = k2 >= st.sband_lo2 && k2 <= st.sband_hi2;
+          const T E1 = !LS && st.kind == kHeunCorrector ? T(1) : T(exp(st.cphi * k2 + (sband ? st.lin_phi : 0.0)));
+          const T E2 = !LS && st.kind >= kSsp2 ? T(exp(st.cphi2 * k2 + (sband ? st.lin_phi2 : 0.0))) : T(0);
+          Cplx<T> hw = czero<T>();
+          phi = scheme_update<T, LS>(st, phi, st.read_h ? sst.at(1, q, h, l) : czero<T>(), nphi, E1, E2, &hw);
           S[si] = phi;
-          if (!st.last) H[si] = scale(hh, E);
+          if (st.write_h) H[si] = hw;
         }
         x.v[b][sl] = phi;
       });
@@ -1053,7 +1094,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
   codes[n++] = 0;
   codes[n++] = 1;
   codes[n++] = 2;
-  if (!st.first) {
+  if (st.read_h) {
     codes[n++] = 4;
     codes[n++] = 5;
     codes[n++] = 6;
@@ -1092,20 +1133,14 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
           n1 = n1 + scale(u1, Af);
           n2 = n2 + scale(u2, Af);
         }
-        const T dt = T(st.dt), a = T(st.a), bb = T(st.b);
-        Cplx<T> h0, h1, h2;
-        if (st.first) {
-          h0 = scale(n0, dt); h1 = scale(n1, dt); h2 = scale(n2, dt);
-        } else {
-          h0 = scale(sst.at(3, q, h, l), a) + scale(n0, dt);
-          h1 = scale(sst.at(4, q, h, l), a) + scale(n1, dt);
-          h2 = scale(sst.at(5, q, h, l), a) + scale(n2, dt);
-        }
-        const double ru = (k2 >= st.band_lo2 && k2 <= st.band_hi2) ? st.lin_u : 0.0;
-        const T E = T(exp(st.cu * k2 + ru));
-        u0 = scale(u0 + scale(h0, bb), E);
-        u1 = scale(u1 + scale(h1, bb), E);
-        u2 = scale(u2 + scale(h2, bb), E);
+        const bool vband = k2 >= st.band_lo2 && k2 <= st.band_hi2;
+        const T E1 = !LS && st.kind == kHeunCorrector ? T(1) : T(exp(st.cu * k2 + (vband ? st.lin_u : 0.0)));
+        const T E2 = !LS && st.kind >= kSsp2 ? T(exp(st.cu2 * k2 + (vband ? st.lin_u2 : 0.0))) : T(0);
+        const bool rh = st.read_h;
+        Cplx<T> w0 = czero<T>(), w1 = czero<T>(), w2 = czero<T>();
+        u0 = scheme_update<T, LS>(st, u0, rh ? sst.at(3, q, h, l) : czero<T>(), n0, E1, E2, &w0);
+        u1 = scheme_update<T, LS>(st, u1, rh ? sst.at(4, q, h, l) : czero<T>(), n1, E1, E2, &w1);
+        u2 = scheme_update<T, LS>(st, u2, rh ? sst.at(5, q, h, l) : czero<T>(), n2, E1, E2, &w2);
         if (st.last) {
           if (k2 > 0.0) {
             const T kX = T(kxd), kY = T(ky), kZ = T(kzd);
@@ -1115,10 +1150,11 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
             u1 = u1 - scale(kd, kY);
             u2 = u2 - scale(kd, kZ);
           }
-        } else {
-          H[s0] = scale(h0, E);
-          H[s1] = scale(h1, E);
-          H[s2] = scale(h2, E);
+        }
+        if (st.write_h) {
+          H[s0] = w0;
+          H[s1] = w1;
+          H[s2] = w2;
         }
         S[s0] = u0;
         S[s1] = u1;

@@ -23,7 +23,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "libgbght.so")
 
 FP64, FP32_MIXED = 0, 1
-IFRK4, IFRK3 = 0, 1
+IFRK4, IFRK3, IFHEUN, IFSSPRK3 = 0, 1, 2, 3
+SCHEMES = {"IFLowStorageRK4": IFRK4, "IFLowStorageRK3": IFRK3, "IFHeun": IFHEUN, "IFSSPRK3": IFSSPRK3}
 FORCING_NONE, FORCING_CONSTANT_POWER, FORCING_LINEAR, FORCING_VARIANCE_CONTROLLER, FORCING_VARIANCE_RESCALING = 0, 1, 2, 3, 4
 OVER = {"band": 0, "total": 1}
 OK, ERR_ARGUMENT, ERR_SCHEDULE, ERR_CUDA, ERR_DEVICE = 0, 1, 2, 3, 4
@@ -81,6 +82,7 @@ _SIGNATURES = {
     "gbght_state_import": (C.c_int, [C.c_void_p, _DP, _DP]),
     "gbght_state_export": (C.c_int, [C.c_void_p, _DP, _DP]),
     "gbght_step": (C.c_int, [C.c_void_p, C.c_double]),
+    "gbght_recommended_cfl": (C.c_int, [C.c_int, _DP]),
     "gbght_deposit": (C.c_int, [C.c_void_p]),
     "gbght_max_speed": (C.c_int, [C.c_void_p, _DP]),
     "gbght_cfl_timestep": (C.c_int, [C.c_void_p, _DP]),
@@ -211,7 +213,7 @@ class Setup:
     scalar_forcing: object = field(default_factory=NoForcing)
     mean_gradient: tuple = (0.0, 0.0, 0.0)
     precision: str = "fp64"          # "fp64" or "fp32_mixed"
-    scheme: str = "IFLowStorageRK4"  # or "IFLowStorageRK3"
+    scheme: str = "IFLowStorageRK4"  # or "IFLowStorageRK3", "IFHeun", "IFSSPRK3"
     tracers: int = 0
     cfl: float = 0.5
     max_dt: float = math.inf
@@ -230,7 +232,9 @@ class Run:
         cfg.grid_points_per_axis = int(setup.grid_points_per_axis)
         cfg.side_length = float(setup.side_length)
         cfg.precision = {"fp64": FP64, "fp32_mixed": FP32_MIXED}[setup.precision]
-        cfg.scheme = {"IFLowStorageRK4": IFRK4, "IFLowStorageRK3": IFRK3}[setup.scheme]
+        if setup.scheme not in SCHEMES:
+            raise ValueError(f"unknown field integration scheme {setup.scheme!r}")
+        cfg.scheme = SCHEMES[setup.scheme]
         cfg.viscosity = float(setup.viscosity)
         cfg.schmidt = float(setup.schmidt)
         cfg.scalar = 1 if setup.scalar else 0
@@ -430,6 +434,15 @@ class Run:
         ms = C.c_double()
         self._check(self.lib.gbght_timer(self.h, 1, C.byref(ms)))
         return ms.value
+
+
+def recommended_cfl(scheme: str, library: str | None = None) -> float:
+    """`recommended_cfl(scheme, domain)` (src/Propagator.jl:906-919) for the 2/3 rule."""
+    lib = load_library(library)
+    v = C.c_double()
+    if scheme not in SCHEMES or lib.gbght_recommended_cfl(SCHEMES[scheme], C.byref(v)) != OK:
+        raise ValueError(f"unknown field integration scheme {scheme!r}")
+    return v.value
 
 
 def simulation(setup: Setup, uh: np.ndarray, phih: np.ndarray | None = None, X: np.ndarray | None = None,

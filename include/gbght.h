@@ -41,7 +41,9 @@ enum gbght_status {
 };
 
 enum gbght_precision { GBGHT_FP64 = 0, GBGHT_FP32_MIXED = 1 };
-enum gbght_scheme { GBGHT_IFRK4 = 0, GBGHT_IFRK3 = 1 };
+/* The field integration schemes (src/Propagator.jl): IFLowStorageRK4 (:304-320), IFLowStorageRK3
+ * (:267-274), IFHeun (:456-544), IFSSPRK3 (:599-691). */
+enum gbght_scheme { GBGHT_IFRK4 = 0, GBGHT_IFRK3 = 1, GBGHT_IFHEUN = 2, GBGHT_IFSSPRK3 = 3 };
 /* The forcing strategies (src/Forcing.jl), for either field:
  *  NONE                 NoForcing.
  *  CONSTANT_POWER       ConstantPower (:1069-1117): A = ε/(2 k_band) re-solved at every stage, a
@@ -132,11 +134,16 @@ int gbght_state_import(gbght_run* run, const double* u_hat, const double* phi_ha
 int gbght_state_export(gbght_run* run, double* u_hat, double* phi_hat);
 
 /* One field step of the configured scheme with step dt > 0, in place. Requires a current field
- * deposit, i.e. gbght_deposit after the last state change; otherwise SCHEDULE. The step is the
- * coupled velocity + scalar 2N loop with the end-of-step Leray and reality projections.
- * Replaces step!(::IFLowStorageRK4 / ::IFLowStorageRK3, state, generator, domain, buffers, cache,
- * dt) (src/Propagator.jl:267-274,304-419). */
+ * deposit, i.e. gbght_deposit after the last state change; otherwise SCHEDULE. The step advances
+ * velocity and scalar together, then applies the forcings' post-step projections and the Leray
+ * and reality projections. Replaces step!(::IFLowStorageRK4 / ::IFLowStorageRK3 / ::IFHeun /
+ * ::IFSSPRK3, state, generator, domain, buffers, cache, dt) (src/Propagator.jl:267-274,304-419,
+ * 456-544,599-691). */
 int gbght_step(gbght_run* run, double dt);
+
+/* A scheme's advective-CFL ceiling under the 2/3 rule: 0.96 (RK4), 0.5 (RK3, SSPRK3), 0.25 (Heun).
+ * Replaces recommended_cfl(scheme, domain) (src/Propagator.jl:906-919) for TwoThirds. */
+int gbght_recommended_cfl(int scheme, double* cfl);
 
 /* The closing field deposit: the velocity in physical representation and max|u|.
  * Replaces deposit!(cache, state, domain, buffers) (src/Propagator.jl:808-842). */

@@ -380,7 +380,32 @@ def integrating_factor(dom: Domain, diffusivity: float, rate: np.ndarray, delta:
     return np.exp((-(diffusivity * delta)) * dom.k2 + delta * rate)
 
 
-def step(dom: Domain, cond: Conditions, st: State, dt: float, scheme: str = "rk4") -> State:
+def _rhs(dom: Domain, cond: Conditions, uh, ph, eps_T):
+    """Both fields' right-hand sides at a stage state (ph None without a scalar)."""
+    u = dom.to_physical(uh)
+    w = dom.to_physical(curl(dom, uh))
+    nu_ = velocity_rhs(dom, cond, uh, u, w, eps_T)
+    np_ = None
+    if ph is not None:
+        np_ = scalar_rhs(dom, cond, uh, u, dom.to_physical(ph), ph, eps_T)
+    return nu_, np_
+
+
+def _close(dom: Domain, cond: Conditions, uh, ph, eps_T) -> State:
+    """The end of every scheme's step: the forcings' post-step projections, velocity first
+    (`finalize!` src/Generator.jl:396-400), then the Leray and reality projections of the state
+    (src/Propagator.jl:394-412)."""
+    uh = project_forcing(dom, cond.velocity_forcing, uh, eps_T)
+    if ph is not None:
+        ph = project_forcing(dom, cond.scalar_forcing, ph, eps_T)
+    uh = leray(dom, uh)
+    uh = reality_projection(dom, uh)
+    if ph is not None:
+        ph = reality_projection(dom, ph)
+    return State(uh, ph)
+
+
+def _step_low_storage(dom: Domain, cond: Conditions, st: State, dt: float, scheme: str) -> State:
     """One step of `_low_storage_2n_step!` (src/Propagator.jl:326-419) with scheme "rk4"
     (`IFLowStorageRK4`, :304-320) or "rk3" (`IFLowStorageRK3`, :267-274)."""
     a, b, d = TABLEAUX[scheme]
@@ -390,16 +415,10 @@ def step(dom: Domain, cond: Conditions, st: State, dt: float, scheme: str = "rk4
     has_scalar = ph is not None
     hu = None
     hp = None
-    dt = float(dt)
     rate_u = steady_rate(dom, cond.velocity_forcing)
     rate_p = steady_rate(dom, cond.scalar_forcing) if has_scalar else None
     for i in range(len(a)):
-        u = dom.to_physical(uh)
-        w = dom.to_physical(curl(dom, uh))
-        nu_ = velocity_rhs(dom, cond, uh, u, w, eps_T)
-        if has_scalar:
-            phi = dom.to_physical(ph)
-            np_ = scalar_rhs(dom, cond, uh, u, phi, ph, eps_T)
+        nu_, np_ = _rhs(dom, cond, uh, ph, eps_T)
         hu = dt * nu_ if i == 0 else a[i] * hu + dt * nu_
         E = integrating_factor(dom, cond.viscosity, rate_u, d[i] * dt)
         uh = E * (uh + b[i] * hu)
@@ -411,15 +430,74 @@ def step(dom: Domain, cond: Conditions, st: State, dt: float, scheme: str = "rk4
             ph = Ep * (ph + b[i] * hp)
             if i < len(a) - 1:
                 hp = Ep * hp
-    # post-step forcing projections, velocity first (`finalize!` src/Generator.jl:396-400)
-    uh = project_forcing(dom, cond.velocity_forcing, uh, eps_T)
-    if has_scalar:
-        ph = project_forcing(dom, cond.scalar_forcing, ph, eps_T)
-    uh = leray(dom, uh)
-    uh = reality_projection(dom, uh)
-    if has_scalar:
-        ph = reality_projection(dom, ph)
-    return State(uh, ph)
+    return _close(dom, cond, uh, ph, eps_T)
+
+
+def _step_heun(dom: Domain, cond: Conditions, st: State, dt: float) -> State:
+    """One step of `step!(::IFHeun, …)` (src/Propagator.jl:456-544): the predictor
+    q* = E(q + Δt N₁), then q ← (E q + (Δt/2)(E N₁)) + (Δt/2) N₂ with N₂ at q*, in the reference's
+    order of rotations and accumulations."""
+    eps_T = np.finfo(np.float64).eps
+    half = dt / 2
+    fields = [(st.uh.copy(), cond.viscosity, steady_rate(dom, cond.velocity_forcing))]
+    if st.phih is not None:
+        fields.append((st.phih.copy(), cond.diffusivity, steady_rate(dom, cond.scalar_forcing)))
+    n1 = _rhs(dom, cond, fields[0][0], fields[1][0] if len(fields) > 1 else None, eps_T)
+    pred, banked = [], []
+    for (q, D, rate), n in zip(fields, n1):
+        E = integrating_factor(dom, D, rate, dt)
+        pred.append(E * (q + dt * n))                    # q* = E(q + Δt N₁)
+        banked.append((E * q) + half * (E * n))          # E q + (Δt/2)(E N₁)
+    n2 = _rhs(dom, cond, pred[0], pred[1] if len(pred) > 1 else None, eps_T)
+    out = [b + half * n for b, n in zip(banked, n2)]
+    return _close(dom, cond, out[0], out[1] if len(out) > 1 else None, eps_T)
+
+
+def _step_ssprk3(dom: Domain, cond: Conditions, st: State, dt: float) -> State:
+    """One step of `step!(::IFSSPRK3, …)` (src/Propagator.jl:599-691), Shu–Osher form with each
+    term carried to its stage's time:
+    q⁽¹⁾ = E(Δt)(q + Δt N), q⁽²⁾ = ¼·E(−Δt/2)(q⁽¹⁾ + Δt N) + E(Δt/2)(¾ q),
+    q ← E(Δt)(⅓ q) + ⅔·E(Δt/2)(q⁽²⁾ + Δt N)."""
+    eps_T = np.finfo(np.float64).eps
+    fields = [(st.uh.copy(), cond.viscosity, steady_rate(dom, cond.velocity_forcing))]
+    if st.phih is not None:
+        fields.append((st.phih.copy(), cond.diffusivity, steady_rate(dom, cond.scalar_forcing)))
+
+    def rhs(stages):
+        return _rhs(dom, cond, stages[0], stages[1] if len(stages) > 1 else None, eps_T)
+
+    def E(D, rate, delta):
+        return integrating_factor(dom, D, rate, delta)
+
+    n = rhs([q for q, _, _ in fields])
+    s1 = [E(D, r, dt) * (q + dt * nn) for (q, D, r), nn in zip(fields, n)]
+    n = rhs(s1)
+    s2 = [0.25 * (E(D, r, -dt / 2) * (s + dt * nn)) + E(D, r, dt / 2) * (0.75 * q)
+          for (q, D, r), s, nn in zip(fields, s1, n)]
+    n = rhs(s2)
+    out = [E(D, r, dt) * ((1 / 3) * q) + (2 / 3) * (E(D, r, dt / 2) * (s + dt * nn))
+           for (q, D, r), s, nn in zip(fields, s2, n)]
+    return _close(dom, cond, out[0], out[1] if len(out) > 1 else None, eps_T)
+
+
+SCHEMES = ("rk4", "rk3", "heun", "ssprk3")
+
+
+def step(dom: Domain, cond: Conditions, st: State, dt: float, scheme: str = "rk4") -> State:
+    """One field step of `scheme`: "rk4" (IFLowStorageRK4), "rk3" (IFLowStorageRK3), "heun"
+    (IFHeun) or "ssprk3" (IFSSPRK3)."""
+    dt = float(dt)
+    if scheme == "heun":
+        return _step_heun(dom, cond, st, dt)
+    if scheme == "ssprk3":
+        return _step_ssprk3(dom, cond, st, dt)
+    return _step_low_storage(dom, cond, st, dt, scheme)
+
+
+def recommended_cfl(scheme: str) -> float:
+    """A scheme's advective-CFL ceiling under TwoThirds dealiasing (`recommended_cfl`,
+    src/Propagator.jl:906-919; the 2/3 band leaves the base ceiling unchanged)."""
+    return {"heun": 0.25, "rk3": 0.5, "ssprk3": 0.5, "rk4": 0.96}[scheme]
 
 
 # ---------------------------------------------------------------------------------------------

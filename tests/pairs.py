@@ -17,6 +17,9 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
+ORACLE_SCHEME = {"IFLowStorageRK4": "rk4", "IFLowStorageRK3": "rk3", "IFHeun": "heun", "IFSSPRK3": "ssprk3"}
+
+
 def oracle_forcing(f):
     """The oracle's counterpart of a library forcing object (None for NoForcing)."""
     if f is None or isinstance(f, gbght.NoForcing):
@@ -59,7 +62,7 @@ def make_case(N, *, viscosity=0.01, schmidt=1.0, scalar=True, forcing=None, G=(0
                         velocity_forcing=oracle_forcing(lib_forcing), mean_gradient=G,
                         scalar_forcing=oracle_forcing(lib_sforcing))
     orun = O.Run(dom, cond, O.State(uh.copy(), ph.copy() if scalar else None),
-                 X=None if not tracers else X.copy(), scheme={"IFLowStorageRK4": "rk4", "IFLowStorageRK3": "rk3"}[scheme],
+                 X=None if not tracers else X.copy(), scheme=ORACLE_SCHEME[scheme],
                  cfl=cfl)
     return run, orun
 

@@ -106,6 +106,23 @@ def test_band_forcings_both_fields(cuda_library, name, N, precision, steps):
         compare(run, orun, tol=1e-5, check_tracers=False)
 
 
+@pytest.mark.parametrize("scheme", ["IFHeun", "IFSSPRK3"])
+@pytest.mark.parametrize("N,precision,steps", [(64, "fp64", 10), (256, "fp64", 1), (64, "fp32_mixed", 5)])
+def test_heun_and_ssprk3(cuda_library, scheme, N, precision, steps):
+    # the two schemes outside the low-storage loop: ConstantPower on the velocity, Linear on the
+    # scalar, G, CFL steps at the schemes' own ceilings, tracers
+    run, orun = make_case(N, viscosity=0.005, forcing=0.1, scalar_forcing=gbght.Linear(0.3), G=(1.0, 0.0, 0.0),
+                          tracers=1000, scheme=scheme, cfl=0.25, precision=precision, library=cuda_library)
+    taken = advance_both(run, orun, steps, dt=None)
+    if precision == "fp64":
+        for d_lib, d_ora in taken:
+            assert d_lib == pytest.approx(d_ora, rel=1e-12)
+        res = compare(run, orun, tol=1e-12)
+        assert res["X_err"] < 1e-10
+    else:
+        compare(run, orun, tol=1e-5, check_tracers=False)
+
+
 def test_rescaling_holds_the_target_exactly(cuda_library):
     run, _ = make_case(64, forcing=gbght.VarianceRescaling(0.45, "total"),
                        scalar_forcing=gbght.VarianceRescaling(0.6, "total", 1, math.inf), library=cuda_library)

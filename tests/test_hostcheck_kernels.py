@@ -65,6 +65,30 @@ def test_rescaling_holds_the_target_exactly(hostcheck_library):
         assert ob["scalar_variance"] == pytest.approx(0.6, rel=1e-13)
 
 
+@pytest.mark.parametrize("scheme", ["IFHeun", "IFSSPRK3"])
+@pytest.mark.parametrize("vf,sf", [(0.1, None), (gbght.Linear(0.5), gbght.VarianceRescaling(0.3, "total")),
+                                   (gbght.VarianceController(0.4, turnover_time=0.5), gbght.ConstantPower(0.2))],
+                         ids=["cp", "linear+rescale", "controller+cp"])
+def test_heun_and_ssprk3_match_oracle(hostcheck_library, scheme, vf, sf):
+    # the two schemes outside the low-storage loop, with the forcings, G, CFL steps and tracers
+    run, orun = make_case(16, forcing=vf, scalar_forcing=sf, G=(0.0, 0.0, 1.0), tracers=16, scheme=scheme,
+                          cfl=0.25, library=hostcheck_library)
+    taken = advance_both(run, orun, 4, dt=None)
+    for d_lib, d_ora in taken:
+        assert d_lib == pytest.approx(d_ora, rel=1e-13)
+    res = compare(run, orun, tol=2e-14)
+    assert res["X_err"] < 1e-13
+
+
+def test_recommended_cfl(hostcheck_library):
+    # test/integrators.jl:114-118, and the ceilings themselves (src/Propagator.jl:906-913)
+    got = {s: gbght.recommended_cfl(s, library=hostcheck_library)
+           for s in ("IFLowStorageRK4", "IFLowStorageRK3", "IFHeun", "IFSSPRK3")}
+    assert got == {"IFLowStorageRK4": 0.96, "IFLowStorageRK3": 0.5, "IFHeun": 0.25, "IFSSPRK3": 0.5}
+    with pytest.raises(ValueError):
+        gbght.recommended_cfl("IFEuler", library=hostcheck_library)
+
+
 def test_rk3_and_cfl_steps_match(hostcheck_library):
     run, orun = make_case(16, forcing=0.2, scheme="IFLowStorageRK3", tracers=16, library=hostcheck_library)
     taken = advance_both(run, orun, 5, dt=None)

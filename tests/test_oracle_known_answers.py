@@ -145,9 +145,57 @@ def test_rk4_self_convergence_ratio():
     assert 10.0 < diffnorm(u1.uh, u2.uh) / diffnorm(u2.uh, u4.uh) < 26.0
 
 
+def test_temporal_convergence_orders_of_the_four_schemes():
+    # test/integrators.jl:47-80: RK3 and SSPRK3 third order, Heun second, RK3 faster than Heun;
+    # the two RK3 tableaux agree as Δt → 0 but differ at one Δt
+    N = 16
+    dom = O.Domain(N)
+    cond = O.Conditions(viscosity=0.1, scalar=False)
+    uh0 = S.seed_velocity(N, 0.5, seed=7)
+    T, n = 0.5, 8
+    runs = {sch: [_integrate(dom, cond, uh0, None, T / (k * n), k * n, sch).uh for k in (1, 2, 4)]
+            for sch in ("rk3", "ssprk3", "heun")}
+    ratio = {sch: diffnorm(r[0], r[1]) / diffnorm(r[1], r[2]) for sch, r in runs.items()}
+    assert 5.0 < ratio["rk3"] < 12.0
+    assert 5.0 < ratio["ssprk3"] < 12.0
+    assert 3.0 < ratio["heun"] < 6.0
+    assert ratio["rk3"] > ratio["heun"]
+    assert diffnorm(runs["rk3"][2], runs["ssprk3"][2]) < diffnorm(runs["rk3"][0], runs["ssprk3"][0])
+    assert diffnorm(runs["rk3"][0], runs["ssprk3"][0]) > 0
+
+
+@pytest.mark.parametrize("scheme", ["heun", "ssprk3"])
+def test_exact_diffusion_and_linear_growth_heun_ssprk3(scheme):
+    # test/scalar.jl:42-60 for the other two schemes: with u = 0 the scalar moves by the
+    # integrating factor alone (the SSPRK3 stages transport back and forth and recombine to E(Δt));
+    # and a shear mode under Linear grows at exactly A − ν|κ|²
+    N, nu, Sc = 16, 0.1, 0.7
+    dom = O.Domain(N)
+    ph0 = S.seed_scalar(N, 1.0, seed=3)
+    st = O.State(np.zeros((3,) + dom.shape_spectral, complex), ph0.copy())
+    dt, n = 0.02, 25
+    for _ in range(n):
+        st = O.step(dom, O.Conditions(viscosity=nu, schmidt=Sc), st, dt, scheme)
+    expected = ph0 * np.exp(-(nu / Sc) * dom.k2 * dt * n)
+    assert diffnorm(st.phih, expected) / math.sqrt(float(np.sum(np.abs(expected) ** 2))) < 1e-12
+    x3, y3, z3 = _grid(N)
+    uh0 = dom.to_spectral(np.stack([np.sin(y3), np.zeros_like(y3), np.zeros_like(y3)]))
+    cond = O.Conditions(viscosity=0.05, scalar=False, velocity_forcing=O.Linear(0.7))
+    st = _integrate(dom, cond, uh0, None, dt, n, scheme)
+    expected = uh0 * math.exp((0.7 - 0.05) * dt * n)
+    assert diffnorm(st.uh, expected) / math.sqrt(float(np.sum(np.abs(expected) ** 2))) < 1e-12
+
+
+def test_recommended_cfl():
+    # test/integrators.jl:114-118
+    assert O.recommended_cfl("rk3") > O.recommended_cfl("heun")
+    assert 0 < O.recommended_cfl("heun") < 1 and 0 < O.recommended_cfl("rk3") < 1
+    assert O.recommended_cfl("ssprk3") == O.recommended_cfl("rk3")
+
+
 @pytest.mark.parametrize("forcing", [O.ConstantPower(0.2), O.Linear(0.5), O.VarianceController(1.5, turnover_time=1.0)],
                          ids=["constant_power", "linear", "variance_controller"])
-@pytest.mark.parametrize("scheme,floor", [("rk3", 2.5), ("rk4", 3.5)])
+@pytest.mark.parametrize("scheme,floor", [("rk3", 2.5), ("rk4", 3.5), ("ssprk3", 2.5), ("heun", 1.7)])
 def test_order_kept_under_forcing(scheme, floor, forcing):
     # test/integrators.jl:132-162: a state-dependent forcing through the per-stage source and a
     # steady rate through the integrating factor keep the scheme's order (measured ≥ 2.5 for RK3;
