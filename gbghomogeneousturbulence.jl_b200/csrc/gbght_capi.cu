@@ -21,11 +21,15 @@ struct gbght_run {
   int64_t fields_epoch = 0;
   int64_t deposit_epoch = -1;
   double max_speed = 0.0;
-  // the tracer side: the newest trail sample
-  bool sample_valid = false;
+  // the tracer side: the trail of the velocity at the particles (src/Particles.jl:440-520), a ring
+  // of `capacity` device slots, and the epoch pairing of src/Cache.jl:340-390
+  int trail_capacity = 1;
+  int trail_count = 0;          // samples held
+  int trail_newest = -1;        // ring slot of the newest
+  double trail_time[gbght::kTrailMax] = {};
+  bool sampled = false;         // a particle deposit has paired the tracer and field epochs
   bool sample_at_positions = false;
   int64_t sample_epoch = 0;
-  double sample_time = 0.0;
   // the clock
   double time = 0.0;
   int64_t step = 0;
@@ -187,7 +191,63 @@ int do_deposit(gbght_run* r) {
   return GBGHT_OK;
 }
 
-double cfl_dt(const gbght_run* r) {
+// The trail's j-th newest sample's slot.
+int trail_slot(const gbght_run* r, int j) {
+  return ((r->trail_newest - j) % r->trail_capacity + r->trail_capacity) % r->trail_capacity;
+}
+// The slot the next sample goes to (the oldest once the ring is full).
+int trail_next(const gbght_run* r) { return (r->trail_newest + 1) % r->trail_capacity; }
+void trail_push(gbght_run* r, double t) {
+  r->trail_newest = trail_next(r);
+  r->trail_time[r->trail_newest] = t;
+  if (r->trail_count < r->trail_capacity) r->trail_count += 1;
+}
+double trail_newest_time(const gbght_run* r) { return r->trail_time[r->trail_newest]; }
+
+// The particle scheme's step over h from the trail (`advect!`, src/ParticlePropagator.jl:339-352):
+// its own k samples once the trail holds them, else the corrected ABM of the samples present.
+gbght::AdamsStep adams_step(const gbght_run* r, double h) {
+  const int k = r->cfg.tracer_steps;
+  const bool full = r->trail_count >= k;
+  const int J = full ? k : r->trail_count;
+  const bool corrected = full ? r->cfg.tracer_scheme != GBGHT_AB : true;
+  double times[gbght::kTrailMax];
+  gbght::AdamsStep w{};
+  for (int j = 0; j < J; ++j) {
+    w.slot[j] = trail_slot(r, j);
+    times[j] = r->trail_time[w.slot[j]];
+  }
+  gbght::adams_step_weights(times, J, h, corrected, &w);
+  w.out_slot = -1;
+  return w;
+}
+
+int tracer_order(const gbght_config& c) { return c.tracer_scheme == GBGHT_AB ? c.tracer_steps : c.tracer_steps + 1; }
+
+// The start-up bound under shortened_first_steps (`_startup_bound`, src/SimulationRun.jl:1117-1132):
+// growth(order)·(t₀ − t₋₁) once the trail holds two samples, else τ(Δt/τ)^(order/3) with τ = √(ν/ε),
+// ε the state's dissipation; infinite otherwise.
+int startup_bound(gbght_run* r, double dt, double* bound) {
+  const gbght_config& c = r->cfg;
+  *bound = INFINITY;
+  if (!(c.shortened_first_steps && c.tracers > 0 && c.tracer_steps > 1)) return GBGHT_OK;
+  const int order = tracer_order(c);
+  if (r->trail_count > 1) {
+    const double growth = order <= 5 ? 2.0 : order <= 7 ? 1.5 : 1.25;
+    *bound = growth * (r->trail_time[trail_slot(r, 0)] - r->trail_time[trail_slot(r, 1)]);
+    return GBGHT_OK;
+  }
+  gbght::Observables o{};
+  int rc = engine_call(r, r->eng->observables(&o));
+  if (rc) return rc;
+  const double tau = std::sqrt(c.viscosity / o.eps);
+  if (std::isfinite(tau) && tau > 0) *bound = tau * std::pow(dt / tau, order / 3.0);
+  return GBGHT_OK;
+}
+
+// cfl_timestep (src/SimulationRun.jl:1051-1096): the advective, resolution and caller's bounds, and
+// the start-up bound.
+int cfl_dt(gbght_run* r, double* out) {
   const gbght_config& c = r->cfg;
   const double dx = c.side_length / c.grid_points_per_axis;
   const double advective = r->max_speed > 0 ? c.cfl * dx / r->max_speed : c.cfl * dx;
@@ -195,7 +255,11 @@ double cfl_dt(const gbght_run* r) {
   const double D = c.scalar ? std::max(nu, kap) : nu;
   const double kmin = 2.0 * M_PI / c.side_length;
   const double resolution = 1.0 / (D * kmin * kmin);
-  return std::min(std::min(advective, resolution), c.max_dt);
+  const double base = std::min(std::min(advective, resolution), c.max_dt);
+  double bound;
+  if (int rc = startup_bound(r, base, &bound)) return rc;
+  *out = std::min(bound, base);
+  return GBGHT_OK;
 }
 
 }  // namespace
@@ -220,6 +284,9 @@ void gbght_config_default(gbght_config* c) {
   forcing_default(&c->velocity_forcing);
   forcing_default(&c->scalar_forcing);
   c->tracers = 0;
+  c->tracer_scheme = GBGHT_HEUN;
+  c->tracer_steps = 1;
+  c->shortened_first_steps = 0;
   c->cfl = 0.5;
   c->max_dt = INFINITY;
   c->device = 0;
@@ -279,11 +346,27 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
   if (!cfg->scalar && (cfg->mean_gradient[0] != 0 || cfg->mean_gradient[1] != 0 || cfg->mean_gradient[2] != 0))
     return bad("a mean scalar gradient was given, but the run carries no scalar");
   if (cfg->tracers < 0) return bad("tracers must be non-negative");
+  if (cfg->tracer_scheme == GBGHT_HEUN) {
+    if (cfg->tracer_steps != 1) return bad("Heun is ABM(1): `tracer_steps` must be 1");
+  } else if (cfg->tracer_scheme == GBGHT_ABM) {
+    if (cfg->tracer_steps < 1 || cfg->tracer_steps > 7)
+      return bad("`ABM(k)` takes a number of steps `k` from 1 to 7, got " + std::to_string(cfg->tracer_steps) +
+                 ": the four-point Gauss–Legendre rule that integrates the weights is exact only through the "
+                 "degree `k = 7` needs");
+  } else if (cfg->tracer_scheme == GBGHT_AB) {
+    if (cfg->tracer_steps < 1 || cfg->tracer_steps > 8)
+      return bad("`AB(k)` takes a number of steps `k` from 1 to 8, got " + std::to_string(cfg->tracer_steps) +
+                 ": the four-point Gauss–Legendre rule that integrates the weights is exact only through "
+                 "degree 7");
+  } else {
+    return bad("unknown particle integration scheme");
+  }
   if (!finite_positive(cfg->cfl)) return bad("cfl must be positive and finite");
   if (!(cfg->max_dt > 0)) return bad("max_dt must be positive");
 
   auto r = std::make_unique<gbght_run>();
   r->cfg = *cfg;
+  r->trail_capacity = cfg->tracer_steps;
   std::string err;
   r->eng.reset(gbght::make_engine(cfg->grid_points_per_axis, cfg->precision, &err));
   if (!r->eng) return bad(err);
@@ -299,6 +382,7 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
   p.sf = cfg->scalar ? to_forcing(cfg->scalar_forcing) : gbght::ForcingParams{};
   for (int i = 0; i < 3; ++i) p.G[i] = cfg->mean_gradient[i];
   p.tracers = cfg->tracers;
+  p.trail_capacity = cfg->tracer_steps;
   p.device = cfg->device;
   if (const char* e = r->eng->init(p)) {
     g_global_error = e;
@@ -369,7 +453,9 @@ int gbght_cfl_timestep(gbght_run* r, double* dt) {
   if (!std::isfinite(r->max_speed))
     return fail(r, GBGHT_ERR_SCHEDULE,
                 "non-finite velocity at step " + std::to_string(r->step) + ": the run appears to have blown up");
-  if (dt) *dt = cfl_dt(r);
+  double D = 0.0;
+  if (int rc = cfl_dt(r, &D)) return rc;
+  if (dt) *dt = D;
   return GBGHT_OK;
 }
 
@@ -423,8 +509,33 @@ int gbght_tracers_import(gbght_run* r, const double* X) {
   if (!X) return fail(r, GBGHT_ERR_ARGUMENT, "X is null");
   int rc = engine_call(r, r->eng->tracers_set(X));
   if (rc) return rc;
-  r->sample_valid = false;
+  r->trail_count = 0;   // new positions: the trail starts again
+  r->trail_newest = -1;
+  r->sampled = false;
   r->sample_at_positions = false;
+  return GBGHT_OK;
+}
+
+int gbght_tracer_trail_reset(gbght_run* r) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (r->cfg.tracers <= 0) return fail(r, GBGHT_ERR_ARGUMENT, "the run was built without tracers");
+  r->trail_count = 0;
+  r->trail_newest = -1;
+  r->sampled = false;
+  r->sample_at_positions = false;
+  return GBGHT_OK;
+}
+
+int gbght_tracer_sample_restore(gbght_run* r, const double* values, double t) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (r->cfg.tracers <= 0) return fail(r, GBGHT_ERR_ARGUMENT, "the run was built without tracers");
+  if (!values) return fail(r, GBGHT_ERR_ARGUMENT, "values is null");
+  if (!std::isfinite(t)) return fail(r, GBGHT_ERR_ARGUMENT, "the sample time must be finite");
+  if (r->trail_count > 0 && !(t > trail_newest_time(r)))
+    return fail(r, GBGHT_ERR_ARGUMENT, "the sample time must be later than the previous sample's");
+  int rc = engine_call(r, r->eng->tracer_sample_set(values, trail_next(r)));
+  if (rc) return rc;
+  trail_push(r, t);
   return GBGHT_OK;
 }
 
@@ -438,11 +549,11 @@ int gbght_tracers_export(gbght_run* r, double* X) {
 int gbght_tracer_sample_export(gbght_run* r, double* values, double* t) {
   if (check_run(r)) return GBGHT_ERR_ARGUMENT;
   if (r->cfg.tracers <= 0) return fail(r, GBGHT_ERR_ARGUMENT, "the run was built without tracers");
-  if (!r->sample_valid) return fail(r, GBGHT_ERR_SCHEDULE, "the trail holds no sample yet");
+  if (r->trail_count == 0) return fail(r, GBGHT_ERR_SCHEDULE, "the trail holds no sample yet");
   if (!r->sample_at_positions)
     return fail(r, GBGHT_ERR_SCHEDULE, "the trail is stale: the positions moved since its newest sample");
-  if (t) *t = r->sample_time;
-  return values ? engine_call(r, r->eng->tracer_sample_get(values)) : GBGHT_OK;
+  if (t) *t = trail_newest_time(r);
+  return values ? engine_call(r, r->eng->tracer_sample_get(values, r->trail_newest)) : GBGHT_OK;
 }
 
 static int advect_checks(gbght_run* r, double dt) {
@@ -451,7 +562,7 @@ static int advect_checks(gbght_run* r, double dt) {
     return fail(r, GBGHT_ERR_ARGUMENT,
                 "`dt` must be positive and finite, got " + std::to_string(dt) +
                     ": the samples a particle scheme integrates over must lie at increasing times");
-  if (!r->sample_valid || !r->sample_at_positions)
+  if (r->trail_count == 0 || !r->sample_at_positions)
     return fail(r, GBGHT_ERR_SCHEDULE, "the trail's newest sample was not taken at the current positions");
   if (int rc = require_deposit(r, "advect")) return rc;
   if (r->fields_epoch != r->sample_epoch + 1)
@@ -463,7 +574,7 @@ static int advect_checks(gbght_run* r, double dt) {
 int gbght_advect(gbght_run* r, double dt) {
   if (check_run(r)) return GBGHT_ERR_ARGUMENT;
   if (int rc = advect_checks(r, dt)) return rc;
-  int rc = engine_call(r, r->eng->tracers_run(1, gbght::heun_weights(dt)));
+  int rc = engine_call(r, r->eng->tracers_run(adams_step(r, dt)));
   if (rc) return rc;
   rc = engine_call(r, r->eng->sync());
   if (rc) return rc;
@@ -476,22 +587,24 @@ int gbght_deposit_tracers(gbght_run* r, double t) {
   if (r->cfg.tracers <= 0) return fail(r, GBGHT_ERR_ARGUMENT, "the cache was built without tracers");
   if (!std::isfinite(t)) return fail(r, GBGHT_ERR_ARGUMENT, "the sample time must be finite");
   if (int rc = require_deposit(r, "deposit (particles)")) return rc;
-  if (r->sample_valid) {
-    if (!(t > r->sample_time))
-      return fail(r, GBGHT_ERR_ARGUMENT, "the sample time must be later than the previous sample's");
+  if (r->trail_count > 0 && !(t > trail_newest_time(r)))
+    return fail(r, GBGHT_ERR_ARGUMENT, "the sample time must be later than the previous sample's");
+  if (r->sampled) {
     if (r->sample_at_positions)
       return fail(r, GBGHT_ERR_SCHEDULE, "a second sample at the same positions: advance the tracers first");
     if (r->fields_epoch != r->sample_epoch + 1)
       return fail(r, GBGHT_ERR_SCHEDULE, "the fields and the tracer positions belong to different times");
   }
-  int rc = engine_call(r, r->eng->tracers_run(0, gbght::HeunWeights{0, 0, 0}));
+  gbght::AdamsStep w{};   // the gather alone, into the trail's next slot
+  w.out_slot = trail_next(r);
+  int rc = engine_call(r, r->eng->tracers_run(w));
   if (rc) return rc;
   rc = engine_call(r, r->eng->sync());
   if (rc) return rc;
-  r->sample_valid = true;
+  trail_push(r, t);
+  r->sampled = true;
   r->sample_at_positions = true;
   r->sample_epoch = r->fields_epoch;
-  r->sample_time = t;
   return GBGHT_OK;
 }
 
@@ -505,12 +618,17 @@ int gbght_interpolate_velocity(gbght_run* r, const double* X, int64_t M, double*
 int gbght_advance(gbght_run* r, double dt, double* dt_taken) {
   if (check_run(r)) return GBGHT_ERR_ARGUMENT;
   if (int rc = require_deposit(r, "advance")) return rc;
+  if (dt > 0 && r->cfg.shortened_first_steps && r->cfg.tracers > 0 && r->cfg.tracer_steps > 1)
+    return fail(r, GBGHT_ERR_ARGUMENT,
+                "this run was built with `shortened_first_steps`, which chooses the timestep itself while the "
+                "particle scheme starts, and a fixed `dt` was given: drop `dt`, or build the run without "
+                "`shortened_first_steps`");
   double D = dt;
   if (!(dt > 0)) {
     if (!std::isfinite(r->max_speed))
       return fail(r, GBGHT_ERR_SCHEDULE, "non-finite velocity at step " + std::to_string(r->step) +
                                              ": the run appears to have blown up");
-    D = cfl_dt(r);
+    if (int rc = cfl_dt(r, &D)) return rc;
   }
   if (!finite_positive(D))
     return fail(r, GBGHT_ERR_ARGUMENT, "the timestep must be positive and finite, got " + std::to_string(D));
@@ -518,7 +636,7 @@ int gbght_advance(gbght_run* r, double dt, double* dt_taken) {
   if (!(t_new > r->time))
     return fail(r, GBGHT_ERR_ARGUMENT, "the timestep is too small to advance the clock");
   const bool tracers = r->cfg.tracers > 0;
-  if (tracers && (!r->sample_valid || !r->sample_at_positions))
+  if (tracers && (r->trail_count == 0 || !r->sample_at_positions))
     return fail(r, GBGHT_ERR_SCHEDULE, "the tracers' last push was never closed by a particle deposit");
   if (tracers && r->sample_epoch != r->fields_epoch)
     return fail(r, GBGHT_ERR_SCHEDULE, "the fields were stepped alone since the tracers' last sample");
@@ -529,10 +647,12 @@ int gbght_advance(gbght_run* r, double dt, double* dt_taken) {
   if ((rc = do_deposit(r))) return rc;
   if (tracers) {
     // push and closing particle deposit in one launch; the same functions as advect + deposit
-    rc = engine_call(r, r->eng->tracers_run(2, gbght::heun_weights(D)));
+    gbght::AdamsStep w = adams_step(r, D);
+    w.out_slot = trail_next(r);
+    rc = engine_call(r, r->eng->tracers_run(w));
     if (rc) return rc;
+    trail_push(r, t_new);
     r->sample_epoch = r->fields_epoch;
-    r->sample_time = t_new;
     r->sample_at_positions = true;
   }
   if (!std::isfinite(r->max_speed))

@@ -190,7 +190,8 @@ class EngineImpl final : public Engine {
     if (p.tracers > 0) {
       if (p.tracers > int64_t(UINT32_MAX)) return "too many tracers for a 32-bit traversal order";
       if ((err = alloc(&X_, 3 * size_t(p.tracers) * sizeof(double)))) return err;
-      if ((err = alloc(&F_, 3 * size_t(p.tracers) * sizeof(double)))) return err;
+      if (p.trail_capacity < 1 || p.trail_capacity > kTrailMax) return "bad trail capacity";
+      if ((err = alloc(&F_, size_t(p.trail_capacity) * 3 * size_t(p.tracers) * sizeof(double)))) return err;
       const size_t nt = size_t(traversal_tiles(N));
       nbins_ = int(nt * nt * nt);
       if ((err = alloc(&tkey_, size_t(p.tracers) * sizeof(uint32_t)))) return err;
@@ -457,14 +458,26 @@ class EngineImpl final : public Engine {
     if (!X_) return "the run carries no tracers";
     return rt_d2h(X, X_, 3 * size_t(p_.tracers) * sizeof(double), stream_);
   }
-  const char* tracer_sample_get(double* F) override {
+  const char* tracer_sample_get(double* F, int slot) override {
     if (!F_) return "the run carries no tracers";
-    return rt_d2h(F, F_, 3 * size_t(p_.tracers) * sizeof(double), stream_);
+    if (slot < 0 || slot >= p_.trail_capacity) return "no such trail slot";
+    const size_t n = 3 * size_t(p_.tracers);
+    return rt_d2h(F, F_ + size_t(slot) * n, n * sizeof(double), stream_);
   }
-  const char* tracers_run(int mode, HeunWeights w) override {
+  const char* tracer_sample_set(const double* F, int slot) override {
+    if (!F_) return "the run carries no tracers";
+    if (slot < 0 || slot >= p_.trail_capacity) return "no such trail slot";
+    const size_t n = 3 * size_t(p_.tracers);
+    const char* err = rt_h2d(F_ + size_t(slot) * n, F, n * sizeof(double), stream_);
+    return err ? err : rt_sync(stream_);
+  }
+  const char* tracers_run(const AdamsStep& w) override {
     if (!X_) return "the run carries no tracers";
+    if (w.J < 0 || w.J > p_.trail_capacity || w.out_slot >= p_.trail_capacity) return "bad tracer step";
+    for (int j = 0; j < w.J; ++j)
+      if (w.slot[j] < 0 || w.slot[j] >= p_.trail_capacity) return "bad tracer step";
     if (const char* e = rebuild_traversal()) return e;
-    run_tracers(p_.tracers, mode, X_, F_, w, torder_);
+    run_tracers(p_.tracers, X_, F_, w, torder_);
     return rt_check();
   }
   const char* gather(const double* X, int64_t M, double* out) override {
@@ -474,7 +487,8 @@ class EngineImpl final : public Engine {
     if (!err) err = rt_alloc(reinterpret_cast<void**>(&dF), 3 * size_t(M) * sizeof(double));
     if (!err) err = rt_h2d(dX, X, 3 * size_t(M) * sizeof(double), stream_);
     if (!err) {
-      run_tracers(M, 0, dX, dF, HeunWeights{0, 0, 0});
+      AdamsStep w{};   // a gather alone, into slot 0 of a one-slot trail
+      run_tracers(M, dX, dF, w);
       err = rt_check();
     }
     if (!err) err = rt_d2h(out, dF, 3 * size_t(M) * sizeof(double), stream_);
@@ -956,13 +970,13 @@ class EngineImpl final : public Engine {
     }
     return rt_check();
   }
-  void run_tracers(int64_t M, int mode, double* X, double* F, HeunWeights w, const uint32_t* order = nullptr) {
+  void run_tracers(int64_t M, double* X, double* F, const AdamsStep& w, const uint32_t* order = nullptr) {
 #ifdef GBGHT_EMU
-    for (int64_t i = 0; i < M; ++i) tracer_one<T>(order ? int64_t(order[i]) : i, M, mode, U_, N, p_.L, X, F, w);
+    for (int64_t i = 0; i < M; ++i) tracer_one<T>(order ? int64_t(order[i]) : i, M, U_, N, p_.L, X, F, w);
 #else
     const int bs = 128;
     pbegin(PROF_TRACERS);
-    k_tracers<T><<<unsigned((M + bs - 1) / bs), bs, 0, stream_>>>(M, mode, U_, N, p_.L, X, F, w, order);
+    k_tracers<T><<<unsigned((M + bs - 1) / bs), bs, 0, stream_>>>(M, U_, N, p_.L, X, F, w, order);
     pend();
 #endif
   }

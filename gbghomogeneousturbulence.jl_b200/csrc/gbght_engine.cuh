@@ -48,6 +48,7 @@ struct RunParams {
   ForcingParams sf;          // scalar forcing (kind 0 when the run carries no scalar)
   double G[3];
   int64_t tracers;
+  int trail_capacity;        // sample slots of the tracers' trail (the Adams scheme's k)
   int device;
 };
 
@@ -73,9 +74,10 @@ class Engine {
   virtual const char* spectrum(int which, double* out, int nshell) = 0;
   virtual const char* tracers_set(const double* X) = 0;
   virtual const char* tracers_get(double* X) = 0;
-  virtual const char* tracer_sample_get(double* F) = 0;
+  virtual const char* tracer_sample_get(double* F, int slot) = 0;
+  virtual const char* tracer_sample_set(const double* F, int slot) = 0;
   // mode 0: sample at the positions; 1: Heun push; 2: Heun push + sample at the new positions
-  virtual const char* tracers_run(int mode, HeunWeights w) = 0;
+  virtual const char* tracers_run(const AdamsStep& w) = 0;
   virtual const char* gather(const double* X, int64_t M, double* out) = 0;
   virtual const char* sync() = 0;
   // CUDA-event timing on the run's stream: per-kernel launch counts and total milliseconds while

@@ -244,10 +244,10 @@ __global__ void __launch_bounds__(NT) k_spectrum(Geometry g, const Cplx<T>* S, i
   body_spectrum<T, NT>(c, hist, hist + nshell, g, S, c0, nc, nshell, out);
 }
 template <class T>
-__global__ void k_tracers(int64_t M, int mode, const T* u, int N, double L, double* X, double* F, HeunWeights w,
+__global__ void k_tracers(int64_t M, const T* u, int N, double L, double* X, double* F, const __grid_constant__ AdamsStep w,
                           const uint32_t* order) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i < M) tracer_one<T>(order ? int64_t(order[i]) : i, M, mode, u, N, L, X, F, w);
+  if (i < M) tracer_one<T>(order ? int64_t(order[i]) : i, M, u, N, L, X, F, w);
 }
 
 // The traversal rebuild, a counting sort by tile: keys and tile counts, an exclusive scan of the

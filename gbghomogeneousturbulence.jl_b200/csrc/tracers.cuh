@@ -124,35 +124,55 @@ GBGHT_HD uint32_t traversal_key(const double* GBGHT_RESTRICT X, int64_t p, int64
   return (uint32_t(i[2] >> 3) * T + uint32_t(i[1] >> 3)) * T + uint32_t(i[0] >> 3);
 }
 
-struct HeunWeights {
-  double b0;      // predictor weight on f₀
-  double beta0;   // corrector weight on f*
-  double beta1m;  // corrector weight on f₀, β₁ − b₀
+// One step of the Adams family for every tracer (src/ParticlePropagator.jl:282-307): the
+// predictor X* = X + Σ_j b_j f_{n−j} over J samples of the trail, and, when corrected (ABM),
+// X ← X* + β*·f* + Σ_j (β_{j+1} − b_j) f_{n−j} with f* gathered at X*. J = 0 moves nothing.
+// The trail is a ring of sample slots [slot][3][M]; out_slot ≥ 0 receives the sample at the new
+// positions (the closing particle deposit, or a gather alone when J = 0).
+constexpr int kTrailMax = 8;
+struct AdamsStep {
+  int J;                    // samples the predictor integrates over (0: no push)
+  int corrected;            // gather f* at X* and correct
+  int out_slot;             // slot of the sample at the new positions; −1: none
+  int slot[kTrailMax];      // ring slot of f_{n−j}, j = 0 the newest
+  double b[kTrailMax];      // predictor weights
+  double beta_star;         // corrector weight on f*
+  double beta_m[kTrailMax]; // corrector weights β_{j+1} − b_j
 };
 
-// One tracer: gather only (mode 0), Heun push (mode 1), or Heun push then the particle deposit
-// gather at the new position (mode 2). X and F are [3][M].
+// One tracer. X is [3][M]; F is the trail's slots, 3·M doubles apart. Each displacement is summed
+// term by term in the weights' order, then added, and the position wrapped into [0, L).
 template <class T>
-GBGHT_HD void tracer_one(int64_t p, int64_t M, int mode, const T* GBGHT_RESTRICT u, int N, double L,
-                         double* GBGHT_RESTRICT X, double* GBGHT_RESTRICT F, HeunWeights w) {
+GBGHT_HD void tracer_one(int64_t p, int64_t M, const T* GBGHT_RESTRICT u, int N, double L,
+                         double* GBGHT_RESTRICT X, double* GBGHT_RESTRICT F, const AdamsStep& w) {
   const double dx = div_rn(L, double(N));
+  const size_t S3 = 3 * size_t(M);
   double x[3] = {X[p], X[M + p], X[2 * M + p]};
-  double f[3];
-  if (mode != 0) {
-    const double f0[3] = {F[p], F[M + p], F[2 * M + p]};
+  if (w.J > 0) {
+    double disp[3];
+    for (int c = 0; c < 3; ++c) disp[c] = mul_rn(w.b[0], F[size_t(w.slot[0]) * S3 + size_t(c) * M + p]);
+    for (int j = 1; j < w.J; ++j)
+      for (int c = 0; c < 3; ++c)
+        disp[c] = add_rn(disp[c], mul_rn(w.b[j], F[size_t(w.slot[j]) * S3 + size_t(c) * M + p]));
     double xs[3];
-    for (int c = 0; c < 3; ++c) xs[c] = wrap_periodic(add_rn(x[c], mul_rn(w.b0, f0[c])), L);
-    double fs[3];
-    gather3(u, N, dx, xs[0], xs[1], xs[2], fs);
-    for (int c = 0; c < 3; ++c) {
-      const double disp = add_rn(mul_rn(w.beta0, fs[c]), mul_rn(w.beta1m, f0[c]));
-      x[c] = wrap_periodic(add_rn(xs[c], disp), L);
-      X[c * M + p] = x[c];
+    for (int c = 0; c < 3; ++c) xs[c] = wrap_periodic(add_rn(x[c], disp[c]), L);
+    if (w.corrected) {
+      double fs[3];
+      gather3(u, N, dx, xs[0], xs[1], xs[2], fs);
+      for (int c = 0; c < 3; ++c) disp[c] = mul_rn(w.beta_star, fs[c]);
+      for (int j = 0; j < w.J; ++j)
+        for (int c = 0; c < 3; ++c)
+          disp[c] = add_rn(disp[c], mul_rn(w.beta_m[j], F[size_t(w.slot[j]) * S3 + size_t(c) * M + p]));
+      for (int c = 0; c < 3; ++c) x[c] = wrap_periodic(add_rn(xs[c], disp[c]), L);
+    } else {
+      for (int c = 0; c < 3; ++c) x[c] = xs[c];
     }
-    if (mode == 1) return;
+    for (int c = 0; c < 3; ++c) X[c * M + p] = x[c];
   }
+  if (w.out_slot < 0) return;
+  double f[3];
   gather3(u, N, dx, x[0], x[1], x[2], f);
-  for (int c = 0; c < 3; ++c) F[c * M + p] = f[c];
+  for (int c = 0; c < 3; ++c) F[size_t(w.out_slot) * S3 + size_t(c) * M + p] = f[c];
 }
 
 // 4-point Gauss–Legendre Adams weights (src/ParticlePropagator.jl:263-280), host side.
@@ -176,18 +196,21 @@ inline void adams_weights(const double* nodes, int n, double h, double* out) {
   }
 }
 
-inline HeunWeights heun_weights(double h) {
-  HeunWeights w;
-  const double n1[1] = {0.0};
-  double b[1];
-  adams_weights(n1, 1, h, b);
-  const double n2[2] = {h, 0.0};
-  double beta[2];
-  adams_weights(n2, 2, h, beta);
-  w.b0 = b[0];
-  w.beta0 = beta[0];
-  w.beta1m = beta[1] - b[0];
-  return w;
+// The step's weights from the trail's sample times (newest first, at most kTrailMax): the
+// predictor through the nodes t_{n−j} − t_n, the corrector through (h, nodes…).
+inline void adams_step_weights(const double* times, int J, double h, bool corrected, AdamsStep* w) {
+  double nodes[kTrailMax + 1];
+  for (int j = 0; j < J; ++j) nodes[j] = times[j] - times[0];
+  adams_weights(nodes, J, h, w->b);
+  w->J = J;
+  w->corrected = corrected ? 1 : 0;
+  if (!corrected) return;
+  double with_end[kTrailMax + 1], beta[kTrailMax + 1];
+  with_end[0] = h;
+  for (int j = 0; j < J; ++j) with_end[j + 1] = nodes[j];
+  adams_weights(with_end, J + 1, h, beta);
+  w->beta_star = beta[0];
+  for (int j = 0; j < J; ++j) w->beta_m[j] = beta[j + 1] - w->b[j];
 }
 
 }  // namespace gbght

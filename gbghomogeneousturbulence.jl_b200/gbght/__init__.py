@@ -27,6 +27,7 @@ IFRK4, IFRK3, IFHEUN, IFSSPRK3 = 0, 1, 2, 3
 SCHEMES = {"IFLowStorageRK4": IFRK4, "IFLowStorageRK3": IFRK3, "IFHeun": IFHEUN, "IFSSPRK3": IFSSPRK3}
 FORCING_NONE, FORCING_CONSTANT_POWER, FORCING_LINEAR, FORCING_VARIANCE_CONTROLLER, FORCING_VARIANCE_RESCALING = 0, 1, 2, 3, 4
 OVER = {"band": 0, "total": 1}
+TRACER_SCHEMES = {"Heun": 0, "ABM": 1, "AB": 2}
 OK, ERR_ARGUMENT, ERR_SCHEDULE, ERR_CUDA, ERR_DEVICE = 0, 1, 2, 3, 4
 
 
@@ -67,6 +68,9 @@ class Config(C.Structure):
         ("cfl", C.c_double),
         ("max_dt", C.c_double),
         ("device", C.c_int),
+        ("tracer_scheme", C.c_int),
+        ("tracer_steps", C.c_int),
+        ("shortened_first_steps", C.c_int),
     ]
 
 
@@ -94,6 +98,8 @@ _SIGNATURES = {
     "gbght_tracers_import": (C.c_int, [C.c_void_p, _DP]),
     "gbght_tracers_export": (C.c_int, [C.c_void_p, _DP]),
     "gbght_tracer_sample_export": (C.c_int, [C.c_void_p, _DP, _DP]),
+    "gbght_tracer_trail_reset": (C.c_int, [C.c_void_p]),
+    "gbght_tracer_sample_restore": (C.c_int, [C.c_void_p, _DP, C.c_double]),
     "gbght_advect": (C.c_int, [C.c_void_p, C.c_double]),
     "gbght_deposit_tracers": (C.c_int, [C.c_void_p, C.c_double]),
     "gbght_interpolate_velocity": (C.c_int, [C.c_void_p, _DP, C.c_int64, _DP]),
@@ -215,6 +221,9 @@ class Setup:
     precision: str = "fp64"          # "fp64" or "fp32_mixed"
     scheme: str = "IFLowStorageRK4"  # or "IFLowStorageRK3", "IFHeun", "IFSSPRK3"
     tracers: int = 0
+    tracer_scheme: str = "Heun"      # "Heun" (= ABM(1)), "ABM" or "AB" (src/ParticlePropagator.jl)
+    tracer_steps: int = 1            # k of ABM(k) / AB(k)
+    shortened_first_steps: bool = False
     cfl: float = 0.5
     max_dt: float = math.inf
     device: int = 0
@@ -243,6 +252,11 @@ class Run:
         for i in range(3):
             cfg.mean_gradient[i] = float(setup.mean_gradient[i])
         cfg.tracers = int(setup.tracers)
+        if setup.tracer_scheme not in TRACER_SCHEMES:
+            raise ValueError(f"unknown particle integration scheme {setup.tracer_scheme!r}")
+        cfg.tracer_scheme = TRACER_SCHEMES[setup.tracer_scheme]
+        cfg.tracer_steps = int(setup.tracer_steps)
+        cfg.shortened_first_steps = 1 if setup.shortened_first_steps else 0
         cfg.cfl = float(setup.cfl)
         cfg.max_dt = float(setup.max_dt)
         cfg.device = int(setup.device)
@@ -381,6 +395,17 @@ class Run:
         t = C.c_double()
         self._check(self.lib.gbght_tracer_sample_export(self.h, _ptr(F), C.byref(t)))
         return F, t.value
+
+    def reset_tracer_trail(self):
+        """`reset_velocity_at_particles!` (src/Cache.jl:382-386)."""
+        self._check(self.lib.gbght_tracer_trail_reset(self.h))
+
+    def restore_tracer_sample(self, values: np.ndarray, t: float):
+        """`restore_velocity_at_particles!` (src/Cache.jl:388-389): push an earlier sample."""
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        if a.shape != (3, self.setup.tracers):
+            raise ValueError(f"a sample must have shape (3, {self.setup.tracers})")
+        self._check(self.lib.gbght_tracer_sample_restore(self.h, _ptr(a), float(t)))
 
     def advect(self, dt: float):
         self._check(self.lib.gbght_advect(self.h, float(dt)))

@@ -79,7 +79,11 @@ typedef struct gbght_forcing_params {
   double highest_shell;   /* ≥ lowest_shell */
 } gbght_forcing_params;
 
-enum gbght_tracer_scheme { GBGHT_HEUN = 0 };
+/* The particle integration schemes (src/ParticlePropagator.jl:48-256): Heun = ABM(1); ABM(k),
+ * k = 1..7, the k-step Adams–Bashforth–Moulton predictor–corrector of order k + 1; AB(k), k = 1..8,
+ * the k-step Adams–Bashforth of order k. The weights are re-solved every step from the samples'
+ * times; while the trail holds fewer than k samples the step is ABM(samples held). */
+enum gbght_tracer_scheme { GBGHT_HEUN = 0, GBGHT_ABM = 1, GBGHT_AB = 2 };
 
 /* Device status bits (gbght_status_word). */
 #define GBGHT_STATUS_NONFINITE_SPEED 0x1u
@@ -101,11 +105,15 @@ typedef struct gbght_config {
   double cfl;                /* C of the advective CFL rule */
   double max_dt;             /* caller's ceiling on Δt (INFINITY = none) */
   int device;                /* CUDA device ordinal */
+  int tracer_scheme;         /* gbght_tracer_scheme */
+  int tracer_steps;          /* k of ABM(k) / AB(k); 1 for Heun. The trail keeps k samples */
+  int shortened_first_steps; /* 1: shorten the first steps while a k > 1 scheme's trail fills
+                                (src/SimulationRun.jl:1099-1132); a fixed dt is then refused */
 } gbght_config;
 
 /* Fill `cfg` with the defaults: N=64, L=2π, FP64, IF-RK4, ν=0.01, Sc=1, scalar on, no forcing
  * of either field (each forcing block: rate 0, target 0, gain 1, turnover time 0, over = band,
- * shells 1–2), G=0, no tracers, CFL 0.5, max_dt=∞, device 0. */
+ * shells 1–2), G=0, no tracers, Heun, no shortened start, CFL 0.5, max_dt=∞, device 0. */
 void gbght_config_default(gbght_config* cfg);
 
 /* Build a run on a FixedDomain with TwoThirds dealiasing, with its generator and registers.
@@ -187,10 +195,18 @@ int gbght_tracers_export(gbght_run* run, double* X);
  * velocity_at_particles_trail (src/Cache.jl). */
 int gbght_tracer_sample_export(gbght_run* run, double* values, double* t);
 
-/* Advance the tracers one Heun (= ABM(1)) step of size dt through the deposited velocity. The
- * step requires the newest trail sample to be at the current positions, and the fields to be
- * exactly one step ahead of it; otherwise SCHEDULE. Replaces advect!(Heun(), tracers, domain,
- * cache, dt; traversal) (src/ParticlePropagator.jl:288-372). */
+/* Empty the trail, and push an earlier sample [3][M] at time t (later than the newest held) without
+ * moving the tracers or pairing the epochs: a checkpoint's restore of the samples a multistep
+ * scheme integrates over, before the ordinary particle deposit adds the newest. Replaces
+ * reset_velocity_at_particles! and restore_velocity_at_particles! (src/Cache.jl:380-389). */
+int gbght_tracer_trail_reset(gbght_run* run);
+int gbght_tracer_sample_restore(gbght_run* run, const double* values, double t);
+
+/* Advance the tracers one step of size dt of the configured particle scheme (Heun, ABM(k), AB(k))
+ * through the deposited velocity and the trail's samples. The step requires the newest trail sample
+ * to be at the current positions, and the fields to be exactly one step ahead of it; otherwise
+ * SCHEDULE. Replaces advect!(scheme, tracers, domain, cache, dt; traversal)
+ * (src/ParticlePropagator.jl:282-352). */
 int gbght_advect(gbght_run* run, double dt);
 
 /* The particle deposit: sample the deposited velocity at the tracers, labelled with time t.

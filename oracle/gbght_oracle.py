@@ -607,6 +607,43 @@ def interpolate(dom: Domain, f: np.ndarray, X: np.ndarray) -> np.ndarray:
     return out[0] if scalar else out
 
 
+def advect_adams(dom: Domain, X: np.ndarray, samples, times, u_new: np.ndarray, h: float, corrected: bool):
+    """One step of the Adams family (`_advance_positions!`, src/ParticlePropagator.jl:282-307) over
+    the J samples f_{n−j} (newest first) taken at `times` (newest first): the predictor
+    X* = wrap(X + Σ_j b_j f_{n−j}) with b the weights through the nodes t_{n−j} − t_n, and, when
+    corrected, X ← wrap(X* + (β* f* + Σ_j (β_{j+1} − b_j) f_{n−j})) with f* = u(X*) and β the
+    weights through (h, nodes…). Each displacement is summed term by term, then added.
+    Returns the new positions and f* (None when not corrected)."""
+    J = len(samples)
+    nodes = tuple(times[j] - times[0] for j in range(J))
+    b = adams_weights(nodes, h)
+    disp = b[0] * samples[0]
+    for j in range(1, J):
+        disp = disp + b[j] * samples[j]
+    Xs = wrap(X + disp, dom.L)
+    if not corrected:
+        return Xs, None
+    fstar = interpolate(dom, u_new, Xs)
+    beta = adams_weights((h,) + nodes, h)
+    disp = beta[0] * fstar
+    for j in range(J):
+        disp = disp + (beta[j + 1] - b[j]) * samples[j]
+    return wrap(Xs + disp, dom.L), fstar
+
+
+TRACER_STEPS_MAX = {"abm": 7, "ab": 8}
+
+
+def tracer_order(scheme: str, k: int) -> int:
+    """`_order_of_accuracy` (src/ParticlePropagator.jl:255-256): k + 1 for ABM(k), k for AB(k)."""
+    return k + 1 if scheme == "abm" else k
+
+
+def startup_growth(order: int) -> float:
+    """`_startup_growth` (src/SimulationRun.jl:1117)."""
+    return 2.0 if order <= 5 else 1.5 if order <= 7 else 1.25
+
+
 def advect_heun(dom: Domain, X: np.ndarray, f0: np.ndarray, u_new: np.ndarray, h: float):
     """Heun = ABM(1) (src/ParticlePropagator.jl:165,288-315): X* = wrap(X + b₀f₀); f* = u(X*);
     X ← wrap(X* + (β₀f* + (β₁ − b₀)f₀)). Each displacement is summed term by term, then added."""
@@ -684,17 +721,42 @@ class Run:
     nstep: int = 0
     u: np.ndarray = field(default=None, repr=False)
     speed: float = 0.0
-    f0: np.ndarray | None = None
-    trail_time: float = 0.0
+    tracer_scheme: tuple = ("abm", 1)  # ("abm", k) = ABM(k), Heun = ABM(1); ("ab", k) = AB(k)
+    shortened_first_steps: bool = False
+    trail: list = field(default_factory=list, repr=False)   # (time, value), newest first
 
     def __post_init__(self):
         self.u, _, _, self.speed = deposit(self.dom, self.state)
         if self.X is not None:
-            self.f0 = interpolate(self.dom, self.u, self.X)
-            self.trail_time = self.time
+            self.trail = [(self.time, interpolate(self.dom, self.u, self.X))]
+
+    @property
+    def f0(self):
+        return self.trail[0][1]
+
+    @property
+    def trail_time(self):
+        return self.trail[0][0]
+
+    def startup_bound(self, dt: float) -> float:
+        """`_startup_bound` (src/SimulationRun.jl:1119-1132)."""
+        kind, k = self.tracer_scheme
+        if not (self.shortened_first_steps and self.X is not None and k > 1):
+            return math.inf
+        order = tracer_order(kind, k)
+        if len(self.trail) > 1:
+            return startup_growth(order) * (self.trail[0][0] - self.trail[1][0])
+        nu = self.cond.viscosity
+        eps = dissipation(self.dom, self.state.uh, nu)
+        tau = math.sqrt(nu / eps) if eps > 0 else math.inf
+        return tau * (dt / tau) ** (order / 3) if (math.isfinite(tau) and tau > 0) else math.inf
+
+    def timestep(self) -> float:
+        base = cfl_timestep(self.dom, self.cond, self.speed, self.cfl, self.max_dt)
+        return min(self.startup_bound(base), base)
 
     def advance(self, dt: float | None = None):
-        D = cfl_timestep(self.dom, self.cond, self.speed, self.cfl, self.max_dt) if dt is None else float(dt)
+        D = self.timestep() if dt is None else float(dt)
         if not (math.isfinite(D) and D > 0):
             raise ValueError(f"the timestep must be positive and finite, got {D}")
         t_new = self.time + D
@@ -703,9 +765,16 @@ class Run:
         self.state = step(self.dom, self.cond, self.state, D, self.scheme)
         self.u, _, _, self.speed = deposit(self.dom, self.state)
         if self.X is not None:
-            self.X, _ = advect_heun(self.dom, self.X, self.f0, self.u, D)
-            self.f0 = interpolate(self.dom, self.u, self.X)
-            self.trail_time = t_new
+            kind, k = self.tracer_scheme
+            capacity = k
+            if len(self.trail) >= k:
+                J, corrected = k, kind == "abm"
+            else:
+                J, corrected = len(self.trail), True
+            samples = [v for _, v in self.trail[:J]]
+            times = [t for t, _ in self.trail[:J]]
+            self.X, _ = advect_adams(self.dom, self.X, samples, times, self.u, D, corrected)
+            self.trail = [(t_new, interpolate(self.dom, self.u, self.X))] + self.trail[:capacity - 1]
         if not math.isfinite(self.speed):
             raise FloatingPointError(f"non-finite velocity at step {self.nstep + 1}")
         if self.state.phih is not None and not math.isfinite(scalar_variance(self.dom, self.state.phih)):

@@ -123,6 +123,22 @@ def test_heun_and_ssprk3(cuda_library, scheme, N, precision, steps):
         compare(run, orun, tol=1e-5, check_tracers=False)
 
 
+@pytest.mark.parametrize("scheme,shortened", [(("AB", 4), False), (("ABM", 3), True), (("AB", 8), True)])
+def test_adams_particle_schemes(cuda_library, scheme, shortened):
+    # AB(k)/ABM(k) tracers on a forced 64³ run: the trail fills through the lower ABM members and,
+    # when shortened, the first steps follow the start-up bound; positions and samples match
+    run, orun = make_case(64, forcing=0.1, tracers=3000, tracer_scheme=scheme, shortened_first_steps=shortened,
+                          library=cuda_library)
+    taken = advance_both(run, orun, 10, dt=None)
+    for d_lib, d_ora in taken:
+        assert d_lib == pytest.approx(d_ora, rel=1e-12)
+    res = compare(run, orun, tol=1e-12)
+    assert res["X_err"] < 1e-10
+    F, t = run.tracer_sample()
+    assert t == pytest.approx(orun.time, rel=1e-12)   # the sum of CFL steps equal to 1e-12
+    assert np.max(np.abs(F - orun.f0)) < 1e-10
+
+
 def test_rescaling_holds_the_target_exactly(cuda_library):
     run, _ = make_case(64, forcing=gbght.VarianceRescaling(0.45, "total"),
                        scalar_forcing=gbght.VarianceRescaling(0.6, "total", 1, math.inf), library=cuda_library)

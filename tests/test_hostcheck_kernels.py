@@ -161,6 +161,75 @@ def test_reality_projection_removes_planted_violation(hostcheck_library):
         assert np.max(np.abs(plane - partner)) == 0.0
 
 
+@pytest.mark.parametrize("scheme", [("AB", 4), ("ABM", 3), ("AB", 8), ("ABM", 7), ("Heun", 1)])
+def test_adams_schemes_in_a_prescribed_straining_flow(hostcheck_library, scheme):
+    # test/particles.jl:46-67 through the library: the straining flow written into the deposit slot,
+    # the trail seeded with the exact earlier samples by the checkpoint restore, then per step the
+    # field at the new time, the particle step and the deposit. Positions equal the oracle's.
+    from test_oracle_known_answers import CENTRE, FREQUENCY, START, STRAIN, _strain_exact, _strain_field
+    N, k = 16, scheme[1]
+    dom = O.Domain(N)
+    run = gbght.Run(gbght.Setup(grid_points_per_axis=N, tracers=1, tracer_scheme=scheme[0], tracer_steps=k),
+                    library=hostcheck_library)
+    X = np.array([[START], [1.0], [1.0]])
+    steps = [2.0 / 48 * (1 + 0.3 * math.sin(7 * (i + 1))) for i in range(24)]
+    run.deposit_prescribed_velocity(_strain_field(dom, 0.0))
+    run.import_tracers(X)
+    trail = []
+    for j in range(k - 1, 0, -1):
+        t = -j * steps[0]
+        v = np.array([[math.cos(FREQUENCY * t) * STRAIN * (_strain_exact(t) - CENTRE)], [0.0], [0.0]])
+        run.restore_tracer_sample(v, t)
+        trail.insert(0, (t, v))
+    run.deposit_tracers(0.0)
+    trail.insert(0, (0.0, O.interpolate(dom, _strain_field(dom, 0.0), X)))
+    kind = "ab" if scheme[0] == "AB" else "abm"
+    t = 0.0
+    for h in steps:
+        u = _strain_field(dom, t + h)
+        run.deposit_prescribed_velocity(u)
+        run.advect(h)
+        t += h
+        run.deposit_tracers(t)
+        J, corrected = (k, kind == "abm") if len(trail) >= k else (len(trail), True)
+        X, _ = O.advect_adams(dom, X, [v for _, v in trail[:J]], [tt for tt, _ in trail[:J]], u, h, corrected)
+        trail = [(t, O.interpolate(dom, u, X))] + trail[:k - 1]
+        assert np.max(np.abs(run.tracers() - X)) < 1e-14
+        F, tf = run.tracer_sample()
+        assert tf == t and np.max(np.abs(F - trail[0][1])) < 1e-14
+    assert abs(X[0, 0] - _strain_exact(t)) < 1e-4
+
+
+@pytest.mark.parametrize("scheme,shortened", [(("AB", 4), False), (("ABM", 3), True), (("AB", 6), True)])
+def test_adams_run_matches_oracle(hostcheck_library, scheme, shortened):
+    # advance! with a multistep particle scheme on a forced flow: the trail fills through the lower
+    # ABM members, and under shortened_first_steps the first steps follow the start-up bound
+    run, orun = make_case(16, forcing=0.1, tracers=24, tracer_scheme=scheme, shortened_first_steps=shortened,
+                          library=hostcheck_library)
+    taken = advance_both(run, orun, 8, dt=None)
+    for d_lib, d_ora in taken:
+        assert d_lib == pytest.approx(d_ora, rel=1e-13)
+    if shortened:
+        assert taken[0][0] < 0.7 * taken[-1][0]   # the start is shortened, then grows back
+    res = compare(run, orun, tol=2e-14)
+    assert res["X_err"] < 1e-13
+    if shortened:
+        with pytest.raises(ValueError, match="shortened_first_steps"):
+            run.advance(0.01)
+
+
+def test_particle_scheme_refusals(hostcheck_library):
+    # test/particles.jl:184-192
+    def run(scheme, k):
+        return gbght.Run(gbght.Setup(grid_points_per_axis=16, tracers=4, tracer_scheme=scheme, tracer_steps=k),
+                         library=hostcheck_library)
+    for scheme, k in (("AB", 0), ("AB", 9), ("ABM", 0), ("ABM", 8), ("Heun", 2)):
+        with pytest.raises(ValueError):
+            run(scheme, k)
+    run("AB", 8).close()
+    run("ABM", 7).close()
+
+
 def test_prescribed_uniform_flow_advects_exactly(hostcheck_library):
     # test/particles.jl:94-108 through the prescribed-flow fake (test/prescribed_flow.jl)
     N = 16

@@ -519,6 +519,123 @@ def test_adams_weights_classical():
     assert np.allclose(O.adams_weights(nodes(4), 1.0), np.array([55, -59, 37, -9]) / 24)
     assert np.allclose(O.adams_weights((1.0,) + nodes(1), 1.0), np.array([1, 1]) / 2)
     assert np.allclose(O.adams_weights((1.0,) + nodes(2), 1.0), np.array([5, 8, -1]) / 12)
+    assert np.allclose(O.adams_weights(nodes(3), 1.0), np.array([23, -16, 5]) / 12)
+    assert np.allclose(O.adams_weights((1.0,) + nodes(3), 1.0), np.array([9, 19, -5, 1]) / 24)
+    assert np.allclose(O.adams_weights((1.0,) + nodes(4), 1.0), np.array([251, 646, -264, 106, -19]) / 720)
+    uneven = (0.0, -0.3, -1.2, -1.4)
+    assert sum(O.adams_weights(uneven, 0.7)) == pytest.approx(0.7, rel=1e-14)
+    assert sum(w * x ** 3 for w, x in zip(O.adams_weights(uneven, 0.7), uneven)) == pytest.approx(0.7 ** 4 / 4,
+                                                                                                 rel=1e-12)
+    eight = tuple(-0.37 * i - 0.05 * (i + 1) ** 2 for i in range(8))
+    assert sum(w * x ** 7 for w, x in zip(O.adams_weights(eight, 0.9), eight)) == pytest.approx(0.9 ** 8 / 8,
+                                                                                                rel=1e-8)
+
+
+# The straining flow of test/particles.jl:24-40: u_x = cos(ωt)·s·(x − x_c), reproduced exactly by
+# Catmull–Rom, with the trajectory known in closed form.
+STRAIN, FREQUENCY, CENTRE, START = 1.0, 3.0, math.pi, math.pi + 0.4
+
+
+def _strain_exact(t):
+    return CENTRE + (START - CENTRE) * math.exp(STRAIN * math.sin(FREQUENCY * t) / FREQUENCY)
+
+
+def _strain_field(dom, t):
+    u = np.zeros((3, dom.N, dom.N, dom.N))
+    u[0] = (math.cos(FREQUENCY * t) * STRAIN * (np.arange(dom.N) * dom.dx - CENTRE))[None, None, :]
+    return u
+
+
+def strain_error(scheme, steps, exact_start):
+    """test/particles.jl:46-67: the largest error along a pass; `exact_start` seeds the trail with
+    the exact earlier samples at −h, −2h, … (h the first step)."""
+    kind, k = scheme
+    dom = O.Domain(16)
+    X = np.array([[START], [1.0], [1.0]])
+    trail = []
+    if exact_start:
+        h = steps[0]
+        for j in range(k - 1, 0, -1):
+            t = -j * h
+            trail.insert(0, (t, np.array([[math.cos(FREQUENCY * t) * STRAIN * (_strain_exact(t) - CENTRE)], [0.0], [0.0]])))
+    trail.insert(0, (0.0, O.interpolate(dom, _strain_field(dom, 0.0), X)))
+    t, largest = 0.0, 0.0
+    for h in steps:
+        u = _strain_field(dom, t + h)
+        J, corrected = (k, kind == "abm") if len(trail) >= k else (len(trail), True)
+        X, _ = O.advect_adams(dom, X, [v for _, v in trail[:J]], [tt for tt, _ in trail[:J]], u, h, corrected)
+        t += h
+        trail = [(t, O.interpolate(dom, u, X))] + trail[:k - 1]
+        largest = max(largest, abs(X[0, 0] - _strain_exact(t)))
+    return largest
+
+
+def _uniform(n, T=2.0):
+    return [T / n] * n
+
+
+def _uneven(n, T=2.0):
+    h = np.array([1 + 0.3 * math.sin(7 * (i + 1)) for i in range(n)])
+    return list(h * (T / h.sum()))
+
+
+def _shortened(scheme, n, T=2.0, tau=1 / FREQUENCY):
+    p = O.tracer_order(*scheme)
+    dt = T / n
+    steps, t = [], 0.0
+    while t < T - 1e-12:
+        h = min(dt, tau * (dt / tau) ** (p / 3)) if not steps else min(dt, O.startup_growth(p) * steps[-1])
+        h = min(h, T - t)
+        steps.append(h)
+        t += h
+    return steps
+
+
+def _order(errors):
+    return math.log2(errors[-2] / errors[-1])
+
+
+@pytest.mark.parametrize("steps_of", [_uniform, _uneven], ids=["uniform", "uneven"])
+def test_each_particle_scheme_converges_at_its_order(steps_of):
+    # test/particles.jl:216-231: AB(k) at order k, ABM(k) at order k + 1, from exact earlier samples
+    for scheme in [("ab", k) for k in range(1, 9)] + [("abm", k) for k in range(1, 8)]:
+        p = O.tracer_order(*scheme)
+        counts = (32, 64, 128) if p >= 6 else (64, 128, 256)
+        errors = [strain_error(scheme, steps_of(n), True) for n in counts]
+        assert abs(_order(errors) - p) < 0.5, (scheme, _order(errors))
+    for k in range(1, 8):
+        assert strain_error(("abm", k), _uniform(64), True) < strain_error(("ab", k + 1), _uniform(64), True)
+
+
+def test_particle_startup_orders():
+    # test/particles.jl:233-251: the ordinary start-up leaves a third-order error
+    counts = (64, 128, 256)
+    ref = [strain_error(("abm", 4), _uniform(n), False) for n in counts]
+    assert 2.7 < _order(ref) < 3.3
+    for scheme in (("ab", 6), ("ab", 8), ("abm", 7)):
+        errors = [strain_error(scheme, _uniform(n), False) for n in counts]
+        assert 2.7 < _order(errors) < 3.3
+        assert errors[-1] == pytest.approx(ref[-1], rel=0.05)
+    errors = [strain_error(("ab", 4), _uniform(n), False) for n in counts]
+    assert 2.7 < _order(errors) < 3.5 and ref[-1] / 2 < errors[-1] < 2 * ref[-1]
+    errors = [strain_error(("ab", 2), _uniform(n), False) for n in counts]
+    assert 1.7 < _order(errors) < 2.3
+
+
+def test_shortened_first_steps_restore_the_order():
+    # test/particles.jl:253-271
+    for scheme in [("ab", k) for k in range(3, 9)] + [("abm", k) for k in range(2, 8)]:
+        errors = [strain_error(scheme, _shortened(scheme, n), False) for n in (32, 64, 128)]
+        assert _order(errors) > O.tracer_order(*scheme) - 0.6, scheme
+        assert errors[1] < 4 * strain_error(scheme, _uniform(64), True)
+    p, tau, dt = 8, 1 / FREQUENCY, 2.0 / 64
+    steps, t = [], 0.0
+    while t < 2.0 - 1e-12:
+        h = min(dt, tau * (dt / tau) ** (p / 3)) if not steps else min(dt, 2.0 * steps[-1])
+        h = min(h, 2.0 - t)
+        steps.append(h)
+        t += h
+    assert strain_error(("ab", 8), steps, False) > 20 * strain_error(("ab", 8), _shortened(("ab", 8), 64), False)
 
 
 def test_tracers_uniform_flow_exact_and_wrap():
