@@ -217,6 +217,23 @@ def timed_steps(run, K, sampler=None):
     return ms, prof
 
 
+def time_diagnostics(run):
+    """The occasional diagnostics on the end state, outside the timed region: the time between CUDA
+    events on the run's stream around one call each (the call's own host work included), and the
+    values."""
+    out = {}
+    run.synchronize()
+    run.timer_start()
+    sk = run.derivative_skewness()
+    out["derivative_skewness_ms"] = round(run.timer_stop(), 3)
+    out["derivative_skewness"] = sk
+    run.timer_start()
+    _, k, _ = run.energy_below_scale()
+    out["energy_below_scale_ms"] = round(run.timer_stop(), 3)
+    out["energy_below_scale_k_at_dx"] = float(k[0])
+    return out
+
+
 def e2e_run(args, precision, device, inputs, K):
     """Through the public API from pinned host buffers: upload the state and tracers, K steps with
     their per-step host readbacks, download the final state."""
@@ -313,7 +330,8 @@ def ours(args):
             ms, prof = timed_steps(run, args.steps)
         el = max_over_ranks(ms / 1e3, f"cuda:{device}")
         spectra = (run.energy_spectrum(), run.scalar_spectrum())
-        results[form] = dict(el=el, prof=prof, clocks=cs.summary(), K=run.K, spectra=spectra)
+        results[form] = dict(el=el, prof=prof, clocks=cs.summary(), K=run.K, spectra=spectra,
+                             diagnostics=time_diagnostics(run))
         run.close()
         del run
     # end-to-end through the public API (host buffers), the headline form
@@ -346,6 +364,7 @@ def ours(args):
             "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in prof.items() if v[0]},
             "gpu_launches": int(sum(v[0] for v in prof.values())),
             "clocks": head["clocks"],
+            "diagnostics": head["diagnostics"],
             "e2e": {"value": round(e2e_val, 4), "unit": "steps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
         }

@@ -503,6 +503,23 @@ int gbght_spectrum(gbght_run* r, int which, double* out, int n) {
   return engine_call(r, r->eng->spectrum(which, out, n));
 }
 
+int gbght_derivative_skewness(gbght_run* r, double* skewness) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!skewness) return fail(r, GBGHT_ERR_ARGUMENT, "skewness is null");
+  return engine_call(r, r->eng->skewness(skewness));
+}
+
+int gbght_energy_below_scale(gbght_run* r, double* scales, double* k, double* eps, int n) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  const int N = r->cfg.grid_points_per_axis;
+  if (n < N || !k || !eps) return fail(r, GBGHT_ERR_ARGUMENT, "the outputs must hold grid_points_per_axis values");
+  int rc = engine_call(r, r->eng->below_scale(r->cfg.viscosity, k, eps));
+  if (rc) return rc;
+  if (scales)
+    for (int i = 0; i < N; ++i) scales[i] = (i + 1) * r->cfg.side_length / N;
+  return GBGHT_OK;
+}
+
 int gbght_tracers_import(gbght_run* r, const double* X) {
   if (check_run(r)) return GBGHT_ERR_ARGUMENT;
   if (r->cfg.tracers <= 0) return fail(r, GBGHT_ERR_ARGUMENT, "the run was built without tracers");

@@ -421,6 +421,98 @@ class EngineImpl final : public Engine {
     return nullptr;
   }
 
+  // derivative_skewness (src/Observables.jl:466-478): C·3⟨det S⟩/⟨S:S⟩^{3/2}, ⟨S:S⟩ = ½Σκ²|û|².
+  // The strain's z-inverse replaces the A slots, its y-inverse takes B slots 0..5, the deposit's x
+  // pass turns each triple into physical components in a transient buffer, and the determinants
+  // are summed in a fixed order. The A slots are rebuilt from the state afterwards.
+  const char* skewness(double* out) override {
+    double sums[4];
+    if (const char* err = observable_sums(0, sums)) return err;
+    const double n6 = double(N) * N * N * double(N) * N * N;
+    const double ss = 0.5 * (sums[1] / n6);
+    if (!(ss > 0)) {
+      *out = 0.0;
+      return nullptr;
+    }
+    const size_t n3 = size_t(N) * N * N;
+    constexpr int NTD = 256;
+    const size_t chunk = size_t(64) * NTD;
+    const size_t nblk = (n3 + chunk - 1) / chunk;
+    T* s6 = nullptr;
+    double* part = nullptr;
+    unsigned long long* mb = nullptr;
+    const char* err = rt_alloc(reinterpret_cast<void**>(&s6), 6 * n3 * sizeof(T));
+    if (!err) err = rt_alloc(reinterpret_cast<void**>(&part), nblk * sizeof(double));
+    if (!err) err = rt_alloc(reinterpret_cast<void**>(&mb), sizeof(unsigned long long));
+    if (!err) err = z_init(2);
+    if (!err) {
+      y_inverse(0, 6);
+      x_velocity_into(B_, s6, mb);
+      x_velocity_into(B_ + idxB(g_, 3, 0, 0, 0), s6 + 3 * n3, mb);
+#ifdef GBGHT_EMU
+      emu_grid(int(nblk), 1, 1, sizeof(double), [&](const Cta& c, void* sm) {
+        body_det_sum<T, 1>(c, static_cast<double*>(sm), s6, n3, chunk, part);
+      });
+#else
+      pbegin(PROF_OBSERVABLES);
+      k_det_sum<T, NTD><<<unsigned(nblk), NTD, 0, stream_>>>(s6, n3, chunk, part);
+      pend();
+#endif
+      err = rt_check();
+    }
+    std::vector<double> host(nblk);
+    if (!err) err = rt_d2h(host.data(), part, nblk * sizeof(double), stream_);
+    const char* err2 = z_init(1);   // the A slots hold the state's z-inverse again
+    rt_free(s6);
+    rt_free(part);
+    rt_free(mb);
+    if (err) return err;
+    if (err2) return err2;
+    double sum = 0.0;
+    for (size_t b = 0; b < nblk; ++b) sum += host[b];
+    const double mean_det = sum / double(n3);
+    const double C = (4.0 / 7.0) * std::sqrt(15.0 / 2.0);
+    *out = 3.0 * C * mean_det / std::pow(ss, 1.5);
+    return nullptr;
+  }
+  const char* below_scale(double nu, double* k, double* eps) override {
+    constexpr int CH = 16;
+    double sums[4];
+    if (const char* err = observable_sums(0, sums)) return err;
+    const size_t nrow = size_t(N) * 2;
+    double* rows = nullptr;
+    const char* err = rt_alloc(reinterpret_cast<void**>(&rows), size_t(g_.NY2) * nrow * sizeof(double));
+    if (err) return err;
+    const int nchunk = (N + CH - 1) / CH;
+#ifdef GBGHT_EMU
+    emu_grid(g_.NY2, nchunk, 1, (size_t(CH) * (g_.K + 1) + 1) * sizeof(double), [&](const Cta& c, void* sm) {
+      double* tab = static_cast<double*>(sm);
+      body_below_scale<T, 1, CH>(c, tab, tab + CH * (g_.K + 1), g_, p_.L, S_, rows);
+    });
+#else
+    const size_t smem = (size_t(CH) * (g_.K + 1) + NTR) * sizeof(double);
+    pbegin(PROF_OBSERVABLES);
+    k_below_scale<T, NTR, CH><<<dim3(g_.NY2, nchunk, 1), NTR, smem, stream_>>>(g_, p_.L, S_, rows);
+    pend();
+#endif
+    err = rt_check();
+    std::vector<double> host(size_t(g_.NY2) * nrow);
+    if (!err) err = rt_d2h(host.data(), rows, host.size() * sizeof(double), stream_);
+    rt_free(rows);
+    if (err) return err;
+    const double n6 = double(N) * N * N * double(N) * N * N;
+    const double whole = sums[0] / n6, dirichlet = sums[1] / n6;
+    for (int n = 0; n < N; ++n) {
+      double rk = 0.0, re = 0.0;
+      for (int qy = 0; qy < g_.NY2; ++qy) {
+        rk += host[size_t(qy) * nrow + size_t(n) * 2];
+        re += host[size_t(qy) * nrow + size_t(n) * 2 + 1];
+      }
+      k[n] = (whole - rk / n6) / 2;
+      eps[n] = nu * (dirichlet - re / n6);
+    }
+    return nullptr;
+  }
   const char* spectrum(int which, double* out, int nshell) override {
     const int c0 = which == 0 ? 0 : 3, nc = which == 0 ? 3 : 1;
     const size_t smem = (size_t(nshell_) + 2 * size_t(g_.KXP)) * sizeof(double);
@@ -781,25 +873,28 @@ class EngineImpl final : public Engine {
     pend();
 #endif
   }
-  void x_velocity() {
+  void x_velocity() { x_velocity_into(B_, U_, maxbits_); }
+  // The deposit's x pass over three B slots starting at `src`: their c2r into `out` ([3][N³]) and
+  // the max of the sum of their squares into `mb`.
+  void x_velocity_into(const Cplx<T>* src, T* out, unsigned long long* mb_out) {
     using X = XShape<T>;
     const int KXS = x_kxs(g_.K, int(sizeof(Cplx<T>)));
     const int ntiles = (N / X::PV) * N;
     const int grid = (ntiles + XT - 1) / XT;   // XT tiles per CTA
 #ifdef GBGHT_EMU
-    unsigned long long* mb = maxbits_;
+    unsigned long long* mb = mb_out;
     emu_grid(grid, 1, 1, smem_xv(), [&](const Cta& c, void* sm) {
       Cplx<T>* t = static_cast<Cplx<T>*>(sm);
       double* red = reinterpret_cast<double*>(t + N * X::ACT_V);
       Cplx<T>* stg = reinterpret_cast<Cplx<T>*>(red + 2);   // NT = 1 double, padded to 16 bytes
-      const double m = body_x_velocity<T, N, 1>(c, t, red, stg, KXS, nullptr, grid, g_, B_, U_, tw_, status_);
+      const double m = body_x_velocity<T, N, 1>(c, t, red, stg, KXS, nullptr, grid, g_, src, out, tw_, status_);
       unsigned long long bits;
       std::memcpy(&bits, &m, sizeof bits);
       if (bits > *mb) *mb = bits;
     });
 #else
     pbegin(PROF_X_VELOCITY);
-    k_x_velocity<T, N, NTXV><<<grid, NTXV, smem_xv(), stream_>>>(g_, B_, U_, maxbits_, KXS, tw_, status_);
+    k_x_velocity<T, N, NTXV><<<grid, NTXV, smem_xv(), stream_>>>(g_, src, out, mb_out, KXS, tw_, status_);
     pend();
 #endif
   }
@@ -832,19 +927,23 @@ class EngineImpl final : public Engine {
     pend();
 #endif
   }
-  const char* z_init() {
+  // The z-inverse of the state into the A slots (u, iκ×û, φ), or with `vorticity` = 2 of the six
+  // strain components into slots 0..5.
+  const char* z_init(int vorticity = 1) {
     bu_fresh_ = false;   // A is rewritten
+    const int with_scalar = vorticity == 2 ? 0 : p_.scalar;
 #ifdef GBGHT_EMU
     const int gx = g_.KXP / TLZ;
     emu_grid(gx, g_.NY2, 1, smem_z(), [&](const Cta& c, void* sm) {
       Cplx<T>* W = static_cast<Cplx<T>*>(sm);
       double* red = reinterpret_cast<double*>(W + N * TLZ);
       ZRowsReg<T, ZOwn<T, N, TLZ, 1>> rows;
-      partial_[c.by * gx + c.bx] = body_z_init<T, N, TLZ, 1>(c, W, red, g_, rows, A_, S_, p_.scalar, tw_);
+      partial_[c.by * gx + c.bx] =
+          body_z_init<T, N, TLZ, 1>(c, W, red, g_, rows, A_, S_, with_scalar, tw_, vorticity);
     });
 #else
-    k_z_init<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, S_, p_.scalar, partial_,
-                                                                                       tw_);
+    k_z_init<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, S_, with_scalar,
+                                                                                       partial_, tw_, vorticity);
 #endif
     return rt_check();
   }

@@ -72,6 +72,10 @@ class Engine {
   // the scalar variance alone (the blow-up guard of advance!), reading φ̂ only
   virtual const char* scalar_variance(double* var) = 0;
   virtual const char* spectrum(int which, double* out, int nshell) = 0;
+  // k(l) and ε(l) for every side l = nL/N, n = 1..N (src/Observables.jl:253-263)
+  virtual const char* below_scale(double nu, double* k, double* eps) = 0;
+  // derivative_skewness of the state (src/Observables.jl:466-478)
+  virtual const char* skewness(double* out) = 0;
   virtual const char* tracers_set(const double* X) = 0;
   virtual const char* tracers_get(double* X) = 0;
   virtual const char* tracer_sample_get(double* F, int slot) = 0;

@@ -162,6 +162,18 @@ __global__ void __launch_bounds__(NT, NT > 256 ? 1 : 2) k_z_init(Geometry g, Cpl
   });
   if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
 }
+template <class T, int NT, int CH>
+__global__ void __launch_bounds__(NT) k_below_scale(Geometry g, double L, const Cplx<T>* S, double* out) {
+  CTA_CTX;
+  double* tab = reinterpret_cast<double*>(g_smem);
+  body_below_scale<T, NT, CH>(c, tab, tab + CH * (g.K + 1), g, L, S, out);
+}
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) k_det_sum(const T* s6, size_t n, size_t chunk, double* out) {
+  CTA_CTX;
+  __shared__ double red[NT];
+  body_det_sum<T, NT>(c, red, s6, n, chunk, out);
+}
 template <class T>
 __global__ void k_reality(Geometry g, Cplx<T>* S, int ncomp) {
   reality_mode<T>(int(blockIdx.x * blockDim.x + threadIdx.x), g, S, ncomp);

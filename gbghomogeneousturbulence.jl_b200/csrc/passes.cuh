@@ -900,12 +900,50 @@ GBGHT_HD Cplx<T> curl_of(int o, Cplx<T> u0, Cplx<T> u1, Cplx<T> u2, T kX, T kY, 
   return mul_i(cr);
 }
 
+// Component o of the strain rate Ŝ_ij = ½ i(κ_j û_i + κ_i û_j), in the order S11, S22, S33, S12,
+// S13, S23 (src/Observables.jl:470, `symmetric_gradient`).
+template <class T>
+GBGHT_HD Cplx<T> strain_of(int o, Cplx<T> u0, Cplx<T> u1, Cplx<T> u2, T kX, T kY, T kZ) {
+  const T h = T(0.5);
+  switch (o) {
+    case 0: return mul_i(scale(u0, kX));
+    case 1: return mul_i(scale(u1, kY));
+    case 2: return mul_i(scale(u2, kZ));
+    case 3: return mul_i(scale(scale(u0, kY) + scale(u1, kX), h));
+    case 4: return mul_i(scale(scale(u0, kZ) + scale(u2, kX), h));
+    default: return mul_i(scale(scale(u1, kZ) + scale(u2, kY), h));
+  }
+}
+
+// ⟨det S⟩'s partial sums: block b adds the determinants of the points [b·chunk, (b+1)·chunk) of
+// the six physical components (S11, S22, S33, S12, S13, S23, n points apart), per thread and then
+// in thread order through `red` (NT doubles), into out[b].
+template <class T, int NT>
+GBGHT_HD void body_det_sum(const Cta& c, double* red, const T* GBGHT_RESTRICT s6, size_t n, size_t chunk,
+                           double* GBGHT_RESTRICT out) {
+  const size_t p0 = size_t(c.bx) * chunk;
+  const size_t p1 = p0 + chunk < n ? p0 + chunk : n;
+  double acc = 0.0;
+  for (size_t p = p0 + c.tid; p < p1; p += NT) {
+    const double a = s6[p], d = s6[n + p], f = s6[2 * n + p];
+    const double b = s6[3 * n + p], cc = s6[4 * n + p], e = s6[5 * n + p];
+    acc += a * (d * f - e * e) - b * (b * f - e * cc) + cc * (b * e - d * cc);
+  }
+  red[c.tid] = acc;
+  GBGHT_SYNC();
+  if (c.tid == 0) {
+    double s = 0.0;
+    for (int i = 0; i < NT; ++i) s += red[i];
+    out[c.bx] = s;
+  }
+}
+
 // The z-inverse of the owned velocity rows into A slots 0..2, and of iκ × û into slots 3..5
-// (3..5 only when `vorticity`).
+// (3..5 only when `vorticity`); with `vorticity` = 2 the six strain components into slots 0..5.
 template <class T, int N, int TL, int NT, class O, class Rows, class TW>
 GBGHT_HD void z_inverse_velocity(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* A, int qy, int kx0, double ky,
                                  const Rows& rows, int vorticity, const TW& tw) {
-  for (int o = 0; o < 3; ++o) {
+  for (int o = 0; o < 3 && vorticity != 2; ++o) {
     OwnVals<T, O> x;
 #pragma unroll
     for (int b = 0; b < O::BPT; ++b)
@@ -915,6 +953,18 @@ GBGHT_HD void z_inverse_velocity(const Cta& c, Cplx<T>* W, const Geometry& g, Cp
   }
   if (!vorticity) return;
   const T kY = T(ky);
+  if (vorticity == 2) {   // the strain rate instead: S11, S22, S33 into slots 0..2, S12, S13, S23 into 3..5
+    for (int o = 0; o < 6; ++o) {
+      OwnVals<T, O> x;
+      for_own_slots<T, N, TL, NT>(c, g, [&](int b, int sl, bool, int, int mz, int l) {
+        Cplx<T> u0, u1, u2;
+        rows.get3(b, sl, u0, u1, u2);
+        x.v[b][sl] = strain_of<T>(o, u0, u1, u2, T(g.s * double(kx0 + l)), kY, T(g.s * double(mz)));
+      });
+      z_inverse_own<T, N, TL, NT, O>(c, W, g, A, o, qy, kx0, x, tw);
+    }
+    return;
+  }
   for (int o = 0; o < 3; ++o) {
     OwnVals<T, O> x;
     for_own_slots<T, N, TL, NT>(c, g, [&](int b, int sl, bool, int, int mz, int l) {
@@ -1419,6 +1469,63 @@ GBGHT_HD void body_observables(const Cta& c, double* red, const Geometry& g, con
       double s = 0.0;
       for (int i = 0; i < NT; ++i) s += red[j * NT + i];
       out[qy * 4 + j] = s;
+    }
+}
+
+// ================================================================================================
+// Energy and dissipation below scale (src/Observables.jl:253-263): per ky' row and chunk of CH box
+// sides l = nL/N (n = n0+1 … n0+CH), the Hermitian-weighted Σ W_l²|û|² and Σ κ² W_l²|û|² with
+// W_l(κ) = ∏_a sinc(κ_a l/2). The sinc factors of the chunk are tabulated per |m| in `tab`
+// (CH·(K+1) doubles); each sum runs per thread and then in thread order through `red` (NT
+// doubles). out[(qy·N + n − 1)·2 + {0, 1}]. Grid: (NY2, ⌈N/CH⌉).
+// ================================================================================================
+template <class T, int NT, int CH>
+GBGHT_HD void body_below_scale(const Cta& c, double* tab, double* red, const Geometry& g, double L,
+                               const Cplx<T>* GBGHT_RESTRICT S, double* GBGHT_RESTRICT out) {
+  const int qy = c.bx, n0 = c.by * CH, N = g.N;
+  const int KX1 = g.K + 1, NY2 = g.NY2;
+  const int nch = N - n0 < CH ? N - n0 : CH;
+  for (int i = c.tid; i < CH * KX1; i += NT) {
+    const int j = i / KX1, m = i % KX1;
+    const double l = double(n0 + j + 1) * L / double(N);
+    const double y = (g.s * double(m)) * l / 2.0;
+    tab[i] = m == 0 ? 1.0 : sin(y) / y;
+  }
+  GBGHT_SYNC();
+  const int my = q_to_m(qy, g.K, NY2);
+  const double ky = g.s * double(my);
+  const double* ty = tab + (my < 0 ? -my : my);
+  double ak[CH], ae[CH];
+  for (int j = 0; j < CH; ++j) ak[j] = ae[j] = 0.0;
+  for (int i = c.tid; i < NY2 * KX1; i += NT) {
+    const int qz = i / KX1, kx = i % KX1;
+    const int mz = q_to_m(qz, g.K, NY2);
+    const double kxd = g.s * kx, kzd = g.s * mz;
+    const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
+    double e = 0.0;
+    for (int cc = 0; cc < 3; ++cc) {
+      const Cplx<T> v = S[idxS(g, cc, qy, qz, kx)];
+      e += double(v.x) * v.x + double(v.y) * v.y;
+    }
+    const double we = (kx == 0 ? 1.0 : 2.0) * e;
+    const double* tz = tab + (mz < 0 ? -mz : mz);
+    for (int j = 0; j < CH; ++j) {
+      const double W = (tab[j * KX1 + kx] * ty[j * KX1]) * tz[j * KX1];
+      const double p = (W * W) * we;
+      ak[j] += p;
+      ae[j] += k2 * p;
+    }
+  }
+  for (int j = 0; j < nch; ++j)
+    for (int which = 0; which < 2; ++which) {
+      red[c.tid] = which == 0 ? ak[j] : ae[j];
+      GBGHT_SYNC();
+      if (c.tid == 0) {
+        double s = 0.0;
+        for (int i = 0; i < NT; ++i) s += red[i];
+        out[(size_t(qy) * N + n0 + j) * 2 + which] = s;
+      }
+      GBGHT_SYNC();
     }
 }
 

@@ -95,6 +95,8 @@ _SIGNATURES = {
     "gbght_observables": (C.c_int, [C.c_void_p, _DP]),
     "gbght_spectrum_length": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "gbght_spectrum": (C.c_int, [C.c_void_p, C.c_int, _DP, C.c_int]),
+    "gbght_energy_below_scale": (C.c_int, [C.c_void_p, _DP, _DP, _DP, C.c_int]),
+    "gbght_derivative_skewness": (C.c_int, [C.c_void_p, _DP]),
     "gbght_tracers_import": (C.c_int, [C.c_void_p, _DP]),
     "gbght_tracers_export": (C.c_int, [C.c_void_p, _DP]),
     "gbght_tracer_sample_export": (C.c_int, [C.c_void_p, _DP, _DP]),
@@ -371,6 +373,20 @@ class Run:
         out = np.zeros(n.value)
         self._check(self.lib.gbght_spectrum(self.h, which, _ptr(out), n.value))
         return out
+
+    def derivative_skewness(self) -> float:
+        """`derivative_skewness(û, domain)` (src/Observables.jl:466-478)."""
+        v = C.c_double()
+        self._check(self.lib.gbght_derivative_skewness(self.h, C.byref(v)))
+        return v.value
+
+    def energy_below_scale(self):
+        """`kinetic_energy_and_dissipation_below_scale(û, domain, ν)` (src/Observables.jl:253-263):
+        (scales, k(l), ε(l)) for l = nL/N, n = 1..N."""
+        N = self.N
+        scales, k, eps = np.zeros(N), np.zeros(N), np.zeros(N)
+        self._check(self.lib.gbght_energy_below_scale(self.h, _ptr(scales), _ptr(k), _ptr(eps), N))
+        return scales, k, eps
 
     def energy_spectrum(self) -> np.ndarray:
         return self._spectrum(0)

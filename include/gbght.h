@@ -186,6 +186,19 @@ int gbght_observables(gbght_run* run, double out[4]);
 int gbght_spectrum_length(const gbght_run* run, int* n);
 int gbght_spectrum(gbght_run* run, int which, double* out, int n);
 
+/* The derivative skewness of the state, C·3⟨det S⟩/⟨S:S⟩^{3/2} with S the strain rate in physical
+ * space, ⟨S:S⟩ = ½Σ|κ|²|û|² and C = (4/7)√(15/2); 0 for a strain-free state. It allocates a
+ * transient buffer of six physical fields and leaves the state and the deposit unchanged.
+ * Replaces derivative_skewness(û, domain) (src/Observables.jl:466-478). */
+int gbght_derivative_skewness(gbght_run* run, double* skewness);
+
+/* The kinetic energy and dissipation below scale: for every box side l = nL/N (n = 1..N),
+ * k(l) = ½Σ(1 − W_l²)|û|² and ε(l) = νΣ|κ|²(1 − W_l²)|û|², W_l(κ) = ∏_a sinc(κ_a l/2) the
+ * transfer function of the box mean (normalised sums, FP64). `n` is the capacity of each output
+ * (at least N); `scales` may be NULL. Replaces kinetic_energy_and_dissipation_below_scale(û, domain,
+ * viscosity) (src/Observables.jl:253-263). An occasional diagnostic: its cost grows as N⁴. */
+int gbght_energy_below_scale(gbght_run* run, double* scales, double* k, double* eps, int n);
+
 /* Tracer positions [3][M], copied as given (the push wraps them into [0, L)). Import clears the
  * trail. Replaces Tracers(domain; positions) (src/Particles.jl:145-176). */
 int gbght_tracers_import(gbght_run* run, const double* X);

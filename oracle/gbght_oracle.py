@@ -675,6 +675,46 @@ def scalar_dissipation(dom, ph, kappa):
     return 2 * kappa * dom.inner(ph, ph, dom.k2)
 
 
+def energy_below_scale(dom: Domain, uh: np.ndarray, nu: float):
+    """`kinetic_energy_and_dissipation_below_scale` (src/Observables.jl:253-263): for every side
+    l = nL/N, k(l) = (Σ|û|² − ΣW_l²|û|²)/2 and ε(l) = ν(Σκ²|û|² − Σκ²W_l²|û|²), normalised sums with
+    the Hermitian weights, W_l(κ) = ∏_a sinc(κ_a l/2) the transfer function of the box mean."""
+    N, L = dom.N, dom.L
+    p = (np.abs(uh) ** 2).sum(axis=0) * dom.hweight
+    whole = float(p.sum()) / float(N) ** 6
+    dirichlet = float((p * dom.k2).sum()) / float(N) ** 6
+    scales = np.array([n * L / N for n in range(1, N + 1)])
+    k = np.zeros(N)
+    eps = np.zeros(N)
+    for i, l in enumerate(scales):
+        W = np.sinc(dom.kx * l / (2 * math.pi)) * np.sinc(dom.ky * l / (2 * math.pi)) * np.sinc(dom.kz * l / (2 * math.pi))
+        W2 = W * W
+        k[i] = (whole - float((p * W2).sum()) / float(N) ** 6) / 2
+        eps[i] = nu * (dirichlet - float((p * dom.k2 * W2).sum()) / float(N) ** 6)
+    return scales, k, eps
+
+
+SKEWNESS_ISOTROPY_CONSTANT = (4 / 7) * math.sqrt(15 / 2)   # src/Observables.jl:403-406
+
+
+def strain_physical(dom: Domain, uh: np.ndarray) -> np.ndarray:
+    """S_ij = ½(∂_j u_i + ∂_i u_j) in physical space, as (S11, S22, S33, S12, S13, S23)."""
+    d = (dom.dkx, dom.dky, dom.dkz)
+    pairs = ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))
+    return np.stack([dom.to_physical(0.5j * (d[j] * uh[i] + d[i] * uh[j])) for i, j in pairs])
+
+
+def derivative_skewness(dom: Domain, uh: np.ndarray) -> float:
+    """`derivative_skewness` (src/Observables.jl:466-478): C·3⟨det S⟩/⟨S:S⟩^{3/2}, with
+    ⟨S:S⟩ = ½Σ|κ|²|û|² read from û and ⟨det S⟩ the grid mean of the strain's determinant."""
+    ss = dom.inner(uh, uh, dom.k2) / 2
+    if ss <= 0:
+        return 0.0
+    s11, s22, s33, s12, s13, s23 = strain_physical(dom, uh)
+    det = s11 * (s22 * s33 - s23 * s23) - s12 * (s12 * s33 - s23 * s13) + s13 * (s12 * s23 - s22 * s13)
+    return 3 * SKEWNESS_ISOTROPY_CONSTANT * float(det.mean()) / ss ** 1.5
+
+
 def n_shells(N: int) -> int:
     return int(math.floor(math.sqrt(3) * N / 2 + 0.5)) + 1
 

@@ -139,6 +139,30 @@ def test_adams_particle_schemes(cuda_library, scheme, shortened):
     assert np.max(np.abs(F - orun.f0)) < 1e-10
 
 
+@pytest.mark.parametrize("N,precision", [(64, "fp64"), (128, "fp64"), (64, "fp32_mixed")])
+def test_energy_below_scale(cuda_library, N, precision):
+    # kinetic_energy_and_dissipation_below_scale against the oracle's sums
+    run, orun = make_case(N, viscosity=0.01, energy=1.5, forcing=0.1, precision=precision, library=cuda_library)
+    advance_both(run, orun, 2, dt=0.004)
+    scales, k, eps = run.energy_below_scale()
+    s_o, k_o, e_o = O.energy_below_scale(orun.dom, orun.state.uh, 0.01)
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert np.array_equal(scales, s_o)
+    assert np.allclose(k, k_o, rtol=tol, atol=0) and np.allclose(eps, e_o, rtol=tol, atol=0)
+    assert np.all(np.diff(k) >= 0) and k[-1] == pytest.approx(run.observables()["kinetic_energy"], rel=1e-12)
+
+
+@pytest.mark.parametrize("N,precision", [(64, "fp64"), (192, "fp64"), (64, "fp32_mixed")])
+def test_derivative_skewness(cuda_library, N, precision):
+    run, orun = make_case(N, viscosity=0.005, forcing=0.1, tracers=500, precision=precision, library=cuda_library)
+    advance_both(run, orun, 2, dt=0.004)
+    sk = run.derivative_skewness()
+    assert sk == pytest.approx(O.derivative_skewness(orun.dom, orun.state.uh), rel=1e-12 if precision == "fp64" else 1e-4)
+    if precision == "fp64":   # the diagnostic leaves the run as it was
+        advance_both(run, orun, 1, dt=0.004)
+        compare(run, orun, tol=1e-12)
+
+
 def test_rescaling_holds_the_target_exactly(cuda_library):
     run, _ = make_case(64, forcing=gbght.VarianceRescaling(0.45, "total"),
                        scalar_forcing=gbght.VarianceRescaling(0.6, "total", 1, math.inf), library=cuda_library)

@@ -117,6 +117,26 @@ def test_observables_and_spectra(hostcheck_library):
     assert run.max_speed() == pytest.approx(orun.speed, rel=1e-13)
 
 
+@pytest.mark.parametrize("N", [16, 12])
+def test_energy_below_scale_matches_oracle(hostcheck_library, N):
+    run, orun = make_case(N, viscosity=0.02, energy=1.5, forcing=0.1, library=hostcheck_library)
+    advance_both(run, orun, 2, dt=0.01)
+    scales, k, eps = run.energy_below_scale()
+    s_o, k_o, e_o = O.energy_below_scale(orun.dom, orun.state.uh, 0.02)
+    assert np.array_equal(scales, s_o)
+    assert np.allclose(k, k_o, rtol=1e-12, atol=0) and np.allclose(eps, e_o, rtol=1e-12, atol=0)
+
+
+def test_derivative_skewness_matches_oracle(hostcheck_library):
+    run, orun = make_case(16, forcing=0.1, tracers=8, library=hostcheck_library)
+    advance_both(run, orun, 2, dt=0.01)
+    sk = run.derivative_skewness()
+    assert sk == pytest.approx(O.derivative_skewness(orun.dom, orun.state.uh), rel=1e-12)
+    # the diagnostic leaves the run as it was: the next step is the oracle's
+    advance_both(run, orun, 2, dt=0.01)
+    compare(run, orun, tol=2e-14)
+
+
 def test_deposited_velocity_and_interpolation(hostcheck_library):
     run, orun = make_case(16, tracers=8, library=hostcheck_library)
     u = run.velocity_physical()

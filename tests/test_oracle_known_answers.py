@@ -698,3 +698,80 @@ def test_heun_second_order_on_straining_flow():
 
     e = [err(n) for n in (64, 128, 256)]
     assert abs(math.log2(e[1] / e[2]) - 2.0) < 0.5
+
+
+# --- test/below_scale.jl -------------------------------------------------------------------------
+
+def _embed(uh, N, M):
+    """The band-limited field's coefficients on an M-point grid (zero padding, rescaled for the
+    unnormalised transform)."""
+    out = np.zeros((3, M, M, M // 2 + 1), complex)
+    m = np.fft.fftfreq(N, 1.0 / N).round().astype(int)
+    for iz, mz in enumerate(m):
+        for iy, my in enumerate(m):
+            out[:, mz % M, my % M, : N // 2 + 1] = uh[:, iz, iy, :]
+    return out * (M / N) ** 3
+
+
+def _box_mean(a, q, axis):
+    n = a.shape[axis]
+    ext = np.concatenate([a, np.take(a, range(q), axis=axis)], axis=axis)
+    c = np.cumsum(ext, axis=axis)
+    lead = np.take(c, range(q - 1, q - 1 + n), axis=axis)
+    lag = np.concatenate([np.zeros_like(np.take(a, [0], axis=axis)), np.take(c, range(n - 1), axis=axis)], axis=axis)
+    return (lead - lag) / q
+
+
+@pytest.mark.parametrize("N", [16, 12])
+def test_energy_below_scale(N):
+    # test/below_scale.jl:66-100: the largest side returns the whole-field pair, both rise with l,
+    # and the definition in physical space (remove each box's mean on an 8× finer grid, average over
+    # positions) agrees elementwise to 2/q² for a box of q fine points
+    dom = O.Domain(N)
+    uh = S.seed_velocity(N, 1.5, seed=N)
+    nu = 0.02
+    scales, k, eps = O.energy_below_scale(dom, uh, nu)
+    assert np.allclose(scales, [n * 2 * math.pi / N for n in range(1, N + 1)], rtol=1e-15)
+    assert k[-1] == pytest.approx(O.kinetic_energy(dom, uh), rel=1e-12)
+    assert eps[-1] == pytest.approx(O.dissipation(dom, uh, nu), rel=1e-12)
+    assert np.all(np.diff(k) >= 0) and np.all(np.diff(eps) >= 0) and np.all(k > 0)
+    refine = 8
+    M = refine * N
+    u = sfft_irfft(_embed(uh, N, M), M)
+    total = float((u ** 2).sum()) / M ** 3 / 2
+    q = refine * np.arange(1, N + 1)
+    for i, qq in enumerate(q):
+        b = u
+        for axis in (1, 2, 3):
+            b = _box_mean(b, qq, axis)
+        phys = total - float((b ** 2).sum()) / M ** 3 / 2
+        assert abs(k[i] - phys) / phys < 2 / qq ** 2
+
+
+def sfft_irfft(fh, M):
+    return np.fft.irfftn(fh, s=(M, M, M), axes=(-3, -2, -1))
+
+
+# --- test/observables_analytic.jl:78-110 ---------------------------------------------------------
+
+def test_derivative_skewness():
+    # zero for a field of three single modes, odd in the velocity, non-zero for a random field
+    N = 16
+    dom = O.Domain(N)
+    x, y, z = _grid(N)
+    uh = dom.to_spectral(np.stack([0.7 * np.sin(y), -0.4 * np.sin(z), 1.1 * np.sin(x)]))
+    assert abs(O.derivative_skewness(dom, uh)) < 1e-12
+    seeded = S.seed_velocity(N, 1.0, seed=5)
+    sk = O.derivative_skewness(dom, seeded)
+    assert sk != 0
+    assert O.derivative_skewness(dom, -seeded) == pytest.approx(-sk, rel=1e-12)
+
+
+def test_skewness_denominator_dirichlet_route():
+    # ⟨S:S⟩ from the physical strain equals ½Σ|κ|²|û|² for a solenoidal field
+    N = 32
+    dom = O.Domain(N)
+    uh = S.seed_velocity(N, 1.5, seed=8)
+    s = O.strain_physical(dom, uh)
+    direct = float((s[:3] ** 2).sum() + 2 * (s[3:] ** 2).sum()) / N ** 3
+    assert direct == pytest.approx(dom.inner(uh, uh, dom.k2) / 2, rel=1e-12)
