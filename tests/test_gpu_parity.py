@@ -300,3 +300,60 @@ def test_fp32_mixed_short_time_error(cuda_library):
                       (run.scalar_spectrum(), O.scalar_spectrum(orun.dom, orun.state.phih))):
         live = want > 1e-6 * want.max()
         assert np.max(np.abs(got[live] - want[live]) / want[live]) < 1e-5
+
+
+def test_full_size_512_cubed_properties(cuda_library):
+    # The benchmark's 512³ workload (ConstantPower on shells 1–2, G along x, tracers), two CFL steps
+    # in each precision form, held to properties that do not depend on the size:
+    # - the state stays solenoidal and its kx = 0 plane exactly Hermitian;
+    # - the observables and the spectrum agree with sums over the exported state (Parseval);
+    # - the deposited max speed is the max over the exported physical velocity;
+    # - the FP32-mixed spectra stay within 1e-5 of the FP64 ones on every live shell.
+    N, M = 512, 100_000
+    uh0 = S.seed_velocity(N, 0.5, seed=0)
+    ph0 = S.seed_scalar(N, 0.5, seed=1)
+    X0 = S.seed_tracers(M, seed=2)
+    spectra = {}
+    for precision in ("fp64", "fp32_mixed"):
+        setup = gbght.Setup(grid_points_per_axis=N, viscosity=8.5e-4, velocity_forcing=gbght.ConstantPower(0.1),
+                            mean_gradient=(1.0, 0.0, 0.0), tracers=M, precision=precision)
+        run = gbght.simulation(setup, uh0, ph0, X0, library=cuda_library)
+        for _ in range(2):
+            run.advance(None)
+        spectra[precision] = (run.energy_spectrum(), run.scalar_spectrum())
+        if precision == "fp64":
+            ue, pe = run.export_state()
+            kx, ky, kz, k2 = S.wavenumbers(N)
+            num, den = 0.0, 0.0
+            for z in range(0, N, 64):   # |κ·û| against |κ||û|, in slabs
+                sl = slice(z, z + 64)
+                div = (kx * ue[0, sl] + ky * ue[1, sl]) + kz[sl] * ue[2, sl]
+                num += float(np.sum(np.abs(div) ** 2))
+                den += float(np.sum(k2[sl] * (np.abs(ue[0, sl]) ** 2 + np.abs(ue[1, sl]) ** 2 + np.abs(ue[2, sl]) ** 2)))
+            assert math.sqrt(num / den) < 1e-13
+            neg = (-np.arange(N)) % N
+            for f in (ue, pe):
+                plane = f[..., 0]
+                assert np.max(np.abs(plane - np.conj(plane[..., neg, :][..., :, neg]))) == 0.0
+            w = np.full(N // 2 + 1, 2.0)
+            w[0] = 1.0
+            w[N // 2] = 1.0
+            n6 = float(N) ** 6
+            k_host = sum(float(np.sum((np.abs(ue[c]) ** 2) * w)) for c in range(3)) / n6 / 2
+            var_host = float(np.sum((np.abs(pe) ** 2) * w)) / n6
+            ob = run.observables()
+            assert ob["kinetic_energy"] == pytest.approx(k_host, rel=1e-12)
+            assert ob["scalar_variance"] == pytest.approx(var_host, rel=1e-12)
+            E, P = spectra[precision]
+            assert float(E.sum()) == pytest.approx(ob["kinetic_energy"], rel=1e-12)   # Δκ = 1 at L = 2π
+            assert float(P.sum()) == pytest.approx(ob["scalar_variance"], rel=1e-12)
+            del ue, pe
+            u = run.velocity_physical()
+            speed = math.sqrt(float(np.max(u[0] * u[0] + u[1] * u[1] + u[2] * u[2])))
+            assert run.max_speed() == pytest.approx(speed, rel=1e-14)
+            del u
+        run.close()
+    for i in (0, 1):
+        ref, got = spectra["fp64"][i], spectra["fp32_mixed"][i]
+        live = ref > 1e-6 * ref.max()
+        assert np.max(np.abs(got[live] - ref[live]) / ref[live]) < 1e-5
