@@ -80,11 +80,21 @@ def _peaks():
         return FALLBACK_HBM, "fallback"
 
 
+SCHEME_NAME = {"IFLowStorageRK4": "IF-RK4", "IFLowStorageRK3": "IF-RK3", "IFHeun": "IFHeun", "IFSSPRK3": "IFSSPRK3"}
+# the schemes' advective-CFL ceilings under the 2/3 rule (src/Propagator.jl:906-919)
+SCHEME_CFL = {"IFLowStorageRK4": 0.96, "IFLowStorageRK3": 0.5, "IFHeun": 0.25, "IFSSPRK3": 0.5}
+
+
+def _cfl(args):
+    """The workload's CFL number, lowered to the scheme's own ceiling where that is smaller."""
+    return min(WORKLOAD["cfl"], SCHEME_CFL[args.scheme])
+
+
 def _config(args, N):
-    return {"workload": f"{N}^3 forced velocity+scalar IF-RK4, nu=kappa={WORKLOAD['viscosity']}, "
+    return {"workload": f"{N}^3 forced velocity+scalar {SCHEME_NAME[args.scheme]}, nu=kappa={WORKLOAD['viscosity']}, "
                         f"ConstantPower eps={WORKLOAD['injection_rate']} |k|<=2.5, G=1 along x, "
-                        f"{args.tracers} Heun/Catmull-Rom tracers, CFL {WORKLOAD['cfl']}",
-            "grid": N, "tracers": args.tracers, "scheme": "IFLowStorageRK4", "dealiasing": "2/3 closed ball",
+                        f"{args.tracers} Heun/Catmull-Rom tracers, CFL {_cfl(args)}",
+            "grid": N, "tracers": args.tracers, "scheme": args.scheme, "dealiasing": "2/3 closed ball",
             "start": "seeded k^4 spectrum (synthetic), not a stationary state",
             "l2": "inputs larger than L2 (state alone >= 1.3 GB)",
             "parallelism": f"replicas x{args.gpus}"}
@@ -197,7 +207,7 @@ def run_form(args, precision, device, inputs, timed=True):
     uh, ph, X = inputs
     setup = gbght.Setup(grid_points_per_axis=N, viscosity=WORKLOAD["viscosity"], schmidt=WORKLOAD["schmidt"],
                         velocity_forcing=gbght.ConstantPower(WORKLOAD["injection_rate"], *WORKLOAD["shells"]),
-                        mean_gradient=WORKLOAD["G"], tracers=M, cfl=WORKLOAD["cfl"], precision=precision,
+                        mean_gradient=WORKLOAD["G"], tracers=M, cfl=_cfl(args), scheme=args.scheme, precision=precision,
                         device=device)
     run = gbght.simulation(setup, uh, ph, X)
     for _ in range(args.warmup):
@@ -249,7 +259,7 @@ def e2e_run(args, precision, device, inputs, K):
     pp, t5 = pinned_like(out_p)
     setup = gbght.Setup(grid_points_per_axis=N, viscosity=WORKLOAD["viscosity"], schmidt=WORKLOAD["schmidt"],
                         velocity_forcing=gbght.ConstantPower(WORKLOAD["injection_rate"], *WORKLOAD["shells"]),
-                        mean_gradient=WORKLOAD["G"], tracers=M, cfl=WORKLOAD["cfl"], precision=precision,
+                        mean_gradient=WORKLOAD["G"], tracers=M, cfl=_cfl(args), scheme=args.scheme, precision=precision,
                         device=device)
     run = gbght.Run(setup)
     run.synchronize()
@@ -422,6 +432,8 @@ def main():
     ap.add_argument("--grid", type=int, default=WORKLOAD["N"])
     ap.add_argument("--tracers", type=int, default=WORKLOAD["tracers"])
     ap.add_argument("--form", default="both", choices=["both", "fp64", "fp32_mixed"])
+    ap.add_argument("--scheme", default=WORKLOAD["scheme"], choices=list(SCHEME_NAME),
+                    help="the field integration scheme (the metric is quoted on IFLowStorageRK4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (quick kernel timing)")
     args = ap.parse_args()

@@ -769,8 +769,12 @@ class EngineImpl final : public Engine {
     set(reinterpret_cast<const void*>(k_y_forward<T, N, TLY, NTY>), smem_y());
     set(reinterpret_cast<const void*>(k_x_products<T, N, NTXP>), smem_x());
     set(reinterpret_cast<const void*>(k_x_velocity<T, N, NTXV>), smem_xv());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, true>), smem_ze());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, false>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kLowStorage>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kHeunPredictor>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kHeunCorrector>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp1>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp2>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp3>), smem_ze());
     set(reinterpret_cast<const void*>(k_z_init<T, N, TLZ, NTZ>), smem_z());
     return e;
   }
@@ -899,6 +903,17 @@ class EngineImpl final : public Engine {
 #endif
   }
   void z_epilogue(const StageArgs& st) {
+    switch (st.kind) {   // one instantiation per stage kind
+      case kHeunPredictor: return z_epilogue_kind<kHeunPredictor>(st);
+      case kHeunCorrector: return z_epilogue_kind<kHeunCorrector>(st);
+      case kSsp1: return z_epilogue_kind<kSsp1>(st);
+      case kSsp2: return z_epilogue_kind<kSsp2>(st);
+      case kSsp3: return z_epilogue_kind<kSsp3>(st);
+      default: return z_epilogue_kind<kLowStorage>(st);
+    }
+  }
+  template <int KIND>
+  void z_epilogue_kind(const StageArgs& st) {
 #ifdef GBGHT_EMU
     const int gx = g_.KXP / TLZ;
     emu_grid(gx, g_.NY2, 1, ZLayout<T, N, TLZ, 1>::bytes(g_.K), [&](const Cta& c, void* sm) {
@@ -909,21 +924,12 @@ class EngineImpl final : public Engine {
       Cplx<T>* R = reinterpret_cast<Cplx<T>*>(base + L::kStage);
       ZRowsReg<T, ZOwn<T, N, TLZ, 1>> rows;
       partial_[c.by * gx + c.bx] =
-          st.kind == kLowStorage
-              ? body_z_epilogue<T, N, TLZ, 1, true>(c, W, R, nullptr, red, g_, maps_, rows, A_, S_, H_, st, amp_, tw_,
-                                                    status_)
-              : body_z_epilogue<T, N, TLZ, 1, false>(c, W, R, nullptr, red, g_, maps_, rows, A_, S_, H_, st, amp_, tw_,
-                                                     status_);
+          body_z_epilogue<T, N, TLZ, 1, KIND>(c, W, R, nullptr, red, g_, maps_, rows, A_, S_, H_, st, amp_, tw_, status_);
     });
 #else
     pbegin(PROF_Z_EPILOGUE);
-    // the low-storage schemes run an instantiation without the other schemes' stage kinds
-    if (st.kind == kLowStorage)
-      k_z_epilogue<T, N, TLZ, NTZ, true><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_ze(), stream_>>>(
-          maps_, g_, A_, S_, H_, st, amp_, partial_, tw_, status_);
-    else
-      k_z_epilogue<T, N, TLZ, NTZ, false><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_ze(), stream_>>>(
-          maps_, g_, A_, S_, H_, st, amp_, partial_, tw_, status_);
+    k_z_epilogue<T, N, TLZ, NTZ, KIND><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_ze(), stream_>>>(
+        maps_, g_, A_, S_, H_, st, amp_, partial_, tw_, status_);
     pend();
 #endif
   }

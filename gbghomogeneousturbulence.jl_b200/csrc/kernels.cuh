@@ -130,7 +130,7 @@ __device__ __forceinline__ double with_z_rows(uint32_t* slot, const F& run) {
 
 // Shared memory: ZLayout (the FFT tile, NT doubles, barriers, the TMEM address, the twiddle table,
 // the staging region).
-template <class T, int N, int TL, int NT, bool LS>
+template <class T, int N, int TL, int NT, int KIND>
 __global__ void __launch_bounds__(NT, NT > 256 ? 1 : (sizeof(T) == 8 ? 2 : 4)) k_z_epilogue(const __grid_constant__ TmaMaps m, Geometry g, Cplx<T>* A,
                                                       Cplx<T>* S, Cplx<T>* H, StageArgs st, const double* amp,
                                                       double* partial, const Cplx<T>* tw, unsigned int* status) {
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(NT, NT > 256 ? 1 : (sizeof(T) == 8 ? 2 : 4)) k
   for (int i = c.tid; i < N; i += NT) twS[i] = tw[i];
   init_bars(bar, 3);   // its barrier also publishes the twiddle table
   const double e = with_z_rows<T, N, TL, NT>(slot, [&](auto& rows) {
-    return body_z_epilogue<T, N, TL, NT, LS>(c, W, R, bar, red, g, m, rows, A, S, H, st, amp, twS, status);
+    return body_z_epilogue<T, N, TL, NT, KIND>(c, W, R, bar, red, g, m, rows, A, S, H, st, amp, twS, status);
   });
   if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
 }

@@ -1013,37 +1013,28 @@ struct StageArgs {
 // stage 3 q ← E₂(⅓ h) + ⅔·E₁(q + Δt N) (E₁ = E(Δt/2), E₂ = E(Δt)). Each grouping is the reference's.
 enum StageKind { kLowStorage = 0, kHeunPredictor = 1, kHeunCorrector = 2, kSsp1 = 3, kSsp2 = 4, kSsp3 = 5 };
 
-// LS selects the low-storage update at compile time: the benchmark's path carries no other kind.
-template <class T, bool LS>
+// KIND is the stage kind, fixed at compile time: each kind has its own epilogue instantiation, so
+// no stage carries another kind's arithmetic (a runtime switch here made the kernel 1.76× slower).
+template <class T, int KIND>
 GBGHT_HD Cplx<T> scheme_update(const StageArgs& st, Cplx<T> q, Cplx<T> h, Cplx<T> n, T E1, T E2, Cplx<T>* hw) {
   const T dt = T(st.dt);
-  if (LS) {
-    const Cplx<T> hh = st.first ? scale(n, dt) : scale(h, T(st.a)) + scale(n, dt);
-    *hw = scale(hh, E1);
-    return scale(q + scale(hh, T(st.b)), E1);
+  if (KIND == kHeunPredictor) {
+    *hw = scale(q, E1) + scale(scale(n, E1), dt / T(2));
+    return scale(q + scale(n, dt), E1);
   }
-  switch (st.kind) {
-    case kHeunPredictor:
-      *hw = scale(q, E1) + scale(scale(n, E1), dt / T(2));
-      return scale(q + scale(n, dt), E1);
-    case kHeunCorrector:
-      return h + scale(n, dt / T(2));
-    case kSsp1:
-      *hw = q;
-      return scale(q + scale(n, dt), E1);
-    case kSsp2:
-      return scale(scale(q + scale(n, dt), E1), T(0.25)) + scale(scale(h, T(0.75)), E2);
-    case kSsp3:
-      return scale(scale(h, T(1.0 / 3.0)), E2) + scale(scale(q + scale(n, dt), E1), T(2.0 / 3.0));
-    default: {
-      const Cplx<T> hh = st.first ? scale(n, dt) : scale(h, T(st.a)) + scale(n, dt);
-      *hw = scale(hh, E1);
-      return scale(q + scale(hh, T(st.b)), E1);
-    }
+  if (KIND == kHeunCorrector) return h + scale(n, dt / T(2));
+  if (KIND == kSsp1) {
+    *hw = q;
+    return scale(q + scale(n, dt), E1);
   }
+  if (KIND == kSsp2) return scale(scale(q + scale(n, dt), E1), T(0.25)) + scale(scale(h, T(0.75)), E2);
+  if (KIND == kSsp3) return scale(scale(h, T(1.0 / 3.0)), E2) + scale(scale(q + scale(n, dt), E1), T(2.0 / 3.0));
+  const Cplx<T> hh = st.first ? scale(n, dt) : scale(h, T(st.a)) + scale(n, dt);   // low storage
+  *hw = scale(hh, E1);
+  return scale(q + scale(hh, T(st.b)), E1);
 }
 
-template <class T, int N, int TL, int NT, bool LS, class Rows>
+template <class T, int N, int TL, int NT, int KIND, class Rows>
 GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* bar, double* red, const Geometry& g,
                                 const TmaMaps& maps, Rows& rows, Cplx<T>* GBGHT_RESTRICT A, Cplx<T>* GBGHT_RESTRICT S,
                                 Cplx<T>* GBGHT_RESTRICT H, const StageArgs& st, const double* GBGHT_RESTRICT force_amp,
@@ -1115,10 +1106,10 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
           }
           if (A_s != 0.0 && k2 >= st.sband_lo2 && k2 <= st.sband_hi2) nphi = nphi + scale(phi, T(A_s));
           const bool sband = k2 >= st.sband_lo2 && k2 <= st.sband_hi2;
-          const T E1 = !LS && st.kind == kHeunCorrector ? T(1) : T(exp(st.cphi * k2 + (sband ? st.lin_phi : 0.0)));
-          const T E2 = !LS && st.kind >= kSsp2 ? T(exp(st.cphi2 * k2 + (sband ? st.lin_phi2 : 0.0))) : T(0);
+          const T E1 = KIND == kHeunCorrector ? T(1) : T(exp(st.cphi * k2 + (sband ? st.lin_phi : 0.0)));
+          const T E2 = KIND >= kSsp2 ? T(exp(st.cphi2 * k2 + (sband ? st.lin_phi2 : 0.0))) : T(0);
           Cplx<T> hw = czero<T>();
-          phi = scheme_update<T, LS>(st, phi, st.read_h ? sst.at(1, q, h, l) : czero<T>(), nphi, E1, E2, &hw);
+          phi = scheme_update<T, KIND>(st, phi, st.read_h ? sst.at(1, q, h, l) : czero<T>(), nphi, E1, E2, &hw);
           S[si] = phi;
           if (st.write_h) H[si] = hw;
         }
@@ -1184,13 +1175,13 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
           n2 = n2 + scale(u2, Af);
         }
         const bool vband = k2 >= st.band_lo2 && k2 <= st.band_hi2;
-        const T E1 = !LS && st.kind == kHeunCorrector ? T(1) : T(exp(st.cu * k2 + (vband ? st.lin_u : 0.0)));
-        const T E2 = !LS && st.kind >= kSsp2 ? T(exp(st.cu2 * k2 + (vband ? st.lin_u2 : 0.0))) : T(0);
+        const T E1 = KIND == kHeunCorrector ? T(1) : T(exp(st.cu * k2 + (vband ? st.lin_u : 0.0)));
+        const T E2 = KIND >= kSsp2 ? T(exp(st.cu2 * k2 + (vband ? st.lin_u2 : 0.0))) : T(0);
         const bool rh = st.read_h;
         Cplx<T> w0 = czero<T>(), w1 = czero<T>(), w2 = czero<T>();
-        u0 = scheme_update<T, LS>(st, u0, rh ? sst.at(3, q, h, l) : czero<T>(), n0, E1, E2, &w0);
-        u1 = scheme_update<T, LS>(st, u1, rh ? sst.at(4, q, h, l) : czero<T>(), n1, E1, E2, &w1);
-        u2 = scheme_update<T, LS>(st, u2, rh ? sst.at(5, q, h, l) : czero<T>(), n2, E1, E2, &w2);
+        u0 = scheme_update<T, KIND>(st, u0, rh ? sst.at(3, q, h, l) : czero<T>(), n0, E1, E2, &w0);
+        u1 = scheme_update<T, KIND>(st, u1, rh ? sst.at(4, q, h, l) : czero<T>(), n1, E1, E2, &w1);
+        u2 = scheme_update<T, KIND>(st, u2, rh ? sst.at(5, q, h, l) : czero<T>(), n2, E1, E2, &w2);
         if (st.last) {
           if (k2 > 0.0) {
             const T kX = T(kxd), kY = T(ky), kZ = T(kzd);
