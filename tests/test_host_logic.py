@@ -140,3 +140,42 @@ def test_empty_band_clamps_and_flags(hostcheck_library):
     run, _ = make_case(N, uh=uh, forcing=0.1, library=hostcheck_library)
     run.advance(0.01)
     assert run.status_word() & 0x2
+
+
+@pytest.mark.parametrize("sf", [gbght.ConstantPower(0.2), gbght.VarianceController(0.5, turnover_time=1.0),
+                                gbght.VarianceRescaling(0.5, "total"), gbght.VarianceRescaling(0.5, "band")],
+                         ids=["constant_power", "controller", "rescale_total", "rescale_band"])
+def test_empty_scalar_band_is_left_alone_and_flagged(hostcheck_library, sf):
+    # src/Forcing.jl:110-111 with 575-596 and 1091-1101: an empty band gets no amplitude and no
+    # rescale. With u = 0 the scalar band stays empty through the step, so the scalar moves by
+    # diffusion alone, as the oracle's does, and the status word carries the empty-band bit.
+    from pairs import advance_both
+    N = 16
+    k2 = S.wavenumbers(N)[3]
+    ph = S.seed_scalar(N, 0.5, seed=1) * ~((k2 >= 0.25) & (k2 <= 6.25))
+    run, orun = make_case(N, uh=np.zeros((3, N, N, N // 2 + 1), complex), ph=ph, scalar_forcing=sf,
+                          library=hostcheck_library)
+    advance_both(run, orun, 3, dt=0.01)
+    ue, pe = run.export_state()
+    assert not np.any(ue)
+    assert np.linalg.norm(pe - orun.state.phih) <= 2e-14 * np.linalg.norm(orun.state.phih)
+    expected = ph * np.exp(-0.01 * k2 * 0.03)
+    assert np.max(np.abs(pe - expected)) <= 1e-14 * np.max(np.abs(ph))
+    assert run.status_word() & 0x2
+
+
+def test_empty_velocity_band_skips_the_rescale(hostcheck_library):
+    # a single shear mode on shell 3 has a gradient Lamb vector: the band 1–2 stays empty, the
+    # rescale is skipped, and the mode decays by viscosity alone
+    from pairs import advance_both, compare
+    N = 16
+    uh = np.zeros((3, N, N, N // 2 + 1), complex)   # u_x = sin 3y, exactly
+    uh[0, 0, 3, 0] = -0.5j * N ** 3
+    uh[0, 0, N - 3, 0] = 0.5j * N ** 3
+    run, orun = make_case(N, uh=uh, scalar=False, forcing=gbght.VarianceRescaling(0.45, "total"),
+                          library=hostcheck_library)
+    advance_both(run, orun, 2, dt=0.01)
+    compare(run, orun, tol=2e-14)
+    ue, _ = run.export_state()
+    assert np.max(np.abs(ue - uh * np.exp(-0.01 * 9 * 0.02))) <= 1e-13 * np.max(np.abs(uh))
+    assert run.status_word() & 0x2
