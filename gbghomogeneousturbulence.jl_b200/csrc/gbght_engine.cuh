@@ -80,7 +80,8 @@ class Engine {
   virtual const char* tracers_get(double* X) = 0;
   virtual const char* tracer_sample_get(double* F, int slot) = 0;
   virtual const char* tracer_sample_set(const double* F, int slot) = 0;
-  // mode 0: sample at the positions; 1: Heun push; 2: Heun push + sample at the new positions
+  // One Adams step of every tracer (J = 0: none) and, when w.out_slot ≥ 0, the sample at the new
+  // positions into that trail slot
   virtual const char* tracers_run(const AdamsStep& w) = 0;
   virtual const char* gather(const double* X, int64_t M, double* out) = 0;
   virtual const char* sync() = 0;

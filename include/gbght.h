@@ -230,9 +230,10 @@ int gbght_deposit_tracers(gbght_run* run, double t);
  * Replaces interpolate_at_particles!(out, u, tracers) (src/Particles.jl:290-293). */
 int gbght_interpolate_velocity(gbght_run* run, const double* X, int64_t M, double* out);
 
-/* One iteration of the run layer: Δt (dt > 0 fixed, dt <= 0 the CFL rule), step, deposit, tracer
- * push and particle deposit, blow-up guards, clock. The Δt taken is returned in *dt_taken (may be
- * NULL). Replaces advance!(sim; dt) (src/SimulationRun.jl:1155-1229). */
+/* One iteration of the run layer: Δt (dt > 0 fixed, dt <= 0 the CFL rule with the start-up bound
+ * under shortened_first_steps, where a fixed dt is refused), step, deposit, the particle scheme's
+ * push and the particle deposit, blow-up guards, clock. The Δt taken is returned in *dt_taken (may
+ * be NULL). Replaces advance!(sim; dt) (src/SimulationRun.jl:1155-1229). */
 int gbght_advance(gbght_run* run, double dt, double* dt_taken);
 
 /* The run's clock. Replaces current_time / current_step (src/SimulationRun.jl). */
@@ -255,10 +256,11 @@ enum gbght_kernel {
   GBGHT_KERNEL_Y_FORWARD = 2,   /* forward y-transform pass */
   GBGHT_KERNEL_Z_EPILOGUE = 3,  /* z-forward, IF-RK stage update, z-inverse */
   GBGHT_KERNEL_X_VELOCITY = 4,  /* deposit: physical velocity and max|u| */
-  GBGHT_KERNEL_FORCE_AMP = 5,   /* ConstantPower amplitude */
+  GBGHT_KERNEL_FORCE_AMP = 5,   /* band-forcing amplitudes, VarianceRescaling's rescale */
   GBGHT_KERNEL_REALITY = 6,     /* end-of-step reality projection */
-  GBGHT_KERNEL_TRACERS = 7,     /* tracer gather / Heun push */
-  GBGHT_KERNEL_OBSERVABLES = 8, /* k, ε, ⟨φ²⟩, ε_φ reduction */
+  GBGHT_KERNEL_TRACERS = 7,     /* tracer gather / Adams push */
+  GBGHT_KERNEL_OBSERVABLES = 8, /* k, ε, ⟨φ²⟩, ε_φ reductions, their row sums for the band forcings,
+                                   the diagnostics' reductions */
   GBGHT_KERNEL_TRAVERSAL = 9    /* tracer traversal order: tile keys, scan, scatter */
 };
 int gbght_profile(gbght_run* run, int enable);
