@@ -29,7 +29,7 @@ def test_decaying_64_cubed_100_steps(cuda_library):
     assert np.max(np.abs(F - orun.f0)) < 1e-10
 
 
-@pytest.mark.parametrize("N,steps", [(32, 20), (48, 5), (12, 10), (16, 10)])
+@pytest.mark.parametrize("N,steps", [(32, 20), (48, 5), (12, 10), (16, 10), (8, 10), (24, 10)])
 def test_forced_with_mean_gradient_cfl(cuda_library, N, steps):
     run, orun = make_case(N, viscosity=0.01, forcing=0.1, G=(1.0, 0.0, 0.0), tracers=256, library=cuda_library)
     taken = advance_both(run, orun, steps, dt=None)
@@ -51,9 +51,10 @@ def test_larger_grids_short(cuda_library):
         compare(run, orun, tol=1e-12)
 
 
-@pytest.mark.parametrize("N,precision", [(192, "fp64"), (256, "fp64"), (256, "fp32_mixed")])
+@pytest.mark.parametrize("N,precision", [(192, "fp64"), (256, "fp64"), (256, "fp32_mixed"), (384, "fp64")])
 def test_production_paths_one_step(cuda_library, N, precision):
-    # The paths the 512³ benchmark runs, on a radix-3 plan (192 = 8·3·8) and on 256 = 8·4·8:
+    # The paths the 512³ benchmark runs, on radix-3 plans (192 = 8·3·8, 384 = 8·2·3·8) and on
+    # 256 = 8·4·8:
     # - TMEM-resident z rows;
     # - the FP64 turnaround with the φ lines transformed aside;
     # - the FP32 occupancy of the y and z passes;
