@@ -8,6 +8,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "gbght_engine.cuh"
 
@@ -438,6 +439,151 @@ int gbght_step(gbght_run* r, double dt) {
 int gbght_deposit(gbght_run* r) {
   if (check_run(r)) return GBGHT_ERR_ARGUMENT;
   return do_deposit(r);
+}
+
+struct gbght_ensemble {
+  std::vector<gbght_run*> members;
+  std::string err;
+#ifndef GBGHT_EMU
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t exec = nullptr;
+  double exec_dt = 0.0;
+#endif
+};
+
+namespace {
+int ens_fail(gbght_ensemble* e, int code, const std::string& m) {
+  e->err = m;
+  return code;
+}
+#ifndef GBGHT_EMU
+void ens_release_graph(gbght_ensemble* e) {
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  e->exec = nullptr;
+}
+// Capture every member's step and deposit launches as one graph: member 0's stream forks to the
+// others through an event and joins them back at the end.
+int ens_capture(gbght_ensemble* e, double dt) {
+  ens_release_graph(e);
+  cudaStream_t s0 = static_cast<cudaStream_t>(e->members[0]->eng->cuda_stream());
+  cudaError_t ce = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal);
+  if (ce != cudaSuccess) return ens_fail(e, GBGHT_ERR_CUDA, std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(ce));
+  const char* err = nullptr;
+  cudaEventRecord(e->fork, s0);
+  for (size_t i = 1; i < e->members.size(); ++i)
+    cudaStreamWaitEvent(static_cast<cudaStream_t>(e->members[i]->eng->cuda_stream()), e->fork, 0);
+  for (gbght_run* m : e->members) {
+    const Tableau t = tableau(m->cfg.scheme);
+    if (!err) err = m->eng->step(dt, t.a, t.b, t.d, t.S);
+    if (!err) err = m->eng->deposit_launch();
+  }
+  for (size_t i = 1; i < e->members.size(); ++i) {
+    cudaEventRecord(e->join[i], static_cast<cudaStream_t>(e->members[i]->eng->cuda_stream()));
+    cudaStreamWaitEvent(s0, e->join[i], 0);
+  }
+  cudaGraph_t graph = nullptr;
+  ce = cudaStreamEndCapture(s0, &graph);
+  if (err || ce != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return ens_fail(e, GBGHT_ERR_CUDA, err ? std::string(err) : std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce));
+  }
+  ce = cudaGraphInstantiate(&e->exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ce != cudaSuccess) {
+    e->exec = nullptr;
+    return ens_fail(e, GBGHT_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ce));
+  }
+  e->exec_dt = dt;
+  return GBGHT_OK;
+}
+#endif
+}  // namespace
+
+int gbght_ensemble_create(gbght_ensemble** out, gbght_run* const* members, int n) {
+  if (!out || !members || n < 1) {
+    g_global_error = "an ensemble needs at least one member";
+    return GBGHT_ERR_ARGUMENT;
+  }
+  *out = nullptr;
+  auto e = std::make_unique<gbght_ensemble>();
+  for (int i = 0; i < n; ++i) {
+    if (!members[i]) {
+      g_global_error = "a member is null";
+      return GBGHT_ERR_ARGUMENT;
+    }
+    for (gbght_run* m : e->members)
+      if (m == members[i]) {
+        g_global_error = "a run appears twice in the ensemble";
+        return GBGHT_ERR_ARGUMENT;
+      }
+    if (members[i]->cfg.device != members[0]->cfg.device) {
+      g_global_error = "the members must share one device";
+      return GBGHT_ERR_ARGUMENT;
+    }
+    e->members.push_back(members[i]);
+  }
+#ifndef GBGHT_EMU
+  cudaError_t ce = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+  e->join.assign(size_t(n), nullptr);
+  for (int i = 1; i < n && ce == cudaSuccess; ++i) ce = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming);
+  if (ce != cudaSuccess) {
+    g_global_error = std::string("cudaEventCreate: ") + cudaGetErrorString(ce);
+    return GBGHT_ERR_CUDA;
+  }
+#endif
+  *out = e.release();
+  return GBGHT_OK;
+}
+
+void gbght_ensemble_destroy(gbght_ensemble* e) {
+  if (!e) return;
+#ifndef GBGHT_EMU
+  ens_release_graph(e);
+  if (e->fork) cudaEventDestroy(e->fork);
+  for (cudaEvent_t ev : e->join)
+    if (ev) cudaEventDestroy(ev);
+#endif
+  delete e;
+}
+
+const char* gbght_ensemble_last_error(const gbght_ensemble* e) { return e ? e->err.c_str() : "null ensemble"; }
+
+int gbght_ensemble_step(gbght_ensemble* e, double dt) {
+  if (!e) return GBGHT_ERR_ARGUMENT;
+  if (!finite_positive(dt))
+    return ens_fail(e, GBGHT_ERR_ARGUMENT, "the timestep must be positive and finite, got " + std::to_string(dt));
+  // every member starts from a current deposit whose slots the first stage may reuse
+  for (gbght_run* m : e->members) {
+    if (m->deposit_epoch != m->fields_epoch || !m->eng->deposit_fresh()) {
+      if (int rc = do_deposit(m)) return ens_fail(e, rc, m->err);
+    }
+    if (m->eng->profiling()) return ens_fail(e, GBGHT_ERR_ARGUMENT, "a member has per-launch profiling on");
+  }
+#ifdef GBGHT_EMU
+  for (gbght_run* m : e->members) {
+    const Tableau t = tableau(m->cfg.scheme);
+    if (int rc = engine_call(m, m->eng->step(dt, t.a, t.b, t.d, t.S))) return ens_fail(e, rc, m->err);
+    m->fields_epoch += 1;
+    if (int rc = do_deposit(m)) return ens_fail(e, rc, m->err);
+  }
+  return GBGHT_OK;
+#else
+  if (!e->exec || e->exec_dt != dt)
+    if (int rc = ens_capture(e, dt)) return rc;
+  cudaStream_t s0 = static_cast<cudaStream_t>(e->members[0]->eng->cuda_stream());
+  cudaError_t ce = cudaGraphLaunch(e->exec, s0);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(s0);
+  if (ce != cudaSuccess) return ens_fail(e, GBGHT_ERR_CUDA, std::string("ensemble graph: ") + cudaGetErrorString(ce));
+  for (gbght_run* m : e->members) {
+    m->fields_epoch += 1;
+    double m2 = 0.0;
+    if (int rc = engine_call(m, m->eng->deposit_read(&m2))) return ens_fail(e, rc, m->err);
+    m->max_speed = std::sqrt(m2);
+    m->deposit_epoch = m->fields_epoch;
+  }
+  return GBGHT_OK;
+#endif
 }
 
 int gbght_max_speed(gbght_run* r, double* speed) {

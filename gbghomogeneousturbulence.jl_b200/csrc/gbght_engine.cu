@@ -350,12 +350,28 @@ class EngineImpl final : public Engine {
   }
 
   const char* deposit(double* max_speed2) override {
+    if (const char* err = deposit_launch()) return err;
+    return deposit_read(max_speed2);
+  }
+  const char* deposit_launch() override {
     const char* err = rt_memset(maxbits_, 0, sizeof(unsigned long long), stream_);
     if (err) return err;
     y_inverse(0, 3);
     bu_fresh_ = true;
     x_velocity();
-    if ((err = rt_check())) return err;
+    return rt_check();
+  }
+  void* cuda_stream() const override {
+#ifdef GBGHT_EMU
+    return nullptr;
+#else
+    return stream_;
+#endif
+  }
+  bool deposit_fresh() const override { return bu_fresh_; }
+  bool profiling() const override { return prof_on_; }
+  const char* deposit_read(double* max_speed2) override {
+    const char* err = nullptr;
     unsigned long long bits = 0;
     if ((err = rt_d2h(&bits, maxbits_, sizeof bits, stream_))) return err;
     double m;

@@ -66,6 +66,16 @@ class Engine {
   virtual const char* export_state(double* uh, double* ph) = 0;
   virtual const char* step(double dt, const double* a, const double* b, const double* d, int S) = 0;
   virtual const char* deposit(double* max_speed2) = 0;
+  // The deposit split in two: its launches alone (no host synchronisation, so a CUDA graph can
+  // hold them), and the readback of max|u|² and of the device status once they have run.
+  virtual const char* deposit_launch() = 0;
+  virtual const char* deposit_read(double* max_speed2) = 0;
+  // The run's CUDA stream (nullptr in the host-check build); whether B slots 0..2 hold the
+  // deposit's y-inverse (the next step's first stage reuses them); whether per-launch profiling
+  // is on (its events cannot sit in a captured graph).
+  virtual void* cuda_stream() const = 0;
+  virtual bool deposit_fresh() const = 0;
+  virtual bool profiling() const = 0;
   virtual const char* velocity_export(double* u) = 0;
   virtual const char* velocity_import(const double* u) = 0;
   virtual const char* observables(Observables* o) = 0;

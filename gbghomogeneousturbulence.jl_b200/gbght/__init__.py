@@ -87,6 +87,10 @@ _SIGNATURES = {
     "gbght_state_export": (C.c_int, [C.c_void_p, _DP, _DP]),
     "gbght_step": (C.c_int, [C.c_void_p, C.c_double]),
     "gbght_recommended_cfl": (C.c_int, [C.c_int, _DP]),
+    "gbght_ensemble_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int]),
+    "gbght_ensemble_destroy": (None, [C.c_void_p]),
+    "gbght_ensemble_step": (C.c_int, [C.c_void_p, C.c_double]),
+    "gbght_ensemble_last_error": (C.c_char_p, [C.c_void_p]),
     "gbght_deposit": (C.c_int, [C.c_void_p]),
     "gbght_max_speed": (C.c_int, [C.c_void_p, _DP]),
     "gbght_cfl_timestep": (C.c_int, [C.c_void_p, _DP]),
@@ -475,6 +479,40 @@ class Run:
         ms = C.c_double()
         self._check(self.lib.gbght_timer(self.h, 1, C.byref(ms)))
         return ms.value
+
+
+class Ensemble:
+    """Runs stepped together (`gbght_ensemble_*`): `step(dt)` is `step(dt)` then `deposit()` of
+    every member, one captured CUDA graph per dt on the GPU. The members stay usable runs."""
+
+    def __init__(self, runs):
+        self.runs = list(runs)
+        if not self.runs:
+            raise ValueError("an ensemble needs at least one member")
+        self.lib = self.runs[0].lib
+        arr = (C.c_void_p * len(self.runs))(*[r.h.value for r in self.runs])
+        h = C.c_void_p()
+        rc = self.lib.gbght_ensemble_create(C.byref(h), arr, len(self.runs))
+        if rc != OK:
+            raise (ValueError if rc == ERR_ARGUMENT else DeviceError)(self.lib.gbght_global_error().decode())
+        self.h = h
+
+    def step(self, dt: float):
+        rc = self.lib.gbght_ensemble_step(self.h, float(dt))
+        if rc != OK:
+            msg = self.lib.gbght_ensemble_last_error(self.h).decode()
+            raise {ERR_ARGUMENT: ValueError, ERR_SCHEDULE: ScheduleError}.get(rc, DeviceError)(msg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.gbght_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def recommended_cfl(scheme: str, library: str | None = None) -> float:

@@ -149,6 +149,20 @@ int gbght_state_export(gbght_run* run, double* u_hat, double* phi_hat);
  * 456-544,599-691). */
 int gbght_step(gbght_run* run, double dt);
 
+/* An ensemble of runs stepped together: members of any supported sizes and configurations, on one
+ * device, each a distinct run. gbght_ensemble_step is gbght_step then gbght_deposit for every
+ * member with the same dt. On the GPU the members' launches are captured once per dt as one CUDA
+ * graph whose branches run on the members' own streams (so small grids run side by side), and the
+ * graph is replayed on later calls; the max-speed readbacks follow the replay. A member whose
+ * deposit is not current, or whose deposit slots were reused by another call since, is deposited
+ * first. Tracers are not moved (as with gbght_step). The ensemble holds the member handles, which
+ * must outlive it. The batching form of the configs: ensembles of uneven grids (32³, 48³, 64³). */
+typedef struct gbght_ensemble gbght_ensemble;
+int gbght_ensemble_create(gbght_ensemble** out, gbght_run* const* members, int n);
+void gbght_ensemble_destroy(gbght_ensemble* ensemble);
+int gbght_ensemble_step(gbght_ensemble* ensemble, double dt);
+const char* gbght_ensemble_last_error(const gbght_ensemble* ensemble);
+
 /* A scheme's advective-CFL ceiling under the 2/3 rule: 0.96 (RK4), 0.5 (RK3, SSPRK3), 0.25 (Heun).
  * Replaces recommended_cfl(scheme, domain) (src/Propagator.jl:906-919) for TwoThirds. */
 int gbght_recommended_cfl(int scheme, double* cfl);

@@ -358,3 +358,59 @@ def test_full_size_512_cubed_properties(cuda_library):
         ref, got = spectra["fp64"][i], spectra["fp32_mixed"][i]
         live = ref > 1e-6 * ref.max()
         assert np.max(np.abs(got[live] - ref[live]) / ref[live]) < 1e-5
+
+
+def test_ensemble_graph_equals_separate_runs(cuda_library):
+    # one captured CUDA graph over members of uneven sizes, schemes and forcings (each on its own
+    # stream), replayed: bitwise the runs stepped alone
+    def members():
+        return [make_case(32, forcing=0.1, library=cuda_library)[0],
+                make_case(48, scalar=False, scheme="IFLowStorageRK3", library=cuda_library)[0],
+                make_case(64, forcing=gbght.Linear(0.3), scheme="IFSSPRK3", library=cuda_library)[0],
+                make_case(64, forcing=0.1, precision="fp32_mixed", library=cuda_library)[0]]
+    ens_runs, alone = members(), members()
+    ens = gbght.Ensemble(ens_runs)
+    for k in range(4):
+        dt = 0.004 if k < 3 else 0.003   # a new dt captures a new graph
+        ens.step(dt)
+        for r in alone:
+            r.step(dt)
+            r.deposit()
+    for a, b in zip(ens_runs, alone):
+        ua, pa = a.export_state()
+        ub, pb = b.export_state()
+        assert np.array_equal(ua, ub) and (pa is None or np.array_equal(pa, pb))
+        assert a.max_speed() == b.max_speed()
+    ens.close()
+
+
+def test_ensemble_of_uneven_grids_throughput(cuda_library):
+    # 96 FP32-mixed members, 32 each of 32³, 48³ and 64³, ν drawn per member from a seed: the
+    # graph-replayed ensemble step against stepping the members one by one
+    import time
+    rng = np.random.default_rng(7)
+    runs = []
+    for i, N in enumerate([32] * 32 + [48] * 32 + [64] * 32):
+        nu = float(rng.uniform(0.005, 0.02))
+        runs.append(make_case(N, viscosity=nu, forcing=0.1, precision="fp32_mixed", seeds=(i, i + 1000, i + 2000),
+                              library=cuda_library)[0])
+    ens = gbght.Ensemble(runs)
+    ens.step(0.002)          # capture
+    K = 20
+    runs[0].synchronize()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        ens.step(0.002)
+    t_graph = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for _ in range(K):
+        for r in runs:
+            r.step(0.002)
+            r.deposit()
+    t_seq = time.perf_counter() - t0
+    pts = sum(r.N ** 3 for r in runs)
+    print(f"\nensemble 96 members (32x 32^3, 48^3, 64^3), FP32-mixed, IF-RK4: graph {K * 96 / t_graph:.0f} "
+          f"member-steps/s ({5 * pts * K / t_graph:.3e} grid-point-stages/s), one by one "
+          f"{K * 96 / t_seq:.0f} member-steps/s, ratio {t_seq / t_graph:.2f}")
+    assert t_graph < t_seq
+    ens.close()

@@ -89,6 +89,29 @@ def test_recommended_cfl(hostcheck_library):
         gbght.recommended_cfl("IFEuler", library=hostcheck_library)
 
 
+def test_ensemble_steps_equal_separate_runs(hostcheck_library):
+    # members of uneven sizes and configurations stepped together equal the same runs stepped alone
+    def members():
+        return [make_case(12, forcing=0.1, library=hostcheck_library)[0],
+                make_case(16, scalar=False, scheme="IFLowStorageRK3", library=hostcheck_library)[0],
+                make_case(24, forcing=gbght.Linear(0.3), scheme="IFHeun", library=hostcheck_library)[0]]
+    ens_runs, alone = members(), members()
+    ens = gbght.Ensemble(ens_runs)
+    for _ in range(3):
+        ens.step(0.01)
+        for r in alone:
+            r.step(0.01)
+            r.deposit()
+    for a, b in zip(ens_runs, alone):
+        ua, pa = a.export_state()
+        ub, pb = b.export_state()
+        assert np.array_equal(ua, ub) and (pa is None or np.array_equal(pa, pb))
+        assert a.max_speed() == b.max_speed()
+    ens.close()
+    with pytest.raises(ValueError, match="twice"):
+        gbght.Ensemble([ens_runs[0], ens_runs[0]])
+
+
 def test_rk3_and_cfl_steps_match(hostcheck_library):
     run, orun = make_case(16, forcing=0.2, scheme="IFLowStorageRK3", tracers=16, library=hostcheck_library)
     taken = advance_both(run, orun, 5, dt=None)
