@@ -26,6 +26,11 @@ reference's own known-answer tests, re-expressed in ``tests/test_oracle_known_an
 - the Linear rate's exact growth of a single mode, and the Linear scalar's variance growth;
 - VarianceController's amplitude, its scalar dissipation, the marginal law at gain 0 and the
   order kept; VarianceRescaling's uniform rescale on an unbounded band and its first order;
+- the box-mean definition behind the energy below scale, and the skewness identities.
+
+The tangent-linear model and discrete adjoint of the low-storage step (``step_tangent``,
+``step_adjoint``) have no counterpart in the reference, which has no AD. They are pinned by central
+finite differences and by the dot-product identity ⟨Jv, w⟩ = ⟨v, Jᵀw⟩.
 - injected power equal to ε, and a solenoidal state;
 - the 2/3 closed ball against a 2N zero-padded product;
 - Parseval, and the planted reality violation;
@@ -431,6 +436,158 @@ def _step_low_storage(dom: Domain, cond: Conditions, st: State, dt: float, schem
             if i < len(a) - 1:
                 hp = Ep * hp
     return _close(dom, cond, uh, ph, eps_T)
+
+
+# ---------------------------------------------------------------------------------------------
+# Tangent-linear model and discrete adjoint of the low-storage step, velocity only: the checker
+# for a GPU adjoint of the step. The reference has no AD; these are derived here from the step's
+# own operations, and pinned by central finite differences and the dot-product identity.
+# Inner products: physical ⟨a, b⟩ = Σ_x a·b; spectral ⟨x, y⟩ = Σ w·Re(conj(x)·y), w the Hermitian
+# weights. Then irfft* = rfft/N³ and rfft* = N³·irfft; ℙ (with the mask), the curl iκ×, the
+# integrating factor and the reality projection are self-adjoint; for m = u×ω the adjoint sends
+# m̄ to ū = ω×m̄ and ω̄ = m̄×u.
+# ---------------------------------------------------------------------------------------------
+
+def spectral_dot(dom: Domain, x: np.ndarray, y: np.ndarray) -> float:
+    return float(np.sum((np.conj(x) * y).real * dom.hweight))
+
+
+def _cross(a, b):
+    return np.stack([a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]])
+
+
+def _tangent_supported(cond: Conditions, scheme: str):
+    if scheme not in ("rk4", "rk3"):
+        raise ValueError("the tangent and adjoint are restated for the low-storage schemes")
+    for f in (cond.velocity_forcing, cond.scalar_forcing):
+        if f is not None and not isinstance(f, Linear):
+            raise ValueError("the tangent and adjoint are restated for no forcing or a steady Linear rate")
+
+
+def _nonlinear(dom: Domain, u, w):
+    """N̂ = 𝔻ℙ FFT(u×ω), κ = 0 zeroed (the unforced part of `velocity_rhs`)."""
+    nh = leray(dom, dom.to_spectral(_cross(u, w)), dom.mask)
+    nh[:, 0, 0, 0] = 0.0
+    return nh
+
+
+def _flux_divergence(dom: Domain, f):
+    """−𝔻 iκ·FFT(f) (the advective part of `scalar_rhs`)."""
+    fh = dom.to_spectral(f)
+    return -(dom.mask * (1j * ((dom.dkx * fh[0] + dom.dky * fh[1]) + dom.dkz * fh[2])))
+
+
+def _gradient_source(cond: Conditions, uh):
+    G = cond.mean_gradient
+    return -((G[0] * uh[0] + G[1] * uh[1]) + G[2] * uh[2])
+
+
+def step_tangent(dom: Domain, cond: Conditions, uh: np.ndarray, duh: np.ndarray, dt: float,
+                 scheme: str = "rk4", ph: np.ndarray | None = None, dph: np.ndarray | None = None):
+    """One step F of `_step_low_storage` and its tangent J·δ in the same pass, for the velocity
+    alone (ph None) or the coupled velocity + scalar. Returns (F_u, J_u) or (F_u, F_φ, J_u, J_φ)."""
+    _tangent_supported(cond, scheme)
+    a, b, d = TABLEAUX[scheme]
+    scalar = ph is not None
+    rate_u = steady_rate(dom, cond.velocity_forcing)
+    rate_p = steady_rate(dom, cond.scalar_forcing) if scalar else None
+    q, dq = uh.copy(), duh.copy()
+    if scalar:
+        p, dp = ph.copy(), dph.copy()
+    h = dh = hp = dhp = None
+    for i in range(len(a)):
+        u, w = dom.to_physical(q), dom.to_physical(curl(dom, q))
+        du, dw = dom.to_physical(dq), dom.to_physical(curl(dom, dq))
+        n = _nonlinear(dom, u, w)
+        dn = _nonlinear(dom, du, w) + _nonlinear(dom, u, dw)
+        if scalar:
+            phi, dphi = dom.to_physical(p), dom.to_physical(dp)
+            npp = _flux_divergence(dom, u * phi[None]) + _gradient_source(cond, q)
+            dnp = _flux_divergence(dom, du * phi[None] + u * dphi[None]) + _gradient_source(cond, dq)
+        h = dt * n if i == 0 else a[i] * h + dt * n
+        dh = dt * dn if i == 0 else a[i] * dh + dt * dn
+        E = integrating_factor(dom, cond.viscosity, rate_u, d[i] * dt)
+        q, dq = E * (q + b[i] * h), E * (dq + b[i] * dh)
+        if i < len(a) - 1:
+            h, dh = E * h, E * dh
+        if scalar:
+            hp = dt * npp if i == 0 else a[i] * hp + dt * npp
+            dhp = dt * dnp if i == 0 else a[i] * dhp + dt * dnp
+            Ep = integrating_factor(dom, cond.diffusivity, rate_p, d[i] * dt)
+            p, dp = Ep * (p + b[i] * hp), Ep * (dp + b[i] * dhp)
+            if i < len(a) - 1:
+                hp, dhp = Ep * hp, Ep * dhp
+    q, dq = reality_projection(dom, leray(dom, q)), reality_projection(dom, leray(dom, dq))
+    if not scalar:
+        return q, dq
+    return q, reality_projection(dom, p), dq, reality_projection(dom, dp)
+
+
+def step_adjoint(dom: Domain, cond: Conditions, uh: np.ndarray, lam: np.ndarray, dt: float,
+                 scheme: str = "rk4", ph: np.ndarray | None = None, lam_p: np.ndarray | None = None):
+    """Jᵀ·λ for the step at (û, φ̂): a forward pass that keeps each stage's fields, then the stages
+    in reverse, each operation replaced by its adjoint. Returns λ_u, or (λ_u, λ_φ) with a scalar."""
+    _tangent_supported(cond, scheme)
+    a, b, d = TABLEAUX[scheme]
+    S = len(a)
+    scalar = ph is not None
+    rate_u = steady_rate(dom, cond.velocity_forcing)
+    rate_p = steady_rate(dom, cond.scalar_forcing) if scalar else None
+    N3 = float(dom.N) ** 3
+    q = uh.copy()
+    p = ph.copy() if scalar else None
+    h = hp = None
+    saved = []
+    for i in range(S):
+        u, w = dom.to_physical(q), dom.to_physical(curl(dom, q))
+        phi = dom.to_physical(p) if scalar else None
+        saved.append((u, w, phi))
+        n = _nonlinear(dom, u, w)
+        h = dt * n if i == 0 else a[i] * h + dt * n
+        E = integrating_factor(dom, cond.viscosity, rate_u, d[i] * dt)
+        if scalar:
+            npp = _flux_divergence(dom, u * phi[None]) + _gradient_source(cond, q)
+            hp = dt * npp if i == 0 else a[i] * hp + dt * npp
+            Ep = integrating_factor(dom, cond.diffusivity, rate_p, d[i] * dt)
+        q = E * (q + b[i] * h)
+        if i < S - 1:
+            h = E * h
+        if scalar:
+            p = Ep * (p + b[i] * hp)
+            if i < S - 1:
+                hp = Ep * hp
+    lq = leray(dom, reality_projection(dom, lam))   # the end-of-step projections
+    lp = reality_projection(dom, lam_p) if scalar else None
+    lh_next = np.zeros_like(lq)                     # adjoints of the registers carried out of stage i
+    lhp_next = np.zeros_like(lp) if scalar else None
+    G = cond.mean_gradient
+    for i in range(S - 1, -1, -1):
+        E = integrating_factor(dom, cond.viscosity, rate_u, d[i] * dt)
+        lv = E * lq                                 # q' = E·v, v = q + b h'
+        lh = b[i] * lv + (E * lh_next if i < S - 1 else 0.0)
+        ln = dt * lh
+        lh_next = a[i] * lh if i > 0 else np.zeros_like(lh)
+        u, w, phi = saved[i]
+        lF = leray(dom, ln, dom.mask)
+        lF[:, 0, 0, 0] = 0.0
+        lm = N3 * dom.to_physical(lF)
+        lu, lw = _cross(w, lm), _cross(lm, u)
+        lq_new = lv.copy()
+        if scalar:
+            Ep = integrating_factor(dom, cond.diffusivity, rate_p, d[i] * dt)
+            lvp = Ep * lp
+            lhp = b[i] * lvp + (Ep * lhp_next if i < S - 1 else 0.0)
+            lnp = dt * lhp
+            lhp_next = a[i] * lhp if i > 0 else np.zeros_like(lhp)
+            # ψ = Σ_c (−i 𝔻 κ_c) f̂_c − G·q with f = uφ
+            lfh = np.stack([1j * dom.mask * dk * lnp for dk in (dom.dkx, dom.dky, dom.dkz)])
+            lf = N3 * dom.to_physical(lfh)
+            lu = lu + lf * phi[None]
+            lphi = (lf[0] * u[0] + lf[1] * u[1]) + lf[2] * u[2]
+            lq_new = lq_new - np.stack([G[0] * lnp, G[1] * lnp, G[2] * lnp])
+            lp = lvp + dom.to_spectral(lphi) / N3
+        lq = lq_new + dom.to_spectral(lu) / N3 + curl(dom, dom.to_spectral(lw)) / N3
+    return lq if not scalar else (lq, lp)
 
 
 def _step_heun(dom: Domain, cond: Conditions, st: State, dt: float) -> State:

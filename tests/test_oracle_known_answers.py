@@ -775,3 +775,107 @@ def test_skewness_denominator_dirichlet_route():
     s = O.strain_physical(dom, uh)
     direct = float((s[:3] ** 2).sum() + 2 * (s[3:] ** 2).sum()) / N ** 3
     assert direct == pytest.approx(dom.inner(uh, uh, dom.k2) / 2, rel=1e-12)
+
+
+# --- the tangent-linear model and the discrete adjoint of the step (the adjoint form's checker) ---
+
+def _random_state(dom, seed):
+    v = S.seed_velocity(dom.N, 0.3, seed=seed)
+    return O.reality_projection(dom, O.leray(dom, v, dom.mask))
+
+
+@pytest.mark.parametrize("scheme,forcing", [("rk4", None), ("rk3", None), ("rk4", O.Linear(0.4))])
+def test_tangent_matches_central_differences(scheme, forcing):
+    # J·δû against (F(û + εδû) − F(û − εδû))/(2ε), relative 1e-6
+    dom = O.Domain(16)
+    cond = O.Conditions(viscosity=0.02, scalar=False, velocity_forcing=forcing)
+    uh, v = S.seed_velocity(16, 0.5, seed=3), _random_state(dom, 4)
+    dt, eps = 0.02, 1e-5
+    F0, Jv = O.step_tangent(dom, cond, uh, v, dt, scheme)
+    Fp = O.step(dom, cond, O.State(uh + eps * v), dt, scheme).uh
+    Fm = O.step(dom, cond, O.State(uh - eps * v), dt, scheme).uh
+    assert np.array_equal(F0, O.step(dom, cond, O.State(uh), dt, scheme).uh)
+    fd = (Fp - Fm) / (2 * eps)
+    assert np.linalg.norm(Jv - fd) / np.linalg.norm(fd) < 1e-6
+
+
+@pytest.mark.parametrize("scheme,forcing", [("rk4", None), ("rk3", None), ("rk4", O.Linear(0.4))])
+def test_adjoint_dot_product_identity(scheme, forcing):
+    # ⟨J v, w⟩ = ⟨v, Jᵀ w⟩ to round-off, for states in the retained, Hermitian space
+    dom = O.Domain(16)
+    cond = O.Conditions(viscosity=0.02, scalar=False, velocity_forcing=forcing)
+    uh = S.seed_velocity(16, 0.5, seed=5)
+    v, w = _random_state(dom, 6), _random_state(dom, 7)
+    _, Jv = O.step_tangent(dom, cond, uh, v, 0.02, scheme)
+    JTw = O.step_adjoint(dom, cond, uh, w, 0.02, scheme)
+    lhs, rhs = O.spectral_dot(dom, Jv, w), O.spectral_dot(dom, v, JTw)
+    assert lhs == pytest.approx(rhs, rel=1e-12)
+
+
+def test_adjoint_gradient_of_the_kinetic_energy():
+    # ∇ of k(F(û)) by the adjoint against central differences along three directions, 1e-6
+    dom = O.Domain(16)
+    cond = O.Conditions(viscosity=0.02, scalar=False)
+    uh = S.seed_velocity(16, 0.5, seed=8)
+    dt, eps = 0.02, 1e-5
+    F0 = O.step(dom, cond, O.State(uh), dt).uh
+    # k = ½Σw|û|²/N⁶, so its gradient in the spectral inner product is F/N⁶
+    grad = O.step_adjoint(dom, cond, uh, F0 / float(dom.N) ** 6, dt)
+    for seed in (9, 10, 11):
+        v = _random_state(dom, seed)
+        kp = O.kinetic_energy(dom, O.step(dom, cond, O.State(uh + eps * v), dt).uh)
+        km = O.kinetic_energy(dom, O.step(dom, cond, O.State(uh - eps * v), dt).uh)
+        assert O.spectral_dot(dom, grad, v) == pytest.approx((kp - km) / (2 * eps), rel=1e-6)
+
+
+def _random_scalar(dom, seed):
+    return O.reality_projection(dom, S.seed_scalar(dom.N, 0.3, seed=seed) * dom.mask)
+
+
+@pytest.mark.parametrize("G", [(0.0, 0.0, 0.0), (1.0, 0.0, 0.0)])
+def test_coupled_tangent_and_adjoint(G):
+    # the coupled velocity + scalar step (the benchmark's pair, with its mean gradient): the
+    # tangent against central differences, and the dot-product identity over both fields
+    dom = O.Domain(16)
+    cond = O.Conditions(viscosity=0.02, schmidt=0.7, mean_gradient=G, scalar_forcing=O.Linear(0.2))
+    uh, ph = S.seed_velocity(16, 0.5, seed=12), S.seed_scalar(16, 0.5, seed=13)
+    v, vp = _random_state(dom, 14), _random_scalar(dom, 15)
+    w, wp = _random_state(dom, 16), _random_scalar(dom, 17)
+    dt, eps = 0.02, 1e-5
+    Fu, Fp, Ju, Jp = O.step_tangent(dom, cond, uh, v, dt, ph=ph, dph=vp)
+    st0 = O.step(dom, cond, O.State(uh, ph), dt)
+    assert np.array_equal(Fu, st0.uh) and np.array_equal(Fp, st0.phih)
+    sp = O.step(dom, cond, O.State(uh + eps * v, ph + eps * vp), dt)
+    sm = O.step(dom, cond, O.State(uh - eps * v, ph - eps * vp), dt)
+    for J, fp, fm in ((Ju, sp.uh, sm.uh), (Jp, sp.phih, sm.phih)):
+        fd = (fp - fm) / (2 * eps)
+        assert np.linalg.norm(J - fd) / np.linalg.norm(fd) < 1e-6
+    lu, lp = O.step_adjoint(dom, cond, uh, w, dt, ph=ph, lam_p=wp)
+    lhs = O.spectral_dot(dom, Ju, w) + O.spectral_dot(dom, Jp, wp)
+    rhs = O.spectral_dot(dom, v, lu) + O.spectral_dot(dom, vp, lp)
+    assert lhs == pytest.approx(rhs, rel=1e-12)
+
+
+def test_adjoint_chained_over_steps():
+    # the gradient of k after three coupled steps: the one-step adjoint applied backwards over
+    # the stored step states (what a checkpointed gradient recomputes), against central differences
+    dom = O.Domain(16)
+    cond = O.Conditions(viscosity=0.02, mean_gradient=(0.0, 1.0, 0.0))
+    uh, ph = S.seed_velocity(16, 0.5, seed=18), S.seed_scalar(16, 0.5, seed=19)
+    dt, eps, n = 0.02, 1e-5, 3
+    states = [O.State(uh, ph)]
+    for _ in range(n):
+        states.append(O.step(dom, cond, states[-1], dt))
+    lu, lp = states[-1].uh / float(dom.N) ** 6, np.zeros_like(ph)   # ∇k in the spectral product
+    for st in reversed(states[:-1]):
+        lu, lp = O.step_adjoint(dom, cond, st.uh, lu, dt, ph=st.phih, lam_p=lp)
+
+    def k_after(du, dp):
+        st = O.State(uh + du, ph + dp)
+        for _ in range(n):
+            st = O.step(dom, cond, st, dt)
+        return O.kinetic_energy(dom, st.uh)
+
+    v, vp = _random_state(dom, 20), _random_scalar(dom, 21)
+    fd = (k_after(eps * v, eps * vp) - k_after(-eps * v, -eps * vp)) / (2 * eps)
+    assert O.spectral_dot(dom, v, lu) + O.spectral_dot(dom, vp, lp) == pytest.approx(fd, rel=1e-6)
