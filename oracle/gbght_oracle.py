@@ -440,7 +440,8 @@ def _step_low_storage(dom: Domain, cond: Conditions, st: State, dt: float, schem
 
 # ---------------------------------------------------------------------------------------------
 # Tangent-linear model and discrete adjoint of the low-storage step, velocity only: the checker
-# for a GPU adjoint of the step. The reference has no AD; these are derived here from the step's
+# for a GPU adjoint of the step (no forcing, Linear or ConstantPower on either field). The reference
+# has no AD; these are derived here from the step's
 # own operations, and pinned by central finite differences and the dot-product identity.
 # Inner products: physical ⟨a, b⟩ = Σ_x a·b; spectral ⟨x, y⟩ = Σ w·Re(conj(x)·y), w the Hermitian
 # weights. Then irfft* = rfft/N³ and rfft* = N³·irfft; ℙ (with the mask), the curl iκ×, the
@@ -460,8 +461,34 @@ def _tangent_supported(cond: Conditions, scheme: str):
     if scheme not in ("rk4", "rk3"):
         raise ValueError("the tangent and adjoint are restated for the low-storage schemes")
     for f in (cond.velocity_forcing, cond.scalar_forcing):
-        if f is not None and not isinstance(f, Linear):
-            raise ValueError("the tangent and adjoint are restated for no forcing or a steady Linear rate")
+        if f is not None and not isinstance(f, (Linear, ConstantPower)):
+            raise ValueError("the tangent and adjoint are restated for no forcing, Linear or ConstantPower")
+
+
+def _cp_source(dom: Domain, f, x, dx=None):
+    """ConstantPower's source s = A·𝟙_band·x at the stage field x, A = ε/(2 c⟨x, 𝟙x⟩), and its
+    tangent ds = δA·𝟙x + A·𝟙δx, δA = −2A·⟨𝟙x, δx⟩/⟨x, 𝟙x⟩ (the clamp to 0 has no tangent)."""
+    if not isinstance(f, ConstantPower):
+        return (0.0, 0.0) if dx is not None else 0.0
+    A, band = constant_power_amplitude(dom, f, x, np.finfo(np.float64).eps)
+    s = A * band * x
+    if dx is None:
+        return s
+    if A == 0.0:
+        return s, 0.0
+    dA = -2.0 * A * dom.inner(band * x, dx) / dom.inner(x, x, band)
+    return s, dA * band * x + A * band * dx
+
+
+def _cp_source_adjoint(dom: Domain, f, x, lam):
+    """The adjoint of x ↦ A(x)·𝟙x at x, applied to λ (spectral inner product)."""
+    if not isinstance(f, ConstantPower):
+        return 0.0
+    A, band = constant_power_amplitude(dom, f, x, np.finfo(np.float64).eps)
+    if A == 0.0:
+        return 0.0
+    # ⟨λ, δA·𝟙x⟩ = δA·⟨𝟙x, λ⟩ and δA = −2A⟨𝟙x, δx⟩/⟨x, 𝟙x⟩
+    return A * band * lam - (2.0 * A * dom.inner(band * x, lam) / dom.inner(x, x, band)) * (band * x)
 
 
 def _nonlinear(dom: Domain, u, w):
@@ -500,10 +527,14 @@ def step_tangent(dom: Domain, cond: Conditions, uh: np.ndarray, duh: np.ndarray,
         du, dw = dom.to_physical(dq), dom.to_physical(curl(dom, dq))
         n = _nonlinear(dom, u, w)
         dn = _nonlinear(dom, du, w) + _nonlinear(dom, u, dw)
+        su, dsu = _cp_source(dom, cond.velocity_forcing, q, dq)
+        n, dn = n + su, dn + dsu
         if scalar:
             phi, dphi = dom.to_physical(p), dom.to_physical(dp)
             npp = _flux_divergence(dom, u * phi[None]) + _gradient_source(cond, q)
             dnp = _flux_divergence(dom, du * phi[None] + u * dphi[None]) + _gradient_source(cond, dq)
+            sp, dsp = _cp_source(dom, cond.scalar_forcing, p, dp)
+            npp, dnp = npp + sp, dnp + dsp
         h = dt * n if i == 0 else a[i] * h + dt * n
         dh = dt * dn if i == 0 else a[i] * dh + dt * dn
         E = integrating_factor(dom, cond.viscosity, rate_u, d[i] * dt)
@@ -541,12 +572,13 @@ def step_adjoint(dom: Domain, cond: Conditions, uh: np.ndarray, lam: np.ndarray,
     for i in range(S):
         u, w = dom.to_physical(q), dom.to_physical(curl(dom, q))
         phi = dom.to_physical(p) if scalar else None
-        saved.append((u, w, phi))
-        n = _nonlinear(dom, u, w)
+        saved.append((u, w, phi, q, p))
+        n = _nonlinear(dom, u, w) + _cp_source(dom, cond.velocity_forcing, q)
         h = dt * n if i == 0 else a[i] * h + dt * n
         E = integrating_factor(dom, cond.viscosity, rate_u, d[i] * dt)
         if scalar:
             npp = _flux_divergence(dom, u * phi[None]) + _gradient_source(cond, q)
+            npp = npp + _cp_source(dom, cond.scalar_forcing, p)
             hp = dt * npp if i == 0 else a[i] * hp + dt * npp
             Ep = integrating_factor(dom, cond.diffusivity, rate_p, d[i] * dt)
         q = E * (q + b[i] * h)
@@ -567,12 +599,12 @@ def step_adjoint(dom: Domain, cond: Conditions, uh: np.ndarray, lam: np.ndarray,
         lh = b[i] * lv + (E * lh_next if i < S - 1 else 0.0)
         ln = dt * lh
         lh_next = a[i] * lh if i > 0 else np.zeros_like(lh)
-        u, w, phi = saved[i]
+        u, w, phi, qi, pi_ = saved[i]
         lF = leray(dom, ln, dom.mask)
         lF[:, 0, 0, 0] = 0.0
         lm = N3 * dom.to_physical(lF)
         lu, lw = _cross(w, lm), _cross(lm, u)
-        lq_new = lv.copy()
+        lq_new = lv + _cp_source_adjoint(dom, cond.velocity_forcing, qi, ln)
         if scalar:
             Ep = integrating_factor(dom, cond.diffusivity, rate_p, d[i] * dt)
             lvp = Ep * lp
@@ -585,7 +617,7 @@ def step_adjoint(dom: Domain, cond: Conditions, uh: np.ndarray, lam: np.ndarray,
             lu = lu + lf * phi[None]
             lphi = (lf[0] * u[0] + lf[1] * u[1]) + lf[2] * u[2]
             lq_new = lq_new - np.stack([G[0] * lnp, G[1] * lnp, G[2] * lnp])
-            lp = lvp + dom.to_spectral(lphi) / N3
+            lp = lvp + dom.to_spectral(lphi) / N3 + _cp_source_adjoint(dom, cond.scalar_forcing, pi_, lnp)
         lq = lq_new + dom.to_spectral(lu) / N3 + curl(dom, dom.to_spectral(lw)) / N3
     return lq if not scalar else (lq, lp)
 

@@ -784,7 +784,8 @@ def _random_state(dom, seed):
     return O.reality_projection(dom, O.leray(dom, v, dom.mask))
 
 
-@pytest.mark.parametrize("scheme,forcing", [("rk4", None), ("rk3", None), ("rk4", O.Linear(0.4))])
+@pytest.mark.parametrize("scheme,forcing", [("rk4", None), ("rk3", None), ("rk4", O.Linear(0.4)),
+                                            ("rk4", O.ConstantPower(0.1))])
 def test_tangent_matches_central_differences(scheme, forcing):
     # J·δû against (F(û + εδû) − F(û − εδû))/(2ε), relative 1e-6
     dom = O.Domain(16)
@@ -799,7 +800,8 @@ def test_tangent_matches_central_differences(scheme, forcing):
     assert np.linalg.norm(Jv - fd) / np.linalg.norm(fd) < 1e-6
 
 
-@pytest.mark.parametrize("scheme,forcing", [("rk4", None), ("rk3", None), ("rk4", O.Linear(0.4))])
+@pytest.mark.parametrize("scheme,forcing", [("rk4", None), ("rk3", None), ("rk4", O.Linear(0.4)),
+                                            ("rk4", O.ConstantPower(0.1))])
 def test_adjoint_dot_product_identity(scheme, forcing):
     # ⟨J v, w⟩ = ⟨v, Jᵀ w⟩ to round-off, for states in the retained, Hermitian space
     dom = O.Domain(16)
@@ -832,12 +834,16 @@ def _random_scalar(dom, seed):
     return O.reality_projection(dom, S.seed_scalar(dom.N, 0.3, seed=seed) * dom.mask)
 
 
-@pytest.mark.parametrize("G", [(0.0, 0.0, 0.0), (1.0, 0.0, 0.0)])
-def test_coupled_tangent_and_adjoint(G):
-    # the coupled velocity + scalar step (the benchmark's pair, with its mean gradient): the
-    # tangent against central differences, and the dot-product identity over both fields
+@pytest.mark.parametrize("G,vf,sf", [((0.0, 0.0, 0.0), None, O.Linear(0.2)),
+                                     ((1.0, 0.0, 0.0), O.ConstantPower(0.1), O.Linear(0.2)),
+                                     ((0.0, 0.0, 1.0), O.Linear(0.3), O.ConstantPower(0.05))],
+                         ids=["linear_phi", "benchmark_forcing", "cp_phi"])
+def test_coupled_tangent_and_adjoint(G, vf, sf):
+    # the coupled velocity + scalar step (the benchmark's pair: ConstantPower on the velocity, the
+    # mean gradient): the tangent against central differences, and the dot-product identity over
+    # both fields
     dom = O.Domain(16)
-    cond = O.Conditions(viscosity=0.02, schmidt=0.7, mean_gradient=G, scalar_forcing=O.Linear(0.2))
+    cond = O.Conditions(viscosity=0.02, schmidt=0.7, mean_gradient=G, velocity_forcing=vf, scalar_forcing=sf)
     uh, ph = S.seed_velocity(16, 0.5, seed=12), S.seed_scalar(16, 0.5, seed=13)
     v, vp = _random_state(dom, 14), _random_scalar(dom, 15)
     w, wp = _random_state(dom, 16), _random_scalar(dom, 17)
@@ -860,7 +866,7 @@ def test_adjoint_chained_over_steps():
     # the gradient of k after three coupled steps: the one-step adjoint applied backwards over
     # the stored step states (what a checkpointed gradient recomputes), against central differences
     dom = O.Domain(16)
-    cond = O.Conditions(viscosity=0.02, mean_gradient=(0.0, 1.0, 0.0))
+    cond = O.Conditions(viscosity=0.02, mean_gradient=(0.0, 1.0, 0.0), velocity_forcing=O.ConstantPower(0.1))
     uh, ph = S.seed_velocity(16, 0.5, seed=18), S.seed_scalar(16, 0.5, seed=19)
     dt, eps, n = 0.02, 1e-5, 3
     states = [O.State(uh, ph)]
