@@ -440,8 +440,8 @@ def _step_low_storage(dom: Domain, cond: Conditions, st: State, dt: float, schem
 
 # ---------------------------------------------------------------------------------------------
 # Tangent-linear model and discrete adjoint of the low-storage step, velocity only: the checker
-# for a GPU adjoint of the step (no forcing, Linear or ConstantPower on either field). The reference
-# has no AD; these are derived here from the step's
+# for a GPU adjoint of the step (the low-storage schemes, every band forcing on either field). The
+# reference has no AD; these are derived here from the step's
 # own operations, and pinned by central finite differences and the dot-product identity.
 # Inner products: physical ⟨a, b⟩ = Σ_x a·b; spectral ⟨x, y⟩ = Σ w·Re(conj(x)·y), w the Hermitian
 # weights. Then irfft* = rfft/N³ and rfft* = N³·irfft; ℙ (with the mask), the curl iκ×, the
@@ -460,35 +460,79 @@ def _cross(a, b):
 def _tangent_supported(cond: Conditions, scheme: str):
     if scheme not in ("rk4", "rk3"):
         raise ValueError("the tangent and adjoint are restated for the low-storage schemes")
-    for f in (cond.velocity_forcing, cond.scalar_forcing):
-        if f is not None and not isinstance(f, (Linear, ConstantPower)):
-            raise ValueError("the tangent and adjoint are restated for no forcing, Linear or ConstantPower")
 
 
-def _cp_source(dom: Domain, f, x, dx=None):
-    """ConstantPower's source s = A·𝟙_band·x at the stage field x, A = ε/(2 c⟨x, 𝟙x⟩), and its
-    tangent ds = δA·𝟙x + A·𝟙δx, δA = −2A·⟨𝟙x, δx⟩/⟨x, 𝟙x⟩ (the clamp to 0 has no tangent)."""
-    if not isinstance(f, ConstantPower):
+def _amplitude_gradient(dom: Domain, f, x, A, band, D):
+    """g with δA = ⟨g, δx⟩ (normalised inner product) for a per-stage amplitude A(x):
+    ConstantPower A = ε/(2c⟨x, 𝟙x⟩); VarianceController A = (2cD⟨x, κ²x⟩ − G(c⟨x, x⟩ − k∞)/tℓ)/(2c⟨x, 𝟙x⟩)."""
+    Ib = dom.inner(x, x, band)
+    g = -2.0 * A * band * x / Ib
+    if isinstance(f, VarianceController):
+        c = target_factor(x)
+        g = g + (4.0 * c * D * dom.k2 * x - 2.0 * f.gain * c * x / f.turnover_time) / (2.0 * c * Ib)
+    return g
+
+
+def _stage_source(dom: Domain, f, x, D, dx=None):
+    """A per-stage band source s = A(x)·𝟙x (ConstantPower, VarianceController) and its tangent
+    ds = δA·𝟙x + A·𝟙δx (an empty band's clamp to 0 has no tangent)."""
+    if not isinstance(f, (ConstantPower, VarianceController)):
         return (0.0, 0.0) if dx is not None else 0.0
-    A, band = constant_power_amplitude(dom, f, x, np.finfo(np.float64).eps)
+    A, band = constant_power_amplitude(dom, f, x, np.finfo(np.float64).eps, D)
     s = A * band * x
     if dx is None:
         return s
     if A == 0.0:
         return s, 0.0
-    dA = -2.0 * A * dom.inner(band * x, dx) / dom.inner(x, x, band)
+    dA = dom.inner(_amplitude_gradient(dom, f, x, A, band, D), dx)
     return s, dA * band * x + A * band * dx
 
 
-def _cp_source_adjoint(dom: Domain, f, x, lam):
-    """The adjoint of x ↦ A(x)·𝟙x at x, applied to λ (spectral inner product)."""
-    if not isinstance(f, ConstantPower):
+def _stage_source_adjoint(dom: Domain, f, x, D, lam):
+    """The adjoint of x ↦ A(x)·𝟙x at x, applied to λ: A·𝟙λ + ⟨𝟙x, λ⟩·g."""
+    if not isinstance(f, (ConstantPower, VarianceController)):
         return 0.0
-    A, band = constant_power_amplitude(dom, f, x, np.finfo(np.float64).eps)
+    A, band = constant_power_amplitude(dom, f, x, np.finfo(np.float64).eps, D)
     if A == 0.0:
         return 0.0
-    # ⟨λ, δA·𝟙x⟩ = δA·⟨𝟙x, λ⟩ and δA = −2A⟨𝟙x, δx⟩/⟨x, 𝟙x⟩
-    return A * band * lam - (2.0 * A * dom.inner(band * x, lam) / dom.inner(x, x, band)) * (band * x)
+    return A * band * lam + dom.inner(band * x, lam) * _amplitude_gradient(dom, f, x, A, band, D)
+
+
+def _rescale_parts(dom: Domain, f, x):
+    """VarianceRescaling's factor s at x and g with δs = ⟨g, δx⟩, or None when it leaves x alone."""
+    if not isinstance(f, VarianceRescaling):
+        return None
+    c = target_factor(x)
+    band = band_indicator(dom, f)
+    Ib, Iw = dom.inner(x, x, band), dom.inner(x, x)
+    if band_is_empty(Ib, Iw, np.finfo(np.float64).eps):
+        return None
+    bv = c * Ib
+    if f.over == "total":
+        Tb = f.target - c * Iw + bv
+        if Tb <= 0.0:
+            return 0.0, np.zeros_like(x), band
+        dTb = -2.0 * c * x + 2.0 * c * band * x
+    else:
+        Tb, dTb = f.target, np.zeros_like(x)
+    s = math.sqrt(Tb / bv)
+    return s, (s / 2.0) * (dTb / Tb - 2.0 * c * band * x / bv), band
+
+
+def _rescale_tangent(dom: Domain, f, x, dx):
+    parts = _rescale_parts(dom, f, x)
+    if parts is None:
+        return dx
+    s, g, band = parts
+    return dx + (s - 1.0) * band * dx + dom.inner(g, dx) * band * x
+
+
+def _rescale_adjoint(dom: Domain, f, x, lam):
+    parts = _rescale_parts(dom, f, x)
+    if parts is None:
+        return lam
+    s, g, band = parts
+    return lam + (s - 1.0) * band * lam + dom.inner(band * x, lam) * g
 
 
 def _nonlinear(dom: Domain, u, w):
@@ -527,13 +571,13 @@ def step_tangent(dom: Domain, cond: Conditions, uh: np.ndarray, duh: np.ndarray,
         du, dw = dom.to_physical(dq), dom.to_physical(curl(dom, dq))
         n = _nonlinear(dom, u, w)
         dn = _nonlinear(dom, du, w) + _nonlinear(dom, u, dw)
-        su, dsu = _cp_source(dom, cond.velocity_forcing, q, dq)
+        su, dsu = _stage_source(dom, cond.velocity_forcing, q, cond.viscosity, dq)
         n, dn = n + su, dn + dsu
         if scalar:
             phi, dphi = dom.to_physical(p), dom.to_physical(dp)
             npp = _flux_divergence(dom, u * phi[None]) + _gradient_source(cond, q)
             dnp = _flux_divergence(dom, du * phi[None] + u * dphi[None]) + _gradient_source(cond, dq)
-            sp, dsp = _cp_source(dom, cond.scalar_forcing, p, dp)
+            sp, dsp = _stage_source(dom, cond.scalar_forcing, p, cond.diffusivity, dp)
             npp, dnp = npp + sp, dnp + dsp
         h = dt * n if i == 0 else a[i] * h + dt * n
         dh = dt * dn if i == 0 else a[i] * dh + dt * dn
@@ -548,9 +592,14 @@ def step_tangent(dom: Domain, cond: Conditions, uh: np.ndarray, duh: np.ndarray,
             p, dp = Ep * (p + b[i] * hp), Ep * (dp + b[i] * dhp)
             if i < len(a) - 1:
                 hp, dhp = Ep * hp, Ep * dhp
+    # the forcings' post-step projections (VarianceRescaling), then the Leray and reality projections
+    dq = _rescale_tangent(dom, cond.velocity_forcing, q, dq)
+    q = project_forcing(dom, cond.velocity_forcing, q, np.finfo(np.float64).eps)
     q, dq = reality_projection(dom, leray(dom, q)), reality_projection(dom, leray(dom, dq))
     if not scalar:
         return q, dq
+    dp = _rescale_tangent(dom, cond.scalar_forcing, p, dp)
+    p = project_forcing(dom, cond.scalar_forcing, p, np.finfo(np.float64).eps)
     return q, reality_projection(dom, p), dq, reality_projection(dom, dp)
 
 
@@ -573,12 +622,12 @@ def step_adjoint(dom: Domain, cond: Conditions, uh: np.ndarray, lam: np.ndarray,
         u, w = dom.to_physical(q), dom.to_physical(curl(dom, q))
         phi = dom.to_physical(p) if scalar else None
         saved.append((u, w, phi, q, p))
-        n = _nonlinear(dom, u, w) + _cp_source(dom, cond.velocity_forcing, q)
+        n = _nonlinear(dom, u, w) + _stage_source(dom, cond.velocity_forcing, q, cond.viscosity)
         h = dt * n if i == 0 else a[i] * h + dt * n
         E = integrating_factor(dom, cond.viscosity, rate_u, d[i] * dt)
         if scalar:
             npp = _flux_divergence(dom, u * phi[None]) + _gradient_source(cond, q)
-            npp = npp + _cp_source(dom, cond.scalar_forcing, p)
+            npp = npp + _stage_source(dom, cond.scalar_forcing, p, cond.diffusivity)
             hp = dt * npp if i == 0 else a[i] * hp + dt * npp
             Ep = integrating_factor(dom, cond.diffusivity, rate_p, d[i] * dt)
         q = E * (q + b[i] * h)
@@ -588,8 +637,9 @@ def step_adjoint(dom: Domain, cond: Conditions, uh: np.ndarray, lam: np.ndarray,
             p = Ep * (p + b[i] * hp)
             if i < S - 1:
                 hp = Ep * hp
-    lq = leray(dom, reality_projection(dom, lam))   # the end-of-step projections
-    lp = reality_projection(dom, lam_p) if scalar else None
+    # the end-of-step projections: reality and Leray, then the post-step rescale, in reverse
+    lq = _rescale_adjoint(dom, cond.velocity_forcing, q, leray(dom, reality_projection(dom, lam)))
+    lp = _rescale_adjoint(dom, cond.scalar_forcing, p, reality_projection(dom, lam_p)) if scalar else None
     lh_next = np.zeros_like(lq)                     # adjoints of the registers carried out of stage i
     lhp_next = np.zeros_like(lp) if scalar else None
     G = cond.mean_gradient
@@ -604,7 +654,7 @@ def step_adjoint(dom: Domain, cond: Conditions, uh: np.ndarray, lam: np.ndarray,
         lF[:, 0, 0, 0] = 0.0
         lm = N3 * dom.to_physical(lF)
         lu, lw = _cross(w, lm), _cross(lm, u)
-        lq_new = lv + _cp_source_adjoint(dom, cond.velocity_forcing, qi, ln)
+        lq_new = lv + _stage_source_adjoint(dom, cond.velocity_forcing, qi, cond.viscosity, ln)
         if scalar:
             Ep = integrating_factor(dom, cond.diffusivity, rate_p, d[i] * dt)
             lvp = Ep * lp
@@ -617,7 +667,7 @@ def step_adjoint(dom: Domain, cond: Conditions, uh: np.ndarray, lam: np.ndarray,
             lu = lu + lf * phi[None]
             lphi = (lf[0] * u[0] + lf[1] * u[1]) + lf[2] * u[2]
             lq_new = lq_new - np.stack([G[0] * lnp, G[1] * lnp, G[2] * lnp])
-            lp = lvp + dom.to_spectral(lphi) / N3 + _cp_source_adjoint(dom, cond.scalar_forcing, pi_, lnp)
+            lp = lvp + dom.to_spectral(lphi) / N3 + _stage_source_adjoint(dom, cond.scalar_forcing, pi_, cond.diffusivity, lnp)
         lq = lq_new + dom.to_spectral(lu) / N3 + curl(dom, dom.to_spectral(lw)) / N3
     return lq if not scalar else (lq, lp)
 

@@ -785,7 +785,10 @@ def _random_state(dom, seed):
 
 
 @pytest.mark.parametrize("scheme,forcing", [("rk4", None), ("rk3", None), ("rk4", O.Linear(0.4)),
-                                            ("rk4", O.ConstantPower(0.1))])
+                                            ("rk4", O.ConstantPower(0.1)),
+                                            ("rk4", O.VarianceController(0.4, turnover_time=0.5, gain=2.0)),
+                                            ("rk4", O.VarianceRescaling(0.45, "total")),
+                                            ("rk3", O.VarianceRescaling(0.3, "band"))])
 def test_tangent_matches_central_differences(scheme, forcing):
     # J·δû against (F(û + εδû) − F(û − εδû))/(2ε), relative 1e-6
     dom = O.Domain(16)
@@ -801,7 +804,10 @@ def test_tangent_matches_central_differences(scheme, forcing):
 
 
 @pytest.mark.parametrize("scheme,forcing", [("rk4", None), ("rk3", None), ("rk4", O.Linear(0.4)),
-                                            ("rk4", O.ConstantPower(0.1))])
+                                            ("rk4", O.ConstantPower(0.1)),
+                                            ("rk4", O.VarianceController(0.4, turnover_time=0.5, gain=2.0)),
+                                            ("rk4", O.VarianceRescaling(0.45, "total")),
+                                            ("rk3", O.VarianceRescaling(0.3, "band"))])
 def test_adjoint_dot_product_identity(scheme, forcing):
     # ⟨J v, w⟩ = ⟨v, Jᵀ w⟩ to round-off, for states in the retained, Hermitian space
     dom = O.Domain(16)
@@ -836,8 +842,10 @@ def _random_scalar(dom, seed):
 
 @pytest.mark.parametrize("G,vf,sf", [((0.0, 0.0, 0.0), None, O.Linear(0.2)),
                                      ((1.0, 0.0, 0.0), O.ConstantPower(0.1), O.Linear(0.2)),
-                                     ((0.0, 0.0, 1.0), O.Linear(0.3), O.ConstantPower(0.05))],
-                         ids=["linear_phi", "benchmark_forcing", "cp_phi"])
+                                     ((0.0, 0.0, 1.0), O.Linear(0.3), O.ConstantPower(0.05)),
+                                     ((0.0, 1.0, 0.0), O.VarianceController(0.4, turnover_time=0.5),
+                                      O.VarianceRescaling(0.3, "total"))],
+                         ids=["linear_phi", "benchmark_forcing", "cp_phi", "controller_u_rescale_phi"])
 def test_coupled_tangent_and_adjoint(G, vf, sf):
     # the coupled velocity + scalar step (the benchmark's pair: ConstantPower on the velocity, the
     # mean gradient): the tangent against central differences, and the dot-product identity over
