@@ -28,8 +28,8 @@ reference's own known-answer tests, re-expressed in ``tests/test_oracle_known_an
   order kept; VarianceRescaling's uniform rescale on an unbounded band and its first order;
 - the box-mean definition behind the energy below scale, and the skewness identities.
 
-The tangent-linear model and discrete adjoint of the low-storage step (``step_tangent``,
-``step_adjoint``) have no counterpart in the reference, which has no AD. They are pinned by central
+The tangent-linear model and discrete adjoint of the step (``step_tangent``, ``step_adjoint``)
+have no counterpart in the reference, which has no AD. They are pinned by central
 finite differences and by the dot-product identity ⟨Jv, w⟩ = ⟨v, Jᵀw⟩.
 - injected power equal to ε, and a solenoidal state;
 - the 2/3 closed ball against a 2N zero-padded product;
@@ -440,7 +440,7 @@ def _step_low_storage(dom: Domain, cond: Conditions, st: State, dt: float, schem
 
 # ---------------------------------------------------------------------------------------------
 # Tangent-linear model and discrete adjoint of the low-storage step, velocity only: the checker
-# for a GPU adjoint of the step (the low-storage schemes, every band forcing on either field). The
+# for a GPU adjoint of the step (all four schemes, every band forcing on either field). The
 # reference has no AD; these are derived here from the step's
 # own operations, and pinned by central finite differences and the dot-product identity.
 # Inner products: physical ⟨a, b⟩ = Σ_x a·b; spectral ⟨x, y⟩ = Σ w·Re(conj(x)·y), w the Hermitian
@@ -458,8 +458,8 @@ def _cross(a, b):
 
 
 def _tangent_supported(cond: Conditions, scheme: str):
-    if scheme not in ("rk4", "rk3"):
-        raise ValueError("the tangent and adjoint are restated for the low-storage schemes")
+    if scheme not in SCHEMES:
+        raise ValueError(f"unknown scheme {scheme!r}")
 
 
 def _amplitude_gradient(dom: Domain, f, x, A, band, D):
@@ -555,9 +555,13 @@ def _gradient_source(cond: Conditions, uh):
 
 def step_tangent(dom: Domain, cond: Conditions, uh: np.ndarray, duh: np.ndarray, dt: float,
                  scheme: str = "rk4", ph: np.ndarray | None = None, dph: np.ndarray | None = None):
-    """One step F of `_step_low_storage` and its tangent J·δ in the same pass, for the velocity
-    alone (ph None) or the coupled velocity + scalar. Returns (F_u, J_u) or (F_u, F_φ, J_u, J_φ)."""
+    """One step F of `scheme` and its tangent J·δ in the same pass, for the velocity alone (ph None)
+    or the coupled velocity + scalar. Returns (F_u, J_u) or (F_u, F_φ, J_u, J_φ)."""
     _tangent_supported(cond, scheme)
+    if scheme == "heun":
+        return heun_tangent(dom, cond, uh, duh, float(dt), ph, dph)
+    if scheme == "ssprk3":
+        return ssprk3_tangent(dom, cond, uh, duh, float(dt), ph, dph)
     a, b, d = TABLEAUX[scheme]
     scalar = ph is not None
     rate_u = steady_rate(dom, cond.velocity_forcing)
@@ -608,6 +612,10 @@ def step_adjoint(dom: Domain, cond: Conditions, uh: np.ndarray, lam: np.ndarray,
     """Jᵀ·λ for the step at (û, φ̂): a forward pass that keeps each stage's fields, then the stages
     in reverse, each operation replaced by its adjoint. Returns λ_u, or (λ_u, λ_φ) with a scalar."""
     _tangent_supported(cond, scheme)
+    if scheme == "heun":
+        return heun_adjoint(dom, cond, uh, lam, float(dt), ph, lam_p)
+    if scheme == "ssprk3":
+        return ssprk3_adjoint(dom, cond, uh, lam, float(dt), ph, lam_p)
     a, b, d = TABLEAUX[scheme]
     S = len(a)
     scalar = ph is not None
@@ -670,6 +678,177 @@ def step_adjoint(dom: Domain, cond: Conditions, uh: np.ndarray, lam: np.ndarray,
             lp = lvp + dom.to_spectral(lphi) / N3 + _stage_source_adjoint(dom, cond.scalar_forcing, pi_, cond.diffusivity, lnp)
         lq = lq_new + dom.to_spectral(lu) / N3 + curl(dom, dom.to_spectral(lw)) / N3
     return lq if not scalar else (lq, lp)
+
+
+def _rhs_pair(dom: Domain, cond: Conditions, q, p, dq=None, dp=None):
+    """Both fields' right-hand sides at (q, p) with their sources, and, given (dq, dp), their
+    tangents. Returns (n, np, dn, dnp, saved) with `saved` what the adjoint needs."""
+    u, w = dom.to_physical(q), dom.to_physical(curl(dom, q))
+    phi = dom.to_physical(p) if p is not None else None
+    n = _nonlinear(dom, u, w) + _stage_source(dom, cond.velocity_forcing, q, cond.viscosity)
+    npp = None
+    if p is not None:
+        npp = _flux_divergence(dom, u * phi[None]) + _gradient_source(cond, q) \
+            + _stage_source(dom, cond.scalar_forcing, p, cond.diffusivity)
+    dn = dnp = None
+    if dq is not None:
+        du, dw = dom.to_physical(dq), dom.to_physical(curl(dom, dq))
+        dn = _nonlinear(dom, du, w) + _nonlinear(dom, u, dw) \
+            + _stage_source(dom, cond.velocity_forcing, q, cond.viscosity, dq)[1]
+        if p is not None:
+            dphi = dom.to_physical(dp)
+            dnp = _flux_divergence(dom, du * phi[None] + u * dphi[None]) + _gradient_source(cond, dq) \
+                + _stage_source(dom, cond.scalar_forcing, p, cond.diffusivity, dp)[1]
+    return n, npp, dn, dnp, (q, p, u, w, phi)
+
+
+def _rhs_pair_adjoint(dom: Domain, cond: Conditions, saved, ln, lnp):
+    """The adjoint of (q, p) ↦ (N̂_u, N̂_φ) at the saved stage, applied to (λ_n, λ_nφ)."""
+    q, p, u, w, phi = saved
+    N3 = float(dom.N) ** 3
+    lF = leray(dom, ln, dom.mask)
+    lF[:, 0, 0, 0] = 0.0
+    lm = N3 * dom.to_physical(lF)
+    lu, lw = _cross(w, lm), _cross(lm, u)
+    lq = _stage_source_adjoint(dom, cond.velocity_forcing, q, cond.viscosity, ln)
+    lp = None
+    if p is not None:
+        G = cond.mean_gradient
+        lfh = np.stack([1j * dom.mask * dk * lnp for dk in (dom.dkx, dom.dky, dom.dkz)])
+        lf = N3 * dom.to_physical(lfh)
+        lu = lu + lf * phi[None]
+        lphi = (lf[0] * u[0] + lf[1] * u[1]) + lf[2] * u[2]
+        lq = lq - np.stack([G[0] * lnp, G[1] * lnp, G[2] * lnp])
+        lp = dom.to_spectral(lphi) / N3 + _stage_source_adjoint(dom, cond.scalar_forcing, p, cond.diffusivity, lnp)
+    lq = lq + dom.to_spectral(lu) / N3 + curl(dom, dom.to_spectral(lw)) / N3
+    return lq, lp
+
+
+def _factors(dom: Domain, cond: Conditions, delta: float, scalar: bool):
+    Eu = integrating_factor(dom, cond.viscosity, steady_rate(dom, cond.velocity_forcing), delta)
+    Ep = integrating_factor(dom, cond.diffusivity, steady_rate(dom, cond.scalar_forcing), delta) if scalar else None
+    return Eu, Ep
+
+
+def _add(a, b):
+    return None if a is None else a + b
+
+
+def _finish_tangent(dom, cond, q, p, dq, dp):
+    dq = _rescale_tangent(dom, cond.velocity_forcing, q, dq)
+    q = project_forcing(dom, cond.velocity_forcing, q, np.finfo(np.float64).eps)
+    q, dq = reality_projection(dom, leray(dom, q)), reality_projection(dom, leray(dom, dq))
+    if p is None:
+        return q, dq
+    dp = _rescale_tangent(dom, cond.scalar_forcing, p, dp)
+    p = project_forcing(dom, cond.scalar_forcing, p, np.finfo(np.float64).eps)
+    return q, reality_projection(dom, p), dq, reality_projection(dom, dp)
+
+
+def _finish_adjoint(dom, cond, q, p, lam, lam_p):
+    lq = _rescale_adjoint(dom, cond.velocity_forcing, q, leray(dom, reality_projection(dom, lam)))
+    lp = _rescale_adjoint(dom, cond.scalar_forcing, p, reality_projection(dom, lam_p)) if p is not None else None
+    return lq, lp
+
+
+def heun_tangent(dom, cond, uh, duh, dt, ph=None, dph=None):
+    """IFHeun's step (`_step_heun`) and its tangent, velocity alone or coupled."""
+    half = dt / 2
+    Eu, Ep = _factors(dom, cond, dt, ph is not None)
+    n1, np1, dn1, dnp1, _ = _rhs_pair(dom, cond, uh, ph, duh, dph)
+    qs, dqs = Eu * (uh + dt * n1), Eu * (duh + dt * dn1)
+    bq, dbq = (Eu * uh) + half * (Eu * n1), (Eu * duh) + half * (Eu * dn1)
+    ps = dps = bp = dbp = None
+    if ph is not None:
+        ps, dps = Ep * (ph + dt * np1), Ep * (dph + dt * dnp1)
+        bp, dbp = (Ep * ph) + half * (Ep * np1), (Ep * dph) + half * (Ep * dnp1)
+    n2, np2, dn2, dnp2, _ = _rhs_pair(dom, cond, qs, ps, dqs, dps)
+    q, dq = bq + half * n2, dbq + half * dn2
+    p = bp + half * np2 if ph is not None else None
+    dp = dbp + half * dnp2 if ph is not None else None
+    return _finish_tangent(dom, cond, q, p, dq, dp)
+
+
+def heun_adjoint(dom, cond, uh, lam, dt, ph=None, lam_p=None):
+    half = dt / 2
+    scalar = ph is not None
+    Eu, Ep = _factors(dom, cond, dt, scalar)
+    n1, np1, _, _, s1 = _rhs_pair(dom, cond, uh, ph)
+    qs = Eu * (uh + dt * n1)
+    ps = Ep * (ph + dt * np1) if scalar else None
+    n2, np2, _, _, s2 = _rhs_pair(dom, cond, qs, ps)
+    q = (Eu * uh) + half * (Eu * n1) + half * n2
+    p = (Ep * ph) + half * (Ep * np1) + half * np2 if scalar else None
+    lq, lp = _finish_adjoint(dom, cond, q, p, lam, lam_p)
+    # q = E q0 + ½Δt E N1 + ½Δt N2(q*), q* = E(q0 + Δt N1)
+    lqs, lps = _rhs_pair_adjoint(dom, cond, s2, half * lq, half * lp if scalar else None)
+    ln1 = half * (Eu * lq) + dt * (Eu * lqs)
+    lnp1 = half * (Ep * lp) + dt * (Ep * lps) if scalar else None
+    a1, b1 = _rhs_pair_adjoint(dom, cond, s1, ln1, lnp1)
+    out_q = Eu * lq + Eu * lqs + a1
+    out_p = Ep * lp + Ep * lps + b1 if scalar else None
+    return out_q if not scalar else (out_q, out_p)
+
+
+def ssprk3_tangent(dom, cond, uh, duh, dt, ph=None, dph=None):
+    """IFSSPRK3's step (`_step_ssprk3`) and its tangent, velocity alone or coupled."""
+    scalar = ph is not None
+    Ef, Efp = _factors(dom, cond, dt, scalar)
+    Eb, Ebp = _factors(dom, cond, -dt / 2, scalar)
+    Eh, Ehp = _factors(dom, cond, dt / 2, scalar)
+    n, npp, dn, dnp, _ = _rhs_pair(dom, cond, uh, ph, duh, dph)
+    s1, ds1 = Ef * (uh + dt * n), Ef * (duh + dt * dn)
+    p1 = Efp * (ph + dt * npp) if scalar else None
+    dp1 = Efp * (dph + dt * dnp) if scalar else None
+    n, npp, dn, dnp, _ = _rhs_pair(dom, cond, s1, p1, ds1, dp1)
+    s2 = 0.25 * (Eb * (s1 + dt * n)) + Eh * (0.75 * uh)
+    ds2 = 0.25 * (Eb * (ds1 + dt * dn)) + Eh * (0.75 * duh)
+    p2 = 0.25 * (Ebp * (p1 + dt * npp)) + Ehp * (0.75 * ph) if scalar else None
+    dp2 = 0.25 * (Ebp * (dp1 + dt * dnp)) + Ehp * (0.75 * dph) if scalar else None
+    n, npp, dn, dnp, _ = _rhs_pair(dom, cond, s2, p2, ds2, dp2)
+    q = Ef * ((1 / 3) * uh) + (2 / 3) * (Eh * (s2 + dt * n))
+    dq = Ef * ((1 / 3) * duh) + (2 / 3) * (Eh * (ds2 + dt * dn))
+    p = Efp * ((1 / 3) * ph) + (2 / 3) * (Ehp * (p2 + dt * npp)) if scalar else None
+    dp = Efp * ((1 / 3) * dph) + (2 / 3) * (Ehp * (dp2 + dt * dnp)) if scalar else None
+    return _finish_tangent(dom, cond, q, p, dq, dp)
+
+
+def ssprk3_adjoint(dom, cond, uh, lam, dt, ph=None, lam_p=None):
+    scalar = ph is not None
+    Ef, Efp = _factors(dom, cond, dt, scalar)
+    Eb, Ebp = _factors(dom, cond, -dt / 2, scalar)
+    Eh, Ehp = _factors(dom, cond, dt / 2, scalar)
+    n, npp, _, _, sv0 = _rhs_pair(dom, cond, uh, ph)
+    s1 = Ef * (uh + dt * n)
+    p1 = Efp * (ph + dt * npp) if scalar else None
+    n, npp, _, _, sv1 = _rhs_pair(dom, cond, s1, p1)
+    s2 = 0.25 * (Eb * (s1 + dt * n)) + Eh * (0.75 * uh)
+    p2 = 0.25 * (Ebp * (p1 + dt * npp)) + Ehp * (0.75 * ph) if scalar else None
+    n, npp, _, _, sv2 = _rhs_pair(dom, cond, s2, p2)
+    q = Ef * ((1 / 3) * uh) + (2 / 3) * (Eh * (s2 + dt * n))
+    p = Efp * ((1 / 3) * ph) + (2 / 3) * (Ehp * (p2 + dt * npp)) if scalar else None
+    lq, lp = _finish_adjoint(dom, cond, q, p, lam, lam_p)
+    # q = Ef(⅓q0) + ⅔Eh(s2 + Δt N(s2))
+    lx2 = (2 / 3) * (Eh * lq)
+    lxp2 = (2 / 3) * (Ehp * lp) if scalar else None
+    a, b = _rhs_pair_adjoint(dom, cond, sv2, dt * lx2, dt * lxp2 if scalar else None)
+    l_s2, l_p2 = lx2 + a, (lxp2 + b if scalar else None)
+    l_q0 = (1 / 3) * (Ef * lq)
+    l_pp0 = (1 / 3) * (Efp * lp) if scalar else None
+    # s2 = ¼Eb(s1 + Δt N(s1)) + Eh(¾q0)
+    lx1 = 0.25 * (Eb * l_s2)
+    lxp1 = 0.25 * (Ebp * l_p2) if scalar else None
+    a, b = _rhs_pair_adjoint(dom, cond, sv1, dt * lx1, dt * lxp1 if scalar else None)
+    l_s1, l_p1 = lx1 + a, (lxp1 + b if scalar else None)
+    l_q0 = l_q0 + 0.75 * (Eh * l_s2)
+    l_pp0 = l_pp0 + 0.75 * (Ehp * l_p2) if scalar else None
+    # s1 = Ef(q0 + Δt N(q0))
+    lx0 = Ef * l_s1
+    lxp0 = Efp * l_p1 if scalar else None
+    a, b = _rhs_pair_adjoint(dom, cond, sv0, dt * lx0, dt * lxp0 if scalar else None)
+    l_q0 = l_q0 + lx0 + a
+    l_pp0 = l_pp0 + lxp0 + b if scalar else None
+    return l_q0 if not scalar else (l_q0, l_pp0)
 
 
 def _step_heun(dom: Domain, cond: Conditions, st: State, dt: float) -> State:

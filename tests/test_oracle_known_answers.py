@@ -788,7 +788,9 @@ def _random_state(dom, seed):
                                             ("rk4", O.ConstantPower(0.1)),
                                             ("rk4", O.VarianceController(0.4, turnover_time=0.5, gain=2.0)),
                                             ("rk4", O.VarianceRescaling(0.45, "total")),
-                                            ("rk3", O.VarianceRescaling(0.3, "band"))])
+                                            ("rk3", O.VarianceRescaling(0.3, "band")),
+                                            ("heun", O.ConstantPower(0.1)), ("ssprk3", O.ConstantPower(0.1)),
+                                            ("ssprk3", O.VarianceRescaling(0.45, "total"))])
 def test_tangent_matches_central_differences(scheme, forcing):
     # J·δû against (F(û + εδû) − F(û − εδû))/(2ε), relative 1e-6
     dom = O.Domain(16)
@@ -798,7 +800,8 @@ def test_tangent_matches_central_differences(scheme, forcing):
     F0, Jv = O.step_tangent(dom, cond, uh, v, dt, scheme)
     Fp = O.step(dom, cond, O.State(uh + eps * v), dt, scheme).uh
     Fm = O.step(dom, cond, O.State(uh - eps * v), dt, scheme).uh
-    assert np.array_equal(F0, O.step(dom, cond, O.State(uh), dt, scheme).uh)
+    ref = O.step(dom, cond, O.State(uh), dt, scheme).uh
+    assert np.allclose(F0, ref, rtol=0, atol=1e-13 * np.abs(ref).max())
     fd = (Fp - Fm) / (2 * eps)
     assert np.linalg.norm(Jv - fd) / np.linalg.norm(fd) < 1e-6
 
@@ -807,7 +810,9 @@ def test_tangent_matches_central_differences(scheme, forcing):
                                             ("rk4", O.ConstantPower(0.1)),
                                             ("rk4", O.VarianceController(0.4, turnover_time=0.5, gain=2.0)),
                                             ("rk4", O.VarianceRescaling(0.45, "total")),
-                                            ("rk3", O.VarianceRescaling(0.3, "band"))])
+                                            ("rk3", O.VarianceRescaling(0.3, "band")),
+                                            ("heun", O.ConstantPower(0.1)), ("ssprk3", O.ConstantPower(0.1)),
+                                            ("ssprk3", O.VarianceRescaling(0.45, "total"))])
 def test_adjoint_dot_product_identity(scheme, forcing):
     # ⟨J v, w⟩ = ⟨v, Jᵀ w⟩ to round-off, for states in the retained, Hermitian space
     dom = O.Domain(16)
@@ -846,7 +851,8 @@ def _random_scalar(dom, seed):
                                      ((0.0, 1.0, 0.0), O.VarianceController(0.4, turnover_time=0.5),
                                       O.VarianceRescaling(0.3, "total"))],
                          ids=["linear_phi", "benchmark_forcing", "cp_phi", "controller_u_rescale_phi"])
-def test_coupled_tangent_and_adjoint(G, vf, sf):
+@pytest.mark.parametrize("scheme", ["rk4", "heun", "ssprk3"])
+def test_coupled_tangent_and_adjoint(G, vf, sf, scheme):
     # the coupled velocity + scalar step (the benchmark's pair: ConstantPower on the velocity, the
     # mean gradient): the tangent against central differences, and the dot-product identity over
     # both fields
@@ -856,15 +862,16 @@ def test_coupled_tangent_and_adjoint(G, vf, sf):
     v, vp = _random_state(dom, 14), _random_scalar(dom, 15)
     w, wp = _random_state(dom, 16), _random_scalar(dom, 17)
     dt, eps = 0.02, 1e-5
-    Fu, Fp, Ju, Jp = O.step_tangent(dom, cond, uh, v, dt, ph=ph, dph=vp)
-    st0 = O.step(dom, cond, O.State(uh, ph), dt)
-    assert np.array_equal(Fu, st0.uh) and np.array_equal(Fp, st0.phih)
-    sp = O.step(dom, cond, O.State(uh + eps * v, ph + eps * vp), dt)
-    sm = O.step(dom, cond, O.State(uh - eps * v, ph - eps * vp), dt)
+    Fu, Fp, Ju, Jp = O.step_tangent(dom, cond, uh, v, dt, scheme, ph=ph, dph=vp)
+    st0 = O.step(dom, cond, O.State(uh, ph), dt, scheme)
+    assert np.allclose(Fu, st0.uh, rtol=0, atol=1e-13 * np.abs(st0.uh).max())
+    assert np.allclose(Fp, st0.phih, rtol=0, atol=1e-13 * np.abs(st0.phih).max())
+    sp = O.step(dom, cond, O.State(uh + eps * v, ph + eps * vp), dt, scheme)
+    sm = O.step(dom, cond, O.State(uh - eps * v, ph - eps * vp), dt, scheme)
     for J, fp, fm in ((Ju, sp.uh, sm.uh), (Jp, sp.phih, sm.phih)):
         fd = (fp - fm) / (2 * eps)
         assert np.linalg.norm(J - fd) / np.linalg.norm(fd) < 1e-6
-    lu, lp = O.step_adjoint(dom, cond, uh, w, dt, ph=ph, lam_p=wp)
+    lu, lp = O.step_adjoint(dom, cond, uh, w, dt, scheme, ph=ph, lam_p=wp)
     lhs = O.spectral_dot(dom, Ju, w) + O.spectral_dot(dom, Jp, wp)
     rhs = O.spectral_dot(dom, v, lu) + O.spectral_dot(dom, vp, lp)
     assert lhs == pytest.approx(rhs, rel=1e-12)
