@@ -1062,6 +1062,107 @@ def startup_growth(order: int) -> float:
     return 2.0 if order <= 5 else 1.5 if order <= 7 else 1.25
 
 
+def catmull_rom_slopes(t: np.ndarray):
+    """d/dt of the Catmull–Rom weights (the tangent of the gather through the positions)."""
+    return ((-3.0 * t + 4.0) * t - 1.0) * 0.5, (9.0 * t - 10.0) * t * 0.5, \
+        ((-9.0 * t + 8.0) * t + 1.0) * 0.5, (3.0 * t - 2.0) * t * 0.5
+
+
+def _gather_taps(dom: Domain, X: np.ndarray):
+    cells, weights, slopes = [], [], []
+    for a in range(3):
+        i, t = cell_and_fraction(X[a], dom.dx)
+        cells.append(i)
+        weights.append(catmull_rom_weights(t))
+        slopes.append(catmull_rom_slopes(t))
+    return cells, weights, slopes
+
+
+def interpolate_tangent(dom: Domain, f: np.ndarray, X: np.ndarray, df: np.ndarray, dX: np.ndarray):
+    """The tangent of the gather f(X) (`interpolate`): Σ w·δf at the taps plus the weights' slopes
+    (per Δx) times δX. The cell index is locally constant, so it has no tangent."""
+    N = dom.N
+    (ix, iy, iz), (wx, wy, wz), (sx, sy, sz) = _gather_taps(dom, X)
+    out = np.zeros((f.shape[0], X.shape[1]))
+    for cz in range(4):
+        zz = (iz + cz - 1) % N
+        for cy in range(4):
+            yy = (iy + cy - 1) % N
+            for cx in range(4):
+                xx = (ix + cx - 1) % N
+                w = wz[cz] * wy[cy] * wx[cx]
+                dw = (sx[cx] * wy[cy] * wz[cz] * dX[0] + wx[cx] * sy[cy] * wz[cz] * dX[1]
+                      + wx[cx] * wy[cy] * sz[cz] * dX[2]) / dom.dx
+                for c in range(f.shape[0]):
+                    out[c] += w * df[c, zz, yy, xx] + dw * f[c, zz, yy, xx]
+    return out
+
+
+def interpolate_adjoint(dom: Domain, f: np.ndarray, X: np.ndarray, lam: np.ndarray):
+    """The adjoint of (f, X) ↦ f(X) at (f, X), applied to λ (values at the points): the field part
+    scatters w·λ onto the taps, the position part sums the slopes against f·λ."""
+    N = dom.N
+    (ix, iy, iz), (wx, wy, wz), (sx, sy, sz) = _gather_taps(dom, X)
+    lf = np.zeros_like(f)
+    lX = np.zeros_like(X)
+    for cz in range(4):
+        zz = (iz + cz - 1) % N
+        for cy in range(4):
+            yy = (iy + cy - 1) % N
+            for cx in range(4):
+                xx = (ix + cx - 1) % N
+                w = wz[cz] * wy[cy] * wx[cx]
+                fl = sum(f[c, zz, yy, xx] * lam[c] for c in range(f.shape[0]))
+                lX[0] += sx[cx] * wy[cy] * wz[cz] * fl / dom.dx
+                lX[1] += wx[cx] * sy[cy] * wz[cz] * fl / dom.dx
+                lX[2] += wx[cx] * wy[cy] * sz[cz] * fl / dom.dx
+                for c in range(f.shape[0]):
+                    np.add.at(lf[c], (zz, yy, xx), w * lam[c])
+    return lf, lX
+
+
+def heun_push_tangent(dom: Domain, uh_new: np.ndarray, X: np.ndarray, f0: np.ndarray, h: float,
+                      duh: np.ndarray, dX: np.ndarray, df0: np.ndarray):
+    """The Heun push and closing deposit (X, f0; û at the end of the step) ↦ (X_new, f_new) and its
+    tangent. The wrap is locally the identity."""
+    u = dom.to_physical(uh_new)
+    du = dom.to_physical(duh)
+    (b0,) = adams_weights((0.0,), h)
+    beta = adams_weights((h, 0.0), h)
+    Xs = wrap(X + b0 * f0, dom.L)
+    dXs = dX + b0 * df0
+    fs = interpolate(dom, u, Xs)
+    dfs = interpolate_tangent(dom, u, Xs, du, dXs)
+    Xn = wrap(Xs + (beta[0] * fs + (beta[1] - b0) * f0), dom.L)
+    dXn = dXs + beta[0] * dfs + (beta[1] - b0) * df0
+    fn = interpolate(dom, u, Xn)
+    dfn = interpolate_tangent(dom, u, Xn, du, dXn)
+    return Xn, fn, dXn, dfn
+
+
+def heun_push_adjoint(dom: Domain, uh_new: np.ndarray, X: np.ndarray, f0: np.ndarray, h: float,
+                      lXn: np.ndarray, lfn: np.ndarray):
+    """The adjoint of the Heun push and closing deposit: (λ_X_new, λ_f_new) ↦ (λ_û, λ_X, λ_f0)."""
+    u = dom.to_physical(uh_new)
+    N3 = float(dom.N) ** 3
+    (b0,) = adams_weights((0.0,), h)
+    beta = adams_weights((h, 0.0), h)
+    Xs = wrap(X + b0 * f0, dom.L)
+    fs = interpolate(dom, u, Xs)
+    Xn = wrap(Xs + (beta[0] * fs + (beta[1] - b0) * f0), dom.L)
+    lu, lX_n2 = interpolate_adjoint(dom, u, Xn, lfn)
+    lXn_total = lXn + lX_n2
+    lXs = lXn_total.copy()
+    lfs = beta[0] * lXn_total
+    lf0 = (beta[1] - b0) * lXn_total
+    lu2, lXs2 = interpolate_adjoint(dom, u, Xs, lfs)
+    lu = lu + lu2
+    lXs = lXs + lXs2
+    lX = lXs.copy()
+    lf0 = lf0 + b0 * lXs
+    return dom.to_spectral(lu) / N3, lX, lf0
+
+
 def advect_heun(dom: Domain, X: np.ndarray, f0: np.ndarray, u_new: np.ndarray, h: float):
     """Heun = ABM(1) (src/ParticlePropagator.jl:165,288-315): X* = wrap(X + b₀f₀); f* = u(X*);
     X ← wrap(X* + (β₀f* + (β₁ − b₀)f₀)). Each displacement is summed term by term, then added."""

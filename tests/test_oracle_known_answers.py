@@ -900,3 +900,31 @@ def test_adjoint_chained_over_steps():
     v, vp = _random_state(dom, 20), _random_scalar(dom, 21)
     fd = (k_after(eps * v, eps * vp) - k_after(-eps * v, -eps * vp)) / (2 * eps)
     assert O.spectral_dot(dom, v, lu) + O.spectral_dot(dom, vp, lp) == pytest.approx(fd, rel=1e-6)
+
+
+def test_tracer_push_tangent_and_adjoint():
+    # the Heun push and closing deposit through the Catmull–Rom gather, as a map of (û, X, f0):
+    # the tangent against central differences, and the dot-product identity
+    dom = O.Domain(16)
+    rng = np.random.default_rng(3)
+    uh = S.seed_velocity(16, 0.5, seed=22)
+    X = S.seed_tracers(40, seed=23)
+    f0 = O.interpolate(dom, dom.to_physical(uh), X) + 0.01 * rng.standard_normal((3, 40))
+    h, eps = 0.03, 1e-6
+    v, vX, vf = _random_state(dom, 24), rng.standard_normal((3, 40)), rng.standard_normal((3, 40))
+    Xn, fn, dXn, dfn = O.heun_push_tangent(dom, uh, X, f0, h, v, vX, vf)
+    Xr, _ = O.advect_heun(dom, X, f0, dom.to_physical(uh), h)
+    assert np.max(np.abs(Xn - Xr)) < 1e-14
+
+    def push(e):
+        u = dom.to_physical(uh + e * v)
+        Xa, _ = O.advect_heun(dom, X + e * vX, f0 + e * vf, u, h)
+        return Xa, O.interpolate(dom, u, Xa)
+    (Xp, fp), (Xm, fm) = push(eps), push(-eps)
+    assert np.linalg.norm(dXn - (Xp - Xm) / (2 * eps)) / np.linalg.norm(dXn) < 1e-6
+    assert np.linalg.norm(dfn - (fp - fm) / (2 * eps)) / np.linalg.norm(dfn) < 1e-6
+    wX, wf = rng.standard_normal((3, 40)), rng.standard_normal((3, 40))
+    lu, lX, lf0 = O.heun_push_adjoint(dom, uh, X, f0, h, wX, wf)
+    lhs = float(np.sum(dXn * wX) + np.sum(dfn * wf))
+    rhs = O.spectral_dot(dom, v, lu) + float(np.sum(vX * lX) + np.sum(vf * lf0))
+    assert lhs == pytest.approx(rhs, rel=1e-12)
