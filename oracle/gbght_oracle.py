@@ -1062,6 +1062,65 @@ def startup_growth(order: int) -> float:
     return 2.0 if order <= 5 else 1.5 if order <= 7 else 1.25
 
 
+def binomial_repetitions(n: int, snaps: int) -> int:
+    """The fewest repetitions r with C(snaps + r, snaps) ≥ n: a binomial schedule reverses n steps
+    with `snaps` snapshots in at most r·n forward steps (Griewank & Walther 2000). With no snapshot
+    every state is recomputed from the start, n(n − 1)/2 steps, so r = n bounds it."""
+    if snaps == 0:
+        return n
+    r = 1
+    while math.comb(snaps + r, snaps) < n:
+        r += 1
+    return r
+
+
+def _binomial_split(n: int, snaps: int) -> int:
+    """Where a binomial (revolve-style) schedule places its next snapshot in a span of n steps
+    with `snaps` snapshots free: the left part keeps the steps that C(snaps + r − 1, snaps) leaves
+    to the recursion."""
+    r = binomial_repetitions(n, snaps)
+    m = math.comb(snaps + r - 1, snaps)
+    return min(max(1, n - m), n - 1)
+
+
+def gradient_checkpointed(dom: Domain, cond: Conditions, st: State, dt: float, n: int, loss_grad, snaps: int,
+                          scheme: str = "rk4"):
+    """The gradient of a loss of the state after n steps, by the step's adjoint applied backwards
+    over recomputed states, keeping at most `snaps` stored states besides the start (binomial
+    checkpointing). `loss_grad(state)` gives (λ_u, λ_φ) at the end. Returns the gradient at the
+    start, and the counts of recomputed forward steps and of the most states held at once."""
+    stats = {"forward_steps": 0, "held": 0, "peak": 0}
+
+    def advance(x, k):
+        for _ in range(k):
+            x = step(dom, cond, x, dt, scheme)
+            stats["forward_steps"] += 1
+        return x
+
+    def back(x, k, free, lam):
+        if k == 1:
+            if x.phih is None:
+                return step_adjoint(dom, cond, x.uh, lam[0], dt, scheme), None
+            return step_adjoint(dom, cond, x.uh, lam[0], dt, scheme, ph=x.phih, lam_p=lam[1])
+        if free == 0:   # no snapshot left: recompute every state from x
+            for i in range(k - 1, -1, -1):
+                lam = back(advance(x, i), 1, 0, lam)
+            return lam
+        m = _binomial_split(k, free)
+        y = advance(x, m)
+        stats["held"] += 1
+        stats["peak"] = max(stats["peak"], stats["held"])
+        lam = back(y, k - m, free - 1, lam)
+        stats["held"] -= 1
+        return back(x, m, free, lam)
+
+    end = advance(st, n)
+    lam = loss_grad(end)
+    stats["forward_steps"] = 0
+    grad = back(st, n, snaps, lam)
+    return grad, stats
+
+
 def catmull_rom_slopes(t: np.ndarray):
     """d/dt of the Catmull–Rom weights (the tangent of the gather through the positions)."""
     return ((-3.0 * t + 4.0) * t - 1.0) * 0.5, (9.0 * t - 10.0) * t * 0.5, \

@@ -928,3 +928,28 @@ def test_tracer_push_tangent_and_adjoint():
     lhs = float(np.sum(dXn * wX) + np.sum(dfn * wf))
     rhs = O.spectral_dot(dom, v, lu) + float(np.sum(vX * lX) + np.sum(vf * lf0))
     assert lhs == pytest.approx(rhs, rel=1e-12)
+
+
+@pytest.mark.parametrize("n,snaps", [(8, 2), (10, 3), (6, 1), (5, 0), (20, 3)])
+def test_binomial_checkpointing_gives_the_stored_gradient(n, snaps):
+    # the checkpointed gradient over n coupled steps equals, bitwise, the one with every state
+    # stored, while holding at most `snaps` states besides the start
+    dom = O.Domain(12)
+    cond = O.Conditions(viscosity=0.03, mean_gradient=(1.0, 0.0, 0.0), velocity_forcing=O.ConstantPower(0.1))
+    st0 = O.State(S.seed_velocity(12, 0.5, seed=25), S.seed_scalar(12, 0.5, seed=26))
+    dt = 0.02
+
+    def loss_grad(st):   # k + ⟨φ²⟩ in the spectral product
+        n6 = float(dom.N) ** 6
+        return st.uh / n6, 2.0 * st.phih / n6
+
+    states = [st0]
+    for _ in range(n):
+        states.append(O.step(dom, cond, states[-1], dt))
+    lu, lp = loss_grad(states[-1])
+    for x in reversed(states[:-1]):
+        lu, lp = O.step_adjoint(dom, cond, x.uh, lu, dt, ph=x.phih, lam_p=lp)
+    (gu, gp), stats = O.gradient_checkpointed(dom, cond, st0, dt, n, loss_grad, snaps)
+    assert np.array_equal(gu, lu) and np.array_equal(gp, lp)
+    assert stats["peak"] <= snaps
+    assert stats["forward_steps"] <= O.binomial_repetitions(n, snaps) * n
