@@ -953,3 +953,38 @@ def test_binomial_checkpointing_gives_the_stored_gradient(n, snaps):
     assert np.array_equal(gu, lu) and np.array_equal(gp, lp)
     assert stats["peak"] <= snaps
     assert stats["forward_steps"] <= O.binomial_repetitions(n, snaps) * n
+
+
+def test_adjoint_of_a_whole_iteration_with_tracers():
+    # one `advance` iteration: the coupled step, then the Heun push and closing deposit in the new
+    # field. The loss reads the fields and the tracers, L = k + ½Σ|X_new − X₀|² + ½Σf_new²; its
+    # gradient with respect to (û, φ̂, X, f₀) by the chained adjoints, against central differences
+    dom = O.Domain(16)
+    cond = O.Conditions(viscosity=0.02, mean_gradient=(1.0, 0.0, 0.0), velocity_forcing=O.ConstantPower(0.1))
+    rng = np.random.default_rng(11)
+    uh, ph = S.seed_velocity(16, 0.5, seed=27), S.seed_scalar(16, 0.5, seed=28)
+    X = S.seed_tracers(30, seed=29)
+    f0 = O.interpolate(dom, dom.to_physical(uh), X)
+    dt = 0.02
+    n6 = float(dom.N) ** 6
+
+    def forward(uh_, ph_, X_, f0_):
+        st = O.step(dom, cond, O.State(uh_, ph_), dt)
+        Xn, _ = O.advect_heun(dom, X_, f0_, dom.to_physical(st.uh), dt)
+        fn = O.interpolate(dom, dom.to_physical(st.uh), Xn)
+        return st, Xn, fn
+
+    def loss(uh_, ph_, X_, f0_):
+        st, Xn, fn = forward(uh_, ph_, X_, f0_)
+        return O.kinetic_energy(dom, st.uh) + 0.5 * float(np.sum((Xn - X) ** 2)) + 0.5 * float(np.sum(fn ** 2))
+
+    st, Xn, fn = forward(uh, ph, X, f0)
+    lu_push, lX, lf0 = O.heun_push_adjoint(dom, st.uh, X, f0, dt, Xn - X, fn)
+    lu, lp = O.step_adjoint(dom, cond, uh, st.uh / n6 + lu_push, dt, ph=ph, lam_p=np.zeros_like(ph))
+    v, vp = _random_state(dom, 30), _random_scalar(dom, 31)
+    vX, vf = rng.standard_normal((3, 30)), rng.standard_normal((3, 30))
+    eps = 1e-6
+    fd = (loss(uh + eps * v, ph + eps * vp, X + eps * vX, f0 + eps * vf)
+          - loss(uh - eps * v, ph - eps * vp, X - eps * vX, f0 - eps * vf)) / (2 * eps)
+    ad = O.spectral_dot(dom, v, lu) + O.spectral_dot(dom, vp, lp) + float(np.sum(vX * lX) + np.sum(vf * lf0))
+    assert ad == pytest.approx(fd, rel=1e-6)
