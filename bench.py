@@ -14,7 +14,9 @@ K steps and the state download. Under torchrun every rank runs its own replica (
 not shard), and the timed region is the max over ranks.
 
 --impl reference times the CPU restatement of the reference's step (NumPy + scipy.fft on all host
-cores) on a bounded sample of the same workload: one RK4 stage of the 512³ step per sample.
+cores) on the same workload: whole iterations of its run layer (step, deposit, tracer push and
+particle deposit, guards), as many as fit a time budget and at least one, and beside them one
+iteration each at 64³ and 256³.
 """
 from __future__ import annotations
 
@@ -39,10 +41,10 @@ METRIC = "512³ IF-RK4 steps/s, FP32-mixed vs FP64 on one B200 at ≤1e-5 spectr
 WORKLOAD = dict(N=512, viscosity=8.5e-4, schmidt=1.0, injection_rate=0.1, shells=(1, 2), G=(1.0, 0.0, 0.0),
                 tracers=1_000_000, cfl=0.5, scheme="IFLowStorageRK4")
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
-# DRAM traffic per launch over algorithmic bytes, from the ncu capture of the kernel at 256³
-# (profiles/x_products_256cubed_fp64.md), applied to the 512³ launch: the traffic scales with the
-# tiles processed.
-TRAFFIC_RATIO = {("x_products", "fp64"): 1.141 / 1.171}
+# DRAM traffic per launch over algorithmic bytes (dram__bytes_read + dram__bytes_write of one ncu
+# capture of the kernel at 256³, one launch, over the launch's algorithmic bytes), applied to the
+# 512³ launch: the kernel's traffic scales with the tiles it processes.
+TRAFFIC_RATIO = {("x_products", "fp64"): 1.141 / 1.171, ("x_products", "fp32_mixed"): 0.596 / 0.586}
 FALLBACK_HBM = 6650.0
 
 
@@ -108,15 +110,14 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device: int, path: str | None):
-        self.device, self.path, self.proc = device, path, None
+    def __init__(self, device: int):
+        self.device, self.proc = device, None
 
     def __enter__(self):
         try:
-            self.out = open(self.path, "w") if self.path else subprocess.PIPE
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=self.out, stderr=subprocess.DEVNULL, text=True)
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
         return self
@@ -131,12 +132,7 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
             out = ""
-        if self.path:
-            self.out.close()
-            with open(self.path) as f:
-                self.text = f.read()
-        else:
-            self.text = out or ""
+        self.text = out or ""
 
     def summary(self):
         rows = []
@@ -280,39 +276,39 @@ def e2e_run(args, precision, device, inputs, K):
     return K / el, h2d / K, d2h / K
 
 
-def cpu_sample(args, inputs, n_samples=1, budget_s=150.0):
-    """One RK4 stage of the 512³ workload on the host oracle, plus a fifth of the tracer push."""
+def cpu_steps(N, M, budget_s, min_steps=1, max_steps=None):
+    """Whole iterations of the oracle's run layer (`advance!`: the IF-RK4 step, the deposit, the
+    Heun push and particle deposit, the guards) on the workload at N³ with M tracers, NumPy +
+    scipy.fft on every host core: as many as fit `budget_s` seconds, at least `min_steps` and at most
+    `max_steps`. The run's
+    construction (seeding, the first deposit and particle sample) is not timed. Returns the steps
+    run and the seconds they took."""
     from oracle import gbght_oracle as O
-    N = args.grid
-    uh, ph, X = inputs
+    uh, ph, X = make_inputs(N, M, seed_base=0)
     dom = O.Domain(N)
     cond = O.Conditions(viscosity=WORKLOAD["viscosity"], schmidt=WORKLOAD["schmidt"],
                         velocity_forcing=O.ConstantPower(WORKLOAD["injection_rate"], *WORKLOAD["shells"]),
                         mean_gradient=WORKLOAD["G"])
-    Msub = max(1, args.tracers // 5)
-    Xs = X[:, :Msub].copy()
-    times = []
-    t_start = time.perf_counter()
-    for _ in range(n_samples):
+    run = O.Run(dom, cond, O.State(uh, ph), X=X, scheme="rk4", cfl=WORKLOAD["cfl"])
+    del uh, ph, X
+    n, total = 0, 0.0
+    while (n < min_steps or total < budget_s) and (max_steps is None or n < max_steps):
         t0 = time.perf_counter()
-        st = O.State(uh, ph)
-        # one stage: recoveries, both right-hand sides, the accumulator and IF update
-        u = dom.to_physical(st.uh)
-        w = dom.to_physical(O.curl(dom, st.uh))
-        phi = dom.to_physical(st.phih)
-        nu_ = O.velocity_rhs(dom, cond, st.uh, u, w, np.finfo(float).eps)
-        np_ = O.scalar_rhs(dom, cond, st.uh, u, phi)
-        E = np.exp((-(cond.viscosity * (0.2 * 1e-3))) * dom.k2)
-        _ = E * (st.uh + 0.1 * (1e-3 * nu_))
-        _ = E * (st.phih + 0.1 * (1e-3 * np_))
-        f0 = O.interpolate(dom, u, Xs)
-        O.advect_heun(dom, Xs, f0, u, 1e-3)
-        times.append(time.perf_counter() - t0)
-        del u, w, phi, nu_, np_, E
-        if time.perf_counter() - t_start > budget_s:
+        run.advance(None)
+        total += time.perf_counter() - t0
+        n += 1
+        if n >= min_steps and total + total / n > budget_s:
             break
-    stage = statistics.mean(times)
-    return 1.0 / (5 * stage), len(times), stage
+    return n, total
+
+
+def cpu_baseline_line(args, budget_s, max_steps=None):
+    """The `cpu_baseline` object: full oracle iterations of the benchmark's workload."""
+    n, total = cpu_steps(args.grid, args.tracers, budget_s, max_steps=max_steps)
+    return {"value": n / total, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{n} full step(s) of the {args.grid}^3 workload with {args.tracers} tracers (advance!: "
+                      f"IF-RK4 step, deposit, Heun push, particle deposit, guards) on the NumPy/scipy.fft "
+                      f"oracle, {total:.1f} s"}
 
 
 def ours(args):
@@ -334,9 +330,7 @@ def ours(args):
         if ws > 1:
             import torch.distributed as dist
             dist.barrier()
-        clock_path = os.path.join(ROOT, "gpurun_out", f"clocks_{form}_rank{rank}.csv") \
-            if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else None
-        with ClockSampler(device, clock_path) as cs:
+        with ClockSampler(device) as cs:
             ms, prof = timed_steps(run, args.steps)
         el = max_over_ranks(ms / 1e3, f"cuda:{device}")
         spectra = (run.energy_spectrum(), run.scalar_spectrum())
@@ -370,7 +364,8 @@ def ours(args):
                          "avg_launch_ms": tot_ms / max(1, n_launch),
                          "traffic": (round(ab[kind] / max(1, n_launch / args.steps) * TRAFFIC_RATIO[(kind, forms[0])])
                                      if (kind, forms[0]) in TRAFFIC_RATIO else None),
-                         "traffic_source": "ncu dram__bytes_read+write at 256^3 scaled by units (profiles/)"},
+                         "traffic_source": "ncu dram__bytes_read+write of one launch at 256^3, scaled to this "
+                                           "launch by the tiles processed"},
             "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in prof.items() if v[0]},
             "gpu_launches": int(sum(v[0] for v in prof.values())),
             "clocks": head["clocks"],
@@ -393,10 +388,7 @@ def ours(args):
                                             "spectrum_rel_err_after_K_steps": float(np.max(np.abs(E32[live] - E64[live]) / E64[live])),
                                             "scalar_spectrum_rel_err_after_K_steps": float(np.max(np.abs(P32[livep] - P64[livep]) / P64[livep]))}}
         if ws == 1 and not args.no_cpu_baseline:
-            v, n, stage = cpu_sample(args, inputs, n_samples=1)
-            line["cpu_baseline"] = {"value": v, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
-                                    "sample": f"one RK4 stage of the {N}^3 step (+ the push of {args.tracers // 5} tracers) "
-                                              f"on the NumPy/scipy.fft oracle, {stage:.1f} s; steps/s = 1/(5 x stage)"}
+            line["cpu_baseline"] = cpu_baseline_line(args, budget_s=60.0)
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
@@ -409,16 +401,18 @@ def reference(args):
     if rank != 0:
         return
     N = args.grid
-    inputs = make_inputs(N, args.tracers, seed_base=0)
-    v, n, stage = cpu_sample(args, inputs, n_samples=max(1, args.steps), budget_s=150.0)
+    cb = cpu_baseline_line(args, budget_s=120.0, max_steps=max(1, args.steps))
+    n = int(cb["sample"].split()[0])
+    small = {}
+    for n_small, m_small in ((64, 4096), (256, 100_000)):
+        if n_small < N:
+            k, t = cpu_steps(n_small, m_small, budget_s=0.0)
+            small[f"{n_small}^3"] = {"ms_per_step": round(t / k * 1e3, 1), "tracers": m_small}
+    v = cb["value"]
     line = {"metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": ws, "steps": n, "warmup": 0,
-            "ms_per_step": 5 * stage * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded k^4 spectrum, uniform tracers)", "config": _config(args, N),
-            "impl": "reference",
-            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
-                             "sample": f"{n} sample(s) of one RK4 stage of the {N}^3 step (+ the push of "
-                                       f"{args.tracers // 5} tracers) on the NumPy/scipy.fft restatement; "
-                                       f"steps/s = 1/(5 x mean stage)"},
+            "impl": "reference", "cpu_baseline": cb, "cpu_smaller_grids": small,
             "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

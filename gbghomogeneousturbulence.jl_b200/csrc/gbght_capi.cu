@@ -47,7 +47,7 @@ int fail(gbght_run* r, int code, const std::string& msg) {
 
 int engine_call(gbght_run* r, const char* e) {
   if (!e) return GBGHT_OK;
-  return fail(r, GBGHT_ERR_CUDA, e);
+  return fail(r, e == gbght::kDeviceTimeoutMessage ? GBGHT_ERR_DEVICE : GBGHT_ERR_CUDA, e);
 }
 
 // Carpenter & Kennedy (1994) five-stage 2N tableau and Williamson's three-stage one, as rounded
@@ -717,6 +717,24 @@ int gbght_tracer_sample_export(gbght_run* r, double* values, double* t) {
     return fail(r, GBGHT_ERR_SCHEDULE, "the trail is stale: the positions moved since its newest sample");
   if (t) *t = trail_newest_time(r);
   return values ? engine_call(r, r->eng->tracer_sample_get(values, r->trail_newest)) : GBGHT_OK;
+}
+
+int gbght_tracer_trail_export(gbght_run* r, int j, double* values, double* t) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (r->cfg.tracers <= 0) return fail(r, GBGHT_ERR_ARGUMENT, "the run was built without tracers");
+  if (j < 0 || j >= r->trail_count)
+    return fail(r, GBGHT_ERR_ARGUMENT, "the trail holds " + std::to_string(r->trail_count) + " sample(s); sample " +
+                                           std::to_string(j) + " was asked for");
+  const int slot = trail_slot(r, j);
+  if (t) *t = r->trail_time[slot];
+  return values ? engine_call(r, r->eng->tracer_sample_get(values, slot)) : GBGHT_OK;
+}
+
+int gbght_selftest_wait_timeout(gbght_run* r, int64_t cycles) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (cycles < 1 || cycles > 1000000000LL)
+    return fail(r, GBGHT_ERR_ARGUMENT, "cycles must lie in [1, 1e9]");
+  return engine_call(r, r->eng->expire_wait(static_cast<long long>(cycles)));
 }
 
 static int advect_checks(gbght_run* r, double dt) {

@@ -30,6 +30,7 @@ static const char* rt_d2h(void* h, const void* d, size_t n, Stream) { std::memcp
 static const char* rt_d2d(void* d, const void* s, size_t n, Stream) { std::memcpy(d, s, n); return nullptr; }
 static const char* rt_sync(Stream) { return nullptr; }
 static const char* rt_check() { return nullptr; }
+static const char* rt_copy(void* d, const void* s, size_t n, Stream) { std::memcpy(d, s, n); return nullptr; }
 #else
 using Stream = cudaStream_t;
 static thread_local char g_cuda_msg[256];
@@ -58,7 +59,15 @@ static const char* rt_d2h(void* h, const void* d, size_t n, Stream s) {
 }
 static const char* rt_sync(Stream s) { return cuda_err(cudaStreamSynchronize(s), "cudaStreamSynchronize"); }
 static const char* rt_check() { return cuda_err(cudaGetLastError(), "kernel launch"); }
+// A copy between any two of host memory and device memory (unified addressing tells them apart),
+// then a synchronisation.
+static const char* rt_copy(void* d, const void* src, size_t n, Stream s) {
+  const char* e = cuda_err(cudaMemcpyAsync(d, src, n, cudaMemcpyDefault, s), "cudaMemcpyAsync");
+  if (!e) e = cuda_err(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  return e;
+}
 #endif
+
 
 // ------------------------------------------------------------------------------------------------
 // Launch shapes.
@@ -214,23 +223,45 @@ class EngineImpl final : public Engine {
   int K() const override { return g_.K; }
   double cutoff() const override { return cutoff_; }
 
-  // ---- state import / export (host arrays in the reference layout) ------------------------------
-  // Each component crosses in the reference layout through B (scratch between steps), and a
-  // kernel converts it on the device. Import compacts into H, which is dead between steps, so a
-  // refused import (content outside the retained ball) leaves S as it was.
+  // ---- state import / export (the reference layout, host or device memory) --------------------------
+  // Each component of a host array crosses through B (scratch between steps), and a kernel converts
+  // it on the device; a device array of the run's device is read or written by the kernel in place.
+  // Import compacts into H, which is dead between steps, so a refused import (content outside the
+  // retained ball) leaves S as it was.
   size_t ref_comp_elems() const { return size_t(N) * N * (N / 2 + 1); }
+  // 1: memory of the run's device (device or managed), 0: host memory, −1: another device's memory.
+  int where(const void* p) const {
+#ifdef GBGHT_EMU
+    (void)p;
+    return 0;
+#else
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+      cudaGetLastError();   // an unregistered host pointer on older runtimes
+      return 0;
+    }
+    if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return a.device == p_.device ? 1 : -1;
+    return 0;
+#endif
+  }
   const char* import_state(const double* uh, const double* ph, bool* outside) override {
     const int nc = p_.scalar ? 4 : 3;
     const size_t nref = ref_comp_elems();
     *outside = false;
+    const int wu = where(uh), wp = nc == 4 ? where(ph) : 0;
+    if (wu < 0 || wp < 0) return "a state array is device memory of another device";
     bu_fresh_ = false;   // B is overwritten
-    Cplx<double>* ref = reinterpret_cast<Cplx<double>*>(B_);
+    Cplx<double>* stage = reinterpret_cast<Cplx<double>*>(B_);
     const char* err = rt_memset(H_, 0, 4 * nS_ * sizeof(Cplx<T>), stream_);
     if (!err) err = rt_memset(flag_, 0, sizeof(unsigned int), stream_);
     for (int cc = 0; cc < nc && !err; ++cc) {
       const double* src = cc < 3 ? uh + size_t(cc) * nref * 2 : ph;
-      err = rt_h2d(ref, src, nref * sizeof(Cplx<double>), stream_);
-      if (err) break;
+      const Cplx<double>* ref = reinterpret_cast<const Cplx<double>*>(src);
+      if (!(cc < 3 ? wu : wp)) {
+        err = rt_h2d(stage, src, nref * sizeof(Cplx<double>), stream_);
+        if (err) break;
+        ref = stage;
+      }
 #ifdef GBGHT_EMU
       for (size_t i = 0; i < nref; ++i) import_mode<T>(i, g_, ref, H_ + cc * nS_, flag_);
 #else
@@ -254,19 +285,24 @@ class EngineImpl final : public Engine {
   const char* export_state(double* uh, double* ph) override {
     const size_t nref = ref_comp_elems();
     const int nc = (p_.scalar && ph) ? 4 : 3;
+    const int wu = where(uh), wp = nc == 4 ? where(ph) : 0;
+    if (wu < 0 || wp < 0) return "a state array is device memory of another device";
     bu_fresh_ = false;   // B is overwritten
-    Cplx<double>* ref = reinterpret_cast<Cplx<double>*>(B_);
+    Cplx<double>* stage = reinterpret_cast<Cplx<double>*>(B_);
     for (int cc = 0; cc < nc; ++cc) {
       double* dst = cc < 3 ? uh + size_t(cc) * nref * 2 : ph;
+      const bool direct = (cc < 3 ? wu : wp) == 1;
+      Cplx<double>* ref = direct ? reinterpret_cast<Cplx<double>*>(dst) : stage;
 #ifdef GBGHT_EMU
       for (size_t i = 0; i < nref; ++i) export_mode<T>(i, g_, S_ + cc * nS_, ref);
 #else
       k_export<T><<<unsigned((nref + 255) / 256), 256, 0, stream_>>>(g_, S_ + cc * nS_, ref);
       if (const char* e = rt_check()) return e;
 #endif
-      if (const char* e = rt_d2h(dst, ref, nref * sizeof(Cplx<double>), stream_)) return e;
+      if (!direct)
+        if (const char* e = rt_d2h(dst, ref, nref * sizeof(Cplx<double>), stream_)) return e;
     }
-    return nullptr;
+    return rt_sync(stream_);
   }
 
   // ---- the step ---------------------------------------------------------------------------------
@@ -379,7 +415,7 @@ class EngineImpl final : public Engine {
     *max_speed2 = m;
     unsigned int st = 0;
     if ((err = rt_d2h(&st, status_, sizeof st, stream_))) return err;
-    if (st & GBGHT_DEV_TIMEOUT) return "a bulk copy did not complete within its bounded wait (device status 0x4)";
+    if (st & GBGHT_DEV_TIMEOUT) return kDeviceTimeoutMessage;
     return nullptr;
   }
 
@@ -558,26 +594,27 @@ class EngineImpl final : public Engine {
   // ---- tracers ----------------------------------------------------------------------------------
   const char* tracers_set(const double* X) override {
     if (!X_) return "the run carries no tracers";
-    const char* err = rt_h2d(X_, X, 3 * size_t(p_.tracers) * sizeof(double), stream_);
-    if (err) return err;
-    return rt_sync(stream_);
+    if (where(X) < 0) return "the positions are device memory of another device";
+    return rt_copy(X_, X, 3 * size_t(p_.tracers) * sizeof(double), stream_);
   }
   const char* tracers_get(double* X) override {
     if (!X_) return "the run carries no tracers";
-    return rt_d2h(X, X_, 3 * size_t(p_.tracers) * sizeof(double), stream_);
+    if (where(X) < 0) return "the positions are device memory of another device";
+    return rt_copy(X, X_, 3 * size_t(p_.tracers) * sizeof(double), stream_);
   }
   const char* tracer_sample_get(double* F, int slot) override {
     if (!F_) return "the run carries no tracers";
     if (slot < 0 || slot >= p_.trail_capacity) return "no such trail slot";
     const size_t n = 3 * size_t(p_.tracers);
-    return rt_d2h(F, F_ + size_t(slot) * n, n * sizeof(double), stream_);
+    if (where(F) < 0) return "the sample is device memory of another device";
+    return rt_copy(F, F_ + size_t(slot) * n, n * sizeof(double), stream_);
   }
   const char* tracer_sample_set(const double* F, int slot) override {
     if (!F_) return "the run carries no tracers";
     if (slot < 0 || slot >= p_.trail_capacity) return "no such trail slot";
     const size_t n = 3 * size_t(p_.tracers);
-    const char* err = rt_h2d(F_ + size_t(slot) * n, F, n * sizeof(double), stream_);
-    return err ? err : rt_sync(stream_);
+    if (where(F) < 0) return "the sample is device memory of another device";
+    return rt_copy(F_ + size_t(slot) * n, F, n * sizeof(double), stream_);
   }
   const char* tracers_run(const AdamsStep& w) override {
     if (!X_) return "the run carries no tracers";
@@ -649,6 +686,20 @@ class EngineImpl final : public Engine {
     if (ms) *ms = double(f);
     return err;
 #endif
+  }
+
+  const char* expire_wait(long long cycles) override {
+#ifdef GBGHT_EMU
+    (void)cycles;
+    *status_ |= GBGHT_DEV_TIMEOUT;   // the host-check build has no barrier to wait on
+#else
+    k_expire_wait<<<1, 32, 0, stream_>>>(status_, cycles);
+    if (const char* e = rt_check()) return e;
+#endif
+    unsigned int st = 0;
+    const char* err = rt_d2h(&st, status_, sizeof st, stream_);
+    if (err) return err;
+    return (st & GBGHT_DEV_TIMEOUT) ? kDeviceTimeoutMessage : nullptr;
   }
 
   const char* status(uint32_t* word) override {

@@ -57,11 +57,18 @@ struct Observables {
   double k, eps, var, chi;
 };
 
+// The message an engine call returns when a bounded device wait expired (device status 0x4); the
+// C ABI reports it as GBGHT_ERR_DEVICE rather than as a CUDA runtime error.
+inline const char* const kDeviceTimeoutMessage =
+    "a bulk copy did not complete within its bounded wait (device status 0x4)";
+
 class Engine {
  public:
   virtual ~Engine() {}
   // All methods return nullptr on success, else a static or engine-owned error message.
   virtual const char* init(const RunParams& p) = 0;
+  // The state crosses in the reference layout, from and into host memory or device memory of the
+  // run's device (told apart by the pointer's attributes).
   virtual const char* import_state(const double* uh, const double* ph, bool* outside) = 0;
   virtual const char* export_state(double* uh, double* ph) = 0;
   virtual const char* step(double dt, const double* a, const double* b, const double* d, int S) = 0;
@@ -101,6 +108,10 @@ class Engine {
   virtual const char* profile_read(int kind, int64_t* launches, double* total_ms) = 0;
   virtual const char* timer(int op, double* ms) = 0;
   virtual const char* status(uint32_t* word) = 0;
+  // A bounded device wait made to expire after `cycles` clock cycles on the run's stream (a copy
+  // that is never issued); returns kDeviceTimeoutMessage once the expiry is seen, as any call that
+  // reads the status word does. The run stays usable.
+  virtual const char* expire_wait(long long cycles) = 0;
   virtual int K() const = 0;
   virtual double cutoff() const = 0;
 };

@@ -8,17 +8,20 @@
 // (docs/ARCHITECTURE.md:921-930 of the reference). Such a caller owns the input spectrum and the
 // output field and hands them in. Every intermediate lives here, in one file-scope
 // __device__ array of kScratchBytes, which each GPU that loads the library holds until the
-// process exits. This path calls no cudaMalloc, no cudaFree, and no routine that allocates.
+// process exits. This path calls no cudaMalloc, no cudaFree, and no routine that allocates; on the
+// host it uses static storage only (the twiddle table and the per-device set-up below).
 //
 // The array is shared by every call on a device and keeps the contents of the last call. Each call
 // clears what must start at zero: the compact spectrum, the maximum and the flag word. Two calls
 // whose work overlaps on the GPU (on different streams, or from different host threads) race on
 // the array. Serialise them.
 //
-// Set-up: the first call on each device looks up the array's device address with
+// Set-up, per device: the first call looks up the array's device address with
 // cudaGetSymbolAddress (in host code the array's name stands for a host-side shadow, not a device
-// address, so it is never passed to a kernel directly) and encodes the tensor maps of the y pass.
-// Make that first call before capturing any stream, because the set-up does synchronous work.
+// address, so it is never passed to a kernel directly). The tensor maps of the y pass and the
+// twiddle table in the array are rebuilt only when a call's grid differs from the previous call's
+// on that device. Every call synchronises its stream once, to read back max|u| and the flag word,
+// so no call can be made inside a stream capture.
 #include "../../include/gbght.h"
 
 #include <cuda.h>
@@ -29,7 +32,6 @@
 #include <cstring>
 #include <mutex>
 #include <string>
-#include <vector>
 
 #include "kernels.cuh"
 
@@ -126,25 +128,38 @@ __global__ void k_compact_reference(Geometry g, const Cplx<double>* __restrict__
   }
 }
 
-struct DeviceSetup {
-  bool ready = false;
-  unsigned char* base = nullptr;   // device address of g_noalloc_scratch on this device
-};
-constexpr int kMaxDevices = 64;
-DeviceSetup g_setup[kMaxDevices];
-std::mutex g_setup_mutex;
-
 using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
                             const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
                             CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+// What a device keeps between calls: the array's address, and the grid (N, L) whose tensor maps
+// are encoded and whose twiddles sit at the start of the array. A call with another grid
+// overwrites both (its layout also reuses the bytes that held the old twiddles).
+struct DeviceSetup {
+  bool ready = false;
+  unsigned char* base = nullptr;   // device address of g_noalloc_scratch on this device
+  int N = 0;
+  double L = 0.0;
+  gbght::TmaMaps maps{};
+};
+constexpr int kMaxDevices = 64;
+DeviceSetup g_setup[kMaxDevices];
+std::mutex g_setup_mutex;
+Encode g_encode = nullptr;
+// The host copy of the twiddles e^(−2πi k/N), k < N, of the last grid uploaded (static storage;
+// cudaMemcpyAsync from pageable memory has consumed it when it returns).
+Cplx<double> g_tw_host[kMaxN];
+
 int encode_maps(const Layout& o, unsigned char* base, gbght::TmaMaps* m) {
-  void* fn = nullptr;
-  cudaDriverEntryPointQueryResult q{};
-  cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDriverEntryPoint");
-  if (!fn || q != cudaDriverEntryPointSuccess) return fail(GBGHT_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
-  Encode encode = reinterpret_cast<Encode>(fn);
+  if (!g_encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDriverEntryPoint");
+    if (!fn || q != cudaDriverEntryPointSuccess) return fail(GBGHT_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+    g_encode = reinterpret_cast<Encode>(fn);
+  }
+  Encode encode = g_encode;
   const Geometry& g = o.g;
   const int N = g.N;
   constexpr int TLY = 128 / int(sizeof(Cplx<double>));
@@ -164,8 +179,27 @@ int encode_maps(const Layout& o, unsigned char* base, gbght::TmaMaps* m) {
   return GBGHT_OK;
 }
 
+// The grid-dependent set-up of a device, redone only when the grid changes: the tensor maps, and
+// the twiddles copied into the array from the static host table. Called with g_setup_mutex held.
+int prepare_grid(DeviceSetup& ds, const Layout& o, double L, cudaStream_t st) {
+  const int N = o.g.N;
+  if (ds.N == N && ds.L == L) return GBGHT_OK;
+  ds.N = 0;
+  if (int rc = encode_maps(o, ds.base, &ds.maps)) return rc;
+  for (int k = 0; k < N; ++k) {   // extended precision, as the run's own table
+    const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)N;
+    g_tw_host[k] = gbght::cmk<double>(double(cosl(a)), double(-sinl(a)));
+  }
+  cudaError_t e = cudaMemcpyAsync(ds.base + o.tw, g_tw_host, N * sizeof(Cplx<double>), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync (twiddles)");
+  ds.N = N;
+  ds.L = L;
+  return GBGHT_OK;
+}
+
 template <int N>
-int run_n(const Layout& o, unsigned char* base, const double* u_hat, double* u, cudaStream_t st) {
+int run_n(const Layout& o, unsigned char* base, const gbght::TmaMaps& maps, const double* u_hat, double* u,
+          cudaStream_t st) {
   constexpr int TLY = 128 / int(sizeof(Cplx<double>));
   constexpr int TLZ = 64 / int(sizeof(Cplx<double>));
   constexpr int NTY = N * TLY / 8 < 64 ? 64 : (N * TLY / 8 > 256 ? 256 : N * TLY / 8);
@@ -179,16 +213,7 @@ int run_n(const Layout& o, unsigned char* base, const double* u_hat, double* u, 
   auto* partial = reinterpret_cast<double*>(base + o.partial);
   auto* maxbits = reinterpret_cast<unsigned long long*>(base + o.maxbits);
   auto* flag = reinterpret_cast<unsigned int*>(base + o.flag);
-  gbght::TmaMaps maps{};
-  if (int rc = encode_maps(o, base, &maps)) return rc;
-  // twiddles e^(−2πi k/N) in extended precision, copied in (no allocation)
-  std::vector<Cplx<double>> h(N);
-  for (int k = 0; k < N; ++k) {
-    const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)N;
-    h[k] = gbght::cmk<double>(double(cosl(a)), double(-sinl(a)));
-  }
-  cudaError_t e = cudaMemcpyAsync(tw, h.data(), N * sizeof(Cplx<double>), cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync (twiddles)");
+  cudaError_t e;
   // what must start at zero: the compact spectrum (modes of the box outside the ball), the
   // maximum and the flag word
   if ((e = cudaMemsetAsync(S, 0, o.A - o.S, st)) != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
@@ -228,7 +253,9 @@ extern "C" int gbght_velocity_physical_noalloc(int grid_points_per_axis, double 
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
   if (dev < 0 || dev >= kMaxDevices) return fail(GBGHT_ERR_ARGUMENT, "device ordinal out of range");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
   unsigned char* base = nullptr;
+  gbght::TmaMaps maps{};
   {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     DeviceSetup& ds = g_setup[dev];
@@ -239,18 +266,19 @@ extern "C" int gbght_velocity_physical_noalloc(int grid_points_per_axis, double 
       ds.base = static_cast<unsigned char*>(p);
       ds.ready = true;
     }
+    if (int rc = prepare_grid(ds, o, side_length, st)) return rc;
     base = ds.base;
+    maps = ds.maps;
   }
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   int rc = GBGHT_OK;
   switch (N) {
-    case 8: rc = run_n<8>(o, base, u_hat, u, st); break;
-    case 12: rc = run_n<12>(o, base, u_hat, u, st); break;
-    case 16: rc = run_n<16>(o, base, u_hat, u, st); break;
-    case 24: rc = run_n<24>(o, base, u_hat, u, st); break;
-    case 32: rc = run_n<32>(o, base, u_hat, u, st); break;
-    case 48: rc = run_n<48>(o, base, u_hat, u, st); break;
-    case 64: rc = run_n<64>(o, base, u_hat, u, st); break;
+    case 8: rc = run_n<8>(o, base, maps, u_hat, u, st); break;
+    case 12: rc = run_n<12>(o, base, maps, u_hat, u, st); break;
+    case 16: rc = run_n<16>(o, base, maps, u_hat, u, st); break;
+    case 24: rc = run_n<24>(o, base, maps, u_hat, u, st); break;
+    case 32: rc = run_n<32>(o, base, maps, u_hat, u, st); break;
+    case 48: rc = run_n<48>(o, base, maps, u_hat, u, st); break;
+    case 64: rc = run_n<64>(o, base, maps, u_hat, u, st); break;
   }
   if (rc) return rc;
   // read back the maximum of |u|² and the flag word (the call's one synchronisation)

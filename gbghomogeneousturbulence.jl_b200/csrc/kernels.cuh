@@ -315,6 +315,20 @@ static __global__ void k_trav_scatter(int64_t M, const uint32_t* key, uint32_t* 
   if (p >= M) return;
   order[atomicAdd(offset + key[p], 1u)] = uint32_t(p);
 }
+// The bounded wait's expiry, made on purpose: one thread arms a barrier for a copy of 128 bytes
+// that is never issued and waits at most `limit` cycles. The wait gives up, raises
+// GBGHT_DEV_TIMEOUT in `status` and returns, as a wait on a lost copy would; no copy is in
+// flight when the block exits, and the barrier is retired first.
+static __global__ void k_expire_wait(unsigned int* status, long long limit) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  mbar_expect_tx(&bar, 128u);
+  mbar_wait_for(&bar, 0u, status, limit);
+  mbar_inval(&bar);
+}
+
 template <class T>
 __global__ void k_import(Geometry g, const Cplx<double>* ref, Cplx<T>* Sc, unsigned int* flag) {
   import_mode<T>(size_t(blockIdx.x) * blockDim.x + threadIdx.x, g, ref, Sc, flag);

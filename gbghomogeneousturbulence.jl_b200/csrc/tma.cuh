@@ -27,6 +27,11 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 
+// Retire a barrier: its memory may then hold anything else.
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // Make generic-proxy writes to shared memory (and a barrier's initialisation) visible to the
 // async proxy that the bulk copies run in.
 __device__ __forceinline__ void fence_proxy_async() {
@@ -50,16 +55,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Wait for the barrier's phase `parity` to complete, for at most kWaitCycles.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned int* status) {
+// Wait for the barrier's phase `parity` to complete, for at most `limit` clock cycles; on expiry
+// set GBGHT_DEV_TIMEOUT in `status` and return false.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t* bar, uint32_t parity, unsigned int* status, long long limit) {
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > kWaitCycles) {
+    if (clock64() - t0 > limit) {
       if (status) atomicOr(status, GBGHT_DEV_TIMEOUT);
       return false;
     }
   }
   return true;
+}
+// Wait for the barrier's phase `parity` to complete, for at most kWaitCycles.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned int* status) {
+  return mbar_wait_for(bar, parity, status, kWaitCycles);
 }
 
 // 2-D and 3-D tiled loads into shared memory, completing on `bar`. Coordinates are in elements,

@@ -105,6 +105,8 @@ _SIGNATURES = {
     "gbght_tracers_export": (C.c_int, [C.c_void_p, _DP]),
     "gbght_tracer_sample_export": (C.c_int, [C.c_void_p, _DP, _DP]),
     "gbght_tracer_trail_reset": (C.c_int, [C.c_void_p]),
+    "gbght_tracer_trail_export": (C.c_int, [C.c_void_p, C.c_int, _DP, _DP]),
+    "gbght_selftest_wait_timeout": (C.c_int, [C.c_void_p, C.c_int64]),
     "gbght_tracer_sample_restore": (C.c_int, [C.c_void_p, _DP, C.c_double]),
     "gbght_advect": (C.c_int, [C.c_void_p, C.c_double]),
     "gbght_deposit_tracers": (C.c_int, [C.c_void_p, C.c_double]),
@@ -144,6 +146,28 @@ def load_library(path: str | None = None):
 
 def _ptr(a: np.ndarray):
     return a.ctypes.data_as(_DP)
+
+
+def _is_device(a) -> bool:
+    """Whether `a` is a CUDA tensor (device memory the library reads or writes in place)."""
+    return getattr(a, "is_cuda", False)
+
+
+def _dev_ptr(t, shape, what, real=False):
+    """The address of a contiguous CUDA tensor: complex128 of `shape`, or float64 of `shape` + (2,)
+    (interleaved re, im); with `real`, float64 of `shape`."""
+    import torch
+    if not t.is_contiguous():
+        raise ValueError(f"{what} must be contiguous")
+    if real:
+        ok = t.dtype == torch.float64 and tuple(t.shape) == tuple(shape)
+    else:
+        ok = (t.dtype == torch.complex128 and tuple(t.shape) == tuple(shape)) or \
+             (t.dtype == torch.float64 and tuple(t.shape) == tuple(shape) + (2,))
+    if not ok:
+        kind = "float64" if real else "complex128"
+        raise ValueError(f"{what} must be a contiguous {kind} CUDA tensor of shape {shape}")
+    return C.cast(C.c_void_p(t.data_ptr()), _DP)
 
 
 @dataclass
@@ -305,7 +329,16 @@ class Run:
     def spectral_shape(self):
         return (self.N, self.N, self.N // 2 + 1)
 
-    def import_state(self, uh: np.ndarray, phih: np.ndarray | None = None):
+    def import_state(self, uh, phih=None):
+        """ResolvedFields(û, φ̂): NumPy arrays (host memory) or CUDA tensors (device memory of the run's
+        device, converted in place by the library), complex128 in the reference layout."""
+        if _is_device(uh):
+            if self.setup.scalar and phih is None:
+                raise ValueError("this run carries a passive scalar, so phi_hat must be given")
+            pu = _dev_ptr(uh, (3,) + self.spectral_shape, "u_hat")
+            pp = _dev_ptr(phih, self.spectral_shape, "phi_hat") if self.setup.scalar else None
+            self._check(self.lib.gbght_state_import(self.h, pu, pp))
+            return
         u = np.ascontiguousarray(uh, dtype=np.complex128)
         if u.shape != (3,) + self.spectral_shape:
             raise ValueError(f"u_hat must have shape {(3,) + self.spectral_shape}")
@@ -322,6 +355,12 @@ class Run:
     def export_state(self, out=None):
         """û (and φ̂) in the reference layout. `out = (u, p)` receives them in place (contiguous
         complex128 arrays of the right shapes, e.g. in pinned memory); by default new arrays."""
+        if out is not None and _is_device(out[0]):
+            u, p = out
+            pu = _dev_ptr(u, (3,) + self.spectral_shape, "out u")
+            pp = _dev_ptr(p, self.spectral_shape, "out p") if self.setup.scalar else None
+            self._check(self.lib.gbght_state_export(self.h, pu, pp))
+            return u, (p if self.setup.scalar else None)
         if out is None:
             u = np.zeros((3,) + self.spectral_shape, np.complex128)
             p = np.zeros(self.spectral_shape, np.complex128) if self.setup.scalar else None
@@ -399,13 +438,21 @@ class Run:
         return self._spectrum(1)
 
     # -- tracers (advect!, particle deposit!) -------------------------------------------------------
-    def import_tracers(self, X: np.ndarray):
+    def import_tracers(self, X):
+        """Tracer positions (3, M): a NumPy array, or a float64 CUDA tensor read in place."""
+        if _is_device(X):
+            self._check(self.lib.gbght_tracers_import(self.h, _dev_ptr(X, (3, self.setup.tracers), "X", real=True)))
+            return
         a = np.ascontiguousarray(X, dtype=np.float64)
         if a.shape != (3, self.setup.tracers):
             raise ValueError(f"positions must have shape (3, {self.setup.tracers})")
         self._check(self.lib.gbght_tracers_import(self.h, _ptr(a)))
 
-    def tracers(self) -> np.ndarray:
+    def tracers(self, out=None):
+        """Tracer positions (3, M), into `out` (a float64 CUDA tensor) when given, else a new array."""
+        if out is not None and _is_device(out):
+            self._check(self.lib.gbght_tracers_export(self.h, _dev_ptr(out, (3, self.setup.tracers), "out", real=True)))
+            return out
         X = np.zeros((3, self.setup.tracers))
         self._check(self.lib.gbght_tracers_export(self.h, _ptr(X)))
         return X
@@ -415,6 +462,22 @@ class Run:
         t = C.c_double()
         self._check(self.lib.gbght_tracer_sample_export(self.h, _ptr(F), C.byref(t)))
         return F, t.value
+
+    def tracer_trail(self):
+        """Every sample of the trail as held, oldest first: [(t, values (3, M)), ...] (what a
+        checkpoint stores to restore a multistep scheme)."""
+        out = []
+        j = 0
+        while True:
+            F = np.zeros((3, self.setup.tracers))
+            t = C.c_double()
+            rc = self.lib.gbght_tracer_trail_export(self.h, j, _ptr(F), C.byref(t))
+            if rc == ERR_ARGUMENT and j > 0:
+                break
+            self._check(rc)
+            out.append((t.value, F))
+            j += 1
+        return out[::-1]
 
     def reset_tracer_trail(self):
         """`reset_velocity_at_particles!` (src/Cache.jl:382-386)."""
@@ -458,6 +521,14 @@ class Run:
 
     def synchronize(self):
         self._check(self.lib.gbght_synchronize(self.h))
+
+    def selftest_wait_timeout(self, cycles: int):
+        """Expire a bounded device wait on purpose (`gbght_selftest_wait_timeout`); raises the
+        DeviceError a lost copy raises."""
+        self._check(self.lib.gbght_selftest_wait_timeout(self.h, int(cycles)))
+
+    def set_clock(self, time: float, step: int):
+        self._check(self.lib.gbght_set_clock(self.h, float(time), int(step)))
 
     # -- CUDA-event timing on the run's stream ------------------------------------------------------
     def profile(self, enable: bool):

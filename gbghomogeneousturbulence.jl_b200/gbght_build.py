@@ -48,15 +48,36 @@ def _units():
     return units
 
 
-def _compile(unit, verbose):
+def _unit_digest(unit) -> str:
+    """The inputs of one translation unit: every header, its own source, the flags and defines."""
+    name, defs, src = unit
+    h = hashlib.sha256()
+    for p in [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith(".cuh")] + \
+             [os.path.join(CSRC, src), os.path.join(HERE, "..", "include", "gbght.h")]:
+        with open(p, "rb") as f:
+            h.update(f.read())
+    h.update(" ".join(ARCH + FLAGS + defs).encode())
+    return h.hexdigest()
+
+
+def _compile(unit, verbose, force=False):
+    """Compile one unit, unless its object is current (a stamp of the unit's inputs)."""
     name, defs, src = unit
     obj = os.path.join(BUILD, name + ".o")
+    stamp = obj + ".sha256"
+    digest = _unit_digest(unit)
+    if not force and os.path.exists(obj) and os.path.exists(stamp):
+        with open(stamp) as f:
+            if f.read().strip() == digest:
+                return obj
     cmd = [NVCC] + ARCH + FLAGS + defs + ["-c", os.path.join(CSRC, src), "-o", obj]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for {name}:\n{r.stdout}\n{r.stderr}")
+    with open(stamp, "w") as f:
+        f.write(digest)
     return obj
 
 
@@ -71,7 +92,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     units = _units()
     jobs = max(1, min(len(units), os.cpu_count() or 1))
     with cf.ThreadPoolExecutor(jobs) as ex:
-        objs = list(ex.map(lambda u: _compile(u, verbose), units))
+        objs = list(ex.map(lambda u: _compile(u, verbose, force), units))
     tmp = OUT + ".tmp"
     cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -132,8 +132,10 @@ const char* gbght_version(void);
  * Replaces max_retained_wavenumber (src/SimulationDomain.jl:413-419). */
 int gbght_geometry(const gbght_run* run, int* K, double* cutoff);
 
-/* Spectral state import/export, host arrays in the reference layout. phi_hat may be NULL when
- * the run carries no scalar. Import refuses (ARGUMENT) a state with content outside the retained
+/* Spectral state import/export in the reference layout, from and into host memory or device memory
+ * of the run's device (a CUDA.jl CuArray or a torch tensor; unified addressing tells them apart):
+ * a device array is converted by a kernel in place, with no staging through the host. Memory of
+ * another device is refused with ARGUMENT. phi_hat may be NULL when the run carries no scalar. Import refuses (ARGUMENT) a state with content outside the retained
  * 2/3 ball: the library stores only the retained modes. Every state the reference's seeders
  * and steps produce is band-limited. Import invalidates the deposit.
  * Replaces ResolvedFields(û, φ̂) (src/State.jl:119-137) and the state read/write of
@@ -213,14 +215,20 @@ int gbght_derivative_skewness(gbght_run* run, double* skewness);
  * viscosity) (src/Observables.jl:253-263). An occasional diagnostic: its cost grows as N⁴. */
 int gbght_energy_below_scale(gbght_run* run, double* scales, double* k, double* eps, int n);
 
-/* Tracer positions [3][M], copied as given (the push wraps them into [0, L)). Import clears the
- * trail. Replaces Tracers(domain; positions) (src/Particles.jl:145-176). */
+/* Tracer positions [3][M], copied as given (the push wraps them into [0, L)), from and into host
+ * memory or device memory of the run's device. Import clears the trail. Replaces
+ * Tracers(domain; positions) (src/Particles.jl:145-176). */
 int gbght_tracers_import(gbght_run* run, const double* X);
 int gbght_tracers_export(gbght_run* run, double* X);
 
 /* The newest velocity sample at the tracers [3][M] and its time. Replaces
  * velocity_at_particles_trail (src/Cache.jl). */
 int gbght_tracer_sample_export(gbght_run* run, double* values, double* t);
+
+/* The j-th newest sample of the trail (j = 0 the newest, j < the samples held) [3][M] and its time,
+ * as held: a checkpoint stores them all, oldest to newest, to restore a multistep scheme's trail.
+ * Replaces the trail's read in write_simulation (ext/GBGHomogeneousTurbulenceHDF5Ext.jl:426-561). */
+int gbght_tracer_trail_export(gbght_run* run, int j, double* values, double* t);
 
 /* Empty the trail, and push an earlier sample [3][M] at time t (later than the newest held) without
  * moving the tracers or pairing the epochs: a checkpoint's restore of the samples a multistep
@@ -257,6 +265,14 @@ int gbght_set_clock(gbght_run* run, double time, int64_t step);
 /* Device status bits raised since the last call (GBGHT_STATUS_*); reading clears them. */
 int gbght_status_word(gbght_run* run, uint32_t* word);
 
+/* No counterpart in the reference: the failure path of the device's bounded waits, exercised on
+ * purpose. A kernel on the run's stream arms a barrier for a copy that is never issued and waits at
+ * most `cycles` clock cycles (1 ≤ cycles ≤ 1e9); the wait expires, raises
+ * GBGHT_STATUS_COPY_TIMEOUT, and returns, exactly as a wait on a lost copy does in the step's
+ * kernels. The call then returns GBGHT_ERR_DEVICE, as a deposit does after such an expiry; the bit
+ * stays raised until gbght_status_word reads it. Nothing faults, and the run stays usable. */
+int gbght_selftest_wait_timeout(gbght_run* run, int64_t cycles);
+
 /* CUDA-event timing on the run's own stream (no counterpart in the reference, which has no
  * profiling; used by the benchmark to time kernels where they are launched).
  * gbght_profile(run, 1) clears the counters and brackets every later kernel launch with events;
@@ -290,13 +306,17 @@ int gbght_timer(gbght_run* run, int op, double* ms);
  * physical velocity u (device memory, float64 [3][N][N][N]) and, if max_speed is not NULL,
  * returns max|u| on the host. The values are those gbght_deposit + gbght_velocity_physical_export
  * give for the same spectrum (FP64).
- * Every intermediate lives in one file-scope device array of 12 MiB, held by each GPU that loads
- * the library until the process exits. N is limited to 8, 12, 16, 24, 32, 48 or 64; a larger N is
- * refused with GBGHT_ERR_ARGUMENT, as is a spectrum with content outside the retained 2/3 ball.
- * The first call on a device looks up the array's address and should come before any stream
- * capture. Calls share the array, so two calls whose work overlaps on the GPU race: serialise
- * them. `stream` is a cudaStream_t (NULL: the default stream). The call synchronises that stream
- * once, to read back max|u|. Errors are reported through gbght_global_error(). */
+ * Every intermediate lives in one file-scope device array of 12 MiB, held by each GPU that loads the
+ * library until the process exits; on the host the call uses static storage only. N is limited to
+ * 8, 12, 16, 24, 32, 48 or 64; a larger N is refused with GBGHT_ERR_ARGUMENT before any work. A
+ * spectrum with content outside the retained 2/3 ball is also refused with GBGHT_ERR_ARGUMENT, but
+ * only after the kernels have run: `u` then holds the velocity of the truncated spectrum.
+ * The first call on a device looks up the array's address; a call whose grid differs from the
+ * previous call's on that device re-encodes its tensor maps and re-uploads its twiddles into the
+ * array. Calls share the array, so two calls whose work overlaps on the GPU (other streams, other
+ * host threads) race: serialise them. `stream` is a cudaStream_t (NULL: the default stream). Every
+ * call synchronises that stream once, to read back max|u| and the status word, so no call may be
+ * made inside a stream capture. Errors are reported through gbght_global_error(). */
 int gbght_velocity_physical_noalloc(int grid_points_per_axis, double side_length, const double* u_hat,
                                     double* u, double* max_speed, void* stream);
 

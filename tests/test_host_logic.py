@@ -179,3 +179,39 @@ def test_empty_velocity_band_skips_the_rescale(hostcheck_library):
     ue, _ = run.export_state()
     assert np.max(np.abs(ue - uh * np.exp(-0.01 * 9 * 0.02))) <= 1e-13 * np.max(np.abs(uh))
     assert run.status_word() & 0x2
+
+
+def test_expired_device_wait_is_a_device_error(hostcheck_library):
+    # the host-check build stands the expiry in for the device's barrier; the path from the raised
+    # bit to GBGHT_ERR_DEVICE and the status word is the library's own
+    run, _ = make_case(16, forcing=0.1, tracers=64, library=hostcheck_library)
+    with pytest.raises(gbght.DeviceError, match="bounded wait"):
+        run.selftest_wait_timeout(1000)
+    assert run.status_word() & 0x4
+    assert run.status_word() == 0
+    run.advance(0.01)
+    with pytest.raises(ValueError):
+        run.selftest_wait_timeout(0)
+
+
+def test_trail_export_holds_every_sample(hostcheck_library):
+    run, _ = make_case(16, forcing=0.1, tracers=64, tracer_scheme=("AB", 3), library=hostcheck_library)
+    assert [t for t, _ in run.tracer_trail()] == [0.0]
+    for _ in range(4):
+        run.advance(0.01)
+    trail = run.tracer_trail()
+    assert len(trail) == 3
+    assert [t for t, _ in trail] == pytest.approx([0.02, 0.03, 0.04], abs=1e-15)
+    F, t = run.tracer_sample()
+    assert t == trail[-1][0] and np.array_equal(F, trail[-1][1])
+
+
+@pytest.mark.parametrize("tracer_scheme", [("Heun", 1), ("AB", 3)])
+def test_checkpoint_continues_bitwise(hostcheck_library, tracer_scheme):
+    from checkpoint import continuation_is_bitwise
+    N, M = 16, 100
+    setup = gbght.Setup(grid_points_per_axis=N, viscosity=0.01, velocity_forcing=gbght.ConstantPower(0.1),
+                        mean_gradient=(1.0, 0.0, 0.0), tracers=M, tracer_scheme=tracer_scheme[0],
+                        tracer_steps=tracer_scheme[1])
+    continuation_is_bitwise(setup, S.seed_velocity(N, 0.5, seed=0), S.seed_scalar(N, 0.5, seed=1),
+                            S.seed_tracers(M, seed=2), before=4, after=3, library=hostcheck_library)
