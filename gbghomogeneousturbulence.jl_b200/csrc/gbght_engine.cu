@@ -1002,12 +1002,13 @@ class EngineImpl final : public Engine {
   }
   // The z-inverse of the state into the A slots (u, iκ×û, φ), or with `vorticity` = 2 of the six
   // strain components into slots 0..5.
-  const char* z_init(int vorticity = 1) {
+  // `columns` = 1 rebuilds only the first tile column (kx = 0..TLZ−1) and its partial sums.
+  const char* z_init(int vorticity = 1, int columns = 0) {
     bu_fresh_ = false;   // A is rewritten
     const int with_scalar = vorticity == 2 ? 0 : p_.scalar;
+    const int gx = g_.KXP / TLZ, gl = columns ? columns : gx;
 #ifdef GBGHT_EMU
-    const int gx = g_.KXP / TLZ;
-    emu_grid(gx, g_.NY2, 1, smem_z(), [&](const Cta& c, void* sm) {
+    emu_grid(gl, g_.NY2, 1, smem_z(), [&](const Cta& c, void* sm) {
       Cplx<T>* W = static_cast<Cplx<T>*>(sm);
       double* red = reinterpret_cast<double*>(W + N * TLZ);
       ZRowsReg<T, ZOwn<T, N, TLZ, 1>> rows;
@@ -1015,8 +1016,8 @@ class EngineImpl final : public Engine {
           body_z_init<T, N, TLZ, 1>(c, W, red, g_, rows, A_, S_, with_scalar, tw_, vorticity);
     });
 #else
-    k_z_init<T, N, TLZ, NTZ><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, S_, with_scalar,
-                                                                                       partial_, tw_, vorticity);
+    k_z_init<T, N, TLZ, NTZ><<<dim3(gl, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, S_, with_scalar, partial_,
+                                                                            tw_, vorticity, gx);
 #endif
     return rt_check();
   }
@@ -1136,9 +1137,13 @@ class EngineImpl final : public Engine {
       const bool rescaled = project();
       reality();
       // The last epilogue left the z-inverse of the unrescaled state in A; the deposit and the next
-      // stage read A, so it is rebuilt from the rescaled state. (The reality projection needs no
-      // rebuild: it changes only the anti-Hermitian part, which the real inverse does not see.)
+      // stage read A, so it is rebuilt from the rescaled state. The reality projection changes only
+      // the kx = 0 plane's anti-Hermitian part, which the real inverse does not see in exact
+      // arithmetic but does see at round-off; the first tile column of A (and its energy partial)
+      // is rebuilt from the projected state, so A is exactly what an import of the end-of-step
+      // state builds, and a run restored from a checkpoint continues this one bit for bit.
       if (rescaled) return z_init();
+      return z_init(1, 1);
     }
     return rt_check();
   }

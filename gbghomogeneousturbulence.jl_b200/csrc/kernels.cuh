@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(NT, NT > 256 ? 1 : (sizeof(T) == 8 ? 2 : 4)) k
 
 template <class T, int N, int TL, int NT>
 __global__ void __launch_bounds__(NT, NT > 256 ? 1 : 2) k_z_init(Geometry g, Cplx<T>* A, const Cplx<T>* S, int has_scalar, double* partial,
-                                                  const Cplx<T>* tw, int vorticity = 1) {
+                                                  const Cplx<T>* tw, int vorticity = 1, int pstride = 0) {
   CTA_CTX;
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
   double* red = reinterpret_cast<double*>(W + N * TL);
@@ -160,7 +160,8 @@ __global__ void __launch_bounds__(NT, NT > 256 ? 1 : 2) k_z_init(Geometry g, Cpl
   const double e = with_z_rows<T, N, TL, NT>(slot, [&](auto& rows) {
     return body_z_init<T, N, TL, NT>(c, W, red, g, rows, A, S, has_scalar, tw, vorticity);
   });
-  if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
+  // pstride: the tiles per row of the partials (the full grid's, when a launch covers fewer columns)
+  if (c.tid == 0) partial[blockIdx.y * (pstride ? pstride : gridDim.x) + blockIdx.x] = e;
 }
 template <class T, int NT, int CH>
 __global__ void __launch_bounds__(NT) k_below_scale(Geometry g, double L, const Cplx<T>* S, double* out) {

@@ -1344,7 +1344,9 @@ GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, double* red, const Geometr
   const int kx0 = c.bx * TL, qy = c.by;
   const double ky = g.s * double(q_to_m(qy, g.K, g.NY2));
   double esum = 0.0;
-  for_own_slots<T, N, TL, NT>(c, g, [&](int b, int sl, bool ret, int q, int, int l) {
+  // the retained rows of half 0, then of half 1: the epilogue's order, so the tile's energy sum
+  // (the next stage's forcing amplitude reads it) is the epilogue's to the last bit
+  const auto own = [&](int b, int sl, bool ret, int q, int, int l) {
     Cplx<T> u0 = czero<T>(), u1 = czero<T>(), u2 = czero<T>();
     if (ret) {
       const int kx = kx0 + l;
@@ -1358,7 +1360,9 @@ GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, double* red, const Geometr
     rows.put(0, b, sl, u0);
     rows.put(1, b, sl, u1);
     rows.put(2, b, sl, u2);
-  });
+  };
+  for_own_slots<T, N, TL, NT, 0>(c, g, own);
+  for_own_slots<T, N, TL, NT, 1>(c, g, own);
   rows.put_done();
   red[c.tid] = esum;
   GBGHT_SYNC();
