@@ -877,6 +877,96 @@ int gbght_status_word(gbght_run* r, uint32_t* word) {
   return GBGHT_OK;
 }
 
+// ---- the discrete adjoint of the step ----------------------------------------------------------------
+int gbght_adjoint_create(gbght_run* r, int snapshots) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  const gbght_config& c = r->cfg;
+  if (c.scheme != GBGHT_IFRK4 && c.scheme != GBGHT_IFRK3)
+    return fail(r, GBGHT_ERR_ARGUMENT, "the adjoint is built for the low-storage schemes IFLowStorageRK4 and "
+                                       "IFLowStorageRK3");
+  auto ok_forcing = [](int k) {
+    return k == GBGHT_FORCING_NONE || k == GBGHT_FORCING_CONSTANT_POWER || k == GBGHT_FORCING_LINEAR;
+  };
+  if (!ok_forcing(c.velocity_forcing.kind) || (c.scalar && !ok_forcing(c.scalar_forcing.kind)))
+    return fail(r, GBGHT_ERR_ARGUMENT, "the adjoint is built for NoForcing, ConstantPower and Linear forcing");
+  if (snapshots < 0 || snapshots > 64) return fail(r, GBGHT_ERR_ARGUMENT, "snapshots must lie in [0, 64]");
+  return engine_call(r, r->eng->adjoint_init(snapshots));
+}
+
+int gbght_adjoint_import(gbght_run* r, const double* lam_u, const double* lam_phi) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!lam_u) return fail(r, GBGHT_ERR_ARGUMENT, "lam_u is null");
+  if (r->cfg.scalar && !lam_phi)
+    return fail(r, GBGHT_ERR_ARGUMENT, "this run carries a passive scalar, so lam_phi must be given");
+  bool outside = false;
+  int rc = engine_call(r, r->eng->adjoint_import(lam_u, lam_phi, &outside));
+  if (rc) return rc;
+  if (outside)
+    return fail(r, GBGHT_ERR_ARGUMENT, "the cotangent has content outside the retained 2/3 ball, where the state "
+                                       "has none; the adjoint register was cleared");
+  return GBGHT_OK;
+}
+
+int gbght_adjoint_export(gbght_run* r, double* lam_u, double* lam_phi) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!lam_u) return fail(r, GBGHT_ERR_ARGUMENT, "lam_u is null");
+  return engine_call(r, r->eng->adjoint_export(lam_u, r->cfg.scalar ? lam_phi : nullptr));
+}
+
+int gbght_adjoint_step(gbght_run* r, double dt) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!finite_positive(dt))
+    return fail(r, GBGHT_ERR_ARGUMENT, "the timestep must be positive and finite, got " + std::to_string(dt));
+  const Tableau t = tableau(r->cfg.scheme);
+  return engine_call(r, r->eng->adjoint_step(dt, t.a, t.b, t.d, t.S));
+}
+
+int gbght_adjoint_add_observable(gbght_run* r, int which, double weight) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!std::isfinite(weight)) return fail(r, GBGHT_ERR_ARGUMENT, "the weight must be finite");
+  const double n = r->cfg.grid_points_per_axis, n6 = n * n * n * n * n * n;
+  if (which == GBGHT_OBSERVABLE_KINETIC_ENERGY) return engine_call(r, r->eng->adjoint_add(weight / n6, 0.0));
+  if (which == GBGHT_OBSERVABLE_SCALAR_VARIANCE) {
+    if (!r->cfg.scalar) return fail(r, GBGHT_ERR_ARGUMENT, "the run carries no scalar");
+    return engine_call(r, r->eng->adjoint_add(0.0, 2.0 * weight / n6));
+  }
+  return fail(r, GBGHT_ERR_ARGUMENT, "unknown observable");
+}
+
+int gbght_adjoint_forcing_gradient(gbght_run* r, double out[2], int reset) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  double g[2] = {0.0, 0.0};
+  int rc = engine_call(r, r->eng->adjoint_gradient(g, reset));
+  if (rc) return rc;
+  if (out) {
+    out[0] = g[0];
+    out[1] = g[1];
+  }
+  return GBGHT_OK;
+}
+
+int gbght_adjoint_clear(gbght_run* r) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  return engine_call(r, r->eng->adjoint_clear());
+}
+
+int gbght_snapshot_save(gbght_run* r, int slot) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  const char* e = r->eng->snapshot_save(slot);
+  if (e && std::strstr(e, "snapshot")) return fail(r, GBGHT_ERR_ARGUMENT, e);
+  return engine_call(r, e);
+}
+
+int gbght_snapshot_load(gbght_run* r, int slot) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  const char* e = r->eng->snapshot_load(slot);
+  if (e && std::strstr(e, "snapshot")) return fail(r, GBGHT_ERR_ARGUMENT, e);
+  int rc = engine_call(r, e);
+  if (rc) return rc;
+  r->fields_epoch += 1;   // a new state: the deposit is stale
+  return GBGHT_OK;
+}
+
 int gbght_profile(gbght_run* r, int enable) {
   if (check_run(r)) return GBGHT_ERR_ARGUMENT;
   return engine_call(r, r->eng->profile(enable));

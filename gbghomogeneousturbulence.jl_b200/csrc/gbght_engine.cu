@@ -130,6 +130,12 @@ class EngineImpl final : public Engine {
   // up to 512
   static constexpr int NTZ = kNTZ(N * TLZ / Radices<N>::r[0]);
   static constexpr int NTR = kNT(256);
+#ifdef GBGHT_EMU
+  static constexpr int NTXA = 1, NTZA = 1;
+#else
+  static constexpr int NTXA = 32 * XAdjShape<T>::NW;   // the adjoint x pass: one warp per line
+  static constexpr int NTZA = kNT(N * TLZ / 8);       // the adjoint z pass
+#endif
 
  public:
   ~EngineImpl() override {
@@ -702,6 +708,185 @@ class EngineImpl final : public Engine {
     return (st & GBGHT_DEV_TIMEOUT) ? kDeviceTimeoutMessage : nullptr;
   }
 
+  // ---- the adjoint of the step ----------------------------------------------------------------------
+  static constexpr int kMaxStages = 5;
+  const char* adjoint_init(int snapshots) override {
+    if (adj_ready_) {
+      if (snapshots == nsnap_) return nullptr;
+      return "the adjoint registers exist already with another snapshot count";
+    }
+    const size_t s4 = 4 * nS_ * sizeof(Cplx<T>);
+    const char* err = nullptr;
+    if ((err = alloc(&L_, s4))) return err;
+    if ((err = alloc(&LH_, s4))) return err;
+    if ((err = alloc(&Qs_, kMaxStages * s4))) return err;
+    if ((err = alloc(&Aa_, 7 * nA_ * sizeof(Cplx<T>)))) return err;
+    if ((err = alloc(&Ba_, 7 * nB_ * sizeof(Cplx<T>)))) return err;
+    if (snapshots > 0 && (err = alloc(&snaps_, size_t(snapshots) * s4))) return err;
+    if ((err = alloc(&ampsave_, 2 * kMaxStages * sizeof(double)))) return err;
+    if ((err = alloc(&coef_, 4 * sizeof(double)))) return err;
+    if ((err = alloc(&grad_, 2 * sizeof(double)))) return err;
+#ifndef GBGHT_EMU
+    if ((err = make_maps_on(&maps_adj_, Aa_, Ba_))) return err;
+#endif
+    nsnap_ = snapshots;
+    adj_ready_ = true;
+    return rt_sync(stream_);
+  }
+  const char* adjoint_import(const double* lu, const double* lp, bool* outside) override {
+    if (!adj_ready_) return "the adjoint is not set up";
+    const int nc = p_.scalar ? 4 : 3;
+    const size_t nref = ref_comp_elems();
+    *outside = false;
+    const int wu = where(lu), wp = nc == 4 ? where(lp) : 0;
+    if (wu < 0 || wp < 0) return "an adjoint array is device memory of another device";
+    bu_fresh_ = false;   // B is the host staging
+    Cplx<double>* stage = reinterpret_cast<Cplx<double>*>(B_);
+    const char* err = rt_memset(L_, 0, 4 * nS_ * sizeof(Cplx<T>), stream_);
+    if (!err) err = rt_memset(flag_, 0, sizeof(unsigned int), stream_);
+    for (int cc = 0; cc < nc && !err; ++cc) {
+      const double* src = cc < 3 ? lu + size_t(cc) * nref * 2 : lp;
+      const Cplx<double>* ref = reinterpret_cast<const Cplx<double>*>(src);
+      if (!(cc < 3 ? wu : wp)) {
+        if ((err = rt_h2d(stage, src, nref * sizeof(Cplx<double>), stream_))) break;
+        ref = stage;
+      }
+#ifdef GBGHT_EMU
+      for (size_t i = 0; i < nref; ++i) import_mode<T>(i, g_, ref, L_ + cc * nS_, flag_);
+#else
+      k_import<T><<<unsigned((nref + 255) / 256), 256, 0, stream_>>>(g_, ref, L_ + cc * nS_, flag_);
+      err = rt_check();
+#endif
+    }
+    unsigned int fl = 0;
+    if (!err) err = rt_d2h(&fl, flag_, sizeof fl, stream_);
+    if (err) return err;
+    if (fl & 1u) {
+      *outside = true;
+      return rt_memset(L_, 0, 4 * nS_ * sizeof(Cplx<T>), stream_);
+    }
+    return rt_sync(stream_);
+  }
+  const char* adjoint_export(double* lu, double* lp) override {
+    if (!adj_ready_) return "the adjoint is not set up";
+    const size_t nref = ref_comp_elems();
+    const int nc = (p_.scalar && lp) ? 4 : 3;
+    const int wu = where(lu), wp = nc == 4 ? where(lp) : 0;
+    if (wu < 0 || wp < 0) return "an adjoint array is device memory of another device";
+    bu_fresh_ = false;
+    Cplx<double>* stage = reinterpret_cast<Cplx<double>*>(B_);
+    for (int cc = 0; cc < nc; ++cc) {
+      double* dst = cc < 3 ? lu + size_t(cc) * nref * 2 : lp;
+      const bool direct = (cc < 3 ? wu : wp) == 1;
+      Cplx<double>* ref = direct ? reinterpret_cast<Cplx<double>*>(dst) : stage;
+#ifdef GBGHT_EMU
+      for (size_t i = 0; i < nref; ++i) export_mode<T>(i, g_, L_ + cc * nS_, ref);
+#else
+      k_export<T><<<unsigned((nref + 255) / 256), 256, 0, stream_>>>(g_, L_ + cc * nS_, ref);
+      if (const char* e = rt_check()) return e;
+#endif
+      if (!direct)
+        if (const char* e = rt_d2h(dst, ref, nref * sizeof(Cplx<double>), stream_)) return e;
+    }
+    return rt_sync(stream_);
+  }
+  const char* adjoint_add(double wu, double wp) override {
+    if (!adj_ready_) return "the adjoint is not set up";
+    const int nc = p_.scalar ? 4 : 3;
+#ifdef GBGHT_EMU
+    for (size_t i = 0; i < nS_; ++i) adj_add_mode<T>(i, nS_, nc, L_, S_, wu, wp);
+#else
+    k_adj_add<T><<<unsigned((nS_ + 255) / 256), 256, 0, stream_>>>(nS_, nc, L_, S_, wu, wp);
+#endif
+    return rt_check();
+  }
+  const char* adjoint_gradient(double* g2, int reset) override {
+    if (!adj_ready_) return "the adjoint is not set up";
+    if (const char* e = rt_d2h(g2, grad_, 2 * sizeof(double), stream_)) return e;
+    return reset ? rt_memset(grad_, 0, 2 * sizeof(double), stream_) : nullptr;
+  }
+  const char* adjoint_clear() override {
+    if (!adj_ready_) return "the adjoint is not set up";
+    const char* e = rt_memset(L_, 0, 4 * nS_ * sizeof(Cplx<T>), stream_);
+    if (!e) e = rt_memset(grad_, 0, 2 * sizeof(double), stream_);
+    return e ? e : rt_sync(stream_);
+  }
+  const char* snapshot_save(int slot) override {
+    if (slot < 0 || slot >= nsnap_) return "no such snapshot slot";
+    return rt_d2d(snaps_ + size_t(slot) * 4 * nS_, S_, 4 * nS_ * sizeof(Cplx<T>), stream_);
+  }
+  const char* snapshot_load(int slot) override {
+    if (slot < 0 || slot >= nsnap_) return "no such snapshot slot";
+    const char* e = rt_d2d(S_, snaps_ + size_t(slot) * 4 * nS_, 4 * nS_ * sizeof(Cplx<T>), stream_);
+    if (!e) e = z_init();
+    return e;
+  }
+
+  // The reverse of one low-storage step at the current state q: the forward stages again, keeping
+  // each stage's state and amplitudes; then, per stage in reverse, the stage's forward fields
+  // (z- and y-inverse of the saved state), the adjoint x pass, its y-forward, the band coefficients
+  // and the adjoint z pass; finally the state is put back.
+  const char* adjoint_step(double dt, const double* a, const double* b, const double* d, int S) override {
+    if (!adj_ready_) return "the adjoint is not set up";
+    if (S < 1 || S > kMaxStages) return "the adjoint needs a low-storage scheme";
+    const size_t s4 = 4 * nS_;
+    for (int i = 0; i < S; ++i) {
+      if (const char* e = rt_d2d(Qs_ + i * s4, S_, s4 * sizeof(Cplx<T>), stream_)) return e;
+      StageArgs st = stage_base(dt);
+      st.kind = kLowStorage;
+      st.a = a[i];
+      st.b = b[i];
+      st.first = i == 0;
+      st.last = i == S - 1;
+      st.read_h = !st.first;
+      st.write_h = !st.last;
+      set_factor(st, d[i] * dt, false);
+      amp_save_to_ = ampsave_ + 2 * i;
+      const char* e = stage(st);
+      amp_save_to_ = nullptr;
+      if (e) return e;
+    }
+    const int nc = p_.scalar ? 4 : 3;
+    const int ninv = p_.scalar ? 7 : 6, nsrc = p_.scalar ? 6 : 3, nprod = p_.scalar ? 7 : 6;
+    // the end-of-step projections in reverse: the reality projection (self-adjoint), then the
+    // start launch applies the Leray projection and opens the last stage
+#ifdef GBGHT_EMU
+    for (int i = 0; i < g_.NY2 * g_.NY2; ++i) reality_mode<T>(i, g_, L_, nc);
+#else
+    k_reality<T><<<(g_.NY2 * g_.NY2 + 255) / 256, 256, 0, stream_>>>(g_, L_, nc);
+#endif
+    AdjArgs base = adj_base(dt);
+    AdjArgs st = base;
+    st.combine = 0;
+    st.prologue = 1;
+    adj_factor(st, d[S - 1] * dt);
+    st.b = b[S - 1];
+    st.a_next = 0.0;
+    adj_z(st, nullptr);
+    for (int i = S - 1; i >= 0; --i) {
+      if (const char* e = z_init(1, 0, Qs_ + i * s4)) return e;   // the stage's u, ω, φ
+      y_inverse_on(0, ninv, maps_, A_, B_);
+      y_inverse_on(0, nsrc, maps_adj_, Aa_, Ba_);
+      x_adjoint();
+      y_forward_on(nprod, maps_adj_, Ba_, Aa_);
+      if (base.forced || base.sforced) adj_band(dt, i);
+      st = base;
+      st.combine = 1;
+      st.prologue = i > 0;
+      if (i > 0) {
+        adj_factor(st, d[i - 1] * dt);
+        st.b = b[i - 1];
+        st.a_next = a[i];
+      }
+      adj_z(st, Qs_ + i * s4);
+      if (const char* e = rt_check()) return e;
+    }
+    // the state as it was, its z-inverse in A (the deposit is unchanged)
+    if (const char* e = rt_d2d(S_, Qs_, s4 * sizeof(Cplx<T>), stream_)) return e;
+    if (const char* e = z_init()) return e;
+    return rt_check();
+  }
+
   const char* status(uint32_t* word) override {
     unsigned int v = 0;
     const char* err = rt_d2h(&v, status_, sizeof v, stream_);
@@ -809,6 +994,9 @@ class EngineImpl final : public Engine {
   }
 
   static constexpr size_t kBarBytes = 32;
+  // the adjoint's x pass (its lines) and z pass (the FFT tile and six retained-row components)
+  size_t smem_xa() const { return size_t(XAdjShape<T>::NIN) * N * sizeof(Cplx<T>); }
+  size_t smem_za() const { return (size_t(N) * TLZ + size_t(6) * g_.NY2 * TLZ) * sizeof(Cplx<T>); }
   size_t smem_y() const { return size_t(N) * TLY * sizeof(Cplx<T>) + kBarBytes; }
   size_t smem_x() const {
     return size_t(N) * XShape<T>::ACT_INV * sizeof(Cplx<T>) +
@@ -843,11 +1031,15 @@ class EngineImpl final : public Engine {
     set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp2>), smem_ze());
     set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp3>), smem_ze());
     set(reinterpret_cast<const void*>(k_z_init<T, N, TLZ, NTZ>), smem_z());
+    set(reinterpret_cast<const void*>(k_x_adjoint<T, N, NTXA>), smem_xa());
+    set(reinterpret_cast<const void*>(k_adj_z<T, N, TLZ, NTZA>), smem_za());
     return e;
   }
 
   // Tensor maps over A and B (see TmaMaps in passes.cuh), encoded through the driver entry point.
-  const char* make_maps() {
+  const char* make_maps() { return make_maps_on(&maps_, A_, B_); }
+  const char* make_maps_on(TmaMaps* mp, Cplx<T>* A, Cplx<T>* B) {
+    TmaMaps& maps = *mp;
     using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -873,15 +1065,15 @@ class EngineImpl final : public Engine {
     const cuuint32_t bxy = 2 * TLY, bxz = 2 * TLZ;
     const cuuint32_t K1 = cuuint32_t(g_.K + 1), K0 = cuuint32_t(g_.K);
     const cuuint32_t BY = cuuint32_t(box_rows<N>());
-    if (!map2(&maps_.a_ld, A_, cuuint64_t(7) * N * g_.NY2, bxy, K1)) return "tensor map a_ld";
-    if (!map2(&maps_.a_st1, A_, cuuint64_t(7) * N * g_.NY2, bxy, K1)) return "tensor map a_st1";
-    if (!map2(&maps_.a_st2, A_, cuuint64_t(7) * N * g_.NY2, bxy, K0)) return "tensor map a_st2";
-    if (!map2(&maps_.b, B_, cuuint64_t(7) * N * N, bxy, BY)) return "tensor map b";
+    if (!map2(&maps.a_ld, A, cuuint64_t(7) * N * g_.NY2, bxy, K1)) return "tensor map a_ld";
+    if (!map2(&maps.a_st1, A, cuuint64_t(7) * N * g_.NY2, bxy, K1)) return "tensor map a_st1";
+    if (!map2(&maps.a_st2, A, cuuint64_t(7) * N * g_.NY2, bxy, K0)) return "tensor map a_st2";
+    if (!map2(&maps.b, B, cuuint64_t(7) * N * N, bxy, BY)) return "tensor map b";
     {
       const cuuint64_t dims[3] = {inner, cuuint64_t(g_.NY2), cuuint64_t(7) * N};
       const cuuint64_t strides[2] = {pitch, pitch * g_.NY2};
       const cuuint32_t box[3] = {bxz, 1, BY};
-      if (encode(&maps_.az, dt, 3, A_, dims, strides, box, ones, CU_TENSOR_MAP_INTERLEAVE_NONE,
+      if (encode(&maps.az, dt, 3, A, dims, strides, box, ones, CU_TENSOR_MAP_INTERLEAVE_NONE,
                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return "tensor map az";
@@ -890,7 +1082,7 @@ class EngineImpl final : public Engine {
       const cuuint64_t dims[3] = {inner, cuuint64_t(g_.NY2), cuuint64_t(4) * g_.NY2};
       const cuuint64_t strides[2] = {pitch, pitch * g_.NY2};
       const cuuint32_t box[3] = {bxz, K1, 1};
-      if (encode(which == 0 ? &maps_.s3 : &maps_.h3, dt, 3, which == 0 ? S_ : H_, dims, strides, box, ones,
+      if (encode(which == 0 ? &maps.s3 : &maps.h3, dt, 3, which == 0 ? S_ : H_, dims, strides, box, ones,
                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return which == 0 ? "tensor map s3" : "tensor map h3";
@@ -899,31 +1091,40 @@ class EngineImpl final : public Engine {
   }
 #endif
 
-  void y_inverse(int c0, int nc) {
+  // The y passes over an (A, B) pair: the run's own (A_, B_, maps_) or the adjoint's.
+  void y_inverse(int c0, int nc) { y_inverse_on(c0, nc, maps_, A_, B_); }
+  void y_forward(int nc) { y_forward_on(nc, maps_, B_, A_); }
+  void y_inverse_on(int c0, int nc, const TmaMaps& m, Cplx<T>* A, Cplx<T>* B) {
 #ifdef GBGHT_EMU
+    (void)m;
     emu_grid(g_.KXP / TLY, N, nc, smem_y(), [&](const Cta& c, void* sm) {
       Cplx<T>* t = static_cast<Cplx<T>*>(sm);
-      y_inverse_load_host<T, N, TLY>(c, t, g_, A_, c0);
+      y_inverse_load_host<T, N, TLY>(c, t, g_, A, c0);
       y_inverse_compute<T, N, TLY, 1>(c, t, g_, tw_);
-      y_store_host<T, N, TLY>(c, t, g_, B_, c0 + c.bz);
+      y_store_host<T, N, TLY>(c, t, g_, B, c0 + c.bz);
     });
 #else
+    (void)A;
+    (void)B;
     pbegin(PROF_Y_INVERSE);
-    k_y_inverse<T, N, TLY, NTY><<<dim3(g_.KXP / TLY, N, nc), NTY, smem_y(), stream_>>>(maps_, g_, c0, tw_, status_);
+    k_y_inverse<T, N, TLY, NTY><<<dim3(g_.KXP / TLY, N, nc), NTY, smem_y(), stream_>>>(m, g_, c0, tw_, status_);
     pend();
 #endif
   }
-  void y_forward(int nc) {
+  void y_forward_on(int nc, const TmaMaps& m, Cplx<T>* B, Cplx<T>* A) {
 #ifdef GBGHT_EMU
+    (void)m;
     emu_grid(g_.KXP / TLY, N, nc, smem_y(), [&](const Cta& c, void* sm) {
       Cplx<T>* t = static_cast<Cplx<T>*>(sm);
-      y_forward_load_host<T, N, TLY>(c, t, g_, B_);
+      y_forward_load_host<T, N, TLY>(c, t, g_, B);
       tile_fft<T, N, TLY, 1, -1>(c, t, tw_);
-      y_forward_store_host<T, N, TLY>(c, t, g_, A_);
+      y_forward_store_host<T, N, TLY>(c, t, g_, A);
     });
 #else
+    (void)A;
+    (void)B;
     pbegin(PROF_Y_FORWARD);
-    k_y_forward<T, N, TLY, NTY><<<dim3(g_.KXP / TLY, N, nc), NTY, smem_y(), stream_>>>(maps_, g_, tw_, status_);
+    k_y_forward<T, N, TLY, NTY><<<dim3(g_.KXP / TLY, N, nc), NTY, smem_y(), stream_>>>(m, g_, tw_, status_);
     pend();
 #endif
   }
@@ -1003,7 +1204,9 @@ class EngineImpl final : public Engine {
   // The z-inverse of the state into the A slots (u, iκ×û, φ), or with `vorticity` = 2 of the six
   // strain components into slots 0..5.
   // `columns` = 1 rebuilds only the first tile column (kx = 0..TLZ−1) and its partial sums.
-  const char* z_init(int vorticity = 1, int columns = 0) {
+  // `from` replaces the state by another S-layout array (a saved stage state of the adjoint).
+  const char* z_init(int vorticity = 1, int columns = 0, const Cplx<T>* from = nullptr) {
+    const Cplx<T>* Ssrc = from ? from : S_;
     bu_fresh_ = false;   // A is rewritten
     const int with_scalar = vorticity == 2 ? 0 : p_.scalar;
     const int gx = g_.KXP / TLZ, gl = columns ? columns : gx;
@@ -1013,13 +1216,92 @@ class EngineImpl final : public Engine {
       double* red = reinterpret_cast<double*>(W + N * TLZ);
       ZRowsReg<T, ZOwn<T, N, TLZ, 1>> rows;
       partial_[c.by * gx + c.bx] =
-          body_z_init<T, N, TLZ, 1>(c, W, red, g_, rows, A_, S_, with_scalar, tw_, vorticity);
+          body_z_init<T, N, TLZ, 1>(c, W, red, g_, rows, A_, Ssrc, with_scalar, tw_, vorticity);
     });
 #else
-    k_z_init<T, N, TLZ, NTZ><<<dim3(gl, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, S_, with_scalar, partial_,
+    k_z_init<T, N, TLZ, NTZ><<<dim3(gl, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, Ssrc, with_scalar, partial_,
                                                                             tw_, vorticity, gx);
 #endif
     return rt_check();
+  }
+  // ---- adjoint launches -------------------------------------------------------------------------------
+  AdjArgs adj_base(double dt) const {
+    AdjArgs a{};
+    a.has_scalar = p_.scalar;
+    a.dt = dt;
+    for (int k = 0; k < 3; ++k) a.G[k] = p_.G[k];
+    a.forced = p_.vf.kind == kForceConstantPower;
+    a.sforced = p_.scalar && p_.sf.kind == kForceConstantPower;
+    a.band_lo2 = band_lo2();
+    a.band_hi2 = band_hi2();
+    a.sband_lo2 = sband_lo2();
+    a.sband_hi2 = sband_hi2();
+    return a;
+  }
+  // the integrating factor of a span δ, as the forward stage's (set_factor)
+  void adj_factor(AdjArgs& a, double delta) const {
+    StageArgs st{};
+    set_factor(st, delta, false);
+    a.cu = st.cu;
+    a.cphi = st.cphi;
+    a.lin_u = st.lin_u;
+    a.lin_phi = st.lin_phi;
+  }
+  void x_adjoint() {
+    using X = XAdjShape<T>;
+    const int ntiles = (N / X::P) * N;
+#ifdef GBGHT_EMU
+    emu_grid(ntiles, 1, 1, smem_xa(), [&](const Cta& c, void* sm) {
+      body_x_adjoint<T, N, 1>(c, static_cast<Cplx<T>*>(sm), g_, B_, Ba_, p_.scalar, tw_);
+    });
+#else
+    pbegin(PROF_X_ADJOINT);
+    k_x_adjoint<T, N, NTXA><<<ntiles, NTXA, smem_xa(), stream_>>>(g_, B_, Ba_, p_.scalar, tw_);
+    pend();
+#endif
+  }
+  void adj_z(const AdjArgs& a, const Cplx<T>* Q) {
+#ifdef GBGHT_EMU
+    emu_grid(g_.KXP / TLZ, g_.NY2, 1, smem_za(), [&](const Cta& c, void* sm) {
+      Cplx<T>* W = static_cast<Cplx<T>*>(sm);
+      body_adj_z<T, N, TLZ, 1>(c, W, W + N * TLZ, g_, a, Aa_, L_, LH_, Q, coef_, tw_);
+    });
+#else
+    pbegin(PROF_Z_ADJOINT);
+    k_adj_z<T, N, TLZ, NTZA><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZA, smem_za(), stream_>>>(g_, a, Aa_, L_, LH_, Q,
+                                                                                        coef_, tw_);
+    pend();
+#endif
+  }
+  // stage i's ConstantPower coefficients from its saved state and amplitudes and λ_h in LH
+  void adj_band(double dt, int i) {
+    AdjBandArgs a{};
+    a.dt = dt;
+    a.n6 = double(N) * N * N * double(N) * N * N;
+    a.lo2 = band_lo2();
+    a.hi2 = band_hi2();
+    a.slo2 = sband_lo2();
+    a.shi2 = sband_hi2();
+    a.eps_u = p_.vf.kind == kForceConstantPower ? p_.vf.rate : 0.0;
+    a.eps_p = p_.scalar && p_.sf.kind == kForceConstantPower ? p_.sf.rate : 0.0;
+    const Cplx<T>* Q = Qs_ + size_t(i) * 4 * nS_;
+    const double* amp = ampsave_ + 2 * i;
+#ifdef GBGHT_EMU
+    double su = 0.0, sp = 0.0;
+    if (a.eps_u != 0.0) {
+      const int mb = band_box_side(g_, a.hi2), side = 2 * mb + 1, n = 3 * side * side * (mb + 1);
+      for (int k = 0; k < n; ++k) su += band_pair_term<T>(g_, Q, LH_, 0, mb, a.lo2, a.hi2, k);
+    }
+    if (a.eps_p != 0.0) {
+      const int mb = band_box_side(g_, a.shi2), side = 2 * mb + 1, n = side * side * (mb + 1);
+      for (int k = 0; k < n; ++k) sp += band_pair_term<T>(g_, Q, LH_, 3, mb, a.slo2, a.shi2, k);
+    }
+    adj_band_finish(a, amp, su, sp, coef_, grad_);
+#else
+    pbegin(PROF_FORCE_AMP);
+    k_adj_band<T><<<1, 256, 0, stream_>>>(g_, Q, LH_, a, amp, coef_, grad_);
+    pend();
+#endif
   }
   void reality() {
     const int n = g_.NY2 * g_.NY2;
@@ -1132,6 +1414,11 @@ class EngineImpl final : public Engine {
     x_products();
     y_forward(nfwd);
     if (st.forced || st.sforced) force_amp(st);
+    if (amp_save_to_) {   // the adjoint's forward pass keeps the stage's amplitudes
+      const char* e = rt_d2d(amp_save_to_, amp_, sizeof(double), stream_);
+      if (!e) e = rt_d2d(amp_save_to_ + 1, amp_ + 4, sizeof(double), stream_);
+      if (e) return e;
+    }
     z_epilogue(st);
     if (st.last) {
       const bool rescaled = project();
@@ -1210,6 +1497,15 @@ class EngineImpl final : public Engine {
   unsigned int* flag_ = nullptr;     // import: content outside the retained ball
   uint32_t *tkey_ = nullptr, *torder_ = nullptr, *tcount_ = nullptr;   // the traversal sort
   int nbins_ = 0;
+  // the adjoint (allocated by adjoint_init): λ and λ_h, the saved stage states and amplitudes, the
+  // adjoint A and B slots with their tensor maps, the band coefficients, the rates' gradients, the
+  // snapshot slots
+  bool adj_ready_ = false;
+  int nsnap_ = 0;
+  Cplx<T>*L_ = nullptr, *LH_ = nullptr, *Qs_ = nullptr, *Aa_ = nullptr, *Ba_ = nullptr, *snaps_ = nullptr;
+  double *ampsave_ = nullptr, *coef_ = nullptr, *grad_ = nullptr;
+  double* amp_save_to_ = nullptr;
+  TmaMaps maps_adj_{};
 };
 
 #if defined(GBGHT_UNIT_FACTORY)

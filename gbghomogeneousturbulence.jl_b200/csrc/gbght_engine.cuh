@@ -112,6 +112,19 @@ class Engine {
   // that is never issued); returns kDeviceTimeoutMessage once the expiry is seen, as any call that
   // reads the status word does. The run stays usable.
   virtual const char* expire_wait(long long cycles) = 0;
+  // The discrete adjoint of the low-storage schemes' step (adjoint.cuh). adjoint_init allocates
+  // the adjoint registers and `snapshots` device state slots. λ crosses in the reference layout
+  // (host or device memory). adjoint_step replaces λ by J(q)ᵀλ for the step of size dt at the
+  // current state q, accumulating the ConstantPower rates' gradients, and leaves q as it was.
+  virtual const char* adjoint_init(int snapshots) = 0;
+  virtual const char* adjoint_import(const double* lu, const double* lp, bool* outside) = 0;
+  virtual const char* adjoint_export(double* lu, double* lp) = 0;
+  virtual const char* adjoint_step(double dt, const double* a, const double* b, const double* d, int S) = 0;
+  virtual const char* adjoint_add(double wu, double wp) = 0;
+  virtual const char* adjoint_gradient(double* g, int reset) = 0;
+  virtual const char* adjoint_clear() = 0;
+  virtual const char* snapshot_save(int slot) = 0;
+  virtual const char* snapshot_load(int slot) = 0;
   virtual int K() const = 0;
   virtual double cutoff() const = 0;
 };
@@ -128,7 +141,9 @@ enum ProfileKind {
   PROF_TRACERS = 7,
   PROF_OBSERVABLES = 8,
   PROF_TRAVERSAL = 9,
-  PROF_KINDS = 10
+  PROF_X_ADJOINT = 10,
+  PROF_Z_ADJOINT = 11,
+  PROF_KINDS = 12
 };
 
 Engine* make_engine(int N, int precision, std::string* err);

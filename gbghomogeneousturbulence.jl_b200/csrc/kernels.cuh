@@ -3,6 +3,7 @@
 // entry point.
 #pragma once
 
+#include "adjoint.cuh"
 #include "passes.cuh"
 #include "tracers.cuh"
 
@@ -342,6 +343,53 @@ template <class T>
 __global__ void k_to_T(const double* in, T* out, size_t n) {
   const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < n) out[i] = T(in[i]);
+}
+
+// ---- the adjoint of the step (adjoint.cuh) ------------------------------------------------------
+// x pass: shared memory = the NIN lines of N elements.
+template <class T, int N, int NT>
+__global__ void __launch_bounds__(NT, 2) k_x_adjoint(Geometry g, const Cplx<T>* Bf, Cplx<T>* Ba, int has_scalar,
+                                                     const Cplx<T>* tw) {
+  CTA_CTX;
+  body_x_adjoint<T, N, NT>(c, reinterpret_cast<Cplx<T>*>(g_smem), g, Bf, Ba, has_scalar, tw);
+}
+// z pass: shared memory = the FFT tile (N·TL) and the retained rows (6·NY2·TL).
+template <class T, int N, int TL, int NT>
+__global__ void __launch_bounds__(NT) k_adj_z(Geometry g, AdjArgs a, Cplx<T>* Aa, Cplx<T>* L, Cplx<T>* LH,
+                                              const Cplx<T>* Q, const double* coef, const Cplx<T>* tw) {
+  CTA_CTX;
+  Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
+  body_adj_z<T, N, TL, NT>(c, W, W + N * TL, g, a, Aa, L, LH, Q, coef, tw);
+}
+// The band coefficients of one stage: 256 strided partial sums per field, then a fixed tree.
+template <class T>
+__global__ void k_adj_band(Geometry g, const Cplx<T>* Q, const Cplx<T>* LH, AdjBandArgs a, const double* amp,
+                           double* coef, double* grad) {
+  __shared__ double su[256], sp[256];
+  double u = 0.0, p = 0.0;
+  if (a.eps_u != 0.0) {
+    const int mb = band_box_side(g, a.hi2), side = 2 * mb + 1, n = 3 * side * side * (mb + 1);
+    for (int i = threadIdx.x; i < n; i += 256) u += band_pair_term<T>(g, Q, LH, 0, mb, a.lo2, a.hi2, i);
+  }
+  if (a.eps_p != 0.0) {
+    const int mb = band_box_side(g, a.shi2), side = 2 * mb + 1, n = side * side * (mb + 1);
+    for (int i = threadIdx.x; i < n; i += 256) p += band_pair_term<T>(g, Q, LH, 3, mb, a.slo2, a.shi2, i);
+  }
+  su[threadIdx.x] = u;
+  sp[threadIdx.x] = p;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      su[threadIdx.x] += su[threadIdx.x + w];
+      sp[threadIdx.x] += sp[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) adj_band_finish(a, amp, su[0], sp[0], coef, grad);
+}
+template <class T>
+__global__ void k_adj_add(size_t nS, int nc, Cplx<T>* L, const Cplx<T>* S, double wu, double wp) {
+  adj_add_mode<T>(size_t(blockIdx.x) * blockDim.x + threadIdx.x, nS, nc, L, S, wu, wp);
 }
 #endif
 

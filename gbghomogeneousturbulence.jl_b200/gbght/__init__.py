@@ -119,10 +119,20 @@ _SIGNATURES = {
     "gbght_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "gbght_profile_read": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64), _DP]),
     "gbght_timer": (C.c_int, [C.c_void_p, C.c_int, _DP]),
+    "gbght_adjoint_create": (C.c_int, [C.c_void_p, C.c_int]),
+    "gbght_adjoint_import": (C.c_int, [C.c_void_p, _DP, _DP]),
+    "gbght_adjoint_export": (C.c_int, [C.c_void_p, _DP, _DP]),
+    "gbght_adjoint_step": (C.c_int, [C.c_void_p, C.c_double]),
+    "gbght_adjoint_add_observable": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    "gbght_adjoint_forcing_gradient": (C.c_int, [C.c_void_p, _DP, C.c_int]),
+    "gbght_adjoint_clear": (C.c_int, [C.c_void_p]),
+    "gbght_snapshot_save": (C.c_int, [C.c_void_p, C.c_int]),
+    "gbght_snapshot_load": (C.c_int, [C.c_void_p, C.c_int]),
 }
 
 KERNELS = ("y_inverse", "x_products", "y_forward", "z_epilogue", "x_velocity", "force_amp", "reality",
-           "tracers", "observables", "traversal")
+           "tracers", "observables", "traversal", "x_adjoint", "z_adjoint")
+OBSERVABLES = {"kinetic_energy": 0, "scalar_variance": 1}
 
 _loaded: dict = {}
 
@@ -521,6 +531,55 @@ class Run:
 
     def synchronize(self):
         self._check(self.lib.gbght_synchronize(self.h))
+
+    # -- the discrete adjoint of the step (gbght_adjoint_*) ------------------------------------------
+    def adjoint_create(self, snapshots: int = 0):
+        """Allocate the adjoint registers and `snapshots` device state slots."""
+        self._check(self.lib.gbght_adjoint_create(self.h, int(snapshots)))
+
+    def adjoint_import(self, lam_u, lam_phi=None):
+        """The cotangent λ of the state, in the state's layout (NumPy arrays or CUDA tensors)."""
+        if _is_device(lam_u):
+            pu = _dev_ptr(lam_u, (3,) + self.spectral_shape, "lam_u")
+            pp = _dev_ptr(lam_phi, self.spectral_shape, "lam_phi") if self.setup.scalar else None
+            self._check(self.lib.gbght_adjoint_import(self.h, pu, pp))
+            return
+        u = np.ascontiguousarray(lam_u, dtype=np.complex128)
+        p = np.ascontiguousarray(lam_phi, dtype=np.complex128) if self.setup.scalar else None
+        self._check(self.lib.gbght_adjoint_import(self.h, u.view(np.float64).ctypes.data_as(_DP),
+                                                  None if p is None else p.view(np.float64).ctypes.data_as(_DP)))
+
+    def adjoint_export(self):
+        u = np.zeros((3,) + self.spectral_shape, np.complex128)
+        p = np.zeros(self.spectral_shape, np.complex128) if self.setup.scalar else None
+        self._check(self.lib.gbght_adjoint_export(self.h, u.view(np.float64).ctypes.data_as(_DP),
+                                                  None if p is None else p.view(np.float64).ctypes.data_as(_DP)))
+        return u, p
+
+    def adjoint_step(self, dt: float):
+        """λ ← J(q)ᵀλ for one step of size dt at the current state q (left unchanged)."""
+        self._check(self.lib.gbght_adjoint_step(self.h, float(dt)))
+
+    def adjoint_add_observable(self, which: str, weight: float):
+        """λ += weight · ∂(observable)/∂state, for "kinetic_energy" or "scalar_variance"."""
+        if which not in OBSERVABLES:
+            raise ValueError(f"unknown observable {which!r}")
+        self._check(self.lib.gbght_adjoint_add_observable(self.h, OBSERVABLES[which], float(weight)))
+
+    def forcing_gradient(self, reset: bool = False):
+        """The accumulated dL/dε of the velocity's and the scalar's ConstantPower rates."""
+        out = np.zeros(2)
+        self._check(self.lib.gbght_adjoint_forcing_gradient(self.h, _ptr(out), 1 if reset else 0))
+        return float(out[0]), float(out[1])
+
+    def adjoint_clear(self):
+        self._check(self.lib.gbght_adjoint_clear(self.h))
+
+    def snapshot_save(self, slot: int):
+        self._check(self.lib.gbght_snapshot_save(self.h, int(slot)))
+
+    def snapshot_load(self, slot: int):
+        self._check(self.lib.gbght_snapshot_load(self.h, int(slot)))
 
     def selftest_wait_timeout(self, cycles: int):
         """Expire a bounded device wait on purpose (`gbght_selftest_wait_timeout`); raises the

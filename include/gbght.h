@@ -291,7 +291,9 @@ enum gbght_kernel {
   GBGHT_KERNEL_TRACERS = 7,     /* tracer gather / Adams push */
   GBGHT_KERNEL_OBSERVABLES = 8, /* k, ε, ⟨φ²⟩, ε_φ reductions, their row sums for the band forcings,
                                    the diagnostics' reductions */
-  GBGHT_KERNEL_TRAVERSAL = 9    /* tracer traversal order: tile keys, scan, scatter */
+  GBGHT_KERNEL_TRAVERSAL = 9,   /* tracer traversal order: tile keys, scan, scatter */
+  GBGHT_KERNEL_X_ADJOINT = 10,  /* the adjoint x pass: c2r of fields and sources, their products, r2c */
+  GBGHT_KERNEL_Z_ADJOINT = 11   /* the adjoint z pass: z-forward, the λ update, the next stage's sources */
 };
 int gbght_profile(gbght_run* run, int enable);
 int gbght_profile_read(gbght_run* run, int kind, int64_t* launches, double* total_ms);
@@ -319,6 +321,38 @@ int gbght_timer(gbght_run* run, int op, double* ms);
  * made inside a stream capture. Errors are reported through gbght_global_error(). */
 int gbght_velocity_physical_noalloc(int grid_points_per_axis, double side_length, const double* u_hat,
                                     double* u, double* max_speed, void* stream);
+
+/* The discrete adjoint of the field step (no counterpart in the reference, which has no AD; the
+ * step it differentiates is _low_storage_2n_step!, src/Propagator.jl:326-419, with velocity_rhs! /
+ * scalar_rhs!, src/Generator.jl:484-534,648-730, and ConstantPower's source,
+ * src/Forcing.jl:1091-1117). It is the exact transpose of the discrete map gbght_step computes for
+ * IFLowStorageRK4 / IFLowStorageRK3 with NoForcing, ConstantPower or Linear forcing on either field
+ * and the mean scalar gradient, for the inner products Σ_x a·b (physical) and Σ w·Re(conj(x)·y)
+ * (spectral, w = 1 on the kx = 0 plane and 2 elsewhere), restricted to the retained 2/3 ball.
+ *
+ * gbght_adjoint_create allocates the adjoint registers (λ, the stage states) and `snapshots`
+ * device slots for the state (0..64), for a checkpointing schedule that stores states on the
+ * device. λ crosses in the reference layout, host or device memory (as gbght_state_import);
+ * content outside the retained ball is refused and clears λ. gbght_adjoint_step replaces λ by
+ * J(q)ᵀλ, J the Jacobian of one step of size dt at the run's current state q; it runs the step's
+ * stages again to keep their states, leaves q (and the deposit) as they were, and adds to the
+ * forcing gradient the derivative of the loss with respect to each ConstantPower injection rate
+ * ε (velocity, scalar) through that step. gbght_adjoint_add_observable adds `weight` times the
+ * gradient of an observable of the current state to λ: the kinetic energy k (which = 0, gradient
+ * û/N⁶) or the scalar variance ⟨φ²⟩ (which = 1, gradient 2φ̂/N⁶). gbght_adjoint_forcing_gradient
+ * returns the accumulated dL/dε of the two fields (and clears it when `reset`);
+ * gbght_adjoint_clear sets λ and the gradient to zero. gbght_snapshot_save / _load copy the state
+ * into / out of a slot (load makes the deposit stale, as an import does). */
+enum gbght_observable { GBGHT_OBSERVABLE_KINETIC_ENERGY = 0, GBGHT_OBSERVABLE_SCALAR_VARIANCE = 1 };
+int gbght_adjoint_create(gbght_run* run, int snapshots);
+int gbght_adjoint_import(gbght_run* run, const double* lam_u, const double* lam_phi);
+int gbght_adjoint_export(gbght_run* run, double* lam_u, double* lam_phi);
+int gbght_adjoint_step(gbght_run* run, double dt);
+int gbght_adjoint_add_observable(gbght_run* run, int which, double weight);
+int gbght_adjoint_forcing_gradient(gbght_run* run, double out[2], int reset);
+int gbght_adjoint_clear(gbght_run* run);
+int gbght_snapshot_save(gbght_run* run, int slot);
+int gbght_snapshot_load(gbght_run* run, int slot);
 
 /* Wait for all work queued on the run's stream. */
 int gbght_synchronize(gbght_run* run);

@@ -1,0 +1,196 @@
+"""The discrete adjoint of the field step against the oracle's (oracle.step_adjoint, pinned there by
+central finite differences and the dot-product identity), through the C ABI.
+
+CPU tests run the host-check build (the same CTA bodies on one CPU thread); GPU tests run the CUDA
+library. The adjoint lives on the retained 2/3 ball, so the oracle's Jᵀλ is compared on the ball.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import gbght
+from gbght import adjoint as AD
+from gbght import seed as S
+from oracle import gbght_oracle as O
+from pairs import oracle_forcing, rel_l2
+
+
+def _rand_ball(dom, rng, shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) * dom.mask
+
+
+def adjoint_pair(library, N, *, forcing=None, scalar_forcing=None, G=(0.0, 0.0, 0.0), scalar=True,
+                 scheme="IFLowStorageRK4", precision="fp64", dt=0.01, viscosity=0.01, seed=5):
+    """(library Jᵀλ, oracle Jᵀλ on the ball, run, setup) for one step at a seeded state."""
+    uh = S.seed_velocity(N, 0.5, seed=0)
+    ph = S.seed_scalar(N, 0.5, seed=1) if scalar else None
+    dom = O.Domain(N)
+    rng = np.random.default_rng(seed)
+    lam = _rand_ball(dom, rng, (3,) + dom.shape_spectral)
+    lamp = _rand_ball(dom, rng, dom.shape_spectral) if scalar else None
+    setup = gbght.Setup(grid_points_per_axis=N, viscosity=viscosity, scalar=scalar,
+                        velocity_forcing=forcing or gbght.NoForcing(),
+                        scalar_forcing=scalar_forcing or gbght.NoForcing(), mean_gradient=G, scheme=scheme,
+                        precision=precision)
+    run = gbght.simulation(setup, uh, ph, library=library)
+    run.adjoint_create(2)
+    run.adjoint_import(lam, lamp)
+    run.adjoint_step(dt)
+    lib = run.adjoint_export()
+    cond = O.Conditions(viscosity=viscosity, scalar=scalar, velocity_forcing=oracle_forcing(forcing),
+                        scalar_forcing=oracle_forcing(scalar_forcing), mean_gradient=G)
+    osch = {"IFLowStorageRK4": "rk4", "IFLowStorageRK3": "rk3"}[scheme]
+    if scalar:
+        ou, op = O.step_adjoint(dom, cond, uh, lam, dt, osch, ph, lamp)
+        ora = (ou * dom.mask, op * dom.mask)
+    else:
+        ora = (O.step_adjoint(dom, cond, uh, lam, dt, osch) * dom.mask, None)
+    return lib, ora, run, (uh, ph, lam, lamp, dom, cond, osch)
+
+
+CASES = {
+    "unforced_G": dict(G=(1.0, 0.5, 0.0)),
+    "constant_power": dict(forcing=gbght.ConstantPower(0.1), G=(1.0, 0.0, 0.0)),
+    "both_fields": dict(forcing=gbght.Linear(0.3), scalar_forcing=gbght.ConstantPower(0.05, 1, 3), G=(0.0, 1.0, 0.0)),
+    "rk3_velocity_only": dict(forcing=gbght.ConstantPower(0.2), scalar=False, scheme="IFLowStorageRK3"),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES), ids=list(CASES))
+def test_adjoint_step_matches_the_oracle_hostcheck(hostcheck_library, case):
+    (lu, lp), (ou, op), run, _ = adjoint_pair(hostcheck_library, 12, **CASES[case])
+    assert rel_l2(lu, ou) <= 1e-13
+    if op is not None:
+        assert rel_l2(lp, op) <= 1e-13
+    uh = S.seed_velocity(12, 0.5, seed=0)
+    ue, _ = run.export_state()
+    assert np.array_equal(ue, uh)   # the state is left as it was
+
+
+def _spectral_dot(dom, a, b):
+    return O.spectral_dot(dom, a, b)
+
+
+def test_forcing_gradient_matches_finite_differences_hostcheck(hostcheck_library):
+    # d⟨λ, F(q; ε)⟩/dε for both fields' ConstantPower rates, against central differences of the oracle
+    N, dt = 12, 0.01
+    vf, sf = gbght.ConstantPower(0.1), gbght.ConstantPower(0.05)
+    _, _, run, (uh, ph, lam, lamp, dom, cond, osch) = adjoint_pair(hostcheck_library, N, forcing=vf, scalar_forcing=sf,
+                                                                   G=(1.0, 0.0, 0.0), dt=dt)
+    gu, gp = run.forcing_gradient()
+    h = 1e-6
+
+    def pairing(eu, ep):
+        c = O.Conditions(viscosity=0.01, velocity_forcing=O.ConstantPower(eu), scalar_forcing=O.ConstantPower(ep),
+                         mean_gradient=(1.0, 0.0, 0.0))
+        st = O.step(dom, c, O.State(uh.copy(), ph.copy()), dt, osch)
+        return _spectral_dot(dom, lam, st.uh) + _spectral_dot(dom, lamp, st.phih)
+    fu = (pairing(0.1 + h, 0.05) - pairing(0.1 - h, 0.05)) / (2 * h)
+    fp = (pairing(0.1, 0.05 + h) - pairing(0.1, 0.05 - h)) / (2 * h)
+    assert gu == pytest.approx(fu, rel=1e-6)
+    assert gp == pytest.approx(fp, rel=1e-6)
+
+
+def test_adjoint_refusals_hostcheck(hostcheck_library):
+    run = gbght.Run(gbght.Setup(grid_points_per_axis=12, scheme="IFHeun"), library=hostcheck_library)
+    with pytest.raises(ValueError, match="low-storage"):
+        run.adjoint_create(2)
+    run = gbght.Run(gbght.Setup(grid_points_per_axis=12, velocity_forcing=gbght.VarianceRescaling(0.5, "band")),
+                    library=hostcheck_library)
+    with pytest.raises(ValueError, match="ConstantPower"):
+        run.adjoint_create(2)
+    run = gbght.Run(gbght.Setup(grid_points_per_axis=12), library=hostcheck_library)
+    with pytest.raises(gbght.DeviceError, match="not set up"):
+        run.adjoint_step(0.01)
+    run.adjoint_create(1)
+    dom = O.Domain(12)
+    bad = np.ones((3,) + dom.shape_spectral, np.complex128)
+    with pytest.raises(ValueError, match="outside the retained"):
+        run.adjoint_import(bad, np.zeros(dom.shape_spectral, np.complex128))
+    lu, _ = run.adjoint_export()
+    assert not lu.any()
+    with pytest.raises(ValueError, match="snapshot"):
+        run.snapshot_save(3)
+
+
+def test_snapshots_restore_the_state_hostcheck(hostcheck_library):
+    N = 12
+    setup = gbght.Setup(grid_points_per_axis=N, velocity_forcing=gbght.ConstantPower(0.1))
+    run = gbght.simulation(setup, S.seed_velocity(N, 0.5, seed=0), S.seed_scalar(N, 0.5, seed=1),
+                           library=hostcheck_library)
+    run.adjoint_create(2)
+    u0, p0 = run.export_state()
+    run.snapshot_save(1)
+    run.advance(0.01)
+    run.snapshot_load(1)
+    with pytest.raises(gbght.ScheduleError):
+        run.step(0.01)   # the deposit is stale after a load
+    run.deposit()
+    u1, p1 = run.export_state()
+    assert np.array_equal(u0, u1) and np.array_equal(p0, p1)
+
+
+def oracle_window_gradient(dom, cond, uh, ph, dts, n0, n1):
+    """∂L/∂q_0 of L = mean over n0..n1 of ⟨φ²⟩ by the oracle: every state stored, the adjoints
+    chained backwards."""
+    states = [O.State(uh.copy(), ph.copy())]
+    for d in dts:
+        states.append(O.step(dom, cond, states[-1], d, "rk4"))
+    N6 = float(dom.N) ** 6
+    w = 1.0 / (n1 - n0 + 1)
+    lu = np.zeros_like(uh)
+    lp = np.zeros_like(ph)
+    for k in range(len(dts), -1, -1):
+        if k < len(dts):
+            lu, lp = O.step_adjoint(dom, cond, states[k].uh, lu, dts[k], "rk4", states[k].phih, lp)
+        if n0 <= k <= n1:
+            lp = lp + w * 2.0 * states[k].phih / N6
+    return lu * dom.mask, lp * dom.mask
+
+
+def test_checkpointed_sweep_matches_the_oracle_hostcheck(hostcheck_library):
+    # 7 uneven steps, a window loss over steps 3..7, two snapshot slots: recomputation from slots
+    N = 12
+    uh, ph = S.seed_velocity(N, 0.5, seed=0), S.seed_scalar(N, 0.5, seed=1)
+    dts = [0.01, 0.012, 0.009, 0.011, 0.01, 0.008, 0.013]
+    setup = gbght.Setup(grid_points_per_axis=N, velocity_forcing=gbght.ConstantPower(0.1), mean_gradient=(1.0, 0.0, 0.0))
+    run = gbght.simulation(setup, uh, ph, library=hostcheck_library)
+    run.adjoint_create(2)
+    (lu, lp), _, sweep = AD.gradient(run, dts, AD.scalar_variance_window(3, 7), snapshots=2)
+    dom = O.Domain(N)
+    cond = O.Conditions(viscosity=0.01, velocity_forcing=O.ConstantPower(0.1), mean_gradient=(1.0, 0.0, 0.0))
+    ou, op = oracle_window_gradient(dom, cond, uh, ph, dts, 3, 7)
+    assert rel_l2(lu, ou) <= 1e-12 and rel_l2(lp, op) <= 1e-12
+    assert sweep.adjoint_steps == 7 and sweep.peak <= 2
+    ue, pe = run.export_state()
+    assert np.array_equal(ue, uh) and np.array_equal(pe, ph)
+
+
+# ------------------------------------------------------------------------------------------------
+# GPU
+# ------------------------------------------------------------------------------------------------
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", list(CASES), ids=list(CASES))
+@pytest.mark.parametrize("N,precision,tol", [(64, "fp64", 1e-12), (64, "fp32_mixed", 1e-5), (128, "fp64", 1e-12)])
+def test_adjoint_step_matches_the_oracle(cuda_library, case, N, precision, tol):
+    (lu, lp), (ou, op), _, _ = adjoint_pair(cuda_library, N, precision=precision, **CASES[case])
+    assert rel_l2(lu, ou) <= tol
+    if op is not None:
+        assert rel_l2(lp, op) <= tol
+
+
+@pytest.mark.gpu
+def test_dot_product_identity_against_the_oracle_tangent(cuda_library):
+    # ⟨J v, w⟩ = ⟨v, Jᵀ w⟩ with J v the oracle's tangent-linear step and Jᵀ w the GPU adjoint
+    N, dt = 64, 0.01
+    vf = gbght.ConstantPower(0.1)
+    (lu, lp), _, _, (uh, ph, lam, lamp, dom, cond, osch) = adjoint_pair(cuda_library, N, forcing=vf,
+                                                                        G=(1.0, 0.0, 0.0), dt=dt)
+    rng = np.random.default_rng(11)
+    vu, vp = _rand_ball(dom, rng, (3,) + dom.shape_spectral), _rand_ball(dom, rng, dom.shape_spectral)
+    vu = O.leray(dom, vu)
+    _, _, ju, jp = O.step_tangent(dom, cond, uh, vu, dt, osch, ph, vp)
+    left = O.spectral_dot(dom, ju, lam) + O.spectral_dot(dom, jp, lamp)
+    right = O.spectral_dot(dom, vu, lu) + O.spectral_dot(dom, vp, lp)
+    assert right == pytest.approx(left, rel=1e-12)
