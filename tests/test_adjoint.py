@@ -194,3 +194,57 @@ def test_dot_product_identity_against_the_oracle_tangent(cuda_library):
     left = O.spectral_dot(dom, ju, lam) + O.spectral_dot(dom, jp, lamp)
     right = O.spectral_dot(dom, vu, lu) + O.spectral_dot(dom, vp, lp)
     assert right == pytest.approx(left, rel=1e-12)
+
+
+def _c4_forward_loss(library, setup, uh, ph, dts, n0, n1):
+    run = gbght.simulation(setup, uh, ph, library=library)
+    total = 0.0
+    for k in range(len(dts) + 1):
+        if k > 0:
+            run.step(dts[k - 1])
+            run.deposit()
+        if n0 <= k <= n1:
+            total += run.observables()["scalar_variance"]
+    run.close()
+    return total / (n1 - n0 + 1)
+
+
+@pytest.mark.gpu
+def test_c4_gradient_against_central_differences(cuda_library):
+    # 128³ forced velocity + scalar, ν = ϰ = 6e-3, ConstantPower ε = 0.1 on shells 1–2, G = 1 along x,
+    # IF-RK4; loss the scalar variance averaged over steps 100..200 (Δt held at the CFL sequence
+    # of the unperturbed run); gradients with respect to ε and the initial velocity, by the
+    # checkpointed reverse sweep with 16 stored states, against central differences (h = 1e-6)
+    # of the FP64 forward along 8 seeded directions
+    N, nsteps, n0 = 128, 200, 100
+    uh, ph = S.seed_velocity(N, 0.5, seed=0), S.seed_scalar(N, 0.5, seed=1)
+    eps = 0.1
+
+    def setup(e):
+        return gbght.Setup(grid_points_per_axis=N, viscosity=6e-3, velocity_forcing=gbght.ConstantPower(e),
+                           mean_gradient=(1.0, 0.0, 0.0), cfl=0.5)
+    ref = gbght.simulation(setup(eps), uh, ph, library=cuda_library)
+    dts = [ref.advance(None) for _ in range(nsteps)]
+    ref.close()
+    run = gbght.simulation(setup(eps), uh, ph, library=cuda_library)
+    run.adjoint_create(16)
+    (lu, lp), (geps, _), sweep = AD.gradient(run, dts, AD.scalar_variance_window(n0, nsteps), snapshots=16)
+    assert sweep.peak <= 16 and sweep.adjoint_steps == nsteps
+    h = 1e-6
+    fd = (_c4_forward_loss(cuda_library, setup(eps + h), uh, ph, dts, n0, nsteps)
+          - _c4_forward_loss(cuda_library, setup(eps - h), uh, ph, dts, n0, nsteps)) / (2 * h)
+    errs = [abs(geps - fd) / abs(fd)]
+    dom = O.Domain(N)
+    rng = np.random.default_rng(2024)
+    for _ in range(8):
+        v = O.leray(dom, _rand_ball(dom, rng, (3,) + dom.shape_spectral))
+        v *= np.linalg.norm(uh) / np.linalg.norm(v)
+        # a Hermitian kx = 0 plane keeps the perturbed state a real field
+        v = O.reality_projection(dom, v)
+        dL = (_c4_forward_loss(cuda_library, setup(eps), uh + h * v, ph, dts, n0, nsteps)
+              - _c4_forward_loss(cuda_library, setup(eps), uh - h * v, ph, dts, n0, nsteps)) / (2 * h)
+        ad = O.spectral_dot(dom, lu, v)
+        errs.append(abs(ad - dL) / abs(dL))
+    print(f"C4 128^3: dL/deps adjoint {geps:.10e} fd {fd:.10e}; relative errors {['%.1e' % e for e in errs]}; "
+          f"{sweep.forward_steps} recomputed steps, {sweep.peak} slots")
+    assert max(errs) <= 1e-6
