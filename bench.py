@@ -276,6 +276,137 @@ def e2e_run(args, precision, device, inputs, K):
     return K / el, h2d / K, d2h / K
 
 
+def adjoint_cost(args, device, inputs, reps=3):
+    """The discrete adjoint's cost on the workload (FP64, no tracers): CUDA-event time of one
+    gbght_adjoint_step (the step's stages run again, then reversed) against one field step
+    (gbght_step + gbght_deposit), each the mean of `reps` after one untimed call."""
+    import gbght
+    N = args.grid
+    uh, ph, _ = inputs
+    setup = gbght.Setup(grid_points_per_axis=N, viscosity=WORKLOAD["viscosity"], schmidt=WORKLOAD["schmidt"],
+                        velocity_forcing=gbght.ConstantPower(WORKLOAD["injection_rate"], *WORKLOAD["shells"]),
+                        mean_gradient=WORKLOAD["G"], cfl=_cfl(args), scheme=args.scheme, device=device)
+    if args.scheme not in ("IFLowStorageRK4", "IFLowStorageRK3"):
+        return None
+    run = gbght.simulation(setup, uh, ph)
+    dt = run.cfl_timestep()
+    run.adjoint_create(0)
+    run.adjoint_import(uh, ph)
+
+    def timed(fn):
+        fn()
+        run.synchronize()
+        run.timer_start()
+        for _ in range(reps):
+            fn()
+        return run.timer_stop() / reps
+
+    def field_step():
+        run.step(dt)
+        run.deposit()
+    fwd = timed(field_step)
+    run.profile(True)
+    adj = timed(lambda: run.adjoint_step(dt))
+    prof = run.profile_read()
+    run.profile(False)
+    run.close()
+    return {"forward_field_step_ms": round(fwd, 3), "adjoint_step_ms": round(adj, 3),
+            "ratio": round(adj / fwd, 3), "form": "fp64", "grid": N,
+            "kernels_per_adjoint_step_ms": {k: round(v[1] / (reps + 1), 3) for k, v in prof.items() if v[0]}}
+
+
+def c1_statistics(device, steps=500, burn=100, window=100, batch=20, short=20):
+    """The 256³ forced configuration (ν = ϰ = 2.1e-3, ConstantPower ε = 0.1 on shells 1–2, G = 1,
+    CFL 0.5, 10⁵ tracers) in both forms on the GPU: the FP32-mixed form's relative L2 field error
+    against the FP64 form after `short` steps of the FP64 Δt sequence, and the long-time spectra
+    over `steps` steps, each form at its own CFL Δt, compared window by window (mean E(κ), E_φ(κ)
+    after `burn` steps, in windows of `window` steps, standard errors from batch means)."""
+    import gbght
+    N, M = 256, 100_000
+    uh, ph, X = make_inputs(N, M, seed_base=0)
+
+    def make(form):
+        setup = gbght.Setup(grid_points_per_axis=N, viscosity=2.1e-3, velocity_forcing=gbght.ConstantPower(0.1),
+                            mean_gradient=(1.0, 0.0, 0.0), tracers=M, cfl=0.5, precision=form, device=device)
+        return gbght.simulation(setup, uh, ph, X)
+    a, b = make("fp64"), make("fp32_mixed")
+    for _ in range(short):
+        b.advance(a.advance(None))
+    ua, pa = a.export_state()
+    ub, pb = b.export_state()
+    out = {"short_steps": short,
+           "field_rel_l2_u": float(np.linalg.norm(ub - ua) / np.linalg.norm(ua)),
+           "field_rel_l2_phi": float(np.linalg.norm(pb - pa) / np.linalg.norm(pa))}
+    a.close()
+    b.close()
+    wins = {}
+    for form in ("fp64", "fp32_mixed"):
+        run = make(form)
+        Es, Ps = [], []
+        for k in range(steps):
+            run.advance(None)
+            if k >= burn:
+                Es.append(run.energy_spectrum())
+                Ps.append(run.scalar_spectrum())
+        run.close()
+        res = []
+        for w0 in range(0, len(Es) - window + 1, window):
+            pair = []
+            for series in (np.array(Es[w0:w0 + window]), np.array(Ps[w0:w0 + window])):
+                bm = series.reshape(window // batch, batch, -1).mean(axis=1)
+                pair.append((series.mean(axis=0), bm.std(axis=0, ddof=1) / math.sqrt(bm.shape[0])))
+            res.append(pair)
+        wins[form] = res
+    rel, z = [], []
+    for w64, w32 in zip(wins["fp64"], wins["fp32_mixed"]):
+        for (m64, s64), (m32, s32) in zip(w64, w32):
+            live = m64 > 1e-6 * m64.max()
+            d = np.abs(m32 - m64)[live]
+            rel.append(float(np.max(d / m64[live])))
+            z.append(float(np.max(d / np.hypot(s64, s32)[live].clip(min=1e-300))))
+    out.update({"long_steps": steps, "windows": len(wins["fp64"]), "window_steps": window,
+                "spectrum_window_max_rel_diff": max(rel[0::2]), "scalar_spectrum_window_max_rel_diff": max(rel[1::2]),
+                "max_diff_in_standard_errors": max(z)})
+    return out
+
+
+def ensemble_rate(device, steps=300, alone_steps=30):
+    """The batched ensemble: 96 FP32-mixed members, 32 each of 32³, 48³ and 64³, ν drawn from
+    [0.005, 0.02] per member, ConstantPower ε = 0.1, G = 1, IF-RK4, stepped together under one CUDA
+    graph (gbght_ensemble_step) for `steps` steps, against stepping them one by one."""
+    import gbght
+    from gbght import seed as S
+    rng = np.random.default_rng(7)
+    runs = []
+    for i, n in enumerate([32] * 32 + [48] * 32 + [64] * 32):
+        setup = gbght.Setup(grid_points_per_axis=n, viscosity=float(rng.uniform(0.005, 0.02)),
+                            velocity_forcing=gbght.ConstantPower(0.1), mean_gradient=(1.0, 0.0, 0.0),
+                            precision="fp32_mixed", device=device)
+        runs.append(gbght.simulation(setup, S.seed_velocity(n, 0.5, seed=100 + i), S.seed_scalar(n, 0.5, seed=300 + i)))
+    dt = 0.002
+    ens = gbght.Ensemble(runs)
+    ens.step(dt)
+    runs[0].synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ens.step(dt)
+    graph = len(runs) * steps / (time.perf_counter() - t0)
+    ens.close()
+    for r in runs:
+        r.advance(dt)
+    t0 = time.perf_counter()
+    for _ in range(alone_steps):
+        for r in runs:
+            r.step(dt)
+            r.deposit()
+    alone = len(runs) * alone_steps / (time.perf_counter() - t0)
+    for r in runs:
+        r.close()
+    return {"members": len(runs), "grids": "32x32^3 + 32x48^3 + 32x64^3", "form": "fp32_mixed", "steps": steps,
+            "member_steps_per_s_graph": round(graph, 1), "member_steps_per_s_one_by_one": round(alone, 1),
+            "speedup": round(graph / alone, 3), "timing": "host wall clock around synchronising calls"}
+
+
 def cpu_steps(N, M, budget_s, min_steps=1, max_steps=None):
     """Whole iterations of the oracle's run layer (`advance!`: the IF-RK4 step, the deposit, the
     Heun push and particle deposit, the guards) on the workload at N³ with M tracers, NumPy +
@@ -387,6 +518,10 @@ def ours(args):
                                             "clocks": m["clocks"],
                                             "spectrum_rel_err_after_K_steps": float(np.max(np.abs(E32[live] - E64[live]) / E64[live])),
                                             "scalar_spectrum_rel_err_after_K_steps": float(np.max(np.abs(P32[livep] - P64[livep]) / P64[livep]))}}
+        if ws == 1 and not args.no_extras:
+            line["adjoint"] = adjoint_cost(args, device, inputs)
+            line.setdefault("forms", {}).setdefault("fp32_mixed", {})["c1_256cubed"] = c1_statistics(device)
+            line["forms"]["ensemble"] = ensemble_rate(device)
         if ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_line(args, budget_s=60.0)
         print(json.dumps(line), flush=True)
@@ -430,6 +565,8 @@ def main():
                     help="the field integration scheme (the metric is quoted on IFLowStorageRK4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (quick kernel timing)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the adjoint, 256^3 precision and ensemble legs (rank 0 at N=1 runs them)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

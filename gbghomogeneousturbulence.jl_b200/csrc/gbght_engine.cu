@@ -1000,7 +1000,8 @@ class EngineImpl final : public Engine {
   size_t smem_y() const { return size_t(N) * TLY * sizeof(Cplx<T>) + kBarBytes; }
   size_t smem_x() const {
     return size_t(N) * XShape<T>::ACT_INV * sizeof(Cplx<T>) +
-           size_t(7) * XShape<T>::P * x_kxs(g_.K, int(sizeof(Cplx<T>))) * sizeof(Cplx<T>) + kBarBytes;
+           (XShape<T>::STAGED ? size_t(7) * XShape<T>::P * x_kxs(g_.K, int(sizeof(Cplx<T>))) * sizeof(Cplx<T>) : 0) +
+           kBarBytes;
   }
   size_t smem_xv() const {
     return size_t(N) * XShape<T>::ACT_V * sizeof(Cplx<T>) + size_t((NTXV + 1) & ~1) * sizeof(double) +

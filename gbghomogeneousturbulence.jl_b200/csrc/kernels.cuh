@@ -78,12 +78,13 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_y_forward(const 
 }
 
 template <class T, int N, int NT>
-__global__ void __launch_bounds__(NT, 2) k_x_products(Geometry g, Cplx<T>* B, int has_scalar, int KXS,
-                                                      const Cplx<T>* tw, unsigned int* status) {
+__global__ void __launch_bounds__(NT, XShape<T>::STAGED ? 2 : 3) k_x_products(Geometry g, Cplx<T>* B, int has_scalar,
+                                                                             int KXS, const Cplx<T>* tw,
+                                                                             unsigned int* status) {
   CTA_CTX;
   Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
   Cplx<T>* stg = sm + N * XShape<T>::ACT_INV;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(stg + 7 * XShape<T>::P * KXS);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(stg + (XShape<T>::STAGED ? 7 * XShape<T>::P * KXS : 0));
   init_bars(bar, 1);
   body_x_products<T, N, NT>(c, sm, stg, KXS, bar, int(gridDim.x), g, B, has_scalar, tw, status);
 }

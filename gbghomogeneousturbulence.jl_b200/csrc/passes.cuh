@@ -134,6 +134,10 @@ template <class T> struct XShape {
   static constexpr int ACT_INV = 3 * P + P / 2;
   static constexpr int ACT_FWD = 3 * P;
   static constexpr int NW = sizeof(Cplx<T>) == 16 ? 7 : 8;   // warps of the x pass (≥ 1 turnaround item per thread)
+  // FP64 stages a tile's spectra in shared memory by bulk copies (overlapping the next tile's load
+  // with the current tile's transforms); FP32 reads them in the first inverse stage straight from
+  // global memory, which frees the staging's shared memory for a third CTA per SM.
+  static constexpr bool STAGED = sizeof(Cplx<T>) == 16;
   static constexpr int PV = TL / 2;                // points per tile (deposit pass)
   static constexpr int ACT_V = PV + PV / 2;
 };
@@ -163,6 +167,12 @@ struct XStagedSource {
   const Cplx<T>* stg;
   int KXS, has_scalar;
   T sc;
+  const Cplx<T>* B = nullptr;   // unstaged (XShape<T>::STAGED false): the tile's rows in B
+  int z = 0, y0 = 0;
+  GBGHT_HD Cplx<T> row(int r, int m) const {
+    if constexpr (XShape<T>::STAGED) return stg[r * KXS + m];
+    else return B[idxB(g, r / P, z, y0 + r % P, m)];
+  }
   GBGHT_HD Cplx<T> load(int e, int l) const {
     const int K = g.K;
     if (e > K && e < N - K) return czero<T>();
@@ -178,7 +188,7 @@ struct XStagedSource {
       rb = ra + 1;
     }
     const int m = e <= K ? e : N - e;
-    const Cplx<T> a = stg[ra * KXS + m], b = stg[rb * KXS + m];
+    const Cplx<T> a = row(ra, m), b = row(rb, m);
     if (e == 0) return cmk<T>(a.x * sc, b.x * sc);
     if (e <= K) return cmk<T>((a.x - b.y) * sc, (a.y + b.x) * sc);
     return cmk<T>((a.x + b.y) * sc, (b.x - a.y) * sc);
@@ -187,7 +197,7 @@ struct XStagedSource {
 
 // Staging of one x tile: the rows B[c][z][y0+p][0..KXS) of comps c < nin, as untiled bulk copies
 // completing on `bar` (device), or plain copies (host-check build).
-template <class T, int P>
+template <class T, int P, bool ON = true>
 struct XStaging {
   const Geometry& g;
   const Cplx<T>* B;
@@ -196,6 +206,7 @@ struct XStaging {
   uint64_t* bar;
   unsigned int* status;
   GBGHT_HD void issue(const Cta& c, int z, int y0) const {
+    if constexpr (!ON) return;
 #ifdef __CUDA_ARCH__
     if (c.tid == 0) {
       const uint32_t row = uint32_t(KXS * sizeof(Cplx<T>));
@@ -211,6 +222,7 @@ struct XStaging {
 #endif
   }
   GBGHT_HD void wait(uint32_t phase) const {
+    if constexpr (!ON) return;
 #ifdef __CUDA_ARCH__
     mbar_wait(bar, phase, status);
 #else
@@ -218,6 +230,7 @@ struct XStaging {
 #endif
   }
 };
+template <class T> using XProductStaging = XStaging<T, XShape<T>::P, XShape<T>::STAGED>;
 
 // A host-device function kept out of line on the device: one copy of a body that a kernel calls
 // several times, to keep the kernel's code within the instruction cache.
@@ -334,13 +347,16 @@ GBGHT_HD void x_turnaround(const Cta& c, Cplx<T>* sm, const Cplx<T>* GBGHT_RESTR
 // staging is free and the next tile's copies are issued), the turnaround (last inverse stage,
 // products, first forward stage), the rest of the forward transform, and the unpack into B.
 template <class T, int N, int NT>
-GBGHT_HD void x_tile(const Cta& c, Cplx<T>* sm, const XStaging<T, XShape<T>::P>& stage,
-                                    const XStagedSource<T, N, XShape<T>::P>& src, const Geometry& g,
+GBGHT_HD void x_tile(const Cta& c, Cplx<T>* sm, const XProductStaging<T>& stage,
+                                    const XStagedSource<T, N, XShape<T>::P>& src0, const Geometry& g,
                                     Cplx<T>* GBGHT_RESTRICT B, int nout, int z, int y0, int next_z, int next_y0,
                                     const Cplx<T>* GBGHT_RESTRICT tw) {
   using X = XShape<T>;
   constexpr int P = X::P, NW = X::NW;
   const int KX1 = g.K + 1;
+  XStagedSource<T, N, P> src = src0;   // the tile's position, for the unstaged source
+  src.z = z;
+  src.y0 = y0;
   const auto lines = [&](int l) { return sm + l * N; };
   const auto from_stg = [&](int l) { return LineOfSource<XStagedSource<T, N, P>>{src, l}; };
   const auto in_smem = [&](int l) { return LineBuf<T>{sm + l * N}; };
@@ -407,7 +423,7 @@ GBGHT_HD void x_tile(const Cta& c, Cplx<T>* sm, const XStaging<T, XShape<T>::P>&
 // copied into the staging rows.
 constexpr int XT = 2;
 template <class T, int N, int NT, int I>
-GBGHT_HD void x_tile_chain(const Cta& c, Cplx<T>* sm, const XStaging<T, XShape<T>::P>& stage,
+GBGHT_HD void x_tile_chain(const Cta& c, Cplx<T>* sm, const XProductStaging<T>& stage,
                            const XStagedSource<T, N, XShape<T>::P>& src, const Geometry& g, Cplx<T>* B, int nout,
                            int grid, int ntiles, const Cplx<T>* tw) {
   if constexpr (I < XT) {
@@ -432,8 +448,9 @@ GBGHT_HD void body_x_products(const Cta& c, Cplx<T>* sm, Cplx<T>* stg, int KXS, 
   constexpr int P = X::P;
   const int nin = has_scalar ? 7 : 6, nout = has_scalar ? 6 : 3;
   const int tiles_y = N / P, ntiles = tiles_y * N;
-  const XStaging<T, P> stage{g, B, stg, KXS, nin, bar, status};
-  const XStagedSource<T, N, P> src{g, stg, KXS, has_scalar, T(g.inv_norm)};
+  const XProductStaging<T> stage{g, B, stg, KXS, nin, bar, status};
+  XStagedSource<T, N, P> src{g, stg, KXS, has_scalar, T(g.inv_norm)};
+  src.B = B;
   // XT tiles per CTA, written out by template recursion rather than looped (a loop around the
   // tile makes the compiler keep the tile's index arithmetic live across iterations, and the
   // kernel spills): tile bx + i·grid, with the spectra of tile i + 1 copied in while tile i is
