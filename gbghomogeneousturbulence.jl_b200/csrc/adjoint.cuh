@@ -22,6 +22,7 @@
 #pragma once
 
 #include "passes.cuh"
+#include "tracers.cuh"
 
 namespace gbght {
 
@@ -197,6 +198,7 @@ GBGHT_HD void body_x_adjoint(const Cta& c, Cplx<T>* sm, const Geometry& g, const
 // Shared memory: the FFT tile W (N·TL) and the retained rows R ([6][NY2][TL]).
 // ================================================================================================
 struct AdjArgs {
+  int add_only;         // the launch adds the z-forward of A slots 0..2 to λ's velocity (nothing else)
   int combine;          // the launch ends reverse stage i
   int prologue;         // the launch starts reverse stage j
   int has_scalar;
@@ -277,6 +279,20 @@ GBGHT_HD void body_adj_z(const Cta& c, Cplx<T>* W, Cplx<T>* R, const Geometry& g
     const ZRetainedSink<T, N, TL> dst{g, R, comp, add};
     tile_fft_io<T, N, TL, NT, -1>(c, W, tw, src, dst);
   };
+  if (a.add_only) {   // λ_u += the z-forward of A slots 0..2 on the ball (the tracers' part)
+    for (int k = 0; k < 3; ++k) zfwd(k, k, false);
+    for (int idx = c.tid; idx < NY2 * TL; idx += NT) {
+      const int q = idx / TL, l = idx % TL, kx = kx0 + l;
+      const double kxd = s * double(kx), kzd = s * double(q_to_m(q, g.K, NY2));
+      const double k2 = (kxd * kxd + ky * ky) + kzd * kzd;
+      if (!(kx <= g.K && k2 <= g.cut2)) continue;
+      for (int cc = 0; cc < 3; ++cc) {
+        const size_t at = idxS(g, cc, qy, q, kx);
+        L[at] = L[at] + Rat(cc, q, l);
+      }
+    }
+    return;
+  }
   if (a.combine) {
     // ω̄ (slots 3..5), its curl in place, then + ū (slots 0..2); φ̄ (slot 6) into component 3
     for (int k = 0; k < 3; ++k) zfwd(3 + k, k, false);
@@ -415,6 +431,163 @@ GBGHT_HD void adj_add_mode(size_t i, size_t nS, int nc, Cplx<T>* L, const Cplx<T
   for (int cc = 0; cc < nc; ++cc) {
     const double w = cc < 3 ? wu : wp;
     if (w != 0.0) L[cc * nS + i] = L[cc * nS + i] + scale(S[cc * nS + i], T(w));
+  }
+}
+
+// ================================================================================================
+// The tracers' adjoint (src/ParticlePropagator.jl:288-315,378-386), Heun with Catmull–Rom. The wrap
+// is locally the identity and a cell index locally constant, so the gather f(X) = Σ w(X)·u at the
+// taps has the adjoint λ ↦ (scatter of w·λ onto the taps, Σ ∂w/∂X·(u·λ) per position).
+//   particle deposit f = u(X):                 λ_u += Wᵀλ_f, λ_X += ∂_X(u·λ_f), λ_f ← 0
+//   Heun push and closing deposit at step h:   X* = X + b₀f₀, f* = u(X*), X' = X* + β*f* + (β₀ − b₀)f₀,
+//                                              f' = u(X'); given (λ_X', λ_f'), λ_u collects both
+//                                              gathers' scatters and (λ_X, λ_f₀) replace (λ_X', λ_f').
+// λ_u is a physical field [3][N³] in FP64, added to by atomics; its rfft/N³ on the ball then joins λ.
+// ================================================================================================
+// d/dt of the Catmull–Rom weights.
+GBGHT_HD void catmull_rom_slopes(double t, double s[4]) {
+  s[0] = ((-3.0 * t + 4.0) * t - 1.0) * 0.5;
+  s[1] = (9.0 * t - 10.0) * t * 0.5;
+  s[2] = ((-9.0 * t + 8.0) * t + 1.0) * 0.5;
+  s[3] = (3.0 * t - 2.0) * t * 0.5;
+}
+
+GBGHT_HD void add_to(double* p, double v) {
+#ifdef __CUDA_ARCH__
+  atomicAdd(p, v);
+#else
+  *p += v;
+#endif
+}
+
+// The gather's adjoint at (x, y, z) for values λ[3]: w·λ scattered into lu ([3][N³]); returns the
+// positions' part in lX[3] (per unit length).
+template <class T>
+GBGHT_HD void gather3_adjoint(const T* GBGHT_RESTRICT u, double* lu, int N, double dx, double x, double y, double z,
+                              const double lam[3], double lX[3]) {
+  int ix, iy, iz;
+  double tx, ty, tz;
+  cell_fraction(x, dx, N, ix, tx);
+  cell_fraction(y, dx, N, iy, ty);
+  cell_fraction(z, dx, N, iz, tz);
+  double wx[4], wy[4], wz[4], sx[4], sy[4], sz[4];
+  catmull_rom(tx, wx);
+  catmull_rom(ty, wy);
+  catmull_rom(tz, wz);
+  catmull_rom_slopes(tx, sx);
+  catmull_rom_slopes(ty, sy);
+  catmull_rom_slopes(tz, sz);
+  const size_t comp = size_t(N) * N * N;
+  lX[0] = lX[1] = lX[2] = 0.0;
+  for (int cz = 0; cz < 4; ++cz) {
+    const int zz = (iz + cz - 1 + N) % N;
+    for (int cy = 0; cy < 4; ++cy) {
+      const int yy = (iy + cy - 1 + N) % N;
+      for (int cx = 0; cx < 4; ++cx) {
+        const int xx = (ix + cx - 1 + N) % N;
+        const size_t at = (size_t(zz) * N + yy) * N + xx;
+        double fl = 0.0;
+        for (int c = 0; c < 3; ++c) fl += double(ldg(u + c * comp + at)) * lam[c];
+        lX[0] += sx[cx] * wy[cy] * wz[cz] * fl;
+        lX[1] += wx[cx] * sy[cy] * wz[cz] * fl;
+        lX[2] += wx[cx] * wy[cy] * sz[cz] * fl;
+        const double w = wz[cz] * wy[cy] * wx[cx];
+        for (int c = 0; c < 3; ++c) add_to(lu + c * comp + at, w * lam[c]);
+      }
+    }
+  }
+  for (int c = 0; c < 3; ++c) lX[c] /= dx;
+}
+
+// One tracer p. `push` = 1: the Heun push and closing deposit with the forward's own weights b₀, β*
+// and β_m = β₀ − b₀ (adams_step_weights for one sample: h, h/2, −h/2 as the quadrature rounds them),
+// so X* and X' are the forward's to the bit; X and f₀ are the positions and the newest sample before
+// the push. `push` = 0: the particle deposit alone at X. lX, lf: the cotangents [3][M], replaced.
+template <class T>
+GBGHT_HD void tracer_adjoint_one(int64_t p, int64_t M, const T* GBGHT_RESTRICT u, double* lu, int N, double L,
+                                 const double* GBGHT_RESTRICT X, const double* GBGHT_RESTRICT f0, double* lX,
+                                 double* lf, int push, double b0, double beta_star, double beta_m) {
+  const double dx = div_rn(L, double(N));
+  double x[3], lXn[3], lfn[3], g[3];
+  for (int c = 0; c < 3; ++c) {
+    x[c] = X[c * M + p];
+    lXn[c] = lX[c * M + p];
+    lfn[c] = lf[c * M + p];
+  }
+  if (!push) {
+    gather3_adjoint<T>(u, lu, N, dx, x[0], x[1], x[2], lfn, g);
+    for (int c = 0; c < 3; ++c) {
+      lX[c * M + p] = lXn[c] + g[c];
+      lf[c * M + p] = 0.0;
+    }
+    return;
+  }
+  double f[3], xs[3], fs[3], xn[3];
+  for (int c = 0; c < 3; ++c) {
+    f[c] = f0[c * M + p];
+    xs[c] = wrap_periodic(add_rn(x[c], mul_rn(b0, f[c])), L);
+  }
+  gather3(u, N, dx, xs[0], xs[1], xs[2], fs);
+  for (int c = 0; c < 3; ++c)
+    xn[c] = wrap_periodic(add_rn(xs[c], add_rn(mul_rn(beta_star, fs[c]), mul_rn(beta_m, f[c]))), L);
+  gather3_adjoint<T>(u, lu, N, dx, xn[0], xn[1], xn[2], lfn, g);
+  double lXt[3], lfs[3], lf0[3];
+  for (int c = 0; c < 3; ++c) {
+    lXt[c] = lXn[c] + g[c];
+    lfs[c] = beta_star * lXt[c];
+    lf0[c] = beta_m * lXt[c];
+  }
+  gather3_adjoint<T>(u, lu, N, dx, xs[0], xs[1], xs[2], lfs, g);
+  for (int c = 0; c < 3; ++c) {
+    const double lxs = lXt[c] + g[c];
+    lX[c * M + p] = lxs;
+    lf[c * M + p] = lf0[c] + b0 * lxs;
+  }
+}
+
+// The r2c of one pair of physical lines of λ_u (component c, rows y and y + 1 of plane z) into B
+// slot c: line pair `pair` of the [3][N][N/2] pairs, scaled by 1/N³; columns past K get zeros.
+template <class T, int N>
+struct PhysPairSource {
+  static constexpr bool kExternal = true;
+  const double* lu;
+  size_t base;   // element (c, z, y, 0)
+  GBGHT_HD Cplx<T> load(int e) const { return cmk<T>(T(lu[base + e]), T(lu[base + N + e])); }
+};
+template <class T, int N, int NW, int NT>
+GBGHT_HD void body_phys_forward(const Cta& c, Cplx<T>* sm, const Geometry& g, const double* GBGHT_RESTRICT lu,
+                                Cplx<T>* Ba, const Cplx<T>* GBGHT_RESTRICT tw) {
+  const int npairs = 3 * N * (N / 2);
+  const int pair0 = c.bx * NW;
+  const auto lines = [&](int l) { return sm + l * N; };
+  const auto src = [&](int l) {
+    const int pr = pair0 + l;
+    const int cc = pr / (N * (N / 2)), rem = pr % (N * (N / 2)), z = rem / (N / 2), y = 2 * (rem % (N / 2));
+    return PhysPairSource<T, N>{lu, ((size_t(cc) * N + z) * N + y) * N};
+  };
+  const auto in_smem = [&](int l) { return LineBuf<T>{sm + l * N}; };
+  const int nl = npairs - pair0 < NW ? npairs - pair0 : NW;
+  warp_fft_lines<T, N, NW, NT, -1>(c, nl, lines, src, in_smem, tw);
+  GBGHT_SYNC();
+  const T sc = T(g.inv_norm);
+  for (int t = c.tid; t < 32 * NW; t += NT) {
+    const int w = t >> 5, lane = t & 31;
+    if (w >= nl) continue;
+    const int pr = pair0 + w;
+    const int cc = pr / (N * (N / 2)), rem = pr % (N * (N / 2)), z = rem / (N / 2), y = 2 * (rem % (N / 2));
+    const Cplx<T>* Lp = sm + w * N;
+    for (int k = lane; k < g.KXP; k += 32) {
+      Cplx<T> a = czero<T>(), b = czero<T>();
+      if (k <= g.K) {
+        const Cplx<T> zk = Lp[lidx<T>(k)];
+        const Cplx<T> zc = conj(Lp[lidx<T>((N - k) % N)]);
+        const Cplx<T> sp = zk + zc, sd = zk - zc;
+        a = cmk<T>(sp.x * T(0.5) * sc, sp.y * T(0.5) * sc);
+        b = cmk<T>(sd.y * T(0.5) * sc, -sd.x * T(0.5) * sc);
+      }
+      Ba[idxB(g, cc, z, y, k)] = a;
+      Ba[idxB(g, cc, z, y + 1, k)] = b;
+    }
   }
 }
 

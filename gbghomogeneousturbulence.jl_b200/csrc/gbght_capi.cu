@@ -34,6 +34,9 @@ struct gbght_run {
   // the clock
   double time = 0.0;
   int64_t step = 0;
+  // the snapshot slots' clocks and newest-sample times (the device holds their states)
+  std::vector<double> snap_time, snap_sample_time;
+  std::vector<int64_t> snap_step;
 };
 
 namespace {
@@ -952,19 +955,77 @@ int gbght_adjoint_clear(gbght_run* r) {
 
 int gbght_snapshot_save(gbght_run* r, int slot) {
   if (check_run(r)) return GBGHT_ERR_ARGUMENT;
-  const char* e = r->eng->snapshot_save(slot);
+  const bool tr = r->cfg.tracers > 0;
+  if (tr && (r->trail_count == 0 || !r->sample_at_positions))
+    return fail(r, GBGHT_ERR_SCHEDULE, "a snapshot of a run with tracers needs the newest sample at the positions");
+  const char* e = r->eng->snapshot_save(slot, tr ? r->trail_newest : 0);
   if (e && std::strstr(e, "snapshot")) return fail(r, GBGHT_ERR_ARGUMENT, e);
-  return engine_call(r, e);
+  if (int rc = engine_call(r, e)) return rc;
+  if (size_t(slot) >= r->snap_time.size()) {
+    r->snap_time.resize(slot + 1);
+    r->snap_step.resize(slot + 1);
+    r->snap_sample_time.resize(slot + 1);
+  }
+  r->snap_time[slot] = r->time;
+  r->snap_step[slot] = r->step;
+  r->snap_sample_time[slot] = tr ? trail_newest_time(r) : 0.0;
+  return GBGHT_OK;
 }
 
 int gbght_snapshot_load(gbght_run* r, int slot) {
   if (check_run(r)) return GBGHT_ERR_ARGUMENT;
-  const char* e = r->eng->snapshot_load(slot);
+  if (slot < 0 || size_t(slot) >= r->snap_time.size()) return fail(r, GBGHT_ERR_ARGUMENT, "no such snapshot slot");
+  const bool tr = r->cfg.tracers > 0;
+  if (tr && r->trail_newest < 0) return fail(r, GBGHT_ERR_SCHEDULE, "the tracers' trail is empty");
+  const char* e = r->eng->snapshot_load(slot, tr ? r->trail_newest : 0);
   if (e && std::strstr(e, "snapshot")) return fail(r, GBGHT_ERR_ARGUMENT, e);
   int rc = engine_call(r, e);
   if (rc) return rc;
   r->fields_epoch += 1;   // a new state: the deposit is stale
+  r->time = r->snap_time[slot];
+  r->step = r->snap_step[slot];
+  if (tr) {   // the trail holds the snapshot's newest sample, at the restored positions
+    r->trail_count = 1;
+    r->trail_time[r->trail_newest] = r->snap_sample_time[slot];
+    r->sampled = true;
+    r->sample_at_positions = true;
+    r->sample_epoch = r->fields_epoch;
+  }
   return GBGHT_OK;
+}
+
+int gbght_adjoint_advance(gbght_run* r, double dt) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (r->cfg.tracers <= 0 || r->cfg.tracer_scheme != GBGHT_HEUN)
+    return fail(r, GBGHT_ERR_ARGUMENT, "the adjoint of an iteration's tracer push is built for Heun tracers");
+  if (!finite_positive(dt))
+    return fail(r, GBGHT_ERR_ARGUMENT, "the timestep must be positive and finite, got " + std::to_string(dt));
+  if (r->trail_count == 0 || !r->sample_at_positions)
+    return fail(r, GBGHT_ERR_SCHEDULE, "the trail's newest sample was not taken at the current positions");
+  const Tableau t = tableau(r->cfg.scheme);
+  gbght::AdamsStep w = adams_step(r, dt);
+  int rc = engine_call(r, r->eng->adjoint_step(dt, t.a, t.b, t.d, t.S, &w, r->trail_newest));
+  if (rc) return rc;
+  r->deposit_epoch = r->fields_epoch;   // the deposit of the state was rebuilt
+  return GBGHT_OK;
+}
+
+int gbght_adjoint_tracers_import(gbght_run* r, const double* lam_X, const double* lam_f) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!lam_X || !lam_f) return fail(r, GBGHT_ERR_ARGUMENT, "lam_X and lam_f must be given");
+  return engine_call(r, r->eng->adjoint_tracers_import(lam_X, lam_f));
+}
+
+int gbght_adjoint_tracers_export(gbght_run* r, double* lam_X, double* lam_f) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (!lam_X || !lam_f) return fail(r, GBGHT_ERR_ARGUMENT, "lam_X and lam_f must be given");
+  return engine_call(r, r->eng->adjoint_tracers_export(lam_X, lam_f));
+}
+
+int gbght_adjoint_deposit_tracers(gbght_run* r) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (int rc = require_deposit(r, "adjoint of the particle deposit")) return rc;
+  return engine_call(r, r->eng->adjoint_deposit_tracers());
 }
 
 int gbght_profile(gbght_run* r, int enable) {

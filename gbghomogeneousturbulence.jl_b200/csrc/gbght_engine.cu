@@ -726,6 +726,13 @@ class EngineImpl final : public Engine {
     if ((err = alloc(&ampsave_, 2 * kMaxStages * sizeof(double)))) return err;
     if ((err = alloc(&coef_, 4 * sizeof(double)))) return err;
     if ((err = alloc(&grad_, 2 * sizeof(double)))) return err;
+    if (p_.tracers > 0) {
+      const size_t m3 = 3 * size_t(p_.tracers) * sizeof(double);
+      if ((err = alloc(&LX_, m3))) return err;
+      if ((err = alloc(&LF_, m3))) return err;
+      if ((err = alloc(&LU_, 3 * nP_ * sizeof(double)))) return err;
+      if (snapshots > 0 && (err = alloc(&snapX_, size_t(snapshots) * 2 * m3))) return err;
+    }
 #ifndef GBGHT_EMU
     if ((err = make_maps_on(&maps_adj_, Aa_, Ba_))) return err;
 #endif
@@ -811,23 +818,55 @@ class EngineImpl final : public Engine {
     if (!e) e = rt_memset(grad_, 0, 2 * sizeof(double), stream_);
     return e ? e : rt_sync(stream_);
   }
-  const char* snapshot_save(int slot) override {
+  const char* snapshot_save(int slot, int f_slot) override {
     if (slot < 0 || slot >= nsnap_) return "no such snapshot slot";
-    return rt_d2d(snaps_ + size_t(slot) * 4 * nS_, S_, 4 * nS_ * sizeof(Cplx<T>), stream_);
+    const char* e = rt_d2d(snaps_ + size_t(slot) * 4 * nS_, S_, 4 * nS_ * sizeof(Cplx<T>), stream_);
+    if (!e && X_ && snapX_) {
+      const size_t m3 = 3 * size_t(p_.tracers);
+      e = rt_d2d(snapX_ + size_t(slot) * 2 * m3, X_, m3 * sizeof(double), stream_);
+      if (!e) e = rt_d2d(snapX_ + size_t(slot) * 2 * m3 + m3, F_ + size_t(f_slot) * m3, m3 * sizeof(double), stream_);
+    }
+    return e;
   }
-  const char* snapshot_load(int slot) override {
+  const char* snapshot_load(int slot, int f_slot) override {
     if (slot < 0 || slot >= nsnap_) return "no such snapshot slot";
     const char* e = rt_d2d(S_, snaps_ + size_t(slot) * 4 * nS_, 4 * nS_ * sizeof(Cplx<T>), stream_);
+    if (!e && X_ && snapX_) {
+      const size_t m3 = 3 * size_t(p_.tracers);
+      e = rt_d2d(X_, snapX_ + size_t(slot) * 2 * m3, m3 * sizeof(double), stream_);
+      if (!e) e = rt_d2d(F_ + size_t(f_slot) * m3, snapX_ + size_t(slot) * 2 * m3 + m3, m3 * sizeof(double), stream_);
+    }
     if (!e) e = z_init();
     return e;
+  }
+  const char* adjoint_tracers_import(const double* lX, const double* lf) override {
+    if (!adj_ready_ || !LX_) return "the adjoint of the tracers is not set up";
+    const size_t m3 = 3 * size_t(p_.tracers) * sizeof(double);
+    if (where(lX) < 0 || where(lf) < 0) return "a tracer cotangent is device memory of another device";
+    const char* e = rt_copy(LX_, lX, m3, stream_);
+    return e ? e : rt_copy(LF_, lf, m3, stream_);
+  }
+  const char* adjoint_tracers_export(double* lX, double* lf) override {
+    if (!adj_ready_ || !LX_) return "the adjoint of the tracers is not set up";
+    const size_t m3 = 3 * size_t(p_.tracers) * sizeof(double);
+    if (where(lX) < 0 || where(lf) < 0) return "a tracer cotangent is device memory of another device";
+    const char* e = rt_copy(lX, LX_, m3, stream_);
+    return e ? e : rt_copy(lf, LF_, m3, stream_);
+  }
+  const char* adjoint_deposit_tracers() override {
+    if (!adj_ready_ || !LX_) return "the adjoint of the tracers is not set up";
+    tracer_adjoint(nullptr, 0);
+    return rt_check();
   }
 
   // The reverse of one low-storage step at the current state q: the forward stages again, keeping
   // each stage's state and amplitudes; then, per stage in reverse, the stage's forward fields
   // (z- and y-inverse of the saved state), the adjoint x pass, its y-forward, the band coefficients
   // and the adjoint z pass; finally the state is put back.
-  const char* adjoint_step(double dt, const double* a, const double* b, const double* d, int S) override {
+  const char* adjoint_step(double dt, const double* a, const double* b, const double* d, int S, const AdamsStep* push,
+                           int f_slot) override {
     if (!adj_ready_) return "the adjoint is not set up";
+    if (push && !LX_) return "the adjoint of the tracers is not set up";
     if (S < 1 || S > kMaxStages) return "the adjoint needs a low-storage scheme";
     const size_t s4 = 4 * nS_;
     for (int i = 0; i < S; ++i) {
@@ -845,6 +884,10 @@ class EngineImpl final : public Engine {
       const char* e = stage(st);
       amp_save_to_ = nullptr;
       if (e) return e;
+    }
+    if (push) {   // the iteration's tracer part, reversed first: it ran last
+      if (const char* e = deposit_launch()) return e;
+      tracer_adjoint(push, f_slot);
     }
     const int nc = p_.scalar ? 4 : 3;
     const int ninv = p_.scalar ? 7 : 6, nsrc = p_.scalar ? 6 : 3, nprod = p_.scalar ? 7 : 6;
@@ -881,9 +924,11 @@ class EngineImpl final : public Engine {
       adj_z(st, Qs_ + i * s4);
       if (const char* e = rt_check()) return e;
     }
-    // the state as it was, its z-inverse in A (the deposit is unchanged)
+    // the state as it was, its z-inverse in A, and its deposit (the tracers' part overwrote it)
     if (const char* e = rt_d2d(S_, Qs_, s4 * sizeof(Cplx<T>), stream_)) return e;
     if (const char* e = z_init()) return e;
+    if (push)
+      if (const char* e = deposit_launch()) return e;
     return rt_check();
   }
 
@@ -1034,6 +1079,7 @@ class EngineImpl final : public Engine {
     set(reinterpret_cast<const void*>(k_z_init<T, N, TLZ, NTZ>), smem_z());
     set(reinterpret_cast<const void*>(k_x_adjoint<T, N, NTXA>), smem_xa());
     set(reinterpret_cast<const void*>(k_adj_z<T, N, TLZ, NTZA>), smem_za());
+    set(reinterpret_cast<const void*>(k_phys_forward<T, N, 8>), size_t(8) * N * sizeof(Cplx<T>));
     return e;
   }
 
@@ -1226,6 +1272,38 @@ class EngineImpl final : public Engine {
     return rt_check();
   }
   // ---- adjoint launches -------------------------------------------------------------------------------
+  // The tracers' adjoint at the deposited field U: the Heun push and closing deposit (w, the sample
+  // before the push in trail slot f_slot) or, with w = nullptr, the particle deposit alone; then
+  // λ_u += rfft(λ_u physical)/N³ on the ball.
+  void tracer_adjoint(const AdamsStep* w, int f_slot) {
+    const int64_t M = p_.tracers;
+    const double* f0 = F_ + size_t(f_slot) * 3 * size_t(M);
+    rt_memset(LU_, 0, 3 * nP_ * sizeof(double), stream_);
+    const int push = w ? 1 : 0;
+    const double b0 = w ? w->b[0] : 0.0, bs = w ? w->beta_star : 0.0, bm = w ? w->beta_m[0] : 0.0;
+    constexpr int NWP = 8;
+#ifdef GBGHT_EMU
+    for (int64_t p = 0; p < M; ++p) tracer_adjoint_one<T>(p, M, U_, LU_, N, p_.L, X_, f0, LX_, LF_, push, b0, bs, bm);
+    const int npairs = 3 * N * (N / 2);
+    emu_grid((npairs + NWP - 1) / NWP, 1, 1, size_t(NWP) * N * sizeof(Cplx<T>), [&](const Cta& c, void* sm) {
+      body_phys_forward<T, N, NWP, 1>(c, static_cast<Cplx<T>*>(sm), g_, LU_, Ba_, tw_);
+    });
+#else
+    pbegin(PROF_TRACERS);
+    k_tracer_adjoint<T><<<unsigned((M + 127) / 128), 128, 0, stream_>>>(M, U_, LU_, N, p_.L, X_, f0, LX_, LF_, push, b0,
+                                                                        bs, bm);
+    pend();
+    const int npairs = 3 * N * (N / 2);
+    pbegin(PROF_X_ADJOINT);
+    k_phys_forward<T, N, NWP><<<unsigned((npairs + NWP - 1) / NWP), 32 * NWP, size_t(NWP) * N * sizeof(Cplx<T>),
+                                stream_>>>(g_, LU_, Ba_, tw_);
+    pend();
+#endif
+    y_forward_on(3, maps_adj_, Ba_, Aa_);
+    AdjArgs a{};
+    a.add_only = 1;
+    adj_z(a, nullptr);
+  }
   AdjArgs adj_base(double dt) const {
     AdjArgs a{};
     a.has_scalar = p_.scalar;
@@ -1507,6 +1585,7 @@ class EngineImpl final : public Engine {
   double *ampsave_ = nullptr, *coef_ = nullptr, *grad_ = nullptr;
   double* amp_save_to_ = nullptr;
   TmaMaps maps_adj_{};
+  double *LX_ = nullptr, *LF_ = nullptr, *LU_ = nullptr, *snapX_ = nullptr;   // the tracers' adjoint
 };
 
 #if defined(GBGHT_UNIT_FACTORY)

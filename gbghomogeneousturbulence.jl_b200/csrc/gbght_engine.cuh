@@ -119,12 +119,22 @@ class Engine {
   virtual const char* adjoint_init(int snapshots) = 0;
   virtual const char* adjoint_import(const double* lu, const double* lp, bool* outside) = 0;
   virtual const char* adjoint_export(double* lu, double* lp) = 0;
-  virtual const char* adjoint_step(double dt, const double* a, const double* b, const double* d, int S) = 0;
+  // `push` (nullptr: the fields alone): the tracers' Heun push and closing deposit of the same
+  // iteration, with the forward's weights and the trail slot of the sample before the push; its
+  // adjoint updates the tracer cotangents and adds the gathers' part to λ before the field stages.
+  virtual const char* adjoint_step(double dt, const double* a, const double* b, const double* d, int S,
+                                   const AdamsStep* push = nullptr, int f_slot = 0) = 0;
+  // the tracer cotangents (positions, newest sample), [3][M] each, host or device memory
+  virtual const char* adjoint_tracers_import(const double* lX, const double* lf) = 0;
+  virtual const char* adjoint_tracers_export(double* lX, double* lf) = 0;
+  // the particle deposit's adjoint at the current positions and deposit: λ_u += Wᵀλ_f, λ_X += …, λ_f = 0
+  virtual const char* adjoint_deposit_tracers() = 0;
   virtual const char* adjoint_add(double wu, double wp) = 0;
   virtual const char* adjoint_gradient(double* g, int reset) = 0;
   virtual const char* adjoint_clear() = 0;
-  virtual const char* snapshot_save(int slot) = 0;
-  virtual const char* snapshot_load(int slot) = 0;
+  // a snapshot holds the state and, with tracers, the positions and the trail sample in `f_slot`
+  virtual const char* snapshot_save(int slot, int f_slot) = 0;
+  virtual const char* snapshot_load(int slot, int f_slot) = 0;
   virtual int K() const = 0;
   virtual double cutoff() const = 0;
 };

@@ -389,6 +389,17 @@ __global__ void k_adj_band(Geometry g, const Cplx<T>* Q, const Cplx<T>* LH, AdjB
   if (threadIdx.x == 0) adj_band_finish(a, amp, su[0], sp[0], coef, grad);
 }
 template <class T>
+__global__ void k_tracer_adjoint(int64_t M, const T* u, double* lu, int N, double L, const double* X, const double* f0,
+                                 double* lX, double* lf, int push, double b0, double beta_star, double beta_m) {
+  const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p < M) tracer_adjoint_one<T>(p, M, u, lu, N, L, X, f0, lX, lf, push, b0, beta_star, beta_m);
+}
+template <class T, int N, int NW>
+__global__ void __launch_bounds__(32 * NW) k_phys_forward(Geometry g, const double* lu, Cplx<T>* Ba, const Cplx<T>* tw) {
+  CTA_CTX;
+  body_phys_forward<T, N, NW, 32 * NW>(c, reinterpret_cast<Cplx<T>*>(g_smem), g, lu, Ba, tw);
+}
+template <class T>
 __global__ void k_adj_add(size_t nS, int nc, Cplx<T>* L, const Cplx<T>* S, double wu, double wp) {
   adj_add_mode<T>(size_t(blockIdx.x) * blockDim.x + threadIdx.x, nS, nc, L, S, wu, wp);
 }

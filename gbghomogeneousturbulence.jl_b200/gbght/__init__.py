@@ -128,6 +128,10 @@ _SIGNATURES = {
     "gbght_adjoint_clear": (C.c_int, [C.c_void_p]),
     "gbght_snapshot_save": (C.c_int, [C.c_void_p, C.c_int]),
     "gbght_snapshot_load": (C.c_int, [C.c_void_p, C.c_int]),
+    "gbght_adjoint_advance": (C.c_int, [C.c_void_p, C.c_double]),
+    "gbght_adjoint_deposit_tracers": (C.c_int, [C.c_void_p]),
+    "gbght_adjoint_tracers_import": (C.c_int, [C.c_void_p, _DP, _DP]),
+    "gbght_adjoint_tracers_export": (C.c_int, [C.c_void_p, _DP, _DP]),
 }
 
 KERNELS = ("y_inverse", "x_products", "y_forward", "z_epilogue", "x_velocity", "force_amp", "reality",
@@ -574,6 +578,26 @@ class Run:
 
     def adjoint_clear(self):
         self._check(self.lib.gbght_adjoint_clear(self.h))
+
+    def adjoint_advance(self, dt: float):
+        """The reverse of one advance! iteration (field step, Heun push, particle deposit) at the
+        current state, for λ and the tracer cotangents."""
+        self._check(self.lib.gbght_adjoint_advance(self.h, float(dt)))
+
+    def adjoint_deposit_tracers(self):
+        """The reverse of the particle deposit f = u(X) at the current state."""
+        self._check(self.lib.gbght_adjoint_deposit_tracers(self.h))
+
+    def adjoint_tracers_import(self, lam_X, lam_f):
+        a = np.ascontiguousarray(lam_X, dtype=np.float64)
+        b = np.ascontiguousarray(lam_f, dtype=np.float64)
+        self._check(self.lib.gbght_adjoint_tracers_import(self.h, _ptr(a), _ptr(b)))
+
+    def adjoint_tracers_export(self):
+        a = np.zeros((3, self.setup.tracers))
+        b = np.zeros((3, self.setup.tracers))
+        self._check(self.lib.gbght_adjoint_tracers_export(self.h, _ptr(a), _ptr(b)))
+        return a, b
 
     def snapshot_save(self, slot: int):
         self._check(self.lib.gbght_snapshot_save(self.h, int(slot)))

@@ -17,6 +17,8 @@ from __future__ import annotations
 
 import math
 
+import numpy as np
+
 
 def binomial_repetitions(n: int, snaps: int) -> int:
     """The fewest r with C(snaps + r, snaps) ≥ n (r = n without snapshots)."""
@@ -45,6 +47,8 @@ class Reverse:
         if snapshots < 1:
             raise ValueError("the reverse sweep needs at least the start's snapshot slot")
         self.run, self.dts, self.loss_grad, self.snapshots = run, [float(d) for d in dts], loss_grad, snapshots
+        # with tracers, a step is a whole advance! iteration (the push and the particle deposit too)
+        self.tracers = run.setup.tracers > 0
         self.cur = None          # the step index of the state the run holds
         self.forward_steps = 0   # steps recomputed by the reverse sweep
         self.adjoint_steps = 0
@@ -58,14 +62,20 @@ class Reverse:
     def _advance(self, k: int, count=True):
         for _ in range(k):
             self.run.deposit()
-            self.run.step(self.dts[self.cur])
+            if self.tracers:
+                self.run.advance(self.dts[self.cur])
+            else:
+                self.run.step(self.dts[self.cur])
             self.cur += 1
             if count:
                 self.forward_steps += 1
 
     def _reverse_one(self, k0: int):
         # the run holds q_k0; λ holds ∂L/∂q_(k0+1) (with every later term)
-        self.run.adjoint_step(self.dts[k0])
+        if self.tracers:
+            self.run.adjoint_advance(self.dts[k0])
+        else:
+            self.run.adjoint_step(self.dts[k0])
         self.adjoint_steps += 1
         self.loss_grad(self.run, k0)
 
@@ -101,17 +111,46 @@ class Reverse:
         run.snapshot_load(0)
         run.deposit()
         self.cur = 0
+        if self.tracers:   # the construction's particle deposit f₀ = u₀(X₀)
+            run.adjoint_deposit_tracers()
         return self
 
 
 def gradient(run, dts, loss_grad, snapshots: int = 16):
     """∂L/∂q_0 (λ_u, λ_φ in the state's layout) and ∂L/∂ε (velocity, scalar) of the loss
     Σ_k ℓ_k(q_k) over `len(dts)` steps from the run's current state, by the checkpointed reverse
-    sweep. The adjoint register and the forcing gradient are cleared first."""
+    sweep. The adjoint register and the forcing gradient are cleared first (and the tracer
+    cotangents, for a run with tracers: then a step is an advance! iteration, `loss_grad` may add
+    to the tracer cotangents through `Run.adjoint_tracers_import`, and `sweep.tracer_gradient`
+    holds ∂L/∂X_0 at the end)."""
     run.adjoint_clear()
+    if run.setup.tracers:
+        z = np.zeros((3, run.setup.tracers))
+        run.adjoint_tracers_import(z, z)
     sweep = Reverse(run, dts, loss_grad, snapshots).run_sweep()
     lam = run.adjoint_export()
+    if run.setup.tracers:
+        sweep.tracer_gradient = run.adjoint_tracers_export()[0]
     return lam, run.forcing_gradient(), sweep
+
+
+def tracer_kinetic_energy(step: int, weight: float = 1.0):
+    """loss_grad of L = weight · (1/M) Σ_p |u(X_p)|² over the tracers' newest samples at `step`
+    (λ_f += 2·weight·f/M there)."""
+    def loss_grad(run, k):
+        if k == step:
+            f, _ = run.tracer_sample()
+            lX, lf = run.adjoint_tracers_export()
+            run.adjoint_tracers_import(lX, lf + 2.0 * weight * f / f.shape[1])
+    return loss_grad
+
+
+def combined(*terms):
+    """The loss_grad of a sum of losses."""
+    def loss_grad(run, k):
+        for t in terms:
+            t(run, k)
+    return loss_grad
 
 
 def scalar_variance_window(n0: int, n1: int):

@@ -354,6 +354,23 @@ int gbght_adjoint_clear(gbght_run* run);
 int gbght_snapshot_save(gbght_run* run, int slot);
 int gbght_snapshot_load(gbght_run* run, int slot);
 
+/* The tracers in the adjoint (Heun tracers with Catmull–Rom gathers; the reference's
+ * src/ParticlePropagator.jl:288-315,378-386 differentiated). A snapshot of a run with tracers also
+ * holds the positions and the trail's newest sample with its time, and the clock.
+ * gbght_adjoint_advance is the reverse of one whole advance! iteration at the run's current state
+ * (q, X, f): λ holds the cotangent of the state after the iteration and the tracer register that
+ * of (X', f'); the tracers' push and closing deposit are reversed first (their gathers add to λ),
+ * then the field step; the run is left at (q, X, f) with its deposit current.
+ * gbght_adjoint_deposit_tracers reverses the particle deposit f = u(X) alone at the current state
+ * (the sample a Simulation takes at construction): λ += its gathers' part, λ_X += …, λ_f = 0.
+ * gbght_adjoint_tracers_import / _export move the tracer cotangents (λ_X, λ_f), [3][M] each, host
+ * or device memory. The gathers' adjoint adds with atomics, so results agree with any other order
+ * to round-off, not bit for bit. */
+int gbght_adjoint_advance(gbght_run* run, double dt);
+int gbght_adjoint_deposit_tracers(gbght_run* run);
+int gbght_adjoint_tracers_import(gbght_run* run, const double* lam_X, const double* lam_f);
+int gbght_adjoint_tracers_export(gbght_run* run, double* lam_X, double* lam_f);
+
 /* Wait for all work queued on the run's stream. */
 int gbght_synchronize(gbght_run* run);
 

@@ -196,43 +196,47 @@ def test_dot_product_identity_against_the_oracle_tangent(cuda_library):
     assert right == pytest.approx(left, rel=1e-12)
 
 
-def _c4_forward_loss(library, setup, uh, ph, dts, n0, n1):
-    run = gbght.simulation(setup, uh, ph, library=library)
+def _c4_forward_loss(library, setup, uh, ph, X, dts, n0, n1):
+    """L = mean over steps n0..n1 of ⟨φ²⟩ + (1/M) Σ_p |u(X_p)|² at step n1, the tracers advected by
+    Heun from X along the fixed Δt sequence."""
+    run = gbght.simulation(setup, uh, ph, X, library=library)
     total = 0.0
     for k in range(len(dts) + 1):
         if k > 0:
-            run.step(dts[k - 1])
-            run.deposit()
+            run.advance(dts[k - 1])
         if n0 <= k <= n1:
             total += run.observables()["scalar_variance"]
+    f, _ = run.tracer_sample()
     run.close()
-    return total / (n1 - n0 + 1)
+    return total / (n1 - n0 + 1) + float(np.sum(f * f)) / f.shape[1]
 
 
 @pytest.mark.gpu
 def test_c4_gradient_against_central_differences(cuda_library):
     # 128³ forced velocity + scalar, ν = ϰ = 6e-3, ConstantPower ε = 0.1 on shells 1–2, G = 1 along x,
-    # IF-RK4; loss the scalar variance averaged over steps 100..200 (Δt held at the CFL sequence
-    # of the unperturbed run); gradients with respect to ε and the initial velocity, by the
-    # checkpointed reverse sweep with 16 stored states, against central differences (h = 1e-6)
-    # of the FP64 forward along 8 seeded directions
-    N, nsteps, n0 = 128, 200, 100
-    uh, ph = S.seed_velocity(N, 0.5, seed=0), S.seed_scalar(N, 0.5, seed=1)
+    # IF-RK4, 16384 Heun tracers. Loss: the scalar variance averaged over steps 100..200 plus the
+    # mean squared velocity sampled at the tracers at step 200 (Δt held at the CFL sequence of the
+    # unperturbed run). Gradients with respect to ε and the initial velocity, by the checkpointed
+    # reverse sweep with 16 stored states, against central differences (h = 1e-6) of the FP64
+    # forward along 8 seeded directions.
+    N, M, nsteps, n0 = 128, 16384, 200, 100
+    uh, ph, X = S.seed_velocity(N, 0.5, seed=0), S.seed_scalar(N, 0.5, seed=1), S.seed_tracers(M, seed=2)
     eps = 0.1
 
     def setup(e):
         return gbght.Setup(grid_points_per_axis=N, viscosity=6e-3, velocity_forcing=gbght.ConstantPower(e),
-                           mean_gradient=(1.0, 0.0, 0.0), cfl=0.5)
-    ref = gbght.simulation(setup(eps), uh, ph, library=cuda_library)
+                           mean_gradient=(1.0, 0.0, 0.0), cfl=0.5, tracers=M)
+    ref = gbght.simulation(setup(eps), uh, ph, X, library=cuda_library)
     dts = [ref.advance(None) for _ in range(nsteps)]
     ref.close()
-    run = gbght.simulation(setup(eps), uh, ph, library=cuda_library)
+    run = gbght.simulation(setup(eps), uh, ph, X, library=cuda_library)
     run.adjoint_create(16)
-    (lu, lp), (geps, _), sweep = AD.gradient(run, dts, AD.scalar_variance_window(n0, nsteps), snapshots=16)
+    loss_grad = AD.combined(AD.scalar_variance_window(n0, nsteps), AD.tracer_kinetic_energy(nsteps))
+    (lu, lp), (geps, _), sweep = AD.gradient(run, dts, loss_grad, snapshots=16)
     assert sweep.peak <= 16 and sweep.adjoint_steps == nsteps
     h = 1e-6
-    fd = (_c4_forward_loss(cuda_library, setup(eps + h), uh, ph, dts, n0, nsteps)
-          - _c4_forward_loss(cuda_library, setup(eps - h), uh, ph, dts, n0, nsteps)) / (2 * h)
+    fd = (_c4_forward_loss(cuda_library, setup(eps + h), uh, ph, X, dts, n0, nsteps)
+          - _c4_forward_loss(cuda_library, setup(eps - h), uh, ph, X, dts, n0, nsteps)) / (2 * h)
     errs = [abs(geps - fd) / abs(fd)]
     dom = O.Domain(N)
     rng = np.random.default_rng(2024)
@@ -241,10 +245,75 @@ def test_c4_gradient_against_central_differences(cuda_library):
         v *= np.linalg.norm(uh) / np.linalg.norm(v)
         # a Hermitian kx = 0 plane keeps the perturbed state a real field
         v = O.reality_projection(dom, v)
-        dL = (_c4_forward_loss(cuda_library, setup(eps), uh + h * v, ph, dts, n0, nsteps)
-              - _c4_forward_loss(cuda_library, setup(eps), uh - h * v, ph, dts, n0, nsteps)) / (2 * h)
+        dL = (_c4_forward_loss(cuda_library, setup(eps), uh + h * v, ph, X, dts, n0, nsteps)
+              - _c4_forward_loss(cuda_library, setup(eps), uh - h * v, ph, X, dts, n0, nsteps)) / (2 * h)
         ad = O.spectral_dot(dom, lu, v)
         errs.append(abs(ad - dL) / abs(dL))
+    # and the initial positions, along one seeded direction
+    vX = rng.standard_normal((3, M)) * 1e-2
+    dL = (_c4_forward_loss(cuda_library, setup(eps), uh, ph, X + h * vX, dts, n0, nsteps)
+          - _c4_forward_loss(cuda_library, setup(eps), uh, ph, X - h * vX, dts, n0, nsteps)) / (2 * h)
+    errs.append(abs(float(np.sum(sweep.tracer_gradient * vX)) - dL) / abs(dL))
     print(f"C4 128^3: dL/deps adjoint {geps:.10e} fd {fd:.10e}; relative errors {['%.1e' % e for e in errs]}; "
           f"{sweep.forward_steps} recomputed steps, {sweep.peak} slots")
     assert max(errs) <= 1e-6
+
+
+def iteration_adjoint_pair(library, N, M, *, precision="fp64", dt=0.01, seed=9):
+    """The reverse of one advance! iteration with Heun tracers through the library and the oracle
+    (heun_push_adjoint, then step_adjoint on the state cotangent with the push's part added)."""
+    uh, ph, X = S.seed_velocity(N, 0.5, seed=0), S.seed_scalar(N, 0.5, seed=1), S.seed_tracers(M, seed=2)
+    dom = O.Domain(N)
+    rng = np.random.default_rng(seed)
+    lam, lamp = _rand_ball(dom, rng, (3,) + dom.shape_spectral), _rand_ball(dom, rng, dom.shape_spectral)
+    lX, lf = rng.standard_normal((3, M)), rng.standard_normal((3, M))
+    setup = gbght.Setup(grid_points_per_axis=N, viscosity=0.01, velocity_forcing=gbght.ConstantPower(0.1),
+                        mean_gradient=(1.0, 0.0, 0.0), tracers=M, precision=precision)
+    run = gbght.simulation(setup, uh, ph, X, library=library)
+    f0, _ = run.tracer_sample()
+    run.adjoint_create(1)
+    run.adjoint_import(lam, lamp)
+    run.adjoint_tracers_import(lX, lf)
+    run.adjoint_advance(dt)
+    lib = run.adjoint_export() + run.adjoint_tracers_export()
+    cond = O.Conditions(viscosity=0.01, velocity_forcing=O.ConstantPower(0.1), mean_gradient=(1.0, 0.0, 0.0))
+    st = O.step(dom, cond, O.State(uh.copy(), ph.copy()), dt)
+    lu_push, oX, of = O.heun_push_adjoint(dom, st.uh, X, f0, dt, lX, lf)
+    ou, op = O.step_adjoint(dom, cond, uh, lam + lu_push, dt, "rk4", ph, lamp)
+    return lib, (ou * dom.mask, op * dom.mask, oX, of), run, (uh, ph, X, f0)
+
+
+def test_iteration_adjoint_with_tracers_matches_the_oracle_hostcheck(hostcheck_library):
+    (lu, lp, lX, lf), (ou, op, oX, of), run, (uh, ph, X, f0) = iteration_adjoint_pair(hostcheck_library, 12, 40)
+    assert rel_l2(lu, ou) <= 1e-12 and rel_l2(lp, op) <= 1e-12
+    assert rel_l2(lX, oX) <= 1e-12 and rel_l2(lf, of) <= 1e-12
+    ue, _ = run.export_state()
+    assert np.array_equal(ue, uh) and np.array_equal(run.tracers(), X)
+    F, _ = run.tracer_sample()
+    assert np.array_equal(F, f0)   # the run is left at (q, X, f)
+    run.advance(0.01)              # and its schedule is intact
+
+
+def test_particle_deposit_adjoint_matches_the_oracle_hostcheck(hostcheck_library):
+    N, M = 12, 40
+    uh, ph, X = S.seed_velocity(N, 0.5, seed=0), S.seed_scalar(N, 0.5, seed=1), S.seed_tracers(M, seed=2)
+    setup = gbght.Setup(grid_points_per_axis=N, tracers=M)
+    run = gbght.simulation(setup, uh, ph, X, library=hostcheck_library)
+    run.adjoint_create(0)
+    lf = np.random.default_rng(3).standard_normal((3, M))
+    run.adjoint_tracers_import(np.zeros((3, M)), lf)
+    run.adjoint_deposit_tracers()
+    lu, _ = run.adjoint_export()
+    lX, lf_after = run.adjoint_tracers_export()
+    dom = O.Domain(N)
+    ou_phys, oX = O.interpolate_adjoint(dom, dom.to_physical(uh), X, lf)
+    ou = dom.to_spectral(ou_phys) / float(N) ** 3 * dom.mask
+    assert rel_l2(lu, ou) <= 1e-12 and rel_l2(lX, oX) <= 1e-12 and not lf_after.any()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32_mixed", 1e-5)])
+def test_iteration_adjoint_with_tracers_matches_the_oracle(cuda_library, precision, tol):
+    (lu, lp, lX, lf), (ou, op, oX, of), _, _ = iteration_adjoint_pair(cuda_library, 64, 2000, precision=precision)
+    assert rel_l2(lu, ou) <= tol and rel_l2(lp, op) <= tol
+    assert rel_l2(lX, oX) <= tol and rel_l2(lf, of) <= tol
