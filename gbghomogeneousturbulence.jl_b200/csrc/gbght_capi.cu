@@ -31,6 +31,8 @@ struct gbght_run {
   bool sampled = false;         // a particle deposit has paired the tracer and field epochs
   bool sample_at_positions = false;
   int64_t sample_epoch = 0;
+  // StochasticOU: whether each field's force was set for the next step
+  bool source_fresh[2] = {false, false};
   // the clock
   double time = 0.0;
   int64_t step = 0;
@@ -136,6 +138,18 @@ std::string forcing_error(const gbght_forcing_params& f, const char* who) {
       if (!finite_positive(f.turnover_time))
         return w + "VarianceController `turnover_time` must be finite and positive, got " +
                std::to_string(f.turnover_time);
+      break;
+    case GBGHT_FORCING_STOCHASTIC_OU:
+      if (!(std::isfinite(f.target) && f.target >= 0))
+        return w + "StochasticOU `forcing_variance` must be finite and non-negative, got " + std::to_string(f.target) +
+               ": it is the stationary mean square of the term the forcing adds, and its square root sets the "
+               "amplitude of every draw";
+      if (!finite_positive(f.turnover_time))
+        return w + "StochasticOU `correlation_time` must be finite and positive, got " +
+               std::to_string(f.turnover_time) + ": it is the Ornstein–Uhlenbeck relaxation time T_L";
+      if (!std::isfinite(f.highest_shell))
+        return w + "StochasticOU needs a finite `highest_shell`, got Inf: it adds its process rather than "
+                   "multiplying the field, so its band must stay below the dealias cutoff";
       break;
     case GBGHT_FORCING_VARIANCE_RESCALING:
       if (f.over != GBGHT_OVER_BAND && f.over != GBGHT_OVER_TOTAL)
@@ -392,6 +406,17 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
     g_global_error = e;
     return GBGHT_ERR_CUDA;
   }
+  for (int f = 0; f < 2; ++f) {   // StochasticOU's band below the dealias cutoff (src/Forcing.jl:1327-1333)
+    const gbght_forcing_params& fp = f == 0 ? cfg->velocity_forcing : cfg->scalar_forcing;
+    if (fp.kind != GBGHT_FORCING_STOCHASTIC_OU) continue;
+    const double high = (fp.highest_shell + 0.5) * (2.0 * M_PI / cfg->side_length);
+    if (!(high <= r->eng->cutoff()))
+      return bad("the forcing band (shells " + std::to_string(fp.lowest_shell) + "-" +
+                 std::to_string(int(fp.highest_shell)) + ") reaches |κ| = " + std::to_string(high) +
+                 ", past the dealias cutoff " + std::to_string(r->eng->cutoff()) +
+                 "; an additive force would fill modes the dealiasing holds empty. Lower the shells, or "
+                 "enlarge the grid.");
+  }
   *out = r.release();
   return GBGHT_OK;
 }
@@ -427,14 +452,44 @@ int gbght_state_export(gbght_run* r, double* u_hat, double* phi_hat) {
   return engine_call(r, r->eng->export_state(u_hat, r->cfg.scalar ? phi_hat : nullptr));
 }
 
+namespace {
+bool stochastic(const gbght_run* r, int f) {
+  return (f == 0 ? r->cfg.velocity_forcing.kind : r->cfg.scalar_forcing.kind) == GBGHT_FORCING_STOCHASTIC_OU;
+}
+// A StochasticOU field's force is set once per step (prepare_forcing!, src/Forcing.jl:1401-1411).
+int require_sources(gbght_run* r) {
+  for (int f = 0; f < 2; ++f)
+    if (stochastic(r, f) && !r->source_fresh[f])
+      return fail(r, GBGHT_ERR_SCHEDULE, std::string("the ") + (f == 0 ? "velocity" : "scalar") +
+                                             "'s StochasticOU force was not set for this step: advance its process "
+                                             "and hand it in with gbght_forcing_source_set");
+  return GBGHT_OK;
+}
+void consume_sources(gbght_run* r) { r->source_fresh[0] = r->source_fresh[1] = false; }
+}  // namespace
+
+int gbght_forcing_source_set(gbght_run* r, int field, const double* amplitudes, int companion_points) {
+  if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (field != 0 && field != 1) return fail(r, GBGHT_ERR_ARGUMENT, "field must be 0 (velocity) or 1 (scalar)");
+  if (!stochastic(r, field)) return fail(r, GBGHT_ERR_ARGUMENT, "the field carries no StochasticOU forcing");
+  if (!amplitudes) return fail(r, GBGHT_ERR_ARGUMENT, "amplitudes is null");
+  const char* e = r->eng->forcing_source(field, amplitudes, companion_points);
+  if (e && std::strstr(e, "companion")) return fail(r, GBGHT_ERR_ARGUMENT, e);
+  if (int rc = engine_call(r, e)) return rc;
+  r->source_fresh[field] = true;
+  return GBGHT_OK;
+}
+
 int gbght_step(gbght_run* r, double dt) {
   if (check_run(r)) return GBGHT_ERR_ARGUMENT;
   if (!finite_positive(dt))
     return fail(r, GBGHT_ERR_ARGUMENT, "the timestep must be positive and finite, got " + std::to_string(dt));
   if (int rc = require_deposit(r, "step")) return rc;
+  if (int rc = require_sources(r)) return rc;
   const Tableau t = tableau(r->cfg.scheme);
   int rc = engine_call(r, r->eng->step(dt, t.a, t.b, t.d, t.S));
   if (rc) return rc;
+  consume_sources(r);
   r->fields_epoch += 1;
   return GBGHT_OK;
 }
@@ -520,6 +575,10 @@ int gbght_ensemble_create(gbght_ensemble** out, gbght_run* const* members, int n
         g_global_error = "a run appears twice in the ensemble";
         return GBGHT_ERR_ARGUMENT;
       }
+    if (stochastic(members[i], 0) || stochastic(members[i], 1)) {
+      g_global_error = "a StochasticOU member takes its force per step; step it alone";
+      return GBGHT_ERR_ARGUMENT;
+    }
     if (members[i]->cfg.device != members[0]->cfg.device) {
       g_global_error = "the members must share one device";
       return GBGHT_ERR_ARGUMENT;
@@ -824,9 +883,11 @@ int gbght_advance(gbght_run* r, double dt, double* dt_taken) {
     return fail(r, GBGHT_ERR_SCHEDULE, "the tracers' last push was never closed by a particle deposit");
   if (tracers && r->sample_epoch != r->fields_epoch)
     return fail(r, GBGHT_ERR_SCHEDULE, "the fields were stepped alone since the tracers' last sample");
+  if (int rc = require_sources(r)) return rc;
   const Tableau t = tableau(r->cfg.scheme);
   int rc = engine_call(r, r->eng->step(D, t.a, t.b, t.d, t.S));
   if (rc) return rc;
+  consume_sources(r);
   r->fields_epoch += 1;
   if ((rc = do_deposit(r))) return rc;
   if (tracers) {

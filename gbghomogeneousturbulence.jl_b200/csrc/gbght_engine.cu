@@ -213,6 +213,13 @@ class EngineImpl final : public Engine {
       if ((err = alloc(&torder_, size_t(p.tracers) * sizeof(uint32_t)))) return err;
       if ((err = alloc(&tcount_, size_t(nbins_) * sizeof(uint32_t)))) return err;
     }
+    for (int f = 0; f < 2; ++f) {   // StochasticOU: the companion grid's force
+      const ForcingParams& fp = f == 0 ? p.vf : p.sf;
+      if (fp.kind != kForceStochastic) continue;
+      const int nc = 2 * (int(fp.highest_shell) + 1);
+      src_nc_[f] = nc;
+      if ((err = alloc(&src_[f], size_t(f == 0 ? 3 : 1) * nc * nc * (nc / 2 + 1) * sizeof(Cplx<double>)))) return err;
+    }
 #ifndef GBGHT_EMU
     if ((err = make_maps())) return err;
 #endif
@@ -425,6 +432,13 @@ class EngineImpl final : public Engine {
     return nullptr;
   }
 
+  const char* forcing_source(int field, const double* amplitudes, int nc) override {
+    if (field < 0 || field > 1 || !src_[field]) return "the field carries no StochasticOU forcing";
+    if (nc != src_nc_[field]) return "the force is given on a companion grid of another size";
+    if (where(amplitudes) < 0) return "the force is device memory of another device";
+    const size_t n = size_t(field == 0 ? 3 : 1) * nc * nc * (nc / 2 + 1) * sizeof(Cplx<double>);
+    return rt_copy(src_[field], amplitudes, n, stream_);
+  }
   const char* velocity_export(double* u) override {
     std::vector<T> host(3 * nP_);
     const char* err = rt_d2h(host.data(), U_, 3 * nP_ * sizeof(T), stream_);
@@ -1382,6 +1396,39 @@ class EngineImpl final : public Engine {
     pend();
 #endif
   }
+  // StochasticOU's force into the y-forward products (inject_source)
+  void inject() {
+    SourceArgs a{};
+    a.nc = src_nc_[0] ? src_nc_[0] : src_nc_[1];
+    if (src_[0] && src_[1] && src_nc_[0] != src_nc_[1]) {   // two companions of different sizes
+      SourceArgs b{};
+      b.nc = src_nc_[1];
+      b.sca = 1;
+      b.slo2 = sband_lo2();
+      b.shi2 = sband_hi2();
+      inject_launch(b);
+      a.nc = src_nc_[0];
+      a.vel = 1;
+    } else {
+      a.vel = src_[0] != nullptr;
+      a.sca = src_[1] != nullptr;
+      a.slo2 = sband_lo2();
+      a.shi2 = sband_hi2();
+    }
+    a.lo2 = band_lo2();
+    a.hi2 = band_hi2();
+    inject_launch(a);
+  }
+  void inject_launch(const SourceArgs& a) {
+    const long n = long(a.nc - 1) * (a.nc / 2) * N;
+#ifdef GBGHT_EMU
+    for (long t = 0; t < n; ++t) inject_source<T>(t, g_, A_, src_[0], src_[1], a);
+#else
+    pbegin(PROF_FORCE_AMP);
+    k_inject_source<T><<<unsigned((n + 255) / 256), 256, 0, stream_>>>(g_, A_, src_[0], src_[1], a);
+    pend();
+#endif
+  }
   void reality() {
     const int n = g_.NY2 * g_.NY2;
     const int nc = p_.scalar ? 4 : 3;
@@ -1492,6 +1539,7 @@ class EngineImpl final : public Engine {
     bu_fresh_ = false;
     x_products();
     y_forward(nfwd);
+    if (src_[0] || src_[1]) inject();
     if (st.forced || st.sforced) force_amp(st);
     if (amp_save_to_) {   // the adjoint's forward pass keeps the stage's amplitudes
       const char* e = rt_d2d(amp_save_to_, amp_, sizeof(double), stream_);
@@ -1576,6 +1624,8 @@ class EngineImpl final : public Engine {
   unsigned int* flag_ = nullptr;     // import: content outside the retained ball
   uint32_t *tkey_ = nullptr, *torder_ = nullptr, *tcount_ = nullptr;   // the traversal sort
   int nbins_ = 0;
+  Cplx<double>* src_[2] = {nullptr, nullptr};   // StochasticOU: each field's companion force
+  int src_nc_[2] = {0, 0};
   // the adjoint (allocated by adjoint_init): λ and λ_h, the saved stage states and amplitudes, the
   // adjoint A and B slots with their tensor maps, the band coefficients, the rates' gradients, the
   // snapshot slots

@@ -34,7 +34,10 @@ struct ForcingParams {
   int lowest_shell;
   double highest_shell;
 };
-enum ForcingKind { kForceNone = 0, kForceConstantPower = 1, kForceLinear = 2, kForceController = 3, kForceRescaling = 4 };
+enum ForcingKind {
+  kForceNone = 0, kForceConstantPower = 1, kForceLinear = 2, kForceController = 3, kForceRescaling = 4,
+  kForceStochastic = 5
+};
 
 // The parameters of a run that the engine needs (a copy of the public config, validated).
 struct RunParams {
@@ -83,6 +86,8 @@ class Engine {
   virtual void* cuda_stream() const = 0;
   virtual bool deposit_fresh() const = 0;
   virtual bool profiling() const = 0;
+  // a StochasticOU field's force for the next step: companion amplitudes [comp][nc][nc][nc/2+1]
+  virtual const char* forcing_source(int field, const double* amplitudes, int nc) = 0;
   virtual const char* velocity_export(double* u) = 0;
   virtual const char* velocity_import(const double* u) = 0;
   virtual const char* observables(Observables* o) = 0;

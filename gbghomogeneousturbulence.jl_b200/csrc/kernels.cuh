@@ -178,6 +178,10 @@ __global__ void __launch_bounds__(NT) k_det_sum(const T* s6, size_t n, size_t ch
   body_det_sum<T, NT>(c, red, s6, n, chunk, out);
 }
 template <class T>
+__global__ void k_inject_source(Geometry g, Cplx<T>* A, const Cplx<double>* su, const Cplx<double>* sp, SourceArgs a) {
+  inject_source<T>(long(blockIdx.x) * blockDim.x + threadIdx.x, g, A, su, sp, a);
+}
+template <class T>
 __global__ void k_reality(Geometry g, Cplx<T>* S, int ncomp) {
   reality_mode<T>(int(blockIdx.x * blockDim.x + threadIdx.x), g, S, ncomp);
 }

@@ -1243,6 +1243,67 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
 }
 
 // ================================================================================================
+// StochasticOU's force (src/Forcing.jl:1362-1415), added to a stage's right-hand side through the
+// products the z epilogue transforms last: after the y-forward pass, A holds the products
+// transformed in x and y, still physical in z. Adding g(z) = Σ_mz N²·a(m)·e^{2πi m_z z/N} to a
+// column (m_x, m_y) adds N³·a(m) to the z-transformed product at every m_z of the companion. The
+// velocity's force a_u is transverse, so the epilogue's Leray projection keeps it; the scalar's
+// force s enters the flux slots as f = iκ s/|κ|², whose −iκ·f the epilogue forms is s. Thread t
+// takes one column of the companion's retained box (|m_y| < Nc/2, 0 ≤ m_x < Nc/2) at one z. The
+// companion arrays are complex128 [comp][kz][ky][kx] (kx ≤ Nc/2); only band modes are added.
+// ================================================================================================
+struct SourceArgs {
+  int nc;                        // companion points per axis
+  int vel, sca;                  // which fields carry the force
+  double lo2, hi2, slo2, shi2;   // the bands, squared edges
+};
+template <class T>
+GBGHT_HD void inject_source(long t, const Geometry& g, Cplx<T>* A, const Cplx<double>* su, const Cplx<double>* sp,
+                            const SourceArgs& a) {
+  const int nc = a.nc, half = nc / 2, ncol = (nc - 1) * half;
+  if (t >= long(ncol) * g.N) return;
+  const int col = int(t % ncol), z = int(t / ncol);
+  const int mx = col % half, my = col / half - (half - 1);
+  const int qy = my >= 0 ? my : my + g.NY2;
+  const double n2 = double(g.N) * double(g.N);
+  const size_t comp = size_t(nc) * nc * (half + 1);
+  double acc[6][2] = {};
+  for (int mz = -(half - 1); mz <= half - 1; ++mz) {
+    const double kxd = g.s * mx, kyd = g.s * my, kzd = g.s * mz;
+    const double k2 = (kxd * kxd + kyd * kyd) + kzd * kzd;
+    const double th = 2.0 * double(mz) * double(z) / double(g.N);
+    double sn, cs;
+#ifdef __CUDA_ARCH__
+    sincospi(th, &sn, &cs);
+#else
+    sn = std::sin(M_PI * th);
+    cs = std::cos(M_PI * th);
+#endif
+    const size_t at = (size_t((mz + nc) % nc) * nc + size_t((my + nc) % nc)) * (half + 1) + mx;
+    if (a.vel && k2 >= a.lo2 && k2 <= a.hi2)
+      for (int c = 0; c < 3; ++c) {
+        const Cplx<double> v = su[c * comp + at];
+        acc[c][0] += n2 * (v.x * cs - v.y * sn);
+        acc[c][1] += n2 * (v.x * sn + v.y * cs);
+      }
+    if (a.sca && k2 >= a.slo2 && k2 <= a.shi2 && k2 > 0.0) {
+      const Cplx<double> v = sp[at];
+      const double kk[3] = {kxd, kyd, kzd};
+      for (int c = 0; c < 3; ++c) {   // f_c = i κ_c s/|κ|²
+        const double fr = -v.y * kk[c] / k2, fi = v.x * kk[c] / k2;
+        acc[3 + c][0] += n2 * (fr * cs - fi * sn);
+        acc[3 + c][1] += n2 * (fr * sn + fi * cs);
+      }
+    }
+  }
+  for (int c = 0; c < 6; ++c) {
+    if ((c < 3 && !a.vel) || (c >= 3 && !a.sca)) continue;
+    Cplx<T>& r = A[idxA(g, c, z, qy, mx)];
+    r = r + cmk<T>(T(acc[c][0]), T(acc[c][1]));
+  }
+}
+
+// ================================================================================================
 // Reality projection of the kx = 0 plane of S slots [0, ncomp) (src/Propagator.jl:411-412): each
 // pair (m_y, m_z) ↔ (−m_y, −m_z) is replaced by its Hermitian part. One thread per compact mode;
 // the member with the smaller flat index writes both. Grid covers NY2·NY2 threads.

@@ -18,6 +18,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import seed  # noqa: F401  (host-side seeding, re-exported)
+from . import stochastic as _stochastic
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "libgbght.so")
@@ -26,6 +27,7 @@ FP64, FP32_MIXED = 0, 1
 IFRK4, IFRK3, IFHEUN, IFSSPRK3 = 0, 1, 2, 3
 SCHEMES = {"IFLowStorageRK4": IFRK4, "IFLowStorageRK3": IFRK3, "IFHeun": IFHEUN, "IFSSPRK3": IFSSPRK3}
 FORCING_NONE, FORCING_CONSTANT_POWER, FORCING_LINEAR, FORCING_VARIANCE_CONTROLLER, FORCING_VARIANCE_RESCALING = 0, 1, 2, 3, 4
+FORCING_STOCHASTIC_OU = 5
 OVER = {"band": 0, "total": 1}
 TRACER_SCHEMES = {"Heun": 0, "ABM": 1, "AB": 2}
 OK, ERR_ARGUMENT, ERR_SCHEDULE, ERR_CUDA, ERR_DEVICE = 0, 1, 2, 3, 4
@@ -86,6 +88,7 @@ _SIGNATURES = {
     "gbght_state_import": (C.c_int, [C.c_void_p, _DP, _DP]),
     "gbght_state_export": (C.c_int, [C.c_void_p, _DP, _DP]),
     "gbght_step": (C.c_int, [C.c_void_p, C.c_double]),
+    "gbght_forcing_source_set": (C.c_int, [C.c_void_p, C.c_int, _DP, C.c_int]),
     "gbght_recommended_cfl": (C.c_int, [C.c_int, _DP]),
     "gbght_ensemble_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int]),
     "gbght_ensemble_destroy": (None, [C.c_void_p]),
@@ -225,6 +228,19 @@ class VarianceRescaling:
 
 
 @dataclass
+class StochasticOU:
+    """`StochasticOU(domain; forcing_variance, correlation_time, lowest_shell = 1, highest_shell = 2,
+    seed)` (src/Forcing.jl:1224-1415): an additive Ornstein–Uhlenbeck force on the band, advanced
+    once per step on the host (`gbght.stochastic.OUProcess`) and handed to the library before the
+    step."""
+    forcing_variance: float
+    correlation_time: float
+    lowest_shell: int = 1
+    highest_shell: int = 2
+    seed: int = 0
+
+
+@dataclass
 class NoForcing:
     """`NoForcing()` (src/Forcing.jl): a freely decaying field."""
 
@@ -241,6 +257,8 @@ def _fill_forcing(p: ForcingParams, f, who: str) -> None:
     elif isinstance(f, VarianceController):
         p.kind, p.target, p.gain, p.turnover_time = (FORCING_VARIANCE_CONTROLLER, float(f.target), float(f.gain),
                                                       float(f.turnover_time))
+    elif isinstance(f, StochasticOU):
+        p.kind, p.target, p.turnover_time = FORCING_STOCHASTIC_OU, float(f.forcing_variance), float(f.correlation_time)
     elif isinstance(f, VarianceRescaling):
         if f.over not in OVER:
             raise ValueError(f"VarianceRescaling `over` must be :band or :total; got :{f.over}")
@@ -315,6 +333,13 @@ class Run:
         cut = C.c_double()
         self.lib.gbght_geometry(self.h, C.byref(K), C.byref(cut))
         self.K, self.cutoff = K.value, cut.value
+        # StochasticOU fields: the host processes (the stationary start is drawn here)
+        self.processes = {}
+        for field, f in ((0, setup.velocity_forcing), (1, setup.scalar_forcing)):
+            if isinstance(f, StochasticOU):
+                self.processes[field] = _stochastic.OUProcess(f.forcing_variance, f.correlation_time, f.lowest_shell,
+                                                              f.highest_shell, f.seed, vector=field == 0,
+                                                              L=setup.side_length)
 
     def close(self):
         if getattr(self, "h", None):
@@ -392,7 +417,20 @@ class Run:
         return u, p
 
     # -- the field step (step!, deposit!) ----------------------------------------------------------
+    def set_forcing_source(self, field: int, amplitudes: np.ndarray):
+        """A StochasticOU field's force for the next step (companion amplitudes, reference layout)."""
+        a = np.ascontiguousarray(amplitudes, dtype=np.complex128)
+        self._check(self.lib.gbght_forcing_source_set(self.h, int(field), a.view(np.float64).ctypes.data_as(_DP),
+                                                      a.shape[-2]))
+
+    def _prepare_forcing(self, dt: float):
+        """`prepare_forcing!` (src/Forcing.jl:1401-1411): one OU transition of each StochasticOU
+        field's process over dt, handed to the library."""
+        for field, proc in self.processes.items():
+            self.set_forcing_source(field, proc.advance(dt))
+
     def step(self, dt: float):
+        self._prepare_forcing(dt)
         self._check(self.lib.gbght_step(self.h, float(dt)))
 
     def deposit(self):
@@ -518,6 +556,9 @@ class Run:
 
     # -- run layer (advance!) ------------------------------------------------------------------------
     def advance(self, dt: float | None = None) -> float:
+        if self.processes:   # the process needs the step's Δt before the step
+            dt = self.cfl_timestep() if dt is None else dt
+            self._prepare_forcing(dt)
         taken = C.c_double()
         self._check(self.lib.gbght_advance(self.h, 0.0 if dt is None else float(dt), C.byref(taken)))
         return taken.value

@@ -55,13 +55,21 @@ enum gbght_scheme { GBGHT_IFRK4 = 0, GBGHT_IFRK3 = 1, GBGHT_IFHEUN = 2, GBGHT_IF
  *  VARIANCE_RESCALING   VarianceRescaling (:575-596): after the step, the band is rescaled by one
  *                       factor so the band's (`over` = 0) or the whole field's (`over` = 1)
  *                       variance equals `target`. First order in time, as in the reference.
+ *  STOCHASTIC_OU        StochasticOU (:1224-1415): an additive force, the same at every stage of a
+ *                       step, held on a companion grid of Nc = 2·(highest_shell + 1) points and
+ *                       advanced once per step on the host (an Ornstein–Uhlenbeck process with
+ *                       stationary mean square `target` = σ² and correlation time `turnover_time`
+ *                       = T_L). The caller hands each step's force in by gbght_forcing_source_set
+ *                       before the step; highest_shell must be finite and its band inside the
+ *                       retained 2/3 ball.
  * The variance is ½⟨|u|²⟩ for the velocity and ⟨φ²⟩ for the scalar (src/Forcing.jl:456). */
 enum gbght_forcing {
   GBGHT_FORCING_NONE = 0,
   GBGHT_FORCING_CONSTANT_POWER = 1,
   GBGHT_FORCING_LINEAR = 2,
   GBGHT_FORCING_VARIANCE_CONTROLLER = 3,
-  GBGHT_FORCING_VARIANCE_RESCALING = 4
+  GBGHT_FORCING_VARIANCE_RESCALING = 4,
+  GBGHT_FORCING_STOCHASTIC_OU = 5
 };
 enum gbght_rescaling_over { GBGHT_OVER_BAND = 0, GBGHT_OVER_TOTAL = 1 };
 
@@ -142,6 +150,17 @@ int gbght_geometry(const gbght_run* run, int* K, double* cutoff);
  * ext/GBGHomogeneousTurbulenceHDF5Ext.jl. */
 int gbght_state_import(gbght_run* run, const double* u_hat, const double* phi_hat);
 int gbght_state_export(gbght_run* run, double* u_hat, double* phi_hat);
+
+/* The force of a StochasticOU field (field 0 velocity, 1 scalar) for the next step: its physical
+ * amplitudes a_k (the coefficients of e^{iκ·x}) on the companion grid, complex128 in the companion's
+ * reference layout [comp][kz][ky][kx] (kx ≤ Nc/2, 3 components for the velocity, 1 for the scalar),
+ * host or device memory. Every stage of the next step adds N³·a_k to the field's right-hand side on
+ * the forcing's band, where the run's modes and the companion's coincide. Each step consumes the
+ * force: a step of a StochasticOU field without a force set since the last step is refused with
+ * SCHEDULE, as the reference advances the process once per step (prepare_forcing!,
+ * src/Forcing.jl:1401-1411). Replaces _advance_process! / add_forcing_source!(::StochasticOU)
+ * (:1362-1415); the host draws and transforms, as the reference's draws are made on the host. */
+int gbght_forcing_source_set(gbght_run* run, int field, const double* amplitudes, int companion_points);
 
 /* One field step of the configured scheme with step dt > 0, in place. Requires a current field
  * deposit, i.e. gbght_deposit after the last state change; otherwise SCHEDULE. The step advances

@@ -209,6 +209,34 @@ class VarianceRescaling:
 
 
 @dataclass
+class StochasticOU:
+    """`StochasticOU(domain; forcing_variance, correlation_time, lowest_shell, highest_shell, seed)`
+    (src/Forcing.jl:1224-1415): an additive force held on a companion grid and advanced once per
+    step on the host. Here `process` is the force for the current step, the companion's physical
+    amplitudes a_k in its reference layout (set from outside before each step, the same arrays the
+    library is given); `add_forcing_source!` (:1415) becomes N̂ += N³·a_k where the run's modes and
+    the companion's coincide (`embed_modes!`)."""
+    forcing_variance: float
+    correlation_time: float
+    lowest_shell: int = 1
+    highest_shell: int = 2
+    process: np.ndarray | None = None
+
+
+def embed_modes(dom: Domain, a: np.ndarray) -> np.ndarray:
+    """The companion's modes m (|m_a| < Nc/2, kx < Nc/2) carried into the run's half spectrum,
+    zero elsewhere."""
+    n = a.shape[-2]
+    N = dom.N
+    out = np.zeros(a.shape[:-3] + dom.shape_spectral, np.complex128)
+    for mz in range(-(n // 2) + 1, n // 2):
+        for my in range(-(n // 2) + 1, n // 2):
+            for mx in range(0, n // 2):
+                out[..., mz % N, my % N, mx] = a[..., mz % n, my % n, mx]
+    return out
+
+
+@dataclass
 class Conditions:
     viscosity: float
     schmidt: float = 1.0
@@ -272,10 +300,13 @@ def constant_power_amplitude(dom: Domain, forcing, fh: np.ndarray, eps_T: float,
 
 
 def stage_source(dom: Domain, forcing, fh: np.ndarray, eps_T: float, diffusivity: float):
-    """The additive source of a per-stage forcing (ConstantPower, VarianceController), else None."""
+    """The additive source of a per-stage forcing (ConstantPower, VarianceController,
+    StochasticOU), else None."""
     if isinstance(forcing, (ConstantPower, VarianceController)):
         A, band = constant_power_amplitude(dom, forcing, fh, eps_T, diffusivity)
         return A * band * fh
+    if isinstance(forcing, StochasticOU):
+        return float(dom.N) ** 3 * embed_modes(dom, forcing.process)
     return None
 
 

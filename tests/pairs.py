@@ -30,6 +30,8 @@ def oracle_forcing(f):
         return O.Linear(f.rate, f.lowest_shell, f.highest_shell)
     if isinstance(f, gbght.VarianceController):
         return O.VarianceController(f.target, f.turnover_time, f.gain, f.lowest_shell, f.highest_shell)
+    if isinstance(f, gbght.StochasticOU):
+        return O.StochasticOU(f.forcing_variance, f.correlation_time, f.lowest_shell, f.highest_shell)
     if isinstance(f, gbght.VarianceRescaling):
         return O.VarianceRescaling(f.target, f.over, f.lowest_shell, f.highest_shell)
     raise ValueError(f"no oracle forcing for {f!r}")
