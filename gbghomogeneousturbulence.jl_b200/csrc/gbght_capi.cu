@@ -308,6 +308,9 @@ void gbght_config_default(gbght_config* c) {
   c->cfl = 0.5;
   c->max_dt = INFINITY;
   c->device = 0;
+  c->interpolation = GBGHT_CATMULL_ROM;
+  c->interpolation_points = 4;
+  c->interpolation_smoothness = 1;
 }
 
 int gbght_recommended_cfl(int scheme, double* cfl) {
@@ -379,6 +382,16 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
   } else {
     return bad("unknown particle integration scheme");
   }
+  gbght::Stencil stencil{};
+  if (cfg->interpolation != GBGHT_CATMULL_ROM) {
+    if (cfg->interpolation != GBGHT_LALESCU && cfg->interpolation != GBGHT_LAGRANGE)
+      return bad("unknown interpolation scheme");
+    if (const char* e = gbght::make_stencil(cfg->interpolation, cfg->interpolation_points,
+                                            cfg->interpolation_smoothness, &stencil))
+      return bad(e);
+    if (cfg->interpolation_points > cfg->grid_points_per_axis)
+      return bad("the interpolation stencil is wider than the grid");
+  }
   if (!finite_positive(cfg->cfl)) return bad("cfl must be positive and finite");
   if (!(cfg->max_dt > 0)) return bad("max_dt must be positive");
 
@@ -401,6 +414,7 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
   for (int i = 0; i < 3; ++i) p.G[i] = cfg->mean_gradient[i];
   p.tracers = cfg->tracers;
   p.trail_capacity = cfg->tracer_steps;
+  p.stencil = stencil;
   p.device = cfg->device;
   if (const char* e = r->eng->init(p)) {
     g_global_error = e;
@@ -1057,8 +1071,9 @@ int gbght_snapshot_load(gbght_run* r, int slot) {
 
 int gbght_adjoint_advance(gbght_run* r, double dt) {
   if (check_run(r)) return GBGHT_ERR_ARGUMENT;
-  if (r->cfg.tracers <= 0 || r->cfg.tracer_scheme != GBGHT_HEUN)
-    return fail(r, GBGHT_ERR_ARGUMENT, "the adjoint of an iteration's tracer push is built for Heun tracers");
+  if (r->cfg.tracers <= 0 || r->cfg.tracer_scheme != GBGHT_HEUN || r->cfg.interpolation != GBGHT_CATMULL_ROM)
+    return fail(r, GBGHT_ERR_ARGUMENT, "the adjoint of an iteration's tracer push is built for Heun tracers with "
+                                       "CatmullRom interpolation");
   if (!finite_positive(dt))
     return fail(r, GBGHT_ERR_ARGUMENT, "the timestep must be positive and finite, got " + std::to_string(dt));
   if (r->trail_count == 0 || !r->sample_at_positions)
@@ -1085,6 +1100,8 @@ int gbght_adjoint_tracers_export(gbght_run* r, double* lam_X, double* lam_f) {
 
 int gbght_adjoint_deposit_tracers(gbght_run* r) {
   if (check_run(r)) return GBGHT_ERR_ARGUMENT;
+  if (r->cfg.interpolation != GBGHT_CATMULL_ROM)
+    return fail(r, GBGHT_ERR_ARGUMENT, "the adjoint of the particle deposit is built for CatmullRom interpolation");
   if (int rc = require_deposit(r, "adjoint of the particle deposit")) return rc;
   return engine_call(r, r->eng->adjoint_deposit_tracers());
 }

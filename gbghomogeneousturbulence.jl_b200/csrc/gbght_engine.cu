@@ -642,7 +642,9 @@ class EngineImpl final : public Engine {
     for (int j = 0; j < w.J; ++j)
       if (w.slot[j] < 0 || w.slot[j] >= p_.trail_capacity) return "bad tracer step";
     if (const char* e = rebuild_traversal()) return e;
-    run_tracers(p_.tracers, X_, F_, w, torder_);
+    AdamsStep ws = w;
+    ws.stencil = p_.stencil;
+    run_tracers(p_.tracers, X_, F_, ws, torder_);
     return rt_check();
   }
   const char* gather(const double* X, int64_t M, double* out) override {
@@ -653,6 +655,7 @@ class EngineImpl final : public Engine {
     if (!err) err = rt_h2d(dX, X, 3 * size_t(M) * sizeof(double), stream_);
     if (!err) {
       AdamsStep w{};   // a gather alone, into slot 0 of a one-slot trail
+      w.stencil = p_.stencil;
       run_tracers(M, dX, dF, w);
       err = rt_check();
     }

@@ -52,6 +52,7 @@ struct RunParams {
   double G[3];
   int64_t tracers;
   int trail_capacity;        // sample slots of the tracers' trail (the Adams scheme's k)
+  Stencil stencil;           // the tracers' interpolation weights (n = 0: Catmull–Rom)
   int device;
 };
 

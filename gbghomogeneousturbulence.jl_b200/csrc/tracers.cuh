@@ -7,6 +7,8 @@
 
 #include "gbght_common.cuh"
 
+#include <utility>
+
 namespace gbght {
 
 GBGHT_HD double add_rn(double a, double b) {
@@ -109,6 +111,170 @@ GBGHT_HD void gather3(const T* GBGHT_RESTRICT u, int N, double dx, double x, dou
   }
 }
 
+// ================================================================================================
+// Wider interpolation stencils (src/Particles.jl:61-70; the schemes of GBGPeriodicFields, which is
+// not vendored, restated from their published definitions):
+//  - LagrangeSpline(n): the degree n − 1 Lagrange polynomial through the n taps around the cell;
+//  - LalescuSpline(n; smoothness m) (Lalescu, Teaca & Carati 2010): on each cell, the degree 2m + 1
+//    Hermite polynomial matching at both ends the value and the derivatives 1..m, each derivative
+//    estimated by the centred difference of the (n − 1)-point Lagrange polynomial about that end.
+//    LalescuSpline(4; 1) is Catmull–Rom.
+// Either is a set of n weight polynomials w_j(t), j = 0..n−1 for the taps i − n/2 + 1 + j at the
+// fraction t of cell i; their coefficients are built once on the host (make_stencil).
+// ================================================================================================
+constexpr int kStencilMax = 8;
+struct Stencil {
+  int n;                                     // taps per axis; 0 selects the Catmull–Rom gather above
+  int deg;                                   // the weights' polynomial degree
+  double c[kStencilMax][kStencilMax];        // w_j(t) = Σ_d c[j][d]·t^d
+};
+
+GBGHT_HD void stencil_weights(const Stencil& s, double t, double* w) {
+  for (int j = 0; j < s.n; ++j) {
+    double v = s.c[j][s.deg];
+    for (int d = s.deg - 1; d >= 0; --d) v = fma(v, t, s.c[j][d]);
+    w[j] = v;
+  }
+}
+
+// The gather of gatherN: the sums run x innermost, then y, then z.
+template <class T>
+GBGHT_HD void gatherN(const T* GBGHT_RESTRICT u, int N, double dx, double x, double y, double z, const Stencil& s,
+                      double out[3]) {
+  int ix, iy, iz;
+  double tx, ty, tz;
+  cell_fraction(x, dx, N, ix, tx);
+  cell_fraction(y, dx, N, iy, ty);
+  cell_fraction(z, dx, N, iz, tz);
+  double wx[kStencilMax], wy[kStencilMax], wz[kStencilMax];
+  stencil_weights(s, tx, wx);
+  stencil_weights(s, ty, wy);
+  stencil_weights(s, tz, wz);
+  const int off = s.n / 2 - 1;
+  const size_t comp = size_t(N) * N * N;
+  for (int c = 0; c < 3; ++c) {
+    const T* f = u + c * comp;
+    double acc_z = 0.0;
+    for (int cz = 0; cz < s.n; ++cz) {
+      const int zz = ((iz + cz - off) % N + N) % N;
+      double acc_y = 0.0;
+      for (int cy = 0; cy < s.n; ++cy) {
+        const int yy = ((iy + cy - off) % N + N) % N;
+        const T* row = f + (size_t(zz) * N + yy) * N;
+        double acc_x = 0.0;
+        for (int cx = 0; cx < s.n; ++cx) acc_x = add_rn(acc_x, mul_rn(wx[cx], double(ldg(row + ((ix + cx - off) % N + N) % N))));
+        acc_y = add_rn(acc_y, mul_rn(wy[cy], acc_x));
+      }
+      acc_z = add_rn(acc_z, mul_rn(wz[cz], acc_y));
+    }
+    out[c] = acc_z;
+  }
+}
+
+// The configured gather: Catmull–Rom (n = 0), or a wider stencil.
+template <class T>
+GBGHT_HD void gather_any(const T* GBGHT_RESTRICT u, int N, double dx, double x, double y, double z, const Stencil& s,
+                         double out[3]) {
+  if (s.n == 0) gather3(u, N, dx, x, y, z, out);
+  else gatherN(u, N, dx, x, y, z, s, out);
+}
+
+// Host: the coefficients of a stencil. kind 1 LalescuSpline(n; m), 2 LagrangeSpline(n); n even in
+// [4, 8]; 1 ≤ m ≤ min(3, n − 2). Returns nullptr, or why the stencil is refused.
+inline const char* make_stencil(int kind, int n, int m, Stencil* s) {
+  *s = Stencil{};
+  if (n < 4 || n > kStencilMax || n % 2) return "the stencil width must be 4, 6 or 8 points per axis";
+  const int off = n / 2 - 1;
+  // p ← p·(t − a)/b, coefficients in increasing degree
+  const auto mul_lin = [](double* p, int deg, double a, double b) {
+    for (int d = deg + 1; d >= 0; --d) p[d] = ((d > 0 ? p[d - 1] : 0.0) - a * p[d]) / b;
+  };
+  if (kind == 2) {   // Lagrange through the taps x_j = j − off
+    s->n = n;
+    s->deg = n - 1;
+    for (int j = 0; j < n; ++j) {
+      double p[kStencilMax + 1] = {1.0};
+      int deg = 0;
+      for (int q = 0; q < n; ++q) {
+        if (q == j) continue;
+        mul_lin(p, deg, double(q - off), double(j - q));
+        ++deg;
+      }
+      for (int d = 0; d < n; ++d) s->c[j][d] = p[d];
+    }
+    return nullptr;
+  }
+  if (kind != 1) return "unknown interpolation scheme";
+  if (m < 1 || m > 3 || m > n - 2) return "LalescuSpline's smoothness must lie in [1, min(3, n − 2)]";
+  const int D = 2 * m + 1;   // Hermite degree
+  // d[e][k][j]: the k-th derivative at end e (t = 0, 1) of the (n − 1)-point Lagrange polynomial
+  // centred there, as weights on the taps
+  double dk[2][4][kStencilMax] = {};
+  for (int e = 0; e < 2; ++e) {
+    const int np = n - 1, half = (np - 1) / 2;
+    for (int i = 0; i < np; ++i) {
+      const int si = i - half;   // point relative to the end
+      double p[kStencilMax + 1] = {1.0};
+      int deg = 0;
+      for (int q = 0; q < np; ++q) {
+        if (q == i) continue;
+        mul_lin(p, deg, double(q - half), double(si - (q - half)));
+        ++deg;
+      }
+      const int tap = e + si + off;   // stencil tap of point si about end e
+      double fact = 1.0;
+      for (int k = 0; k <= m; ++k) {
+        if (k > 0) fact *= k;
+        dk[e][k][tap] += fact * p[k];
+      }
+    }
+  }
+  // the Hermite basis: H[e][k](t) of degree D with H^(l)(e') = δ(e, e')·δ(k, l), l ≤ m
+  double Amat[8][9];
+  double H[2][4][8] = {};
+  for (int e = 0; e < 2; ++e)
+    for (int k = 0; k <= m; ++k) {
+      // rows: the conditions (end e', derivative l); columns: monomials t^d, d ≤ D; last column rhs
+      for (int ee = 0; ee < 2; ++ee)
+        for (int l = 0; l <= m; ++l) {
+          const int row = ee * (m + 1) + l;
+          for (int d = 0; d <= D; ++d) {
+            double v = 0.0;
+            if (d >= l) {
+              double f = 1.0;
+              for (int r = 0; r < l; ++r) f *= double(d - r);
+              v = ee == 0 ? (d == l ? f : 0.0) : f;   // d^l/dt^l t^d at 0 or 1
+            }
+            Amat[row][d] = v;
+          }
+          Amat[row][D + 1] = (ee == e && l == k) ? 1.0 : 0.0;
+        }
+      const int R = D + 1;
+      for (int col = 0; col < R; ++col) {   // Gauss–Jordan with partial pivoting
+        int piv = col;
+        for (int r = col + 1; r < R; ++r)
+          if (std::fabs(Amat[r][col]) > std::fabs(Amat[piv][col])) piv = r;
+        for (int q = 0; q <= R; ++q) std::swap(Amat[col][q], Amat[piv][q]);
+        for (int r = 0; r < R; ++r) {
+          if (r == col) continue;
+          const double fct = Amat[r][col] / Amat[col][col];
+          for (int q = col; q <= R; ++q) Amat[r][q] -= fct * Amat[col][q];
+        }
+      }
+      for (int d = 0; d <= D; ++d) H[e][k][d] = Amat[d][R] / Amat[d][d];
+    }
+  s->n = n;
+  s->deg = D;
+  for (int j = 0; j < n; ++j)
+    for (int d = 0; d <= D; ++d) {
+      double v = 0.0;
+      for (int e = 0; e < 2; ++e)
+        for (int k = 0; k <= m; ++k) v += dk[e][k][j] * H[e][k][d];
+      s->c[j][d] = v;
+    }
+  return nullptr;
+}
+
 // Traversal order (src/Particles.jl:220-271): tracers are visited tile by tile, in tiles of 8³
 // cells, so the 64-point gathers of neighbouring threads share cache lines. Only the visiting
 // order changes; every tracer's arithmetic is the same. The key is the tile of the cell that
@@ -138,6 +304,7 @@ struct AdamsStep {
   double b[kTrailMax];      // predictor weights
   double beta_star;         // corrector weight on f*
   double beta_m[kTrailMax]; // corrector weights β_{j+1} − b_j
+  Stencil stencil;          // the interpolation scheme's weights (n = 0: Catmull–Rom)
 };
 
 // One tracer. X is [3][M]; F is the trail's slots, 3·M doubles apart. Each displacement is summed
@@ -158,7 +325,7 @@ GBGHT_HD void tracer_one(int64_t p, int64_t M, const T* GBGHT_RESTRICT u, int N,
     for (int c = 0; c < 3; ++c) xs[c] = wrap_periodic(add_rn(x[c], disp[c]), L);
     if (w.corrected) {
       double fs[3];
-      gather3(u, N, dx, xs[0], xs[1], xs[2], fs);
+      gather_any(u, N, dx, xs[0], xs[1], xs[2], w.stencil, fs);
       for (int c = 0; c < 3; ++c) disp[c] = mul_rn(w.beta_star, fs[c]);
       for (int j = 0; j < w.J; ++j)
         for (int c = 0; c < 3; ++c)
@@ -171,7 +338,7 @@ GBGHT_HD void tracer_one(int64_t p, int64_t M, const T* GBGHT_RESTRICT u, int N,
   }
   if (w.out_slot < 0) return;
   double f[3];
-  gather3(u, N, dx, x[0], x[1], x[2], f);
+  gather_any(u, N, dx, x[0], x[1], x[2], w.stencil, f);
   for (int c = 0; c < 3; ++c) F[size_t(w.out_slot) * S3 + size_t(c) * M + p] = f[c];
 }
 

@@ -73,6 +73,9 @@ class Config(C.Structure):
         ("tracer_scheme", C.c_int),
         ("tracer_steps", C.c_int),
         ("shortened_first_steps", C.c_int),
+        ("interpolation", C.c_int),
+        ("interpolation_points", C.c_int),
+        ("interpolation_smoothness", C.c_int),
     ]
 
 
@@ -286,6 +289,7 @@ class Setup:
     tracer_scheme: str = "Heun"      # "Heun" (= ABM(1)), "ABM" or "AB" (src/ParticlePropagator.jl)
     tracer_steps: int = 1            # k of ABM(k) / AB(k)
     shortened_first_steps: bool = False
+    interpolation: tuple = ("CatmullRom", 4, 1)   # ("LalescuSpline", n, smoothness) or ("LagrangeSpline", n, 0)
     cfl: float = 0.5
     max_dt: float = math.inf
     device: int = 0
@@ -319,6 +323,12 @@ class Run:
         cfg.tracer_scheme = TRACER_SCHEMES[setup.tracer_scheme]
         cfg.tracer_steps = int(setup.tracer_steps)
         cfg.shortened_first_steps = 1 if setup.shortened_first_steps else 0
+        kinds = {"CatmullRom": 0, "LalescuSpline": 1, "LagrangeSpline": 2}
+        if setup.interpolation[0] not in kinds:
+            raise ValueError(f"unknown interpolation scheme {setup.interpolation[0]!r}")
+        cfg.interpolation = kinds[setup.interpolation[0]]
+        cfg.interpolation_points = int(setup.interpolation[1])
+        cfg.interpolation_smoothness = int(setup.interpolation[2])
         cfg.cfl = float(setup.cfl)
         cfg.max_dt = float(setup.max_dt)
         cfg.device = int(setup.device)

@@ -117,11 +117,22 @@ typedef struct gbght_config {
   int tracer_steps;          /* k of ABM(k) / AB(k); 1 for Heun. The trail keeps k samples */
   int shortened_first_steps; /* 1: shorten the first steps while a k > 1 scheme's trail fills
                                 (src/SimulationRun.jl:1099-1132); a fixed dt is then refused */
+  int interpolation;          /* gbght_interpolation: the tracers' grid→point scheme */
+  int interpolation_points;   /* stencil width per axis, 4, 6 or 8 (Lalescu, Lagrange) */
+  int interpolation_smoothness; /* LalescuSpline's order of continuity, 1..min(3, points − 2) */
 } gbght_config;
+
+/* The tracers' interpolation schemes (src/Particles.jl:61-70, schemes of GBGPeriodicFields):
+ * CatmullRom = LalescuSpline(4) (the default); LalescuSpline(n; smoothness m), the degree 2m + 1
+ * Hermite polynomial per cell with the derivatives from centred (n − 1)-point differences
+ * (Lalescu, Teaca & Carati 2010); LagrangeSpline(n), the degree n − 1 Lagrange polynomial through
+ * the n taps. The adjoint of the tracers is built for CatmullRom. */
+enum gbght_interpolation { GBGHT_CATMULL_ROM = 0, GBGHT_LALESCU = 1, GBGHT_LAGRANGE = 2 };
 
 /* Fill `cfg` with the defaults: N=64, L=2π, FP64, IF-RK4, ν=0.01, Sc=1, scalar on, no forcing
  * of either field (each forcing block: rate 0, target 0, gain 1, turnover time 0, over = band,
- * shells 1–2), G=0, no tracers, Heun, no shortened start, CFL 0.5, max_dt=∞, device 0. */
+ * shells 1–2), G=0, no tracers, Heun, no shortened start, CFL 0.5, max_dt=∞, device 0,
+ * Catmull–Rom interpolation (4 points, smoothness 1). */
 void gbght_config_default(gbght_config* cfg);
 
 /* Build a run on a FixedDomain with TwoThirds dealiasing, with its generator and registers.

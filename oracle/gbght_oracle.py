@@ -1026,10 +1026,59 @@ def cell_and_fraction(x: np.ndarray, dx: float):
     return i.astype(np.int64), q - i
 
 
-def interpolate(dom: Domain, f: np.ndarray, X: np.ndarray) -> np.ndarray:
-    """CatmullRom (= LalescuSpline(4)) gather of the physical field f ([comp][z][y][x] or
-    [z][y][x]) at positions X (3, M) (`interpolate!`, src/Particles.jl:290-293). The sum runs
-    x innermost, then y, then z."""
+def stencil_polynomials(scheme) -> np.ndarray:
+    """The weight polynomials of a wider interpolation scheme (src/Particles.jl:61-70, schemes of
+    the unvendored GBGPeriodicFields, restated from their published definitions), as a (n, degree+1)
+    array of coefficients in increasing degree for taps i − n/2 + 1 + j at fraction t:
+    ("LagrangeSpline", n, _): the Lagrange basis through the taps; ("LalescuSpline", n, m) (Lalescu,
+    Teaca & Carati 2010): the degree 2m + 1 Hermite interpolant on the cell, its derivatives 1..m at
+    each end taken from the (n − 1)-point polynomial centred there (fitted exactly with polyfit)."""
+    kind, n, m = scheme
+    off = n // 2 - 1
+    taps = np.arange(n) - off
+    if kind == "LagrangeSpline":
+        out = np.zeros((n, n))
+        for j in range(n):
+            others = np.delete(taps, j).astype(float)
+            poly = np.polynomial.polynomial.polyfromroots(others) / np.prod(taps[j] - others)
+            out[j] = poly
+        return out
+    if kind != "LalescuSpline":
+        raise ValueError(f"unknown interpolation scheme {kind!r}")
+    D = 2 * m + 1
+    # derivative estimates: for each end e and order k, weights on the taps
+    deriv = np.zeros((2, m + 1, n))
+    for e in (0, 1):
+        pts = np.arange(-(n // 2 - 1), n // 2)   # n − 1 points centred on the end
+        for i, si in enumerate(pts):
+            y = np.zeros(len(pts))
+            y[i] = 1.0
+            c = np.polynomial.polynomial.polyfit(pts.astype(float), y, len(pts) - 1)
+            for k in range(m + 1):
+                deriv[e, k, e + si + off] += math.factorial(k) * (c[k] if k < len(c) else 0.0)
+    # Hermite basis on [0, 1]
+    rows = []
+    for e in (0, 1):
+        for ell in range(m + 1):
+            rows.append([(math.factorial(d) / math.factorial(d - ell) if d >= ell else 0.0) * (float(e) ** (d - ell) if d > ell else 1.0)
+                         if (e == 1 or d == ell) else 0.0 for d in range(D + 1)])
+    V = np.array(rows)
+    out = np.zeros((n, D + 1))
+    for e in (0, 1):
+        for k in range(m + 1):
+            rhs = np.zeros(D + 1)
+            rhs[e * (m + 1) + k] = 1.0
+            H = np.linalg.solve(V, rhs)
+            out += np.outer(deriv[e, k], H)
+    return out
+
+
+def interpolate(dom: Domain, f: np.ndarray, X: np.ndarray, scheme=None) -> np.ndarray:
+    """The gather of the physical field f ([comp][z][y][x] or [z][y][x]) at positions X (3, M)
+    (`interpolate!`, src/Particles.jl:290-293): CatmullRom (= LalescuSpline(4)) by default, or a
+    wider scheme (see `stencil_polynomials`). The sum runs x innermost, then y, then z."""
+    if scheme is not None and tuple(scheme) != ("CatmullRom", 4, 1):
+        return _interpolate_stencil(dom, f, X, stencil_polynomials(scheme))
     N = dom.N
     scalar = f.ndim == 3
     comps = f[None] if scalar else f
@@ -1056,7 +1105,36 @@ def interpolate(dom: Domain, f: np.ndarray, X: np.ndarray) -> np.ndarray:
     return out[0] if scalar else out
 
 
-def advect_adams(dom: Domain, X: np.ndarray, samples, times, u_new: np.ndarray, h: float, corrected: bool):
+def _interpolate_stencil(dom: Domain, f: np.ndarray, X: np.ndarray, polys: np.ndarray) -> np.ndarray:
+    N, n = dom.N, polys.shape[0]
+    off = n // 2 - 1
+    scalar = f.ndim == 3
+    comps = f[None] if scalar else f
+    cells, weights = [], []
+    for a in range(3):
+        i, t = cell_and_fraction(X[a], dom.dx)
+        cells.append(i)
+        weights.append([np.polynomial.polynomial.polyval(t, polys[j]) for j in range(n)])
+    (ix, iy, iz), (wx, wy, wz) = cells, weights
+    out = np.zeros((comps.shape[0], X.shape[1]))
+    for c in range(comps.shape[0]):
+        acc_z = np.zeros(X.shape[1])
+        for cz in range(n):
+            zz = (iz + cz - off) % N
+            acc_y = np.zeros(X.shape[1])
+            for cy in range(n):
+                yy = (iy + cy - off) % N
+                acc_x = np.zeros(X.shape[1])
+                for cx in range(n):
+                    acc_x = acc_x + wx[cx] * comps[c][zz, yy, (ix + cx - off) % N]
+                acc_y = acc_y + wy[cy] * acc_x
+            acc_z = acc_z + wz[cz] * acc_y
+        out[c] = acc_z
+    return out[0] if scalar else out
+
+
+def advect_adams(dom: Domain, X: np.ndarray, samples, times, u_new: np.ndarray, h: float, corrected: bool,
+                 scheme=None):
     """One step of the Adams family (`_advance_positions!`, src/ParticlePropagator.jl:282-307) over
     the J samples f_{n−j} (newest first) taken at `times` (newest first): the predictor
     X* = wrap(X + Σ_j b_j f_{n−j}) with b the weights through the nodes t_{n−j} − t_n, and, when
@@ -1072,7 +1150,7 @@ def advect_adams(dom: Domain, X: np.ndarray, samples, times, u_new: np.ndarray, 
     Xs = wrap(X + disp, dom.L)
     if not corrected:
         return Xs, None
-    fstar = interpolate(dom, u_new, Xs)
+    fstar = interpolate(dom, u_new, Xs, scheme)
     beta = adams_weights((h,) + nodes, h)
     disp = beta[0] * fstar
     for j in range(J):
@@ -1372,12 +1450,13 @@ class Run:
     speed: float = 0.0
     tracer_scheme: tuple = ("abm", 1)  # ("abm", k) = ABM(k), Heun = ABM(1); ("ab", k) = AB(k)
     shortened_first_steps: bool = False
+    interpolation: tuple = None        # the tracers' scheme (None: CatmullRom), see `interpolate`
     trail: list = field(default_factory=list, repr=False)   # (time, value), newest first
 
     def __post_init__(self):
         self.u, _, _, self.speed = deposit(self.dom, self.state)
         if self.X is not None:
-            self.trail = [(self.time, interpolate(self.dom, self.u, self.X))]
+            self.trail = [(self.time, interpolate(self.dom, self.u, self.X, self.interpolation))]
 
     @property
     def f0(self):
@@ -1422,8 +1501,8 @@ class Run:
                 J, corrected = len(self.trail), True
             samples = [v for _, v in self.trail[:J]]
             times = [t for t, _ in self.trail[:J]]
-            self.X, _ = advect_adams(self.dom, self.X, samples, times, self.u, D, corrected)
-            self.trail = [(t_new, interpolate(self.dom, self.u, self.X))] + self.trail[:capacity - 1]
+            self.X, _ = advect_adams(self.dom, self.X, samples, times, self.u, D, corrected, self.interpolation)
+            self.trail = [(t_new, interpolate(self.dom, self.u, self.X, self.interpolation))] + self.trail[:capacity - 1]
         if not math.isfinite(self.speed):
             raise FloatingPointError(f"non-finite velocity at step {self.nstep + 1}")
         if self.state.phih is not None and not math.isfinite(scalar_variance(self.dom, self.state.phih)):
