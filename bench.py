@@ -518,10 +518,11 @@ def ours(args):
                                             "clocks": m["clocks"],
                                             "spectrum_rel_err_after_K_steps": float(np.max(np.abs(E32[live] - E64[live]) / E64[live])),
                                             "scalar_spectrum_rel_err_after_K_steps": float(np.max(np.abs(P32[livep] - P64[livep]) / P64[livep]))}}
-        if ws == 1 and not args.no_extras:
+        if ws == 1 and args.extras != "none":
             line["adjoint"] = adjoint_cost(args, device, inputs)
-            line.setdefault("forms", {}).setdefault("fp32_mixed", {})["c1_256cubed"] = c1_statistics(device)
-            line["forms"]["ensemble"] = ensemble_rate(device)
+            if args.extras == "all":
+                line.setdefault("forms", {}).setdefault("fp32_mixed", {})["c1_256cubed"] = c1_statistics(device)
+                line["forms"]["ensemble"] = ensemble_rate(device)
         if ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_line(args, budget_s=60.0)
         print(json.dumps(line), flush=True)
@@ -565,8 +566,9 @@ def main():
                     help="the field integration scheme (the metric is quoted on IFLowStorageRK4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (quick kernel timing)")
-    ap.add_argument("--no-extras", action="store_true",
-                    help="skip the adjoint, 256^3 precision and ensemble legs (rank 0 at N=1 runs them)")
+    ap.add_argument("--extras", default="all", choices=["all", "adjoint", "none"],
+                    help="the further legs rank 0 runs at N=1: the adjoint's cost, the 256^3 precision statistics "
+                         "and the ensemble (all), the adjoint alone, or none")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

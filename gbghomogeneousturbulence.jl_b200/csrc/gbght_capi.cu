@@ -311,6 +311,9 @@ void gbght_config_default(gbght_config* c) {
   c->interpolation = GBGHT_CATMULL_ROM;
   c->interpolation_points = 4;
   c->interpolation_smoothness = 1;
+  c->dealiasing = GBGHT_TWO_THIRDS;
+  c->houli_order = 36;
+  c->houli_strength = 0.0;
 }
 
 int gbght_recommended_cfl(int scheme, double* cfl) {
@@ -392,6 +395,10 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
     if (cfg->interpolation_points > cfg->grid_points_per_axis)
       return bad("the interpolation stencil is wider than the grid");
   }
+  if (cfg->dealiasing != GBGHT_TWO_THIRDS && cfg->dealiasing != GBGHT_HOULI)
+    return bad("unknown dealiasing strategy (TwoThirds and HouLi are built)");
+  if (cfg->dealiasing == GBGHT_HOULI && (cfg->houli_order < 2 || cfg->houli_order % 2 || !std::isfinite(cfg->houli_strength)))
+    return bad("HouLi's `order` must be an even integer ≥ 2 and its `strength` finite");
   if (!finite_positive(cfg->cfl)) return bad("cfl must be positive and finite");
   if (!(cfg->max_dt > 0)) return bad("max_dt must be positive");
 
@@ -399,7 +406,7 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
   r->cfg = *cfg;
   r->trail_capacity = cfg->tracer_steps;
   std::string err;
-  r->eng.reset(gbght::make_engine(cfg->grid_points_per_axis, cfg->precision, &err));
+  r->eng.reset(gbght::make_engine(cfg->grid_points_per_axis, cfg->precision, cfg->dealiasing, &err));
   if (!r->eng) return bad(err);
   gbght::RunParams p{};
   p.N = cfg->grid_points_per_axis;
@@ -415,6 +422,9 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
   p.tracers = cfg->tracers;
   p.trail_capacity = cfg->tracer_steps;
   p.stencil = stencil;
+  p.dealias = cfg->dealiasing;
+  p.houli_order = cfg->houli_order;
+  p.houli_strength = cfg->houli_strength;
   p.device = cfg->device;
   if (const char* e = r->eng->init(p)) {
     g_global_error = e;
@@ -967,6 +977,7 @@ int gbght_adjoint_create(gbght_run* r, int snapshots) {
   };
   if (!ok_forcing(c.velocity_forcing.kind) || (c.scalar && !ok_forcing(c.scalar_forcing.kind)))
     return fail(r, GBGHT_ERR_ARGUMENT, "the adjoint is built for NoForcing, ConstantPower and Linear forcing");
+  if (c.dealiasing != GBGHT_TWO_THIRDS) return fail(r, GBGHT_ERR_ARGUMENT, "the adjoint is built for TwoThirds dealiasing");
   if (snapshots < 0 || snapshots > 64) return fail(r, GBGHT_ERR_ARGUMENT, "snapshots must lie in [0, 64]");
   return engine_call(r, r->eng->adjoint_init(snapshots));
 }

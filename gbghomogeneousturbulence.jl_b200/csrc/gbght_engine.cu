@@ -112,8 +112,10 @@ static int compute_K(int N, double s, double cut2) {
 }
 
 
-template <class T, int N>
+template <class T, int N, int DEA>
 class EngineImpl final : public Engine {
+  // the retained box's bound on |m|: the 2/3 ball's (TwoThirds), or all but the Nyquist planes (HouLi)
+  static constexpr int KM = DEA ? N / 2 - 1 : N / 3 + 1;
   static constexpr int TLY = Shape<T>::TLY;
   // The y tiles' TMA copies start at row offsets K+1, N−K−1 and N−K, which must be 128-byte
   // aligned in shared memory: rows of exactly 128 bytes make every row offset aligned.
@@ -158,17 +160,29 @@ class EngineImpl final : public Engine {
   const char* init(const RunParams& p) override {
     p_ = p;
     const double s = 2.0 * M_PI / p.L;
-    const double cutoff = (2.0 / 3.0) * (double(N) / 2.0) * s;
-    cutoff_ = cutoff;
     g_.N = N;
     g_.s = s;
-    g_.cut2 = cutoff * cutoff;
-    g_.K = compute_K(N, s, g_.cut2);
+    if (DEA) {   // HouLi (src/SimulationDomain.jl:365-376): every mode but the Nyquist planes, filtered
+      const double kny = (double(N) / 2.0) * s;
+      cutoff_ = kny;
+      g_.cut2 = INFINITY;
+      g_.K = N / 2 - 1;
+      g_.houli = 1;
+      g_.filt_strength = p.houli_strength > 0 ? p.houli_strength
+                                              : -std::log(sizeof(T) == 8 ? DBL_EPSILON : double(FLT_EPSILON));
+      g_.filt_half_order = 0.5 * double(p.houli_order);
+      g_.inv_kny2 = 1.0 / (kny * kny);
+    } else {
+      const double cutoff = (2.0 / 3.0) * (double(N) / 2.0) * s;
+      cutoff_ = cutoff;
+      g_.cut2 = cutoff * cutoff;
+      g_.K = compute_K(N, s, g_.cut2);
+    }
     g_.NY2 = 2 * g_.K + 1;
     g_.KXP = ((g_.K + 1 + TLY - 1) / TLY) * TLY;
     g_.inv_norm = 1.0 / (double(N) * double(N) * double(N));
     if (g_.NY2 > N) return "grid too small for the retained band";
-    if (g_.K > ZOwn<T, N, TLZ, NTZ>::KMAX) return "retained band wider than the z tile's row slots";
+    if (g_.K > ZOwn<T, N, TLZ, NTZ, KM>::KMAX) return "retained band wider than the z tile's row slots";
     nS_ = size_t(g_.NY2) * g_.NY2 * g_.KXP;
     nA_ = size_t(N) * g_.NY2 * g_.KXP;
     nB_ = size_t(N) * N * g_.KXP;
@@ -1087,13 +1101,13 @@ class EngineImpl final : public Engine {
     set(reinterpret_cast<const void*>(k_y_forward<T, N, TLY, NTY>), smem_y());
     set(reinterpret_cast<const void*>(k_x_products<T, N, NTXP>), smem_x());
     set(reinterpret_cast<const void*>(k_x_velocity<T, N, NTXV>), smem_xv());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kLowStorage>), smem_ze());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kHeunPredictor>), smem_ze());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kHeunCorrector>), smem_ze());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp1>), smem_ze());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp2>), smem_ze());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp3>), smem_ze());
-    set(reinterpret_cast<const void*>(k_z_init<T, N, TLZ, NTZ>), smem_z());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kLowStorage, KM>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kHeunPredictor, KM>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kHeunCorrector, KM>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp1, KM>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp2, KM>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp3, KM>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_init<T, N, TLZ, NTZ, KM>), smem_z());
     set(reinterpret_cast<const void*>(k_x_adjoint<T, N, NTXA>), smem_xa());
     set(reinterpret_cast<const void*>(k_adj_z<T, N, TLZ, NTZA>), smem_za());
     set(reinterpret_cast<const void*>(k_phys_forward<T, N, 8>), size_t(8) * N * sizeof(Cplx<T>));
@@ -1254,13 +1268,13 @@ class EngineImpl final : public Engine {
       Cplx<T>* W = reinterpret_cast<Cplx<T>*>(base);
       double* red = reinterpret_cast<double*>(base + L::kRed);
       Cplx<T>* R = reinterpret_cast<Cplx<T>*>(base + L::kStage);
-      ZRowsReg<T, ZOwn<T, N, TLZ, 1>> rows;
+      ZRowsReg<T, ZOwn<T, N, TLZ, 1, KM>> rows;
       partial_[c.by * gx + c.bx] =
           body_z_epilogue<T, N, TLZ, 1, KIND>(c, W, R, nullptr, red, g_, maps_, rows, A_, S_, H_, st, amp_, tw_, status_);
     });
 #else
     pbegin(PROF_Z_EPILOGUE);
-    k_z_epilogue<T, N, TLZ, NTZ, KIND><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_ze(), stream_>>>(
+    k_z_epilogue<T, N, TLZ, NTZ, KIND, KM><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_ze(), stream_>>>(
         maps_, g_, A_, S_, H_, st, amp_, partial_, tw_, status_);
     pend();
 #endif
@@ -1278,12 +1292,12 @@ class EngineImpl final : public Engine {
     emu_grid(gl, g_.NY2, 1, smem_z(), [&](const Cta& c, void* sm) {
       Cplx<T>* W = static_cast<Cplx<T>*>(sm);
       double* red = reinterpret_cast<double*>(W + N * TLZ);
-      ZRowsReg<T, ZOwn<T, N, TLZ, 1>> rows;
+      ZRowsReg<T, ZOwn<T, N, TLZ, 1, KM>> rows;
       partial_[c.by * gx + c.bx] =
           body_z_init<T, N, TLZ, 1>(c, W, red, g_, rows, A_, Ssrc, with_scalar, tw_, vorticity);
     });
 #else
-    k_z_init<T, N, TLZ, NTZ><<<dim3(gl, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, Ssrc, with_scalar, partial_,
+    k_z_init<T, N, TLZ, NTZ, KM><<<dim3(gl, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, Ssrc, with_scalar, partial_,
                                                                             tw_, vorticity, gx);
 #endif
     return rt_check();
@@ -1642,17 +1656,20 @@ class EngineImpl final : public Engine {
 };
 
 #if defined(GBGHT_UNIT_FACTORY)
-template <class T, int N> Engine* new_engine();   // defined in the per-(T, N) units
+template <class T, int N, int DEA> Engine* new_engine();   // defined in the per-(T, N, dealiasing) units
 #else
-template <class T, int N>
+template <class T, int N, int DEA>
 Engine* new_engine() {
-  return new EngineImpl<T, N>();
+  return new EngineImpl<T, N, DEA>();
 }
 #endif
 
 #if defined(GBGHT_UNIT_T) && defined(GBGHT_UNIT_N)
-// one (precision, N) per translation unit, so the library's kernels compile in parallel
-template Engine* new_engine<GBGHT_UNIT_T, GBGHT_UNIT_N>();
+// one (precision, N, dealiasing) per translation unit, so the library's kernels compile in parallel
+#ifndef GBGHT_UNIT_D
+#define GBGHT_UNIT_D 0
+#endif
+template Engine* new_engine<GBGHT_UNIT_T, GBGHT_UNIT_N, GBGHT_UNIT_D>();
 #endif
 
 #if !defined(GBGHT_UNIT_T)
@@ -1666,32 +1683,34 @@ bool supported_N(int N) {
   }
 }
 
-template <class T>
+template <class T, int D>
 static Engine* make_for(int N) {
   switch (N) {
-    case 8: return new_engine<T, 8>();
-    case 12: return new_engine<T, 12>();
-    case 16: return new_engine<T, 16>();
-    case 24: return new_engine<T, 24>();
-    case 32: return new_engine<T, 32>();
-    case 48: return new_engine<T, 48>();
-    case 64: return new_engine<T, 64>();
-    case 96: return new_engine<T, 96>();
-    case 128: return new_engine<T, 128>();
-    case 192: return new_engine<T, 192>();
-    case 256: return new_engine<T, 256>();
-    case 384: return new_engine<T, 384>();
-    case 512: return new_engine<T, 512>();
+    case 8: return new_engine<T, 8, D>();
+    case 12: return new_engine<T, 12, D>();
+    case 16: return new_engine<T, 16, D>();
+    case 24: return new_engine<T, 24, D>();
+    case 32: return new_engine<T, 32, D>();
+    case 48: return new_engine<T, 48, D>();
+    case 64: return new_engine<T, 64, D>();
+    case 96: return new_engine<T, 96, D>();
+    case 128: return new_engine<T, 128, D>();
+    case 192: return new_engine<T, 192, D>();
+    case 256: return new_engine<T, 256, D>();
+    case 384: return new_engine<T, 384, D>();
+    case 512: return new_engine<T, 512, D>();
     default: return nullptr;
   }
 }
 
-Engine* make_engine(int N, int precision, std::string* err) {
+Engine* make_engine(int N, int precision, int dealias, std::string* err) {
   if (!supported_N(N)) {
     *err = "grid_points_per_axis must be one of 8 12 16 24 32 48 64 96 128 192 256 384 512";
     return nullptr;
   }
-  Engine* e = precision == 1 ? make_for<float>(N) : make_for<double>(N);
+  Engine* e = nullptr;
+  if (dealias == 1) e = precision == 1 ? make_for<float, 1>(N) : make_for<double, 1>(N);
+  else e = precision == 1 ? make_for<float, 0>(N) : make_for<double, 0>(N);
   if (!e) *err = "unsupported configuration";
   return e;
 }

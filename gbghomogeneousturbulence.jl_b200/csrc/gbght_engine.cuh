@@ -53,6 +53,9 @@ struct RunParams {
   int64_t tracers;
   int trail_capacity;        // sample slots of the tracers' trail (the Adams scheme's k)
   Stencil stencil;           // the tracers' interpolation weights (n = 0: Catmull–Rom)
+  int dealias;               // 0 TwoThirds, 1 HouLi
+  int houli_order;           // HouLi's filter order (36 by default)
+  double houli_strength;     // HouLi's strength; ≤ 0 for the default −log(eps(T))
   int device;
 };
 
@@ -162,7 +165,7 @@ enum ProfileKind {
   PROF_KINDS = 12
 };
 
-Engine* make_engine(int N, int precision, std::string* err);
+Engine* make_engine(int N, int precision, int dealias, std::string* err);
 bool supported_N(int N);
 
 }  // namespace gbght

@@ -106,9 +106,9 @@ __global__ void __launch_bounds__(NT, 2) k_x_velocity(Geometry g, const Cplx<T>*
 // The owned rows of a z tile (ZOwn) live in TMEM where every warp is fully active in every
 // stage, else in registers. `run(rows)` runs the body between the allocation and the release.
 // `slot` is 4 bytes of shared memory for the allocation's address.
-template <class T, int N, int TL, int NT, class F>
+template <class T, int N, int TL, int NT, int KM, class F>
 __device__ __forceinline__ double with_z_rows(uint32_t* slot, const F& run) {
-  using O = ZOwn<T, N, TL, NT>;
+  using O = ZOwn<T, N, TL, NT, KM>;
   using Sh = ZTmemShape<T, N, O, NT>;
   if constexpr (Sh::kUse) {
     const int warp = int(threadIdx.x) >> 5;
@@ -132,7 +132,7 @@ __device__ __forceinline__ double with_z_rows(uint32_t* slot, const F& run) {
 
 // Shared memory: ZLayout (the FFT tile, NT doubles, barriers, the TMEM address, the twiddle table,
 // the staging region).
-template <class T, int N, int TL, int NT, int KIND>
+template <class T, int N, int TL, int NT, int KIND, int KM = N / 3 + 1>
 __global__ void __launch_bounds__(NT, NT > 256 ? 1 : (sizeof(T) == 8 ? 2 : 4)) k_z_epilogue(const __grid_constant__ TmaMaps m, Geometry g, Cplx<T>* A,
                                                       Cplx<T>* S, Cplx<T>* H, StageArgs st, const double* amp,
                                                       double* partial, const Cplx<T>* tw, unsigned int* status) {
@@ -146,20 +146,20 @@ __global__ void __launch_bounds__(NT, NT > 256 ? 1 : (sizeof(T) == 8 ? 2 : 4)) k
   Cplx<T>* twS = reinterpret_cast<Cplx<T>*>(g_smem + L::kTw);
   for (int i = c.tid; i < N; i += NT) twS[i] = tw[i];
   init_bars(bar, 3);   // its barrier also publishes the twiddle table
-  const double e = with_z_rows<T, N, TL, NT>(slot, [&](auto& rows) {
+  const double e = with_z_rows<T, N, TL, NT, KM>(slot, [&](auto& rows) {
     return body_z_epilogue<T, N, TL, NT, KIND>(c, W, R, bar, red, g, m, rows, A, S, H, st, amp, twS, status);
   });
   if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
 }
 
-template <class T, int N, int TL, int NT>
+template <class T, int N, int TL, int NT, int KM = N / 3 + 1>
 __global__ void __launch_bounds__(NT, NT > 256 ? 1 : 2) k_z_init(Geometry g, Cplx<T>* A, const Cplx<T>* S, int has_scalar, double* partial,
                                                   const Cplx<T>* tw, int vorticity = 1, int pstride = 0) {
   CTA_CTX;
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
   double* red = reinterpret_cast<double*>(W + N * TL);
   uint32_t* slot = reinterpret_cast<uint32_t*>(red + NT);
-  const double e = with_z_rows<T, N, TL, NT>(slot, [&](auto& rows) {
+  const double e = with_z_rows<T, N, TL, NT, KM>(slot, [&](auto& rows) {
     return body_z_init<T, N, TL, NT>(c, W, red, g, rows, A, S, has_scalar, tw, vorticity);
   });
   // pstride: the tiles per row of the partials (the full grid's, when a launch covers fewer columns)

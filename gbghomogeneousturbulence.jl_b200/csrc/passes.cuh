@@ -30,9 +30,17 @@ namespace gbght {
 struct Geometry {
   int N, K, NY2, KXP;
   double s;          // 2π/L, the fundamental wavenumber
-  double cut2;       // square of the dealias cutoff T(2/3)·T(N/2)·T(2π/L)
+  double cut2;       // square of the dealias cutoff T(2/3)·T(N/2)·T(2π/L); ∞ under HouLi (no cutoff)
   double inv_norm;   // 1/N³, the inverse transform's normalisation
+  int houli;         // 1: HouLi's smooth filter multiplies the nonlinear terms (no sharp cutoff)
+  double filt_strength, filt_half_order, inv_kny2;   // its strength, order/2, 1/κ_Ny²
 };
+
+// HouLi's filter exp(−strength·(|κ|/κ_Ny)^order) at |κ|² = k2 (src/SimulationDomain.jl:365-376), or 1.
+GBGHT_HD double dealias_filter(const Geometry& g, double k2) {
+  if (!g.houli) return 1.0;
+  return exp(-g.filt_strength * pow(k2 * g.inv_kny2, g.filt_half_order));
+}
 
 GBGHT_HD int q_to_m(int q, int K, int NY2) { return q <= K ? q : q - NY2; }
 GBGHT_HD int q_to_row(int q, int K, int N, int NY2) { return q <= K ? q : q + N - NY2; }
@@ -703,14 +711,16 @@ struct ZLayout {
 // value is the thread that consumes it, and the retained rows stay in its registers between the
 // transforms (no shared-memory copy, no barrier). Row bands r whose rows j + r·N/R have |m| > K for
 // every j get no register.
-template <class T, int N, int TL, int NT>
+template <class T, int N, int TL, int NT, int KM = N / 3 + 1>
 struct ZOwn {
   static constexpr int R = Radices<N>::r[0];
   static_assert(R == Radices<N>::r[Radices<N>::n - 1], "the z epilogue needs equal first and last radix");
   static constexpr int NB = N / R;
   static constexpr int TOT = NB * TL;
   static constexpr int BPT = (TOT + NT - 1) / NT;
-  static constexpr int KMAX = N / 3 + 1;   // bounds K = max |m| of the 2/3 ball for every side length
+  // bounds K = max |m| of the retained box: N/3 + 1 for the 2/3 ball at every side length, N/2 − 1
+  // under HouLi (everything but the Nyquist planes)
+  static constexpr int KMAX = KM;
   static constexpr int lead() { int a = 0; while (a < R && a * NB <= KMAX) ++a; return a; }
   static constexpr int tail() { int b = R; while (b > 0 && b * NB - 1 >= N - KMAX) --b; return b; }
   static constexpr int A0 = lead(), B0 = tail() > lead() ? tail() : lead();
@@ -729,6 +739,7 @@ struct ZOwn {
 // visible to later gets.
 template <class T, class O>
 struct ZRowsReg {
+  using Own = O;
   Cplx<T> v[3][O::BPT][O::NSLOT];
   GBGHT_HD void put(int c, int b, int sl, Cplx<T> x) { v[c][b][sl] = x; }
   GBGHT_HD void put_done() const {}
@@ -755,6 +766,7 @@ struct ZTmemShape {
 #if defined(__CUDACC__) && !defined(GBGHT_EMU)
 template <class T, class O>
 struct ZRowsTmem {
+  using Own = O;
   static constexpr int WPC = int(sizeof(Cplx<T>)) / 4;
   uint32_t base;   // this thread's warp: lane quarter and column block
   __device__ static uint32_t col(int c, int b, int sl) { return uint32_t(((c * O::BPT + b) * O::NSLOT + sl) * WPC); }
@@ -820,9 +832,8 @@ struct ZOwnSource {
 // Every slot of the thread with a register: slot b, band r (slot index sl), whether the row
 // e = j + r·N/R is retained, its compact index q and m_z, and the column l. The loops unroll, so
 // (b, sl) are compile-time indices.
-template <class T, int N, int TL, int NT, int HALF = -1, class F>
+template <class T, int N, int TL, int NT, int HALF = -1, class O = ZOwn<T, N, TL, NT>, class F>
 GBGHT_HD void for_own_slots(const Cta& c, const Geometry& g, const F& f) {
-  using O = ZOwn<T, N, TL, NT>;
 #pragma unroll
   for (int b = 0; b < O::BPT; ++b) {
     const int idx = c.tid + b * NT;
@@ -974,7 +985,7 @@ GBGHT_HD void z_inverse_velocity(const Cta& c, Cplx<T>* W, const Geometry& g, Cp
   if (vorticity == 2) {   // the strain rate instead: S11, S22, S33 into slots 0..2, S12, S13, S23 into 3..5
     for (int o = 0; o < 6; ++o) {
       OwnVals<T, O> x;
-      for_own_slots<T, N, TL, NT>(c, g, [&](int b, int sl, bool, int, int mz, int l) {
+      for_own_slots<T, N, TL, NT, -1, O>(c, g, [&](int b, int sl, bool, int, int mz, int l) {
         Cplx<T> u0, u1, u2;
         rows.get3(b, sl, u0, u1, u2);
         x.v[b][sl] = strain_of<T>(o, u0, u1, u2, T(g.s * double(kx0 + l)), kY, T(g.s * double(mz)));
@@ -985,7 +996,7 @@ GBGHT_HD void z_inverse_velocity(const Cta& c, Cplx<T>* W, const Geometry& g, Cp
   }
   for (int o = 0; o < 3; ++o) {
     OwnVals<T, O> x;
-    for_own_slots<T, N, TL, NT>(c, g, [&](int b, int sl, bool, int, int mz, int l) {
+    for_own_slots<T, N, TL, NT, -1, O>(c, g, [&](int b, int sl, bool, int, int mz, int l) {
       Cplx<T> u0, u1, u2;
       rows.get3(b, sl, u0, u1, u2);
       x.v[b][sl] = curl_of<T>(o, u0, u1, u2, T(g.s * double(kx0 + l)), kY, T(g.s * double(mz)));
@@ -1057,7 +1068,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
                                 const TmaMaps& maps, Rows& rows, Cplx<T>* GBGHT_RESTRICT A, Cplx<T>* GBGHT_RESTRICT S,
                                 Cplx<T>* GBGHT_RESTRICT H, const StageArgs& st, const double* GBGHT_RESTRICT force_amp,
                                 const Cplx<T>* twS, unsigned int* status) {
-  using O = ZOwn<T, N, TL, NT>;
+  using O = typename Rows::Own;
   using H0 = std::integral_constant<int, 0>;
   const SharedTwiddles<T> tw{twS};
   using H1 = std::integral_constant<int, 1>;
@@ -1099,7 +1110,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
     const auto half = [&](auto hc) {
       constexpr int h = decltype(hc)::value;
       sst.wait(h);
-      for_own_slots<T, N, TL, NT, h>(c, g, [&](int b, int sl, bool ret, int q, int mz, int l) {
+      for_own_slots<T, N, TL, NT, h, O>(c, g, [&](int b, int sl, bool ret, int q, int mz, int l) {
         Cplx<T> fx, fy, fz;
         rows.get3(b, sl, fx, fy, fz);
         Cplx<T> phi = czero<T>();
@@ -1116,6 +1127,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
             const Cplx<T> dsum = cmk<T>(T(kxd) * fx.x + T(ky) * fy.x + T(kzd) * fz.x,
                                         T(kxd) * fx.y + T(ky) * fy.y + T(kzd) * fz.y);
             nphi = mul_mi(dsum);
+            if (g.houli) nphi = scale(nphi, T(dealias_filter(g, k2)));
           }
           if (withG) {
             const Cplx<T> ux = sst.at(iG, q, h, l), uy = sst.at(iG + 1, q, h, l), uz = sst.at(iG + 2, q, h, l);
@@ -1164,7 +1176,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
   const auto half = [&](auto hc) {
     constexpr int h = decltype(hc)::value;
     sst.wait(h);
-    for_own_slots<T, N, TL, NT, h>(c, g, [&](int b, int sl, bool ret, int q, int mz, int l) {
+    for_own_slots<T, N, TL, NT, h, O>(c, g, [&](int b, int sl, bool ret, int q, int mz, int l) {
       Cplx<T> f0, f1, f2;
       rows.get3(b, sl, f0, f1, f2);
       Cplx<T> u0 = czero<T>(), u1 = czero<T>(), u2 = czero<T>();
@@ -1185,6 +1197,12 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
           n0 = f0 - scale(kd, kX);
           n1 = f1 - scale(kd, kY);
           n2 = f2 - scale(kd, kZ);
+          if (g.houli) {
+            const T F = T(dealias_filter(g, k2));
+            n0 = scale(n0, F);
+            n1 = scale(n1, F);
+            n2 = scale(n2, F);
+          }
         }
         if (A_f != 0.0 && k2 >= st.band_lo2 && k2 <= st.band_hi2) {
           const T Af = T(A_f);
@@ -1419,7 +1437,7 @@ template <class T, int N, int TL, int NT, class Rows>
 GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, double* red, const Geometry& g, Rows& rows,
                             Cplx<T>* GBGHT_RESTRICT A, const Cplx<T>* GBGHT_RESTRICT S, int has_scalar,
                             const Cplx<T>* GBGHT_RESTRICT tw, int vorticity = 1) {
-  using O = ZOwn<T, N, TL, NT>;
+  using O = typename Rows::Own;
   const int kx0 = c.bx * TL, qy = c.by;
   const double ky = g.s * double(q_to_m(qy, g.K, g.NY2));
   double esum = 0.0;
@@ -1440,8 +1458,8 @@ GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, double* red, const Geometr
     rows.put(1, b, sl, u1);
     rows.put(2, b, sl, u2);
   };
-  for_own_slots<T, N, TL, NT, 0>(c, g, own);
-  for_own_slots<T, N, TL, NT, 1>(c, g, own);
+  for_own_slots<T, N, TL, NT, 0, O>(c, g, own);
+  for_own_slots<T, N, TL, NT, 1, O>(c, g, own);
   rows.put_done();
   red[c.tid] = esum;
   GBGHT_SYNC();

@@ -76,6 +76,9 @@ class Config(C.Structure):
         ("interpolation", C.c_int),
         ("interpolation_points", C.c_int),
         ("interpolation_smoothness", C.c_int),
+        ("dealiasing", C.c_int),
+        ("houli_order", C.c_int),
+        ("houli_strength", C.c_double),
     ]
 
 
@@ -290,6 +293,9 @@ class Setup:
     tracer_steps: int = 1            # k of ABM(k) / AB(k)
     shortened_first_steps: bool = False
     interpolation: tuple = ("CatmullRom", 4, 1)   # ("LalescuSpline", n, smoothness) or ("LagrangeSpline", n, 0)
+    dealiasing: str = "TwoThirds"    # or "HouLi" (src/SimulationDomain.jl:73-177)
+    houli_order: int = 36
+    houli_strength: float = 0.0      # ≤ 0: −log(eps) of the precision
     cfl: float = 0.5
     max_dt: float = math.inf
     device: int = 0
@@ -329,6 +335,11 @@ class Run:
         cfg.interpolation = kinds[setup.interpolation[0]]
         cfg.interpolation_points = int(setup.interpolation[1])
         cfg.interpolation_smoothness = int(setup.interpolation[2])
+        if setup.dealiasing not in ("TwoThirds", "HouLi"):
+            raise ValueError(f"unknown dealiasing strategy {setup.dealiasing!r} (TwoThirds and HouLi are built)")
+        cfg.dealiasing = 0 if setup.dealiasing == "TwoThirds" else 1
+        cfg.houli_order = int(setup.houli_order)
+        cfg.houli_strength = float(setup.houli_strength)
         cfg.cfl = float(setup.cfl)
         cfg.max_dt = float(setup.max_dt)
         cfg.device = int(setup.device)

@@ -37,14 +37,16 @@ def _digest() -> str:
 
 
 def _units():
-    """(name, defines) of every translation unit: one per (precision, N) for the engine, and the
-    C ABI with the engine factory."""
+    """(name, defines) of every translation unit: one per (precision, N, dealiasing) for the engine,
+    and the C ABI with the engine factory."""
     units = [("capi", ["-DGBGHT_UNIT_CAPI"], "gbght_capi.cu"),
              ("noalloc", [], "gbght_noalloc.cu"),
              ("factory", ["-DGBGHT_UNIT_FACTORY"], "gbght_engine.cu")]
     for t in PRECISIONS:
         for n in SIZES:
             units.append((f"eng_{t}_{n}", [f"-DGBGHT_UNIT_T={t}", f"-DGBGHT_UNIT_N={n}"], "gbght_engine.cu"))
+            units.append((f"eng_{t}_{n}_houli", [f"-DGBGHT_UNIT_T={t}", f"-DGBGHT_UNIT_N={n}", "-DGBGHT_UNIT_D=1"],
+                          "gbght_engine.cu"))
     return units
 
 

@@ -120,7 +120,17 @@ typedef struct gbght_config {
   int interpolation;          /* gbght_interpolation: the tracers' grid→point scheme */
   int interpolation_points;   /* stencil width per axis, 4, 6 or 8 (Lalescu, Lagrange) */
   int interpolation_smoothness; /* LalescuSpline's order of continuity, 1..min(3, points − 2) */
+  int dealiasing;             /* gbght_dealiasing */
+  int houli_order;            /* HouLi's filter order (default 36) */
+  double houli_strength;      /* HouLi's damping at the Nyquist mode; ≤ 0: −log(eps) of the precision */
 } gbght_config;
+
+/* The dealiasing strategies (src/SimulationDomain.jl:73-177). TWO_THIRDS: the closed 2/3 ball, the
+ * state stored on it. HOULI (Hou & Li 2007): no cutoff; the nonlinear terms are multiplied by
+ * exp(−strength·(|κ|/κ_Ny)^order) (src/SimulationDomain.jl:365-376), and the state is stored on
+ * every mode but the Nyquist planes, where the filter is ≈ eps: the reference's retained band is the
+ * whole grid, and what it keeps on those planes is at round-off. PhaseShift is not built. */
+enum gbght_dealiasing { GBGHT_TWO_THIRDS = 0, GBGHT_HOULI = 1 };
 
 /* The tracers' interpolation schemes (src/Particles.jl:61-70, schemes of GBGPeriodicFields):
  * CatmullRom = LalescuSpline(4) (the default); LalescuSpline(n; smoothness m), the degree 2m + 1
@@ -132,10 +142,11 @@ enum gbght_interpolation { GBGHT_CATMULL_ROM = 0, GBGHT_LALESCU = 1, GBGHT_LAGRA
 /* Fill `cfg` with the defaults: N=64, L=2π, FP64, IF-RK4, ν=0.01, Sc=1, scalar on, no forcing
  * of either field (each forcing block: rate 0, target 0, gain 1, turnover time 0, over = band,
  * shells 1–2), G=0, no tracers, Heun, no shortened start, CFL 0.5, max_dt=∞, device 0,
- * Catmull–Rom interpolation (4 points, smoothness 1). */
+ * Catmull–Rom interpolation (4 points, smoothness 1), TwoThirds dealiasing (HouLi: order 36, default
+ * strength). */
 void gbght_config_default(gbght_config* cfg);
 
-/* Build a run on a FixedDomain with TwoThirds dealiasing, with its generator and registers.
+/* Build a run on a FixedDomain with TwoThirds or HouLi dealiasing, with its generator and registers.
  * Replaces FixedDomain(...) (src/SimulationDomain.jl:295-328), FlowConditions
  * (src/Generator.jl:81-140), the forcings of either field (ConstantPower src/Forcing.jl:1069-1075,
  * Linear :636-643, VarianceController :828-875, VarianceRescaling :558-572), allocate_buffers
@@ -147,7 +158,8 @@ const char* gbght_last_error(const gbght_run* run);
 const char* gbght_global_error(void);
 const char* gbght_version(void);
 
-/* Retained-band geometry: K (largest retained |m| per axis) and the dealias cutoff.
+/* Retained-band geometry: K (largest retained |m| per axis) and the dealias cutoff (the Nyquist
+ * wavenumber under HouLi).
  * Replaces max_retained_wavenumber (src/SimulationDomain.jl:413-419). */
 int gbght_geometry(const gbght_run* run, int* K, double* cutoff);
 

@@ -71,9 +71,11 @@ class Domain:
     (src/SimulationDomain.jl:349-363; closed-ball test on the squares).
     """
 
-    def __init__(self, N: int, L: float = 2 * math.pi):
+    def __init__(self, N: int, L: float = 2 * math.pi, dealiasing: str = "TwoThirds", houli_order: int = 36,
+                 houli_strength: float | None = None):
         self.N = int(N)
         self.L = float(L)
+        self.dealiasing = dealiasing
         N = self.N
         s = 2 * math.pi / self.L
         self.k0 = s
@@ -96,6 +98,15 @@ class Domain:
             dz[N // 2, :, :] = 0.0
         self.dkx, self.dky, self.dkz = dx, dy, dz
         self.mask = (self.k2 <= self.cutoff * self.cutoff).astype(np.float64)
+        if dealiasing == "HouLi":
+            # Hou & Li's smooth filter in place of the 0/1 mask (`_build_dealias(::HouLi)`,
+            # src/SimulationDomain.jl:365-376): exp(−strength·(|κ|/κ_Ny)^order), strength −log(eps)
+            kny = (N / 2) * s
+            strength = -math.log(np.finfo(np.float64).eps) if not houli_strength else float(houli_strength)
+            self.cutoff = kny
+            self.mask = np.exp(-strength * (np.sqrt(self.k2) / kny) ** houli_order)
+        elif dealiasing != "TwoThirds":
+            raise ValueError(f"unknown dealiasing strategy {dealiasing!r}")
         # Hermitian weights of the half spectrum: modes with 0 < kx < N/2 stand for a conjugate pair
         w = np.full(N // 2 + 1, 2.0)
         w[0] = 1.0
