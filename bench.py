@@ -315,6 +315,44 @@ def adjoint_cost(args, device, inputs, reps=3):
             "kernels_per_adjoint_step_ms": {k: round(v[1] / (reps + 1), 3) for k, v in prof.items() if v[0]}}
 
 
+def dealiasing_cost(args, device, inputs, reps=3):
+    """The field step's cost under each dealiasing strategy on the workload (FP64 and FP32-mixed, no
+    tracers): CUDA-event time of gbght_step + gbght_deposit, the mean of `reps` after one untimed
+    step, with the per-kernel times of PhaseShift's step."""
+    import gbght
+    N = args.grid
+    uh, ph, _ = inputs
+    out = {}
+    for precision in ("fp64", "fp32_mixed"):
+        row = {}
+        for dea in ("TwoThirds", "HouLi", "PhaseShift"):
+            setup = gbght.Setup(grid_points_per_axis=N, viscosity=WORKLOAD["viscosity"], schmidt=WORKLOAD["schmidt"],
+                                velocity_forcing=gbght.ConstantPower(WORKLOAD["injection_rate"], *WORKLOAD["shells"]),
+                                mean_gradient=WORKLOAD["G"], cfl=_cfl(args), scheme=args.scheme, device=device,
+                                precision=precision, dealiasing=dea)
+            run = gbght.simulation(setup, uh, ph)
+            dt = run.cfl_timestep()
+            run.step(dt)
+            run.deposit()
+            run.synchronize()
+            run.profile(True)
+            run.timer_start()
+            for _ in range(reps):
+                run.step(dt)
+                run.deposit()
+            ms = run.timer_stop() / reps
+            prof = run.profile_read()
+            run.profile(False)
+            run.close()
+            row[dea] = {"field_step_ms": round(ms, 3)}
+            if dea == "PhaseShift":
+                row[dea]["kernels_ms_per_step"] = {k: round(v[1] / reps, 3) for k, v in prof.items() if v[0]}
+        for dea in ("HouLi", "PhaseShift"):
+            row[dea]["ratio_vs_two_thirds"] = round(row[dea]["field_step_ms"] / row["TwoThirds"]["field_step_ms"], 3)
+        out[precision] = row
+    return {"grid": N, "forms": out}
+
+
 def c1_statistics(device, steps=500, burn=100, window=100, batch=20, short=20):
     """The 256³ forced configuration (ν = ϰ = 2.1e-3, ConstantPower ε = 0.1 on shells 1–2, G = 1,
     CFL 0.5, 10⁵ tracers) in both forms on the GPU: the FP32-mixed form's relative L2 field error
@@ -518,9 +556,12 @@ def ours(args):
                                             "clocks": m["clocks"],
                                             "spectrum_rel_err_after_K_steps": float(np.max(np.abs(E32[live] - E64[live]) / E64[live])),
                                             "scalar_spectrum_rel_err_after_K_steps": float(np.max(np.abs(P32[livep] - P64[livep]) / P64[livep]))}}
-        if ws == 1 and args.extras != "none":
+        if ws == 1 and args.extras == "dealiasing":
+            line["dealiasing"] = dealiasing_cost(args, device, inputs)
+        if ws == 1 and args.extras in ("all", "adjoint"):
             line["adjoint"] = adjoint_cost(args, device, inputs)
             if args.extras == "all":
+                line["dealiasing"] = dealiasing_cost(args, device, inputs)
                 line.setdefault("forms", {}).setdefault("fp32_mixed", {})["c1_256cubed"] = c1_statistics(device)
                 line["forms"]["ensemble"] = ensemble_rate(device)
         if ws == 1 and not args.no_cpu_baseline:
@@ -566,7 +607,7 @@ def main():
                     help="the field integration scheme (the metric is quoted on IFLowStorageRK4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (quick kernel timing)")
-    ap.add_argument("--extras", default="all", choices=["all", "adjoint", "none"],
+    ap.add_argument("--extras", default="all", choices=["all", "adjoint", "dealiasing", "none"],
                     help="the further legs rank 0 runs at N=1: the adjoint's cost, the 256^3 precision statistics "
                          "and the ensemble (all), the adjoint alone, or none")
     args = ap.parse_args()

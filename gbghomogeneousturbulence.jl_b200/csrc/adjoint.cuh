@@ -241,16 +241,6 @@ struct ZRetainedSource {
     return q < 0 ? czero<T>() : R[(size_t(comp) * g.NY2 + q) * TL + l];
   }
 };
-// z-forward source: A slot `slot` of the tile, straight from global memory.
-template <class T, int N, int TL>
-struct ZGlobalSource {
-  static constexpr bool kExternal = true;
-  const Geometry& g;
-  const Cplx<T>* A;
-  int slot, qy, kx0;
-  GBGHT_HD Cplx<T> load(int e, int l) const { return A[idxA(g, slot, e, qy, kx0 + l)]; }
-};
-
 // Leray projection ℙ(κ)v = v − κ(κ·v)/|κ|², the identity at κ = 0 (the forward epilogue's form).
 template <class T>
 GBGHT_HD void leray3(Cplx<T>* v, double kxd, double kyd, double kzd, double k2) {

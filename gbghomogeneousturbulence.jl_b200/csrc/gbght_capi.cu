@@ -316,6 +316,19 @@ void gbght_config_default(gbght_config* c) {
   c->houli_strength = 0.0;
 }
 
+int gbght_recommended_cfl_dealiased(int scheme, int dealiasing, double* cfl) {
+  // `recommended_cfl(scheme, domain)` (src/Propagator.jl:915-916): the base ceiling × (2/3)/f, f the
+  // retained fraction of the Nyquist wavenumber (src/SimulationDomain.jl:182-184): × 1 for TwoThirds,
+  // × 2/3 for HouLi (f = 1), × 1/√2 for PhaseShift (f = 2√2/3)
+  if (dealiasing != GBGHT_TWO_THIRDS && dealiasing != GBGHT_HOULI && dealiasing != GBGHT_PHASE_SHIFT)
+    return GBGHT_ERR_ARGUMENT;
+  const int rc = gbght_recommended_cfl(scheme, cfl);
+  if (rc != GBGHT_OK) return rc;
+  if (dealiasing == GBGHT_HOULI) *cfl = *cfl * 2.0 / 3.0;
+  if (dealiasing == GBGHT_PHASE_SHIFT) *cfl = *cfl / std::sqrt(2.0);
+  return rc;
+}
+
 int gbght_recommended_cfl(int scheme, double* cfl) {
   // `_base_cfl` (src/Propagator.jl:906-913); the 2/3 rule's factor (2/3)/(2/3) leaves it unchanged
   if (!cfl) return GBGHT_ERR_ARGUMENT;
@@ -395,8 +408,8 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
     if (cfg->interpolation_points > cfg->grid_points_per_axis)
       return bad("the interpolation stencil is wider than the grid");
   }
-  if (cfg->dealiasing != GBGHT_TWO_THIRDS && cfg->dealiasing != GBGHT_HOULI)
-    return bad("unknown dealiasing strategy (TwoThirds and HouLi are built)");
+  if (cfg->dealiasing != GBGHT_TWO_THIRDS && cfg->dealiasing != GBGHT_HOULI && cfg->dealiasing != GBGHT_PHASE_SHIFT)
+    return bad("unknown dealiasing strategy (TwoThirds, HouLi and PhaseShift are built)");
   if (cfg->dealiasing == GBGHT_HOULI && (cfg->houli_order < 2 || cfg->houli_order % 2 || !std::isfinite(cfg->houli_strength)))
     return bad("HouLi's `order` must be an even integer ≥ 2 and its `strength` finite");
   if (!finite_positive(cfg->cfl)) return bad("cfl must be positive and finite");

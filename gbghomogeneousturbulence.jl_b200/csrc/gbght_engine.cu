@@ -114,7 +114,8 @@ static int compute_K(int N, double s, double cut2) {
 
 template <class T, int N, int DEA>
 class EngineImpl final : public Engine {
-  // the retained box's bound on |m|: the 2/3 ball's (TwoThirds), or all but the Nyquist planes (HouLi)
+  // the retained box's bound on |m|: the 2/3 ball's (TwoThirds), or all but the Nyquist planes (the
+  // wide instantiation: HouLi, and PhaseShift's √2·N/3 ball below it)
   static constexpr int KM = DEA ? N / 2 - 1 : N / 3 + 1;
   static constexpr int TLY = Shape<T>::TLY;
   // The y tiles' TMA copies start at row offsets K+1, N−K−1 and N−K, which must be 128-byte
@@ -162,7 +163,15 @@ class EngineImpl final : public Engine {
     const double s = 2.0 * M_PI / p.L;
     g_.N = N;
     g_.s = s;
-    if (DEA) {   // HouLi (src/SimulationDomain.jl:365-376): every mode but the Nyquist planes, filtered
+    if (DEA && p.dealias == 2) {
+      // PhaseShift (src/SimulationDomain.jl:177-184,362): the closed ball at (2√2/3)·κ_Ny = √2·N/3·κ₀,
+      // inside the wide box's bound
+      const double cutoff = (2.0 * std::sqrt(2.0) / 3.0) * (double(N) / 2.0) * s;
+      cutoff_ = cutoff;
+      g_.cut2 = cutoff * cutoff;
+      g_.K = compute_K(N, s, g_.cut2);
+      phase_ = true;
+    } else if (DEA) {   // HouLi (src/SimulationDomain.jl:365-376): every mode but the Nyquist planes, filtered
       const double kny = (double(N) / 2.0) * s;
       cutoff_ = kny;
       g_.cut2 = INFINITY;
@@ -204,6 +213,7 @@ class EngineImpl final : public Engine {
     if ((err = alloc(&H_, 4 * nS_ * sizeof(Cplx<T>)))) return err;
     if ((err = alloc(&A_, 7 * nA_ * sizeof(Cplx<T>)))) return err;
     if ((err = alloc(&B_, 7 * nB_ * sizeof(Cplx<T>)))) return err;
+    if (phase_ && (err = alloc(&A2_, 7 * nA_ * sizeof(Cplx<T>)))) return err;   // the displaced grid's A
     if ((err = alloc(&U_, 3 * nP_ * sizeof(T)))) return err;
     if ((err = alloc(&tw_, N * sizeof(Cplx<T>)))) return err;
     if ((err = alloc(&partial_, ntile_ * sizeof(double)))) return err;
@@ -236,6 +246,7 @@ class EngineImpl final : public Engine {
     }
 #ifndef GBGHT_EMU
     if ((err = make_maps())) return err;
+    if (phase_ && (err = make_maps_on(&maps_ps_, A2_, B_))) return err;
 #endif
     // twiddles e^(-2πi k/N) in extended precision
     std::vector<Cplx<T>> tw(N);
@@ -1088,7 +1099,8 @@ class EngineImpl final : public Engine {
     return size_t(N) * TLZ * sizeof(Cplx<T>) + size_t(NTZ) * sizeof(double) + 16;
   }
   // z epilogue: the FFT tile, NT doubles, barriers, the TMEM address, the staging region
-  size_t smem_ze() const { return ZLayout<T, N, TLZ, NTZ>::bytes(g_.K); }
+  // the wide instantiation stages at most four state components (H is read from global memory)
+  size_t smem_ze() const { return ZLayout<T, N, TLZ, NTZ>::bytes(g_.K, DEA ? 4 : 6); }
 
 #ifndef GBGHT_EMU
   const char* set_smem_attributes() {
@@ -1101,13 +1113,14 @@ class EngineImpl final : public Engine {
     set(reinterpret_cast<const void*>(k_y_forward<T, N, TLY, NTY>), smem_y());
     set(reinterpret_cast<const void*>(k_x_products<T, N, NTXP>), smem_x());
     set(reinterpret_cast<const void*>(k_x_velocity<T, N, NTXV>), smem_xv());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kLowStorage, KM>), smem_ze());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kHeunPredictor, KM>), smem_ze());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kHeunCorrector, KM>), smem_ze());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp1, KM>), smem_ze());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp2, KM>), smem_ze());
-    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp3, KM>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kLowStorage, KM, (DEA != 0)>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kHeunPredictor, KM, (DEA != 0)>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kHeunCorrector, KM, (DEA != 0)>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp1, KM, (DEA != 0)>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp2, KM, (DEA != 0)>), smem_ze());
+    set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kSsp3, KM, (DEA != 0)>), smem_ze());
     set(reinterpret_cast<const void*>(k_z_init<T, N, TLZ, NTZ, KM>), smem_z());
+    set(reinterpret_cast<const void*>(k_z_shift_back<T, N, TLZ, NTZ, KM>), smem_z());
     set(reinterpret_cast<const void*>(k_x_adjoint<T, N, NTXA>), smem_xa());
     set(reinterpret_cast<const void*>(k_adj_z<T, N, TLZ, NTZA>), smem_za());
     set(reinterpret_cast<const void*>(k_phys_forward<T, N, 8>), size_t(8) * N * sizeof(Cplx<T>));
@@ -1262,7 +1275,7 @@ class EngineImpl final : public Engine {
   void z_epilogue_kind(const StageArgs& st) {
 #ifdef GBGHT_EMU
     const int gx = g_.KXP / TLZ;
-    emu_grid(gx, g_.NY2, 1, ZLayout<T, N, TLZ, 1>::bytes(g_.K), [&](const Cta& c, void* sm) {
+    emu_grid(gx, g_.NY2, 1, ZLayout<T, N, TLZ, 1>::bytes(g_.K, DEA ? 4 : 6), [&](const Cta& c, void* sm) {
       using L = ZLayout<T, N, TLZ, 1>;
       unsigned char* base = static_cast<unsigned char*>(sm);
       Cplx<T>* W = reinterpret_cast<Cplx<T>*>(base);
@@ -1270,11 +1283,11 @@ class EngineImpl final : public Engine {
       Cplx<T>* R = reinterpret_cast<Cplx<T>*>(base + L::kStage);
       ZRowsReg<T, ZOwn<T, N, TLZ, 1, KM>> rows;
       partial_[c.by * gx + c.bx] =
-          body_z_epilogue<T, N, TLZ, 1, KIND>(c, W, R, nullptr, red, g_, maps_, rows, A_, S_, H_, st, amp_, tw_, status_);
+          body_z_epilogue<T, N, TLZ, 1, KIND, (DEA != 0)>(c, W, R, nullptr, red, g_, maps_, rows, A_, S_, H_, st, amp_, tw_, status_);
     });
 #else
     pbegin(PROF_Z_EPILOGUE);
-    k_z_epilogue<T, N, TLZ, NTZ, KIND, KM><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_ze(), stream_>>>(
+    k_z_epilogue<T, N, TLZ, NTZ, KIND, KM, (DEA != 0)><<<dim3(g_.KXP / TLZ, g_.NY2, 1), NTZ, smem_ze(), stream_>>>(
         maps_, g_, A_, S_, H_, st, amp_, partial_, tw_, status_);
     pend();
 #endif
@@ -1301,6 +1314,39 @@ class EngineImpl final : public Engine {
                                                                             tw_, vorticity, gx);
 #endif
     return rt_check();
+  }
+  // ---- PhaseShift (src/Generator.jl:502-519,668-704) -------------------------------------------------
+  // The stage's second evaluation, on the grid displaced by half a cell along every axis: the state's
+  // fields there (z-inverse with the translation), their products through the same y and x passes
+  // (B is free again once the primary y-forward has read it), and the shift back averaged into the
+  // primary products in A.
+  void displaced(int ninv, int nfwd) {
+    const int gx = g_.KXP / TLZ;
+#ifdef GBGHT_EMU
+    emu_grid(gx, g_.NY2, 1, smem_z(), [&](const Cta& c, void* sm) {
+      Cplx<T>* W = static_cast<Cplx<T>*>(sm);
+      double* red = reinterpret_cast<double*>(W + N * TLZ);
+      ZRowsReg<T, ZOwn<T, N, TLZ, 1, KM>> rows;
+      body_z_init<T, N, TLZ, 1>(c, W, red, g_, rows, A2_, S_, p_.scalar, tw_, 1, 1);
+    });
+#else
+    pbegin(PROF_Z_SHIFT);
+    k_z_init<T, N, TLZ, NTZ, KM><<<dim3(gx, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A2_, S_, p_.scalar, nullptr,
+                                                                            tw_, 1, 0, 1);
+    pend();
+#endif
+    y_inverse_on(0, ninv, maps_ps_, A2_, B_);
+    x_products();
+    y_forward_on(nfwd, maps_ps_, B_, A2_);
+#ifdef GBGHT_EMU
+    emu_grid(gx, g_.NY2, 1, smem_z(), [&](const Cta& c, void* sm) {
+      body_z_shift_back<T, N, TLZ, 1, ZOwn<T, N, TLZ, 1, KM>>(c, static_cast<Cplx<T>*>(sm), g_, A_, A2_, nfwd, tw_);
+    });
+#else
+    pbegin(PROF_Z_SHIFT);
+    k_z_shift_back<T, N, TLZ, NTZ, KM><<<dim3(gx, g_.NY2, 1), NTZ, smem_z(), stream_>>>(g_, A_, A2_, nfwd, tw_);
+    pend();
+#endif
   }
   // ---- adjoint launches -------------------------------------------------------------------------------
   // The tracers' adjoint at the deposited field U: the Heun push and closing deposit (w, the sample
@@ -1556,6 +1602,7 @@ class EngineImpl final : public Engine {
     bu_fresh_ = false;
     x_products();
     y_forward(nfwd);
+    if (phase_) displaced(ninv, nfwd);
     if (src_[0] || src_[1]) inject();
     if (st.forced || st.sforced) force_amp(st);
     if (amp_save_to_) {   // the adjoint's forward pass keeps the stage's amplitudes
@@ -1652,6 +1699,11 @@ class EngineImpl final : public Engine {
   double *ampsave_ = nullptr, *coef_ = nullptr, *grad_ = nullptr;
   double* amp_save_to_ = nullptr;
   TmaMaps maps_adj_{};
+  // PhaseShift: the displaced grid's A-layout array (its z-inverse fields, then its y-forward
+  // products) and the y passes' maps over it and B
+  bool phase_ = false;
+  Cplx<T>* A2_ = nullptr;
+  TmaMaps maps_ps_{};
   double *LX_ = nullptr, *LF_ = nullptr, *LU_ = nullptr, *snapX_ = nullptr;   // the tracers' adjoint
 };
 
@@ -1709,7 +1761,8 @@ Engine* make_engine(int N, int precision, int dealias, std::string* err) {
     return nullptr;
   }
   Engine* e = nullptr;
-  if (dealias == 1) e = precision == 1 ? make_for<float, 1>(N) : make_for<double, 1>(N);
+  // HouLi and PhaseShift share the wide instantiation (the box up to the Nyquist planes)
+  if (dealias == 1 || dealias == 2) e = precision == 1 ? make_for<float, 1>(N) : make_for<double, 1>(N);
   else e = precision == 1 ? make_for<float, 0>(N) : make_for<double, 0>(N);
   if (!e) *err = "unsupported configuration";
   return e;

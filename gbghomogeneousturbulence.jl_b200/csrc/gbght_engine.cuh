@@ -53,7 +53,7 @@ struct RunParams {
   int64_t tracers;
   int trail_capacity;        // sample slots of the tracers' trail (the Adams scheme's k)
   Stencil stencil;           // the tracers' interpolation weights (n = 0: Catmull–Rom)
-  int dealias;               // 0 TwoThirds, 1 HouLi
+  int dealias;               // 0 TwoThirds, 1 HouLi, 2 PhaseShift
   int houli_order;           // HouLi's filter order (36 by default)
   double houli_strength;     // HouLi's strength; ≤ 0 for the default −log(eps(T))
   int device;
@@ -162,7 +162,8 @@ enum ProfileKind {
   PROF_TRAVERSAL = 9,
   PROF_X_ADJOINT = 10,
   PROF_Z_ADJOINT = 11,
-  PROF_KINDS = 12
+  PROF_Z_SHIFT = 12,
+  PROF_KINDS = 13
 };
 
 Engine* make_engine(int N, int precision, int dealias, std::string* err);

@@ -132,7 +132,7 @@ __device__ __forceinline__ double with_z_rows(uint32_t* slot, const F& run) {
 
 // Shared memory: ZLayout (the FFT tile, NT doubles, barriers, the TMEM address, the twiddle table,
 // the staging region).
-template <class T, int N, int TL, int NT, int KIND, int KM = N / 3 + 1>
+template <class T, int N, int TL, int NT, int KIND, int KM = N / 3 + 1, bool WIDE = false>
 __global__ void __launch_bounds__(NT, NT > 256 ? 1 : (sizeof(T) == 8 ? 2 : 4)) k_z_epilogue(const __grid_constant__ TmaMaps m, Geometry g, Cplx<T>* A,
                                                       Cplx<T>* S, Cplx<T>* H, StageArgs st, const double* amp,
                                                       double* partial, const Cplx<T>* tw, unsigned int* status) {
@@ -147,23 +147,33 @@ __global__ void __launch_bounds__(NT, NT > 256 ? 1 : (sizeof(T) == 8 ? 2 : 4)) k
   for (int i = c.tid; i < N; i += NT) twS[i] = tw[i];
   init_bars(bar, 3);   // its barrier also publishes the twiddle table
   const double e = with_z_rows<T, N, TL, NT, KM>(slot, [&](auto& rows) {
-    return body_z_epilogue<T, N, TL, NT, KIND>(c, W, R, bar, red, g, m, rows, A, S, H, st, amp, twS, status);
+    return body_z_epilogue<T, N, TL, NT, KIND, WIDE>(c, W, R, bar, red, g, m, rows, A, S, H, st, amp, twS, status);
   });
   if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
 }
 
 template <class T, int N, int TL, int NT, int KM = N / 3 + 1>
 __global__ void __launch_bounds__(NT, NT > 256 ? 1 : 2) k_z_init(Geometry g, Cplx<T>* A, const Cplx<T>* S, int has_scalar, double* partial,
-                                                  const Cplx<T>* tw, int vorticity = 1, int pstride = 0) {
+                                                  const Cplx<T>* tw, int vorticity = 1, int pstride = 0,
+                                                  int shift = 0) {
   CTA_CTX;
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
   double* red = reinterpret_cast<double*>(W + N * TL);
   uint32_t* slot = reinterpret_cast<uint32_t*>(red + NT);
   const double e = with_z_rows<T, N, TL, NT, KM>(slot, [&](auto& rows) {
-    return body_z_init<T, N, TL, NT>(c, W, red, g, rows, A, S, has_scalar, tw, vorticity);
+    return body_z_init<T, N, TL, NT>(c, W, red, g, rows, A, S, has_scalar, tw, vorticity, shift);
   });
-  // pstride: the tiles per row of the partials (the full grid's, when a launch covers fewer columns)
-  if (c.tid == 0) partial[blockIdx.y * (pstride ? pstride : gridDim.x) + blockIdx.x] = e;
+  // pstride: the tiles per row of the partials (the full grid's, when a launch covers fewer columns);
+  // no partials for the displaced grid's fields
+  if (c.tid == 0 && partial) partial[blockIdx.y * (pstride ? pstride : gridDim.x) + blockIdx.x] = e;
+}
+// PhaseShift's shift back of the displaced products into A (body_z_shift_back). Grid (KXP/TL, NY2).
+template <class T, int N, int TL, int NT, int KM>
+__global__ void __launch_bounds__(NT, NT > 256 ? 1 : 2) k_z_shift_back(Geometry g, Cplx<T>* A, const Cplx<T>* A2, int nc,
+                                                        const Cplx<T>* tw) {
+  CTA_CTX;
+  Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
+  body_z_shift_back<T, N, TL, NT, ZOwn<T, N, TL, NT, KM>>(c, W, g, A, A2, nc, tw);
 }
 template <class T, int NT, int CH>
 __global__ void __launch_bounds__(NT) k_below_scale(Geometry g, double L, const Cplx<T>* S, double* out) {

@@ -36,14 +36,33 @@ struct Geometry {
   double filt_strength, filt_half_order, inv_kny2;   // its strength, order/2, 1/κ_Ny²
 };
 
-// HouLi's filter exp(−strength·(|κ|/κ_Ny)^order) at |κ|² = k2 (src/SimulationDomain.jl:365-376), or 1.
+// HouLi's filter exp(−strength·(|κ|/κ_Ny)^order) at |κ|² = k2 (src/SimulationDomain.jl:365-376).
 GBGHT_HD double dealias_filter(const Geometry& g, double k2) {
-  if (!g.houli) return 1.0;
   return exp(-g.filt_strength * pow(k2 * g.inv_kny2, g.filt_half_order));
 }
 
 GBGHT_HD int q_to_m(int q, int K, int NY2) { return q <= K ? q : q - NY2; }
 GBGHT_HD int q_to_row(int q, int K, int N, int NY2) { return q <= K ? q : q + N - NY2; }
+
+// PhaseShift's translation symbol e^{iπ·m/N} for the integer wavenumber sum m = mx + my + mz: the
+// factor that samples a mode on the grid displaced by half a cell along every axis (κ·δ = π·m/N
+// for δ = L/(2N) per axis); its conjugate shifts a displaced term back. m is reduced to (−N, N]
+// first, so the argument of sincospi stays within [−1, 1].
+template <class T>
+GBGHT_HD Cplx<T> half_cell_phase(int m, int N) {
+  int r = m % (2 * N);
+  if (r > N) r -= 2 * N;
+  if (r <= -N) r += 2 * N;
+  double sn, cs;
+#ifdef __CUDA_ARCH__
+  sincospi(double(r) / double(N), &sn, &cs);
+#else
+  const double a = 3.14159265358979323846 * (double(r) / double(N));
+  sn = std::sin(a);
+  cs = std::cos(a);
+#endif
+  return cmk<T>(T(cs), T(sn));
+}
 
 GBGHT_HD size_t idxA(const Geometry& g, int c, int z, int q, int kx) {
   return ((size_t(c) * g.N + z) * g.NY2 + q) * g.KXP + kx;
@@ -697,11 +716,12 @@ struct ZLayout {
   static constexpr size_t kSlot = kBar + 4 * sizeof(uint64_t);
   static constexpr size_t kTw = kSlot + 16;
   static constexpr size_t kStage = (kTw + size_t(N) * sizeof(Cplx<T>) + 127) / 128 * 128;
-  GBGHT_HD static size_t stage_elems(int K) {
-    const size_t a = 2 * size_t(N) * TL, b = 6 * size_t(ZStateStaging<T, N, TL>::rows(K)) * TL;
+  // ncomp: the most state components staged at once (6 with H staged, 4 without)
+  GBGHT_HD static size_t stage_elems(int K, int ncomp = 6) {
+    const size_t a = 2 * size_t(N) * TL, b = size_t(ncomp) * ZStateStaging<T, N, TL>::rows(K) * TL;
     return a > b ? a : b;
   }
-  GBGHT_HD static size_t bytes(int K) { return kStage + stage_elems(K) * sizeof(Cplx<T>); }
+  GBGHT_HD static size_t bytes(int K, int ncomp = 6) { return kStage + stage_elems(K, ncomp) * sizeof(Cplx<T>); }
 };
 
 // Per-thread ownership of a z tile's retained rows. In tile_fft_io, slot b of thread t takes
@@ -910,6 +930,69 @@ GBGHT_HD_OUTLINE void z_inverse_own(const Cta c, Cplx<T>* W, const Geometry g, C
   tile_fft_io<T, N, TL, NT, +1>(c, W, tw, src, dst);
 }
 
+// z-forward source: A slot `slot` of the tile, straight from global memory (the adjoint's z pass,
+// PhaseShift's shift back). For the shift back, the forward's last stage keeps the owned retained
+// rows in x, and the inverse's last stage averages into the A slot (a ← ½·a + v).
+template <class T, int N, int TL>
+struct ZGlobalSource {
+  static constexpr bool kExternal = true;
+  const Geometry& g;
+  const Cplx<T>* A;
+  int slot, qy, kx0;
+  GBGHT_HD Cplx<T> load(int e, int l) const { return A[idxA(g, slot, e, qy, kx0 + l)]; }
+};
+template <class T, class O>
+struct OwnValsSink {
+  static constexpr bool kIndexed = true;
+  Cplx<T> (&x)[O::BPT][O::NSLOT];
+  GBGHT_HD void store_rb(int, int, Cplx<T> v, int r, int b) const {
+    if (O::may(r)) x[b][O::slot(r)] = v;
+  }
+};
+template <class T, int N, int TL>
+struct ZAverageSink {
+  const Geometry& g;
+  Cplx<T>* A;
+  int slot, qy, kx0;
+  GBGHT_HD void store(int e, int l, Cplx<T> v) const {
+    Cplx<T>& a = A[idxA(g, slot, e, qy, kx0 + l)];
+    a = scale(a, T(0.5)) + v;
+  }
+};
+template <class T, int N, int TL, int NT, class O, class TW>
+GBGHT_HD_OUTLINE void z_average_own(const Cta c, Cplx<T>* W, const Geometry g, Cplx<T>* A, int slot, int qy, int kx0,
+                                    const OwnVals<T, O> x, const TW tw) {
+  const ZOwnSource<T, N, O> src{g, x.v};
+  const ZAverageSink<T, N, TL> dst{g, A, slot, qy, kx0};
+  tile_fft_io<T, N, TL, NT, +1>(c, W, tw, src, dst);
+}
+
+// The displaced products shifted back and averaged with the primary ones, one tile per CTA (grid
+// (KXP/TL, NY2)). For each of the nc product components: the z-forward of the displaced grid's
+// y-forward output D (slot c of A2), the retained rows multiplied by e^{−iπ(mx+my+mz)/N}/(2N) (the
+// back translation, the 1/N of the round trip, the average's ½), the z-inverse, and A ← ½·A + that.
+// The rows outside the retained box are dropped: the z epilogue keeps only retained rows of A's
+// z-forward, so what it reads is ½(P + e^{−iκ·δ}·P_δ), P and P_δ the two grids' transformed products
+// (`_velocity_nonlinear!(::PhaseShift)` and `_scalar_nonlinear!(::PhaseShift)`,
+// src/Generator.jl:502-519,668-704, average before the truncation).
+template <class T, int N, int TL, int NT, class O>
+GBGHT_HD void body_z_shift_back(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* GBGHT_RESTRICT A,
+                                const Cplx<T>* GBGHT_RESTRICT A2, int nc, const Cplx<T>* GBGHT_RESTRICT tw) {
+  const int kx0 = c.bx * TL, qy = c.by;
+  const int my = q_to_m(qy, g.K, g.NY2);
+  const T inv2n = T(0.5 / double(N));
+  for (int cc = 0; cc < nc; ++cc) {
+    OwnVals<T, O> x;
+    const ZGlobalSource<T, N, TL> src{g, A2, cc, qy, kx0};
+    const OwnValsSink<T, O> dst{x.v};
+    tile_fft_io<T, N, TL, NT, -1>(c, W, tw, src, dst);
+    for_own_slots<T, N, TL, NT, -1, O>(c, g, [&](int b, int sl, bool ret, int, int mz, int l) {
+      x.v[b][sl] = ret ? scale(x.v[b][sl] * conj(half_cell_phase<T>(kx0 + l + my + mz, N)), inv2n) : czero<T>();
+    });
+    z_average_own<T, N, TL, NT, O>(c, W, g, A, cc, qy, kx0, x, tw);
+  }
+}
+
 // Inverse z-transform of value(q, l) (retained rows q) into A slot `slot` of the tile.
 template <class T, int N, int TL, int NT, class F, class TW>
 GBGHT_HD void z_inverse1(const Cta& c, Cplx<T>* W, const Geometry& g, Cplx<T>* A, int slot, int qy, int kx0,
@@ -1063,12 +1146,19 @@ GBGHT_HD Cplx<T> scheme_update(const StageArgs& st, Cplx<T> q, Cplx<T> h, Cplx<T
   return scale(q + scale(hh, T(st.b)), E1);
 }
 
-template <class T, int N, int TL, int NT, int KIND, class Rows>
+template <class T, int N, int TL, int NT, int KIND, bool WIDE, class Rows>
 GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* bar, double* red, const Geometry& g,
                                 const TmaMaps& maps, Rows& rows, Cplx<T>* GBGHT_RESTRICT A, Cplx<T>* GBGHT_RESTRICT S,
                                 Cplx<T>* GBGHT_RESTRICT H, const StageArgs& st, const double* GBGHT_RESTRICT force_amp,
                                 const Cplx<T>* twS, unsigned int* status) {
   using O = typename Rows::Own;
+  // WIDE: the instantiation of the wide box (HouLi, PhaseShift). The filter's branches exist only
+  // there: in the TwoThirds one even a branch never taken slowed the FP64 epilogue by a third
+  // (2.68 → 3.65 ms at 512³). The wide box's rows (K up to N/2 − 1) would make six staged state
+  // components outgrow two CTAs' shared memory per SM, so there the registers H are read from
+  // global memory in the update instead of staged (at most four staged components).
+  constexpr bool kWide = WIDE;
+  constexpr bool kStageH = !WIDE;
   using H0 = std::integral_constant<int, 0>;
   const SharedTwiddles<T> tw{twS};
   using H1 = std::integral_constant<int, 1>;
@@ -1097,7 +1187,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
     stg.issue(c, 1, 4);
     int codes[6], n = 0;
     codes[n++] = 3;                      // φ̂
-    if (st.read_h) codes[n++] = 4 + 3;   // h_φ
+    if (st.read_h && kStageH) codes[n++] = 4 + 3;   // h_φ
     const int iG = n;
     if (withG) {                         // û for −G·û
       codes[n++] = 0;
@@ -1127,7 +1217,8 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
             const Cplx<T> dsum = cmk<T>(T(kxd) * fx.x + T(ky) * fy.x + T(kzd) * fz.x,
                                         T(kxd) * fx.y + T(ky) * fy.y + T(kzd) * fz.y);
             nphi = mul_mi(dsum);
-            if (g.houli) nphi = scale(nphi, T(dealias_filter(g, k2)));
+            if constexpr (kWide)
+              if (g.houli) nphi = scale(nphi, T(dealias_filter(g, k2)));
           }
           if (withG) {
             const Cplx<T> ux = sst.at(iG, q, h, l), uy = sst.at(iG + 1, q, h, l), uz = sst.at(iG + 2, q, h, l);
@@ -1139,7 +1230,8 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
           const T E1 = KIND == kHeunCorrector ? T(1) : T(exp(st.cphi * k2 + (sband ? st.lin_phi : 0.0)));
           const T E2 = KIND >= kSsp2 ? T(exp(st.cphi2 * k2 + (sband ? st.lin_phi2 : 0.0))) : T(0);
           Cplx<T> hw = czero<T>();
-          phi = scheme_update<T, KIND>(st, phi, st.read_h ? sst.at(1, q, h, l) : czero<T>(), nphi, E1, E2, &hw);
+          const Cplx<T> hphi = st.read_h ? (kStageH ? sst.at(1, q, h, l) : H[si]) : czero<T>();
+          phi = scheme_update<T, KIND>(st, phi, hphi, nphi, E1, E2, &hw);
           S[si] = phi;
           if (st.write_h) H[si] = hw;
         }
@@ -1165,7 +1257,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
   codes[n++] = 0;
   codes[n++] = 1;
   codes[n++] = 2;
-  if (st.read_h) {
+  if (st.read_h && kStageH) {
     codes[n++] = 4;
     codes[n++] = 5;
     codes[n++] = 6;
@@ -1197,7 +1289,7 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
           n0 = f0 - scale(kd, kX);
           n1 = f1 - scale(kd, kY);
           n2 = f2 - scale(kd, kZ);
-          if (g.houli) {
+          if (kWide && g.houli) {
             const T F = T(dealias_filter(g, k2));
             n0 = scale(n0, F);
             n1 = scale(n1, F);
@@ -1215,9 +1307,12 @@ GBGHT_HD double body_z_epilogue(const Cta& c, Cplx<T>* W, Cplx<T>* R, uint64_t* 
         const T E2 = KIND >= kSsp2 ? T(exp(st.cu2 * k2 + (vband ? st.lin_u2 : 0.0))) : T(0);
         const bool rh = st.read_h;
         Cplx<T> w0 = czero<T>(), w1 = czero<T>(), w2 = czero<T>();
-        u0 = scheme_update<T, KIND>(st, u0, rh ? sst.at(3, q, h, l) : czero<T>(), n0, E1, E2, &w0);
-        u1 = scheme_update<T, KIND>(st, u1, rh ? sst.at(4, q, h, l) : czero<T>(), n1, E1, E2, &w1);
-        u2 = scheme_update<T, KIND>(st, u2, rh ? sst.at(5, q, h, l) : czero<T>(), n2, E1, E2, &w2);
+        const Cplx<T> h0 = rh ? (kStageH ? sst.at(3, q, h, l) : H[s0]) : czero<T>();
+        const Cplx<T> h1 = rh ? (kStageH ? sst.at(4, q, h, l) : H[s1]) : czero<T>();
+        const Cplx<T> h2 = rh ? (kStageH ? sst.at(5, q, h, l) : H[s2]) : czero<T>();
+        u0 = scheme_update<T, KIND>(st, u0, h0, n0, E1, E2, &w0);
+        u1 = scheme_update<T, KIND>(st, u1, h1, n1, E1, E2, &w1);
+        u2 = scheme_update<T, KIND>(st, u2, h2, n2, E1, E2, &w2);
         if (st.last) {
           if (k2 > 0.0) {
             const T kX = T(kxd), kY = T(ky), kZ = T(kzd);
@@ -1431,19 +1526,23 @@ GBGHT_HD void rescale_mode(long i, const Geometry& g, Cplx<T>* S, int c0, int mb
 }
 // ================================================================================================
 // z-inverse of the current state into A slots 0..6 (u, iκ×û, φ), and the tile's Hermitian-weighted
-// Σ|û|², with the same tiling as the epilogue. Used after an import to start a step.
+// Σ|û|², with the same tiling as the epilogue. Used after an import to start a step. With `shift`
+// each mode is first multiplied by e^{iπ(mx+my+mz)/N}: the fields on PhaseShift's displaced grid
+// (the translation `to_shifted`, src/Generator.jl:169-175), into another A-layout array; the
+// energy sum is still the state's.
 // ================================================================================================
 template <class T, int N, int TL, int NT, class Rows>
 GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, double* red, const Geometry& g, Rows& rows,
                             Cplx<T>* GBGHT_RESTRICT A, const Cplx<T>* GBGHT_RESTRICT S, int has_scalar,
-                            const Cplx<T>* GBGHT_RESTRICT tw, int vorticity = 1) {
+                            const Cplx<T>* GBGHT_RESTRICT tw, int vorticity = 1, int shift = 0) {
   using O = typename Rows::Own;
   const int kx0 = c.bx * TL, qy = c.by;
-  const double ky = g.s * double(q_to_m(qy, g.K, g.NY2));
+  const int my = q_to_m(qy, g.K, g.NY2);
+  const double ky = g.s * double(my);
   double esum = 0.0;
   // the retained rows of half 0, then of half 1: the epilogue's order, so the tile's energy sum
   // (the next stage's forcing amplitude reads it) is the epilogue's to the last bit
-  const auto own = [&](int b, int sl, bool ret, int q, int, int l) {
+  const auto own = [&](int b, int sl, bool ret, int q, int mz, int l) {
     Cplx<T> u0 = czero<T>(), u1 = czero<T>(), u2 = czero<T>();
     if (ret) {
       const int kx = kx0 + l;
@@ -1453,6 +1552,12 @@ GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, double* red, const Geometr
       const double w = kx == 0 ? 1.0 : 2.0;
       esum += w * ((double(u0.x) * u0.x + double(u0.y) * u0.y) + (double(u1.x) * u1.x + double(u1.y) * u1.y) +
                    (double(u2.x) * u2.x + double(u2.y) * u2.y));
+      if (shift) {   // the state sampled on the displaced grid (PhaseShift)
+        const Cplx<T> p = half_cell_phase<T>(kx + my + mz, N);
+        u0 = u0 * p;
+        u1 = u1 * p;
+        u2 = u2 * p;
+      }
     }
     rows.put(0, b, sl, u0);
     rows.put(1, b, sl, u1);
@@ -1468,7 +1573,10 @@ GBGHT_HD double body_z_init(const Cta& c, Cplx<T>* W, double* red, const Geometr
     for (int i = 0; i < NT; ++i) total += red[i];
   z_inverse_velocity<T, N, TL, NT, O>(c, W, g, A, qy, kx0, ky, rows, vorticity, tw);
   if (has_scalar) {
-    const auto phi = [&](int q, int l) { return S[idxS(g, 3, qy, q, kx0 + l)]; };
+    const auto phi = [&](int q, int l) {
+      const Cplx<T> v = S[idxS(g, 3, qy, q, kx0 + l)];
+      return shift ? v * half_cell_phase<T>(kx0 + l + my + q_to_m(q, g.K, g.NY2), N) : v;
+    };
     z_inverse1<T, N, TL, NT>(c, W, g, A, 6, qy, kx0, phi, tw);
   }
   return total;

@@ -96,6 +96,7 @@ _SIGNATURES = {
     "gbght_step": (C.c_int, [C.c_void_p, C.c_double]),
     "gbght_forcing_source_set": (C.c_int, [C.c_void_p, C.c_int, _DP, C.c_int]),
     "gbght_recommended_cfl": (C.c_int, [C.c_int, _DP]),
+    "gbght_recommended_cfl_dealiased": (C.c_int, [C.c_int, C.c_int, _DP]),
     "gbght_ensemble_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int]),
     "gbght_ensemble_destroy": (None, [C.c_void_p]),
     "gbght_ensemble_step": (C.c_int, [C.c_void_p, C.c_double]),
@@ -144,7 +145,8 @@ _SIGNATURES = {
 }
 
 KERNELS = ("y_inverse", "x_products", "y_forward", "z_epilogue", "x_velocity", "force_amp", "reality",
-           "tracers", "observables", "traversal", "x_adjoint", "z_adjoint")
+           "tracers", "observables", "traversal", "x_adjoint", "z_adjoint", "z_shift")
+DEALIASING = {"TwoThirds": 0, "HouLi": 1, "PhaseShift": 2}
 OBSERVABLES = {"kinetic_energy": 0, "scalar_variance": 1}
 
 _loaded: dict = {}
@@ -293,7 +295,7 @@ class Setup:
     tracer_steps: int = 1            # k of ABM(k) / AB(k)
     shortened_first_steps: bool = False
     interpolation: tuple = ("CatmullRom", 4, 1)   # ("LalescuSpline", n, smoothness) or ("LagrangeSpline", n, 0)
-    dealiasing: str = "TwoThirds"    # or "HouLi" (src/SimulationDomain.jl:73-177)
+    dealiasing: str = "TwoThirds"    # or "HouLi", "PhaseShift" (src/SimulationDomain.jl:73-177)
     houli_order: int = 36
     houli_strength: float = 0.0      # ≤ 0: −log(eps) of the precision
     cfl: float = 0.5
@@ -335,9 +337,10 @@ class Run:
         cfg.interpolation = kinds[setup.interpolation[0]]
         cfg.interpolation_points = int(setup.interpolation[1])
         cfg.interpolation_smoothness = int(setup.interpolation[2])
-        if setup.dealiasing not in ("TwoThirds", "HouLi"):
-            raise ValueError(f"unknown dealiasing strategy {setup.dealiasing!r} (TwoThirds and HouLi are built)")
-        cfg.dealiasing = 0 if setup.dealiasing == "TwoThirds" else 1
+        if setup.dealiasing not in DEALIASING:
+            raise ValueError(f"unknown dealiasing strategy {setup.dealiasing!r} "
+                             "(TwoThirds, HouLi and PhaseShift are built)")
+        cfg.dealiasing = DEALIASING[setup.dealiasing]
         cfg.houli_order = int(setup.houli_order)
         cfg.houli_strength = float(setup.houli_strength)
         cfg.cfl = float(setup.cfl)
@@ -731,12 +734,17 @@ class Ensemble:
             pass
 
 
-def recommended_cfl(scheme: str, library: str | None = None) -> float:
-    """`recommended_cfl(scheme, domain)` (src/Propagator.jl:906-919) for the 2/3 rule."""
+def recommended_cfl(scheme: str, dealiasing: str = "TwoThirds", library: str | None = None) -> float:
+    """`recommended_cfl(scheme, domain)` (src/Propagator.jl:906-919): the scheme's ceiling under the
+    2/3 rule, scaled by (2/3)/f for a strategy that retains the fraction f of the Nyquist wavenumber."""
     lib = load_library(library)
     v = C.c_double()
-    if scheme not in SCHEMES or lib.gbght_recommended_cfl(SCHEMES[scheme], C.byref(v)) != OK:
+    if scheme not in SCHEMES:
         raise ValueError(f"unknown field integration scheme {scheme!r}")
+    if dealiasing not in DEALIASING:
+        raise ValueError(f"unknown dealiasing strategy {dealiasing!r}")
+    if lib.gbght_recommended_cfl_dealiased(SCHEMES[scheme], DEALIASING[dealiasing], C.byref(v)) != OK:
+        raise ValueError(f"no CFL ceiling for {scheme!r} under {dealiasing!r}")
     return v.value
 
 

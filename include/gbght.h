@@ -129,8 +129,12 @@ typedef struct gbght_config {
  * state stored on it. HOULI (Hou & Li 2007): no cutoff; the nonlinear terms are multiplied by
  * exp(−strength·(|κ|/κ_Ny)^order) (src/SimulationDomain.jl:365-376), and the state is stored on
  * every mode but the Nyquist planes, where the filter is ≈ eps: the reference's retained band is the
- * whole grid, and what it keeps on those planes is at round-off. PhaseShift is not built. */
-enum gbght_dealiasing { GBGHT_TWO_THIRDS = 0, GBGHT_HOULI = 1 };
+ * whole grid, and what it keeps on those planes is at round-off. PHASE_SHIFT (Patterson & Orszag
+ * 1971, Rogallo 1981): each stage's nonlinear terms are the average of the grid's and those of the
+ * grid displaced by half a cell along every axis, shifted back, on the closed ball of radius
+ * (2√2/3)·κ_Ny (src/SimulationDomain.jl:177-184, src/Generator.jl:502-519,668-704); twice the
+ * transforms of TWO_THIRDS per stage. The adjoint is built for TWO_THIRDS only. */
+enum gbght_dealiasing { GBGHT_TWO_THIRDS = 0, GBGHT_HOULI = 1, GBGHT_PHASE_SHIFT = 2 };
 
 /* The tracers' interpolation schemes (src/Particles.jl:61-70, schemes of GBGPeriodicFields):
  * CatmullRom = LalescuSpline(4) (the default); LalescuSpline(n; smoothness m), the degree 2m + 1
@@ -146,7 +150,8 @@ enum gbght_interpolation { GBGHT_CATMULL_ROM = 0, GBGHT_LALESCU = 1, GBGHT_LAGRA
  * strength). */
 void gbght_config_default(gbght_config* cfg);
 
-/* Build a run on a FixedDomain with TwoThirds or HouLi dealiasing, with its generator and registers.
+/* Build a run on a FixedDomain with TwoThirds, HouLi or PhaseShift dealiasing, with its generator and
+ * registers.
  * Replaces FixedDomain(...) (src/SimulationDomain.jl:295-328), FlowConditions
  * (src/Generator.jl:81-140), the forcings of either field (ConstantPower src/Forcing.jl:1069-1075,
  * Linear :636-643, VarianceController :828-875, VarianceRescaling :558-572), allocate_buffers
@@ -210,6 +215,10 @@ const char* gbght_ensemble_last_error(const gbght_ensemble* ensemble);
 /* A scheme's advective-CFL ceiling under the 2/3 rule: 0.96 (RK4), 0.5 (RK3, SSPRK3), 0.25 (Heun).
  * Replaces recommended_cfl(scheme, domain) (src/Propagator.jl:906-919) for TwoThirds. */
 int gbght_recommended_cfl(int scheme, double* cfl);
+/* The same ceiling for a dealiasing strategy (gbght_dealiasing): × (2/3)/f, f the fraction of the
+ * Nyquist wavenumber the strategy retains (2/3, 1 for HouLi, 2√2/3 for PhaseShift).
+ * Replaces recommended_cfl(scheme, domain) (src/Propagator.jl:915-916). */
+int gbght_recommended_cfl_dealiased(int scheme, int dealiasing, double* cfl);
 
 /* The closing field deposit: the velocity in physical representation and max|u|.
  * Replaces deposit!(cache, state, domain, buffers) (src/Propagator.jl:808-842). */
@@ -335,7 +344,9 @@ enum gbght_kernel {
                                    the diagnostics' reductions */
   GBGHT_KERNEL_TRAVERSAL = 9,   /* tracer traversal order: tile keys, scan, scatter */
   GBGHT_KERNEL_X_ADJOINT = 10,  /* the adjoint x pass: c2r of fields and sources, their products, r2c */
-  GBGHT_KERNEL_Z_ADJOINT = 11   /* the adjoint z pass: z-forward, the λ update, the next stage's sources */
+  GBGHT_KERNEL_Z_ADJOINT = 11,  /* the adjoint z pass: z-forward, the λ update, the next stage's sources */
+  GBGHT_KERNEL_Z_SHIFT = 12     /* PhaseShift: the displaced grid's z-inverse, and the shift back of its
+                                   products averaged into the grid's */
 };
 int gbght_profile(gbght_run* run, int enable);
 int gbght_profile_read(gbght_run* run, int kind, int64_t* launches, double* total_ms);

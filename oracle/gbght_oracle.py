@@ -33,6 +33,8 @@ have no counterpart in the reference, which has no AD. They are pinned by centra
 finite differences and by the dot-product identity ⟨Jv, w⟩ = ⟨v, Jᵀw⟩.
 - injected power equal to ε, and a solenoidal state;
 - the 2/3 closed ball against a 2N zero-padded product;
+- PhaseShift's displaced-grid average against a 2N zero-padded product, both nonlinear terms
+  (test/dealiasing.jl:69-114);
 - Parseval, and the planted reality violation;
 - tracer uniform flow, wrap, constant field and Heun order;
 - the classical Adams weights.
@@ -63,7 +65,8 @@ def _axis_integers(N: int) -> np.ndarray:
 
 
 class Domain:
-    """The fixed cubic box: `FixedDomain` (src/SimulationDomain.jl:275-328), TwoThirds dealiasing.
+    """The fixed cubic box: `FixedDomain` (src/SimulationDomain.jl:275-328), TwoThirds dealiasing, or
+    HouLi's filter, or PhaseShift's displaced-grid average on the (2√2/3)·κ_Ny ball.
 
     ``cutoff`` is ``T(2/3) * T(N/2) * T(2π/L)`` evaluated left to right in FP64, as
     `_cutoff_wavenumber` does (src/SimulationDomain.jl:342-343). The mask keeps the closed ball
@@ -105,6 +108,16 @@ class Domain:
             strength = -math.log(np.finfo(np.float64).eps) if not houli_strength else float(houli_strength)
             self.cutoff = kny
             self.mask = np.exp(-strength * (np.sqrt(self.k2) / kny) ** houli_order)
+        elif dealiasing == "PhaseShift":
+            # the closed ball at (2√2/3)·κ_Ny = √2·N/3·κ₀ (src/SimulationDomain.jl:177-184,362), and
+            # the translation to the grid displaced by half a cell along every axis: the mode of
+            # integer wavenumbers (mx, my, mz) times e^{iπ(mx+my+mz)/N} (κ·δ with δ = L/(2N) per axis;
+            # `to_shifted`, src/Generator.jl:169-175); `shift_back` is its conjugate
+            self.cutoff = (2 * math.sqrt(2) / 3) * (N / 2) * s
+            self.mask = (self.k2 <= self.cutoff * self.cutoff).astype(np.float64)
+            msum = mx[None, None, :] + my[None, :, None] + mz[:, None, None]
+            self.shift_to = np.exp(1j * math.pi * msum / N)
+            self.shift_back = np.conj(self.shift_to)
         elif dealiasing != "TwoThirds":
             raise ValueError(f"unknown dealiasing strategy {dealiasing!r}")
         # Hermitian weights of the half spectrum: modes with 0 < kx < N/2 stand for a conjugate pair
@@ -346,10 +359,13 @@ def velocity_rhs(dom: Domain, cond: Conditions, uh, u, w, eps_T):
     """N̂_u = 𝔻ℙ FFT(u × ω) (negated Lamb vector, operands u, ω), mean mode zeroed, plus the
     ConstantPower source on the stage û (`velocity_rhs!` src/Generator.jl:484-488,
     `_velocity_advective_term!` :528-534, `mean_free_projection!` :486)."""
-    ux, uy, uz = u
-    wx, wy, wz = w
-    lamb_neg = np.stack([uy * wz - uz * wy, uz * wx - ux * wz, ux * wy - uy * wx])
-    nh = dom.to_spectral(lamb_neg)
+    nh = dom.to_spectral(_cross(u, w))
+    if dom.dealiasing == "PhaseShift":
+        # the average with the same term on the displaced grid, shifted back
+        # (`_velocity_nonlinear!(::PhaseShift)`, src/Generator.jl:502-519)
+        us = dom.to_physical(dom.shift_to * uh)
+        ws = dom.to_physical(dom.shift_to * curl(dom, uh))
+        nh = 0.5 * (nh + dom.shift_back * dom.to_spectral(_cross(us, ws)))
     nh = leray(dom, nh, dom.mask)
     nh[:, 0, 0, 0] = 0.0
     src = stage_source(dom, cond.velocity_forcing, uh, eps_T, cond.viscosity)
@@ -364,6 +380,13 @@ def scalar_rhs(dom: Domain, cond: Conditions, uh, u, phi, ph=None, eps_T: float 
     ∂tφ + u·∇φ = −u·G + ϰ∇²φ)."""
     flux = u * phi[None]
     fh = dom.to_spectral(flux)
+    if dom.dealiasing == "PhaseShift":
+        # the flux on the displaced grid, shifted back and averaged before the divergence
+        # (`_scalar_nonlinear!(::PhaseShift)`, src/Generator.jl:668-704; the shift commutes with iκ·)
+        phs = dom.to_spectral(phi) if ph is None else ph
+        us = dom.to_physical(dom.shift_to * uh)
+        phis = dom.to_physical(dom.shift_to * phs)
+        fh = 0.5 * (fh + dom.shift_back * dom.to_spectral(us * phis[None]))
     div = 1j * ((dom.dkx * fh[0] + dom.dky * fh[1]) + dom.dkz * fh[2])
     nh = -(dom.mask * div)
     G = cond.mean_gradient
@@ -499,9 +522,11 @@ def _cross(a, b):
     return np.stack([a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]])
 
 
-def _tangent_supported(cond: Conditions, scheme: str):
+def _tangent_supported(cond: Conditions, scheme: str, dom: Domain | None = None):
     if scheme not in SCHEMES:
         raise ValueError(f"unknown scheme {scheme!r}")
+    if dom is not None and dom.dealiasing == "PhaseShift":
+        raise ValueError("the tangent and adjoint are restated for the mask strategies, not PhaseShift")
 
 
 def _amplitude_gradient(dom: Domain, f, x, A, band, D):
@@ -599,7 +624,7 @@ def step_tangent(dom: Domain, cond: Conditions, uh: np.ndarray, duh: np.ndarray,
                  scheme: str = "rk4", ph: np.ndarray | None = None, dph: np.ndarray | None = None):
     """One step F of `scheme` and its tangent J·δ in the same pass, for the velocity alone (ph None)
     or the coupled velocity + scalar. Returns (F_u, J_u) or (F_u, F_φ, J_u, J_φ)."""
-    _tangent_supported(cond, scheme)
+    _tangent_supported(cond, scheme, dom)
     if scheme == "heun":
         return heun_tangent(dom, cond, uh, duh, float(dt), ph, dph)
     if scheme == "ssprk3":
@@ -653,7 +678,7 @@ def step_adjoint(dom: Domain, cond: Conditions, uh: np.ndarray, lam: np.ndarray,
                  scheme: str = "rk4", ph: np.ndarray | None = None, lam_p: np.ndarray | None = None):
     """Jᵀ·λ for the step at (û, φ̂): a forward pass that keeps each stage's fields, then the stages
     in reverse, each operation replaced by its adjoint. Returns λ_u, or (λ_u, λ_φ) with a scalar."""
-    _tangent_supported(cond, scheme)
+    _tangent_supported(cond, scheme, dom)
     if scheme == "heun":
         return heun_adjoint(dom, cond, uh, lam, float(dt), ph, lam_p)
     if scheme == "ssprk3":
