@@ -16,9 +16,9 @@ from oracle import gbght_oracle as O
 from pairs import advance_both, compare, make_case
 
 
-def _ball_field(dom, seed, ncomp=3, peak=4.0):
+def _ball_field(dom, seed, ncomp=3, peak=4.0, mean_square=None):
     """A real random field filling PhaseShift's ball, its spectrum peaked at shell `peak`
-    (solenoidal for three components)."""
+    (solenoidal for three components), scaled to the box mean square `mean_square` when given."""
     rng = np.random.default_rng(seed)
     shape = (ncomp,) + dom.shape_spectral
     c = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
@@ -27,6 +27,8 @@ def _ball_field(dom, seed, ncomp=3, peak=4.0):
     if ncomp == 3:
         c = O.leray(dom, c)
     c = dom.to_spectral(dom.to_physical(c)) * dom.mask   # the Hermitian part
+    if mean_square is not None:
+        c = c * math.sqrt(mean_square / (2.0 * dom.inner(c, c)))
     return c if ncomp == 3 else c[0]
 
 
@@ -115,9 +117,12 @@ def test_phase_shift_refuses_the_tangent():
 
 
 def _case(N, library, precision="fp64", tracers=100, **kw):
+    # box mean squares ⟨|u|²⟩ = ⟨φ²⟩ = ½, physical sizes like the seeders' (an unscaled field is
+    # physically tiny, and the ConstantPower rate ε/(2E) would then amplify it by orders of
+    # magnitude in one step)
     dom = O.Domain(N, dealiasing="PhaseShift")
-    uh = 0.3 * _ball_field(dom, 1)
-    ph = 0.3 * _ball_field(dom, 2, ncomp=1)
+    uh = _ball_field(dom, 1, mean_square=1.0)
+    ph = _ball_field(dom, 2, ncomp=1, mean_square=1.0)
     return make_case(N, viscosity=0.01, forcing=0.1, G=(1.0, 0.0, 0.0), tracers=tracers, dealiasing="PhaseShift",
                      precision=precision, library=library, uh=uh, ph=ph, **kw)
 
@@ -158,5 +163,3 @@ def test_phase_shift_matches_the_oracle(cuda_library, N, precision, tol):
     run, orun = _case(N, cuda_library, precision=precision, tracers=1000)
     advance_both(run, orun, 4 if N == 64 else 2, dt=0.005)
     compare(run, orun, tol=tol, check_tracers=precision == "fp64")
-    prof = run.profile_read() if hasattr(run, "profile_read") else None
-    del prof
