@@ -408,10 +408,12 @@ def c1_statistics(device, steps=500, burn=100, window=100, batch=20, short=20):
     return out
 
 
-def ensemble_rate(device, steps=300, alone_steps=30):
+def ensemble_rate(device, steps=300, alone_steps=30, sweep_steps=40):
     """The batched ensemble: 96 FP32-mixed members, 32 each of 32³, 48³ and 64³, ν drawn from
     [0.005, 0.02] per member, ConstantPower ε = 0.1, G = 1, IF-RK4, stepped together under one CUDA
-    graph (gbght_ensemble_step) for `steps` steps, against stepping them one by one."""
+    graph (gbght_ensemble_step). The ensemble's autotuner picks the member batching (the group size,
+    1 = one launch per member and pass), then `steps` steps are timed; each group size is also timed
+    over `sweep_steps` steps, and the members are timed stepped one by one."""
     import gbght
     from gbght import seed as S
     rng = np.random.default_rng(7)
@@ -423,12 +425,24 @@ def ensemble_rate(device, steps=300, alone_steps=30):
         runs.append(gbght.simulation(setup, S.seed_velocity(n, 0.5, seed=100 + i), S.seed_scalar(n, 0.5, seed=300 + i)))
     dt = 0.002
     ens = gbght.Ensemble(runs)
-    ens.step(dt)
-    runs[0].synchronize()
-    t0 = time.perf_counter()
-    for _ in range(steps):
+
+    def timed(nsteps):
+        ens.step(dt)   # a capture when the batching changed
+        runs[0].synchronize()
+        t0 = time.perf_counter()
+        for _ in range(nsteps):
+            ens.step(dt)
+        return len(runs) * nsteps / (time.perf_counter() - t0)
+    sweep = {}
+    for g in (1, 2, 4, 8, 16, 32):
+        ens.set_batching(g)
+        sweep[g] = {"member_steps_per_s": round(timed(sweep_steps), 1), "launching_units": ens.units()}
+    ens.autotune()
+    while not ens.tuning()[1]:
         ens.step(dt)
-    graph = len(runs) * steps / (time.perf_counter() - t0)
+    chosen, _, tune_ms = ens.tuning()
+    rate = timed(steps)
+    units = ens.units()
     ens.close()
     for r in runs:
         r.advance(dt)
@@ -441,8 +455,11 @@ def ensemble_rate(device, steps=300, alone_steps=30):
     for r in runs:
         r.close()
     return {"members": len(runs), "grids": "32x32^3 + 32x48^3 + 32x64^3", "form": "fp32_mixed", "steps": steps,
-            "member_steps_per_s_graph": round(graph, 1), "member_steps_per_s_one_by_one": round(alone, 1),
-            "speedup": round(graph / alone, 3), "timing": "host wall clock around synchronising calls"}
+            "member_steps_per_s": round(rate, 1), "group_size": chosen, "launching_units": units,
+            "autotune_replay_ms": [round(v, 3) for v in tune_ms], "by_group_size": sweep,
+            "member_steps_per_s_one_by_one": round(alone, 1), "speedup_vs_one_by_one": round(rate / alone, 3),
+            "speedup_vs_one_launch_per_member": round(rate / sweep[1]["member_steps_per_s"], 3),
+            "timing": "host wall clock around synchronising calls"}
 
 
 def cpu_steps(N, M, budget_s, min_steps=1, max_steps=None):
@@ -558,6 +575,8 @@ def ours(args):
                                             "scalar_spectrum_rel_err_after_K_steps": float(np.max(np.abs(P32[livep] - P64[livep]) / P64[livep]))}}
         if ws == 1 and args.extras == "dealiasing":
             line["dealiasing"] = dealiasing_cost(args, device, inputs)
+        if ws == 1 and args.extras == "ensemble":
+            line.setdefault("forms", {})["ensemble"] = ensemble_rate(device)
         if ws == 1 and args.extras in ("all", "adjoint"):
             line["adjoint"] = adjoint_cost(args, device, inputs)
             if args.extras == "all":
@@ -607,7 +626,7 @@ def main():
                     help="the field integration scheme (the metric is quoted on IFLowStorageRK4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (quick kernel timing)")
-    ap.add_argument("--extras", default="all", choices=["all", "adjoint", "dealiasing", "none"],
+    ap.add_argument("--extras", default="all", choices=["all", "adjoint", "dealiasing", "ensemble", "none"],
                     help="the further legs rank 0 runs at N=1: the adjoint's cost, the 256^3 precision statistics "
                          "and the ensemble (all), the adjoint alone, or none")
     args = ap.parse_args()

@@ -3,7 +3,9 @@
 // each function's comment in gbght.h cites the interface it replaces.
 #include "../../include/gbght.h"
 
+#include <algorithm>
 #include <cmath>
+#include <map>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -539,11 +541,20 @@ int gbght_deposit(gbght_run* r) {
 struct gbght_ensemble {
   std::vector<gbght_run*> members;
   std::string err;
+  int batching = 1;   // the most members of equal group keys that share one launch per pass (≤ 1: none)
 #ifndef GBGHT_EMU
   cudaEvent_t fork = nullptr;
   std::vector<cudaEvent_t> join;
   cudaGraphExec_t exec = nullptr;
   double exec_dt = 0.0;
+  int units = 0;   // launching units of the captured graph (groups and lone members)
+  // the batching autotuner: candidate group sizes, the one being tried, its step (0: capture and
+  // run untimed, 1: timed replay), the replay times, the events that time them
+  std::vector<int> tune_cands;
+  size_t tune_i = 0;
+  int tune_phase = 0;
+  std::vector<float> tune_ms;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
 #endif
 };
 
@@ -557,31 +568,68 @@ void ens_release_graph(gbght_ensemble* e) {
   if (e->exec) cudaGraphExecDestroy(e->exec);
   e->exec = nullptr;
 }
-// Capture every member's step and deposit launches as one graph: member 0's stream forks to the
-// others through an event and joins them back at the end.
+// Capture every member's step and deposit launches as one graph. With batching on, members with
+// equal group keys form a group whose first member launches each pass once for all of them (its
+// launch records are built before the capture); every other member launches its own. Member 0's
+// stream forks to the other launching streams through an event and joins them back at the end.
 int ens_capture(gbght_ensemble* e, double dt) {
   ens_release_graph(e);
+  std::vector<std::vector<gbght_run*>> units;   // a group (first member launches) or a lone member
+  for (gbght_run* m : e->members) {
+    const uint64_t key = e->batching >= 2 ? m->eng->group_key() : 0;
+    bool placed = false;
+    for (auto& u : units)
+      if (key != 0 && int(u.size()) < e->batching && u[0]->eng->group_key() == key) {
+        u.push_back(m);
+        placed = true;
+        break;
+      }
+    if (!placed) units.push_back({m});
+  }
+  for (auto& u : units) {
+    if (u.size() < 2) continue;
+    std::vector<gbght::Engine*> engines;
+    for (gbght_run* m : u) engines.push_back(m->eng.get());
+    const Tableau t = tableau(u[0]->cfg.scheme);
+    if (const char* err = u[0]->eng->group_prepare(engines.data(), int(engines.size()), dt, t.a, t.b, t.d, t.S))
+      return ens_fail(e, GBGHT_ERR_CUDA, err);
+  }
+  e->units = int(units.size());
   cudaStream_t s0 = static_cast<cudaStream_t>(e->members[0]->eng->cuda_stream());
   cudaError_t ce = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal);
   if (ce != cudaSuccess) return ens_fail(e, GBGHT_ERR_CUDA, std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(ce));
   const char* err = nullptr;
-  cudaEventRecord(e->fork, s0);
-  for (size_t i = 1; i < e->members.size(); ++i)
-    cudaStreamWaitEvent(static_cast<cudaStream_t>(e->members[i]->eng->cuda_stream()), e->fork, 0);
-  for (gbght_run* m : e->members) {
-    const Tableau t = tableau(m->cfg.scheme);
-    if (!err) err = m->eng->step(dt, t.a, t.b, t.d, t.S);
-    if (!err) err = m->eng->deposit_launch();
+  std::string where;   // the first failing call, for the message
+  auto api = [&](cudaError_t r, const char* what, size_t unit) {
+    if (r != cudaSuccess && where.empty())
+      where = std::string(what) + " (unit " + std::to_string(unit) + "): " + cudaGetErrorString(r);
+  };
+  api(cudaEventRecord(e->fork, s0), "cudaEventRecord(fork)", 0);
+  for (size_t i = 1; i < units.size(); ++i)
+    api(cudaStreamWaitEvent(static_cast<cudaStream_t>(units[i][0]->eng->cuda_stream()), e->fork, 0),
+        "cudaStreamWaitEvent(fork)", i);
+  for (size_t i = 0; i < units.size(); ++i) {
+    auto& u = units[i];
+    if (u.size() >= 2) {
+      if (!err) err = u[0]->eng->group_launch();
+    } else {
+      const Tableau t = tableau(u[0]->cfg.scheme);
+      if (!err) err = u[0]->eng->step(dt, t.a, t.b, t.d, t.S);
+      if (!err) err = u[0]->eng->deposit_launch();
+    }
+    if (err && where.empty()) where = std::string(err) + " (unit " + std::to_string(i) + ")";
   }
-  for (size_t i = 1; i < e->members.size(); ++i) {
-    cudaEventRecord(e->join[i], static_cast<cudaStream_t>(e->members[i]->eng->cuda_stream()));
-    cudaStreamWaitEvent(s0, e->join[i], 0);
+  for (size_t i = 1; i < units.size(); ++i) {
+    api(cudaEventRecord(e->join[i], static_cast<cudaStream_t>(units[i][0]->eng->cuda_stream())),
+        "cudaEventRecord(join)", i);
+    api(cudaStreamWaitEvent(s0, e->join[i], 0), "cudaStreamWaitEvent(join)", i);
   }
+  if (!where.empty() && !err) err = "capture";
   cudaGraph_t graph = nullptr;
   ce = cudaStreamEndCapture(s0, &graph);
   if (err || ce != cudaSuccess) {
     if (graph) cudaGraphDestroy(graph);
-    return ens_fail(e, GBGHT_ERR_CUDA, err ? std::string(err) : std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce));
+    return ens_fail(e, GBGHT_ERR_CUDA, !where.empty() ? where : std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce));
   }
   ce = cudaGraphInstantiate(&e->exec, graph, 0);
   cudaGraphDestroy(graph);
@@ -639,6 +687,8 @@ void gbght_ensemble_destroy(gbght_ensemble* e) {
   if (!e) return;
 #ifndef GBGHT_EMU
   ens_release_graph(e);
+  if (e->t0) cudaEventDestroy(e->t0);
+  if (e->t1) cudaEventDestroy(e->t1);
   if (e->fork) cudaEventDestroy(e->fork);
   for (cudaEvent_t ev : e->join)
     if (ev) cudaEventDestroy(ev);
@@ -647,6 +697,64 @@ void gbght_ensemble_destroy(gbght_ensemble* e) {
 }
 
 const char* gbght_ensemble_last_error(const gbght_ensemble* e) { return e ? e->err.c_str() : "null ensemble"; }
+
+int gbght_ensemble_set_batching(gbght_ensemble* e, int max_group) {
+  if (!e || max_group < 0) return GBGHT_ERR_ARGUMENT;
+  if (max_group < 1) max_group = 1;
+  if (e->batching != max_group) {
+    e->batching = max_group;
+#ifndef GBGHT_EMU
+    ens_release_graph(e);   // recaptured at the next step
+#endif
+  }
+  return GBGHT_OK;
+}
+
+int gbght_ensemble_autotune(gbght_ensemble* e) {
+  if (!e) return GBGHT_ERR_ARGUMENT;
+#ifndef GBGHT_EMU
+  // candidates: 1 (no batching), then 2, 4, … up to the largest set of members with one group key
+  std::map<uint64_t, int> count;
+  int largest = 1;
+  for (gbght_run* m : e->members) {
+    const uint64_t k = m->eng->group_key();
+    if (k) largest = std::max(largest, ++count[k]);
+  }
+  e->tune_cands.clear();
+  e->tune_ms.clear();
+  for (int c = 1; c < largest; c *= 2) e->tune_cands.push_back(c);
+  if (largest > 1) e->tune_cands.push_back(largest);
+  e->tune_i = e->tune_cands.size() > 1 ? 0 : e->tune_cands.size();
+  e->tune_phase = 0;
+  if (!e->t0 && cudaEventCreate(&e->t0) != cudaSuccess) return ens_fail(e, GBGHT_ERR_CUDA, "cudaEventCreate");
+  if (!e->t1 && cudaEventCreate(&e->t1) != cudaSuccess) return ens_fail(e, GBGHT_ERR_CUDA, "cudaEventCreate");
+#endif
+  return GBGHT_OK;
+}
+
+int gbght_ensemble_tuning(const gbght_ensemble* e, int* batching, int* done, float* ms, int capacity) {
+  if (!e || !batching || !done) return GBGHT_ERR_ARGUMENT;
+  *batching = e->batching;
+#ifdef GBGHT_EMU
+  *done = 1;
+  (void)ms;
+  (void)capacity;
+#else
+  *done = e->tune_i >= e->tune_cands.size();
+  for (int i = 0; ms && i < capacity && size_t(i) < e->tune_ms.size(); ++i) ms[i] = e->tune_ms[i];
+#endif
+  return GBGHT_OK;
+}
+
+int gbght_ensemble_units(const gbght_ensemble* e, int* units) {
+  if (!e || !units) return GBGHT_ERR_ARGUMENT;
+#ifdef GBGHT_EMU
+  *units = 0;
+#else
+  *units = e->exec ? e->units : 0;
+#endif
+  return GBGHT_OK;
+}
 
 int gbght_ensemble_step(gbght_ensemble* e, double dt) {
   if (!e) return GBGHT_ERR_ARGUMENT;
@@ -668,12 +776,42 @@ int gbght_ensemble_step(gbght_ensemble* e, double dt) {
   }
   return GBGHT_OK;
 #else
-  if (!e->exec || e->exec_dt != dt)
+  const bool tuning = e->tune_i < e->tune_cands.size();
+  if (tuning && e->tune_phase == 0 && e->batching != e->tune_cands[e->tune_i]) {
+    e->batching = e->tune_cands[e->tune_i];
+    ens_release_graph(e);
+  }
+  if (!e->exec || e->exec_dt != dt) {
     if (int rc = ens_capture(e, dt)) return rc;
+    if (tuning) e->tune_phase = 0;   // a capture step is not timed
+  }
   cudaStream_t s0 = static_cast<cudaStream_t>(e->members[0]->eng->cuda_stream());
-  cudaError_t ce = cudaGraphLaunch(e->exec, s0);
+  const bool timed = tuning && e->tune_phase == 1;
+  cudaError_t ce = timed ? cudaEventRecord(e->t0, s0) : cudaSuccess;
+  if (ce == cudaSuccess) ce = cudaGraphLaunch(e->exec, s0);
+  if (ce == cudaSuccess && timed) ce = cudaEventRecord(e->t1, s0);
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(s0);
   if (ce != cudaSuccess) return ens_fail(e, GBGHT_ERR_CUDA, std::string("ensemble graph: ") + cudaGetErrorString(ce));
+  if (tuning) {
+    if (timed) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e->t0, e->t1);
+      e->tune_ms.push_back(ms);
+      e->tune_i += 1;
+      e->tune_phase = 0;
+      if (e->tune_i == e->tune_cands.size()) {   // keep the fastest
+        size_t best = 0;
+        for (size_t i = 1; i < e->tune_ms.size(); ++i)
+          if (e->tune_ms[i] < e->tune_ms[best]) best = i;
+        if (e->batching != e->tune_cands[best]) {
+          e->batching = e->tune_cands[best];
+          ens_release_graph(e);
+        }
+      }
+    } else {
+      e->tune_phase = 1;
+    }
+  }
   for (gbght_run* m : e->members) {
     m->fields_epoch += 1;
     double m2 = 0.0;

@@ -154,6 +154,7 @@ class EngineImpl final : public Engine {
 #endif
     for (void* p : allocs_) rt_free(p);
 #ifndef GBGHT_EMU
+    if (grp_) rt_free(grp_);
     if (stream_) cudaStreamDestroy(stream_);
 #endif
   }
@@ -378,25 +379,27 @@ class EngineImpl final : public Engine {
       st.lin_phi = lphi;
     }
   }
-  const char* step(double dt, const double* a, const double* b, const double* d, int S) override {
+  // The stages of one step of the run's scheme, with their arguments, into out[] (at most
+  // kStepStages); returns their count.
+  static constexpr int kStepStages = 5;
+  int stage_list(double dt, const double* a, const double* b, const double* d, int S, StageArgs* out) const {
     if (p_.scheme == 2) {   // IFHeun: predictor, corrector
-      StageArgs st = stage_base(dt);
-      st.kind = kHeunPredictor;
-      st.first = 1;
-      st.write_h = 1;
-      set_factor(st, dt, false);
-      if (const char* err = stage(st)) return err;
-      st = stage_base(dt);
-      st.kind = kHeunCorrector;
-      st.last = 1;
-      st.read_h = 1;
-      if (const char* err = stage(st)) return err;
-      return rt_check();
+      out[0] = stage_base(dt);
+      out[0].kind = kHeunPredictor;
+      out[0].first = 1;
+      out[0].write_h = 1;
+      set_factor(out[0], dt, false);
+      out[1] = stage_base(dt);
+      out[1].kind = kHeunCorrector;
+      out[1].last = 1;
+      out[1].read_h = 1;
+      return 2;
     }
     if (p_.scheme == 3) {   // IFSSPRK3: forward to t_n+1, back to the midpoint, forward again
       const double span1[3] = {dt, -dt / 2, dt / 2}, span2[3] = {0.0, dt / 2, dt};
       for (int i = 0; i < 3; ++i) {
-        StageArgs st = stage_base(dt);
+        StageArgs& st = out[i];
+        st = stage_base(dt);
         st.kind = kSsp1 + i;
         st.first = i == 0;
         st.last = i == 2;
@@ -404,12 +407,12 @@ class EngineImpl final : public Engine {
         st.write_h = i == 0;
         set_factor(st, span1[i], false);
         if (i > 0) set_factor(st, span2[i], true);
-        if (const char* err = stage(st)) return err;
       }
-      return rt_check();
+      return 3;
     }
-    for (int i = 0; i < S; ++i) {   // the low-storage 2N schemes
-      StageArgs st = stage_base(dt);
+    for (int i = 0; i < S && i < kStepStages; ++i) {   // the low-storage 2N schemes
+      StageArgs& st = out[i];
+      st = stage_base(dt);
       st.kind = kLowStorage;
       st.a = a[i];
       st.b = b[i];
@@ -418,8 +421,15 @@ class EngineImpl final : public Engine {
       st.read_h = !st.first;
       st.write_h = !st.last;
       set_factor(st, d[i] * dt, false);
-      if (const char* err = stage(st)) return err;
     }
+    return S;
+  }
+  const char* step(double dt, const double* a, const double* b, const double* d, int S) override {
+    if (S > kStepStages) return "a scheme of more stages than the step holds";
+    StageArgs st[kStepStages];
+    const int n = stage_list(dt, a, b, d, S, st);
+    for (int i = 0; i < n; ++i)
+      if (const char* err = stage(st[i])) return err;
     return rt_check();
   }
 
@@ -444,6 +454,117 @@ class EngineImpl final : public Engine {
   }
   bool deposit_fresh() const override { return bu_fresh_; }
   bool profiling() const override { return prof_on_; }
+
+  // ---- member-batched stepping (an ensemble's groups) ----------------------------------------------
+  // The key: precision, N, the dealiasing instantiation, the scheme, the scalar, the velocity
+  // forcing's kind. Runs that step alone: PhaseShift (its displaced passes), StochasticOU sources,
+  // VarianceController and VarianceRescaling (row sums, the post-step rescale).
+  uint64_t group_key() const override {
+#ifdef GBGHT_EMU
+    return 0;
+#else
+    const int vk = p_.vf.kind, sk = p_.scalar ? p_.sf.kind : int(kForceNone);
+    if (phase_ || src_[0] || src_[1]) return 0;
+    if (!(vk == kForceNone || vk == kForceConstantPower || vk == kForceLinear)) return 0;
+    if (!(sk == kForceNone || sk == kForceLinear)) return 0;
+    uint64_t k = uint64_t(sizeof(T));
+    k = k * 1024 + uint64_t(N);
+    k = k * 4 + uint64_t(DEA);
+    k = k * 8 + uint64_t(p_.scheme);
+    k = k * 2 + uint64_t(p_.scalar);
+    k = k * 8 + uint64_t(vk);
+    return k;
+#endif
+  }
+#ifdef GBGHT_EMU
+  const char* group_prepare(Engine* const*, int, double, const double*, const double*, const double*, int) override {
+    return "member-batched stepping runs on the device only";
+  }
+  const char* group_launch() override { return "member-batched stepping runs on the device only"; }
+#else
+  const char* group_prepare(Engine* const* ms, int n, double dt, const double* a, const double* b, const double* d,
+                            int S) override {
+    if (n < 1 || S > kStepStages || kStepStages > kGroupStages) return "bad group";
+    std::vector<GroupMember<T>> h(static_cast<size_t>(n));
+    std::vector<EngineImpl*> members(static_cast<size_t>(n));
+    const uint64_t key = group_key();
+    for (int i = 0; i < n; ++i) {
+      EngineImpl* m = dynamic_cast<EngineImpl*>(ms[i]);
+      if (!m || key == 0 || m->group_key() != key) return "a group member launches other kernels";
+      members[size_t(i)] = m;
+      GroupMember<T>& r = h[size_t(i)];
+      std::memset(static_cast<void*>(&r), 0, sizeof r);
+      r.maps = m->maps_;
+      r.g = m->g_;
+      r.A = m->A_;
+      r.B = m->B_;
+      r.S = m->S_;
+      r.H = m->H_;
+      r.U = m->U_;
+      r.partial = m->partial_;
+      r.amp = m->amp_;
+      r.status = m->status_;
+      r.maxbits = m->maxbits_;
+      r.ntile = int(m->ntile_);
+      r.band_lo2 = m->band_lo2();
+      r.band_hi2 = m->band_hi2();
+      r.vamp = m->amp_args(m->p_.vf, false);
+      grp_nst_ = m->stage_list(dt, a, b, d, S, r.st);
+    }
+    const size_t bytes = size_t(n) * sizeof(GroupMember<T>);
+    if (bytes > grp_bytes_) {
+      if (grp_) rt_free(grp_);
+      grp_ = nullptr;
+      grp_bytes_ = 0;
+      if (const char* e = rt_alloc(reinterpret_cast<void**>(&grp_), bytes)) return e;
+      grp_bytes_ = bytes;
+    }
+    if (const char* e = rt_h2d(grp_, h.data(), bytes, stream_)) return e;
+    for (int i = 0; i < grp_nst_; ++i) grp_st_[i] = h[0].st[i];
+    grp_members_ = members;
+    return rt_sync(stream_);
+  }
+  const char* group_launch() override {
+    const int n = int(grp_members_.size());
+    if (n < 1 || !grp_) return "the group is not prepared";
+    for (EngineImpl* m : grp_members_)
+      if (!m->bu_fresh_) return "a group member's deposit is not current";
+    const int ninv = p_.scalar ? 7 : 6, nfwd = p_.scalar ? 6 : 3, nc = p_.scalar ? 4 : 3;
+    const int KXS = x_kxs(g_.K, int(sizeof(Cplx<T>)));
+    const int gx = g_.KXP / TLZ;
+    const int xgrid = ((N / XShape<T>::P) * N + XT - 1) / XT, vgrid = ((N / XShape<T>::PV) * N + XT - 1) / XT;
+    const GroupMember<T>* G = grp_;
+    for (int i = 0; i < grp_nst_; ++i) {
+      const StageArgs& st = grp_st_[i];
+      // the first stage reuses the deposit's y-inverse of the velocity slots
+      const int c0 = i == 0 ? 3 : 0;
+      kg_y_inverse<T, N, TLY, NTY><<<dim3(g_.KXP / TLY, N, (ninv - c0) * n), NTY, smem_y(), stream_>>>(G, c0, ninv - c0, tw_);
+      kg_x_products<T, N, NTXP><<<dim3(xgrid, n), NTXP, smem_x(), stream_>>>(G, p_.scalar, KXS, tw_);
+      kg_y_forward<T, N, TLY, NTY><<<dim3(g_.KXP / TLY, N, nfwd * n), NTY, smem_y(), stream_>>>(G, nfwd, tw_);
+      if (st.forced) kg_force_amp<T><<<n, 256, 0, stream_>>>(G);
+      const dim3 zg(unsigned(gx), unsigned(g_.NY2), unsigned(n));
+      switch (st.kind) {
+        case kHeunPredictor: kg_z_epilogue<T, N, TLZ, NTZ, kHeunPredictor, KM, (DEA != 0)><<<zg, NTZ, smem_ze(), stream_>>>(G, i, tw_); break;
+        case kHeunCorrector: kg_z_epilogue<T, N, TLZ, NTZ, kHeunCorrector, KM, (DEA != 0)><<<zg, NTZ, smem_ze(), stream_>>>(G, i, tw_); break;
+        case kSsp1: kg_z_epilogue<T, N, TLZ, NTZ, kSsp1, KM, (DEA != 0)><<<zg, NTZ, smem_ze(), stream_>>>(G, i, tw_); break;
+        case kSsp2: kg_z_epilogue<T, N, TLZ, NTZ, kSsp2, KM, (DEA != 0)><<<zg, NTZ, smem_ze(), stream_>>>(G, i, tw_); break;
+        case kSsp3: kg_z_epilogue<T, N, TLZ, NTZ, kSsp3, KM, (DEA != 0)><<<zg, NTZ, smem_ze(), stream_>>>(G, i, tw_); break;
+        default: kg_z_epilogue<T, N, TLZ, NTZ, kLowStorage, KM, (DEA != 0)><<<zg, NTZ, smem_ze(), stream_>>>(G, i, tw_);
+      }
+      if (st.last) {   // the reality projection, then the first tile column of A rebuilt
+        kg_reality<T><<<dim3(unsigned((g_.NY2 * g_.NY2 + 255) / 256), unsigned(n)), 256, 0, stream_>>>(G, nc);
+        kg_z_init_column<T, N, TLZ, NTZ, KM><<<dim3(1, unsigned(g_.NY2), unsigned(n)), NTZ, smem_z(), stream_>>>(
+            G, p_.scalar, gx, tw_);
+      }
+    }
+    // the closing deposit: the velocity's y-inverse into B slots 0..2, its physical values and max|u|²
+    kg_zero_maxbits<T><<<unsigned((n + 127) / 128), 128, 0, stream_>>>(G, n);
+    kg_y_inverse<T, N, TLY, NTY><<<dim3(g_.KXP / TLY, N, 3 * n), NTY, smem_y(), stream_>>>(G, 0, 3, tw_);
+    kg_x_velocity<T, N, NTXV><<<dim3(vgrid, n), NTXV, smem_xv(), stream_>>>(G, KXS, tw_);
+    for (EngineImpl* m : grp_members_) m->bu_fresh_ = true;
+    return rt_check();
+  }
+#endif
   const char* deposit_read(double* max_speed2) override {
     const char* err = nullptr;
     unsigned long long bits = 0;
@@ -1105,12 +1226,31 @@ class EngineImpl final : public Engine {
 #ifndef GBGHT_EMU
   const char* set_smem_attributes() {
     const char* e = nullptr;
+    // The attribute belongs to the kernel, not to this run: runs of the same precision and N with
+    // different retained bands (TwoThirds beside HouLi or PhaseShift) share kernels whose shared
+    // memory grows with K, so the attribute is only ever raised, never lowered below what another
+    // run's launches need.
     auto set = [&](const void* f, size_t bytes) {
-      if (!e) e = cuda_err(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)),
-                           "cudaFuncSetAttribute");
+      if (e) return;
+      cudaFuncAttributes fa{};
+      e = cuda_err(cudaFuncGetAttributes(&fa, f), "cudaFuncGetAttributes");
+      if (!e && size_t(fa.maxDynamicSharedSizeBytes) < bytes)
+        e = cuda_err(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)),
+                     "cudaFuncSetAttribute");
     };
     set(reinterpret_cast<const void*>(k_y_inverse<T, N, TLY, NTY>), smem_y());
     set(reinterpret_cast<const void*>(k_y_forward<T, N, TLY, NTY>), smem_y());
+    set(reinterpret_cast<const void*>(kg_y_inverse<T, N, TLY, NTY>), smem_y());
+    set(reinterpret_cast<const void*>(kg_y_forward<T, N, TLY, NTY>), smem_y());
+    set(reinterpret_cast<const void*>(kg_x_products<T, N, NTXP>), smem_x());
+    set(reinterpret_cast<const void*>(kg_x_velocity<T, N, NTXV>), smem_xv());
+    set(reinterpret_cast<const void*>(kg_z_epilogue<T, N, TLZ, NTZ, kLowStorage, KM, (DEA != 0)>), smem_ze());
+    set(reinterpret_cast<const void*>(kg_z_epilogue<T, N, TLZ, NTZ, kHeunPredictor, KM, (DEA != 0)>), smem_ze());
+    set(reinterpret_cast<const void*>(kg_z_epilogue<T, N, TLZ, NTZ, kHeunCorrector, KM, (DEA != 0)>), smem_ze());
+    set(reinterpret_cast<const void*>(kg_z_epilogue<T, N, TLZ, NTZ, kSsp1, KM, (DEA != 0)>), smem_ze());
+    set(reinterpret_cast<const void*>(kg_z_epilogue<T, N, TLZ, NTZ, kSsp2, KM, (DEA != 0)>), smem_ze());
+    set(reinterpret_cast<const void*>(kg_z_epilogue<T, N, TLZ, NTZ, kSsp3, KM, (DEA != 0)>), smem_ze());
+    set(reinterpret_cast<const void*>(kg_z_init_column<T, N, TLZ, NTZ, KM>), smem_z());
     set(reinterpret_cast<const void*>(k_x_products<T, N, NTXP>), smem_x());
     set(reinterpret_cast<const void*>(k_x_velocity<T, N, NTXV>), smem_xv());
     set(reinterpret_cast<const void*>(k_z_epilogue<T, N, TLZ, NTZ, kLowStorage, KM, (DEA != 0)>), smem_ze());
@@ -1704,6 +1844,15 @@ class EngineImpl final : public Engine {
   bool phase_ = false;
   Cplx<T>* A2_ = nullptr;
   TmaMaps maps_ps_{};
+#ifndef GBGHT_EMU
+  // a member-batched group led by this run: the members' launch records on the device, the
+  // members, the step's stages
+  GroupMember<T>* grp_ = nullptr;
+  size_t grp_bytes_ = 0;
+  std::vector<EngineImpl*> grp_members_;
+  StageArgs grp_st_[kStepStages]{};
+  int grp_nst_ = 0;
+#endif
   double *LX_ = nullptr, *LF_ = nullptr, *LU_ = nullptr, *snapX_ = nullptr;   // the tracers' adjoint
 };
 

@@ -90,6 +90,16 @@ class Engine {
   virtual void* cuda_stream() const = 0;
   virtual bool deposit_fresh() const = 0;
   virtual bool profiling() const = 0;
+  // Member-batched stepping of an ensemble. group_key() is equal for runs whose step and deposit
+  // launch the same kernels with the same grids, and 0 for a run that steps alone (PhaseShift, a
+  // StochasticOU source, a forcing with per-stage row sums or a post-step rescale).
+  // group_prepare() builds the members' launch records in this (the first) member's device memory,
+  // synchronously, before a capture; group_launch() then issues the group's step and deposit, one
+  // launch per pass over all members, on this member's stream.
+  virtual uint64_t group_key() const = 0;
+  virtual const char* group_prepare(Engine* const* members, int n, double dt, const double* a, const double* b,
+                                    const double* d, int S) = 0;
+  virtual const char* group_launch() = 0;
   // a StochasticOU field's force for the next step: companion amplitudes [comp][nc][nc][nc/2+1]
   virtual const char* forcing_source(int field, const double* amplitudes, int nc) = 0;
   virtual const char* velocity_export(double* u) = 0;

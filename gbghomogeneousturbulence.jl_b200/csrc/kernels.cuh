@@ -25,14 +25,15 @@ __device__ __forceinline__ void init_bars(uint64_t* bar, int n) {
   __syncthreads();
 }
 
+// Each kernel's CTA runs a __device__ function of its arguments, so that a member-batched kernel
+// (one launch over the members of a group, below) runs the same code with one member's arguments.
 template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_y_inverse(const __grid_constant__ TmaMaps m, Geometry g, int c0,
-                                                     const Cplx<T>* tw, unsigned int* status) {
-  CTA_CTX;
+__device__ __forceinline__ void y_inverse_cta(const Cta& c, const TmaMaps& m, const Geometry& g, int comp,
+                                              const Cplx<T>* tw, unsigned int* status) {
   Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + N * TL);
   init_bars(bar, 1);
-  const int kx0 = c.bx * TL, z = c.by, comp = c0 + c.bz;
+  const int kx0 = c.bx * TL, z = c.by;
   if (c.tid == 0) {
     const int row0 = (comp * N + z) * g.NY2;
     mbar_expect_tx(bar, uint32_t(2 * (g.K + 1) * TL * sizeof(Cplx<T>)));
@@ -50,15 +51,20 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_y_inverse(const 
     bulk_wait_read();
   }
 }
+template <class T, int N, int TL, int NT>
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_y_inverse(const __grid_constant__ TmaMaps m, Geometry g, int c0,
+                                                     const Cplx<T>* tw, unsigned int* status) {
+  CTA_CTX;
+  y_inverse_cta<T, N, TL, NT>(c, m, g, c0 + c.bz, tw, status);
+}
 
 template <class T, int N, int TL, int NT>
-__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_y_forward(const __grid_constant__ TmaMaps m, Geometry g, const Cplx<T>* tw,
-                                                     unsigned int* status) {
-  CTA_CTX;
+__device__ __forceinline__ void y_forward_cta(const Cta& c, const TmaMaps& m, const Geometry& g, int comp,
+                                              const Cplx<T>* tw, unsigned int* status) {
   Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + N * TL);
   init_bars(bar, 1);
-  const int kx0 = c.bx * TL, z = c.by, comp = c.bz;
+  const int kx0 = c.bx * TL, z = c.by;
   constexpr int BY = box_rows<N>();
   if (c.tid == 0) {
     mbar_expect_tx(bar, uint32_t(N * TL * sizeof(Cplx<T>)));
@@ -76,24 +82,35 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_y_forward(const 
     bulk_wait_read();
   }
 }
+template <class T, int N, int TL, int NT>
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_y_forward(const __grid_constant__ TmaMaps m, Geometry g, const Cplx<T>* tw,
+                                                     unsigned int* status) {
+  CTA_CTX;
+  y_forward_cta<T, N, TL, NT>(c, m, g, c.bz, tw, status);
+}
 
 template <class T, int N, int NT>
-__global__ void __launch_bounds__(NT, XShape<T>::STAGED ? 2 : 3) k_x_products(Geometry g, Cplx<T>* B, int has_scalar,
-                                                                             int KXS, const Cplx<T>* tw,
-                                                                             unsigned int* status) {
-  CTA_CTX;
+__device__ __forceinline__ void x_products_cta(const Cta& c, const Geometry& g, Cplx<T>* B, int has_scalar, int KXS,
+                                               const Cplx<T>* tw, unsigned int* status) {
   Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
   Cplx<T>* stg = sm + N * XShape<T>::ACT_INV;
   uint64_t* bar = reinterpret_cast<uint64_t*>(stg + (XShape<T>::STAGED ? 7 * XShape<T>::P * KXS : 0));
   init_bars(bar, 1);
   body_x_products<T, N, NT>(c, sm, stg, KXS, bar, int(gridDim.x), g, B, has_scalar, tw, status);
 }
+template <class T, int N, int NT>
+__global__ void __launch_bounds__(NT, XShape<T>::STAGED ? 2 : 3) k_x_products(Geometry g, Cplx<T>* B, int has_scalar,
+                                                                             int KXS, const Cplx<T>* tw,
+                                                                             unsigned int* status) {
+  CTA_CTX;
+  x_products_cta<T, N, NT>(c, g, B, has_scalar, KXS, tw, status);
+}
 
 // Shared memory: the ACT_V lines, NT doubles, the staging rows (3·PV·KXS), one barrier (32 bytes).
 template <class T, int N, int NT>
-__global__ void __launch_bounds__(NT, 2) k_x_velocity(Geometry g, const Cplx<T>* B, T* u, unsigned long long* maxbits,
-                                                      int KXS, const Cplx<T>* tw, unsigned int* status) {
-  CTA_CTX;
+__device__ __forceinline__ void x_velocity_cta(const Cta& c, const Geometry& g, const Cplx<T>* B, T* u,
+                                               unsigned long long* maxbits, int KXS, const Cplx<T>* tw,
+                                               unsigned int* status) {
   Cplx<T>* sm = reinterpret_cast<Cplx<T>*>(g_smem);
   double* red = reinterpret_cast<double*>(sm + N * XShape<T>::ACT_V);
   Cplx<T>* stg = reinterpret_cast<Cplx<T>*>(red + NT);
@@ -101,6 +118,12 @@ __global__ void __launch_bounds__(NT, 2) k_x_velocity(Geometry g, const Cplx<T>*
   init_bars(bar, 1);
   const double mx = body_x_velocity<T, N, NT>(c, sm, red, stg, KXS, bar, int(gridDim.x), g, B, u, tw, status);
   if (c.tid == 0) atomicMax(maxbits, static_cast<unsigned long long>(__double_as_longlong(mx)));
+}
+template <class T, int N, int NT>
+__global__ void __launch_bounds__(NT, 2) k_x_velocity(Geometry g, const Cplx<T>* B, T* u, unsigned long long* maxbits,
+                                                      int KXS, const Cplx<T>* tw, unsigned int* status) {
+  CTA_CTX;
+  x_velocity_cta<T, N, NT>(c, g, B, u, maxbits, KXS, tw, status);
 }
 
 // The owned rows of a z tile (ZOwn) live in TMEM where every warp is fully active in every
@@ -132,11 +155,10 @@ __device__ __forceinline__ double with_z_rows(uint32_t* slot, const F& run) {
 
 // Shared memory: ZLayout (the FFT tile, NT doubles, barriers, the TMEM address, the twiddle table,
 // the staging region).
-template <class T, int N, int TL, int NT, int KIND, int KM = N / 3 + 1, bool WIDE = false>
-__global__ void __launch_bounds__(NT, NT > 256 ? 1 : (sizeof(T) == 8 ? 2 : 4)) k_z_epilogue(const __grid_constant__ TmaMaps m, Geometry g, Cplx<T>* A,
-                                                      Cplx<T>* S, Cplx<T>* H, StageArgs st, const double* amp,
-                                                      double* partial, const Cplx<T>* tw, unsigned int* status) {
-  CTA_CTX;
+template <class T, int N, int TL, int NT, int KIND, int KM, bool WIDE>
+__device__ __forceinline__ void z_epilogue_cta(const Cta& c, const TmaMaps& m, const Geometry& g, Cplx<T>* A,
+                                               Cplx<T>* S, Cplx<T>* H, const StageArgs& st, const double* amp,
+                                               double* partial, const Cplx<T>* tw, unsigned int* status) {
   using L = ZLayout<T, N, TL, NT>;
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
   double* red = reinterpret_cast<double*>(g_smem + L::kRed);
@@ -151,12 +173,18 @@ __global__ void __launch_bounds__(NT, NT > 256 ? 1 : (sizeof(T) == 8 ? 2 : 4)) k
   });
   if (c.tid == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = e;
 }
-
-template <class T, int N, int TL, int NT, int KM = N / 3 + 1>
-__global__ void __launch_bounds__(NT, NT > 256 ? 1 : 2) k_z_init(Geometry g, Cplx<T>* A, const Cplx<T>* S, int has_scalar, double* partial,
-                                                  const Cplx<T>* tw, int vorticity = 1, int pstride = 0,
-                                                  int shift = 0) {
+template <class T, int N, int TL, int NT, int KIND, int KM = N / 3 + 1, bool WIDE = false>
+__global__ void __launch_bounds__(NT, NT > 256 ? 1 : (sizeof(T) == 8 ? 2 : 4)) k_z_epilogue(const __grid_constant__ TmaMaps m, Geometry g, Cplx<T>* A,
+                                                      Cplx<T>* S, Cplx<T>* H, StageArgs st, const double* amp,
+                                                      double* partial, const Cplx<T>* tw, unsigned int* status) {
   CTA_CTX;
+  z_epilogue_cta<T, N, TL, NT, KIND, KM, WIDE>(c, m, g, A, S, H, st, amp, partial, tw, status);
+}
+
+template <class T, int N, int TL, int NT, int KM>
+__device__ __forceinline__ void z_init_cta(const Cta& c, const Geometry& g, Cplx<T>* A, const Cplx<T>* S,
+                                           int has_scalar, double* partial, const Cplx<T>* tw, int vorticity,
+                                           int pstride, int shift) {
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(g_smem);
   double* red = reinterpret_cast<double*>(W + N * TL);
   uint32_t* slot = reinterpret_cast<uint32_t*>(red + NT);
@@ -166,6 +194,13 @@ __global__ void __launch_bounds__(NT, NT > 256 ? 1 : 2) k_z_init(Geometry g, Cpl
   // pstride: the tiles per row of the partials (the full grid's, when a launch covers fewer columns);
   // no partials for the displaced grid's fields
   if (c.tid == 0 && partial) partial[blockIdx.y * (pstride ? pstride : gridDim.x) + blockIdx.x] = e;
+}
+template <class T, int N, int TL, int NT, int KM = N / 3 + 1>
+__global__ void __launch_bounds__(NT, NT > 256 ? 1 : 2) k_z_init(Geometry g, Cplx<T>* A, const Cplx<T>* S, int has_scalar, double* partial,
+                                                  const Cplx<T>* tw, int vorticity = 1, int pstride = 0,
+                                                  int shift = 0) {
+  CTA_CTX;
+  z_init_cta<T, N, TL, NT, KM>(c, g, A, S, has_scalar, partial, tw, vorticity, pstride, shift);
 }
 // PhaseShift's shift back of the displaced products into A (body_z_shift_back). Grid (KXP/TL, NY2).
 template <class T, int N, int TL, int NT, int KM>
@@ -201,9 +236,9 @@ __global__ void k_reality(Geometry g, Cplx<T>* S, int ncomp) {
 // the band sum runs over the box |m_a| ≤ mb. Each is summed per thread in a strided order and then
 // by a fixed tree, so the result is the same on every run. out[0..2] = (A, band, whole).
 template <class T>
-__global__ void k_force_amp(Geometry g, const Cplx<T>* S, int c0, int nc, const double* whole, const double* dir,
-                            int nwhole, int stride, double lo2, double hi2, AmpArgs a, double* out,
-                            unsigned int* status) {
+__device__ __forceinline__ void force_amp_cta(const Geometry& g, const Cplx<T>* S, int c0, int nc, const double* whole,
+                                              const double* dir, int nwhole, int stride, double lo2, double hi2,
+                                              const AmpArgs& a, double* out, unsigned int* status) {
   __shared__ double red[256], bred[256], dred[256];
   double s = 0.0, d = 0.0;
   for (int i = threadIdx.x; i < nwhole; i += 256) {
@@ -246,6 +281,12 @@ __global__ void k_force_amp(Geometry g, const Cplx<T>* S, int c0, int nc, const 
     out[1] = band_obs;
     out[2] = whole_obs;
   }
+}
+template <class T>
+__global__ void k_force_amp(Geometry g, const Cplx<T>* S, int c0, int nc, const double* whole, const double* dir,
+                            int nwhole, int stride, double lo2, double hi2, AmpArgs a, double* out,
+                            unsigned int* status) {
+  force_amp_cta<T>(g, S, c0, nc, whole, dir, nwhole, stride, lo2, hi2, a, out, status);
 }
 
 // VarianceRescaling's post-step rescale of slots [c0, c0 + nc) over the box |m_a| ≤ mb
@@ -416,6 +457,111 @@ __global__ void __launch_bounds__(32 * NW) k_phys_forward(Geometry g, const doub
 template <class T>
 __global__ void k_adj_add(size_t nS, int nc, Cplx<T>* L, const Cplx<T>* S, double wu, double wp) {
   adj_add_mode<T>(size_t(blockIdx.x) * blockDim.x + threadIdx.x, nS, nc, L, S, wu, wp);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Member-batched kernels: one launch runs a pass for every member of a group of runs with the same
+// kernels (precision, N, dealiasing instantiation, scheme, scalar and forcing kinds). Each member's
+// arguments are a GroupMember in device memory; the member index is the grid dimension the pass
+// does not use (z for the 2-D passes, y for the 1-D ones; the y passes fold it into z with the
+// component). A member's CTAs run the single-run kernel's CTA function with that member's
+// arguments: the same arithmetic, in a separate compilation, so a member stepped in a group agrees
+// with its lone step to round-off. The tensor maps are read from the member's record in global
+// memory, written by the host before the launch and acquired by the thread that issues the copies.
+// ------------------------------------------------------------------------------------------------
+constexpr int kGroupStages = 5;
+// the maps of a member's record, acquired by the thread that issues the TMA copies
+__device__ __forceinline__ void acquire_maps(const TmaMaps& m) {
+  if (threadIdx.x == 0) {
+    tensormap_acquire(&m.a_ld);
+    tensormap_acquire(&m.a_st1);
+    tensormap_acquire(&m.a_st2);
+    tensormap_acquire(&m.b);
+    tensormap_acquire(&m.az);
+    tensormap_acquire(&m.s3);
+    tensormap_acquire(&m.h3);
+  }
+}
+template <class T>
+struct alignas(64) GroupMember {
+  TmaMaps maps;
+  Geometry g;
+  Cplx<T>* A;
+  Cplx<T>* B;
+  Cplx<T>* S;
+  Cplx<T>* H;
+  T* U;
+  double* partial;
+  double* amp;
+  unsigned int* status;
+  unsigned long long* maxbits;
+  int ntile;                      // the epilogue's tile partials (ConstantPower's whole-field sum)
+  double band_lo2, band_hi2;      // the velocity forcing's band
+  AmpArgs vamp;                   // the velocity forcing's amplitude arguments
+  StageArgs st[kGroupStages];     // the step's stages
+};
+
+template <class T, int N, int TL, int NT>
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) kg_y_inverse(const GroupMember<T>* grp, int c0, int nc,
+                                                                         const Cplx<T>* tw) {
+  const GroupMember<T>& M = grp[blockIdx.z / nc];
+  acquire_maps(M.maps);
+  const Cta c{int(threadIdx.x), int(blockIdx.x), int(blockIdx.y), int(blockIdx.z % nc)};
+  y_inverse_cta<T, N, TL, NT>(c, M.maps, M.g, c0 + c.bz, tw, M.status);
+}
+template <class T, int N, int TL, int NT>
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) kg_y_forward(const GroupMember<T>* grp, int nc,
+                                                                         const Cplx<T>* tw) {
+  const GroupMember<T>& M = grp[blockIdx.z / nc];
+  acquire_maps(M.maps);
+  const Cta c{int(threadIdx.x), int(blockIdx.x), int(blockIdx.y), int(blockIdx.z % nc)};
+  y_forward_cta<T, N, TL, NT>(c, M.maps, M.g, c.bz, tw, M.status);
+}
+template <class T, int N, int NT>
+__global__ void __launch_bounds__(NT, XShape<T>::STAGED ? 2 : 3) kg_x_products(const GroupMember<T>* grp, int has_scalar,
+                                                                              int KXS, const Cplx<T>* tw) {
+  const GroupMember<T>& M = grp[blockIdx.y];
+  const Cta c{int(threadIdx.x), int(blockIdx.x), 0, 0};
+  x_products_cta<T, N, NT>(c, M.g, M.B, has_scalar, KXS, tw, M.status);
+}
+template <class T, int N, int NT>
+__global__ void __launch_bounds__(NT, 2) kg_x_velocity(const GroupMember<T>* grp, int KXS, const Cplx<T>* tw) {
+  const GroupMember<T>& M = grp[blockIdx.y];
+  const Cta c{int(threadIdx.x), int(blockIdx.x), 0, 0};
+  x_velocity_cta<T, N, NT>(c, M.g, M.B, M.U, M.maxbits, KXS, tw, M.status);
+}
+template <class T, int N, int TL, int NT, int KIND, int KM, bool WIDE>
+__global__ void __launch_bounds__(NT, NT > 256 ? 1 : (sizeof(T) == 8 ? 2 : 4)) kg_z_epilogue(const GroupMember<T>* grp,
+                                                                                            int stage, const Cplx<T>* tw) {
+  const GroupMember<T>& M = grp[blockIdx.z];
+  acquire_maps(M.maps);
+  const Cta c{int(threadIdx.x), int(blockIdx.x), int(blockIdx.y), 0};
+  z_epilogue_cta<T, N, TL, NT, KIND, KM, WIDE>(c, M.maps, M.g, M.A, M.S, M.H, M.st[stage], M.amp, M.partial, tw,
+                                               M.status);
+}
+// the first tile column of A rebuilt after the reality projection (grid (1, NY2, members))
+template <class T, int N, int TL, int NT, int KM>
+__global__ void __launch_bounds__(NT, NT > 256 ? 1 : 2) kg_z_init_column(const GroupMember<T>* grp, int has_scalar,
+                                                                       int pstride, const Cplx<T>* tw) {
+  const GroupMember<T>& M = grp[blockIdx.z];
+  const Cta c{int(threadIdx.x), int(blockIdx.x), int(blockIdx.y), 0};
+  z_init_cta<T, N, TL, NT, KM>(c, M.g, M.A, M.S, has_scalar, M.partial, tw, 1, pstride, 0);
+}
+template <class T>
+__global__ void kg_reality(const GroupMember<T>* grp, int ncomp) {
+  const GroupMember<T>& M = grp[blockIdx.y];
+  reality_mode<T>(int(blockIdx.x * blockDim.x + threadIdx.x), M.g, M.S, ncomp);
+}
+// ConstantPower's velocity amplitude from the epilogue's tile partials (grid (members), 256 threads)
+template <class T>
+__global__ void __launch_bounds__(256) kg_force_amp(const GroupMember<T>* grp) {
+  const GroupMember<T>& M = grp[blockIdx.x];
+  force_amp_cta<T>(M.g, M.S, 0, 3, M.partial, nullptr, M.ntile, 1, M.band_lo2, M.band_hi2, M.vamp, M.amp, M.status);
+}
+template <class T>
+__global__ void kg_zero_maxbits(const GroupMember<T>* grp, int n) {
+  const int i = int(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i < n) *grp[i].maxbits = 0ull;
 }
 #endif
 

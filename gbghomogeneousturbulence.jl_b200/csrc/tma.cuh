@@ -74,6 +74,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsign
 
 // 2-D and 3-D tiled loads into shared memory, completing on `bar`. Coordinates are in elements,
 // innermost first; the innermost coordinate times the element size is a multiple of 16 bytes.
+// A tensor map in global memory that the host wrote (a group's launch records): order that write
+// before the tensor-map proxy reads the map, from the thread that issues the copies.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+               : "memory");
+}
+
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(

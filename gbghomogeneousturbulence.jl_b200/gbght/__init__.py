@@ -101,6 +101,11 @@ _SIGNATURES = {
     "gbght_ensemble_destroy": (None, [C.c_void_p]),
     "gbght_ensemble_step": (C.c_int, [C.c_void_p, C.c_double]),
     "gbght_ensemble_last_error": (C.c_char_p, [C.c_void_p]),
+    "gbght_ensemble_set_batching": (C.c_int, [C.c_void_p, C.c_int]),
+    "gbght_ensemble_units": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "gbght_ensemble_autotune": (C.c_int, [C.c_void_p]),
+    "gbght_ensemble_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float),
+                                        C.c_int]),
     "gbght_deposit": (C.c_int, [C.c_void_p]),
     "gbght_max_speed": (C.c_int, [C.c_void_p, _DP]),
     "gbght_cfl_timestep": (C.c_int, [C.c_void_p, _DP]),
@@ -721,6 +726,34 @@ class Ensemble:
         if rc != OK:
             msg = self.lib.gbght_ensemble_last_error(self.h).decode()
             raise {ERR_ARGUMENT: ValueError, ERR_SCHEDULE: ScheduleError}.get(rc, DeviceError)(msg)
+
+    def set_batching(self, max_group):
+        """Member batching: one launch per pass for each group of at most `max_group` members with
+        the same kernels (True: every such member in one group), or one launch per member and pass
+        (False, 0 or 1; the default)."""
+        n = len(self.runs) if max_group is True else int(max_group or 0)
+        if self.lib.gbght_ensemble_set_batching(self.h, n) != OK:
+            raise ValueError("bad ensemble")
+
+    def autotune(self):
+        """Let the next steps time the group sizes 1, 2, 4, … (two steps each) and keep the fastest."""
+        if self.lib.gbght_ensemble_autotune(self.h) != OK:
+            raise DeviceError(self.lib.gbght_ensemble_last_error(self.h).decode())
+
+    def tuning(self):
+        """(group size in use, tuning done, replay milliseconds of the candidates tried so far)."""
+        b, d = C.c_int(), C.c_int()
+        ms = (C.c_float * 32)()
+        if self.lib.gbght_ensemble_tuning(self.h, C.byref(b), C.byref(d), ms, 32) != OK:
+            raise ValueError("bad ensemble")
+        return b.value, bool(d.value), [v for v in ms if v > 0]
+
+    def units(self) -> int:
+        """The launching units (groups and lone members) of the last captured graph."""
+        v = C.c_int()
+        if self.lib.gbght_ensemble_units(self.h, C.byref(v)) != OK:
+            raise ValueError("bad ensemble")
+        return v.value
 
     def close(self):
         if getattr(self, "h", None):

@@ -211,6 +211,24 @@ int gbght_ensemble_create(gbght_ensemble** out, gbght_run* const* members, int n
 void gbght_ensemble_destroy(gbght_ensemble* ensemble);
 int gbght_ensemble_step(gbght_ensemble* ensemble, double dt);
 const char* gbght_ensemble_last_error(const gbght_ensemble* ensemble);
+/* Member batching. Members whose step launches the same kernels (precision, N, dealiasing,
+ * scheme, scalar, velocity forcing kind; NoForcing, ConstantPower or Linear, and no PhaseShift or
+ * StochasticOU) may form groups of at most `max_group` members, and the graph then holds one
+ * launch per pass for each group instead of one per member. The group's kernels are a separate
+ * compilation of the same CTA code, so a member's results equal those of stepping it alone to
+ * round-off (not bit for bit: relative differences near 1e-16 in FP64 and 5e-8 in FP32-mixed after
+ * a step); members with equal inputs stay bitwise equal to each other. `max_group` ≤ 1 (the
+ * default) captures one launch per member and pass, bit for bit the lone steps.
+ * gbght_ensemble_autotune makes the following steps try group sizes 1, 2, 4, … up to the largest
+ * set of batchable members, two steps each (a capture, then a replay timed by CUDA events), and then
+ * keep the fastest; gbght_ensemble_tuning reports the current size, whether the tuning is done and
+ * the replay times so far (ms[i] for the i-th candidate). gbght_ensemble_units reports the
+ * launching units (groups and lone members) of the last captured graph, 0 before the first step.
+ * No reference counterpart: the reference steps one simulation per call. */
+int gbght_ensemble_set_batching(gbght_ensemble* ensemble, int max_group);
+int gbght_ensemble_autotune(gbght_ensemble* ensemble);
+int gbght_ensemble_tuning(const gbght_ensemble* ensemble, int* max_group, int* done, float* ms, int capacity);
+int gbght_ensemble_units(const gbght_ensemble* ensemble, int* units);
 
 /* A scheme's advective-CFL ceiling under the 2/3 rule: 0.96 (RK4), 0.5 (RK3, SSPRK3), 0.25 (Heun).
  * Replaces recommended_cfl(scheme, domain) (src/Propagator.jl:906-919) for TwoThirds. */

@@ -55,3 +55,15 @@ def test_houli_matches_the_oracle(cuda_library, N, precision, tol):
                           precision=precision, library=cuda_library)
     advance_both(run, orun, 5 if N == 64 else 2, dt=0.005)
     compare(run, orun, tol=tol, check_tracers=precision == "fp64")
+
+
+@pytest.mark.gpu
+def test_wide_and_two_thirds_runs_share_a_process(cuda_library):
+    # runs of one precision and N under different bands share kernels whose shared memory grows with
+    # K: a TwoThirds run built after a HouLi one must not shrink what the HouLi run's launches need
+    wide, _ = make_case(32, forcing=0.1, dealiasing="HouLi", library=cuda_library)
+    narrow, _ = make_case(32, forcing=0.1, library=cuda_library)
+    for r in (wide, narrow, wide):
+        r.advance(0.004)
+    wide.close()
+    narrow.close()
