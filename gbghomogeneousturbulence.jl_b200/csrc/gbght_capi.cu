@@ -316,6 +316,7 @@ void gbght_config_default(gbght_config* c) {
   c->dealiasing = GBGHT_TWO_THIRDS;
   c->houli_order = 36;
   c->houli_strength = 0.0;
+  c->tracer_gather = 0;
 }
 
 int gbght_recommended_cfl_dealiased(int scheme, int dealiasing, double* cfl) {
@@ -414,6 +415,8 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
     return bad("unknown dealiasing strategy (TwoThirds, HouLi and PhaseShift are built)");
   if (cfg->dealiasing == GBGHT_HOULI && (cfg->houli_order < 2 || cfg->houli_order % 2 || !std::isfinite(cfg->houli_strength)))
     return bad("HouLi's `order` must be an even integer ≥ 2 and its `strength` finite");
+  if (cfg->tracer_gather < 0 || cfg->tracer_gather > 2)
+    return bad("tracer_gather must be 0 (automatic), 1 (per tracer) or 2 (warp-cooperative)");
   if (!finite_positive(cfg->cfl)) return bad("cfl must be positive and finite");
   if (!(cfg->max_dt > 0)) return bad("max_dt must be positive");
 
@@ -440,6 +443,7 @@ int gbght_create(gbght_run** out, const gbght_config* cfg) {
   p.dealias = cfg->dealiasing;
   p.houli_order = cfg->houli_order;
   p.houli_strength = cfg->houli_strength;
+  p.tracer_gather = cfg->tracer_gather;
   p.device = cfg->device;
   if (const char* e = r->eng->init(p)) {
     g_global_error = e;

@@ -56,6 +56,7 @@ struct RunParams {
   int dealias;               // 0 TwoThirds, 1 HouLi, 2 PhaseShift
   int houli_order;           // HouLi's filter order (36 by default)
   double houli_strength;     // HouLi's strength; ≤ 0 for the default −log(eps(T))
+  int tracer_gather;         // Catmull–Rom gathers: 0 automatic, 1 one thread per tracer, 2 warp-cooperative
   int device;
 };
 

@@ -319,6 +319,17 @@ __global__ void k_tracers(int64_t M, const T* u, int N, double L, double* X, dou
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < M) tracer_one<T>(order ? int64_t(order[i]) : i, M, u, N, L, X, F, w);
 }
+// The warp-cooperative form for the Catmull–Rom gather: 16 lanes per tracer (two tracers per
+// warp, tracers taken in the traversal order), see tracer_group.
+template <class T>
+__global__ void __launch_bounds__(256) k_tracers_group(int64_t M, const T* u, int N, double L, double* X, double* F,
+                                                     const __grid_constant__ AdamsStep w, const uint32_t* order) {
+  const int64_t i = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 4;
+  const int sub = int(threadIdx.x & 15u);
+  const bool live = i < M;
+  const int64_t p = live ? (order ? int64_t(order[i]) : i) : 0;
+  tracer_group<T>(p, M, u, N, L, X, F, w, sub, live);
+}
 
 // The traversal rebuild, a counting sort by tile: keys and tile counts, an exclusive scan of the
 // counts (one block), then each tracer takes the next slot of its tile. The order within a tile

@@ -73,6 +73,49 @@ GBGHT_HD void cell_fraction(double x, double dx, int N, int& i, double& t) {
   t = sub_rn(q, f);
 }
 
+// The four x taps ix − 1 .. ix + 2 of one row of a physical field (rows 16-byte aligned: N·sizeof(T)
+// is a multiple of 16 for every supported N). Away from the row's ends the taps come in 16-byte
+// vector loads where their alignment allows (two for FP64 on an even start, one for FP32 on a start
+// divisible by 4), else in narrower aligned pieces; at the ends, one by one with the periodic wrap.
+// The values, and so every sum of them, are those of four scalar loads. The warp-cooperative gather
+// uses it (the lanes of a tracer share ix, so they take one branch); the per-tracer gather loads its
+// taps one by one, since its lanes' alignments differ and the branches diverge (its FP32 push took
+// 1.87 ms per 10⁶ tracers with these loads, 1.00 ms without).
+template <class T>
+GBGHT_HD void row_taps(const T* GBGHT_RESTRICT row, int ix, int N, double v[4]) {
+  const int x0 = ix - 1;
+#ifdef __CUDA_ARCH__
+  if (x0 >= 0 && x0 + 3 < N) {
+    if constexpr (sizeof(T) == 8) {
+      const double* r = reinterpret_cast<const double*>(row);
+      if ((x0 & 1) == 0) {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(r + x0));
+        const double2 b = __ldg(reinterpret_cast<const double2*>(r + x0 + 2));
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+      } else {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(r + x0 + 1));
+        v[0] = __ldg(r + x0); v[1] = a.x; v[2] = a.y; v[3] = __ldg(r + x0 + 3);
+      }
+    } else {
+      const float* r = reinterpret_cast<const float*>(row);
+      if ((x0 & 3) == 0) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(r + x0));
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+      } else if ((x0 & 1) == 0) {
+        const float2 a = __ldg(reinterpret_cast<const float2*>(r + x0));
+        const float2 b = __ldg(reinterpret_cast<const float2*>(r + x0 + 2));
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+      } else {
+        const float2 a = __ldg(reinterpret_cast<const float2*>(r + x0 + 1));
+        v[0] = __ldg(r + x0); v[1] = a.x; v[2] = a.y; v[3] = __ldg(r + x0 + 3);
+      }
+    }
+    return;
+  }
+#endif
+  for (int a = 0; a < 4; ++a) v[a] = double(ldg(row + (x0 + a + N) % N));
+}
+
 // Gather the three components of a physical field [3][N][N][N] at X; sums run x innermost,
 // then y, then z.
 template <class T>
@@ -87,9 +130,8 @@ GBGHT_HD void gather3(const T* GBGHT_RESTRICT u, int N, double dx, double x, dou
   catmull_rom(tx, wx);
   catmull_rom(ty, wy);
   catmull_rom(tz, wz);
-  int xs[4], ys[4], zs[4];
+  int ys[4], zs[4];
   for (int a = 0; a < 4; ++a) {
-    xs[a] = (ix + a - 1 + N) % N;
     ys[a] = (iy + a - 1 + N) % N;
     zs[a] = (iz + a - 1 + N) % N;
   }
@@ -101,8 +143,10 @@ GBGHT_HD void gather3(const T* GBGHT_RESTRICT u, int N, double dx, double x, dou
       double acc_y = 0.0;
       for (int cy = 0; cy < 4; ++cy) {
         const T* row = f + (size_t(zs[cz]) * N + ys[cy]) * N;
+        double tap[4];
+        for (int a = 0; a < 4; ++a) tap[a] = double(ldg(row + (ix + a - 1 + N) % N));
         double acc_x = 0.0;
-        for (int cx = 0; cx < 4; ++cx) acc_x = add_rn(acc_x, mul_rn(wx[cx], double(ldg(row + xs[cx]))));
+        for (int cx = 0; cx < 4; ++cx) acc_x = add_rn(acc_x, mul_rn(wx[cx], tap[cx]));
         acc_y = add_rn(acc_y, mul_rn(wy[cy], acc_x));
       }
       acc_z = add_rn(acc_z, mul_rn(wz[cz], acc_y));
@@ -309,10 +353,11 @@ struct AdamsStep {
 
 // One tracer. X is [3][M]; F is the trail's slots, 3·M doubles apart. Each displacement is summed
 // term by term in the weights' order, then added, and the position wrapped into [0, L).
-template <class T>
-GBGHT_HD void tracer_one(int64_t p, int64_t M, const T* GBGHT_RESTRICT u, int N, double L,
-                         double* GBGHT_RESTRICT X, double* GBGHT_RESTRICT F, const AdamsStep& w) {
-  const double dx = div_rn(L, double(N));
+// gather(x, y, z, out) interpolates the field; only a caller with `writes` stores (the
+// warp-cooperative form runs the tracer's scalar arithmetic on every lane of its group).
+template <class G>
+GBGHT_HD void tracer_step(int64_t p, int64_t M, double L, double* GBGHT_RESTRICT X, double* GBGHT_RESTRICT F,
+                          const AdamsStep& w, const G& gather, bool writes) {
   const size_t S3 = 3 * size_t(M);
   double x[3] = {X[p], X[M + p], X[2 * M + p]};
   if (w.J > 0) {
@@ -325,7 +370,7 @@ GBGHT_HD void tracer_one(int64_t p, int64_t M, const T* GBGHT_RESTRICT u, int N,
     for (int c = 0; c < 3; ++c) xs[c] = wrap_periodic(add_rn(x[c], disp[c]), L);
     if (w.corrected) {
       double fs[3];
-      gather_any(u, N, dx, xs[0], xs[1], xs[2], w.stencil, fs);
+      gather(xs[0], xs[1], xs[2], fs);
       for (int c = 0; c < 3; ++c) disp[c] = mul_rn(w.beta_star, fs[c]);
       for (int j = 0; j < w.J; ++j)
         for (int c = 0; c < 3; ++c)
@@ -334,13 +379,109 @@ GBGHT_HD void tracer_one(int64_t p, int64_t M, const T* GBGHT_RESTRICT u, int N,
     } else {
       for (int c = 0; c < 3; ++c) x[c] = xs[c];
     }
-    for (int c = 0; c < 3; ++c) X[c * M + p] = x[c];
+    if (writes)
+      for (int c = 0; c < 3; ++c) X[c * M + p] = x[c];
   }
   if (w.out_slot < 0) return;
   double f[3];
-  gather_any(u, N, dx, x[0], x[1], x[2], w.stencil, f);
-  for (int c = 0; c < 3; ++c) F[size_t(w.out_slot) * S3 + size_t(c) * M + p] = f[c];
+  gather(x[0], x[1], x[2], f);
+  if (writes)
+    for (int c = 0; c < 3; ++c) F[size_t(w.out_slot) * S3 + size_t(c) * M + p] = f[c];
 }
+template <class T>
+GBGHT_HD void tracer_one(int64_t p, int64_t M, const T* GBGHT_RESTRICT u, int N, double L,
+                         double* GBGHT_RESTRICT X, double* GBGHT_RESTRICT F, const AdamsStep& w) {
+  const double dx = div_rn(L, double(N));
+  tracer_step(p, M, L, X, F, w,
+              [&](double x, double y, double z, double* out) { gather_any(u, N, dx, x, y, z, w.stencil, out); }, true);
+}
+
+#if defined(__CUDACC__) && !defined(GBGHT_EMU)
+// The warp-cooperative tracer step: a group of 16 lanes per tracer. Lane a < 3 carries the
+// tracer's coordinate a through the Adams sums and the wrap, and takes axis a's cell and
+// Catmull–Rom weights; the group reads them by shuffles. Lane (cz, cy) = (sub / 4, sub mod 4) sums
+// the x taps of its (z, y) row for the three components, the lanes cy = 0 take the y sums over their
+// four rows and lane 0 the z sums. Every operation is the per-tracer path's (tracer_one, gather3),
+// on the same values in the same order with the same roundings, so the results are bit for bit
+// those of k_tracers. All 32 lanes of the warp run it (a group past M runs tracer 0 and stores
+// nothing).
+constexpr unsigned kFullWarp = 0xffffffffu;
+template <class T>
+__device__ __forceinline__ double gather3_group(const T* GBGHT_RESTRICT u, int N, double dx, double xa, int sub) {
+  int i = 0;
+  double w[4] = {0.0, 0.0, 0.0, 0.0};
+  if (sub < 3) {
+    double t;
+    cell_fraction(xa, dx, N, i, t);
+    catmull_rom(t, w);
+  }
+  const int ix = __shfl_sync(kFullWarp, i, 0, 16), iy = __shfl_sync(kFullWarp, i, 1, 16),
+            iz = __shfl_sync(kFullWarp, i, 2, 16);
+  double wx[4], wy[4], wz[4];
+  for (int a = 0; a < 4; ++a) {
+    wx[a] = __shfl_sync(kFullWarp, w[a], 0, 16);
+    wy[a] = __shfl_sync(kFullWarp, w[a], 1, 16);
+    wz[a] = __shfl_sync(kFullWarp, w[a], 2, 16);
+  }
+  const int cz = sub >> 2, cy = sub & 3;
+  const int zz = (iz + cz - 1 + N) % N, yy = (iy + cy - 1 + N) % N;
+  const size_t comp = size_t(N) * N * N;
+  double f[3];
+  for (int c = 0; c < 3; ++c) {
+    const T* row = u + c * comp + (size_t(zz) * N + yy) * N;
+    double tap[4];
+    row_taps(row, ix, N, tap);
+    double acc_x = 0.0;
+    for (int cx = 0; cx < 4; ++cx) acc_x = add_rn(acc_x, mul_rn(wx[cx], tap[cx]));
+    const double x1 = __shfl_down_sync(kFullWarp, acc_x, 1, 16);
+    const double x2 = __shfl_down_sync(kFullWarp, acc_x, 2, 16);
+    const double x3 = __shfl_down_sync(kFullWarp, acc_x, 3, 16);
+    double acc_y = 0.0;
+    acc_y = add_rn(acc_y, mul_rn(wy[0], acc_x));
+    acc_y = add_rn(acc_y, mul_rn(wy[1], x1));
+    acc_y = add_rn(acc_y, mul_rn(wy[2], x2));
+    acc_y = add_rn(acc_y, mul_rn(wy[3], x3));
+    const double y1 = __shfl_down_sync(kFullWarp, acc_y, 4, 16);
+    const double y2 = __shfl_down_sync(kFullWarp, acc_y, 8, 16);
+    const double y3 = __shfl_down_sync(kFullWarp, acc_y, 12, 16);
+    double acc_z = 0.0;
+    acc_z = add_rn(acc_z, mul_rn(wz[0], acc_y));
+    acc_z = add_rn(acc_z, mul_rn(wz[1], y1));
+    acc_z = add_rn(acc_z, mul_rn(wz[2], y2));
+    acc_z = add_rn(acc_z, mul_rn(wz[3], y3));
+    f[c] = __shfl_sync(kFullWarp, acc_z, 0, 16);
+  }
+  return sub == 1 ? f[1] : sub == 2 ? f[2] : f[0];   // lane a < 3: component a
+}
+template <class T>
+__device__ __forceinline__ void tracer_group(int64_t p, int64_t M, const T* GBGHT_RESTRICT u, int N, double L,
+                                             double* GBGHT_RESTRICT X, double* GBGHT_RESTRICT F, const AdamsStep& w,
+                                             int sub, bool live) {
+  const double dx = div_rn(L, double(N));
+  const size_t S3 = 3 * size_t(M);
+  const int c = sub < 3 ? sub : 0;   // lanes 3..15 repeat coordinate 0 and store nothing
+  const bool store = live && sub < 3;
+  double x = X[c * M + p];
+  if (w.J > 0) {
+    double disp = mul_rn(w.b[0], F[size_t(w.slot[0]) * S3 + size_t(c) * M + p]);
+    for (int j = 1; j < w.J; ++j) disp = add_rn(disp, mul_rn(w.b[j], F[size_t(w.slot[j]) * S3 + size_t(c) * M + p]));
+    const double xs = wrap_periodic(add_rn(x, disp), L);
+    if (w.corrected) {
+      const double fs = gather3_group(u, N, dx, xs, sub);
+      disp = mul_rn(w.beta_star, fs);
+      for (int j = 0; j < w.J; ++j)
+        disp = add_rn(disp, mul_rn(w.beta_m[j], F[size_t(w.slot[j]) * S3 + size_t(c) * M + p]));
+      x = wrap_periodic(add_rn(xs, disp), L);
+    } else {
+      x = xs;
+    }
+    if (store) X[c * M + p] = x;
+  }
+  if (w.out_slot < 0) return;
+  const double f = gather3_group(u, N, dx, x, sub);
+  if (store) F[size_t(w.out_slot) * S3 + size_t(c) * M + p] = f;
+}
+#endif
 
 // 4-point Gauss–Legendre Adams weights (src/ParticlePropagator.jl:263-280), host side.
 inline void adams_weights(const double* nodes, int n, double h, double* out) {

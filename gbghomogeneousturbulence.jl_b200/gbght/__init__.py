@@ -79,6 +79,7 @@ class Config(C.Structure):
         ("dealiasing", C.c_int),
         ("houli_order", C.c_int),
         ("houli_strength", C.c_double),
+        ("tracer_gather", C.c_int),
     ]
 
 
@@ -303,6 +304,7 @@ class Setup:
     dealiasing: str = "TwoThirds"    # or "HouLi", "PhaseShift" (src/SimulationDomain.jl:73-177)
     houli_order: int = 36
     houli_strength: float = 0.0      # ≤ 0: −log(eps) of the precision
+    tracer_gather: str = "auto"      # or "per_tracer", "warp" (16 lanes per tracer); bit-identical results
     cfl: float = 0.5
     max_dt: float = math.inf
     device: int = 0
@@ -348,6 +350,10 @@ class Run:
         cfg.dealiasing = DEALIASING[setup.dealiasing]
         cfg.houli_order = int(setup.houli_order)
         cfg.houli_strength = float(setup.houli_strength)
+        gathers = {"auto": 0, "per_tracer": 1, "warp": 2}
+        if setup.tracer_gather not in gathers:
+            raise ValueError(f"unknown tracer gather {setup.tracer_gather!r}")
+        cfg.tracer_gather = gathers[setup.tracer_gather]
         cfg.cfl = float(setup.cfl)
         cfg.max_dt = float(setup.max_dt)
         cfg.device = int(setup.device)

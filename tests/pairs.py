@@ -40,7 +40,8 @@ def oracle_forcing(f):
 def make_case(N, *, viscosity=0.01, schmidt=1.0, scalar=True, forcing=None, G=(0.0, 0.0, 0.0), tracers=0,
               scheme="IFLowStorageRK4", precision="fp64", cfl=0.5, seeds=(0, 1, 2), energy=0.5, variance=0.5,
               library=None, uh=None, ph=None, X=None, scalar_forcing=None, tracer_scheme=("Heun", 1),
-              shortened_first_steps=False, interpolation=("CatmullRom", 4, 1), dealiasing="TwoThirds"):
+              shortened_first_steps=False, interpolation=("CatmullRom", 4, 1), dealiasing="TwoThirds",
+              tracer_gather="auto"):
     """Build a library run and an oracle run on identical seeded inputs, both freshly deposited.
 
     `forcing` is a ConstantPower ε (a number) or a library forcing object; `scalar_forcing` is a
@@ -61,7 +62,7 @@ def make_case(N, *, viscosity=0.01, schmidt=1.0, scalar=True, forcing=None, G=(0
                         tracers=tracers, scheme=scheme, precision=precision, cfl=cfl,
                         tracer_scheme=tracer_scheme[0], tracer_steps=tracer_scheme[1],
                         shortened_first_steps=shortened_first_steps, interpolation=interpolation,
-                        dealiasing=dealiasing)
+                        dealiasing=dealiasing, tracer_gather=tracer_gather)
     run = gbght.simulation(setup, uh, ph if scalar else None, X, library=library)
     dom = O.Domain(N, dealiasing=dealiasing)
     cond = O.Conditions(viscosity=viscosity, schmidt=schmidt, scalar=scalar,
