@@ -389,8 +389,23 @@ GBGHT_HD void x_tile(const Cta& c, Cplx<T>* sm, const XProductStaging<T>& stage,
   const auto from_stg = [&](int l) { return LineOfSource<XStagedSource<T, N, P>>{src, l}; };
   const auto in_smem = [&](int l) { return LineBuf<T>{sm + l * N}; };
   warp_fft_lines<T, N, NW, NT, +1, 0, 1>(c, X::ACT_INV, lines, from_stg, in_smem, tw);
+  // The staging is free once every warp's first stage has read it. On the device only the issuing
+  // warp waits for that (barrier 1: the other warps arrive, with release semantics, and go on to
+  // their next stages, which touch only their own lines); the lines themselves are next read across
+  // warps at the turnaround, after the block barrier there.
+#if defined(__CUDA_ARCH__) && !defined(GBGHT_EMU)
+  if (next_z >= 0) {
+    if (c.tid < 32) {
+      asm volatile("barrier.sync 1, %0;" ::"r"(NT) : "memory");
+      stage.issue(c, next_z, next_y0);
+    } else {
+      asm volatile("barrier.arrive 1, %0;" ::"r"(NT) : "memory");
+    }
+  }
+#else
   GBGHT_SYNC();
   if (next_z >= 0) stage.issue(c, next_z, next_y0);
+#endif
   if constexpr (Radices<N>::n >= 2) {
     // inverse stages up to the last, then the turnaround (last inverse stage, products, first
     // forward stage), then the forward's remaining stages
@@ -444,7 +459,10 @@ GBGHT_HD void x_tile(const Cta& c, Cplx<T>* sm, const XProductStaging<T>& stage,
       }
     }
   }
-  GBGHT_SYNC();   // the lines are rewritten by the next tile's inverse
+  // The next tile's first inverse stage rewrites each line from the warp that owns it here (line l
+  // belongs to warp l mod NW in every warp-per-line stage and in the unpack), and every cross-warp
+  // read of the lines (the turnaround) ended at a block barrier, so the warp's own order suffices.
+  warp_sync();
 }
 
 // Tiles I, I+1, … < XT of this CTA (tile index bx + i·grid); tile I's spectra are already being
