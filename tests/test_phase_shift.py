@@ -163,3 +163,20 @@ def test_phase_shift_matches_the_oracle(cuda_library, N, precision, tol):
     run, orun = _case(N, cuda_library, precision=precision, tracers=1000)
     advance_both(run, orun, 4 if N == 64 else 2, dt=0.005)
     compare(run, orun, tol=tol, check_tracers=precision == "fp64")
+
+
+@pytest.mark.parametrize("forcing", ["Linear", "VarianceController", "VarianceRescaling", "StochasticOU"])
+def test_phase_shift_with_the_other_forcings_hostcheck(hostcheck_library, forcing):
+    # the displaced-grid average ahead of the forcings' sources and projections
+    vf = {"Linear": gbght.Linear(0.2), "VarianceController": gbght.VarianceController(0.3, 1.0),
+          "VarianceRescaling": gbght.VarianceRescaling(0.3, "total"),
+          "StochasticOU": gbght.StochasticOU(0.05, 0.5, 1, 2, seed=7)}[forcing]
+    dom = O.Domain(12, dealiasing="PhaseShift")
+    run, orun = make_case(12, viscosity=0.01, forcing=vf, dealiasing="PhaseShift", library=hostcheck_library,
+                          uh=_ball_field(dom, 1, mean_square=1.0), ph=_ball_field(dom, 2, ncomp=1, mean_square=1.0))
+    for _ in range(3):
+        run.advance(0.01)
+        if forcing == "StochasticOU":   # the oracle is given the force the library was given
+            orun.cond.velocity_forcing.process = run.processes[0].amplitudes.copy()
+        orun.advance(0.01)
+    compare(run, orun, tol=1e-12)
