@@ -1771,10 +1771,13 @@ class EngineImpl final : public Engine {
 #else
     const int bs = 128;
     pbegin(PROF_TRACERS);
-    // Catmull–Rom, warp-cooperative (16 lanes per tracer): chosen, or automatic in FP64, where it is
-    // the faster (1.26 against 1.65 ms per 10⁶-tracer push at 512³; in FP32 the per-tracer form is,
-    // 1.00 against 1.14 ms)
-    const bool warp = p_.tracer_gather == 2 || (p_.tracer_gather == 0 && sizeof(T) == 8);
+    // Catmull–Rom, warp-cooperative (16 lanes per tracer): chosen, or automatic in FP64 with sparse
+    // tracers (under one per 50 grid points), where it is the faster: 1.25 against 1.27 ms per
+    // 10⁶-tracer push at 512³ (one per 134 points). With dense tracers the per-tracer form's warps
+    // share cache lines and win (10⁶ at 256³, one per 17 points), and in FP32 it wins at 512³ too
+    // (0.91 against 1.14 ms).
+    const bool sparse = double(M) * 50.0 < double(N) * double(N) * double(N);
+    const bool warp = p_.tracer_gather == 2 || (p_.tracer_gather == 0 && sizeof(T) == 8 && sparse);
     if (w.stencil.n == 0 && warp) {
       const int64_t threads = 16 * M;
       k_tracers_group<T><<<unsigned((threads + 255) / 256), 256, 0, stream_>>>(M, U_, N, p_.L, X, F, w, order);

@@ -124,9 +124,9 @@ typedef struct gbght_config {
   int houli_order;            /* HouLi's filter order (default 36) */
   double houli_strength;      /* HouLi's damping at the Nyquist mode; ≤ 0: −log(eps) of the precision */
   int tracer_gather;          /* Catmull–Rom gathers: 0 automatic (the default: warp-cooperative in
-                                 FP64, per tracer in FP32-mixed, the faster measured in each), 1 one
-                                 thread per tracer, 2 warp-cooperative (16 lanes per tracer); all
-                                 agree bit for bit */
+                                 FP64 with fewer tracers than one per 50 grid points, else per
+                                 tracer, the faster measured in each case), 1 one thread per tracer,
+                                 2 warp-cooperative (16 lanes per tracer); all agree bit for bit */
 } gbght_config;
 
 /* The dealiasing strategies (src/SimulationDomain.jl:73-177). TWO_THIRDS: the closed 2/3 ball, the
