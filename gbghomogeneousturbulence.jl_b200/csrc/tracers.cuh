@@ -143,7 +143,8 @@ GBGHT_HD void gather3(const T* GBGHT_RESTRICT u, int N, double dx, double x, dou
       double acc_y = 0.0;
       for (int cy = 0; cy < 4; ++cy) {
         const T* row = f + (size_t(zs[cz]) * N + ys[cy]) * N;
-        double tap[4];
+        double tap[4];   // the row's loads first, so that they overlap (the push took 1.65 ms with
+                         // each load inside its sum, 1.27 ms so, at 512³ FP64 with 10⁶ tracers)
         for (int a = 0; a < 4; ++a) tap[a] = double(ldg(row + (ix + a - 1 + N) % N));
         double acc_x = 0.0;
         for (int cx = 0; cx < 4; ++cx) acc_x = add_rn(acc_x, mul_rn(wx[cx], tap[cx]));
@@ -205,8 +206,10 @@ GBGHT_HD void gatherN(const T* GBGHT_RESTRICT u, int N, double dx, double x, dou
       for (int cy = 0; cy < s.n; ++cy) {
         const int yy = ((iy + cy - off) % N + N) % N;
         const T* row = f + (size_t(zz) * N + yy) * N;
+        double tap[kStencilMax];   // the row's loads first, so that they overlap
+        for (int cx = 0; cx < s.n; ++cx) tap[cx] = double(ldg(row + ((ix + cx - off) % N + N) % N));
         double acc_x = 0.0;
-        for (int cx = 0; cx < s.n; ++cx) acc_x = add_rn(acc_x, mul_rn(wx[cx], double(ldg(row + ((ix + cx - off) % N + N) % N))));
+        for (int cx = 0; cx < s.n; ++cx) acc_x = add_rn(acc_x, mul_rn(wx[cx], tap[cx]));
         acc_y = add_rn(acc_y, mul_rn(wy[cy], acc_x));
       }
       acc_z = add_rn(acc_z, mul_rn(wz[cz], acc_y));
